@@ -1,0 +1,375 @@
+// Simulation parameters of the quasi-static slice loop, read from reference-style input keys.
+//
+// Keys, defaults and meanings follow the reference:
+//   hipace.*      Hipace.cpp:33-60, 74-244 and Hipace.H:180-300 (defaults)
+//   amr.*, geometry.*, boundary.*   Hipace.cpp:176-230, 297-391
+//   fields.*      Fields.cpp:29-47
+//   <plasma>.*    PlasmaParticleContainer.cpp:27-187, PlasmaParticleContainer.H:151-200
+//   <beam>.*      BeamParticleContainer.cpp:41-290, BeamParticleContainer.H:206-300
+// Features that the reference has but this slice loop does not implement (mesh refinement,
+// lasers, SALAME, ionization, collisions, periodic/open field boundaries, adaptive dt, openPMD
+// beams) are rejected with an explicit error instead of being silently ignored.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "inputs.hpp"
+
+namespace hpq {
+
+enum class ParticleBC : int { Reflecting = 0, Periodic = 1, Absorbing = 2 };
+
+struct PhysConst {
+    double c, ep0, mu0, q_e, m_e, m_p;
+};
+
+inline PhysConst constants_normalized() { return {1.0, 1.0, 1.0, 1.0, 1.0, 1836.15267343}; }
+inline PhysConst constants_SI() {
+    return {299792458.0, 8.8541878128e-12, 1.25663706212e-06, 1.602176634e-19,
+            9.1093837015e-31, 1.67262192369e-27};
+}
+
+struct PlasmaSpecies {
+    std::string name;
+    double charge = 0, mass = 0;
+    Expr density;             // density(x,y,z), z = c*t
+    int ppc[2] = {0, 0};
+    double u_mean[3] = {0, 0, 0};
+    double u_std[3] = {0, 0, 0};
+    double radius = 1e300;    // +inf in the reference
+    double hollow_core_radius = 0;
+    double max_qsa_weighting_factor = 35.0;
+    double min_density = 0;
+    int n_subcycles = 1;
+    bool neutralize_background = true;
+    bool prevent_centered_particle = false;
+};
+
+enum class BeamInjection : int { FixedPPC = 0, FixedWeight = 1 };
+enum class BeamProfile : int { Gaussian = 0, Flattop = 1, Can = 2 };
+
+struct BeamSpecies {
+    std::string name;
+    BeamInjection injection = BeamInjection::FixedWeight;
+    BeamProfile profile = BeamProfile::Gaussian;
+    double charge = 0, mass = 0;
+    double density = 0;              // peak density (fixed_ppc: profile density)
+    double zmin = -1e300, zmax = 1e300, radius = 1e300;
+    double position_mean[3] = {0, 0, 0};
+    double position_std[3] = {0, 0, 0};
+    int ppc[3] = {1, 1, 1};
+    double u_mean[3] = {0, 0, 0};
+    double u_std[3] = {0, 0, 0};
+    long long num_particles = 0;
+    double total_charge = 0;         // fixed_weight: Q (normalized: already divided by dV)
+    double z_foc = 0;
+    double duz_per_uz0_dzeta = 0;
+    bool do_symmetrize = false;
+    bool do_z_push = true;
+    int n_subcycles = 10;
+    double min_density = 0;
+};
+
+struct SimConfig {
+    bool normalized_units = false;
+    PhysConst pc{};
+    int n_cell[3] = {0, 0, 0};
+    double prob_lo[3] = {0, 0, 0};
+    double prob_hi[3] = {0, 0, 0};
+    double dx[3] = {0, 0, 0};
+    ParticleBC particle_bc = ParticleBC::Absorbing;
+    double particle_lo[2] = {0, 0};
+    double particle_hi[2] = {0, 0};
+    int max_step = 0;
+    double dt = 0;
+    double max_time = 1e300;
+    long long random_seed = 0;
+    bool has_random_seed = false;
+    int depos_order_xy = 2;
+    int depos_derivative_type = 2;
+    bool explicit_solver = true;
+    double mg_tol_rel = 1.e-4;
+    double mg_tol_abs = 2.2250738585072014e-308;  // numeric_limits<double>::min()
+    int mg_max_iters = 200;
+    double predcorr_B_error_tolerance = 4e-2;
+    int predcorr_max_iterations = 30;
+    double predcorr_B_mixing_factor = 0.05;
+    bool do_beam_jx_jy_deposition = true;
+    bool do_beam_jz_minus_rho = false;
+    bool deposit_rho = false;
+    std::vector<PlasmaSpecies> plasmas;
+    std::vector<BeamSpecies> beams;
+    bool any_neutralize_background() const {
+        for (auto& p : plasmas) if (p.neutralize_background) return true;
+        return false;
+    }
+};
+
+namespace detail {
+inline bool query_alt_str(const InputStore& in, const std::string& name, const std::string& alt,
+                          const std::string& key, std::string& v) {
+    return in.query_str(name + "." + key, v) || in.query_str(alt + "." + key, v);
+}
+template <class T>
+inline bool query_alt(const InputStore& in, const std::string& name, const std::string& alt,
+                      const std::string& key, T& v) {
+    return in.query(name + "." + key, v) || in.query(alt + "." + key, v);
+}
+template <class T, size_t N>
+inline bool query_alt_arr(const InputStore& in, const std::string& name, const std::string& alt,
+                          const std::string& key, T (&v)[N]) {
+    return in.query_arr(name + "." + key, v) || in.query_arr(alt + "." + key, v);
+}
+inline void reject(const InputStore& in, const std::string& key, const std::string& why) {
+    if (in.contains(key)) throw InputError("input '" + key + "' is not supported: " + why);
+}
+}  // namespace detail
+
+inline SimConfig build_config(const InputStore& in) {
+    using namespace detail;
+    SimConfig c;
+    int nu = 0;
+    in.query("hipace.normalized_units", nu);
+    c.normalized_units = nu != 0;
+    c.pc = c.normalized_units ? constants_normalized() : constants_SI();
+
+    int max_level = 0;
+    in.query("amr.max_level", max_level);
+    if (max_level != 0) throw InputError("amr.max_level > 0 (mesh refinement) is not supported");
+    in.get_arr("amr.n_cell", c.n_cell);
+    in.get_arr("geometry.prob_lo", c.prob_lo);
+    in.get_arr("geometry.prob_hi", c.prob_hi);
+    for (int d = 0; d < 3; ++d) {
+        if (c.n_cell[d] <= 0) throw InputError("amr.n_cell must be positive");
+        if (!(c.prob_hi[d] > c.prob_lo[d])) throw InputError("geometry.prob_hi must exceed prob_lo");
+        c.dx[d] = (c.prob_hi[d] - c.prob_lo[d]) / c.n_cell[d];
+    }
+    if (c.n_cell[0] % 2 != c.n_cell[1] % 2)
+        throw InputError("amr.n_cell in x and y must both be even or both be odd (multigrid)");
+
+    std::string fb;
+    if (!in.query_str("boundary.field", fb)) throw InputError("missing required input 'boundary.field'");
+    if (fb != "Dirichlet")
+        throw InputError("boundary.field = " + fb + " is not supported (only Dirichlet)");
+    std::string pb;
+    if (!in.query_str("boundary.particle", pb)) throw InputError("missing required input 'boundary.particle'");
+    if (pb == "Reflecting") c.particle_bc = ParticleBC::Reflecting;
+    else if (pb == "Periodic") c.particle_bc = ParticleBC::Periodic;
+    else if (pb == "Absorbing") c.particle_bc = ParticleBC::Absorbing;
+    else throw InputError("Unknown particle boundary '" + pb + "'");
+    c.particle_lo[0] = c.prob_lo[0]; c.particle_lo[1] = c.prob_lo[1];
+    c.particle_hi[0] = c.prob_hi[0]; c.particle_hi[1] = c.prob_hi[1];
+    in.query_arr("boundary.particle_lo", c.particle_lo);
+    in.query_arr("boundary.particle_hi", c.particle_hi);
+    if (c.particle_lo[0] < c.prob_lo[0] || c.particle_lo[1] < c.prob_lo[1] ||
+        c.particle_hi[0] > c.prob_hi[0] || c.particle_hi[1] > c.prob_hi[1])
+        throw InputError("Particle boundary must be contained within the simulation domain");
+
+    in.query("max_step", c.max_step);
+    std::string dts;
+    if (in.query_str("hipace.dt", dts)) {
+        if (dts == "adaptive") throw InputError("hipace.dt = adaptive is not supported");
+        in.query("hipace.dt", c.dt);
+    }
+    if (in.query("hipace.max_time", c.max_time)) {
+        c.max_time = std::copysign(c.max_time, c.dt);
+    }
+    if (in.query("random_seed", c.random_seed)) c.has_random_seed = true;
+
+    in.query("hipace.depos_order_xy", c.depos_order_xy);
+    if (c.depos_order_xy != 2)
+        throw InputError("hipace.depos_order_xy = " + std::to_string(c.depos_order_xy) +
+                         " is not supported (only 2)");
+    int dz_order = 0;
+    in.query("hipace.depos_order_z", dz_order);
+    if (dz_order != 0) throw InputError("hipace.depos_order_z must be 0");
+    in.query("hipace.depos_derivative_type", c.depos_derivative_type);
+    if (c.depos_derivative_type < 0 || c.depos_derivative_type > 2)
+        throw InputError("hipace.depos_derivative_type must be 0, 1 or 2");
+
+    std::string solver = "explicit";
+    in.query_str("hipace.bxby_solver", solver);
+    if (solver != "explicit" && solver != "predictor-corrector")
+        throw InputError("hipace.bxby_solver must be explicit or predictor-corrector");
+    c.explicit_solver = solver == "explicit";
+    in.query("hipace.MG_tolerance_rel", c.mg_tol_rel);
+    in.query("hipace.MG_tolerance_abs", c.mg_tol_abs);
+    in.query("hipace.predcorr_B_error_tolerance", c.predcorr_B_error_tolerance);
+    in.query("hipace.predcorr_max_iterations", c.predcorr_max_iterations);
+    in.query("hipace.predcorr_B_mixing_factor", c.predcorr_B_mixing_factor);
+    in.query_bool("hipace.do_beam_jx_jy_deposition", c.do_beam_jx_jy_deposition);
+    in.query_bool("hipace.do_beam_jz_minus_rho", c.do_beam_jz_minus_rho);
+    // diagnostics that name rho switch on its deposition (Diagnostic::needsRho)
+    for (auto& s : in.query_strs("diagnostic.field_data")) if (s == "rho") c.deposit_rho = true;
+    in.query_bool("hipace.deposit_rho", c.deposit_rho);
+
+    std::string ps = "FFTDirichletFast";
+    in.query_str("fields.poisson_solver", ps);
+    if (ps != "FFTDirichletFast" && ps != "FFTDirichletDirect" && ps != "FFTDirichletExpanded")
+        throw InputError("fields.poisson_solver = " + ps + " is not supported (Dirichlet FFT solvers only)");
+
+    reject(in, "lasers.names", "laser envelope solver is outside the slice loop");
+    reject(in, "hipace.collisions", "collisions are outside the slice loop");
+    reject(in, "hipace.use_amrex_mlmg", "the AMReX MLMG path is not part of this build");
+    reject(in, "fields.do_symmetrize", "field symmetrization is not implemented");
+    bool bb = false;
+    if (in.query_bool("hipace.interpolate_neutralizing_background", bb) && bb)
+        throw InputError("hipace.interpolate_neutralizing_background needs mesh refinement");
+
+    const PhysConst& pc = c.pc;
+    // ---------------- plasmas
+    std::vector<std::string> pnames = in.query_strs("plasmas.names");
+    if (!pnames.empty() && pnames[0] == "no_plasma") pnames.clear();
+    for (auto& name : pnames) {
+        PlasmaSpecies p;
+        p.name = name;
+        std::string element;
+        in.query_str(name + ".element", element);
+        double mass_Da = 0;
+        if (element == "electron") { p.charge = -pc.q_e; p.mass = pc.m_e; }
+        else if (element == "positron") { p.charge = pc.q_e; p.mass = pc.m_e; }
+        else if (element == "proton") { p.charge = pc.q_e; p.mass = pc.m_p; }
+        else if (!element.empty())
+            throw InputError(name + ".element = " + element + " is not supported (electron, positron, proton)");
+        if (in.query(name + ".mass_Da", mass_Da) && mass_Da != 0) p.mass = pc.m_p * mass_Da / 1.007276466621;
+        in.query(name + ".mass", p.mass);
+        if (p.mass == 0) throw InputError("The plasma particle mass must be specified");
+        in.query(name + ".charge", p.charge);
+        if (p.charge == 0) throw InputError("The plasma particle charge must be specified");
+        reject(in, name + ".can_ionize", "ionization is outside the slice loop");
+        reject(in, name + ".ionization_product", "ionization is outside the slice loop");
+        reject(in, name + ".fine_ppc", "fine plasma patches need mesh refinement");
+        reject(in, name + ".density_table_file", "density tables are not implemented");
+        reject(in, name + ".temperature_in_ev", "use u_std instead");
+        int ion_lev = -1;
+        if (in.query(name + ".initial_ion_level", ion_lev)) p.charge *= ion_lev;
+        query_alt(in, name, "plasmas", "n_subcycles", p.n_subcycles);
+        if (p.n_subcycles < 1) throw InputError("n_subcycles must be larger or equal to 1");
+        query_alt(in, name, "plasmas", "neutralize_background", p.neutralize_background);
+        std::string dens = "0.";
+        query_alt_str(in, name, "plasmas", "density(x,y,z)", dens);
+        p.density = in.function(dens, {"x", "y", "z"});
+        query_alt(in, name, "plasmas", "min_density", p.min_density);
+        query_alt(in, name, "plasmas", "radius", p.radius);
+        query_alt(in, name, "plasmas", "hollow_core_radius", p.hollow_core_radius);
+        if (!(p.hollow_core_radius < p.radius))
+            throw InputError("The hollow core plasma radius must be smaller than the plasma radius");
+        query_alt(in, name, "plasmas", "max_qsa_weighting_factor", p.max_qsa_weighting_factor);
+        if (!query_alt_arr(in, name, "plasmas", "ppc", p.ppc))
+            throw InputError("missing required input '" + name + ".ppc'");
+        in.query_arr(name + ".u_mean", p.u_mean);
+        in.query_arr(name + ".u_std", p.u_std);
+        query_alt(in, name, "plasmas", "prevent_centered_particle", p.prevent_centered_particle);
+        int reorder = 0;
+        query_alt(in, name, "plasmas", "reorder_period", reorder);  // cache locality only
+        c.plasmas.push_back(p);
+    }
+    // ---------------- beams
+    std::vector<std::string> bnames = in.query_strs("beams.names");
+    if (!bnames.empty() && bnames[0] == "no_beam") bnames.clear();
+    for (auto& name : bnames) {
+        BeamSpecies b;
+        b.name = name;
+        std::string element = "electron";
+        in.query_str(name + ".element", element);
+        if (element == "electron") { b.charge = -pc.q_e; b.mass = pc.m_e; }
+        else if (element == "proton") { b.charge = pc.q_e; b.mass = pc.m_p; }
+        else if (element == "positron") { b.charge = pc.q_e; b.mass = pc.m_e; }
+        in.query(name + ".charge", b.charge);
+        in.query(name + ".mass", b.mass);
+        if (b.mass == 0) throw InputError("The beam particle mass must not be 0");
+        std::string inj;
+        if (!in.query_str(name + ".injection_type", inj))
+            throw InputError("missing required input '" + name + ".injection_type'");
+        in.query(name + ".n_subcycles", b.n_subcycles);
+        if (b.n_subcycles < 1) throw InputError("n_subcycles must be >= 1");
+        in.query_bool(name + ".do_z_push", b.do_z_push);
+        in.query(name + ".duz_per_uz0_dzeta", b.duz_per_uz0_dzeta);
+        reject(in, name + ".do_salame", "SALAME is outside the slice loop");
+        reject(in, name + ".do_spin_tracking", "spin tracking is outside the slice loop");
+        reject(in, name + ".do_radiation_reaction", "radiation reaction is outside the slice loop");
+        reject(in, name + ".external_E(x,y,z,t)", "external fields are not implemented");
+        reject(in, name + ".external_B(x,y,z,t)", "external fields are not implemented");
+        in.query_arr(name + ".u_mean", b.u_mean);
+        in.query_arr(name + ".u_std", b.u_std);
+        std::string profile;
+        if (inj == "fixed_ppc") {
+            b.injection = BeamInjection::FixedPPC;
+            in.query_arr(name + ".ppc", b.ppc);
+            in.get(name + ".zmin", b.zmin);
+            in.get(name + ".zmax", b.zmax);
+            in.get(name + ".radius", b.radius);
+            in.query_arr(name + ".position_mean", b.position_mean);
+            in.query(name + ".min_density", b.min_density);
+            b.min_density = std::fabs(b.min_density);
+            int rnd[3] = {0, 0, 0};
+            if (in.query_arr(name + ".random_ppc", rnd) && (rnd[0] || rnd[1] || rnd[2]))
+                throw InputError(name + ".random_ppc is not supported");
+            if (!in.query_str(name + ".profile", profile))
+                throw InputError("missing required input '" + name + ".profile'");
+            if (profile == "gaussian") {
+                b.profile = BeamProfile::Gaussian;
+                in.get(name + ".density", b.density);
+                in.query_arr(name + ".position_std", b.position_std);
+            } else if (profile == "flattop") {
+                b.profile = BeamProfile::Flattop;
+                in.get(name + ".density", b.density);
+            } else {
+                throw InputError(name + ".profile = " + profile + " is not supported for fixed_ppc");
+            }
+            b.density = std::fabs(b.density);
+            if (b.duz_per_uz0_dzeta != 0.)
+                throw InputError("Tilted beams and correlated energy spreads are only implemented for fixed weight beams");
+        } else if (inj == "fixed_weight") {
+            b.injection = BeamInjection::FixedWeight;
+            profile = "gaussian";
+            in.query_str(name + ".profile", profile);
+            in.query(name + ".radius", b.radius);
+            if (profile == "can") {
+                b.profile = BeamProfile::Can;
+                in.get(name + ".zmin", b.zmin);
+                in.get(name + ".zmax", b.zmax);
+            } else if (profile == "gaussian") {
+                b.profile = BeamProfile::Gaussian;
+                in.query(name + ".zmin", b.zmin);
+                in.query(name + ".zmax", b.zmax);
+            } else {
+                throw InputError("Only gaussian and can are supported with fixed_weight beam injection");
+            }
+            std::vector<std::string> pm = in.query_strs(name + ".position_mean");
+            if (pm.size() != 3) throw InputError(name + ".position_mean expects 3 values");
+            for (int d = 0; d < 3; ++d) {
+                Expr e = in.function(pm[d], {"z"});
+                if (!e.is_constant())
+                    throw InputError(name + ".position_mean depending on z is not supported");
+                b.position_mean[d] = e.eval(nullptr);
+            }
+            in.get_arr(name + ".position_std", b.position_std);
+            in.get(name + ".num_particles", b.num_particles);
+            in.query(name + ".z_foc", b.z_foc);
+            bool has_q = in.query(name + ".total_charge", b.total_charge);
+            bool has_n = in.query(name + ".density", b.density);
+            if (has_q && c.normalized_units)
+                throw InputError("The option 'beam.total_charge' is only valid in SI units.");
+            if ((int)has_q + (int)has_n != 1)
+                throw InputError("Please specify exlusively either total_charge or density of the beam");
+            in.query_bool(name + ".do_symmetrize", b.do_symmetrize);
+            if (b.do_symmetrize && b.num_particles % 4 != 0)
+                throw InputError("To symmetrize the beam, please specify a beam particle number divisible by 4.");
+            // total charge from the peak density (BeamParticleContainer.cpp:179-190)
+            if (has_n) {
+                b.total_charge = b.density * b.charge;
+                for (int d = 0; d < 3; ++d) b.total_charge *= b.position_std[d] * std::sqrt(2. * 3.14159265358979323846);
+            }
+            if (c.normalized_units) b.total_charge *= 1.0 / (c.dx[0] * c.dx[1] * c.dx[2]);
+        } else {
+            throw InputError(name + ".injection_type = " + inj +
+                             " is not supported (fixed_ppc, fixed_weight)");
+        }
+        c.beams.push_back(b);
+    }
+    return c;
+}
+
+}  // namespace hpq

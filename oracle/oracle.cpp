@@ -1,0 +1,1280 @@
+// ORACLE — test infrastructure only. Not part of the product and never linked into it.
+//
+// A plain FP64 CPU restatement of HiPACE++'s quasi-static slice loop (explicit and
+// predictor-corrector Bx/By solvers, Dirichlet fields, transverse shape order 2), used by the
+// tests to check the CUDA implementation and by bench.py as the timed CPU baseline.
+// Each routine cites the reference file:line it restates. Only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline leg load this library.
+//
+// The reference itself (AMReX + FFTW + MPI) cannot be built here; parity of this oracle is
+// pinned instead against the reference's own checksum goldens
+// (tests/checksum/benchmarks_json/*.json), see tests/test_oracle_golden.py.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../hipace2_b200/csrc/config.hpp"
+
+using hpq::SimConfig;
+
+namespace oracle {
+
+// ------------------------------------------------------------------------------------------
+// Shape factors (ShapeFactors.H:122-171 order 2, :212-468 derivative shapes)
+// ------------------------------------------------------------------------------------------
+struct Shape { double s; int cell; };
+struct DShape { double s, ds; int cell; };
+
+static inline Shape shape2(double xmid, int ix) {
+    const double xfloor = std::floor(xmid + 0.5);
+    const double xint = xmid - xfloor;
+    if (ix == 0) return {0.5 * (0.5 - xint) * (0.5 - xint), (int)xfloor - 1};
+    if (ix == 1) return {0.75 - xint * xint, (int)xfloor};
+    return {0.5 * (0.5 + xint) * (0.5 + xint), (int)xfloor + 1};
+}
+
+// derivative shapes for order 2; returns {s_x, -sdx, cell} like the reference
+static inline DShape dshape2(int type, double xmid, int ix) {
+    if (type == 0) {
+        xmid += 0.5;
+        const double xfloor = std::floor(xmid);
+        const double xint = xmid - xfloor, x2 = xint * xint;
+        if (ix == 0) return {0.5 * x2 - 1.0 * xint + 0.5, -(xint - 1.0), (int)xfloor - 1 + ix};
+        if (ix == 1) return {-x2 + 1.0 * xint + 0.5, -(1.0 - 2 * xint), (int)xfloor - 1 + ix};
+        return {0.5 * x2, -xint, (int)xfloor - 1 + ix};
+    } else if (type == 1) {
+        const double xfloor = std::floor(xmid);
+        const double xint = xmid - xfloor, x2 = xint * xint;
+        const bool lo = xint < 0.5;
+        if (ix == 0) return {lo ? 0.5 * x2 - 0.5 * xint + 1.0 / 8.0 : 0,
+                             -(-0.5 * x2 + xint - 0.5), (int)xfloor - 1 + ix};
+        if (ix == 1) return {lo ? 3.0 / 4.0 - x2 : 0.5 * x2 - 1.5 * xint + 9.0 / 8.0,
+                             -(1.5 * x2 - 2 * xint), (int)xfloor - 1 + ix};
+        if (ix == 2) return {lo ? 0.5 * x2 + 0.5 * xint + 1.0 / 8.0 : -x2 + 2 * xint - 1.0 / 4.0,
+                             -(-1.5 * x2 + xint + 0.5), (int)xfloor - 1 + ix};
+        return {lo ? 0 : 0.5 * x2 - 0.5 * xint + 1.0 / 8.0, -(0.5 * x2), (int)xfloor - 1 + ix};
+    } else {
+        xmid += 0.5;
+        const double xfloor = std::floor(xmid);
+        const double xint = xmid - xfloor, x2 = xint * xint;
+        if (ix == 0) return {0, -(-0.25 * x2 + 0.5 * xint - 0.25), (int)xfloor - 2 + ix};
+        if (ix == 1) return {0.5 * x2 - xint + 0.5, -(0.5 * x2 - 0.5 * xint - 0.25), (int)xfloor - 2 + ix};
+        if (ix == 2) return {-x2 + xint + 0.5, -(0.25 - 0.5 * xint), (int)xfloor - 2 + ix};
+        if (ix == 3) return {0.5 * x2, -(-0.5 * x2 + 0.5 * xint + 0.25), (int)xfloor - 2 + ix};
+        return {0, -(0.25 * x2), (int)xfloor - 2 + ix};
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Slice field storage: nx x ny interior plus guard cells (the reference uses
+// (depos_order+1)/2+1 = 2 guards, Fields.cpp:63; one more is allocated so that stencils that
+// touch a zero-weight cell beyond the guard stay in bounds).
+// ------------------------------------------------------------------------------------------
+struct Grid {
+    int nx, ny, g;
+    int px;  // pitch
+    size_t size() const { return (size_t)(nx + 2 * g) * (ny + 2 * g); }
+    size_t idx(int i, int j) const { return (size_t)(j + g) * px + (i + g); }
+};
+
+struct Field {
+    std::vector<double> a;
+    Grid gr;
+    void init(const Grid& g) { gr = g; a.assign(g.size(), 0.0); }
+    double& operator()(int i, int j) { return a[gr.idx(i, j)]; }
+    double operator()(int i, int j) const { return a[gr.idx(i, j)]; }
+    void zero() { std::fill(a.begin(), a.end(), 0.0); }
+};
+
+struct Plasma {
+    std::vector<double> x, y, w, ux, uy, psi, x_prev, y_prev, ux_h, uy_h, psi_h;
+    std::vector<uint8_t> valid;
+    size_t n() const { return x.size(); }
+};
+
+struct BeamParticle {
+    double x, y, z, w, ux, uy, uz;
+    int64_t id;
+    int nsub;
+    bool valid;
+};
+
+struct BeamSlice {
+    std::vector<BeamParticle> p;
+    size_t num_nonslipped = 0;
+};
+
+// ------------------------------------------------------------------------------------------
+// Dirichlet Poisson solver: DST-I in x and y, eigenvalue divide, DST-I back
+// (FFTPoissonSolverDirichletFast.cpp:196-328; FFTW RODFT00 in FFTPoissonSolverDirichletDirect).
+// Restated with an explicit sine matrix; normalisation 1/(4(nx+1)(ny+1)) of two unnormalised
+// RODFT00 transforms per axis is folded into the eigenvalues.
+// ------------------------------------------------------------------------------------------
+struct PoissonDST {
+    int nx = 0, ny = 0;
+    std::vector<double> sx, sy, eig;  // sine matrices (n x n) and eigenvalues (ny x nx)
+    void init(int nx_, int ny_, double dx, double dy) {
+        nx = nx_; ny = ny_;
+        const double pi = 3.14159265358979323846;
+        sx.resize((size_t)nx * nx);
+        sy.resize((size_t)ny * ny);
+        for (int i = 0; i < nx; ++i)
+            for (int k = 0; k < nx; ++k) sx[(size_t)i * nx + k] = 2.0 * std::sin(pi * (i + 1) * (k + 1) / (nx + 1));
+        for (int i = 0; i < ny; ++i)
+            for (int k = 0; k < ny; ++k) sy[(size_t)i * ny + k] = 2.0 * std::sin(pi * (i + 1) * (k + 1) / (ny + 1));
+        const double sxf = pi / (2. * (nx + 1)), syf = pi / (2. * (ny + 1));
+        const double norm = 0.5 / (2 * ((nx + 1) * (ny + 1)));
+        eig.resize((size_t)nx * ny);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double a = std::sin((i + 1) * sxf), b = std::sin((j + 1) * syf);
+                a *= a; b *= b;
+                eig[(size_t)j * nx + i] = (a != 0 && b != 0) ? norm / (-4.0 * (a / (dx * dx) + b / (dy * dy))) : 0.0;
+            }
+    }
+    // in/out: row-major ny x nx
+    void transform_x(std::vector<double>& v) const {
+        std::vector<double> out(v.size());
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nx; ++k) {
+                double s = 0;
+                const double* row = &v[(size_t)j * nx];
+                const double* m = &sx[(size_t)k * nx];
+                for (int i = 0; i < nx; ++i) s += row[i] * m[i];
+                out[(size_t)j * nx + k] = s;
+            }
+        v.swap(out);
+    }
+    void transform_y(std::vector<double>& v) const {
+        std::vector<double> out(v.size(), 0.0);
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < ny; ++k) {
+            double* o = &out[(size_t)k * nx];
+            for (int j = 0; j < ny; ++j) {
+                const double m = sy[(size_t)k * ny + j];
+                const double* row = &v[(size_t)j * nx];
+                for (int i = 0; i < nx; ++i) o[i] += m * row[i];
+            }
+        }
+        v.swap(out);
+    }
+    void solve(std::vector<double>& v) const {
+        transform_x(v);
+        transform_y(v);
+        for (size_t k = 0; k < v.size(); ++k) v[k] *= eig[k];
+        transform_y(v);
+        transform_x(v);
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+// Geometric multigrid for -a*u + Lap(u) = f, two components sharing a (HpMultiGrid.cpp,
+// system type 1). Cell-centred levels when n is even (Dirichlet on the cell face, 4/3 closure
+// :162-183, 265-294), node-centred otherwise (Dirichlet on the first guard node, :1054-1066).
+// ------------------------------------------------------------------------------------------
+struct MGLevel {
+    int lo_i, hi_i, lo_j, hi_j;  // full box (cell: 0..n-1; node: 0..N+1)
+    int vlo_i, vhi_i, vlo_j, vhi_j;  // valid loop box
+    int w, h;
+    std::vector<double> acf, res[2], cor[2], rescor[2];
+    size_t id(int i, int j) const { return (size_t)(j - lo_j) * w + (i - lo_i); }
+};
+
+struct Multigrid {
+    bool cell = true;
+    double dx = 0, dy = 0;
+    std::vector<MGLevel> L;
+    int total_vcycles = 0;
+
+    void init(int nx, int ny, double dx_, double dy_) {
+        dx = dx_; dy = dy_;
+        cell = (nx % 2 == 0);
+        L.clear();
+        int lx, ly;  // box bounds
+        if (cell) { lx = nx - 1; ly = ny - 1; } else { lx = nx + 1; ly = ny + 1; }
+        for (int lev = 0; lev < 40; ++lev) {
+            MGLevel m;
+            m.lo_i = 0; m.lo_j = 0; m.hi_i = lx; m.hi_j = ly;
+            m.w = lx + 1; m.h = ly + 1;
+            if (cell) { m.vlo_i = 0; m.vlo_j = 0; m.vhi_i = lx; m.vhi_j = ly; }
+            else { m.vlo_i = 1; m.vlo_j = 1; m.vhi_i = lx - 1; m.vhi_j = ly - 1; }
+            const size_t n = (size_t)m.w * m.h;
+            m.acf.assign(n, 0.0);
+            for (int c = 0; c < 2; ++c) { m.res[c].assign(n, 0.0); m.cor[c].assign(n, 0.0); m.rescor[c].assign(n, 0.0); }
+            L.push_back(std::move(m));
+            // coarsenable with min width 2 (cell) or 4 (node)  (HpMultiGrid.cpp:1067-1074)
+            const int len_x = lx + 1, len_y = ly + 1;
+            const int minw = cell ? 2 : 4;
+            if (len_x < 2 * minw || len_y < 2 * minw) break;
+            if (cell) {
+                if (len_x % 2 || len_y % 2) break;
+                lx = len_x / 2 - 1; ly = len_y / 2 - 1;
+            } else {
+                if (lx % 2 || ly % 2) break;
+                lx = lx / 2; ly = ly / 2;
+            }
+        }
+    }
+
+    static inline double lap(const MGLevel& m, const std::vector<double>& p, int i, int j,
+                             double facx, double facy, bool cellc) {
+        double l = -2.0 * (facx + facy) * p[m.id(i, j)];
+        if (cellc && i == m.lo_i) l += facx * (4. / 3. * p[m.id(i + 1, j)] - 2. * p[m.id(i, j)]);
+        else if (cellc && i == m.hi_i) l += facx * (4. / 3. * p[m.id(i - 1, j)] - 2. * p[m.id(i, j)]);
+        else l += facx * (p[m.id(i - 1, j)] + p[m.id(i + 1, j)]);
+        if (cellc && j == m.lo_j) l += facy * (4. / 3. * p[m.id(i, j + 1)] - 2. * p[m.id(i, j)]);
+        else if (cellc && j == m.hi_j) l += facy * (4. / 3. * p[m.id(i, j - 1)] - 2. * p[m.id(i, j)]);
+        else l += facy * (p[m.id(i, j - 1)] + p[m.id(i, j + 1)]);
+        return l;
+    }
+    // gs1 (HpMultiGrid.cpp:265-294)
+    static inline void gs(const MGLevel& m, std::vector<double>& p, int i, int j, double rhs, double a,
+                          double facx, double facy, bool cellc) {
+        double l;
+        double c0 = -(a + 2. * (facx + facy));
+        if (cellc && i == m.lo_i) { l = facx * (4. / 3.) * p[m.id(i + 1, j)]; c0 -= 2. * facx; }
+        else if (cellc && i == m.hi_i) { l = facx * (4. / 3.) * p[m.id(i - 1, j)]; c0 -= 2. * facx; }
+        else l = facx * (p[m.id(i - 1, j)] + p[m.id(i + 1, j)]);
+        if (cellc && j == m.lo_j) { l += facy * (4. / 3.) * p[m.id(i, j + 1)]; c0 -= 2. * facy; }
+        else if (cellc && j == m.hi_j) { l += facy * (4. / 3.) * p[m.id(i, j - 1)]; c0 -= 2. * facy; }
+        else l += facy * (p[m.id(i, j - 1)] + p[m.id(i, j + 1)]);
+        const double c0_inv = 1. / c0;
+        p[m.id(i, j)] = (rhs - l) * c0_inv;
+    }
+    // gsrb_4_residual (HpMultiGrid.cpp:697-850): phi_out = 4 red-black colour sweeps starting
+    // from phi_in (or zero), then optionally res_out = rhs - L(phi_out).
+    void smooth4(int lev, std::vector<double>* phi_out, std::vector<double>* const* rhs,
+                 const std::vector<double>* const* phi_in, std::vector<double>* const* res_out,
+                 int nsweeps = 4) {
+        MGLevel& m = L[lev];
+        const double f = (double)(1 << lev);
+        const double ddx = dx * f, ddy = dy * f;
+        const double facx = 1. / (ddx * ddx), facy = 1. / (ddy * ddy);
+        for (int c = 0; c < 2; ++c) {
+            std::vector<double>& p = phi_out[c];
+            for (int j = m.lo_j; j <= m.hi_j; ++j)
+                for (int i = m.lo_i; i <= m.hi_i; ++i) {
+                    const bool v = i >= m.vlo_i && i <= m.vhi_i && j >= m.vlo_j && j <= m.vhi_j;
+                    p[m.id(i, j)] = (v && phi_in) ? (*phi_in[c])[m.id(i, j)] : 0.0;
+                }
+        }
+        for (int is = 0; is < nsweeps; ++is) {
+            for (int c = 0; c < 2; ++c) {
+                std::vector<double>& p = phi_out[c];
+                const std::vector<double>& r = *rhs[c];
+#pragma omp parallel for schedule(static)
+                for (int j = m.vlo_j; j <= m.vhi_j; ++j)
+                    for (int i = m.vlo_i; i <= m.vhi_i; ++i)
+                        if ((i + j + is) % 2 == 0) gs(m, p, i, j, r[m.id(i, j)], m.acf[m.id(i, j)], facx, facy, cell);
+            }
+        }
+        if (res_out) {
+            for (int c = 0; c < 2; ++c) {
+                const std::vector<double>& p = phi_out[c];
+                const std::vector<double>& r = *rhs[c];
+                std::vector<double>& o = *res_out[c];
+#pragma omp parallel for schedule(static)
+                for (int j = m.vlo_j; j <= m.vhi_j; ++j)
+                    for (int i = m.vlo_i; i <= m.vhi_i; ++i) {
+                        const size_t k = m.id(i, j);
+                        o[k] = r[k] + m.acf[k] * p[k] - lap(m, p, i, j, facx, facy, cell);
+                    }
+            }
+        }
+    }
+    // restrict_cc / restrict_nd (HpMultiGrid.cpp:29-53)
+    void restrict_to(int lev_c, const std::vector<double>& fine, std::vector<double>& crse) {
+        const MGLevel& C = L[lev_c];
+        const MGLevel& F = L[lev_c - 1];
+        for (int j = C.vlo_j; j <= C.vhi_j; ++j)
+            for (int i = C.vlo_i; i <= C.vhi_i; ++i) {
+                if (cell) {
+                    crse[C.id(i, j)] = 0.25 * (fine[F.id(2 * i, 2 * j)] + fine[F.id(2 * i + 1, 2 * j)] +
+                                               fine[F.id(2 * i, 2 * j + 1)] + fine[F.id(2 * i + 1, 2 * j + 1)]);
+                } else {
+                    crse[C.id(i, j)] = (1. / 16.) * (fine[F.id(2 * i - 1, 2 * j - 1)] + 2. * fine[F.id(2 * i, 2 * j - 1)] +
+                                                     fine[F.id(2 * i + 1, 2 * j - 1)] + 2. * fine[F.id(2 * i - 1, 2 * j)] +
+                                                     4. * fine[F.id(2 * i, 2 * j)] + 2. * fine[F.id(2 * i + 1, 2 * j)] +
+                                                     fine[F.id(2 * i - 1, 2 * j + 1)] + 2. * fine[F.id(2 * i, 2 * j + 1)] +
+                                                     fine[F.id(2 * i + 1, 2 * j + 1)]);
+                }
+            }
+    }
+    // interpcpy_cc / interpcpy_nd (HpMultiGrid.cpp:79-120): out = fine_in + I(crse)
+    void interp_add(int lev_f, const std::vector<double>& fin, const std::vector<double>& crse,
+                    std::vector<double>& out) {
+        const MGLevel& F = L[lev_f];
+        const MGLevel& C = L[lev_f + 1];
+        auto cdiv = [](int i) { return i >= 0 ? i / 2 : -((-i + 1) / 2); };
+        for (int j = F.vlo_j; j <= F.vhi_j; ++j)
+            for (int i = F.vlo_i; i <= F.vhi_i; ++i) {
+                const int ic = cdiv(i), jc = cdiv(j);
+                const size_t k = F.id(i, j);
+                if (cell) { out[k] = fin[k] + crse[C.id(ic, jc)]; continue; }
+                const bool io = ic * 2 != i, jo = jc * 2 != j;
+                if (io && jo) out[k] = fin[k] + (crse[C.id(ic, jc)] + crse[C.id(ic + 1, jc)] + crse[C.id(ic, jc + 1)] + crse[C.id(ic + 1, jc + 1)]) * 0.25;
+                else if (io) out[k] = fin[k] + (crse[C.id(ic, jc)] + crse[C.id(ic + 1, jc)]) * 0.5;
+                else if (jo) out[k] = fin[k] + (crse[C.id(ic, jc)] + crse[C.id(ic, jc + 1)]) * 0.5;
+                else out[k] = fin[k] + crse[C.id(ic, jc)];
+            }
+    }
+
+    // one V-cycle (HpMultiGrid.cpp:1429-1512 with the bottom solve :1514-1595)
+    void vcycle(std::vector<double>* sol, std::vector<double>* const* rhs0) {
+        const int nl = (int)L.size();
+        for (int lev = 0; lev < nl - 1; ++lev) {
+            if (lev > 0) {
+                std::vector<double>* r[2] = {&L[lev].res[0], &L[lev].res[1]};
+                std::vector<double>* o[2] = {&L[lev].rescor[0], &L[lev].rescor[1]};
+                smooth4(lev, L[lev].cor, r, nullptr, o);
+            }
+            for (int c = 0; c < 2; ++c) restrict_to(lev + 1, L[lev].rescor[c], L[lev + 1].res[c]);
+        }
+        {   // bottom: zero initial guess, 16 sweeps
+            const int lev = nl - 1;
+            std::vector<double>* r[2] = {&L[lev].res[0], &L[lev].res[1]};
+            const int len = std::max(L[lev].w, L[lev].h);
+            const int ns = std::max(16, (len + 1) / 2 * 2);
+            smooth4(lev, L[lev].cor, r, nullptr, nullptr, ns);
+        }
+        for (int lev = nl - 2; lev >= 0; --lev) {
+            for (int c = 0; c < 2; ++c) interp_add(lev, L[lev].cor[c], L[lev + 1].cor[c], L[lev].rescor[c]);
+            const std::vector<double>* in[2] = {&L[lev].rescor[0], &L[lev].rescor[1]};
+            if (lev == 0) {
+                smooth4(0, sol, rhs0, in, nullptr);
+            } else {
+                std::vector<double>* r[2] = {&L[lev].res[0], &L[lev].res[1]};
+                smooth4(lev, L[lev].cor, r, in, nullptr);
+            }
+        }
+        const std::vector<double>* in[2] = {&sol[0], &sol[1]};
+        std::vector<double>* o[2] = {&L[0].rescor[0], &L[0].rescor[1]};
+        smooth4(0, L[0].cor, rhs0, in, o);
+        total_vcycles++;
+    }
+
+    double maxabs_valid(int lev, const std::vector<double>* a) const {
+        const MGLevel& m = L[lev];
+        double r = 0;
+        for (int c = 0; c < 2; ++c)
+            for (int j = m.vlo_j; j <= m.vhi_j; ++j)
+                for (int i = m.vlo_i; i <= m.vhi_i; ++i) r = std::max(r, std::fabs(a[c][m.id(i, j)]));
+        return r;
+    }
+
+    // solve1 + solve_doit (HpMultiGrid.cpp:1169-1427). Field layout: cell (i,j) of the slice maps
+    // to MG index (i,j) for cell-centred and (i+1,j+1) for node-centred levels.
+    // Returns 0 on success, 1 if not converged within maxiter, 2 on divergence.
+    int solve(Field& Bx, Field& By, const Field& Sy, const Field& Sx, const Field& chi,
+              double tol_rel, double tol_abs, int maxiter, int* iters_out) {
+        MGLevel& m0 = L[0];
+        const int off = cell ? 0 : 1;
+        auto map_in = [&](const Field& f, std::vector<double>& dst) {
+            for (int j = m0.lo_j; j <= m0.hi_j; ++j)
+                for (int i = m0.lo_i; i <= m0.hi_i; ++i) dst[m0.id(i, j)] = f(i - off, j - off);
+        };
+        map_in(chi, m0.acf);
+        // average_down_acoef (HpMultiGrid.cpp:1640-1700)
+        for (size_t lev = 1; lev < L.size(); ++lev) restrict_to((int)lev, L[lev - 1].acf, L[lev].acf);
+        std::vector<double> sol[2], rhs[2];
+        for (int c = 0; c < 2; ++c) { sol[c].assign(m0.acf.size(), 0.0); rhs[c].assign(m0.acf.size(), 0.0); }
+        map_in(Bx, sol[0]); map_in(By, sol[1]);
+        map_in(Sy, rhs[0]); map_in(Sx, rhs[1]);
+        std::vector<double>* rp[2] = {&rhs[0], &rhs[1]};
+        const std::vector<double>* sp[2] = {&sol[0], &sol[1]};
+        std::vector<double>* op[2] = {&m0.rescor[0], &m0.rescor[1]};
+        smooth4(0, m0.cor, rp, sp, op);
+        const double resnorm0 = maxabs_valid(0, m0.rescor);
+        const double rhsnorm0 = maxabs_valid(0, rhs);
+        const double max_norm = (rhsnorm0 >= resnorm0) ? rhsnorm0 : resnorm0;
+        const double res_target = std::max(tol_abs, std::max(tol_rel, 1.e-16) * max_norm);
+        int status = 0, it = 0;
+        if (!(resnorm0 <= res_target)) {
+            bool converged = false;
+            for (int iter = 0; iter < maxiter; ++iter) {
+                vcycle(sol, rp);
+                it = iter + 1;
+                const double norminf = maxabs_valid(0, m0.rescor);
+                converged = norminf <= res_target;
+                if (converged) break;
+                if (norminf > 1.e20 * max_norm) { status = 2; break; }
+            }
+            if (!converged && status == 0) status = 1;
+        }
+        if (iters_out) *iters_out = it;
+        for (int j = m0.vlo_j; j <= m0.vhi_j; ++j)
+            for (int i = m0.vlo_i; i <= m0.vhi_i; ++i) {
+                Bx(i - off, j - off) = m0.cor[0][m0.id(i, j)];
+                By(i - off, j - off) = m0.cor[1][m0.id(i, j)];
+            }
+        return status;
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+// The simulation
+// ------------------------------------------------------------------------------------------
+class Sim {
+public:
+    SimConfig cfg;
+    Grid gr{};
+    int nx = 0, ny = 0, nz = 0;
+    double dx = 0, dy = 0, dz = 0, dxi = 0, dyi = 0, dzi = 0;
+    double xoff = 0, yoff = 0;  // GetPosOffset for the guarded slice box
+    std::map<std::string, Field> F;
+    std::vector<Plasma> plasmas;
+    // beams: per beam, per slice storage for the next step
+    std::vector<std::vector<BeamSlice>> store;
+    std::vector<BeamSlice> bthis, bnext;
+    std::vector<bool> store_valid;
+    PoissonDST dst;
+    Multigrid mg;
+    double physical_time = 0;
+    std::string error;
+    int mg_status = 0;
+    long long mg_iters_total = 0;
+    // diagnostics: requested components, 3-D arrays (nz x ny x nx) for the last solved step
+    std::vector<std::string> diag_names;
+    std::map<std::string, std::vector<double>> diag;
+    std::vector<double> pc_errors;
+
+    explicit Sim(const SimConfig& c) : cfg(c) {
+        nx = c.n_cell[0]; ny = c.n_cell[1]; nz = c.n_cell[2];
+        dx = (c.prob_hi[0] - c.prob_lo[0]) / nx;
+        dy = (c.prob_hi[1] - c.prob_lo[1]) / ny;
+        dz = (c.prob_hi[2] - c.prob_lo[2]) / nz;
+        dxi = 1. / dx; dyi = 1. / dy; dzi = 1. / dz;
+        gr.nx = nx; gr.ny = ny; gr.g = 3; gr.px = nx + 2 * gr.g;
+        // GetPosOffset with the 2-guard slice box (Fields.H:72-76)
+        xoff = 0.5 * (c.prob_lo[0] + c.prob_hi[0] - dx * ((-2) + (nx + 1)));
+        yoff = 0.5 * (c.prob_lo[1] + c.prob_hi[1] - dy * ((-2) + (ny + 1)));
+        const char* names_explicit[] = {
+            "chi", "Sy", "Sx", "ExmBy", "EypBx", "Ez", "Bx", "By", "Bz", "Psi", "jx_beam", "jy_beam",
+            "jz_beam", "jx", "jy", "rhomjz", "rho", "rhomjz_beam", "Next.jx_beam", "Next.jy_beam",
+            "Prev.jx_beam", "Prev.jy_beam", "Ions.rhomjz"};
+        const char* names_pc[] = {
+            "ExmBy", "EypBx", "Ez", "Bx", "By", "Bz", "Psi", "jx", "jy", "jz", "rhomjz", "rho",
+            "Next.jx", "Next.jy", "Prev.Bx", "Prev.By", "Prev.jx", "Prev.jy", "PCIter.Bx",
+            "PCIter.By", "PCPrevIter.Bx", "PCPrevIter.By", "Ions.rhomjz"};
+        if (c.explicit_solver) for (auto* n : names_explicit) F[n].init(gr);
+        else for (auto* n : names_pc) F[n].init(gr);
+        dst.init(nx, ny, dx, dy);
+        if (c.explicit_solver) mg.init(nx, ny, dx, dy);
+        store.resize(c.beams.size());
+        for (auto& s : store) s.resize(nz);
+        store_valid.assign(c.beams.size(), false);
+        bthis.resize(c.beams.size());
+        bnext.resize(c.beams.size());
+    }
+
+    Field& f(const char* n) { return F.at(n); }
+
+    // -------------------------------------------------------------- beam initialisation
+    // BoxSort.cpp:14-78: slice = int((z - plo_z) * dzi); outside [0, nz) is dropped. Within a
+    // slice the input order is kept.
+    void set_beam(int b, const double* x, const double* y, const double* z, const double* w,
+                  const double* ux, const double* uy, const double* uz, const int64_t* id, int64_t n) {
+        auto& st = store[b];
+        for (auto& s : st) { s.p.clear(); s.num_nonslipped = 0; }
+        for (int64_t i = 0; i < n; ++i) {
+            int s = (int)((z[i] - cfg.prob_lo[2]) * dzi);
+            if (s < 0 || s >= nz) continue;
+            BeamParticle p{x[i], y[i], z[i], w[i], ux[i], uy[i], uz[i], id ? id[i] : (int64_t)(i + 1), 0, true};
+            if (p.w == 0.0) p.valid = false;
+            st[s].p.push_back(p);
+        }
+        for (auto& s : st) s.num_nonslipped = s.p.size();
+        store_valid[b] = true;
+    }
+
+    // InitBeamFixedPPCSlice (BeamParticleContainerInit.cpp:199-345) for all slices at once
+    void init_beam_fixed_ppc(int b) {
+        const hpq::BeamSpecies& B = cfg.beams[b];
+        auto& st = store[b];
+        const int nppc = B.ppc[0] * B.ppc[1] * B.ppc[2];
+        const double scale = cfg.normalized_units ? 1. / nppc : dx * dy * dz / nppc;
+        int64_t pid = 1;
+        for (int k = 0; k < nz; ++k) {
+            BeamSlice& s = st[k];
+            s.p.clear();
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                    for (int ip = 0; ip < nppc; ++ip) {
+                        const int nyp = B.ppc[1], nzp = B.ppc[2];
+                        const int ixp = ip / (nyp * nzp);
+                        const int iyp = (ip % (nyp * nzp)) % nyp;
+                        const int izp = (ip % (nyp * nzp)) / nyp;
+                        const double r0 = (0.5 + ixp) / B.ppc[0], r1 = (0.5 + iyp) / B.ppc[1], r2 = (0.5 + izp) / B.ppc[2];
+                        const double x = cfg.prob_lo[0] + (i + r0) * dx;
+                        const double y = cfg.prob_lo[1] + (j + r1) * dy;
+                        const double z = cfg.prob_lo[2] + (k + r2) * dz;
+                        if (z >= B.zmax || z < B.zmin ||
+                            ((x - B.position_mean[0]) * (x - B.position_mean[0]) + (y - B.position_mean[1]) * (y - B.position_mean[1])) > B.radius * B.radius)
+                            continue;
+                        double dens;
+                        if (B.profile == hpq::BeamProfile::Gaussian) {
+                            const double ddx = (x - B.position_mean[0]) / B.position_std[0];
+                            const double ddy = (y - B.position_mean[1]) / B.position_std[1];
+                            const double ddz = (z - B.position_mean[2]) / B.position_std[2];
+                            dens = B.density * std::exp(-0.5 * ddx * ddx) * std::exp(-0.5 * ddy * ddy) * std::exp(-0.5 * ddz * ddz);
+                        } else {
+                            dens = B.density;
+                        }
+                        if (dens <= B.min_density) continue;
+                        BeamParticle p{};
+                        double xp = x, yp = y;
+                        double uxp = B.u_mean[0] * cfg.pc.c, uyp = B.u_mean[1] * cfg.pc.c;
+                        bool valid = enforce_bc(xp, yp, uxp, uyp);
+                        p.x = xp; p.y = yp; p.z = z;
+                        p.ux = uxp; p.uy = uyp; p.uz = B.u_mean[2] * cfg.pc.c;
+                        p.w = valid ? std::fabs(dens * scale) : 0.0;
+                        p.id = pid++;
+                        p.nsub = 0;
+                        p.valid = valid;
+                        s.p.push_back(p);
+                    }
+            s.num_nonslipped = s.p.size();
+        }
+        store_valid[b] = true;
+    }
+
+    // EnforceBC (GetAndSetPosition.H:29-99); returns false if the particle is absorbed
+    bool enforce_bc(double& x, double& y, double& ux, double& uy) const {
+        const double plo0 = cfg.particle_lo[0], plo1 = cfg.particle_lo[1];
+        const double phi0 = cfg.particle_hi[0], phi1 = cfg.particle_hi[1];
+        if (x < plo0 || y < plo1 || x > phi0 || y > phi1) {
+            const double lx = phi0 - plo0, ly = phi1 - plo1;
+            if (cfg.particle_bc == hpq::ParticleBC::Reflecting) {
+                x = std::fmod(x - plo0, 2 * lx); if (x < 0) x += 2 * lx; x += plo0;
+                if (x > phi0) { x = 2 * phi0 - x; ux = -ux; }
+                y = std::fmod(y - plo1, 2 * ly); if (y < 0) y += 2 * ly; y += plo1;
+                if (y > phi1) { y = 2 * phi1 - y; uy = -uy; }
+                return true;
+            } else if (cfg.particle_bc == hpq::ParticleBC::Periodic) {
+                x = std::fmod(x - plo0, lx); if (x < 0) x += lx; x += plo0;
+                y = std::fmod(y - plo1, ly); if (y < 0) y += ly; y += plo1;
+                return true;
+            }
+            return false;
+        }
+        return true;
+    }
+
+    // -------------------------------------------------------------- plasma initialisation
+    // PlasmaParticleContainerInit.cpp:17-310 (no fine patch, no symmetrize). Particle order:
+    // loop over i_part outside, cells in x-fastest order inside.
+    void init_plasmas() {
+        plasmas.assign(cfg.plasmas.size(), Plasma{});
+        const double c_t = cfg.pc.c * physical_time;
+        for (size_t s = 0; s < cfg.plasmas.size(); ++s) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[s];
+            Plasma& pl = plasmas[s];
+            const int nppc = P.ppc[0] * P.ppc[1];
+            const double scale = nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : dx * dy * dz / nppc);
+            int ilo = 0, ihi = nx - 1, jlo = 0, jhi = ny - 1;
+            double xo = 0, yo = 0;
+            if (P.prevent_centered_particle) {
+                if (nx % 2 == 1 && P.ppc[0] % 2 == 1) { ilo = 1; ihi = nx - 1; xo = -0.5; }
+                if (ny % 2 == 1 && P.ppc[1] % 2 == 1) { jlo = 1; jhi = ny - 1; yo = -0.5; }
+            }
+            if (P.radius < 1e299) {
+                ilo = std::max(ilo, (int)std::round((-P.radius - cfg.prob_lo[0]) / dx - 2));
+                jlo = std::max(jlo, (int)std::round((-P.radius - cfg.prob_lo[1]) / dy - 2));
+                ihi = std::min(ihi, (int)std::round((P.radius - cfg.prob_lo[0]) / dx + 2));
+                jhi = std::min(jhi, (int)std::round((P.radius - cfg.prob_lo[1]) / dy + 2));
+            }
+            for (int ip = 0; ip < nppc; ++ip) {
+                const int ixp = ip % P.ppc[0], iyp = ip / P.ppc[0];
+                const double r0 = (0.5 + ixp) / P.ppc[0], r1 = (0.5 + iyp) / P.ppc[1];
+                for (int j = jlo; j <= jhi; ++j)
+                    for (int i = ilo; i <= ihi; ++i) {
+                        const double x = cfg.prob_lo[0] + (i + r0 + xo) * dx;
+                        const double y = cfg.prob_lo[1] + (j + r1 + yo) * dy;
+                        const double rsq = x * x + y * y;
+                        double v[3] = {x, y, c_t};
+                        if (x >= cfg.particle_hi[0] || x < cfg.particle_lo[0] || y >= cfg.particle_hi[1] ||
+                            y < cfg.particle_lo[1] || rsq > P.radius * P.radius ||
+                            rsq < P.hollow_core_radius * P.hollow_core_radius || P.density.eval(v) <= P.min_density)
+                            continue;
+                        const double u0 = P.u_mean[0], u1 = P.u_mean[1], u2 = P.u_mean[2];
+                        if (P.u_std[0] != 0 || P.u_std[1] != 0 || P.u_std[2] != 0) {
+                            error = "plasma u_std != 0 needs a random stream; not restated in the oracle";
+                        }
+                        pl.x.push_back(x); pl.y.push_back(y);
+                        pl.w.push_back(P.density.eval(v) * scale);
+                        pl.ux.push_back(u0 * cfg.pc.c); pl.uy.push_back(u1 * cfg.pc.c);
+                        const double psi = std::sqrt(1. + u0 * u0 + u1 * u1 + u2 * u2) - u2;
+                        pl.psi.push_back(psi);
+                        pl.x_prev.push_back(x); pl.y_prev.push_back(y);
+                        pl.ux_h.push_back(u0 * cfg.pc.c); pl.uy_h.push_back(u1 * cfg.pc.c);
+                        pl.psi_h.push_back(psi);
+                        pl.valid.push_back(1);
+                    }
+            }
+        }
+    }
+
+    // -------------------------------------------------------------- plasma deposition
+    // PlasmaDepositCurrent.cpp:22-259, order 2. `which`: 0 = This, 1 = Next, 2 = ions.
+    void plasma_deposit(int which, bool jxjy, bool jz, bool rho, bool chi, bool rhomjz) {
+        for (size_t s = 0; s < plasmas.size(); ++s) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[s];
+            Plasma& pl = plasmas[s];
+            const double charge = (which == 2) ? -P.charge : P.charge;
+            const double invvol = cfg.normalized_units ? dx * dy * dxi * dyi : dxi * dyi * dzi;
+            const double clight = cfg.pc.c, clightinv = 1.0 / cfg.pc.c;
+            const double charge_invvol = charge * invvol;
+            const double charge_mu0_mass_ratio = charge * cfg.pc.mu0 / P.mass;
+            Field *Fjx = nullptr, *Fjy = nullptr, *Fjz = nullptr, *Frho = nullptr, *Fchi = nullptr, *Frm = nullptr;
+            if (which == 2) { Frm = &f("Ions.rhomjz"); }
+            else if (cfg.explicit_solver) {
+                if (which == 0) {
+                    if (jxjy) { Fjx = &f("jx"); Fjy = &f("jy"); }
+                    if (rho) Frho = &f("rho");
+                    if (chi) Fchi = &f("chi");
+                    if (rhomjz) Frm = &f("rhomjz");
+                }
+            } else {
+                if (which == 0) {
+                    if (jxjy) { Fjx = &f("jx"); Fjy = &f("jy"); }
+                    if (jz) Fjz = &f("jz");
+                    if (rho) Frho = &f("rho");
+                    if (rhomjz) Frm = &f("rhomjz");
+                } else {
+                    if (jxjy) { Fjx = &f("Next.jx"); Fjy = &f("Next.jy"); }
+                }
+            }
+            for (size_t ip = 0; ip < pl.n(); ++ip) {
+                if (!pl.valid[ip]) continue;
+                const double psi_inv = 1.0 / pl.psi[ip];
+                const double xp = pl.x[ip], yp = pl.y[ip];
+                const double vx_c = pl.ux[ip] * psi_inv;
+                const double vy_c = pl.uy[ip] * psi_inv;
+                const double q_invvol = charge_invvol * pl.w[ip];
+                const double q_mu0_mass_ratio = charge_mu0_mass_ratio;
+                const double xmid = (xp - xoff) * dxi;
+                const double ymid = (yp - yoff) * dyi;
+                const double gamma_psi = 0.5 * ((1.0 + 0.5 * 0.0) * psi_inv * psi_inv +
+                                                vx_c * vx_c * clightinv * clightinv +
+                                                vy_c * vy_c * clightinv * clightinv + 1.0);
+                if (gamma_psi < 0.0 || gamma_psi > P.max_qsa_weighting_factor || psi_inv < 0.0) {
+                    pl.w[ip] = 0.0;
+                    pl.valid[ip] = 0;
+                    continue;
+                }
+                for (int iy = 0; iy <= 2; ++iy)
+                    for (int ix = 0; ix <= 2; ++ix) {
+                        Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);
+                        const int i = sx.cell, j = sy.cell;
+                        const double cd = q_invvol * sx.s * sy.s;
+                        if (Fjx) { (*Fjx)(i, j) += cd * vx_c; (*Fjy)(i, j) += cd * vy_c; }
+                        if (Fjz) (*Fjz)(i, j) += cd * (gamma_psi - 1.0) * clight;
+                        if (Frho) (*Frho)(i, j) += cd * gamma_psi;
+                        if (Fchi) (*Fchi)(i, j) += cd * q_mu0_mass_ratio * psi_inv;
+                        if (Frm) (*Frm)(i, j) += cd;
+                    }
+            }
+        }
+    }
+
+    // -------------------------------------------------------------- explicit deposition
+    // ExplicitDeposition.cpp:20-265 (no laser): Sx, Sy += plasma contribution
+    void explicit_deposit() {
+        const int dt = cfg.depos_derivative_type;
+        const int ns = 2 + dt;  // stencil extent - 1
+        Field& Sx = f("Sx"); Field& Sy = f("Sy");
+        const Field& Bz = f("Bz"); const Field& Ez = f("Ez");
+        const Field& ExmBy = f("ExmBy"); const Field& EypBx = f("EypBx");
+        for (size_t s = 0; s < plasmas.size(); ++s) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[s];
+            Plasma& pl = plasmas[s];
+            const double invvol = cfg.normalized_units ? dx * dy * dxi * dyi : dxi * dyi * dzi;
+            const double a_clight = cfg.pc.c, clight_inv = 1. / cfg.pc.c;
+            const double charge_invvol_mu0 = P.charge * invvol * cfg.pc.mu0;
+            const double q_mass_ratio = P.charge / P.mass;
+            for (size_t ip = 0; ip < pl.n(); ++ip) {
+                if (!pl.valid[ip]) continue;
+                const double psi_inv = 1. / pl.psi[ip];
+                const double xp = pl.x[ip], yp = pl.y[ip];
+                const double vx = pl.ux[ip] * psi_inv * clight_inv;
+                const double vy = pl.uy[ip] * psi_inv * clight_inv;
+                const double cdm = charge_invvol_mu0 * pl.w[ip];
+                const double xmid = (xp - xoff) * dxi, ymid = (yp - yoff) * dyi;
+                const double gamma_psi = 0.5 * ((1. + 0.5 * 0.0) * psi_inv * psi_inv + vx * vx + vy * vy + 1.);
+                for (int iy = 0; iy <= ns; ++iy)
+                    for (int ix = 0; ix <= ns; ++ix) {
+                        if (dt == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                        DShape sy = dshape2(dt, ymid, iy);
+                        DShape sx = dshape2(dt, xmid, ix);
+                        const int i = sx.cell, j = sy.cell;
+                        const double Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = ExmBy(i, j), EypBx_v = EypBx(i, j);
+                        Sy(i, j) += cdm * (-sx.s * sy.s * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * clight_inv - 0.25 * 0.0 * q_mass_ratio * psi_inv) * q_mass_ratio * psi_inv +
+                                           (-sx.ds * sy.s * dxi * (-vx * vy) - sx.s * sy.ds * dyi * (gamma_psi - vy * vy - 1.)) * a_clight);
+                        Sx(i, j) += cdm * (+sx.s * sy.s * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv - 0.25 * 0.0 * q_mass_ratio * psi_inv) * q_mass_ratio * psi_inv +
+                                           (+sx.ds * sy.s * dxi * (gamma_psi - vx * vx - 1.) + sx.s * sy.ds * dyi * (-vx * vy)) * a_clight);
+                    }
+            }
+        }
+    }
+
+    // -------------------------------------------------------------- beam deposition
+    // BeamDepositCurrent.cpp:21-196: deposits the non-slipped particles of a beam slice
+    void beam_deposit(const BeamSlice& bs, double q, Field* jx, Field* jy, Field* jz, Field* rmj) {
+        const double invvol = cfg.normalized_units ? 1.0 : dxi * dyi * dzi;
+        const double clightinv = 1.0 / cfg.pc.c, clightsq = 1.0 / (cfg.pc.c * cfg.pc.c);
+        for (size_t ip = 0; ip < bs.num_nonslipped; ++ip) {
+            const BeamParticle& p = bs.p[ip];
+            if (!p.valid) continue;
+            const double gaminv = 1.0 / std::sqrt(1.0 + p.ux * p.ux * clightsq + p.uy * p.uy * clightsq + p.uz * p.uz * clightsq);
+            const double wq = q * p.w * invvol;
+            const double vx = p.ux * gaminv, vy = p.uy * gaminv, vz = p.uz * gaminv;
+            const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
+            const double xmid = (p.x - xoff) * dxi, ymid = (p.y - yoff) * dyi;
+            for (int iy = 0; iy <= 2; ++iy)
+                for (int ix = 0; ix <= 2; ++ix) {
+                    Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);
+                    const double S = sx.s * sy.s;
+                    const int i = sx.cell, j = sy.cell;
+                    if (jx) { (*jx)(i, j) += S * wqx; (*jy)(i, j) += S * wqy; }
+                    if (jz) (*jz)(i, j) += S * wqz;
+                    if (rmj) (*rmj)(i, j) += S * wqr;
+                }
+        }
+    }
+
+    // -------------------------------------------------------------- field solves
+    // Fields.cpp:840-957: Psi, Ez, Bz Poisson solves and ExmBy/EypBx = -grad Psi
+    void solve_psi_ez_bz() {
+        const hpq::PhysConst& pc = cfg.pc;
+        if (cfg.explicit_solver && cfg.do_beam_jz_minus_rho) {
+            Field& r = f("rhomjz"); const Field& b = f("rhomjz_beam");
+            for (size_t k = 0; k < r.a.size(); ++k) r.a[k] += b.a[k];
+        }
+        const Field& rm = f("rhomjz");
+        const Field& jx = f("jx");
+        const Field& jy = f("jy");
+        std::vector<double> st((size_t)nx * ny);
+        auto solve_into = [&](Field& out) {
+            dst.solve(st);
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) out(i, j) = st[(size_t)j * nx + i];
+        };
+        const double hx = 0.5 * dxi, hy = 0.5 * dyi;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) st[(size_t)j * nx + i] = -1. / pc.ep0 * rm(i, j);
+        solve_into(f("Psi"));
+        const double fe = 1. / (pc.ep0 * pc.c);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                st[(size_t)j * nx + i] = fe * ((jx(i + 1, j) - jx(i - 1, j)) * hx) + fe * ((jy(i, j + 1) - jy(i, j - 1)) * hy);
+        solve_into(f("Ez"));
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                st[(size_t)j * nx + i] = pc.mu0 * ((jx(i, j + 1) - jx(i, j - 1)) * hy) + (-pc.mu0) * ((jy(i + 1, j) - jy(i - 1, j)) * hx);
+        solve_into(f("Bz"));
+        const Field& Psi = f("Psi");
+        Field& Ex = f("ExmBy"); Field& Ey = f("EypBx");
+        for (int j = -1; j <= ny; ++j)
+            for (int i = -1; i <= nx; ++i) {
+                Ex(i, j) = -(Psi(i + 1, j) - Psi(i - 1, j)) * hx;
+                Ey(i, j) = -(Psi(i, j + 1) - Psi(i, j - 1)) * hy;
+            }
+    }
+
+    // Fields.cpp:1008-1078: PC Bx, By from jz (This) and d/dzeta of jx, jy (Previous, Next)
+    void solve_bxby_pc() {
+        const hpq::PhysConst& pc = cfg.pc;
+        const Field& jz = f("jz");
+        const Field& pjx = f("Prev.jx"); const Field& pjy = f("Prev.jy");
+        const Field& njx = f("Next.jx"); const Field& njy = f("Next.jy");
+        std::vector<double> st((size_t)nx * ny);
+        const double hx = 0.5 * dxi, hy = 0.5 * dyi, hz = 0.5 * dzi;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                st[(size_t)j * nx + i] = -pc.mu0 * ((jz(i, j + 1) - jz(i, j - 1)) * hy) + pc.mu0 * ((pjy(i, j) - njy(i, j)) * hz);
+        dst.solve(st);
+        Field& bx = f("PCIter.Bx");
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) bx(i, j) = st[(size_t)j * nx + i];
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                st[(size_t)j * nx + i] = pc.mu0 * ((jz(i + 1, j) - jz(i - 1, j)) * hx) + (-pc.mu0) * ((pjx(i, j) - njx(i, j)) * hz);
+        dst.solve(st);
+        Field& by = f("PCIter.By");
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) by(i, j) = st[(size_t)j * nx + i];
+    }
+
+    // Hipace.cpp:744-790
+    void init_sxsy_with_beam() {
+        const double mu0 = cfg.pc.mu0;
+        const Field& jzb = f("jz_beam");
+        const Field& pjx = f("Prev.jx_beam"); const Field& pjy = f("Prev.jy_beam");
+        const Field& njx = f("Next.jx_beam"); const Field& njy = f("Next.jy_beam");
+        Field& Sx = f("Sx"); Field& Sy = f("Sy");
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double dx_jzb = (jzb(i + 1, j) - jzb(i - 1, j)) / (2. * dx);
+                const double dy_jzb = (jzb(i, j + 1) - jzb(i, j - 1)) / (2. * dy);
+                const double dz_jxb = (pjx(i, j) - njx(i, j)) / (2. * dz);
+                const double dz_jyb = (pjy(i, j) - njy(i, j)) / (2. * dz);
+                Sy(i, j) = mu0 * (-dy_jzb + dz_jyb);
+                Sx(i, j) = -mu0 * (-dx_jzb + dz_jxb);
+            }
+    }
+
+    // -------------------------------------------------------------- plasma push
+    // PlasmaParticleAdvance.cpp:29-217 with doGatherShapeN (FieldGather.H:45-96, derivative
+    // type 1) and PlasmaMomentumPush (PushPlasmaParticles.H:39-75); leapfrog, 4+2 Taylor substeps.
+    struct Deriv { double ux, uy, psi; };
+    static inline Deriv mom(double ux, double uy, double psi_inv, double ExmBy, double EypBx, double Ez,
+                            double Bxc, double Byc, double Bz, double ci, double qmc) {
+        const double gamma_psi = 0.5 * psi_inv * psi_inv * (1.0 + 0.0 + ux * ux * (ci * ci) + uy * uy * (ci * ci)) + 0.5;
+        return {qmc * (gamma_psi * ExmBy + Byc + (uy * Bz) * psi_inv) - 0.0 * psi_inv,
+                qmc * (gamma_psi * EypBx - Bxc - (ux * Bz) * psi_inv) - 0.0 * psi_inv,
+                qmc * ci * ((ux * ExmBy + uy * EypBx) * ci * psi_inv - Ez)};
+    }
+    // the same expression evaluated on dual numbers (value, epsilon) (DualNumbers.H)
+    struct Dual { double v, e; };
+    static inline Dual dadd(Dual a, Dual b) { return {a.v + b.v, a.e + b.e}; }
+    static inline Dual dsub(Dual a, Dual b) { return {a.v - b.v, a.e - b.e}; }
+    static inline Dual dmul(Dual a, Dual b) { return {a.v * b.v, a.e * b.v + a.v * b.e}; }
+    static inline void mom_dual(Dual ux, Dual uy, Dual pi, double ExmBy, double EypBx, double Ez, double Bxc,
+                                double Byc, double Bz, double ci, double qmc, Dual& dux, Dual& duy, Dual& dpsi) {
+        const Dual c2{ci * ci, 0};
+        Dual t = dadd(dadd(dadd(Dual{1.0, 0}, Dual{0.0, 0}), dmul(dmul(ux, ux), c2)), dmul(dmul(uy, uy), c2));
+        Dual gp = dadd(dmul(dmul(dmul(Dual{0.5, 0}, pi), pi), t), Dual{0.5, 0});
+        dux = dsub(dmul(Dual{qmc, 0}, dadd(dadd(dmul(gp, Dual{ExmBy, 0}), Dual{Byc, 0}), dmul(dmul(uy, Dual{Bz, 0}), pi))), dmul(Dual{0.0, 0}, pi));
+        duy = dsub(dmul(Dual{qmc, 0}, dsub(dsub(dmul(gp, Dual{EypBx, 0}), Dual{Bxc, 0}), dmul(dmul(ux, Dual{Bz, 0}), pi))), dmul(Dual{0.0, 0}, pi));
+        dpsi = dmul(dmul(Dual{qmc, 0}, Dual{ci, 0}), dsub(dmul(dmul(dadd(dmul(ux, Dual{ExmBy, 0}), dmul(uy, Dual{EypBx, 0})), Dual{ci, 0}), pi), Dual{Ez, 0}));
+    }
+
+    void gather(double xp, double yp, double& ExmBy, double& EypBx, double& Ez, double& Bx, double& By, double& Bz) {
+        const Field& Psi = f("Psi"); const Field& FEz = f("Ez");
+        const Field& FBx = f("Bx"); const Field& FBy = f("By"); const Field& FBz = f("Bz");
+        const double x = (xp - xoff) * dxi, y = (yp - yoff) * dyi;
+        for (int iy = 0; iy <= 3; iy++)
+            for (int ix = 0; ix <= 3; ix++) {
+                DShape sy = dshape2(1, y, iy);
+                DShape sx = dshape2(1, x, ix);
+                const int i = sx.cell, j = sy.cell;
+                ExmBy += (sx.ds * sy.s) * Psi(i, j) * dxi;
+                EypBx += (sx.s * sy.ds) * Psi(i, j) * dyi;
+                Ez += (sx.s * sy.s) * FEz(i, j);
+                Bx += (sx.s * sy.s) * FBx(i, j);
+                By += (sx.s * sy.s) * FBy(i, j);
+                Bz += (sx.s * sy.s) * FBz(i, j);
+            }
+    }
+
+    void plasma_push(bool temp) {
+        for (size_t s = 0; s < plasmas.size(); ++s) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[s];
+            Plasma& pl = plasmas[s];
+            const double clight = cfg.pc.c, ci = 1. / cfg.pc.c;
+            const double qmc = P.charge / (P.mass * cfg.pc.c);
+            const int nsubc = P.n_subcycles;
+            const double dzs = dz / nsubc;
+#pragma omp parallel for schedule(static)
+            for (long long ip = 0; ip < (long long)pl.n(); ++ip) {
+                if (!pl.valid[ip]) continue;
+                double ExmBy = 0, EypBx = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+                for (int isc = 0; isc < nsubc; ++isc) {
+                    double xp = pl.x_prev[ip], yp = pl.y_prev[ip];
+                    ExmBy = 0; EypBx = 0; Ez = 0; Bx = 0; By = 0; Bz = 0;
+                    gather(xp, yp, ExmBy, EypBx, Ez, Bx, By, Bz);
+                    Bx *= clight; By *= clight;
+                    const int nsub = 4;
+                    const double sdz = dzs / nsub;
+                    double ux = pl.ux_h[ip], uy = pl.uy_h[ip], psi = pl.psi_h[ip];
+                    auto substep = [&]() {
+                        const double psi_inv = 1. / psi;
+                        Deriv d = mom(ux, uy, psi_inv, ExmBy, EypBx, Ez, Bx, By, Bz, ci, qmc);
+                        Dual dux, duy, dps;
+                        mom_dual({ux, d.ux}, {uy, d.uy}, {psi_inv, -psi_inv * psi_inv * d.psi}, ExmBy, EypBx, Ez, Bx, By, Bz, ci, qmc, dux, duy, dps);
+                        ux += sdz * d.ux + 0.5 * sdz * sdz * dux.e;
+                        uy += sdz * d.uy + 0.5 * sdz * sdz * duy.e;
+                        psi += sdz * d.psi + 0.5 * sdz * sdz * dps.e;
+                    };
+                    for (int k = 0; k < nsub; ++k) substep();
+                    xp += dzs * ci * (ux * (1. / psi));
+                    yp += dzs * ci * (uy * (1. / psi));
+                    if (!enforce_bc(xp, yp, ux, uy)) { pl.w[ip] = 0; pl.valid[ip] = 0; break; }
+                    pl.x[ip] = xp; pl.y[ip] = yp;
+                    if (!temp) {
+                        pl.ux_h[ip] = ux; pl.uy_h[ip] = uy; pl.psi_h[ip] = psi;
+                        pl.x_prev[ip] = xp; pl.y_prev[ip] = yp;
+                    }
+                    for (int k = 0; k < nsub / 2; ++k) substep();
+                    pl.ux[ip] = ux; pl.uy[ip] = uy; pl.psi[ip] = psi;
+                }
+            }
+        }
+    }
+
+    // -------------------------------------------------------------- beam push
+    // BeamParticleAdvance.cpp:19-336 (no external fields, spin or radiation reaction)
+    void beam_push(int b, BeamSlice& bs, int islice) {
+        const hpq::BeamSpecies& B = cfg.beams[b];
+        const double dtb = cfg.dt / B.n_subcycles;
+        const double clight = cfg.pc.c, inv_c2 = 1. / (cfg.pc.c * cfg.pc.c);
+        const double cmr = B.charge / B.mass;
+        const double min_z = cfg.prob_lo[2] + (islice - 0) * dz;
+        for (auto& p : bs.p) {
+            if (!p.valid) continue;
+            double xp = p.x, yp = p.y, zp = p.z, ux = p.ux, uy = p.uy, uz = p.uz;
+            int i = p.nsub;
+            bool absorbed = false;
+            for (; i < B.n_subcycles; i++) {
+                if (zp < min_z) break;
+                const double gammap_inv = 1. / std::sqrt(1. + (ux * ux + uy * uy + uz * uz) * inv_c2);
+                xp += dtb * 0.5 * ux * gammap_inv;
+                yp += dtb * 0.5 * uy * gammap_inv;
+                if (!enforce_bc(xp, yp, ux, uy)) { absorbed = true; break; }
+                double ExmBy = 0, EypBx = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+                gather(xp, yp, ExmBy, EypBx, Ez, Bx, By, Bz);
+                const double ux_next = ux + dtb * cmr * (ExmBy + (clight - uz * gammap_inv) * By + uy * gammap_inv * Bz);
+                const double uy_next = uy + dtb * cmr * (EypBx + (uz * gammap_inv - clight) * Bx - ux * gammap_inv * Bz);
+                const double uxi = (ux_next + ux) * 0.5, uyi = (uy_next + uy) * 0.5;
+                const double uzi = uz + dtb * 0.5 * cmr * Ez;
+                const double gii = 1. / std::sqrt(1. + (uxi * uxi + uyi * uyi + uzi * uzi) * inv_c2);
+                const double uz_next = uz + dtb * cmr * (Ez + (uxi * By - uyi * Bx) * gii);
+                const double gni = 1. / std::sqrt(1. + (ux_next * ux_next + uy_next * uy_next + uz_next * uz_next) * inv_c2);
+                xp += dtb * 0.5 * ux_next * gni;
+                yp += dtb * 0.5 * uy_next * gni;
+                if (B.do_z_push) zp += dtb * (uz_next * gni - clight);
+                ux = ux_next; uy = uy_next; uz = uz_next;
+            }
+            if (absorbed || !enforce_bc(xp, yp, ux, uy)) { p.w = 0; p.valid = false; continue; }
+            p.x = xp; p.y = yp; p.z = zp; p.nsub = i;
+            p.ux = ux; p.uy = uy; p.uz = uz;
+        }
+    }
+
+    // SliceSort.cpp:13-64: drop invalid particles, keep z >= min_z on this slice (stable), move
+    // the rest to the next slice behind the non-slipped ones there
+    void shift_slipped(int b, int islice) {
+        BeamSlice& T = bthis[b];
+        BeamSlice& N = bnext[b];
+        const double min_z = cfg.prob_lo[2] + islice * dz;
+        std::vector<BeamParticle> stay, slip;
+        for (auto& p : T.p) {
+            if (!p.valid) continue;
+            if (p.z >= min_z) stay.push_back(p); else slip.push_back(p);
+        }
+        T.p = stay;
+        T.num_nonslipped = stay.size();
+        if (!slip.empty()) {
+            N.p.resize(N.num_nonslipped);
+            for (auto& p : slip) N.p.push_back(p);
+        }
+    }
+
+    void load_beam_slice(int b, int islice, BeamSlice& dst_slice) {
+        dst_slice = store[b][islice];
+        for (auto& p : dst_slice.p) p.nsub = 0;
+        dst_slice.num_nonslipped = dst_slice.p.size();
+    }
+
+    // -------------------------------------------------------------- PC helpers
+    double rel_b_error(const char* bx, const char* by, const char* bxi, const char* byi) {
+        const Field& Bx = f(bx); const Field& By = f(by);
+        const Field& Bxi = f(bxi); const Field& Byi = f(byi);
+        double nb = 0, nd = 0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                nb += std::sqrt(Bx(i, j) * Bx(i, j) + By(i, j) * By(i, j));
+                nd += std::sqrt((Bx(i, j) - Bxi(i, j)) * (Bx(i, j) - Bxi(i, j)) + (By(i, j) - Byi(i, j)) * (By(i, j) - Byi(i, j)));
+            }
+        return nb > 0 ? nd / nb : 0.0;
+    }
+    static void lincomb(Field& dst, double a, const Field& x, double b, const Field& y) {
+        for (size_t k = 0; k < dst.a.size(); ++k) dst.a[k] = a * x.a[k] + b * y.a[k];
+    }
+    static void copy(Field& dst, const Field& src) { dst.a = src.a; }
+
+    // Hipace.cpp:935-1031
+    void pc_loop(int islice) {
+        (void)islice;
+        double err_prev = 1.0;
+        double err = rel_b_error("Prev.Bx", "Prev.By", "PCPrevIter.Bx", "PCPrevIter.By");
+        // InitialBfieldGuess (Fields.cpp:1149-1171)
+        const double tol = cfg.predcorr_B_error_tolerance;
+        const double mix = std::exp(-0.5 * std::pow(err / (2.5 * tol), 2));
+        lincomb(f("Bx"), 1. + mix, f("Prev.Bx"), -mix, f("PCPrevIter.Bx"));
+        lincomb(f("By"), 1. + mix, f("Prev.By"), -mix, f("PCPrevIter.By"));
+        f("PCIter.Bx").zero(); f("PCIter.By").zero();
+        copy(f("PCPrevIter.Bx"), f("Bx")); copy(f("PCPrevIter.By"), f("By"));
+        int it = 0;
+        err = 1.0;
+        while (err > tol && it < cfg.predcorr_max_iterations) {
+            it++;
+            plasma_push(true);
+            plasma_deposit(1, true, false, false, false, false);
+            for (size_t b = 0; b < cfg.beams.size(); ++b)
+                if (cfg.do_beam_jx_jy_deposition)
+                    beam_deposit(bnext[b], cfg.beams[b].charge, &f("Next.jx"), &f("Next.jy"), nullptr, nullptr);
+            solve_bxby_pc();
+            err = rel_b_error("Bx", "By", "PCIter.Bx", "PCIter.By");
+            if (it == 1) err_prev = err;
+            // MixAndShiftBfields (Fields.cpp:1173-1226)
+            double wi, wp;
+            if (err != 0. || err_prev != 0.) { wi = err_prev / (err + err_prev); wp = err / (err + err_prev); }
+            else { wi = 0.5; wp = 0.5; }
+            lincomb(f("PCPrevIter.Bx"), wi, f("PCIter.Bx"), wp, f("PCPrevIter.Bx"));
+            lincomb(f("PCPrevIter.By"), wi, f("PCIter.By"), wp, f("PCPrevIter.By"));
+            const double a = cfg.predcorr_B_mixing_factor;
+            lincomb(f("Bx"), 1. - a, f("Bx"), a, f("PCPrevIter.Bx"));
+            lincomb(f("By"), 1. - a, f("By"), a, f("PCPrevIter.By"));
+            copy(f("PCPrevIter.Bx"), f("PCIter.Bx")); copy(f("PCPrevIter.By"), f("PCIter.By"));
+            f("Next.jx").zero(); f("Next.jy").zero();
+            err_prev = err;
+        }
+        pc_errors.push_back(err);
+    }
+
+    // -------------------------------------------------------------- one slice
+    // Hipace::SolveOneSlice (Hipace.cpp:556-728), level 0 only
+    void solve_one_slice(int islice, int step) {
+        const bool ex = cfg.explicit_solver;
+        if (islice == nz - 1)
+            for (size_t b = 0; b < cfg.beams.size(); ++b) load_beam_slice((int)b, islice, bthis[b]);
+        // InitializeSlices (Fields.cpp:535-586)
+        if (ex) {
+            for (auto n : {"chi", "Sy", "Sx", "ExmBy", "EypBx", "jz_beam", "rhomjz", "Next.jx_beam", "Next.jy_beam", "rhomjz_beam"}) f(n).zero();
+        } else {
+            for (auto n : {"ExmBy", "EypBx", "jx", "jy", "jz", "rhomjz"}) f(n).zero();
+        }
+        if (cfg.deposit_rho) f("rho").zero();
+        // deposition on This
+        if (ex) {
+            plasma_deposit(0, true, false, cfg.deposit_rho, true, true);
+            for (size_t b = 0; b < cfg.beams.size(); ++b)
+                beam_deposit(bthis[b], cfg.beams[b].charge, nullptr, nullptr, &f("jz_beam"),
+                             cfg.do_beam_jz_minus_rho ? &f("rhomjz_beam") : nullptr);
+        } else {
+            plasma_deposit(0, true, true, cfg.deposit_rho, false, true);
+            for (size_t b = 0; b < cfg.beams.size(); ++b)
+                beam_deposit(bthis[b], cfg.beams[b].charge,
+                             cfg.do_beam_jx_jy_deposition ? &f("jx") : nullptr,
+                             cfg.do_beam_jx_jy_deposition ? &f("jy") : nullptr, &f("jz"),
+                             cfg.do_beam_jz_minus_rho ? &f("rhomjz") : nullptr);
+        }
+        // AddRhoIons (Fields.cpp:606-615)
+        if (cfg.any_neutralize_background()) {
+            Field& r = f("rhomjz"); const Field& ions = f("Ions.rhomjz");
+            for (size_t k = 0; k < r.a.size(); ++k) r.a[k] += ions.a[k];
+            if (cfg.deposit_rho) { Field& rr = f("rho"); for (size_t k = 0; k < rr.a.size(); ++k) rr.a[k] += ions.a[k]; }
+        }
+        solve_psi_ez_bz();
+        if (islice - 1 >= 0)
+            for (size_t b = 0; b < cfg.beams.size(); ++b) load_beam_slice((int)b, islice - 1, bnext[b]);
+        if (ex) {
+            for (size_t b = 0; b < cfg.beams.size(); ++b)
+                if (cfg.do_beam_jx_jy_deposition)
+                    beam_deposit(bnext[b], cfg.beams[b].charge, &f("Next.jx_beam"), &f("Next.jy_beam"), nullptr, nullptr);
+            init_sxsy_with_beam();
+            explicit_deposit();
+            int iters = 0;
+            const int st = mg.solve(f("Bx"), f("By"), f("Sy"), f("Sx"), f("chi"), cfg.mg_tol_rel, cfg.mg_tol_abs,
+                                    cfg.mg_max_iters, &iters);
+            mg_iters_total += iters;
+            if (st != 0 && mg_status == 0) mg_status = st;
+        } else {
+            pc_loop(islice);
+        }
+        // diagnostics (after all fields are known, before the pushes)
+        for (auto& n : diag_names) {
+            auto& d = diag[n];
+            const Field& src = f(n.c_str());
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) d[((size_t)islice * ny + j) * nx + i] = src(i, j);
+        }
+        plasma_push(false);
+        for (size_t b = 0; b < cfg.beams.size(); ++b) {
+            beam_push((int)b, bthis[b], islice);
+            shift_slipped((int)b, islice);
+            const bool is_last_step = (step == cfg.max_step);
+            if (!is_last_step) store[b][islice] = bthis[b];
+            else store[b][islice] = bthis[b];  // kept for inspection after the run
+            store[b][islice].num_nonslipped = store[b][islice].p.size();
+        }
+        // ShiftSlices (Fields.cpp:588-604)
+        if (ex) {
+            copy(f("Prev.jx_beam"), f("jx_beam")); copy(f("Prev.jy_beam"), f("jy_beam"));
+            copy(f("jx_beam"), f("Next.jx_beam")); copy(f("jy_beam"), f("Next.jy_beam"));
+            copy(f("jx"), f("Next.jx_beam")); copy(f("jy"), f("Next.jy_beam"));
+        } else {
+            copy(f("PCPrevIter.Bx"), f("Prev.Bx")); copy(f("PCPrevIter.By"), f("Prev.By"));
+            copy(f("Prev.Bx"), f("Bx")); copy(f("Prev.By"), f("By"));
+            copy(f("Prev.jx"), f("jx")); copy(f("Prev.jy"), f("jy"));
+        }
+        for (size_t b = 0; b < cfg.beams.size(); ++b) {
+            bthis[b] = bnext[b];
+            bnext[b].p.clear();
+            bnext[b].num_nonslipped = 0;
+        }
+    }
+
+    // -------------------------------------------------------------- one step
+    // Hipace::Evolve per-step body (Hipace.cpp:401-492), one rank, fixed dt
+    void begin_step(int step) {
+        for (auto& kv : F) kv.second.zero();  // ResetAllQuantities
+        (void)step;
+        init_plasmas();
+        if (cfg.any_neutralize_background()) {
+            // DepositNeutralizingBackground: rhomjz of ions with the opposite charge
+            std::vector<hpq::PlasmaSpecies> saved = cfg.plasmas;
+            plasma_deposit_ions();
+        }
+        for (auto& n : diag_names) diag[n].assign((size_t)nx * ny * nz, 0.0);
+    }
+    void plasma_deposit_ions() {
+        // only species with neutralize_background deposit (MultiPlasma.cpp:103-115)
+        std::vector<Plasma> saved = plasmas;
+        for (size_t s = 0; s < plasmas.size(); ++s)
+            if (!cfg.plasmas[s].neutralize_background) plasmas[s].valid.assign(plasmas[s].n(), 0);
+        plasma_deposit(2, false, false, false, false, true);
+        // the ion deposit may invalidate QSA-violating particles (same test as the plasma)
+        for (size_t s = 0; s < plasmas.size(); ++s)
+            if (!cfg.plasmas[s].neutralize_background) { plasmas[s].valid = saved[s].valid; plasmas[s].w = saved[s].w; }
+    }
+    void end_step() { physical_time += cfg.dt; }
+
+    int step(int s) {
+        begin_step(s);
+        for (int isl = nz - 1; isl >= 0; --isl) solve_one_slice(isl, s);
+        end_step();
+        return mg_status;
+    }
+};
+
+}  // namespace oracle
+
+// ------------------------------------------------------------------------------------------
+// C interface used by the tests (ctypes)
+// ------------------------------------------------------------------------------------------
+struct OracleHandle {
+    std::unique_ptr<oracle::Sim> sim;
+    std::string err;
+};
+
+extern "C" {
+
+int oracle_create(const char* input_text, OracleHandle** out, char* err, int errlen) {
+    try {
+        hpq::InputStore in;
+        in.parse_text(input_text);
+        hpq::SimConfig cfg = hpq::build_config(in);
+        auto* h = new OracleHandle;
+        h->sim.reset(new oracle::Sim(cfg));
+        *out = h;
+        return 0;
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) { strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return 1;
+    }
+}
+void oracle_destroy(OracleHandle* h) { delete h; }
+
+int oracle_init_beams(OracleHandle* h) {
+    auto& s = *h->sim;
+    for (size_t b = 0; b < s.cfg.beams.size(); ++b) {
+        if (s.cfg.beams[b].injection == hpq::BeamInjection::FixedPPC) s.init_beam_fixed_ppc((int)b);
+        else if (!s.store_valid[b]) return 2;  // fixed_weight beams must be provided
+    }
+    return 0;
+}
+
+int oracle_set_beam(OracleHandle* h, int b, const double* x, const double* y, const double* z, const double* w,
+                    const double* ux, const double* uy, const double* uz, const int64_t* id, int64_t n) {
+    auto& s = *h->sim;
+    if (b < 0 || b >= (int)s.cfg.beams.size()) return 1;
+    s.set_beam(b, x, y, z, w, ux, uy, uz, id, n);
+    return 0;
+}
+
+// number of stored particles of beam b (all slices), and a copy in slice-descending order
+int64_t oracle_beam_count(OracleHandle* h, int b) {
+    auto& s = *h->sim;
+    int64_t n = 0;
+    for (auto& sl : s.store[b]) n += (int64_t)sl.p.size();
+    return n;
+}
+int oracle_get_beam(OracleHandle* h, int b, double* x, double* y, double* z, double* w, double* ux, double* uy,
+                    double* uz, int64_t* id) {
+    auto& s = *h->sim;
+    int64_t k = 0;
+    for (int sl = s.nz - 1; sl >= 0; --sl)
+        for (auto& p : s.store[b][sl].p) {
+            x[k] = p.x; y[k] = p.y; z[k] = p.z; w[k] = p.w; ux[k] = p.ux; uy[k] = p.uy; uz[k] = p.uz;
+            if (id) id[k] = p.id;
+            ++k;
+        }
+    return 0;
+}
+
+int oracle_set_diag(OracleHandle* h, const char* names) {
+    auto& s = *h->sim;
+    s.diag_names.clear();
+    std::string t(names);
+    std::istringstream in(t);
+    std::string n;
+    while (in >> n) {
+        if (!s.F.count(n)) return 1;
+        s.diag_names.push_back(n);
+    }
+    return 0;
+}
+int oracle_get_diag(OracleHandle* h, const char* name, double* out) {
+    auto& s = *h->sim;
+    auto it = s.diag.find(name);
+    if (it == s.diag.end()) return 1;
+    std::memcpy(out, it->second.data(), it->second.size() * sizeof(double));
+    return 0;
+}
+
+int oracle_step(OracleHandle* h, int step) { return h->sim->step(step); }
+int oracle_begin_step(OracleHandle* h, int step) { h->sim->begin_step(step); return 0; }
+int oracle_solve_slice(OracleHandle* h, int islice, int step) { h->sim->solve_one_slice(islice, step); return h->sim->mg_status; }
+int oracle_end_step(OracleHandle* h) { h->sim->end_step(); return 0; }
+
+// interior nx*ny values of a slice component (current slice state)
+int oracle_get_field(OracleHandle* h, const char* name, double* out) {
+    auto& s = *h->sim;
+    auto it = s.F.find(name);
+    if (it == s.F.end()) return 1;
+    for (int j = 0; j < s.ny; ++j)
+        for (int i = 0; i < s.nx; ++i) out[(size_t)j * s.nx + i] = it->second(i, j);
+    return 0;
+}
+
+int64_t oracle_plasma_count(OracleHandle* h, int sp) { return (int64_t)h->sim->plasmas[sp].n(); }
+// attributes: x y w ux uy psi x_prev y_prev ux_half uy_half psi_half valid
+int oracle_get_plasma(OracleHandle* h, int sp, double* out12) {
+    auto& pl = h->sim->plasmas[sp];
+    const size_t n = pl.n();
+    const std::vector<double>* a[11] = {&pl.x, &pl.y, &pl.w, &pl.ux, &pl.uy, &pl.psi, &pl.x_prev, &pl.y_prev, &pl.ux_h, &pl.uy_h, &pl.psi_h};
+    for (int k = 0; k < 11; ++k) std::memcpy(out12 + k * n, a[k]->data(), n * sizeof(double));
+    for (size_t i = 0; i < n; ++i) out12[11 * n + i] = pl.valid[i];
+    return 0;
+}
+
+long long oracle_mg_iterations(OracleHandle* h) { return h->sim->mg_iters_total; }
+int oracle_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+const char* oracle_error(OracleHandle* h) { return h->sim->error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,72 @@
+"""Generate the golden fixtures from the reference's own regression tests.
+
+Reads, from a HiPACE++ source tree (default /root/reference):
+  * the example input decks named by each regression test script,
+  * the command-line overrides that script passes (tests/<name>.sh),
+  * the checksum goldens (tests/checksum/benchmarks_json/<name>.json),
+and writes tests/golden/golden_cases.json: for each case the merged input text, the expected
+per-field checksums (sum |Q| over the 3-D output of the last iteration,
+tests/checksum/backend/openpmd_backend.py:40-62), the beam attribute checksums and the
+relative tolerance the reference applies on CPU builds.
+
+Only deterministic cases (fixed_ppc beams, cold plasma) are kept: the others depend on AMReX's
+random stream.
+
+Usage: python tests/golden/make_golden.py [reference_root]
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASES = {
+    # name: (example deck, overrides, rtol on CPU builds, checksum components to skip)
+    "linear_wake.normalized.1Rank": (
+        "examples/linear_wake/inputs_normalized",
+        ["hipace.tile_size = 8", "diagnostic.field_data = all rho"],
+        1e-12, []),
+    "blowout_wake_explicit.2Rank": (
+        "examples/blowout_wake/inputs_normalized",
+        ["hipace.tile_size = 8", "max_step=1"],
+        1e-9, ["Sy", "Sx", "chi"]),
+    "gaussian_linear_wake.normalized.1Rank": (
+        "examples/linear_wake/inputs_normalized",
+        ["hipace.tile_size = 8", "beam.profile = gaussian", "beam.zmin = -5.9", "beam.zmax = 5.9",
+         "beam.radius = 10", "beam.position_mean = 0. 0. 0", "beam.position_std = 2 2 1.41",
+         "geometry.prob_lo     = -10.   -10.   -6", "geometry.prob_hi     =  10.    10.    6",
+         "diagnostic.field_data = all rho"],
+        1e-12, []),
+}
+
+
+def main(ref):
+    out = {}
+    for name, (deck, overrides, rtol, skip) in CASES.items():
+        with open(os.path.join(ref, deck)) as f:
+            text = f.read()
+        script = os.path.join(ref, "tests", name + ".sh")
+        assert os.path.exists(script), script
+        with open(script) as f:
+            sh = f.read()
+        for o in overrides:
+            # the override must really appear in the reference test script
+            key = o.split("=")[0].strip()
+            assert re.search(re.escape(key), sh), (name, key)
+        with open(os.path.join(ref, "tests/checksum/benchmarks_json", name + ".json")) as f:
+            gold = json.load(f)
+        out[name] = {
+            "deck": deck,
+            "input": text + "\n# overrides from tests/" + name + ".sh\n" + "\n".join(overrides) + "\n",
+            "fields": {k: v for k, v in gold["lev=0"].items() if k not in skip},
+            "beam": gold.get("beam", {}),
+            "rtol_cpu": rtol,
+        }
+    with open(os.path.join(HERE, "golden_cases.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_cases.json"), "cases:", list(out))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
