@@ -1,0 +1,326 @@
+"""Benchmark of the quasi-static slice loop on B200.
+
+Workload (default): the nonlinear blowout wake, plain FP64 — 255 x 255 transverse cells over
+[-6, 6]^2, 256 slices over zeta in [-8, 4], 65k plasma particles (1 per cell), a Gaussian driver
+of 1e6 seeded macro-particles (sigma 0.3, 0.3, 1.0; peak density 10; gamma 2000; normalized
+emittance 0.01), explicit Bx/By solver with multigrid, dt = 20. A "step" is one time step: the
+full slice march (256 slices) including the FP64 beam push.
+
+Metric: slices/s (whole job). `value` is device-timed (CUDA events on the library's stream,
+beam already resident). `e2e` is timed through the public C ABI with the step's inputs (the
+beam particles) uploaded from pinned host memory and the results (the pushed beam) read back
+every step. `roofline` is computed live from per-kernel events of a profiled pass over the same
+steps; `cpu_baseline` times this build's FP64 CPU oracle (oracle/, the reference itself cannot be
+built here) on a bounded sample.
+
+Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config NAME]
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# algorithmic bytes per plasma particle per slice, FP64, explicit path (reads and writes of the
+# particle arrays by deposit, explicit deposit and push): 21*8 + 24
+BYTES_PER_PARTICLE_SLICE = {8: 21 * 8 + 24, 4: 21 * 4 + 24}
+# plasma push alone: reads x_prev, y_prev, ux_h, uy_h, psi_h (+ valid byte), writes 10 reals
+PUSH_BYTES = {8: 5 * 8 + 1 + 10 * 8, 4: 5 * 4 + 1 + 10 * 4}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="blowout_255")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--no-graphs", action="store_true")
+    p.add_argument("--cpu-sample-slices", type=int, default=0)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def peaks():
+    try:
+        d = json.load(open(PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_sim(text, precision, graphs):
+    import hipace2_b200 as hp
+    sim = hp.Hipace(text, precision=hp.MIXED if precision == "mixed" else hp.PLAIN_FP64, graphs=graphs)
+    sim.init_data()
+    return sim
+
+
+def time_device_steps(sim, first, k, torch):
+    stream = torch.cuda.ExternalStream(sim.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    sim.synchronize()
+    e0.record(stream)
+    for s in range(first, first + k):
+        sim.step(s)
+    e1.record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import hipace2_b200 as hp
+    from cases import config
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    text = config(args.config)
+    sim = make_sim(text, args.precision, graphs=not args.no_graphs)
+    nx, ny, nz = sim.n_cell
+    n_plasma = sim.get_plasma(0)["x"].size
+    w = args.warmup
+    k = args.steps
+    for s in range(w):
+        sim.step(s)
+    # ---- device-timed region (replicas: each rank runs its own independent simulation)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    l_before = sim.counters()["kernel_launches"]
+    with ClockSampler(local) as clk:
+        secs = time_device_steps(sim, w, k, torch)
+    launches_in_timed = sim.counters()["kernel_launches"] - l_before
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([secs], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+    slices = nz * k * world
+    value = slices / secs
+    # ---- end to end through the C ABI with host buffers (pinned host copies every step)
+    beam = sim.get_beam(0)
+    nb = beam["x"].size
+    pinned = {key: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for key, v in beam.items()}
+    host = {key: v.numpy() for key, v in pinned.items()}
+    torch.cuda.synchronize()
+    sim.synchronize()
+    t0 = time.perf_counter()
+    for s in range(w + k, w + 2 * k):
+        sim.set_beam(0, host)
+        sim.step(s)
+        out = sim.get_beam(0)
+    sim.synchronize()
+    e2e_secs = time.perf_counter() - t0
+    h2d = nb * (7 * 8 + 8)
+    d2h = out["x"].size * (7 * 8 + 8)
+    # ---- profiled pass (kernel launches with events) for the roofline of the dominant kernel
+    sim.set_profiling(True)
+    for s in range(w + 2 * k, w + 3 * k):
+        sim.step(s)
+    classes = ["plasma_deposit", "beam_deposit", "poisson_psi_ez_bz", "explicit_deposit", "multigrid",
+               "plasma_push", "beam_push", "beam_partition"]
+    prof = {c: sim.profile(c) for c in classes}
+    sim.set_profiling(False)
+    total_prof = sum(v[0] for v in prof.values())
+    dominant = max(prof, key=lambda c: prof[c][0])
+    elem = 8 if args.precision == "fp64" else 4
+    push_ms, push_n = prof["plasma_push"]
+    peak, peak_kind = peaks()
+    push_bytes = n_plasma * PUSH_BYTES[elem]
+    achieved = push_bytes / (push_ms / 1e3 / max(push_n, 1)) / 1e9 if push_n else 0.0
+    counters = sim.counters()
+    line = {
+        "metric": "slices/s",
+        "value": value,
+        "unit": "slices/s",
+        "n_gpus": world,
+        "steps": k,
+        "warmup": w,
+        "ms_per_step": secs / k * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 (beam f64)",
+        "data": "synthetic: seeded Gaussian driver beam (Philox), lattice plasma",
+        "config": {"workload": args.config, "grid": [nx, ny, nz], "plasma_particles": n_plasma,
+                   "beam_particles": int(nb), "solver": "explicit+multigrid", "precision": args.precision,
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 per step (beam store)",
+                   "graphs": not args.no_graphs},
+        "particle_updates_per_s": n_plasma * nz * k * world / secs,
+        "e2e": {"value": nz * k / e2e_secs, "unit": "slices/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "kernel": "plasma_push", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "bytes_per_launch": push_bytes,
+                     "launch_ms": push_ms / max(push_n, 1)},
+        "kernel_share": {c: (prof[c][0] / total_prof if total_prof else 0) for c in classes},
+        "dominant_kernel_class": dominant,
+        "mg_vcycles_per_slice": counters["mg_vcycles"] / max(counters["slices"], 1),
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        line["gpu_launches"] = launches_in_timed
+        line["cpu_baseline"] = cpu_baseline(text, args)
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(text, args):
+    """This build's FP64 CPU oracle on a bounded sample of the same workload."""
+    from oracle_lib import Oracle
+    import hipace2_b200 as hp
+    o = Oracle(text)
+    g = hp.Hipace(text, graphs=False)
+    g.init_data()
+    o.set_beam(0, g.get_beam(0))
+    g.close()
+    nz = o.nz
+    n = args.cpu_sample_slices or max(4, min(nz, 24))
+    threads = o.L.oracle_threads()
+    t0 = time.perf_counter()
+    o.begin_step(0)
+    for s in range(nz - 1, nz - 1 - n, -1):
+        o.solve_slice(s, 0)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "slices/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} slices (head of the box) of step 0 of {args.config}, FP64 oracle"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU implementation of the path. The reference (AMReX,
+    FFTW, MPI) cannot be built on this image, so its restatement (oracle/) runs instead with all
+    host threads, on the same workload, a bounded slice sample per step."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from cases import config
+    from oracle_lib import Oracle, lib
+    text = config(args.config)
+    import hipace2_b200 as hp
+    try:
+        g = hp.Hipace(text, graphs=False)
+        g.init_data()
+        beam = g.get_beam(0)
+        g.close()
+    except Exception as e:  # no GPU: draw the same seeded beam is impossible without the library
+        print(json.dumps({"impl": "reference", "unavailable": f"beam generation needs libhpq: {e}"}))
+        return
+    o = Oracle(text)
+    o.set_beam(0, beam)
+    nz = o.nz
+    n = args.cpu_sample_slices or max(2, min(nz, 8))
+    for s in range(args.warmup):
+        o.begin_step(s)
+        for isl in range(nz - 1, nz - 1 - n, -1):
+            o.solve_slice(isl, s)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        o.begin_step(s)
+        for isl in range(nz - 1, nz - 1 - n, -1):
+            o.solve_slice(isl, s)
+    dt = time.perf_counter() - t0
+    v = n * args.steps / dt
+    threads = lib().oracle_threads()
+    print(json.dumps({
+        "impl": "reference", "metric": "slices/s", "value": v, "unit": "slices/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded Gaussian driver beam (Philox), lattice plasma",
+        "config": {"workload": args.config, "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "slices/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} head slices per step of {args.config}; reference binary not "
+                                   "buildable here (AMReX/FFTW/MPI absent), FP64 oracle restatement"},
+        "e2e": {"value": v, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,223 @@
+"""B200-native quasi-static slice loop (HiPACE++ slice solver) — Python host interface.
+
+The product is the C-ABI library libhpq.so (include/hpq.h) built from hipace2_b200/csrc for
+sm_100a. This module binds it with ctypes and mirrors the reference's driver surface:
+`Hipace(inputs)` (src/Hipace.cpp:74-244), `init_data()` (:246-295), `evolve()` (:393-554) and
+`solve_one_slice(islice, step)` (:556-728). There is no CPU fallback: loading fails loudly if
+the library or a CUDA device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Hipace", "HpqError", "load_library", "PLAIN_FP64", "MIXED"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhpq.so")
+PLAIN_FP64, MIXED = 0, 1
+ERRORS = {1: "input", 2: "cuda", 3: "state", 4: "not converged", 5: "diverged", 6: "argument"}
+
+# every entry point declared in include/hpq.h
+EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "hpq_set_precision",
+           "hpq_init", "hpq_set_beam", "hpq_beam_count", "hpq_get_beam", "hpq_step",
+           "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
+           "hpq_get_diag", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
+           "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
+           "hpq_get_profile")
+
+_lib = None
+
+
+class HpqError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"hpq error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def load_library(path=None):
+    """Load libhpq.so (building it first when the sources are newer and nvcc is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(path)
+    vp, cp, i32, i64 = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int64
+    dp, lp = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
+    sig = {
+        "hpq_create": ([cp, ctypes.POINTER(vp)], i32),
+        "hpq_destroy": ([vp], None),
+        "hpq_last_error": ([vp], cp),
+        "hpq_create_error": ([], cp),
+        "hpq_set_precision": ([vp, i32], i32),
+        "hpq_init": ([vp], i32),
+        "hpq_set_beam": ([vp, i32] + [dp] * 7 + [lp, i64], i32),
+        "hpq_beam_count": ([vp, i32, lp], i32),
+        "hpq_get_beam": ([vp, i32] + [dp] * 7 + [lp], i32),
+        "hpq_step": ([vp, i32], i32),
+        "hpq_begin_step": ([vp, i32], i32),
+        "hpq_solve_slice": ([vp, i32], i32),
+        "hpq_end_step": ([vp], i32),
+        "hpq_get_field": ([vp, cp, dp], i32),
+        "hpq_set_diag": ([vp, cp], i32),
+        "hpq_get_diag": ([vp, cp, dp], i32),
+        "hpq_plasma_count": ([vp, i32, lp], i32),
+        "hpq_get_plasma": ([vp, i32, dp], i32),
+        "hpq_set_graphs": ([vp, i32], i32),
+        "hpq_synchronize": ([vp], i32),
+        "hpq_stream": ([vp], vp),
+        "hpq_get_counters": ([vp, lp, lp, lp, lp], i32),
+        "hpq_set_profiling": ([vp, i32], i32),
+        "hpq_get_profile": ([vp, cp, dp, lp], i32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _lp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+
+
+BEAM_ATTRS = ("x", "y", "z", "w", "ux", "uy", "uz")
+PLASMA_ATTRS = ("x", "y", "w", "ux", "uy", "psi", "x_prev", "y_prev", "ux_half_step",
+                "uy_half_step", "psi_half_step", "valid")
+
+
+class Hipace:
+    """One simulation on one GPU, driven through libhpq."""
+
+    def __init__(self, input_text, precision=PLAIN_FP64, graphs=True):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        rc = self.L.hpq_create(input_text.encode(), ctypes.byref(h))
+        if rc:
+            raise HpqError(rc, self.L.hpq_create_error().decode())
+        self.h = h
+        self._check(self.L.hpq_set_precision(self.h, precision))
+        self._check(self.L.hpq_set_graphs(self.h, int(bool(graphs))))
+        self.n_cell = _n_cell(input_text)
+        self.max_step = _scalar(input_text, "max_step", 0)
+        self._diag = []
+
+    def _check(self, rc):
+        if rc:
+            raise HpqError(rc, self.L.hpq_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hpq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- reference driver surface
+    def init_data(self):
+        self._check(self.L.hpq_init(self.h))
+
+    def evolve(self, first_step=0, last_step=None):
+        last = self.max_step if last_step is None else last_step
+        for s in range(first_step, last + 1):
+            self.step(s)
+
+    def step(self, step):
+        self._check(self.L.hpq_step(self.h, step))
+
+    def begin_step(self, step):
+        self._check(self.L.hpq_begin_step(self.h, step))
+
+    def solve_one_slice(self, islice):
+        self._check(self.L.hpq_solve_slice(self.h, islice))
+
+    def end_step(self):
+        self._check(self.L.hpq_end_step(self.h))
+
+    # ---- data access
+    def set_beam(self, b, beam):
+        arrs = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in BEAM_ATTRS]
+        ids = beam.get("id")
+        ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.int64)
+        self._check(self.L.hpq_set_beam(self.h, b, *[_dp(a) for a in arrs],
+                                        _lp(ids) if ids is not None else None, len(arrs[0])))
+
+    def get_beam(self, b=0):
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_beam_count(self.h, b, ctypes.byref(n)))
+        out = {k: np.zeros(n.value) for k in BEAM_ATTRS}
+        out["id"] = np.zeros(n.value, dtype=np.int64)
+        self._check(self.L.hpq_get_beam(self.h, b, *[_dp(out[k]) for k in BEAM_ATTRS],
+                                        _lp(out["id"])))
+        return out
+
+    def get_field(self, comp):
+        nx, ny, _ = self.n_cell
+        out = np.zeros((ny, nx))
+        self._check(self.L.hpq_get_field(self.h, comp.encode(), _dp(out)))
+        return out
+
+    def set_diag(self, comps):
+        self._diag = list(comps)
+        self._check(self.L.hpq_set_diag(self.h, " ".join(comps).encode()))
+
+    def get_diag(self, comp):
+        nx, ny, nz = self.n_cell
+        out = np.zeros((nz, ny, nx))
+        self._check(self.L.hpq_get_diag(self.h, comp.encode(), _dp(out)))
+        return out
+
+    def get_plasma(self, sp=0):
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_plasma_count(self.h, sp, ctypes.byref(n)))
+        n = n.value
+        out = np.zeros(12 * n)
+        self._check(self.L.hpq_get_plasma(self.h, sp, _dp(out)))
+        return {k: out[i * n:(i + 1) * n] for i, k in enumerate(PLASMA_ATTRS)}
+
+    def synchronize(self):
+        self._check(self.L.hpq_synchronize(self.h))
+
+    def stream(self):
+        return self.L.hpq_stream(self.h)
+
+    def set_profiling(self, on):
+        self._check(self.L.hpq_set_profiling(self.h, int(bool(on))))
+
+    def profile(self, kernel_class):
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        self._check(self.L.hpq_get_profile(self.h, kernel_class.encode(), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def counters(self):
+        a, b, c, d = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.L.hpq_get_counters(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                            ctypes.byref(d)))
+        return {"mg_vcycles": a.value, "slices": b.value, "plasma_pushes": c.value, "kernel_launches": d.value}
+
+
+def _scalar(text, key, default):
+    v = default
+    for line in text.splitlines():
+        line = line.split("#")[0]
+        if "=" in line and line.split("=")[0].strip() == key:
+            v = int(float(line.split("=", 1)[1].split()[0]))
+    return v
+
+
+def _n_cell(text):
+    n = None
+    for line in text.splitlines():
+        line = line.split("#")[0]
+        if "=" in line and line.split("=")[0].strip() == "amr.n_cell":
+            n = [int(float(v)) for v in line.split("=", 1)[1].split()]
+    return n

@@ -1,0 +1,134 @@
+// Device-side building blocks shared by the slice-loop kernels: shape factors, field views,
+// atomics and launch helpers. Everything here is written for sm_100a.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace hpq {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define HPQ_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            throw ::hpq::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) +      \
+                                   " (" __FILE__ ":" + std::to_string(__LINE__) + ")");       \
+    } while (0)
+
+// kernel launches issued by this thread (each launch site is followed by one check)
+inline thread_local long long g_launches = 0;
+#define HPQ_LAUNCH_CHECK()                  \
+    do {                                    \
+        HPQ_CUDA(cudaGetLastError());       \
+        ++::hpq::g_launches;                \
+    } while (0)
+
+constexpr int kGuardAlloc = 3;   // allocated guard cells per side
+constexpr int kGuardPhys = 2;    // guard cells of the reference slice arrays (Fields.cpp:63)
+
+// 2-D view of one field component: element (i, j) of the interior index space.
+template <class R>
+struct F2 {
+    R* p;
+    int pitch;
+    __host__ __device__ R& operator()(int i, int j) const {
+        return p[(ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc)];
+    }
+    __host__ __device__ R* ptr(int i, int j) const {
+        return p + (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc);
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+// Shape factors, transverse order 2 (ShapeFactors.H:150-171 and the derivative shapes of
+// :212-468). Each returns weight and cell index for stencil point ix.
+// ------------------------------------------------------------------------------------------
+template <class R>
+struct Sh { R s; int cell; };
+template <class R>
+struct DSh { R s, ds; int cell; };
+
+template <class R>
+__device__ __forceinline__ Sh<R> shape2(R xmid, int ix) {
+    const R xfloor = floor(xmid + R(0.5));
+    const R xint = xmid - xfloor;
+    const int c = (int)xfloor;
+    if (ix == 0) return {R(0.5) * (R(0.5) - xint) * (R(0.5) - xint), c - 1};
+    if (ix == 1) return {R(0.75) - xint * xint, c};
+    return {R(0.5) * (R(0.5) + xint) * (R(0.5) + xint), c + 1};
+}
+
+// derivative type 1 ("nodal"), 4 points; used by the field gather (FieldGather.H:67)
+template <class R>
+__device__ __forceinline__ DSh<R> dshape_nodal2(R xmid, int ix) {
+    const R xfloor = floor(xmid);
+    const R xint = xmid - xfloor, x2 = xint * xint;
+    const bool lo = xint < R(0.5);
+    const int c = (int)xfloor - 1 + ix;
+    if (ix == 0) return {lo ? R(0.5) * x2 - R(0.5) * xint + R(1.0 / 8.0) : R(0), -(R(-0.5) * x2 + xint - R(0.5)), c};
+    if (ix == 1) return {lo ? R(3.0 / 4.0) - x2 : R(0.5) * x2 - R(1.5) * xint + R(9.0 / 8.0), -(R(1.5) * x2 - R(2) * xint), c};
+    if (ix == 2) return {lo ? R(0.5) * x2 + R(0.5) * xint + R(1.0 / 8.0) : -x2 + R(2) * xint - R(1.0 / 4.0), -(R(-1.5) * x2 + xint + R(0.5)), c};
+    return {lo ? R(0) : R(0.5) * x2 - R(0.5) * xint + R(1.0 / 8.0), -(R(0.5) * x2), c};
+}
+
+// derivative types 0 (analytic, 3 points), 1 (nodal, 4) and 2 (centred, 5) for the explicit
+// Sx/Sy deposition (ExplicitDeposition.cpp:173-176)
+template <class R, int TYPE>
+__device__ __forceinline__ DSh<R> dshape2(R xmid, int ix) {
+    if constexpr (TYPE == 0) {
+        xmid += R(0.5);
+        const R xfloor = floor(xmid);
+        const R xint = xmid - xfloor, x2 = xint * xint;
+        const int c = (int)xfloor - 1 + ix;
+        if (ix == 0) return {R(0.5) * x2 - xint + R(0.5), -(xint - R(1)), c};
+        if (ix == 1) return {-x2 + xint + R(0.5), -(R(1) - R(2) * xint), c};
+        return {R(0.5) * x2, -xint, c};
+    } else if constexpr (TYPE == 1) {
+        return dshape_nodal2<R>(xmid, ix);
+    } else {
+        xmid += R(0.5);
+        const R xfloor = floor(xmid);
+        const R xint = xmid - xfloor, x2 = xint * xint;
+        const int c = (int)xfloor - 2 + ix;
+        if (ix == 0) return {R(0), -(R(-0.25) * x2 + R(0.5) * xint - R(0.25)), c};
+        if (ix == 1) return {R(0.5) * x2 - xint + R(0.5), -(R(0.5) * x2 - R(0.5) * xint - R(0.25)), c};
+        if (ix == 2) return {-x2 + xint + R(0.5), -(R(0.25) - R(0.5) * xint), c};
+        if (ix == 3) return {R(0.5) * x2, -(R(-0.5) * x2 + R(0.5) * xint + R(0.25)), c};
+        return {R(0), -(R(0.25) * x2), c};
+    }
+}
+
+// Position in cell units clamped to [-1, n]: identity for particles inside the domain
+// (xmid in [-0.5, n-0.5]); keeps NaN/inf positions from indexing outside the guard cells.
+template <class R>
+__device__ __forceinline__ R clamp_mid(R xmid, int n) {
+    return fmin(fmax(xmid, R(-1)), R(n));
+}
+
+// grid-stride loop helpers
+__device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ long long gstride() { return (long long)gridDim.x * blockDim.x; }
+
+inline int blocks_for(long long n, int threads, int max_blocks = 148 * 16) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > max_blocks) b = max_blocks;
+    return (int)b;
+}
+
+// atomicMax on non-negative doubles through their bit pattern (monotone for x >= 0)
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+    atomicMax(reinterpret_cast<unsigned int*>(addr), (unsigned int)__float_as_int(v));
+}
+
+}  // namespace hpq

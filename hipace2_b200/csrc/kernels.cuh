@@ -1,0 +1,694 @@
+// Slice-loop kernels: plasma initialisation, deposition, explicit Sx/Sy deposition, push;
+// beam deposition, push and slice partition; elementwise field kernels.
+//
+// Every kernel reads the per-slice control block `Ctl` from device memory (slice index, step
+// parity, beam counters) so that one captured CUDA graph replays any slice of any step.
+#pragma once
+
+#include "common.cuh"
+#include "inputs.hpp"
+
+namespace hpq {
+
+// ------------------------------------------------------------------------------------------
+// Field components of the slice slab. Names follow Fields.cpp:49-148 (explicit and
+// predictor-corrector layouts); "N"/"P" prefixes are the Next/Previous slices.
+// ------------------------------------------------------------------------------------------
+enum Comp : int {
+    C_CHI = 0, C_SY, C_SX, C_EXMBY, C_EYPBX, C_EZ, C_BX, C_BY, C_BZ, C_PSI,
+    C_JXB, C_JYB, C_JZB, C_JX, C_JY, C_RHOMJZ, C_RHO, C_RHOMJZB,
+    C_NJXB, C_NJYB, C_PJXB, C_PJYB, C_IONS,
+    C_JZ, C_NJX, C_NJY, C_PBX, C_PBY, C_PJX, C_PJY, C_PCIBX, C_PCIBY, C_PCPBX, C_PCPBY,
+    C_NCOMP
+};
+
+template <class R>
+struct Slab {
+    R* base = nullptr;
+    int nx = 0, ny = 0, pitch = 0, rows = 0;
+    size_t cstride = 0;
+    __host__ __device__ F2<R> c(int comp) const { return {base + (size_t)comp * cstride, pitch}; }
+};
+
+constexpr int kMaxBeams = 4;
+constexpr int kMaxPlasmas = 4;
+
+struct BeamBuf {
+    double *x, *y, *z, *w, *ux, *uy, *uz;
+    long long* id;
+    int* nsub;
+    uint8_t* valid;
+};
+
+struct BeamDev {
+    BeamBuf buf[2];     // stores of the previous and the current step (by step parity)
+    BeamBuf carry[2];   // slipped particles handed from one slice to the next (by slice parity)
+    int* start[2];      // per-slice start/count in buf[.]
+    int* count[2];
+    double charge, mass;
+    int n_subcycles;
+    int do_z_push;
+    long long cap;
+};
+
+template <class R>
+struct PlasmaDev {
+    R *x, *y, *w, *ux, *uy, *psi, *xp, *yp, *uxh, *uyh, *psih;
+    uint8_t* valid;
+    long long n;
+    double charge, mass, qsa_max;
+    int n_subcycles;
+    int neutralize;
+};
+
+// dynamic per-slice state (device memory)
+struct Ctl {
+    int islice;
+    int step_parity;        // buf[step_parity] is read, buf[1-step_parity] is written
+    int carry_n[kMaxBeams][2];
+    int cursor[kMaxBeams];
+    int err;
+    // multigrid
+    double mg_target, mg_maxnorm, mg_norm;
+    int mg_iter, mg_go, mg_status, mg_pad;
+    long long mg_total_iters;
+    // predictor-corrector
+    double pc_err, pc_err_prev, pc_sum[2], pc_w[2], pc_mix;
+    int pc_iter, pc_go, pc_mixnow, pc_pad;
+};
+
+struct Geo {
+    int nx, ny, nz;
+    double plo[3], phi[3], dx[3], dxi[3];
+    double xoff, yoff;          // GetPosOffset for the 2-guard slice box (Fields.H:72-76)
+    double plo_p[2], phi_p[2];  // particle boundary
+    int bc;                     // ParticleBC
+    double c, ep0, mu0;
+    int normalized;
+};
+
+// ------------------------------------------------------------------------------------------
+// EnforceBC (GetAndSetPosition.H:29-99). Returns false when the particle is absorbed.
+// ------------------------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ bool enforce_bc(const Geo& g, T& x, T& y, T& ux, T& uy) {
+    const T plo0 = (T)g.plo_p[0], plo1 = (T)g.plo_p[1], phi0 = (T)g.phi_p[0], phi1 = (T)g.phi_p[1];
+    if (x < plo0 || y < plo1 || x > phi0 || y > phi1) {
+        const T lx = phi0 - plo0, ly = phi1 - plo1;
+        if (g.bc == 0) {
+            x = fmod(x - plo0, T(2) * lx); if (x < 0) x += T(2) * lx; x += plo0;
+            if (x > phi0) { x = T(2) * phi0 - x; ux = -ux; }
+            y = fmod(y - plo1, T(2) * ly); if (y < 0) y += T(2) * ly; y += plo1;
+            if (y > phi1) { y = T(2) * phi1 - y; uy = -uy; }
+            return true;
+        } else if (g.bc == 1) {
+            x = fmod(x - plo0, lx); if (x < 0) x += lx; x += plo0;
+            y = fmod(y - plo1, ly); if (y < 0) y += ly; y += plo1;
+            return true;
+        }
+        return false;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------
+// Plasma initialisation (PlasmaParticleContainerInit.cpp:17-310): the particle list of one
+// species is fixed on the host (lattice positions that pass the domain/radius tests); the
+// kernel evaluates the density expression at c*t and resets all attributes.
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void k_plasma_reset(PlasmaDev<R> P, const double* __restrict__ x0, const double* __restrict__ y0,
+                               Expr density, double c_t, double scale, double ux0, double uy0, double uz0,
+                               double clight) {
+    for (long long i = gtid(); i < P.n; i += gstride()) {
+        const double x = x0[i], y = y0[i];
+        double v[3] = {x, y, c_t};
+        const double w = density.eval(v) * scale;
+        const double psi = sqrt(1. + ux0 * ux0 + uy0 * uy0 + uz0 * uz0) - uz0;
+        P.x[i] = (R)x; P.y[i] = (R)y; P.xp[i] = (R)x; P.yp[i] = (R)y;
+        P.w[i] = (R)w;
+        P.ux[i] = (R)(ux0 * clight); P.uy[i] = (R)(uy0 * clight);
+        P.uxh[i] = (R)(ux0 * clight); P.uyh[i] = (R)(uy0 * clight);
+        P.psi[i] = (R)psi; P.psih[i] = (R)psi;
+        P.valid[i] = 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Plasma current deposition, order 2 (PlasmaDepositCurrent.cpp:22-259). Null outputs are
+// skipped. QSA-violating particles (gamma/psi outside (0, max]) are invalidated (:199-206).
+// ------------------------------------------------------------------------------------------
+template <class R>
+struct DepOut {
+    R *jx, *jy, *jz, *rho, *chi, *rhomjz;
+    int pitch;
+};
+
+template <class R>
+__device__ __forceinline__ void addc(R* base, int pitch, int i, int j, R v) {
+    atomicAdd(base + (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc), v);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
+                                                        const int* gate = nullptr) {
+    if (gate && !*gate) return;
+    const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
+    const R clight = (R)g.c, clightinv = (R)(1.0 / g.c);
+    const R charge_invvol = (R)charge * invvol;
+    const R q_mu0_mass_ratio = (R)(charge * g.mu0 / P.mass);
+    const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
+    const R qsa = (R)P.qsa_max;
+    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
+        if (!P.valid[ip]) continue;
+        const R psi_inv = R(1) / P.psi[ip];
+        const R vx_c = P.ux[ip] * psi_inv;
+        const R vy_c = P.uy[ip] * psi_inv;
+        const R q_invvol = charge_invvol * P.w[ip];
+        const R xmid = clamp_mid<R>((P.x[ip] - xoff) * dxi, g.nx);
+        const R ymid = clamp_mid<R>((P.y[ip] - yoff) * dyi, g.ny);
+        const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                      vy_c * vy_c * clightinv * clightinv + R(1));
+        if (gamma_psi < R(0) || gamma_psi > qsa || psi_inv < R(0)) {
+            P.w[ip] = R(0);
+            P.valid[ip] = 0;
+            continue;
+        }
+        Sh<R> sx[3], sy[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k); }
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy)
+#pragma unroll
+            for (int ix = 0; ix < 3; ++ix) {
+                const int i = sx[ix].cell, j = sy[iy].cell;
+                const R cd = q_invvol * sx[ix].s * sy[iy].s;
+                if (o.jx) { addc(o.jx, o.pitch, i, j, cd * vx_c); addc(o.jy, o.pitch, i, j, cd * vy_c); }
+                if (o.jz) addc(o.jz, o.pitch, i, j, cd * (gamma_psi - R(1)) * clight);
+                if (o.rho) addc(o.rho, o.pitch, i, j, cd * gamma_psi);
+                if (o.chi) addc(o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
+                if (o.rhomjz) addc(o.rhomjz, o.pitch, i, j, cd);
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Explicit Sx/Sy deposition (ExplicitDeposition.cpp:20-265, no laser)
+// ------------------------------------------------------------------------------------------
+template <class R, int DT>
+__global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g) {
+    const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
+    const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);
+    const R charge_invvol_mu0 = (R)(P.charge * (double)invvol * g.mu0);
+    const R q_mass_ratio = (R)(P.charge / P.mass);
+    const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
+    const F2<R> Bz = S.c(C_BZ), Ez = S.c(C_EZ), Ex = S.c(C_EXMBY), Ey = S.c(C_EYPBX);
+    R* Sx = S.c(C_SX).p;
+    R* Sy = S.c(C_SY).p;
+    constexpr int NS = 3 + DT;
+    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
+        if (!P.valid[ip]) continue;
+        const R psi_inv = R(1) / P.psi[ip];
+        const R vx = P.ux[ip] * psi_inv * clight_inv;
+        const R vy = P.uy[ip] * psi_inv * clight_inv;
+        const R cdm = charge_invvol_mu0 * P.w[ip];
+        const R xmid = clamp_mid<R>((P.x[ip] - xoff) * dxi, g.nx), ymid = clamp_mid<R>((P.y[ip] - yoff) * dyi, g.ny);
+        const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx * vx + vy * vy + R(1));
+        DSh<R> sx[NS], sy[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) { sx[k] = dshape2<R, DT>(xmid, k); sy[k] = dshape2<R, DT>(ymid, k); }
+#pragma unroll
+        for (int iy = 0; iy < NS; ++iy)
+#pragma unroll
+            for (int ix = 0; ix < NS; ++ix) {
+                if (DT == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                const int i = sx[ix].cell, j = sy[iy].cell;
+                const R Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = Ex(i, j), EypBx_v = Ey(i, j);
+                const R sxs = sx[ix].s, sys = sy[iy].s, sxd = sx[ix].ds, syd = sy[iy].ds;
+                const R vsy = cdm * (-sxs * sys * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * clight_inv) * q_mass_ratio * psi_inv +
+                                     (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * (gamma_psi - vy * vy - R(1))) * a_clight);
+                const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
+                                     (+sxd * sys * dxi * (gamma_psi - vx * vx - R(1)) + sxs * syd * dyi * (-vx * vy)) * a_clight);
+                addc(Sy, S.pitch, i, j, vsy);
+                addc(Sx, S.pitch, i, j, vsx);
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Field gather (FieldGather.H:45-96, derivative type 1, 4x4 stencil)
+// ------------------------------------------------------------------------------------------
+template <class R, class T>
+__device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T yp, T& ExmBy, T& EypBx, T& Ez,
+                                       T& Bx, T& By, T& Bz) {
+    const T dxi = (T)g.dxi[0], dyi = (T)g.dxi[1];
+    const T x = clamp_mid<T>((xp - (T)g.xoff) * dxi, g.nx), y = clamp_mid<T>((yp - (T)g.yoff) * dyi, g.ny);
+    const F2<R> Psi = S.c(C_PSI), FEz = S.c(C_EZ), FBx = S.c(C_BX), FBy = S.c(C_BY), FBz = S.c(C_BZ);
+    DSh<T> sx[4], sy[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { sx[k] = dshape_nodal2<T>(x, k); sy[k] = dshape_nodal2<T>(y, k); }
+#pragma unroll
+    for (int iy = 0; iy < 4; iy++)
+#pragma unroll
+        for (int ix = 0; ix < 4; ix++) {
+            const int i = sx[ix].cell, j = sy[iy].cell;
+            const T psi = (T)Psi(i, j);
+            ExmBy += (sx[ix].ds * sy[iy].s) * psi * dxi;
+            EypBx += (sx[ix].s * sy[iy].ds) * psi * dyi;
+            const T s = sx[ix].s * sy[iy].s;
+            Ez += s * (T)FEz(i, j);
+            Bx += s * (T)FBx(i, j);
+            By += s * (T)FBy(i, j);
+            Bz += s * (T)FBz(i, j);
+        }
+}
+
+// ------------------------------------------------------------------------------------------
+// Plasma push (PlasmaParticleAdvance.cpp:29-217; PlasmaMomentumPush PushPlasmaParticles.H:39-75)
+// Leapfrog in zeta: 4 Taylor sub-steps (second order through a dual-number derivative) for
+// u and psi from -1/2 to +1/2, full position step, 2 more sub-steps to the slice.
+// ------------------------------------------------------------------------------------------
+template <class R>
+struct Du { R v, e; };
+template <class R> __device__ __forceinline__ Du<R> operator+(Du<R> a, Du<R> b) { return {a.v + b.v, a.e + b.e}; }
+template <class R> __device__ __forceinline__ Du<R> operator-(Du<R> a, Du<R> b) { return {a.v - b.v, a.e - b.e}; }
+template <class R> __device__ __forceinline__ Du<R> operator*(Du<R> a, Du<R> b) { return {a.v * b.v, a.e * b.v + a.v * b.e}; }
+
+template <class T>
+__device__ __forceinline__ void plasma_rhs(const T& ux, const T& uy, const T& pi, T ExmBy, T EypBx, T Ez, T Bxc, T Byc,
+                                           T Bz, T ci, T qmc, T& dux, T& duy, T& dpsi) {
+    const T gp = T(0.5) * pi * pi * (T(1.0) + ux * ux * T(ci * ci) + uy * uy * T(ci * ci)) + T(0.5);
+    dux = T(qmc) * (gp * T(ExmBy) + T(Byc) + (uy * T(Bz)) * pi);
+    duy = T(qmc) * (gp * T(EypBx) - T(Bxc) - (ux * T(Bz)) * pi);
+    dpsi = T(qmc) * T(ci) * ((ux * T(ExmBy) + uy * T(EypBx)) * T(ci) * pi - T(Ez));
+}
+template <class R>
+__device__ __forceinline__ void plasma_rhs_dual(Du<R> ux, Du<R> uy, Du<R> pi, R ExmBy, R EypBx, R Ez, R Bxc, R Byc,
+                                                R Bz, R ci, R qmc, Du<R>& dux, Du<R>& duy, Du<R>& dpsi) {
+    const Du<R> c2{ci * ci, 0};
+    const Du<R> gp = Du<R>{R(0.5), 0} * pi * pi * (Du<R>{R(1.0), 0} + ux * ux * c2 + uy * uy * c2) + Du<R>{R(0.5), 0};
+    dux = Du<R>{qmc, 0} * (gp * Du<R>{ExmBy, 0} + Du<R>{Byc, 0} + (uy * Du<R>{Bz, 0}) * pi);
+    duy = Du<R>{qmc, 0} * (gp * Du<R>{EypBx, 0} - Du<R>{Bxc, 0} - (ux * Du<R>{Bz, 0}) * pi);
+    dpsi = Du<R>{qmc, 0} * Du<R>{ci, 0} * ((ux * Du<R>{ExmBy, 0} + uy * Du<R>{EypBx, 0}) * Du<R>{ci, 0} * pi - Du<R>{Ez, 0});
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, Geo g, int temp,
+                                                     const int* gate = nullptr) {
+    if (gate && !*gate) return;
+    const R clight = (R)g.c, ci = (R)(1. / g.c);
+    const R qmc = (R)(P.charge / (P.mass * g.c));
+    const int nsubc = P.n_subcycles;
+    const R dzs = (R)(g.dx[2] / nsubc);
+    const R sdz = dzs / R(4);
+    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
+        if (!P.valid[ip]) continue;
+        for (int isc = 0; isc < nsubc; ++isc) {
+            R xp = P.xp[ip], yp = P.yp[ip];
+            R Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+            gather<R, R>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
+            Bx *= clight; By *= clight;
+            R ux = P.uxh[ip], uy = P.uyh[ip], psi = P.psih[ip];
+            auto substep = [&]() {
+                const R pi = R(1) / psi;
+                R d0, d1, d2;
+                plasma_rhs<R>(ux, uy, pi, Ex, Ey, Ez, Bx, By, Bz, ci, qmc, d0, d1, d2);
+                Du<R> e0, e1, e2;
+                plasma_rhs_dual<R>({ux, d0}, {uy, d1}, {pi, -pi * pi * d2}, Ex, Ey, Ez, Bx, By, Bz, ci, qmc, e0, e1, e2);
+                ux += sdz * d0 + R(0.5) * sdz * sdz * e0.e;
+                uy += sdz * d1 + R(0.5) * sdz * sdz * e1.e;
+                psi += sdz * d2 + R(0.5) * sdz * sdz * e2.e;
+            };
+#pragma unroll
+            for (int k = 0; k < 4; ++k) substep();
+            xp += dzs * ci * (ux * (R(1) / psi));
+            yp += dzs * ci * (uy * (R(1) / psi));
+            if (!enforce_bc<R>(g, xp, yp, ux, uy)) { P.w[ip] = R(0); P.valid[ip] = 0; break; }
+            P.x[ip] = xp; P.y[ip] = yp;
+            if (!temp) {
+                P.uxh[ip] = ux; P.uyh[ip] = uy; P.psih[ip] = psi;
+                P.xp[ip] = xp; P.yp[ip] = yp;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) substep();
+            P.ux[ip] = ux; P.uy[ip] = uy; P.psi[ip] = psi;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Beam deposition (BeamDepositCurrent.cpp:21-196): the non-slipped particles of slice
+// `ctl->islice - which` of the current store.
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __restrict__ ctl, int which, R* jx, R* jy,
+                                                      R* jz, R* rmj, int pitch, Geo g, int gated = 0) {
+    if (gated && !ctl->pc_go) return;
+    const int s = ctl->islice - which;
+    if (s < 0) return;
+    const int par = ctl->step_parity;
+    const int start = B.start[par][s], n = B.count[par][s];
+    const BeamBuf b = B.buf[par];
+    const double invvol = g.normalized ? 1.0 : g.dxi[0] * g.dxi[1] * g.dxi[2];
+    const double clightinv = 1.0 / g.c, clightsq = 1.0 / (g.c * g.c);
+    for (long long k = gtid(); k < n; k += gstride()) {
+        const long long ip = start + k;
+        if (!b.valid[ip]) continue;
+        const double ux = b.ux[ip], uy = b.uy[ip], uz = b.uz[ip];
+        const double gaminv = 1.0 / sqrt(1.0 + ux * ux * clightsq + uy * uy * clightsq + uz * uz * clightsq);
+        const double wq = B.charge * b.w[ip] * invvol;
+        const double vx = ux * gaminv, vy = uy * gaminv, vz = uz * gaminv;
+        const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
+        const double xmid = clamp_mid<double>((b.x[ip] - g.xoff) * g.dxi[0], g.nx);
+        const double ymid = clamp_mid<double>((b.y[ip] - g.yoff) * g.dxi[1], g.ny);
+        Sh<double> sx[3], sy[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { sx[q] = shape2<double>(xmid, q); sy[q] = shape2<double>(ymid, q); }
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy)
+#pragma unroll
+            for (int ix = 0; ix < 3; ++ix) {
+                const double S = sx[ix].s * sy[iy].s;
+                const int i = sx[ix].cell, j = sy[iy].cell;
+                if (jx) { addc<R>(jx, pitch, i, j, (R)(S * wqx)); addc<R>(jy, pitch, i, j, (R)(S * wqy)); }
+                if (jz) addc<R>(jz, pitch, i, j, (R)(S * wqz));
+                if (rmj) addc<R>(rmj, pitch, i, j, (R)(S * wqr));
+            }
+    }
+}
+
+// Both beam depositions of the explicit solver in one launch: jz_beam (and rhomjz_beam) from the
+// non-slipped particles of this slice, jx_beam/jy_beam of the next slice from its particles.
+template <class R>
+__global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const Ctl* __restrict__ ctl, R* jz, R* rmj,
+                                                                R* njx, R* njy, int pitch, Geo g) {
+    const int s = ctl->islice;
+    const int par = ctl->step_parity;
+    const int st0 = B.start[par][s], n0 = B.count[par][s];
+    const int st1 = s > 0 ? B.start[par][s - 1] : 0, n1 = (s > 0 && njx) ? B.count[par][s - 1] : 0;
+    const BeamBuf b = B.buf[par];
+    const double invvol = g.normalized ? 1.0 : g.dxi[0] * g.dxi[1] * g.dxi[2];
+    const double clightinv = 1.0 / g.c, clightsq = 1.0 / (g.c * g.c);
+    for (long long k = gtid(); k < n0 + n1; k += gstride()) {
+        const bool nxt = k >= n0;
+        const long long ip = nxt ? st1 + (k - n0) : st0 + k;
+        if (!b.valid[ip]) continue;
+        const double ux = b.ux[ip], uy = b.uy[ip], uz = b.uz[ip];
+        const double gaminv = 1.0 / sqrt(1.0 + ux * ux * clightsq + uy * uy * clightsq + uz * uz * clightsq);
+        const double wq = B.charge * b.w[ip] * invvol;
+        const double vx = ux * gaminv, vy = uy * gaminv, vz = uz * gaminv;
+        const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
+        const double xmid = clamp_mid<double>((b.x[ip] - g.xoff) * g.dxi[0], g.nx);
+        const double ymid = clamp_mid<double>((b.y[ip] - g.yoff) * g.dxi[1], g.ny);
+        Sh<double> sx[3], sy[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { sx[q] = shape2<double>(xmid, q); sy[q] = shape2<double>(ymid, q); }
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy)
+#pragma unroll
+            for (int ix = 0; ix < 3; ++ix) {
+                const double S = sx[ix].s * sy[iy].s;
+                const int i = sx[ix].cell, j = sy[iy].cell;
+                if (nxt) {
+                    addc<R>(njx, pitch, i, j, (R)(S * wqx));
+                    addc<R>(njy, pitch, i, j, (R)(S * wqy));
+                } else {
+                    addc<R>(jz, pitch, i, j, (R)(S * wqz));
+                    if (rmj) addc<R>(rmj, pitch, i, j, (R)(S * wqr));
+                }
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Beam push (BeamParticleAdvance.cpp:19-336; FP64 throughout). Pushes the non-slipped
+// particles of this slice and the particles that slipped in from the previous slice, resuming
+// at their sub-cycle count; a particle stops when it leaves the slice (z < slice lower edge).
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restrict__ ctl, int bi, Slab<R> S, Geo g,
+                                                   double dt) {
+    const int s = ctl->islice;
+    const int par = ctl->step_parity;
+    const int start = B.start[par][s], na = B.count[par][s];
+    const int cin = (s + 1) & 1;
+    const int nc = ctl->carry_n[bi][cin];
+    const BeamBuf a = B.buf[par];
+    const BeamBuf c = B.carry[cin];
+    const int nsubc = B.n_subcycles;
+    const double dtb = dt / nsubc;
+    const double clight = g.c, inv_c2 = 1. / (g.c * g.c);
+    const double cmr = B.charge / B.mass;
+    const double min_z = g.plo[2] + s * g.dx[2];
+    for (long long k = gtid(); k < na + nc; k += gstride()) {
+        const BeamBuf& bb = k < na ? a : c;
+        const long long ip = k < na ? start + k : k - na;
+        if (!bb.valid[ip]) continue;
+        double xp = bb.x[ip], yp = bb.y[ip], zp = bb.z[ip], ux = bb.ux[ip], uy = bb.uy[ip], uz = bb.uz[ip];
+        int i = bb.nsub[ip];
+        bool absorbed = false;
+        for (; i < nsubc; i++) {
+            if (zp < min_z) break;
+            const double gpi = 1. / sqrt(1. + (ux * ux + uy * uy + uz * uz) * inv_c2);
+            xp += dtb * 0.5 * ux * gpi;
+            yp += dtb * 0.5 * uy * gpi;
+            if (!enforce_bc<double>(g, xp, yp, ux, uy)) { absorbed = true; break; }
+            double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+            gather<R, double>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
+            const double uxn = ux + dtb * cmr * (Ex + (clight - uz * gpi) * By + uy * gpi * Bz);
+            const double uyn = uy + dtb * cmr * (Ey + (uz * gpi - clight) * Bx - ux * gpi * Bz);
+            const double uxi = (uxn + ux) * 0.5, uyi = (uyn + uy) * 0.5;
+            const double uzi = uz + dtb * 0.5 * cmr * Ez;
+            const double gii = 1. / sqrt(1. + (uxi * uxi + uyi * uyi + uzi * uzi) * inv_c2);
+            const double uzn = uz + dtb * cmr * (Ez + (uxi * By - uyi * Bx) * gii);
+            const double gni = 1. / sqrt(1. + (uxn * uxn + uyn * uyn + uzn * uzn) * inv_c2);
+            xp += dtb * 0.5 * uxn * gni;
+            yp += dtb * 0.5 * uyn * gni;
+            if (B.do_z_push) zp += dtb * (uzn * gni - clight);
+            ux = uxn; uy = uyn; uz = uzn;
+        }
+        if (absorbed || !enforce_bc<double>(g, xp, yp, ux, uy)) { bb.w[ip] = 0; bb.valid[ip] = 0; continue; }
+        bb.x[ip] = xp; bb.y[ip] = yp; bb.z[ip] = zp; bb.nsub[ip] = i;
+        bb.ux[ip] = ux; bb.uy[ip] = uy; bb.uz[ip] = uz;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Slice partition after the beam push (SliceSort.cpp:13-64 with the MultiBuffer hand-off,
+// MultiBuffer.cpp:806-926): invalid particles are dropped, particles still on this slice are
+// appended to the next step's store (sub-cycle count reset), slipped particles go to the carry
+// buffer of the next slice. One block; stable order via block-wide prefix sums.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void copy_particle(const BeamBuf& d, long long di, const BeamBuf& s, long long si, int nsub) {
+    d.x[di] = s.x[si]; d.y[di] = s.y[si]; d.z[di] = s.z[si]; d.w[di] = s.w[si];
+    d.ux[di] = s.ux[si]; d.uy[di] = s.uy[si]; d.uz[di] = s.uz[si];
+    d.id[di] = s.id[si]; d.nsub[di] = nsub; d.valid[di] = 1;
+}
+
+__global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, int bi, Geo g, int keep_store,
+                                                         int end_slice) {
+    __shared__ int sst[32], ssl[32];
+    __shared__ int base_stay, base_slip;
+    const int s = ctl->islice;
+    const int par = ctl->step_parity;
+    const int start = B.start[par][s], na = B.count[par][s];
+    const int cin = (s + 1) & 1, cout = s & 1;
+    const int nc = ctl->carry_n[bi][cin];
+    const BeamBuf a = B.buf[par];
+    const BeamBuf c = B.carry[cin];
+    const BeamBuf o = B.buf[1 - par];
+    const BeamBuf co = B.carry[cout];
+    const double min_z = g.plo[2] + s * g.dx[2];
+    const int cursor = ctl->cursor[bi];
+    if (threadIdx.x == 0) { base_stay = 0; base_slip = 0; }
+    __syncthreads();
+    const int total = na + nc;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int chunk = 0; chunk < total; chunk += blockDim.x) {
+        const int k = chunk + threadIdx.x;
+        int stay = 0, slip = 0;
+        const BeamBuf& bb = k < na ? a : c;
+        const long long ip = k < na ? start + k : k - na;
+        if (k < total && bb.valid[ip]) {
+            if (bb.z[ip] >= min_z) stay = 1; else slip = 1;
+        }
+        // inclusive warp scans
+        int vs = stay, vl = slip;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int t1 = __shfl_up_sync(0xffffffffu, vs, d), t2 = __shfl_up_sync(0xffffffffu, vl, d);
+            if (lane >= d) { vs += t1; vl += t2; }
+        }
+        if (lane == 31) { sst[warp] = vs; ssl[warp] = vl; }
+        __syncthreads();
+        if (warp == 0) {
+            int ws = lane < (int)(blockDim.x >> 5) ? sst[lane] : 0;
+            int wl = lane < (int)(blockDim.x >> 5) ? ssl[lane] : 0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                int t1 = __shfl_up_sync(0xffffffffu, ws, d), t2 = __shfl_up_sync(0xffffffffu, wl, d);
+                if (lane >= d) { ws += t1; wl += t2; }
+            }
+            sst[lane] = ws; ssl[lane] = wl;
+        }
+        __syncthreads();
+        const int off_s = (warp ? sst[warp - 1] : 0) + vs - stay;
+        const int off_l = (warp ? ssl[warp - 1] : 0) + vl - slip;
+        if (stay && keep_store) copy_particle(o, cursor + base_stay + off_s, bb, ip, 0);
+        if (slip) copy_particle(co, base_slip + off_l, bb, ip, bb.nsub[ip]);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            base_stay += sst[(blockDim.x >> 5) - 1];
+            base_slip += ssl[(blockDim.x >> 5) - 1];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        B.start[1 - par][s] = cursor;
+        B.count[1 - par][s] = keep_store ? base_stay : 0;
+        if (keep_store) ctl->cursor[bi] = cursor + base_stay;
+        ctl->carry_n[bi][cout] = base_slip;
+        if (end_slice) ctl->islice = s - 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Elementwise field kernels
+// ------------------------------------------------------------------------------------------
+struct CompList {
+    int n;
+    int c[24];
+};
+
+// zero listed components over the whole allocated slice (setVal on growntilebox)
+template <class R>
+__global__ void k_zero_comps(Slab<R> S, CompList L) {
+    const size_t n = S.cstride;
+    for (long long k = gtid(); k < (long long)n; k += gstride())
+#pragma unroll 4
+        for (int q = 0; q < L.n; ++q) S.base[(size_t)L.c[q] * S.cstride + k] = R(0);
+}
+
+// dst[q] = src[q] over the whole allocated slice (Fields::shift / duplicate)
+struct CopyList {
+    int n;
+    int dst[8], src[8];
+};
+template <class R>
+__global__ void k_copy_comps(Slab<R> S, CopyList L) {
+    const size_t n = S.cstride;
+    for (long long k = gtid(); k < (long long)n; k += gstride())
+        for (int q = 0; q < L.n; ++q) S.base[(size_t)L.dst[q] * S.cstride + k] = S.base[(size_t)L.src[q] * S.cstride + k];
+}
+
+// AddRhoIons + the three right-hand sides of SolvePoissonPsiExmByEypBxEzBz
+// (Fields.cpp:606-615, 840-903). Staging layout: stage[(j*3 + k)*ldx + i], k = Psi, Ez, Bz.
+template <class R>
+__global__ void k_rhs3(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int sj, int add_ions, int add_rho, int add_rmb) {
+    const int ax = S.nx + 2 * kGuardAlloc;
+    const long long ntot = (long long)ax * S.rows;
+    const F2<R> rm = S.c(C_RHOMJZ), jx = S.c(C_JX), jy = S.c(C_JY), ions = S.c(C_IONS), rho = S.c(C_RHO),
+                rmb = S.c(C_RHOMJZB);
+    const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]);
+    const R fe = (R)(1. / (g.ep0 * g.c)), mu0 = (R)g.mu0, mep = (R)(-1. / g.ep0);
+    for (long long k = gtid(); k < ntot; k += gstride()) {
+        const int i = (int)(k % ax) - kGuardAlloc, j = (int)(k / ax) - kGuardAlloc;
+        R r = rm(i, j);
+        if (add_ions) { r += ions(i, j); if (add_rho) rho(i, j) += ions(i, j); }
+        if (add_rmb) r += rmb(i, j);
+        if (add_ions || add_rmb) rm(i, j) = r;
+        if (i >= 0 && i < S.nx && j >= 0 && j < S.ny) {
+            R* st = stage + (size_t)j * sj + i;
+            st[0] = mep * r;
+            st[sk] = fe * ((jx(i + 1, j) - jx(i - 1, j)) * hx) + fe * ((jy(i, j + 1) - jy(i, j - 1)) * hy);
+            st[2 * (size_t)sk] = mu0 * ((jx(i, j + 1) - jx(i, j - 1)) * hy) + (-mu0) * ((jy(i + 1, j) - jy(i - 1, j)) * hx);
+        }
+    }
+}
+
+// ExmBy = -dPsi/dx, EypBx = -dPsi/dy on the box grown by one guard (Fields.cpp:931-956)
+template <class R>
+__global__ void k_grad_psi(Slab<R> S, Geo g) {
+    const int w = S.nx + 2, h = S.ny + 2;
+    const F2<R> Psi = S.c(C_PSI), Ex = S.c(C_EXMBY), Ey = S.c(C_EYPBX);
+    const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]);
+    for (long long k = gtid(); k < (long long)w * h; k += gstride()) {
+        const int i = (int)(k % w) - 1, j = (int)(k / w) - 1;
+        Ex(i, j) = -(Psi(i + 1, j) - Psi(i - 1, j)) * hx;
+        Ey(i, j) = -(Psi(i, j + 1) - Psi(i, j - 1)) * hy;
+    }
+}
+
+// ExmBy/EypBx = -grad Psi (Fields.cpp:931-956) and the beam part of Sx, Sy
+// (Hipace.cpp:744-790) in one launch
+template <class R>
+__global__ void k_grad_psi_sxsy(Slab<R> S, Geo g) {
+    const int w = S.nx + 2, h = S.ny + 2;
+    const F2<R> Psi = S.c(C_PSI), Ex = S.c(C_EXMBY), Ey = S.c(C_EYPBX);
+    const F2<R> jzb = S.c(C_JZB), pjx = S.c(C_PJXB), pjy = S.c(C_PJYB), njx = S.c(C_NJXB), njy = S.c(C_NJYB),
+                Sx = S.c(C_SX), Sy = S.c(C_SY);
+    const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]);
+    const R mu0 = (R)g.mu0;
+    const R dx2 = (R)(2. * g.dx[0]), dy2 = (R)(2. * g.dx[1]), dz2 = (R)(2. * g.dx[2]);
+    for (long long k = gtid(); k < (long long)w * h; k += gstride()) {
+        const int i = (int)(k % w) - 1, j = (int)(k / w) - 1;
+        Ex(i, j) = -(Psi(i + 1, j) - Psi(i - 1, j)) * hx;
+        Ey(i, j) = -(Psi(i, j + 1) - Psi(i, j - 1)) * hy;
+        if (i >= 0 && i < S.nx && j >= 0 && j < S.ny) {
+            const R dx_jzb = (jzb(i + 1, j) - jzb(i - 1, j)) / dx2;
+            const R dy_jzb = (jzb(i, j + 1) - jzb(i, j - 1)) / dy2;
+            const R dz_jxb = (pjx(i, j) - njx(i, j)) / dz2;
+            const R dz_jyb = (pjy(i, j) - njy(i, j)) / dz2;
+            Sy(i, j) = mu0 * (-dy_jzb + dz_jyb);
+            Sx(i, j) = -mu0 * (-dx_jzb + dz_jxb);
+        }
+    }
+}
+
+// Sx, Sy from the beam currents (Hipace.cpp:744-790)
+template <class R>
+__global__ void k_sxsy_beam(Slab<R> S, Geo g) {
+    const F2<R> jzb = S.c(C_JZB), pjx = S.c(C_PJXB), pjy = S.c(C_PJYB), njx = S.c(C_NJXB), njy = S.c(C_NJYB),
+                Sx = S.c(C_SX), Sy = S.c(C_SY);
+    const R mu0 = (R)g.mu0;
+    const R dx2 = (R)(2. * g.dx[0]), dy2 = (R)(2. * g.dx[1]), dz2 = (R)(2. * g.dx[2]);
+    for (long long k = gtid(); k < (long long)S.nx * S.ny; k += gstride()) {
+        const int i = (int)(k % S.nx), j = (int)(k / S.nx);
+        const R dx_jzb = (jzb(i + 1, j) - jzb(i - 1, j)) / dx2;
+        const R dy_jzb = (jzb(i, j + 1) - jzb(i, j - 1)) / dy2;
+        const R dz_jxb = (pjx(i, j) - njx(i, j)) / dz2;
+        const R dz_jyb = (pjy(i, j) - njy(i, j)) / dz2;
+        Sy(i, j) = mu0 * (-dy_jzb + dz_jyb);
+        Sx(i, j) = -mu0 * (-dx_jzb + dz_jxb);
+    }
+}
+
+// PC: right-hand sides of Bx, By (Fields.cpp:1008-1078) into stage rows k = 0 (Bx), 1 (By)
+template <class R>
+__global__ void k_rhs_bxby(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int sj) {
+    const F2<R> jz = S.c(C_JZ), pjx = S.c(C_PJX), pjy = S.c(C_PJY), njx = S.c(C_NJX), njy = S.c(C_NJY);
+    const R mu0 = (R)g.mu0;
+    const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]), hz = (R)(0.5 * g.dxi[2]);
+    for (long long k = gtid(); k < (long long)S.nx * S.ny; k += gstride()) {
+        const int i = (int)(k % S.nx), j = (int)(k / S.nx);
+        R* st = stage + (size_t)j * sj + i;
+        st[0] = -mu0 * ((jz(i, j + 1) - jz(i, j - 1)) * hy) + mu0 * ((pjy(i, j) - njy(i, j)) * hz);
+        st[sk] = mu0 * ((jz(i + 1, j) - jz(i - 1, j)) * hx) + (-mu0) * ((pjx(i, j) - njx(i, j)) * hz);
+    }
+}
+
+// copy interior of listed components into the 3-D diagnostic buffer at the current slice
+// out layout: [q][nz][ny][nx]
+template <class R>
+__global__ void k_diag_copy(Slab<R> S, const Ctl* ctl, CompList L, double* __restrict__ out, int nz) {
+    const int s = ctl->islice;
+    const long long nxy = (long long)S.nx * S.ny;
+    for (long long k = gtid(); k < nxy * L.n; k += gstride()) {
+        const int q = (int)(k / nxy);
+        const long long r = k % nxy;
+        const int i = (int)(r % S.nx), j = (int)(r / S.nx);
+        out[((size_t)q * nz + s) * nxy + r] = (double)S.c(L.c[q])(i, j);
+    }
+}
+
+}  // namespace hpq

@@ -1,0 +1,985 @@
+// The slice-loop driver: owns device memory, initialises plasma and beams, and sequences the
+// kernels of one slice (Hipace::SolveOneSlice, Hipace.cpp:556-728) for the explicit and the
+// predictor-corrector Bx/By solvers. R is the field/plasma precision (double: plain FP64 path;
+// float: mixed path); beam particles are always FP64.
+#pragma once
+
+#include <algorithm>
+#include <cstdlib>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "config.hpp"
+#include "dst.cuh"
+#include "kernels.cuh"
+#include "mg.cuh"
+#include "rng.hpp"
+
+namespace hpq {
+
+struct HostBeam {
+    std::vector<double> x, y, z, w, ux, uy, uz;
+    std::vector<long long> id;
+    size_t size() const { return x.size(); }
+    void push(double a, double b, double c, double ww, double d, double e, double f, long long i) {
+        x.push_back(a); y.push_back(b); z.push_back(c); w.push_back(ww); ux.push_back(d); uy.push_back(e); uz.push_back(f); id.push_back(i);
+    }
+};
+
+struct Stats {
+    long long mg_vcycles = 0;
+    int mg_status = 0;
+    long long plasma_pushes = 0;
+    long long beam_particles = 0;
+    long long slices = 0;
+    long long launches = 0;
+};
+
+class SimBase {
+public:
+    virtual ~SimBase() = default;
+    virtual void init() = 0;
+    virtual void set_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
+                          const double* uy, const double* uz, const long long* id, long long n) = 0;
+    virtual long long beam_count(int b) = 0;
+    virtual void get_beam(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
+                          long long* id) = 0;
+    virtual void begin_step(int step) = 0;
+    virtual void solve_slice(int islice) = 0;
+    virtual void end_step() = 0;
+    virtual void get_field(const std::string& name, double* out) = 0;
+    virtual void set_diag(const std::vector<std::string>& names) = 0;
+    virtual void get_diag(const std::string& name, double* out) = 0;
+    virtual long long plasma_count(int sp) = 0;
+    virtual void get_plasma(int sp, double* out12) = 0;
+    virtual void synchronize() = 0;
+    virtual cudaStream_t stream() = 0;
+    virtual Stats stats() = 0;
+    virtual void set_graphs(bool on) = 0;
+    virtual void set_profiling(bool on) = 0;
+    virtual bool get_profile(const std::string& name, double* ms, long long* n) = 0;
+    virtual std::string profile_names() = 0;
+    const SimConfig& config() const { return cfg; }
+    SimConfig cfg;
+};
+
+inline int comp_from_name(const std::string& n, bool explicit_solver) {
+    static const std::map<std::string, int> ex = {
+        {"chi", C_CHI}, {"Sy", C_SY}, {"Sx", C_SX}, {"ExmBy", C_EXMBY}, {"EypBx", C_EYPBX}, {"Ez", C_EZ},
+        {"Bx", C_BX}, {"By", C_BY}, {"Bz", C_BZ}, {"Psi", C_PSI}, {"jx_beam", C_JXB}, {"jy_beam", C_JYB},
+        {"jz_beam", C_JZB}, {"jx", C_JX}, {"jy", C_JY}, {"rhomjz", C_RHOMJZ}, {"rho", C_RHO},
+        {"rhomjz_beam", C_RHOMJZB}, {"Next.jx_beam", C_NJXB}, {"Next.jy_beam", C_NJYB},
+        {"Prev.jx_beam", C_PJXB}, {"Prev.jy_beam", C_PJYB}, {"Ions.rhomjz", C_IONS}};
+    static const std::map<std::string, int> pc = {
+        {"ExmBy", C_EXMBY}, {"EypBx", C_EYPBX}, {"Ez", C_EZ}, {"Bx", C_BX}, {"By", C_BY}, {"Bz", C_BZ},
+        {"Psi", C_PSI}, {"jx", C_JX}, {"jy", C_JY}, {"jz", C_JZ}, {"rhomjz", C_RHOMJZ}, {"rho", C_RHO},
+        {"Next.jx", C_NJX}, {"Next.jy", C_NJY}, {"Prev.Bx", C_PBX}, {"Prev.By", C_PBY}, {"Prev.jx", C_PJX},
+        {"Prev.jy", C_PJY}, {"PCIter.Bx", C_PCIBX}, {"PCIter.By", C_PCIBY}, {"PCPrevIter.Bx", C_PCPBX},
+        {"PCPrevIter.By", C_PCPBY}, {"Ions.rhomjz", C_IONS}};
+    const auto& m = explicit_solver ? ex : pc;
+    auto it = m.find(n);
+    if (it == m.end()) throw InputError("unknown field component '" + n + "'");
+    return it->second;
+}
+
+// ------------------------------------------------------------------------------------------
+// PC helper kernels (Fields.cpp:1149-1286)
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl, int gated) {
+    if (gated && !ctl->pc_go) return;
+    const F2<R> Bx = S.c(bx), By = S.c(by), Bxi = S.c(bxi), Byi = S.c(byi);
+    double nb = 0, nd = 0;
+    for (long long k = gtid(); k < (long long)S.nx * S.ny; k += gstride()) {
+        const int i = (int)(k % S.nx), j = (int)(k / S.nx);
+        const double a = Bx(i, j), b = By(i, j), c = Bxi(i, j), d = Byi(i, j);
+        nb += sqrt(a * a + b * b);
+        nd += sqrt((a - c) * (a - c) + (b - d) * (b - d));
+    }
+    for (int o = 16; o > 0; o >>= 1) { nb += __shfl_xor_sync(0xffffffffu, nb, o); nd += __shfl_xor_sync(0xffffffffu, nd, o); }
+    if ((threadIdx.x & 31) == 0) { atomicAdd(&ctl->pc_sum[0], nb); atomicAdd(&ctl->pc_sum[1], nd); }
+}
+// first error of a slice -> initial-guess mixing factor (InitialBfieldGuess)
+__global__ void k_pc_guess_factor(Ctl* ctl, double tol) {
+    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
+    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
+    ctl->pc_mix = exp(-0.5 * pow(err / (2.5 * tol), 2));
+    ctl->pc_iter = 0;
+    ctl->pc_err = 1.0;
+    ctl->pc_err_prev = 1.0;
+    ctl->pc_go = 1.0 > tol;
+}
+template <class R>
+__global__ void k_pc_guess(Slab<R> S, const Ctl* ctl) {
+    const R mix = (R)ctl->pc_mix;
+    R *B = S.c(C_BX).p, *By = S.c(C_BY).p, *PB = S.c(C_PBX).p, *PBy = S.c(C_PBY).p;
+    R *PCP = S.c(C_PCPBX).p, *PCPy = S.c(C_PCPBY).p, *PCI = S.c(C_PCIBX).p, *PCIy = S.c(C_PCIBY).p;
+    for (long long k = gtid(); k < (long long)S.cstride; k += gstride()) {
+        const R bx = (R(1) + mix) * PB[k] + (-mix) * PCP[k];
+        const R by = (R(1) + mix) * PBy[k] + (-mix) * PCPy[k];
+        B[k] = bx; By[k] = by;
+        PCI[k] = 0; PCIy[k] = 0;
+        PCP[k] = bx; PCPy[k] = by;
+    }
+}
+// error of one iteration -> mixing weights and whether to continue (MixAndShiftBfields)
+__global__ void k_pc_iter_factor(Ctl* ctl, double tol, int maxit) {
+    if (!ctl->pc_go) return;
+    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
+    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
+    ctl->pc_iter += 1;
+    double prev = ctl->pc_err_prev;
+    if (ctl->pc_iter == 1) prev = err;
+    double wi, wp;
+    if (err != 0. || prev != 0.) { wi = prev / (err + prev); wp = err / (err + prev); }
+    else { wi = 0.5; wp = 0.5; }
+    ctl->pc_w[0] = wi; ctl->pc_w[1] = wp;
+    ctl->pc_err = err;
+    ctl->pc_err_prev = err;
+    ctl->pc_mixnow = 1;
+}
+template <class R>
+__global__ void k_pc_mix(Slab<R> S, Ctl* ctl, double a, double tol, int maxit) {
+    if (!ctl->pc_mixnow) return;
+    const R wi = (R)ctl->pc_w[0], wp = (R)ctl->pc_w[1], ra = (R)a;
+    R *B = S.c(C_BX).p, *By = S.c(C_BY).p;
+    R *PCP = S.c(C_PCPBX).p, *PCPy = S.c(C_PCPBY).p, *PCI = S.c(C_PCIBX).p, *PCIy = S.c(C_PCIBY).p;
+    R *NJX = S.c(C_NJX).p, *NJY = S.c(C_NJY).p;
+    for (long long k = gtid(); k < (long long)S.cstride; k += gstride()) {
+        const R px = wi * PCI[k] + wp * PCP[k];
+        const R py = wi * PCIy[k] + wp * PCPy[k];
+        B[k] = (R(1) - ra) * B[k] + ra * px;
+        By[k] = (R(1) - ra) * By[k] + ra * py;
+        PCP[k] = PCI[k]; PCPy[k] = PCIy[k];
+        NJX[k] = 0; NJY[k] = 0;
+    }
+}
+__global__ void k_pc_after_mix(Ctl* ctl, double tol, int maxit) {
+    if (!ctl->pc_mixnow) return;
+    ctl->pc_mixnow = 0;
+    ctl->pc_go = (ctl->pc_err > tol) && (ctl->pc_iter < maxit);
+}
+
+__global__ void k_slice_done(Ctl* ctl) { ctl->islice -= 1; }
+
+// ------------------------------------------------------------------------------------------
+template <class R>
+class Sim final : public SimBase {
+public:
+    explicit Sim(const SimConfig& c) { cfg = c; }
+    ~Sim() override { release(); }
+
+    Geo g{};
+    int nx = 0, ny = 0, nz = 0;
+    cudaStream_t st = nullptr;
+    Slab<R> S;
+    PoissonDST<R> dst;
+    PoissonDST<R> pc_dst;  // the two Bx/By solves of the predictor-corrector loop
+    Multigrid<R> mg;
+    std::vector<PlasmaDev<R>> pl;
+    std::vector<double*> px0, py0;
+    std::vector<BeamDev> bm;
+    std::vector<HostBeam> pending_beams;
+    std::vector<bool> beam_set;
+    Ctl* ctl = nullptr;
+    Ctl* ctl_h = nullptr;
+    int parity = 0;
+    int cur_step = 0;
+    int cur_islice = 0;
+    double physical_time = 0;
+    bool use_graphs = false;
+    bool capturing = false;
+    cudaStream_t st2 = nullptr;
+    cudaGraph_t slice_graph = nullptr;
+    cudaGraphExec_t slice_exec = nullptr;
+    long long graph_nodes = 0;
+    long long launches_top = 0, launches_body = 0;  // kernels per slice graph / per V-cycle body
+    long long launches_total = 0;                   // kernels launched or replayed so far
+    long long body_launch_offset = 0;
+    // per-kernel-class timing with CUDA events on the launching stream
+    struct ProfEntry {
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+        double ms = 0;
+        long long n = 0;
+    };
+    std::map<std::string, ProfEntry> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    bool profiling = false;
+    cudaEvent_t ev_get() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            HPQ_CUDA(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    struct Scope {
+        Sim* s;
+        const char* name;
+        cudaEvent_t a = nullptr, b = nullptr;
+        Scope(Sim* s_, const char* n) : s(s_), name(n) {
+            if (s->profiling) { a = s->ev_get(); b = s->ev_get(); HPQ_CUDA(cudaEventRecord(a, s->st)); }
+        }
+        ~Scope() {
+            if (a) { cudaEventRecord(b, s->st); s->prof[name].pending.push_back({a, b}); }
+        }
+    };
+    void prof_collect() {
+        for (auto& kv : prof) {
+            for (auto& pr : kv.second.pending) {
+                float ms = 0;
+                HPQ_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+                kv.second.ms += ms;
+                kv.second.n += 1;
+                ev_pool.push_back(pr.first);
+                ev_pool.push_back(pr.second);
+            }
+            kv.second.pending.clear();
+        }
+    }
+    void set_profiling(bool on) override {
+        synchronize();
+        prof_collect();
+        prof.clear();
+        profiling = on;
+    }
+    bool get_profile(const std::string& name, double* ms, long long* n) override {
+        synchronize();
+        prof_collect();
+        auto it = prof.find(name);
+        if (it == prof.end()) { *ms = 0; *n = 0; return false; }
+        *ms = it->second.ms;
+        *n = it->second.n;
+        return true;
+    }
+    std::string profile_names() override {
+        std::string r;
+        for (auto& kv : prof) r += kv.first + " ";
+        return r;
+    }
+    // diagnostics
+    std::vector<std::string> diag_names;
+    CompList diag_list{};
+    double* diag_buf = nullptr;
+    Stats st_host{};
+
+    cudaStream_t stream() override { return st; }
+    void set_graphs(bool on) override {
+        use_graphs = on;
+        if (!on) invalidate_graph();
+    }
+
+    void release() {
+        if (st) cudaStreamSynchronize(st);
+        if (S.base) cudaFree(S.base);
+        S.base = nullptr;
+        dst.release();
+        pc_dst.release();
+        mg.release();
+        for (auto& p : pl)
+            for (void* q : {(void*)p.x, (void*)p.y, (void*)p.w, (void*)p.ux, (void*)p.uy, (void*)p.psi, (void*)p.xp,
+                            (void*)p.yp, (void*)p.uxh, (void*)p.uyh, (void*)p.psih, (void*)p.valid})
+                if (q) cudaFree(q);
+        pl.clear();
+        for (auto* q : px0) cudaFree(q);
+        for (auto* q : py0) cudaFree(q);
+        px0.clear(); py0.clear();
+        for (auto& b : bm) free_beam(b);
+        bm.clear();
+        if (ctl) cudaFree(ctl);
+        if (ctl_h) cudaFreeHost(ctl_h);
+        ctl = nullptr; ctl_h = nullptr;
+        if (diag_buf) cudaFree(diag_buf);
+        diag_buf = nullptr;
+        for (auto& kv : prof)
+            for (auto& pr : kv.second.pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+        prof.clear();
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        ev_pool.clear();
+        invalidate_graph();
+        if (st2) cudaStreamDestroy(st2);
+        st2 = nullptr;
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+
+    // ----------------------------------------------------------------------------- init
+    void init() override {
+        nx = cfg.n_cell[0]; ny = cfg.n_cell[1]; nz = cfg.n_cell[2];
+        g.nx = nx; g.ny = ny; g.nz = nz;
+        for (int d = 0; d < 3; ++d) {
+            g.plo[d] = cfg.prob_lo[d]; g.phi[d] = cfg.prob_hi[d];
+            g.dx[d] = (cfg.prob_hi[d] - cfg.prob_lo[d]) / cfg.n_cell[d];
+            g.dxi[d] = 1. / g.dx[d];
+        }
+        g.xoff = 0.5 * (cfg.prob_lo[0] + cfg.prob_hi[0] - g.dx[0] * ((-2) + (nx + 1)));
+        g.yoff = 0.5 * (cfg.prob_lo[1] + cfg.prob_hi[1] - g.dx[1] * ((-2) + (ny + 1)));
+        g.plo_p[0] = cfg.particle_lo[0]; g.plo_p[1] = cfg.particle_lo[1];
+        g.phi_p[0] = cfg.particle_hi[0]; g.phi_p[1] = cfg.particle_hi[1];
+        g.bc = (int)cfg.particle_bc;
+        g.c = cfg.pc.c; g.ep0 = cfg.pc.ep0; g.mu0 = cfg.pc.mu0;
+        g.normalized = cfg.normalized_units;
+        if ((int)cfg.beams.size() > kMaxBeams) throw InputError("at most 4 beam species are supported");
+
+        HPQ_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        HPQ_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        // slab
+        S.nx = nx; S.ny = ny;
+        S.pitch = ((nx + 2 * kGuardAlloc + 7) / 8) * 8;
+        S.rows = ny + 2 * kGuardAlloc;
+        S.cstride = (size_t)S.pitch * S.rows;
+        HPQ_CUDA(cudaMalloc(&S.base, S.cstride * C_NCOMP * sizeof(R)));
+        HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * C_NCOMP * sizeof(R)));
+        dst.init(nx, ny, g.dx[0], g.dx[1], 3);
+        if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
+        // HPQ_DST=gemm selects the sine-matrix GEMM path on every grid (cross-checks)
+        if (const char* e = getenv("HPQ_DST")) {
+            if (std::string(e) == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
+        }
+        if (cfg.explicit_solver) mg.init(nx, ny, g.dx[0], g.dx[1]);
+        HPQ_CUDA(cudaMalloc(&ctl, sizeof(Ctl)));
+        HPQ_CUDA(cudaMemset(ctl, 0, sizeof(Ctl)));
+        HPQ_CUDA(cudaMallocHost(&ctl_h, sizeof(Ctl)));
+        std::memset(ctl_h, 0, sizeof(Ctl));
+        init_plasma_lattices();
+        // beams: fixed_ppc generated here, fixed_weight drawn from the seeded generator unless
+        // the caller provides particles with set_beam before the first step
+        beam_set.assign(cfg.beams.size(), false);
+        pending_beams.assign(cfg.beams.size(), HostBeam{});
+        bm.resize(cfg.beams.size());
+        for (size_t b = 0; b < cfg.beams.size(); ++b) {
+            HostBeam hb = cfg.beams[b].injection == BeamInjection::FixedPPC ? make_fixed_ppc((int)b) : make_fixed_weight((int)b);
+            upload_beam((int)b, hb);
+        }
+    }
+
+    void init_plasma_lattices() {
+        for (size_t s = 0; s < cfg.plasmas.size(); ++s) {
+            const PlasmaSpecies& P = cfg.plasmas[s];
+            std::vector<double> hx, hy;
+            const int nppc = P.ppc[0] * P.ppc[1];
+            int ilo = 0, ihi = nx - 1, jlo = 0, jhi = ny - 1;
+            double xo = 0, yo = 0;
+            if (P.prevent_centered_particle) {
+                if (nx % 2 == 1 && P.ppc[0] % 2 == 1) { ilo = 1; xo = -0.5; }
+                if (ny % 2 == 1 && P.ppc[1] % 2 == 1) { jlo = 1; yo = -0.5; }
+            }
+            if (P.radius < 1e299) {
+                ilo = std::max(ilo, (int)std::round((-P.radius - cfg.prob_lo[0]) / g.dx[0] - 2));
+                jlo = std::max(jlo, (int)std::round((-P.radius - cfg.prob_lo[1]) / g.dx[1] - 2));
+                ihi = std::min(ihi, (int)std::round((P.radius - cfg.prob_lo[0]) / g.dx[0] + 2));
+                jhi = std::min(jhi, (int)std::round((P.radius - cfg.prob_lo[1]) / g.dx[1] + 2));
+            }
+            if (P.u_std[0] != 0 || P.u_std[1] != 0 || P.u_std[2] != 0)
+                throw InputError(P.name + ".u_std != 0 (thermal plasma) is not supported");
+            // particles whose density is below min_density at t=0 are dropped; the density of a
+            // kept particle is re-evaluated at c*t every step
+            for (int ip = 0; ip < nppc; ++ip) {
+                const int ixp = ip % P.ppc[0], iyp = ip / P.ppc[0];
+                const double r0 = (0.5 + ixp) / P.ppc[0], r1 = (0.5 + iyp) / P.ppc[1];
+                for (int j = jlo; j <= jhi; ++j)
+                    for (int i = ilo; i <= ihi; ++i) {
+                        const double x = cfg.prob_lo[0] + (i + r0 + xo) * g.dx[0];
+                        const double y = cfg.prob_lo[1] + (j + r1 + yo) * g.dx[1];
+                        const double rsq = x * x + y * y;
+                        double v[3] = {x, y, 0.0};
+                        if (x >= cfg.particle_hi[0] || x < cfg.particle_lo[0] || y >= cfg.particle_hi[1] ||
+                            y < cfg.particle_lo[1] || rsq > P.radius * P.radius ||
+                            rsq < P.hollow_core_radius * P.hollow_core_radius || P.density.eval(v) <= P.min_density)
+                            continue;
+                        hx.push_back(x); hy.push_back(y);
+                    }
+            }
+            PlasmaDev<R> d{};
+            d.n = (long long)hx.size();
+            d.charge = P.charge; d.mass = P.mass; d.qsa_max = P.max_qsa_weighting_factor;
+            d.n_subcycles = P.n_subcycles; d.neutralize = P.neutralize_background;
+            const size_t nb = std::max<size_t>(1, hx.size());
+            R** arrs[] = {&d.x, &d.y, &d.w, &d.ux, &d.uy, &d.psi, &d.xp, &d.yp, &d.uxh, &d.uyh, &d.psih};
+            for (R** a : arrs) HPQ_CUDA(cudaMalloc(a, nb * sizeof(R)));
+            HPQ_CUDA(cudaMalloc(&d.valid, nb));
+            double *dx0, *dy0;
+            HPQ_CUDA(cudaMalloc(&dx0, nb * sizeof(double)));
+            HPQ_CUDA(cudaMalloc(&dy0, nb * sizeof(double)));
+            if (!hx.empty()) {
+                HPQ_CUDA(cudaMemcpy(dx0, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice));
+                HPQ_CUDA(cudaMemcpy(dy0, hy.data(), hy.size() * sizeof(double), cudaMemcpyHostToDevice));
+            }
+            pl.push_back(d);
+            px0.push_back(dx0); py0.push_back(dy0);
+        }
+    }
+
+    // InitBeamFixedPPCSlice for all slices (BeamParticleContainerInit.cpp:199-345)
+    HostBeam make_fixed_ppc(int b) {
+        const BeamSpecies& B = cfg.beams[b];
+        HostBeam hb;
+        const int nppc = B.ppc[0] * B.ppc[1] * B.ppc[2];
+        const double scale = cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc;
+        long long pid = 1;
+        for (int k = 0; k < nz; ++k) {
+            const double z0 = cfg.prob_lo[2] + k * g.dx[2];
+            if (z0 + g.dx[2] < B.zmin || z0 > B.zmax) continue;
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                    for (int ip = 0; ip < nppc; ++ip) {
+                        const int nyp = B.ppc[1], nzp = B.ppc[2];
+                        const int ixp = ip / (nyp * nzp), iyp = (ip % (nyp * nzp)) % nyp, izp = (ip % (nyp * nzp)) / nyp;
+                        const double x = cfg.prob_lo[0] + (i + (0.5 + ixp) / B.ppc[0]) * g.dx[0];
+                        const double y = cfg.prob_lo[1] + (j + (0.5 + iyp) / B.ppc[1]) * g.dx[1];
+                        const double z = cfg.prob_lo[2] + (k + (0.5 + izp) / B.ppc[2]) * g.dx[2];
+                        if (z >= B.zmax || z < B.zmin ||
+                            ((x - B.position_mean[0]) * (x - B.position_mean[0]) + (y - B.position_mean[1]) * (y - B.position_mean[1])) > B.radius * B.radius)
+                            continue;
+                        double dens;
+                        if (B.profile == BeamProfile::Gaussian) {
+                            const double a = (x - B.position_mean[0]) / B.position_std[0];
+                            const double bb = (y - B.position_mean[1]) / B.position_std[1];
+                            const double c = (z - B.position_mean[2]) / B.position_std[2];
+                            dens = B.density * std::exp(-0.5 * a * a) * std::exp(-0.5 * bb * bb) * std::exp(-0.5 * c * c);
+                        } else {
+                            dens = B.density;
+                        }
+                        if (dens <= B.min_density) continue;
+                        double xp = x, yp = y, uxp = B.u_mean[0] * cfg.pc.c, uyp = B.u_mean[1] * cfg.pc.c;
+                        const bool ok = host_bc(xp, yp, uxp, uyp);
+                        hb.push(xp, yp, z, ok ? std::fabs(dens * scale) : 0.0, uxp, uyp, B.u_mean[2] * cfg.pc.c, pid++);
+                    }
+        }
+        return hb;
+    }
+
+    // InitBeamFixedWeight3D/Slice (BeamParticleContainerInit.cpp:349-476) with this build's own
+    // counter-based generator (Philox4x32-10); AMReX's random stream is not reproduced.
+    HostBeam make_fixed_weight(int b) {
+        const BeamSpecies& B = cfg.beams[b];
+        HostBeam hb;
+        long long n = B.num_particles;
+        if (n <= 0) return hb;
+        const long long nbase = B.do_symmetrize ? n / 4 : n;
+        const uint64_t seed = (uint64_t)(cfg.has_random_seed ? cfg.random_seed : 0) * 1000003ull + (uint64_t)b * 7919ull + 12345ull;
+        Philox rng(seed);
+        const bool can = B.profile == BeamProfile::Can;
+        const double z_mean = can ? 0.5 * (B.zmin + B.zmax) : B.position_mean[2];
+        const double weight = B.total_charge / (B.num_particles * B.charge);
+        long long pid = 1;
+        for (long long i = 0; i < nbase; ++i) {
+            double nrm[8];
+            rng.normals(2 * (uint64_t)i, nrm);
+            rng.normals(2 * (uint64_t)i + 1, nrm + 4);
+            const double zc = can ? rng.uniform(2 * (uint64_t)i + 1, 3) * (B.zmax - B.zmin) + B.zmin
+                                  : z_mean + B.position_std[2] * nrm[0];
+            double x = B.position_std[0] * nrm[1];
+            double y = B.position_std[1] * nrm[2];
+            double u[3] = {B.u_mean[0] + B.u_std[0] * nrm[3], B.u_mean[1] + B.u_std[1] * nrm[4],
+                           B.u_mean[2] + B.u_std[2] * nrm[5]};
+            u[2] += (zc - z_mean) * B.duz_per_uz0_dzeta * B.u_mean[2];
+            bool valid = !(zc < B.zmin || zc > B.zmax || x * x + y * y > B.radius * B.radius);
+            x -= B.z_foc * u[0] / u[2];
+            y -= B.z_foc * u[1] / u[2];
+            const double cx = B.position_mean[0], cy = B.position_mean[1];
+            const int ncopy = B.do_symmetrize ? 4 : 1;
+            for (int q = 0; q < ncopy; ++q) {
+                const double sx = (q & 1) ? -1 : 1, sy = (q & 2) ? -1 : 1;
+                double xp = cx + sx * x, yp = cy + sy * y, uxp = sx * u[0] * cfg.pc.c, uyp = sy * u[1] * cfg.pc.c;
+                const bool ok = host_bc(xp, yp, uxp, uyp) && valid;
+                hb.push(xp, yp, zc, ok ? std::fabs(weight) : 0.0, uxp, uyp, u[2] * cfg.pc.c, pid++);
+            }
+        }
+        return hb;
+    }
+
+    bool host_bc(double& x, double& y, double& ux, double& uy) const {
+        const double plo0 = cfg.particle_lo[0], plo1 = cfg.particle_lo[1], phi0 = cfg.particle_hi[0], phi1 = cfg.particle_hi[1];
+        if (x < plo0 || y < plo1 || x > phi0 || y > phi1) {
+            const double lx = phi0 - plo0, ly = phi1 - plo1;
+            if (cfg.particle_bc == ParticleBC::Reflecting) {
+                x = std::fmod(x - plo0, 2 * lx); if (x < 0) x += 2 * lx; x += plo0;
+                if (x > phi0) { x = 2 * phi0 - x; ux = -ux; }
+                y = std::fmod(y - plo1, 2 * ly); if (y < 0) y += 2 * ly; y += plo1;
+                if (y > phi1) { y = 2 * phi1 - y; uy = -uy; }
+                return true;
+            } else if (cfg.particle_bc == ParticleBC::Periodic) {
+                x = std::fmod(x - plo0, lx); if (x < 0) x += lx; x += plo0;
+                y = std::fmod(y - plo1, ly); if (y < 0) y += ly; y += plo1;
+                return true;
+            }
+            return false;
+        }
+        return true;
+    }
+
+    static void alloc_buf(BeamBuf& b, long long cap) {
+        const size_t n = (size_t)std::max<long long>(cap, 1);
+        double** d[] = {&b.x, &b.y, &b.z, &b.w, &b.ux, &b.uy, &b.uz};
+        for (double** p : d) HPQ_CUDA(cudaMalloc(p, n * sizeof(double)));
+        HPQ_CUDA(cudaMalloc(&b.id, n * sizeof(long long)));
+        HPQ_CUDA(cudaMalloc(&b.nsub, n * sizeof(int)));
+        HPQ_CUDA(cudaMalloc(&b.valid, n));
+    }
+    static void free_buf(BeamBuf& b) {
+        for (void* p : {(void*)b.x, (void*)b.y, (void*)b.z, (void*)b.w, (void*)b.ux, (void*)b.uy, (void*)b.uz,
+                        (void*)b.id, (void*)b.nsub, (void*)b.valid})
+            if (p) cudaFree(p);
+        std::memset(&b, 0, sizeof(b));
+    }
+    static void free_beam(BeamDev& d) {
+        for (int q = 0; q < 2; ++q) {
+            free_buf(d.buf[q]); free_buf(d.carry[q]);
+            if (d.start[q]) cudaFree(d.start[q]);
+            if (d.count[q]) cudaFree(d.count[q]);
+            d.start[q] = d.count[q] = nullptr;
+        }
+    }
+
+    // BoxSort (BoxSort.cpp:14-78): slice = int((z - lo) / dz); particles outside [0, nz) are
+    // dropped; stable within a slice. Slices are stored top-down like the slice march.
+    void upload_beam(int b, const HostBeam& hb) {
+        BeamDev& d = bm[b];
+        const BeamSpecies& B = cfg.beams[b];
+        d.charge = B.charge; d.mass = B.mass; d.n_subcycles = B.n_subcycles; d.do_z_push = B.do_z_push;
+        std::vector<int> sl(hb.size());
+        std::vector<int> cnt(nz, 0);
+        for (size_t i = 0; i < hb.size(); ++i) {
+            const int s = (int)((hb.z[i] - cfg.prob_lo[2]) * g.dxi[2]);
+            sl[i] = (s < 0 || s >= nz) ? -1 : s;
+            if (sl[i] >= 0) cnt[sl[i]]++;
+        }
+        std::vector<int> start(nz, 0);
+        long long acc = 0;
+        for (int s = nz - 1; s >= 0; --s) { start[s] = (int)acc; acc += cnt[s]; }
+        const long long n = acc;
+        // device buffers are kept when the new beam fits (captured slice graphs stay valid)
+        if (d.buf[0].x == nullptr || n > d.cap) {
+            free_beam(d);
+            invalidate_graph();
+            d.cap = std::max<long long>(n, 1);
+            for (int q = 0; q < 2; ++q) {
+                alloc_buf(d.buf[q], d.cap);
+                alloc_buf(d.carry[q], d.cap);
+                HPQ_CUDA(cudaMalloc(&d.start[q], nz * sizeof(int)));
+                HPQ_CUDA(cudaMalloc(&d.count[q], nz * sizeof(int)));
+            }
+        }
+        for (int q = 0; q < 2; ++q) {
+            HPQ_CUDA(cudaMemset(d.start[q], 0, nz * sizeof(int)));
+            HPQ_CUDA(cudaMemset(d.count[q], 0, nz * sizeof(int)));
+        }
+        std::vector<double> a[7];
+        for (auto& v : a) v.resize(n);
+        std::vector<long long> ids(n);
+        std::vector<int> nsub(n, 0);
+        std::vector<uint8_t> valid(n);
+        std::vector<int> pos(start);
+        for (size_t i = 0; i < hb.size(); ++i) {
+            if (sl[i] < 0) continue;
+            const int k = pos[sl[i]]++;
+            a[0][k] = hb.x[i]; a[1][k] = hb.y[i]; a[2][k] = hb.z[i]; a[3][k] = hb.w[i];
+            a[4][k] = hb.ux[i]; a[5][k] = hb.uy[i]; a[6][k] = hb.uz[i];
+            ids[k] = hb.id[i];
+            valid[k] = hb.w[i] != 0.0;
+        }
+        const int q = parity;
+        double* dp[7] = {d.buf[q].x, d.buf[q].y, d.buf[q].z, d.buf[q].w, d.buf[q].ux, d.buf[q].uy, d.buf[q].uz};
+        if (n > 0) {
+            for (int k = 0; k < 7; ++k) HPQ_CUDA(cudaMemcpy(dp[k], a[k].data(), n * sizeof(double), cudaMemcpyHostToDevice));
+            HPQ_CUDA(cudaMemcpy(d.buf[q].id, ids.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+            HPQ_CUDA(cudaMemcpy(d.buf[q].nsub, nsub.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+            HPQ_CUDA(cudaMemcpy(d.buf[q].valid, valid.data(), n, cudaMemcpyHostToDevice));
+        }
+        HPQ_CUDA(cudaMemcpy(d.start[q], start.data(), nz * sizeof(int), cudaMemcpyHostToDevice));
+        HPQ_CUDA(cudaMemcpy(d.count[q], cnt.data(), nz * sizeof(int), cudaMemcpyHostToDevice));
+        st_host.beam_particles = 0;
+    }
+
+    void set_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
+                  const double* uy, const double* uz, const long long* id, long long n) override {
+        if (b < 0 || b >= (int)cfg.beams.size()) throw InputError("beam index out of range");
+        HostBeam hb;
+        for (long long i = 0; i < n; ++i) hb.push(x[i], y[i], z[i], w[i], ux[i], uy[i], uz[i], id ? id[i] : i + 1);
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        upload_beam(b, hb);
+    }
+
+    long long beam_count(int b) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        std::vector<int> cnt(nz);
+        HPQ_CUDA(cudaMemcpy(cnt.data(), bm[b].count[parity], nz * sizeof(int), cudaMemcpyDeviceToHost));
+        long long n = 0;
+        for (int c : cnt) n += c;
+        return n;
+    }
+    // particles of the current store in slice-descending order
+    void get_beam(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
+                  long long* id) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        BeamDev& d = bm[b];
+        std::vector<int> cnt(nz), start(nz);
+        HPQ_CUDA(cudaMemcpy(cnt.data(), d.count[parity], nz * sizeof(int), cudaMemcpyDeviceToHost));
+        HPQ_CUDA(cudaMemcpy(start.data(), d.start[parity], nz * sizeof(int), cudaMemcpyDeviceToHost));
+        const BeamBuf& s = d.buf[parity];
+        long long k = 0;
+        for (int sl = nz - 1; sl >= 0; --sl) {
+            const size_t n = cnt[sl], o = start[sl];
+            if (!n) continue;
+            double* outs[7] = {x, y, z, w, ux, uy, uz};
+            double* ins[7] = {s.x, s.y, s.z, s.w, s.ux, s.uy, s.uz};
+            for (int a = 0; a < 7; ++a) HPQ_CUDA(cudaMemcpy(outs[a] + k, ins[a] + o, n * sizeof(double), cudaMemcpyDeviceToHost));
+            if (id) HPQ_CUDA(cudaMemcpy(id + k, s.id + o, n * sizeof(long long), cudaMemcpyDeviceToHost));
+            k += n;
+        }
+    }
+
+    // ----------------------------------------------------------------------------- step
+    // Hipace::Evolve per-step body (Hipace.cpp:401-480): reset slices, re-create the plasma,
+    // deposit the ion background
+    void begin_step(int step) override {
+        cur_step = step;
+        HPQ_CUDA(cudaMemsetAsync(S.base, 0, S.cstride * C_NCOMP * sizeof(R), st));
+        const double c_t = cfg.pc.c * physical_time;
+        for (size_t s = 0; s < pl.size(); ++s) {
+            const PlasmaSpecies& P = cfg.plasmas[s];
+            const int nppc = P.ppc[0] * P.ppc[1];
+            const double scale = nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc);
+            if (pl[s].n == 0) continue;
+            k_plasma_reset<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], px0[s], py0[s], P.density, c_t, scale,
+                                                                         P.u_mean[0], P.u_mean[1], P.u_mean[2], cfg.pc.c);
+            HPQ_LAUNCH_CHECK();
+        }
+        for (size_t s = 0; s < pl.size(); ++s) {
+            if (!pl[s].neutralize || pl[s].n == 0) continue;
+            DepOut<R> o{nullptr, nullptr, nullptr, nullptr, nullptr, S.c(C_IONS).p, S.pitch};
+            k_plasma_deposit<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], o, g, -pl[s].charge);
+            HPQ_LAUNCH_CHECK();
+        }
+        // control block for the slice march
+        std::memset(ctl_h, 0, sizeof(Ctl));
+        ctl_h->islice = nz - 1;
+        ctl_h->step_parity = parity;
+        HPQ_CUDA(cudaMemcpyAsync(ctl, ctl_h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        cur_islice = nz - 1;
+    }
+
+    void end_step() override {
+        physical_time += cfg.dt;
+        parity = 1 - parity;
+        HPQ_CUDA(cudaMemcpyAsync(ctl_h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        prof_collect();
+        st_host.mg_vcycles += ctl_h->mg_total_iters;
+        if (use_graphs && !profiling) launches_total += ctl_h->mg_total_iters * launches_body;
+        st_host.launches = launches_total;
+        if (ctl_h->mg_status && !st_host.mg_status) st_host.mg_status = ctl_h->mg_status;
+        st_host.slices += nz;
+        for (auto& p : pl) st_host.plasma_pushes += p.n * nz;
+        if (st_host.mg_status == 1) throw CudaError("hpmg: failed to converge within the iteration limit");
+        if (st_host.mg_status == 2) throw CudaError("hpmg: diverged");
+    }
+
+    void deposit_plasma(int sp, R* jx, R* jy, R* jz, R* rho, R* chi, R* rhomjz) {
+        if (pl[sp].n == 0) return;
+        DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
+        Scope sc(this, "plasma_deposit");
+        k_plasma_deposit<R><<<blocks_for(pl[sp].n, 256), 256, 0, st>>>(pl[sp], o, g, pl[sp].charge);
+        HPQ_LAUNCH_CHECK();
+    }
+    void deposit_beam(int b, int which, R* jx, R* jy, R* jz, R* rmj) {
+        Scope sc(this, "beam_deposit");
+        k_beam_deposit<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, which, jx, jy, jz, rmj, S.pitch, g);
+        HPQ_LAUNCH_CHECK();
+    }
+    void zero(std::initializer_list<int> comps) {
+        CompList L{};
+        for (int c : comps) L.c[L.n++] = c;
+        k_zero_comps<R><<<blocks_for((long long)S.cstride, 256, 148 * 8), 256, 0, st>>>(S, L);
+        HPQ_LAUNCH_CHECK();
+    }
+    void copies(std::initializer_list<std::pair<int, int>> pairs) {
+        CopyList L{};
+        for (auto& p : pairs) { L.dst[L.n] = p.first; L.src[L.n] = p.second; L.n++; }
+        k_copy_comps<R><<<blocks_for((long long)S.cstride, 256, 148 * 8), 256, 0, st>>>(S, L);
+        HPQ_LAUNCH_CHECK();
+    }
+    void field_solve_psi_ez_bz() {
+        const long long ntot = (long long)(nx + 2 * kGuardAlloc) * S.rows;
+        Scope sc(this, "poisson_psi_ez_bz");
+        k_rhs3<R><<<blocks_for(ntot, 256), 256, 0, st>>>(S, g, dst.stage, dst.sk, dst.sj, cfg.any_neutralize_background(),
+                                                         cfg.deposit_rho && cfg.any_neutralize_background(),
+                                                         cfg.explicit_solver && cfg.do_beam_jz_minus_rho);
+        HPQ_LAUNCH_CHECK();
+        const int comps[3] = {C_PSI, C_EZ, C_BZ};
+        dst.solve(st, 3, S.base, S.cstride, S.pitch, comps);
+        if (cfg.explicit_solver) k_grad_psi_sxsy<R><<<blocks_for((long long)(nx + 2) * (ny + 2), 256), 256, 0, st>>>(S, g);
+        else k_grad_psi<R><<<blocks_for((long long)(nx + 2) * (ny + 2), 256), 256, 0, st>>>(S, g);
+        HPQ_LAUNCH_CHECK();
+    }
+
+    void mg_solve() {
+        Scope sc(this, "multigrid");
+        if (mg.cell) mg_solve_t<true>(); else mg_solve_t<false>();
+    }
+    template <bool CELL>
+    void mg_solve_t() {
+        if (capturing) {
+            // inside the slice graph: a conditional WHILE node repeats the V-cycle body for as
+            // long as the device-side decision (k_mg_init_decide / k_mg_decide) says so
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cg;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            HPQ_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
+            cudaGraphConditionalHandle handle;
+            HPQ_CUDA(cudaGraphConditionalHandleCreate(&handle, cg, 0, cudaGraphCondAssignDefault));
+            mg.template pre<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, (unsigned long long)handle, 1);
+            HPQ_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode;
+            HPQ_CUDA(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            HPQ_CUDA(cudaStreamBeginCaptureToGraph(st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            const long long l0 = g_launches;
+            mg.template vcycle<CELL>(st2, S, ctl, cfg.mg_max_iters, (unsigned long long)handle, 1);
+            launches_body = g_launches - l0;
+            body_launch_offset += launches_body;
+            cudaGraph_t body_out;
+            HPQ_CUDA(cudaStreamEndCapture(st2, &body_out));
+            HPQ_CUDA(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
+            mg.template post<CELL>(st, S);
+            return;
+        }
+        mg.template pre<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, 0, 0);
+        // the device decides after every V-cycle (Ctl::mg_go); without graphs the host reads
+        // the decision back each cycle, like the reference's host-side max reduction
+        HPQ_CUDA(cudaMemcpyAsync(&ctl_h->mg_go, &ctl->mg_go, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        for (int it = 0; it < cfg.mg_max_iters && ctl_h->mg_go; ++it) {
+            mg.template vcycle<CELL>(st, S, ctl, cfg.mg_max_iters, 0, 0);
+            HPQ_CUDA(cudaMemcpyAsync(&ctl_h->mg_go, &ctl->mg_go, sizeof(int), cudaMemcpyDeviceToHost, st));
+            HPQ_CUDA(cudaStreamSynchronize(st));
+        }
+        mg.template post<CELL>(st, S);
+    }
+
+    // one slice: replay the captured graph, or launch kernel by kernel (profiling mode)
+    void solve_slice(int islice) override {
+        if (islice != cur_islice) throw InputError("slices must be solved from the head (nz-1) to the tail (0)");
+        if (use_graphs && !profiling) {
+            if (!slice_exec) capture_slice();
+            HPQ_CUDA(cudaGraphLaunch(slice_exec, st));
+            launches_total += launches_top;
+        } else {
+            const long long l0 = g_launches;
+            record_slice();
+            launches_total += g_launches - l0;
+        }
+        cur_islice--;
+    }
+    void capture_slice() {
+        invalidate_graph();
+        HPQ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        const long long l0 = g_launches;
+        body_launch_offset = 0;
+        try {
+            record_slice();
+        } catch (...) {
+            capturing = false;
+            cudaGraph_t g0;
+            cudaStreamEndCapture(st, &g0);
+            if (g0) cudaGraphDestroy(g0);
+            cudaGetLastError();
+            throw;
+        }
+        capturing = false;
+        launches_top = g_launches - l0 - body_launch_offset;
+        HPQ_CUDA(cudaStreamEndCapture(st, &slice_graph));
+        HPQ_CUDA(cudaGraphInstantiate(&slice_exec, slice_graph, 0));
+        size_t nn = 0;
+        HPQ_CUDA(cudaGraphGetNodes(slice_graph, nullptr, &nn));
+        graph_nodes = (long long)nn;
+    }
+    void invalidate_graph() {
+        if (slice_exec) { cudaGraphExecDestroy(slice_exec); slice_exec = nullptr; }
+        if (slice_graph) { cudaGraphDestroy(slice_graph); slice_graph = nullptr; }
+    }
+
+    // Hipace::SolveOneSlice (Hipace.cpp:556-728)
+    void record_slice() {
+        const bool ex = cfg.explicit_solver;
+        if (ex) {
+            if (cfg.deposit_rho) zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB, C_RHO});
+            else zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB});
+            for (size_t s = 0; s < pl.size(); ++s)
+                deposit_plasma((int)s, S.c(C_JX).p, S.c(C_JY).p, nullptr, cfg.deposit_rho ? S.c(C_RHO).p : nullptr,
+                               S.c(C_CHI).p, S.c(C_RHOMJZ).p);
+            // jz_beam of this slice and jx_beam/jy_beam of the next slice (the reference deposits
+            // the latter after the Psi/Ez/Bz solve, Hipace.cpp:656-657; the two are independent)
+            for (size_t b = 0; b < bm.size(); ++b) {
+                Scope sc(this, "beam_deposit");
+                const bool nj = cfg.do_beam_jx_jy_deposition;
+                k_beam_deposit_this_next<R><<<148 * 2, 256, 0, st>>>(
+                    bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
+                    nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g);
+                HPQ_LAUNCH_CHECK();
+            }
+        } else {
+            if (cfg.deposit_rho) zero({C_EXMBY, C_EYPBX, C_JX, C_JY, C_JZ, C_RHOMJZ, C_RHO});
+            else zero({C_EXMBY, C_EYPBX, C_JX, C_JY, C_JZ, C_RHOMJZ});
+            for (size_t s = 0; s < pl.size(); ++s)
+                deposit_plasma((int)s, S.c(C_JX).p, S.c(C_JY).p, S.c(C_JZ).p, cfg.deposit_rho ? S.c(C_RHO).p : nullptr,
+                               nullptr, S.c(C_RHOMJZ).p);
+            for (size_t b = 0; b < bm.size(); ++b)
+                deposit_beam((int)b, 0, cfg.do_beam_jx_jy_deposition ? S.c(C_JX).p : nullptr,
+                             cfg.do_beam_jx_jy_deposition ? S.c(C_JY).p : nullptr, S.c(C_JZ).p,
+                             cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZ).p : nullptr);
+        }
+        field_solve_psi_ez_bz();
+        if (ex) {
+            for (size_t s = 0; s < pl.size(); ++s) {
+                if (pl[s].n == 0) continue;
+                Scope sc(this, "explicit_deposit");
+                const int nb = blocks_for(pl[s].n, 256);
+                if (cfg.depos_derivative_type == 0) k_explicit_deposit<R, 0><<<nb, 256, 0, st>>>(pl[s], S, g);
+                else if (cfg.depos_derivative_type == 1) k_explicit_deposit<R, 1><<<nb, 256, 0, st>>>(pl[s], S, g);
+                else k_explicit_deposit<R, 2><<<nb, 256, 0, st>>>(pl[s], S, g);
+                HPQ_LAUNCH_CHECK();
+            }
+            mg_solve();
+        } else {
+            pc_loop();
+        }
+        if (diag_list.n > 0) {
+            k_diag_copy<R><<<blocks_for((long long)nx * ny * diag_list.n, 256), 256, 0, st>>>(S, ctl, diag_list, diag_buf, nz);
+            HPQ_LAUNCH_CHECK();
+        }
+        for (size_t s = 0; s < pl.size(); ++s) {
+            if (pl[s].n == 0) continue;
+            Scope sc(this, "plasma_push");
+            k_plasma_push<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], S, g, 0);
+            HPQ_LAUNCH_CHECK();
+        }
+        for (size_t b = 0; b < bm.size(); ++b) {
+            {
+                Scope sc(this, "beam_push");
+                k_beam_push<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, (int)b, S, g, cfg.dt);
+                HPQ_LAUNCH_CHECK();
+            }
+            Scope sc2(this, "beam_partition");
+            k_beam_partition<<<1, 1024, 0, st>>>(bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
+            HPQ_LAUNCH_CHECK();
+        }
+        if (ex) {
+            copies({{C_PJXB, C_JXB}, {C_PJYB, C_JYB}, {C_JXB, C_NJXB}, {C_JYB, C_NJYB}, {C_JX, C_NJXB}, {C_JY, C_NJYB}});
+        } else {
+            copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
+        }
+        if (bm.empty()) {
+            k_slice_done<<<1, 1, 0, st>>>(ctl);
+            HPQ_LAUNCH_CHECK();
+        }
+    }
+
+    // Hipace::PredictorCorrectorLoopToSolveBxBy (Hipace.cpp:935-1031)
+    void pc_loop() {
+        const long long nxy = (long long)nx * ny;
+        const double tol = cfg.predcorr_B_error_tolerance;
+        const int maxit = cfg.predcorr_max_iterations;
+        HPQ_CUDA(cudaMemsetAsync(&ctl->pc_sum[0], 0, 2 * sizeof(double), st));
+        k_pc_norms<R><<<blocks_for(nxy, 256, 148 * 4), 256, 0, st>>>(S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
+        HPQ_LAUNCH_CHECK();
+        k_pc_guess_factor<<<1, 1, 0, st>>>(ctl, tol);
+        HPQ_LAUNCH_CHECK();
+        k_pc_guess<R><<<blocks_for((long long)S.cstride, 256), 256, 0, st>>>(S, ctl);
+        HPQ_LAUNCH_CHECK();
+        for (int it = 0; it < maxit; ++it) {
+            // iterations after convergence are predicated off on the device (Ctl::pc_go)
+            for (size_t s = 0; s < pl.size(); ++s) {
+                if (pl[s].n == 0) continue;
+                k_plasma_push<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], S, g, 1, &ctl->pc_go);
+                HPQ_LAUNCH_CHECK();
+                DepOut<R> o{S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, nullptr, nullptr, S.pitch};
+                k_plasma_deposit<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], o, g, pl[s].charge, &ctl->pc_go);
+                HPQ_LAUNCH_CHECK();
+            }
+            if (cfg.do_beam_jx_jy_deposition)
+                for (size_t b = 0; b < bm.size(); ++b) deposit_beam_if((int)b);
+            const int comps[2] = {C_PCIBX, C_PCIBY};
+            k_rhs_bxby<R><<<blocks_for(nxy, 256), 256, 0, st>>>(S, g, pc_dst.stage, pc_dst.sk, pc_dst.sj);
+            HPQ_LAUNCH_CHECK();
+            pc_dst.solve(st, 2, S.base, S.cstride, S.pitch, comps);
+            k_pc_norms<R><<<blocks_for(nxy, 256, 148 * 4), 256, 0, st>>>(S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
+            HPQ_LAUNCH_CHECK();
+            k_pc_iter_factor<<<1, 1, 0, st>>>(ctl, tol, maxit);
+            HPQ_LAUNCH_CHECK();
+            k_pc_mix<R><<<blocks_for((long long)S.cstride, 256), 256, 0, st>>>(S, ctl, cfg.predcorr_B_mixing_factor, tol, maxit);
+            HPQ_LAUNCH_CHECK();
+            k_pc_after_mix<<<1, 1, 0, st>>>(ctl, tol, maxit);
+            HPQ_LAUNCH_CHECK();
+        }
+    }
+    void deposit_beam_if(int b) {
+        k_beam_deposit<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1);
+        HPQ_LAUNCH_CHECK();
+    }
+
+    // ----------------------------------------------------------------------------- io
+    void get_field(const std::string& name, double* out) override {
+        const int c = comp_from_name(name, cfg.explicit_solver);
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        std::vector<R> tmp(S.cstride);
+        HPQ_CUDA(cudaMemcpy(tmp.data(), S.c(c).p, S.cstride * sizeof(R), cudaMemcpyDeviceToHost));
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) out[(size_t)j * nx + i] = (double)tmp[(size_t)(j + kGuardAlloc) * S.pitch + i + kGuardAlloc];
+    }
+    void set_diag(const std::vector<std::string>& names) override {
+        if (names.size() > 24) throw InputError("at most 24 diagnostic components");
+        synchronize();
+        invalidate_graph();
+        diag_names = names;
+        diag_list = CompList{};
+        for (auto& n : names) diag_list.c[diag_list.n++] = comp_from_name(n, cfg.explicit_solver);
+        if (diag_buf) { cudaFree(diag_buf); diag_buf = nullptr; }
+        if (!names.empty()) {
+            const size_t n = (size_t)names.size() * nx * ny * nz;
+            HPQ_CUDA(cudaMalloc(&diag_buf, n * sizeof(double)));
+            HPQ_CUDA(cudaMemset(diag_buf, 0, n * sizeof(double)));
+        }
+    }
+    void get_diag(const std::string& name, double* out) override {
+        auto it = std::find(diag_names.begin(), diag_names.end(), name);
+        if (it == diag_names.end()) throw InputError("component '" + name + "' is not in the diagnostic list");
+        const size_t q = it - diag_names.begin();
+        const size_t n = (size_t)nx * ny * nz;
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        HPQ_CUDA(cudaMemcpy(out, diag_buf + q * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    long long plasma_count(int sp) override { return pl.at(sp).n; }
+    void get_plasma(int sp, double* out12) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        const PlasmaDev<R>& p = pl.at(sp);
+        const size_t n = p.n;
+        const R* arr[11] = {p.x, p.y, p.w, p.ux, p.uy, p.psi, p.xp, p.yp, p.uxh, p.uyh, p.psih};
+        std::vector<R> tmp(n);
+        for (int k = 0; k < 11; ++k) {
+            HPQ_CUDA(cudaMemcpy(tmp.data(), arr[k], n * sizeof(R), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) out12[k * n + i] = (double)tmp[i];
+        }
+        std::vector<uint8_t> v(n);
+        HPQ_CUDA(cudaMemcpy(v.data(), p.valid, n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) out12[11 * n + i] = v[i];
+    }
+    void synchronize() override { HPQ_CUDA(cudaStreamSynchronize(st)); }
+    Stats stats() override { return st_host; }
+};
+
+}  // namespace hpq

@@ -1,0 +1,118 @@
+/*
+ * hpq — C ABI of the B200 quasi-static slice loop (HiPACE++ slice solver, drop-in).
+ *
+ * Conventions (all entry points):
+ *   - return 0 on success, a non-zero HPQ_ERR_* code otherwise; hpq_last_error() gives the text.
+ *     No C++ exception crosses this boundary. The reference terminates the process through
+ *     amrex::Abort on the same conditions.
+ *   - the handle owns all device memory and one CUDA stream; host buffers belong to the caller.
+ *   - one handle is driven by one host thread at a time (the reference: one host thread per
+ *     rank driving amrex::Gpu::gpuStream()).
+ * Input text uses the reference's input-file syntax and keys (hipace.*, amr.*, geometry.*,
+ * boundary.*, plasmas.*, beams.*, <species>.*, my_constants.*; docs/source/run/parameters.rst).
+ */
+#ifndef HPQ_H_
+#define HPQ_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hpq_handle hpq_handle;
+
+enum {
+    HPQ_OK = 0,
+    HPQ_ERR_INPUT = 1,          /* bad or unsupported input key/value */
+    HPQ_ERR_CUDA = 2,           /* CUDA runtime error */
+    HPQ_ERR_STATE = 3,          /* call out of order (e.g. slice before hpq_begin_step) */
+    HPQ_ERR_NOT_CONVERGED = 4,  /* multigrid hit its iteration limit (hpmg "failed") */
+    HPQ_ERR_DIVERGED = 5,       /* multigrid residual grew by 1e20 (hpmg "failing") */
+    HPQ_ERR_ARG = 6             /* bad argument (index, name, null pointer) */
+};
+
+enum { HPQ_PLAIN_FP64 = 0, HPQ_MIXED = 1 };
+
+/* Parse and validate an input deck; replaces Hipace::Hipace() (src/Hipace.cpp:74-244) reading
+ * amrex::ParmParse. `input_text` holds the file content, later lines override earlier ones
+ * (command-line overrides can be appended as extra lines). */
+int hpq_create(const char* input_text, hpq_handle** out);
+void hpq_destroy(hpq_handle* h);
+const char* hpq_last_error(const hpq_handle* h);
+/* Text of the last hpq_create failure (no handle exists then). */
+const char* hpq_create_error(void);
+
+/* Field/plasma arithmetic: HPQ_PLAIN_FP64 (the reference's FP64 path) or HPQ_MIXED (FP32
+ * plasma, fields and multigrid; FP64 beam). Call before hpq_init. */
+int hpq_set_precision(hpq_handle* h, int mode);
+
+/* Allocate device data and inject the beams; replaces Hipace::InitData()
+ * (src/Hipace.cpp:246-295): fixed_ppc beams follow InitBeamFixedPPCSlice
+ * (src/particles/beam/BeamParticleContainerInit.cpp:199-345); fixed_weight beams are drawn
+ * from this library's seeded Philox stream (hpq_set_beam overrides them). */
+int hpq_init(hpq_handle* h);
+
+/* Replace all particles of beam `beam` (FP64 SoA, momenta are gamma*beta*c like the reference
+ * BeamIdx::ux..uz, src/particles/beam/BeamParticleContainer.H:23-41). Particles are binned
+ * into slices as BoxSorter::sortParticlesByBox (src/particles/sorting/BoxSort.cpp:14-78).
+ * `id` may be NULL. */
+int hpq_set_beam(hpq_handle* h, int beam, const double* x, const double* y, const double* z,
+                 const double* w, const double* ux, const double* uy, const double* uz,
+                 const int64_t* id, int64_t n);
+/* Number of stored particles of a beam and a copy of them (slices from head to tail). */
+int hpq_beam_count(hpq_handle* h, int beam, int64_t* n);
+int hpq_get_beam(hpq_handle* h, int beam, double* x, double* y, double* z, double* w,
+                 double* ux, double* uy, double* uz, int64_t* id);
+
+/* One full time step (all slices, head to tail); replaces the body of the step loop of
+ * Hipace::Evolve (src/Hipace.cpp:401-492). */
+int hpq_step(hpq_handle* h, int step);
+/* The per-slice surface: begin a step (ResetAllQuantities, plasma re-initialisation,
+ * neutralising background; src/Hipace.cpp:403-472), solve one slice — replaces
+ * Hipace::SolveOneSlice(islice, step) (src/Hipace.H:119, src/Hipace.cpp:556-728); slices must
+ * be solved from nz-1 down to 0 — then end the step. */
+int hpq_begin_step(hpq_handle* h, int step);
+int hpq_solve_slice(hpq_handle* h, int islice);
+int hpq_end_step(hpq_handle* h);
+
+/* Interior (ny x nx, x fastest) of a slice field component of the current slice, by the
+ * reference component name (Fields::getField, src/fields/Fields.H:436; names of
+ * src/fields/Fields.cpp:76-148, e.g. "Ez", "Psi", "Bx", "jz_beam", "chi"). */
+int hpq_get_field(hpq_handle* h, const char* comp, double* out);
+
+/* 3-D field diagnostic: record the listed components (space separated) of every slice of the
+ * following steps into nz x ny x nx arrays (replaces Fields::Copy into the openPMD diagnostic,
+ * src/fields/Fields.cpp:413-533, for diag_type=xyz without coarsening). */
+int hpq_set_diag(hpq_handle* h, const char* comps);
+int hpq_get_diag(hpq_handle* h, const char* comp, double* out);
+
+/* Plasma species `sp`: particle count and the 11 real attributes of PlasmaIdx
+ * (src/particles/plasma/PlasmaParticleContainer.H:21-46) plus the valid flag, as 12 blocks of
+ * `n` doubles: x y w ux uy psi x_prev y_prev ux_half_step uy_half_step psi_half_step valid. */
+int hpq_plasma_count(hpq_handle* h, int sp, int64_t* n);
+int hpq_get_plasma(hpq_handle* h, int sp, double* out);
+
+/* Capture each slice in a CUDA graph (default on) or launch kernel by kernel. */
+int hpq_set_graphs(hpq_handle* h, int on);
+/* Wait for all work of the handle. */
+int hpq_synchronize(hpq_handle* h);
+/* Per-kernel-class timing with CUDA events on the launching stream (kernel launch mode only).
+ * Classes: plasma_deposit, beam_deposit, poisson_psi_ez_bz, explicit_deposit, multigrid,
+ * plasma_push, beam_push, beam_partition. hpq_get_profile returns the accumulated device time
+ * and number of timed regions since profiling was switched on. */
+int hpq_set_profiling(hpq_handle* h, int on);
+int hpq_get_profile(hpq_handle* h, const char* kernel_class, double* total_ms, int64_t* launches);
+/* The handle's CUDA stream (cudaStream_t), for timing with events on the launching stream. */
+void* hpq_stream(hpq_handle* h);
+/* Counters since hpq_init, updated at the end of each step: multigrid V-cycles, slices solved,
+ * plasma particle pushes (the reference's performance counters, src/Hipace.H:275-282) and
+ * kernels launched by this library (graph replays included). Any pointer may be NULL. */
+int hpq_get_counters(hpq_handle* h, int64_t* mg_vcycles, int64_t* slices, int64_t* plasma_pushes,
+                     int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPQ_H_ */

@@ -1,0 +1,153 @@
+"""Input decks used by the parity tests and the benchmark (reference keys)."""
+import json
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = json.load(open(os.path.join(HERE, "golden", "golden_cases.json")))
+
+
+def golden_input(name):
+    return GOLDEN[name]["input"]
+
+
+# small explicit-solver case with a moving, spread beam (exercises beam push, slipping,
+# Reflecting plasma boundary and an odd grid -> node-centred multigrid)
+EXPLICIT_MOVING = """
+amr.n_cell = 33 33 40
+hipace.normalized_units = 1
+max_step = 2
+hipace.dt = 20
+hipace.depos_order_xy = 2
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -6. -6. -8.
+geometry.prob_hi =  6.  6.  4.
+beams.names = beam
+beam.injection_type = fixed_weight
+beam.num_particles = 20000
+beam.position_mean = 0. 0. 0.
+beam.position_std = 0.5 0.5 1.0
+beam.density = 5.
+beam.u_mean = 0. 0. 2000.
+beam.u_std = 3. 3. 10.
+beam.n_subcycles = 4
+random_seed = 7
+plasmas.names = plasma
+plasma.density(x,y,z) = 1. + 0.05*(x*x+y*y)
+plasma.ppc = 1 1
+plasma.element = electron
+hipace.MG_tolerance_rel = 1e-12
+"""
+
+# predictor-corrector solver, 3 fixed iterations (the configuration of the CPU-runnable case)
+PC_SMALL = """
+amr.n_cell = 32 32 40
+hipace.normalized_units = 1
+max_step = 2
+hipace.dt = 10
+hipace.bxby_solver = predictor-corrector
+hipace.predcorr_max_iterations = 3
+hipace.predcorr_B_error_tolerance = -1
+boundary.field = Dirichlet
+boundary.particle = Periodic
+geometry.prob_lo = -8. -8. -12.
+geometry.prob_hi =  8.  8.   6.
+beams.names = beam
+beam.injection_type = fixed_weight
+beam.num_particles = 20000
+beam.position_mean = 0. 0. 0.
+beam.position_std = 0.5 0.5 1.41
+beam.density = 0.5
+beam.u_mean = 0. 0. 1000.
+beam.u_std = 0. 0. 0.
+random_seed = 3
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+"""
+
+
+def config(name):
+    """The five benchmark workloads, restated in reference keys (seeded synthetic beams)."""
+    if name == "linear_wake_64":
+        return """
+amr.n_cell = 64 64 100
+hipace.normalized_units = 1
+max_step = 10
+hipace.dt = 10
+hipace.bxby_solver = predictor-corrector
+hipace.predcorr_max_iterations = 3
+hipace.predcorr_B_error_tolerance = -1
+boundary.field = Dirichlet
+boundary.particle = Periodic
+geometry.prob_lo = -8. -8. -12.
+geometry.prob_hi =  8.  8.   6.
+beams.names = beam
+beam.injection_type = fixed_weight
+beam.num_particles = 100000
+beam.position_mean = 0. 0. 0.
+beam.position_std = 0.5 0.5 1.41
+beam.density = 0.01
+beam.u_mean = 0. 0. 1000.
+beam.u_std = 0. 0. 0.
+random_seed = 1234
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+"""
+    if name == "blowout_255":
+        return """
+amr.n_cell = 255 255 256
+hipace.normalized_units = 1
+max_step = 19
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -6. -6. -8.
+geometry.prob_hi =  6.  6.  4.
+beams.names = beam
+beam.injection_type = fixed_weight
+beam.num_particles = 1000000
+beam.position_mean = 0. 0. 0.
+beam.position_std = 0.3 0.3 1.0
+beam.density = 10.
+beam.u_mean = 0. 0. 2000.
+beam.u_std = 0.0333333333333 0.0333333333333 0.
+random_seed = 1234
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+"""
+    if name == "channel_1023":
+        return """
+amr.n_cell = 1023 1023 1024
+hipace.normalized_units = 1
+max_step = 4
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -8. -8. -10.
+geometry.prob_hi =  8.  8.   4.
+beams.names = beam
+beam.injection_type = fixed_weight
+beam.num_particles = 4000000
+beam.position_mean = 0. 0. 0.
+beam.position_std = 0.3 0.3 1.0
+beam.density = 10.
+beam.u_mean = 0. 0. 2000.
+beam.u_std = 0.0333333333333 0.0333333333333 0.
+random_seed = 1234
+plasmas.names = plasma
+plasma.density(x,y,z) = 1. + 0.05*(x*x+y*y)
+plasma.ppc = 2 2
+plasma.element = electron
+"""
+    raise KeyError(name)
+
+
+# power-of-two-plus-one grids take the FFT path of the Poisson solver (2(n+1) = 128)
+EXPLICIT_FFT = EXPLICIT_MOVING.replace("amr.n_cell = 33 33 40", "amr.n_cell = 63 63 48")
+PC_FFT = PC_SMALL.replace("amr.n_cell = 32 32 40", "amr.n_cell = 63 63 40")

@@ -1,0 +1,49 @@
+"""The C-ABI library loads and exports every entry point of include/hpq.h (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import hipace2_b200 as hp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    text = open(os.path.join(ROOT, "include", "hpq.h")).read()
+    return sorted(set(re.findall(r"\b(hpq_[a-z_]+)\s*\(", text)))
+
+
+def test_header_matches_binding():
+    assert declared() == sorted(hp.EXPORTS)
+
+
+def test_library_exports_all_symbols():
+    L = hp.load_library()
+    for name in declared():
+        assert hasattr(L, name), name
+
+
+def test_create_rejects_bad_input():
+    L = hp.load_library()
+    h = ctypes.c_void_p()
+    rc = L.hpq_create(b"amr.n_cell = 8 8 8\n", ctypes.byref(h))
+    assert rc == 1
+    assert b"geometry.prob_lo" in L.hpq_create_error()
+
+
+def test_create_rejects_unsupported_feature():
+    from cases import golden_input
+    text = golden_input("linear_wake.normalized.1Rank") + "\namr.max_level = 1\n"
+    with pytest.raises(hp.HpqError) as e:
+        hp.Hipace(text)
+    assert "mesh refinement" in str(e.value)
+
+
+def test_calls_out_of_order_are_state_errors():
+    from cases import golden_input
+    sim = hp.Hipace(golden_input("linear_wake.normalized.1Rank"))
+    with pytest.raises(hp.HpqError) as e:
+        sim.step(0)
+    assert e.value.code == 3
