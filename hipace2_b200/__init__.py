@@ -24,7 +24,7 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
            "hpq_get_diag", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
-           "hpq_get_profile")
+           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc")
 
 _lib = None
 
@@ -72,6 +72,7 @@ def load_library(path=None):
         "hpq_get_counters": ([vp, lp, lp, lp, lp], i32),
         "hpq_set_profiling": ([vp, i32], i32),
         "hpq_get_profile": ([vp, cp, dp, lp], i32),
+        "hpq_poisson_dirichlet_noalloc": ([vp, vp, i32, i32, ctypes.c_double, ctypes.c_double, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -36,7 +36,8 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", tmp, os.path.join(CSRC, "api.cu")]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", tmp, os.path.join(CSRC, "api.cu"),
+                                   os.path.join(CSRC, "poisson_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

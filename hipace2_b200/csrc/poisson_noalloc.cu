@@ -1,0 +1,166 @@
+// Allocation-free Dirichlet Poisson solve (hpq_poisson_dirichlet_noalloc in include/hpq.h).
+//
+// Some callers of this library cannot call cudaMalloc: code that runs while a CUDA stream is
+// being captured into a graph (allocation is not a capturable operation), plugins of host
+// frameworks that own the device memory pool and forbid side allocations, and real-time loops
+// that must not pay for or fail on an allocation at solve time. This entry point serves them:
+// the caller passes the right-hand side and the solution buffer; the temporaries of the solve
+// (the transposed intermediate, the eigenvalues and the FFT twiddles) live in one file-scope
+// device array of fixed size, reserved when the library is loaded and held by every GPU that
+// loads it until the process exits.
+//
+// Limit: nx and ny of the form 2^k - 1 with 31 <= n <= 1023 (the shared-memory FFT path of the
+// DST-I), i.e. at most 1023 x 1023 cells; the scratch array is 16.1 MiB.
+// All calls share the array and it keeps the contents of the last call. Every element a solve
+// reads is written earlier in the same solve, so nothing needs clearing between calls; two
+// calls whose kernels overlap on the GPU (different streams, or different host threads on one
+// stream without ordering) race on the array and give wrong results.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/hpq.h"
+#include "fftdst.cuh"
+
+namespace {
+
+constexpr int kMaxN = 1023;
+constexpr size_t kPlane = (size_t)kMaxN * kMaxN;          // one nx x ny plane
+constexpr size_t kTw = 2048;                               // complex twiddles: M/2 for x and y
+constexpr size_t kScratchDoubles = 2 * kPlane + 2 * kTw;   // work plane, eigenvalues, twiddles
+
+static __device__ __align__(256) double g_poisson_scratch[kScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+// Set-up, once per device with that device current: the host address of the array is only a
+// stand-in, kernels must be given the device address returned here.
+int scratch_for_current_device(double** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HPQ_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_poisson_scratch) != cudaSuccess || !p) return HPQ_ERR_CUDA;
+        g_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return HPQ_OK;
+}
+
+// eigenvalues of the 5-point Laplacian with the normalisation of the two DST-I per axis
+__global__ void k_fill_eig(double* eig, int nx, int ny, double dx, double dy) {
+    const double pi = 3.14159265358979323846;
+    const double sxf = pi / (2. * (nx + 1)), syf = pi / (2. * (ny + 1));
+    const double norm = (2.0 / (nx + 1)) * (2.0 / (ny + 1));
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)nx * ny;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        double a = sin((i + 1) * sxf), b = sin((j + 1) * syf);
+        a *= a;
+        b *= b;
+        eig[k] = norm / (-4.0 * (a / (dx * dx) + b / (dy * dy)));
+    }
+}
+
+__global__ void k_fill_twiddles(hpq::Cx<double>* tw, int M) {
+    const double pi = 3.14159265358979323846;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M / 2; k += gridDim.x * blockDim.x)
+        tw[k] = {cos(2 * pi * k / M), -sin(2 * pi * k / M)};
+}
+
+template <int M, int LOGM>
+cudaError_t pass_t(cudaStream_t st, const double* in, int nrows, int n, int rpp, double* out,
+                   const hpq::Cx<double>* tw) {
+    const int rb = hpq::DstCfg<M>::RB;
+    const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>);
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_t<double, M, LOGM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    hpq::k_dst_pass_t<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, out, tw);
+    return cudaGetLastError();
+}
+
+template <int M, int LOGM>
+cudaError_t pass_eig(cudaStream_t st, const double* in, int nrows, int n, int rpp, const double* eig,
+                     double* out, const hpq::Cx<double>* tw) {
+    const int rb = hpq::DstCfg<M>::RB;
+    const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>) + (size_t)rb * n * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_eig<double, M, LOGM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    hpq::k_dst_pass_eig<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, eig, out, tw);
+    return cudaGetLastError();
+}
+
+// The last x-pass writes a plain nx x ny plane (the caller's solution buffer): a slab view with
+// no guard cells, i.e. pitch nx and the guard offset removed from the base pointer.
+template <int M, int LOGM>
+cudaError_t pass_plane(cudaStream_t st, const double* in, int nrows, int n, int ny, double* out,
+                       const hpq::Cx<double>* tw) {
+    const int rb = hpq::DstCfg<M>::RB;
+    const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>);
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_field<double, M, LOGM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int G = hpq::kGuardAlloc;
+    double* base = out - ((ptrdiff_t)G * n + G);  // element (i, j) -> out[j * n + i]
+    hpq::k_dst_pass_field<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(
+        in, nrows, n, ny, base, 0, n, 0, 0, 0, tw);
+    return cudaGetLastError();
+}
+
+int pow2_len(int n) {
+    const int m = 2 * (n + 1);
+    return (n >= 31 && n <= kMaxN && (m & (m - 1)) == 0) ? m : 0;
+}
+
+#define HPQ_NOALLOC_DISPATCH(Mval, CALL) \
+    switch (Mval) {                      \
+        case 64: e = CALL(64, 6); break;   \
+        case 128: e = CALL(128, 7); break; \
+        case 256: e = CALL(256, 8); break; \
+        case 512: e = CALL(512, 9); break; \
+        case 1024: e = CALL(1024, 10); break; \
+        case 2048: e = CALL(2048, 11); break; \
+        default: return HPQ_ERR_ARG;     \
+    }
+
+}  // namespace
+
+extern "C" int hpq_poisson_dirichlet_noalloc(const double* f, double* u, int nx, int ny, double dx, double dy,
+                                             void* stream) {
+    if (!f || !u || !(dx > 0) || !(dy > 0)) return HPQ_ERR_ARG;
+    if (nx > kMaxN || ny > kMaxN) return HPQ_ERR_TOO_LARGE;
+    const int Mx = pow2_len(nx), My = pow2_len(ny);
+    if (!Mx || !My) return HPQ_ERR_ARG;
+    double* scratch = nullptr;
+    if (int r = scratch_for_current_device(&scratch)) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* work = scratch;                        // transposed intermediate, nx*ny
+    double* eig = scratch + kPlane;                // eigenvalues, nx*ny
+    auto* twx = reinterpret_cast<hpq::Cx<double>*>(scratch + 2 * kPlane);  // Mx/2 complex
+    auto* twy = twx + kTw / 2;                                              // My/2 complex
+    k_fill_eig<<<148, 256, 0, st>>>(eig, nx, ny, dx, dy);
+    k_fill_twiddles<<<4, 256, 0, st>>>(twx, Mx);
+    k_fill_twiddles<<<4, 256, 0, st>>>(twy, My);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return HPQ_ERR_CUDA;
+    // x-pass of f (read in place) -> work (transposed); y-pass * eig * y-pass -> u (as a
+    // temporary); x-pass of u -> u (each block reads its rows completely before writing them)
+#define CALL1(M, L) pass_t<M, L>(st, f, ny, nx, ny, work, twx)
+    HPQ_NOALLOC_DISPATCH(Mx, CALL1)
+#undef CALL1
+    if (e != cudaSuccess) return HPQ_ERR_CUDA;
+#define CALL2(M, L) pass_eig<M, L>(st, work, nx, ny, nx, eig, u, twy)
+    HPQ_NOALLOC_DISPATCH(My, CALL2)
+#undef CALL2
+    if (e != cudaSuccess) return HPQ_ERR_CUDA;
+#define CALL3(M, L) pass_plane<M, L>(st, u, ny, nx, ny, u, twx)
+    HPQ_NOALLOC_DISPATCH(Mx, CALL3)
+#undef CALL3
+    if (e != cudaSuccess) return HPQ_ERR_CUDA;
+    return HPQ_OK;
+}

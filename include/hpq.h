@@ -29,7 +29,8 @@ enum {
     HPQ_ERR_STATE = 3,          /* call out of order (e.g. slice before hpq_begin_step) */
     HPQ_ERR_NOT_CONVERGED = 4,  /* multigrid hit its iteration limit (hpmg "failed") */
     HPQ_ERR_DIVERGED = 5,       /* multigrid residual grew by 1e20 (hpmg "failing") */
-    HPQ_ERR_ARG = 6             /* bad argument (index, name, null pointer) */
+    HPQ_ERR_ARG = 6,            /* bad argument (index, name, null pointer, unsupported shape) */
+    HPQ_ERR_TOO_LARGE = 7       /* grid larger than a fixed-size scratch area allows */
 };
 
 enum { HPQ_PLAIN_FP64 = 0, HPQ_MIXED = 1 };
@@ -110,6 +111,22 @@ void* hpq_stream(hpq_handle* h);
  * kernels launched by this library (graph replays included). Any pointer may be NULL. */
 int hpq_get_counters(hpq_handle* h, int64_t* mg_vcycles, int64_t* slices, int64_t* plasma_pushes,
                      int64_t* kernel_launches);
+
+/* Allocation-free Dirichlet Poisson solve, Lap(u) = f on an nx x ny grid (x fastest) with
+ * cell sizes dx, dy and u = 0 one cell outside the grid, by DST-I; the same solve as the slice
+ * loop's Psi/Ez/Bz solves. No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory when they solve — code running under CUDA stream capture, plugins whose
+ * host framework owns the memory pool, real-time loops that must not allocate. f and u are
+ * device pointers owned by the caller (u may not alias f); `stream` is a cudaStream_t (NULL =
+ * default stream). Nothing is allocated: the temporaries live in a 16.1 MiB device array that
+ * the library reserves at load time on every GPU that loads it, until the process exits.
+ * Limit: nx, ny of the form 2^k - 1 with 31 <= n <= 1023; larger grids return
+ * HPQ_ERR_TOO_LARGE, other shapes HPQ_ERR_ARG. The first call on a device looks up the device
+ * address of that array (once per device, with the device current), so make the first call on
+ * each device before any stream capture. All calls share the array: calls whose kernels overlap
+ * on the GPU race and give wrong results; serialise them (one stream, or events). */
+int hpq_poisson_dirichlet_noalloc(const double* f, double* u, int nx, int ny, double dx, double dy,
+                                  void* stream);
 
 #ifdef __cplusplus
 }
