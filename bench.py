@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--no-graphs", action="store_true")
     p.add_argument("--cpu-sample-slices", type=int, default=0)
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    p.add_argument("--scale-config", default="channel_1023",
+                   help="larger workload timed for FP64 vs mixed (one step each); '' to skip")
     return p.parse_args()
 
 
@@ -238,11 +241,80 @@ def run_ours(args):
     if rank == 0:
         line["gpu_launches"] = launches_in_timed
         line["cpu_baseline"] = cpu_baseline(text, args)
+    sim.close()
+    if rank == 0 and not args.no_mixed and args.precision == "fp64":
+        line["mixed"] = mixed_vs_fp64(text, args, torch)
+        if args.scale_config:
+            line["scale_point"] = scale_point(args.scale_config, torch)
+    if rank == 0:
         print(json.dumps(line))
     sim.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def mixed_vs_fp64(text, args, torch):
+    """The same workload in mixed precision (FP32 plasma, fields and multigrid; FP64 beam) against
+    the FP64 path on identical inputs: throughput and the relative L2 error of Ez, Psi and jz
+    over every slice of one step. The FP64 GPU path stands in for the FP64 oracle here (it
+    matches the oracle to <= 1e-10 in the parity tests; the oracle is too slow at this size)."""
+    import numpy as np
+    import hipace2_b200 as hp
+    comps = ["Ez", "Psi", "jz_beam", "Bx"]
+    out = {}
+    ref = make_sim(text, "fp64", graphs=True)
+    beam = ref.get_beam(0)
+    mix = make_sim(text, "mixed", graphs=True)
+    mix.set_beam(0, beam)
+    nz = ref.n_cell[2]
+    # speed: warm-up steps then timed steps, like the FP64 headline
+    w, k = max(1, args.warmup), max(1, args.steps)
+    for s in range(w):
+        mix.step(s)
+    secs = time_device_steps(mix, w, k, torch)
+    out["value"] = nz * k / secs
+    out["unit"] = "slices/s"
+    out["ms_per_step"] = secs / k * 1e3
+    # error: one step from identical state (fresh simulations, same beam)
+    ref.close()
+    mix.close()
+    ref = make_sim(text, "fp64", graphs=True)
+    ref.set_beam(0, beam)
+    mix = make_sim(text, "mixed", graphs=True)
+    mix.set_beam(0, beam)
+    ref.set_diag(comps)
+    mix.set_diag(comps)
+    ref.step(0)
+    mix.step(0)
+    for c in comps:
+        a, b = mix.get_diag(c), ref.get_diag(c)
+        out[c + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["error_reference"] = "FP64 GPU path, same inputs, step 0 (all slices)"
+    out["dtype"] = "f32 plasma/fields/multigrid, f64 beam"
+    ref.close()
+    mix.close()
+    return out
+
+
+def scale_point(name, torch):
+    """One step of a larger workload in FP64 and in mixed precision (device time)."""
+    from cases import config
+    text = config(name)
+    res = {"workload": name}
+    for prec in ("fp64", "mixed"):
+        sim = make_sim(text, prec, graphs=True)
+        nz = sim.n_cell[2]
+        sim.step(0)
+        secs = time_device_steps(sim, 1, 1, torch)
+        res[prec + "_slices_per_s"] = nz / secs
+        res[prec + "_ms_per_step"] = secs * 1e3
+        if prec == "fp64":
+            res["grid"] = sim.n_cell
+            res["plasma_particles"] = int(sim.get_plasma(0)["x"].size)
+        sim.close()
+    res["mixed_speedup"] = res["mixed_slices_per_s"] / res["fp64_slices_per_s"]
+    return res
 
 
 def cpu_baseline(text, args):

@@ -5,8 +5,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace hpq {
 
@@ -29,6 +31,39 @@ inline thread_local long long g_launches = 0;
         HPQ_CUDA(cudaGetLastError());       \
         ++::hpq::g_launches;                \
     } while (0)
+
+// Programmatic dependent launch: every kernel starts with this prologue. It lets the next kernel
+// of the stream (or graph) launch once all blocks of this one are running, then waits until the
+// previous kernel has completed and its memory is visible. Without a programmatic predecessor
+// both instructions return at once.
+#define HPQ_PDL_ENTRY()                                                         \
+    do {                                                                        \
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");         \
+        asm volatile("griddepcontrol.wait;" ::: "memory");                      \
+    } while (0)
+
+// launches with the programmatic-serialization attribute (HPQ_PDL=0 in the environment turns it off)
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("HPQ_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <typename... KArgs, typename... Args>
+inline void hpq_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    HPQ_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
 
 constexpr int kGuardAlloc = 3;   // allocated guard cells per side
 constexpr int kGuardPhys = 2;    // guard cells of the reference slice arrays (Fields.cpp:63)

@@ -22,6 +22,7 @@ namespace hpq {
 template <class R, int BM, int BN, int BK, int TM, int TN, class Epi>
 __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const R* __restrict__ A, int lda,
                                               const R* __restrict__ B, int ldb, Epi epi) {
+    HPQ_PDL_ENTRY();
     static_assert((BM / TM) * (BN / TN) == 256, "tile/thread mismatch");
     __shared__ R As[BK][BM + 1];
     __shared__ R Bs[BK][BN];
@@ -151,7 +152,7 @@ public:
     static void gemm(cudaStream_t st, int M, int N, int K, const R* A, int lda, const R* B, int ldb, Epi e) {
         constexpr int BM = 64, BN = 64, BK = 16;
         dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-        k_gemm<R, BM, BN, BK, 4, 4, Epi><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, e);
+        hpq_launch(k_gemm<R, BM, BN, BK, 4, 4, Epi>, dim3(grid), dim3(256), 0, st, M, N, K, A, lda, B, ldb, e);
         HPQ_LAUNCH_CHECK();
     }
 

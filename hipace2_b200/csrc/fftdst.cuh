@@ -24,7 +24,7 @@ struct Cx {
 // rows per block by transform length (shared memory: RB/2 complex arrays of M elements)
 template <int M>
 struct DstCfg {
-    static constexpr int RB = M <= 512 ? 16 : (M <= 2048 ? 8 : 4);
+    static constexpr int RB = M <= 2048 ? 4 : 2;
 };
 
 template <class R, int M>
@@ -76,6 +76,7 @@ __device__ __forceinline__ R dst_val(const Cx<R>* z, int r, int e) {
 template <class R, int M, int LOGM>
 __global__ void __launch_bounds__(256) k_dst_pass_t(const R* __restrict__ in, int nrows, int n, int rows_per_plane,
                                                     R* __restrict__ out, const Cx<R>* __restrict__ tw) {
+    HPQ_PDL_ENTRY();
     constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
@@ -98,6 +99,7 @@ template <class R, int M, int LOGM>
 __global__ void __launch_bounds__(256) k_dst_pass_eig(const R* __restrict__ in, int nrows, int n, int rows_per_plane,
                                                       const R* __restrict__ eig, R* __restrict__ out,
                                                       const Cx<R>* __restrict__ tw) {
+    HPQ_PDL_ENTRY();
     constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
@@ -130,6 +132,7 @@ template <class R, int M, int LOGM>
 __global__ void __launch_bounds__(256) k_dst_pass_field(const R* __restrict__ in, int nrows, int n, int ny, R* base,
                                                         size_t cstride, int pitch, int c0, int c1, int c2,
                                                         const Cx<R>* __restrict__ tw) {
+    HPQ_PDL_ENTRY();
     constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
@@ -197,20 +200,20 @@ public:
     template <int M, int LOGM>
     void pass_t(cudaStream_t st, const R* in, int nrows, int n, int rpp, R* out, const Cx<R>* tw) {
         const int rb = DstCfg<M>::RB;
-        k_dst_pass_t<R, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem_fft<M>(), st>>>(in, nrows, n, rpp, out, tw);
+        hpq_launch(k_dst_pass_t<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_fft<M>(), st, in, nrows, n, rpp, out, tw);
         HPQ_LAUNCH_CHECK();
     }
     template <int M, int LOGM>
     void pass_eig(cudaStream_t st, const R* in, int nrows, int n, int rpp, const R* eig, R* out, const Cx<R>* tw) {
         const int rb = DstCfg<M>::RB;
-        k_dst_pass_eig<R, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem_eig<M>(n), st>>>(in, nrows, n, rpp, eig, out, tw);
+        hpq_launch(k_dst_pass_eig<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_eig<M>(n), st, in, nrows, n, rpp, eig, out, tw);
         HPQ_LAUNCH_CHECK();
     }
     template <int M, int LOGM>
     void pass_field(cudaStream_t st, const R* in, int nrows, int n, R* base, size_t cs, int pitch, const int* comps,
                     int nrhs, const Cx<R>* tw) {
         const int rb = DstCfg<M>::RB;
-        k_dst_pass_field<R, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem_fft<M>(), st>>>(
+        hpq_launch(k_dst_pass_field<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_fft<M>(), st, 
             in, nrows, n, ny, base, cs, pitch, comps[0], nrhs > 1 ? comps[1] : comps[0], nrhs > 2 ? comps[2] : comps[0], tw);
         HPQ_LAUNCH_CHECK();
     }

@@ -120,6 +120,7 @@ template <class R>
 __global__ void k_plasma_reset(PlasmaDev<R> P, const double* __restrict__ x0, const double* __restrict__ y0,
                                Expr density, double c_t, double scale, double ux0, double uy0, double uz0,
                                double clight) {
+    HPQ_PDL_ENTRY();
     for (long long i = gtid(); i < P.n; i += gstride()) {
         const double x = x0[i], y = y0[i];
         double v[3] = {x, y, c_t};
@@ -151,7 +152,8 @@ __device__ __forceinline__ void addc(R* base, int pitch, int i, int j, R v) {
 
 template <class R>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
-                                                        const int* gate = nullptr) {
+                                                        const int* gate) {
+    HPQ_PDL_ENTRY();
     if (gate && !*gate) return;
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R clight = (R)g.c, clightinv = (R)(1.0 / g.c);
@@ -197,6 +199,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
 // ------------------------------------------------------------------------------------------
 template <class R, int DT>
 __global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g) {
+    HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);
     const R charge_invvol_mu0 = (R)(P.charge * (double)invvol * g.mu0);
@@ -294,7 +297,8 @@ __device__ __forceinline__ void plasma_rhs_dual(Du<R> ux, Du<R> uy, Du<R> pi, R 
 
 template <class R>
 __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, Geo g, int temp,
-                                                     const int* gate = nullptr) {
+                                                     const int* gate) {
+    HPQ_PDL_ENTRY();
     if (gate && !*gate) return;
     const R clight = (R)g.c, ci = (R)(1. / g.c);
     const R qmc = (R)(P.charge / (P.mass * g.c));
@@ -342,7 +346,8 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
 // ------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __restrict__ ctl, int which, R* jx, R* jy,
-                                                      R* jz, R* rmj, int pitch, Geo g, int gated = 0) {
+                                                      R* jz, R* rmj, int pitch, Geo g, int gated) {
+    HPQ_PDL_ENTRY();
     if (gated && !ctl->pc_go) return;
     const int s = ctl->islice - which;
     if (s < 0) return;
@@ -382,6 +387,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __re
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const Ctl* __restrict__ ctl, R* jz, R* rmj,
                                                                 R* njx, R* njy, int pitch, Geo g) {
+    HPQ_PDL_ENTRY();
     const int s = ctl->islice;
     const int par = ctl->step_parity;
     const int st0 = B.start[par][s], n0 = B.count[par][s];
@@ -428,6 +434,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restrict__ ctl, int bi, Slab<R> S, Geo g,
                                                    double dt) {
+    HPQ_PDL_ENTRY();
     const int s = ctl->islice;
     const int par = ctl->step_parity;
     const int start = B.start[par][s], na = B.count[par][s];
@@ -487,6 +494,8 @@ __device__ __forceinline__ void copy_particle(const BeamBuf& d, long long di, co
 
 __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, int bi, Geo g, int keep_store,
                                                          int end_slice) {
+    HPQ_PDL_ENTRY();
+    constexpr int IT = 8;  // consecutive particles per thread and round
     __shared__ int sst[32], ssl[32];
     __shared__ int base_stay, base_slip;
     const int s = ctl->islice;
@@ -503,17 +512,23 @@ __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, in
     if (threadIdx.x == 0) { base_stay = 0; base_slip = 0; }
     __syncthreads();
     const int total = na + nc;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int chunk = 0; chunk < total; chunk += blockDim.x) {
-        const int k = chunk + threadIdx.x;
-        int stay = 0, slip = 0;
-        const BeamBuf& bb = k < na ? a : c;
-        const long long ip = k < na ? start + k : k - na;
-        if (k < total && bb.valid[ip]) {
-            if (bb.z[ip] >= min_z) stay = 1; else slip = 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int round = 0; round < total; round += blockDim.x * IT) {
+        const int first = round + threadIdx.x * IT;
+        unsigned stay_m = 0, slip_m = 0;
+#pragma unroll
+        for (int q = 0; q < IT; ++q) {
+            const int k = first + q;
+            if (k >= total) break;
+            const BeamBuf& bb = k < na ? a : c;
+            const long long ip = k < na ? start + k : k - na;
+            if (bb.valid[ip]) {
+                if (bb.z[ip] >= min_z) stay_m |= 1u << q; else slip_m |= 1u << q;
+            }
         }
-        // inclusive warp scans
-        int vs = stay, vl = slip;
+        const int ns = __popc(stay_m), nl = __popc(slip_m);
+        // block-wide exclusive scans of the per-thread counts
+        int vs = ns, vl = nl;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             int t1 = __shfl_up_sync(0xffffffffu, vs, d), t2 = __shfl_up_sync(0xffffffffu, vl, d);
@@ -522,8 +537,8 @@ __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, in
         if (lane == 31) { sst[warp] = vs; ssl[warp] = vl; }
         __syncthreads();
         if (warp == 0) {
-            int ws = lane < (int)(blockDim.x >> 5) ? sst[lane] : 0;
-            int wl = lane < (int)(blockDim.x >> 5) ? ssl[lane] : 0;
+            int ws = lane < nwarps ? sst[lane] : 0;
+            int wl = lane < nwarps ? ssl[lane] : 0;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 int t1 = __shfl_up_sync(0xffffffffu, ws, d), t2 = __shfl_up_sync(0xffffffffu, wl, d);
@@ -532,14 +547,22 @@ __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, in
             sst[lane] = ws; ssl[lane] = wl;
         }
         __syncthreads();
-        const int off_s = (warp ? sst[warp - 1] : 0) + vs - stay;
-        const int off_l = (warp ? ssl[warp - 1] : 0) + vl - slip;
-        if (stay && keep_store) copy_particle(o, cursor + base_stay + off_s, bb, ip, 0);
-        if (slip) copy_particle(co, base_slip + off_l, bb, ip, bb.nsub[ip]);
+        int os = base_stay + (warp ? sst[warp - 1] : 0) + vs - ns;
+        int ol = base_slip + (warp ? ssl[warp - 1] : 0) + vl - nl;
+#pragma unroll
+        for (int q = 0; q < IT; ++q) {
+            const int k = first + q;
+            const bool st_ = (stay_m >> q) & 1u, sl_ = (slip_m >> q) & 1u;
+            if (!st_ && !sl_) continue;
+            const BeamBuf& bb = k < na ? a : c;
+            const long long ip = k < na ? start + k : k - na;
+            if (st_) { if (keep_store) copy_particle(o, cursor + os, bb, ip, 0); ++os; }
+            else { copy_particle(co, ol, bb, ip, bb.nsub[ip]); ++ol; }
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
-            base_stay += sst[(blockDim.x >> 5) - 1];
-            base_slip += ssl[(blockDim.x >> 5) - 1];
+            base_stay += sst[nwarps - 1];
+            base_slip += ssl[nwarps - 1];
         }
         __syncthreads();
     }
@@ -563,6 +586,7 @@ struct CompList {
 // zero listed components over the whole allocated slice (setVal on growntilebox)
 template <class R>
 __global__ void k_zero_comps(Slab<R> S, CompList L) {
+    HPQ_PDL_ENTRY();
     const size_t n = S.cstride;
     for (long long k = gtid(); k < (long long)n; k += gstride())
 #pragma unroll 4
@@ -576,6 +600,7 @@ struct CopyList {
 };
 template <class R>
 __global__ void k_copy_comps(Slab<R> S, CopyList L) {
+    HPQ_PDL_ENTRY();
     const size_t n = S.cstride;
     for (long long k = gtid(); k < (long long)n; k += gstride())
         for (int q = 0; q < L.n; ++q) S.base[(size_t)L.dst[q] * S.cstride + k] = S.base[(size_t)L.src[q] * S.cstride + k];
@@ -585,6 +610,7 @@ __global__ void k_copy_comps(Slab<R> S, CopyList L) {
 // (Fields.cpp:606-615, 840-903). Staging layout: stage[(j*3 + k)*ldx + i], k = Psi, Ez, Bz.
 template <class R>
 __global__ void k_rhs3(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int sj, int add_ions, int add_rho, int add_rmb) {
+    HPQ_PDL_ENTRY();
     const int ax = S.nx + 2 * kGuardAlloc;
     const long long ntot = (long long)ax * S.rows;
     const F2<R> rm = S.c(C_RHOMJZ), jx = S.c(C_JX), jy = S.c(C_JY), ions = S.c(C_IONS), rho = S.c(C_RHO),
@@ -609,6 +635,7 @@ __global__ void k_rhs3(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int sj, 
 // ExmBy = -dPsi/dx, EypBx = -dPsi/dy on the box grown by one guard (Fields.cpp:931-956)
 template <class R>
 __global__ void k_grad_psi(Slab<R> S, Geo g) {
+    HPQ_PDL_ENTRY();
     const int w = S.nx + 2, h = S.ny + 2;
     const F2<R> Psi = S.c(C_PSI), Ex = S.c(C_EXMBY), Ey = S.c(C_EYPBX);
     const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]);
@@ -623,6 +650,7 @@ __global__ void k_grad_psi(Slab<R> S, Geo g) {
 // (Hipace.cpp:744-790) in one launch
 template <class R>
 __global__ void k_grad_psi_sxsy(Slab<R> S, Geo g) {
+    HPQ_PDL_ENTRY();
     const int w = S.nx + 2, h = S.ny + 2;
     const F2<R> Psi = S.c(C_PSI), Ex = S.c(C_EXMBY), Ey = S.c(C_EYPBX);
     const F2<R> jzb = S.c(C_JZB), pjx = S.c(C_PJXB), pjy = S.c(C_PJYB), njx = S.c(C_NJXB), njy = S.c(C_NJYB),
@@ -648,6 +676,7 @@ __global__ void k_grad_psi_sxsy(Slab<R> S, Geo g) {
 // Sx, Sy from the beam currents (Hipace.cpp:744-790)
 template <class R>
 __global__ void k_sxsy_beam(Slab<R> S, Geo g) {
+    HPQ_PDL_ENTRY();
     const F2<R> jzb = S.c(C_JZB), pjx = S.c(C_PJXB), pjy = S.c(C_PJYB), njx = S.c(C_NJXB), njy = S.c(C_NJYB),
                 Sx = S.c(C_SX), Sy = S.c(C_SY);
     const R mu0 = (R)g.mu0;
@@ -666,6 +695,7 @@ __global__ void k_sxsy_beam(Slab<R> S, Geo g) {
 // PC: right-hand sides of Bx, By (Fields.cpp:1008-1078) into stage rows k = 0 (Bx), 1 (By)
 template <class R>
 __global__ void k_rhs_bxby(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int sj) {
+    HPQ_PDL_ENTRY();
     const F2<R> jz = S.c(C_JZ), pjx = S.c(C_PJX), pjy = S.c(C_PJY), njx = S.c(C_NJX), njy = S.c(C_NJY);
     const R mu0 = (R)g.mu0;
     const R hx = (R)(0.5 * g.dxi[0]), hy = (R)(0.5 * g.dxi[1]), hz = (R)(0.5 * g.dxi[2]);
@@ -681,6 +711,7 @@ __global__ void k_rhs_bxby(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int 
 // out layout: [q][nz][ny][nx]
 template <class R>
 __global__ void k_diag_copy(Slab<R> S, const Ctl* ctl, CompList L, double* __restrict__ out, int nz) {
+    HPQ_PDL_ENTRY();
     const int s = ctl->islice;
     const long long nxy = (long long)S.nx * S.ny;
     for (long long k = gtid(); k < nxy * L.n; k += gstride()) {

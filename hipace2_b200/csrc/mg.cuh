@@ -73,6 +73,7 @@ __device__ __forceinline__ R mg_restrict1(const MV<R>& f, int i, int j, int c) {
 
 template <class R, bool CELL>
 __global__ void k_mg_restrict(MGLev C, MV<R> crse, MV<R> fine, int nc) {
+    HPQ_PDL_ENTRY();
     const int vw = C.vhi_i - C.vlo + 1, vh = C.vhi_j - C.vlo + 1;
     for (long long k = gtid(); k < (long long)vw * vh; k += gstride()) {
         const int i = C.vlo + (int)(k % vw), j = C.vlo + (int)(k / vw);
@@ -94,6 +95,7 @@ __device__ __forceinline__ R mg_interp1(const MV<R>& crse, int i, int j, int c) 
 
 template <class R, bool CELL>
 __global__ void k_mg_interp(MGLev F, MV<R> out, MV<R> fin, MV<R> crse) {
+    HPQ_PDL_ENTRY();
     const int vw = F.vhi_i - F.vlo + 1, vh = F.vhi_j - F.vlo + 1;
     for (long long k = gtid(); k < (long long)vw * vh; k += gstride()) {
         const int i = F.vlo + (int)(k % vw), j = F.vlo + (int)(k / vw);
@@ -123,6 +125,9 @@ template <class R>
 struct SmoothArgs {
     MGLev L, Lc;
     MV<R> out, rhs, acf, in, crse_in, crse_res;
+    // ping-pong: when set, iteration parity (Ctl::mg_iter & 1) == 1 swaps in/out for in2/out2
+    MV<R> in2, out2;
+    int pingpong;
     R facx, facy;
     Ctl* ctl;
     unsigned int* counter;
@@ -164,43 +169,63 @@ __device__ __forceinline__ void mg_decide_iter(Ctl* ctl, double norminf, int max
 #endif
 }
 
-template <class R, bool CELL, int T, int INIT, bool RES, bool RESTR, int NORM>
+template <int T, int NSW>
+struct SmoothSmem {
+    static constexpr int H = NSW + 2;  // exact residual on the tile and its ring after NSW sweeps
+    static constexpr int E = T + 2 * H;
+    static constexpr int Q = T + 2;
+    template <class R>
+    static constexpr size_t bytes() { return (size_t)(5 * E * E + 2 * Q * Q) * sizeof(R); }
+};
+
+template <class R, bool CELL, int T, int INIT, bool RES, bool RESTR, int NORM, int NSW>
 __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
-    constexpr int H = 6;
-    constexpr int E = T + 2 * H;
-    constexpr int Q = T + 2;  // residual tile with its ring
-    __shared__ R sp[2][E * E];
-    __shared__ R sr[RES ? 2 : 1][RES ? Q * Q : 1];
+    HPQ_PDL_ENTRY();
+    using SM = SmoothSmem<T, NSW>;
+    constexpr int H = SM::H;
+    constexpr int E = SM::E;
+    constexpr int Q = SM::Q;  // residual tile with its ring
+    extern __shared__ unsigned char smem_raw[];
+    R (*sp)[E * E] = reinterpret_cast<R (*)[E * E]>(smem_raw);                 // phi, 2 comps
+    R (*srh)[E * E] = reinterpret_cast<R (*)[E * E]>(smem_raw + 2 * E * E * sizeof(R));  // rhs
+    R* sa = reinterpret_cast<R*>(smem_raw + 4 * E * E * sizeof(R));             // coefficient
+    R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 5 * E * E * sizeof(R));   // residual
     __shared__ double wmax[8], wrhs[8];
     const MGLev& L = A.L;
     const int t0i = L.vlo + blockIdx.x * T, t0j = L.vlo + blockIdx.y * T;
     const int ti0 = t0i - H, tj0 = t0j - H;
+    const bool swap = A.pingpong && (A.ctl->mg_iter & 1);
+    const MV<R> vin = swap ? A.in2 : A.in;
+    const MV<R> vout = swap ? A.out2 : A.out;
+    // every global read of the block happens here, all in flight together
     for (int e = threadIdx.x; e < E * E; e += blockDim.x) {
         const int i = ti0 + e % E, j = tj0 + e / E;
         const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
+        sa[e] = v ? A.acf(i, j, 0) : R(0);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             R val = R(0);
             if (v) {
-                if (INIT == MG_INIT_VIEW) val = A.in(i, j, c);
-                else if (INIT == MG_INIT_INTERP) val = A.in(i, j, c) + mg_interp1<R, CELL>(A.crse_in, i, j, c);
+                if (INIT == MG_INIT_VIEW) val = vin(i, j, c);
+                else if (INIT == MG_INIT_INTERP) val = vin(i, j, c) + mg_interp1<R, CELL>(A.crse_in, i, j, c);
             }
             sp[c][e] = val;
+            srh[c][e] = v ? A.rhs(i, j, c) : R(0);
         }
     }
     __syncthreads();
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < NSW; ++s) {
         for (int e = threadIdx.x; e < E * E; e += blockDim.x) {
             const int li = e % E, lj = e / E;
             if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1) continue;
             const int i = ti0 + li, j = tj0 + lj;
             if (((i + j + s) & 1) != 0) continue;
             if (i < L.vlo || i > L.vhi_i || j < L.vlo || j > L.vhi_j) continue;
-            const R a = A.acf(i, j, 0);
+            const R a = sa[e];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const R* q = sp[c];
-                sp[c][e] = mg_gs<R, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], A.rhs(i, j, c), a, A.facx, A.facy);
+                sp[c][e] = mg_gs<R, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], a, A.facx, A.facy);
             }
         }
         __syncthreads();
@@ -218,8 +243,8 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
                 R r = R(0);
                 if (v) {
                     const R* q = sp[c];
-                    const R rh = A.rhs(i, j, c);
-                    r = rh + A.acf(i, j, 0) * q[k] - mg_lap<R, CELL>(L, i, j, q[k], q[k - 1], q[k + 1], q[k - E], q[k + E], A.facx, A.facy);
+                    const R rh = srh[c][k];
+                    r = rh + sa[k] * q[k] - mg_lap<R, CELL>(L, i, j, q[k], q[k - 1], q[k + 1], q[k - E], q[k + E], A.facx, A.facy);
                     if (NORM != MG_NORM_NONE && in_tile) {
                         bmax = fmax(bmax, fabs((double)r));
                         if (NORM == MG_NORM_FIRST) brhs = fmax(brhs, fabs((double)rh));
@@ -234,8 +259,8 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
         const int i = t0i + li, j = t0j + lj;
         if (i > L.vhi_i || j > L.vhi_j) continue;
         const int k = (lj + H) * E + (li + H);
-        A.out(i, j, 0) = sp[0][k];
-        A.out(i, j, 1) = sp[1][k];
+        vout(i, j, 0) = sp[0][k];
+        vout(i, j, 1) = sp[1][k];
     }
     if (RESTR) {
         __syncthreads();
@@ -331,6 +356,7 @@ __device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* acf, const R
 template <class R, bool CELL>
 __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restrict__ res_g, const R* __restrict__ acf_g,
                                                     R* __restrict__ cor_g, R facx0, R facy0) {
+    HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
     R* arena = reinterpret_cast<R*>(smem_raw);
     // level l: cor (2n), res (2n), rescor (2n), acf (n)
@@ -422,7 +448,9 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
 }
 
 template <class R>
-__global__ void k_mg_copy_out(MGLev L, MV<R> sol, MV<R> cor) {
+__global__ void k_mg_copy_out(MGLev L, MV<R> sol, MV<R> cor_even, MV<R> cor_odd, const Ctl* ctl) {
+    HPQ_PDL_ENTRY();
+    const MV<R> cor = (ctl->mg_iter & 1) ? cor_odd : cor_even;
     const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
     for (long long k = gtid(); k < (long long)vw * vh; k += gstride()) {
         const int i = L.vlo + (int)(k % vw), j = L.vlo + (int)(k / vw);
@@ -518,7 +546,7 @@ public:
     }
     double fac(int l, double d) const { const double f = (double)(1 << l); return 1. / ((d * f) * (d * f)); }
 
-    template <bool CELL, int INIT, bool RES, bool RESTR, int NORM>
+    template <bool CELL, int INIT, bool RES, bool RESTR, int NORM, int NSW = 4>
     void smooth(cudaStream_t st, int l, SmoothArgs<R> a) {
         const MGLev& L = lev[l];
         a.L = L;
@@ -527,13 +555,15 @@ public:
         a.facy = (R)fac(l, dy);
         a.counter = counter;
         const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
-        if (vw * (long long)vh >= 600 * 600) {
-            dim3 grid((vw + 23) / 24, (vh + 23) / 24);
-            k_mg_smooth<R, CELL, 24, INIT, RES, RESTR, NORM><<<grid, 256, 0, st>>>(a);
-        } else {
-            dim3 grid((vw + 15) / 16, (vh + 15) / 16);
-            k_mg_smooth<R, CELL, 16, INIT, RES, RESTR, NORM><<<grid, 256, 0, st>>>(a);
+        dim3 grid((vw + 15) / 16, (vh + 15) / 16);
+        constexpr size_t smem = SmoothSmem<16, NSW>::template bytes<R>();
+        auto kern = k_mg_smooth<R, CELL, 16, INIT, RES, RESTR, NORM, NSW>;
+        static bool attr_done = false;  // one per instantiation
+        if (!attr_done) {
+            HPQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_done = true;
         }
+        hpq_launch(kern, grid, dim3(256), smem, st, a);
         HPQ_LAUNCH_CHECK();
     }
 
@@ -552,7 +582,7 @@ public:
         for (int l = 1; l <= sb; ++l) {
             MV<R> fine = (l == 1) ? a0 : own(acf, l - 1, 1);
             const long long n = (long long)lev[l].w * lev[l].h;
-            k_mg_restrict<R, CELL><<<blocks_for(n, 256), 256, 0, st>>>(lev[l], own(acf, l, 1), fine, 1);
+            hpq_launch(k_mg_restrict<R, CELL>, dim3(blocks_for(n, 256)), dim3(256), 0, st, lev[l], own(acf, l, 1), fine, 1);
             HPQ_LAUNCH_CHECK();
         }
         HPQ_CUDA(cudaMemsetAsync(&ctl->mg_norm, 0, sizeof(double), st));
@@ -572,8 +602,8 @@ public:
             a.out = own(cor, l); a.rhs = own(res, l); a.acf = own(acf, l, 1); a.crse_res = own(res, l + 1);
             smooth<CELL, MG_INIT_ZERO, true, true, MG_NORM_NONE>(st, l, a);
         }
-        if (cell) k_mg_bottom<R, true><<<1, 1024, bottom_smem, st>>>(coarse, res[sb], acf[sb], cor[sb], (R)fac(sb, dx), (R)fac(sb, dy));
-        else k_mg_bottom<R, false><<<1, 1024, bottom_smem, st>>>(coarse, res[sb], acf[sb], cor[sb], (R)fac(sb, dx), (R)fac(sb, dy));
+        if (cell) hpq_launch(k_mg_bottom<R, true>, dim3(1), dim3(1024), bottom_smem, st, coarse, res[sb], acf[sb], cor[sb], (R)fac(sb, dx), (R)fac(sb, dy));
+        else hpq_launch(k_mg_bottom<R, false>, dim3(1), dim3(1024), bottom_smem, st, coarse, res[sb], acf[sb], cor[sb], (R)fac(sb, dx), (R)fac(sb, dy));
         HPQ_LAUNCH_CHECK();
         for (int l = sb - 1; l >= 1; --l) {
             SmoothArgs<R> a = b;
@@ -582,23 +612,28 @@ public:
             smooth<CELL, MG_INIT_INTERP, false, false, MG_NORM_NONE>(st, l, a);
         }
         {
+            // level 0: the up-sweep smoothing (cor0 + I(coarse) -> sol) and the closing
+            // smoothing + residual (sol -> cor0) are 8 consecutive colour sweeps; sol between the
+            // two is not read anywhere else, so one kernel does both (solve_doit copies cor0
+            // into the solution after the last cycle)
             SmoothArgs<R> a = b;
-            a.out = sol; a.rhs = rhs; a.acf = a0; a.in = own(cor, 0);
+            // cor0 is read over halos and written per tile: iterations alternate between cor[0] and
+            // up[0] by the device-side iteration parity
+            a.in = own(cor, 0); a.out = own(up, 0);
+            a.in2 = own(up, 0); a.out2 = own(cor, 0);
+            a.pingpong = 1;
+            a.rhs = rhs; a.acf = a0;
             a.crse_in = (sb == 1) ? own(cor, 1) : own(up, 1);
-            smooth<CELL, MG_INIT_INTERP, false, false, MG_NORM_NONE>(st, 0, a);
-        }
-        {
-            SmoothArgs<R> a = b;
-            a.out = own(cor, 0); a.rhs = rhs; a.acf = a0; a.in = sol; a.crse_res = own(res, 1);
-            smooth<CELL, MG_INIT_VIEW, true, true, MG_NORM_ITER>(st, 0, a);
+            a.crse_res = own(res, 1);
+            smooth<CELL, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(st, 0, a);
         }
     }
 
     template <bool CELL>
-    void post(cudaStream_t st, const Slab<R>& S) {
+    void post(cudaStream_t st, const Slab<R>& S, const Ctl* ctl) {
         MV<R> sol = slab_view(S, C_BX, C_BY);
         const long long n0 = (long long)lev[0].w * lev[0].h;
-        k_mg_copy_out<R><<<blocks_for(n0, 256), 256, 0, st>>>(lev[0], sol, own(cor, 0));
+        hpq_launch(k_mg_copy_out<R>, dim3(blocks_for(n0, 256)), dim3(256), 0, st, lev[0], sol, own(cor, 0), own(up, 0), ctl);
         HPQ_LAUNCH_CHECK();
     }
 };

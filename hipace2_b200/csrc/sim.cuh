@@ -91,6 +91,7 @@ inline int comp_from_name(const std::string& n, bool explicit_solver) {
 // ------------------------------------------------------------------------------------------
 template <class R>
 __global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl, int gated) {
+    HPQ_PDL_ENTRY();
     if (gated && !ctl->pc_go) return;
     const F2<R> Bx = S.c(bx), By = S.c(by), Bxi = S.c(bxi), Byi = S.c(byi);
     double nb = 0, nd = 0;
@@ -105,6 +106,7 @@ __global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl
 }
 // first error of a slice -> initial-guess mixing factor (InitialBfieldGuess)
 __global__ void k_pc_guess_factor(Ctl* ctl, double tol) {
+    HPQ_PDL_ENTRY();
     const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
     ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
     ctl->pc_mix = exp(-0.5 * pow(err / (2.5 * tol), 2));
@@ -115,6 +117,7 @@ __global__ void k_pc_guess_factor(Ctl* ctl, double tol) {
 }
 template <class R>
 __global__ void k_pc_guess(Slab<R> S, const Ctl* ctl) {
+    HPQ_PDL_ENTRY();
     const R mix = (R)ctl->pc_mix;
     R *B = S.c(C_BX).p, *By = S.c(C_BY).p, *PB = S.c(C_PBX).p, *PBy = S.c(C_PBY).p;
     R *PCP = S.c(C_PCPBX).p, *PCPy = S.c(C_PCPBY).p, *PCI = S.c(C_PCIBX).p, *PCIy = S.c(C_PCIBY).p;
@@ -128,6 +131,7 @@ __global__ void k_pc_guess(Slab<R> S, const Ctl* ctl) {
 }
 // error of one iteration -> mixing weights and whether to continue (MixAndShiftBfields)
 __global__ void k_pc_iter_factor(Ctl* ctl, double tol, int maxit) {
+    HPQ_PDL_ENTRY();
     if (!ctl->pc_go) return;
     const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
     ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
@@ -144,6 +148,7 @@ __global__ void k_pc_iter_factor(Ctl* ctl, double tol, int maxit) {
 }
 template <class R>
 __global__ void k_pc_mix(Slab<R> S, Ctl* ctl, double a, double tol, int maxit) {
+    HPQ_PDL_ENTRY();
     if (!ctl->pc_mixnow) return;
     const R wi = (R)ctl->pc_w[0], wp = (R)ctl->pc_w[1], ra = (R)a;
     R *B = S.c(C_BX).p, *By = S.c(C_BY).p;
@@ -159,12 +164,14 @@ __global__ void k_pc_mix(Slab<R> S, Ctl* ctl, double a, double tol, int maxit) {
     }
 }
 __global__ void k_pc_after_mix(Ctl* ctl, double tol, int maxit) {
+    HPQ_PDL_ENTRY();
     if (!ctl->pc_mixnow) return;
     ctl->pc_mixnow = 0;
     ctl->pc_go = (ctl->pc_err > tol) && (ctl->pc_iter < maxit);
 }
 
-__global__ void k_slice_done(Ctl* ctl) { ctl->islice -= 1; }
+__global__ void k_slice_done(Ctl* ctl) {
+    HPQ_PDL_ENTRY(); ctl->islice -= 1; }
 
 // ------------------------------------------------------------------------------------------
 template <class R>
@@ -648,14 +655,14 @@ public:
             const int nppc = P.ppc[0] * P.ppc[1];
             const double scale = nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc);
             if (pl[s].n == 0) continue;
-            k_plasma_reset<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], px0[s], py0[s], P.density, c_t, scale,
+            hpq_launch(k_plasma_reset<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], px0[s], py0[s], P.density, c_t, scale,
                                                                          P.u_mean[0], P.u_mean[1], P.u_mean[2], cfg.pc.c);
             HPQ_LAUNCH_CHECK();
         }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (!pl[s].neutralize || pl[s].n == 0) continue;
             DepOut<R> o{nullptr, nullptr, nullptr, nullptr, nullptr, S.c(C_IONS).p, S.pitch};
-            k_plasma_deposit<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], o, g, -pl[s].charge);
+            hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr);
             HPQ_LAUNCH_CHECK();
         }
         // control block for the slice march
@@ -686,37 +693,37 @@ public:
         if (pl[sp].n == 0) return;
         DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
         Scope sc(this, "plasma_deposit");
-        k_plasma_deposit<R><<<blocks_for(pl[sp].n, 256), 256, 0, st>>>(pl[sp], o, g, pl[sp].charge);
+        hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr);
         HPQ_LAUNCH_CHECK();
     }
     void deposit_beam(int b, int which, R* jx, R* jy, R* jz, R* rmj) {
         Scope sc(this, "beam_deposit");
-        k_beam_deposit<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, which, jx, jy, jz, rmj, S.pitch, g);
+        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], (const Ctl*)ctl, which, jx, jy, jz, rmj, S.pitch, g, 0);
         HPQ_LAUNCH_CHECK();
     }
     void zero(std::initializer_list<int> comps) {
         CompList L{};
         for (int c : comps) L.c[L.n++] = c;
-        k_zero_comps<R><<<blocks_for((long long)S.cstride, 256, 148 * 8), 256, 0, st>>>(S, L);
+        hpq_launch(k_zero_comps<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 8)), dim3(256), 0, st, S, L);
         HPQ_LAUNCH_CHECK();
     }
     void copies(std::initializer_list<std::pair<int, int>> pairs) {
         CopyList L{};
         for (auto& p : pairs) { L.dst[L.n] = p.first; L.src[L.n] = p.second; L.n++; }
-        k_copy_comps<R><<<blocks_for((long long)S.cstride, 256, 148 * 8), 256, 0, st>>>(S, L);
+        hpq_launch(k_copy_comps<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 8)), dim3(256), 0, st, S, L);
         HPQ_LAUNCH_CHECK();
     }
     void field_solve_psi_ez_bz() {
         const long long ntot = (long long)(nx + 2 * kGuardAlloc) * S.rows;
         Scope sc(this, "poisson_psi_ez_bz");
-        k_rhs3<R><<<blocks_for(ntot, 256), 256, 0, st>>>(S, g, dst.stage, dst.sk, dst.sj, cfg.any_neutralize_background(),
+        hpq_launch(k_rhs3<R>, dim3(blocks_for(ntot, 256)), dim3(256), 0, st, S, g, dst.stage, dst.sk, dst.sj, cfg.any_neutralize_background(),
                                                          cfg.deposit_rho && cfg.any_neutralize_background(),
                                                          cfg.explicit_solver && cfg.do_beam_jz_minus_rho);
         HPQ_LAUNCH_CHECK();
         const int comps[3] = {C_PSI, C_EZ, C_BZ};
         dst.solve(st, 3, S.base, S.cstride, S.pitch, comps);
-        if (cfg.explicit_solver) k_grad_psi_sxsy<R><<<blocks_for((long long)(nx + 2) * (ny + 2), 256), 256, 0, st>>>(S, g);
-        else k_grad_psi<R><<<blocks_for((long long)(nx + 2) * (ny + 2), 256), 256, 0, st>>>(S, g);
+        if (cfg.explicit_solver) hpq_launch(k_grad_psi_sxsy<R>, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, S, g);
+        else hpq_launch(k_grad_psi<R>, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, S, g);
         HPQ_LAUNCH_CHECK();
     }
 
@@ -754,7 +761,7 @@ public:
             cudaGraph_t body_out;
             HPQ_CUDA(cudaStreamEndCapture(st2, &body_out));
             HPQ_CUDA(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
-            mg.template post<CELL>(st, S);
+            mg.template post<CELL>(st, S, ctl);
             return;
         }
         mg.template pre<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, 0, 0);
@@ -767,7 +774,7 @@ public:
             HPQ_CUDA(cudaMemcpyAsync(&ctl_h->mg_go, &ctl->mg_go, sizeof(int), cudaMemcpyDeviceToHost, st));
             HPQ_CUDA(cudaStreamSynchronize(st));
         }
-        mg.template post<CELL>(st, S);
+        mg.template post<CELL>(st, S, ctl);
     }
 
     // one slice: replay the captured graph, or launch kernel by kernel (profiling mode)
@@ -827,7 +834,7 @@ public:
             for (size_t b = 0; b < bm.size(); ++b) {
                 Scope sc(this, "beam_deposit");
                 const bool nj = cfg.do_beam_jx_jy_deposition;
-                k_beam_deposit_this_next<R><<<148 * 2, 256, 0, st>>>(
+                hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st, 
                     bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
                     nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g);
                 HPQ_LAUNCH_CHECK();
@@ -849,9 +856,9 @@ public:
                 if (pl[s].n == 0) continue;
                 Scope sc(this, "explicit_deposit");
                 const int nb = blocks_for(pl[s].n, 256);
-                if (cfg.depos_derivative_type == 0) k_explicit_deposit<R, 0><<<nb, 256, 0, st>>>(pl[s], S, g);
-                else if (cfg.depos_derivative_type == 1) k_explicit_deposit<R, 1><<<nb, 256, 0, st>>>(pl[s], S, g);
-                else k_explicit_deposit<R, 2><<<nb, 256, 0, st>>>(pl[s], S, g);
+                if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
+                else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
+                else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
                 HPQ_LAUNCH_CHECK();
             }
             mg_solve();
@@ -859,23 +866,23 @@ public:
             pc_loop();
         }
         if (diag_list.n > 0) {
-            k_diag_copy<R><<<blocks_for((long long)nx * ny * diag_list.n, 256), 256, 0, st>>>(S, ctl, diag_list, diag_buf, nz);
+            hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)nx * ny * diag_list.n, 256)), dim3(256), 0, st, S, ctl, diag_list, diag_buf, nz);
             HPQ_LAUNCH_CHECK();
         }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "plasma_push");
-            k_plasma_push<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], S, g, 0);
+            hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 0, (const int*)nullptr);
             HPQ_LAUNCH_CHECK();
         }
         for (size_t b = 0; b < bm.size(); ++b) {
             {
                 Scope sc(this, "beam_push");
-                k_beam_push<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, (int)b, S, g, cfg.dt);
+                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, S, g, cfg.dt);
                 HPQ_LAUNCH_CHECK();
             }
             Scope sc2(this, "beam_partition");
-            k_beam_partition<<<1, 1024, 0, st>>>(bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
+            hpq_launch(k_beam_partition, dim3(1), dim3(1024), 0, st, bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
             HPQ_LAUNCH_CHECK();
         }
         if (ex) {
@@ -884,7 +891,7 @@ public:
             copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
         }
         if (bm.empty()) {
-            k_slice_done<<<1, 1, 0, st>>>(ctl);
+            hpq_launch(k_slice_done, dim3(1), dim3(1), 0, st, ctl);
             HPQ_LAUNCH_CHECK();
         }
     }
@@ -895,40 +902,40 @@ public:
         const double tol = cfg.predcorr_B_error_tolerance;
         const int maxit = cfg.predcorr_max_iterations;
         HPQ_CUDA(cudaMemsetAsync(&ctl->pc_sum[0], 0, 2 * sizeof(double), st));
-        k_pc_norms<R><<<blocks_for(nxy, 256, 148 * 4), 256, 0, st>>>(S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
+        hpq_launch(k_pc_norms<R>, dim3(blocks_for(nxy, 256, 148 * 4)), dim3(256), 0, st, S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
         HPQ_LAUNCH_CHECK();
-        k_pc_guess_factor<<<1, 1, 0, st>>>(ctl, tol);
+        hpq_launch(k_pc_guess_factor, dim3(1), dim3(1), 0, st, ctl, tol);
         HPQ_LAUNCH_CHECK();
-        k_pc_guess<R><<<blocks_for((long long)S.cstride, 256), 256, 0, st>>>(S, ctl);
+        hpq_launch(k_pc_guess<R>, dim3(blocks_for((long long)S.cstride, 256)), dim3(256), 0, st, S, ctl);
         HPQ_LAUNCH_CHECK();
         for (int it = 0; it < maxit; ++it) {
             // iterations after convergence are predicated off on the device (Ctl::pc_go)
             for (size_t s = 0; s < pl.size(); ++s) {
                 if (pl[s].n == 0) continue;
-                k_plasma_push<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], S, g, 1, &ctl->pc_go);
+                hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, &ctl->pc_go);
                 HPQ_LAUNCH_CHECK();
                 DepOut<R> o{S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, nullptr, nullptr, S.pitch};
-                k_plasma_deposit<R><<<blocks_for(pl[s].n, 256), 256, 0, st>>>(pl[s], o, g, pl[s].charge, &ctl->pc_go);
+                hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go);
                 HPQ_LAUNCH_CHECK();
             }
             if (cfg.do_beam_jx_jy_deposition)
                 for (size_t b = 0; b < bm.size(); ++b) deposit_beam_if((int)b);
             const int comps[2] = {C_PCIBX, C_PCIBY};
-            k_rhs_bxby<R><<<blocks_for(nxy, 256), 256, 0, st>>>(S, g, pc_dst.stage, pc_dst.sk, pc_dst.sj);
+            hpq_launch(k_rhs_bxby<R>, dim3(blocks_for(nxy, 256)), dim3(256), 0, st, S, g, pc_dst.stage, pc_dst.sk, pc_dst.sj);
             HPQ_LAUNCH_CHECK();
             pc_dst.solve(st, 2, S.base, S.cstride, S.pitch, comps);
-            k_pc_norms<R><<<blocks_for(nxy, 256, 148 * 4), 256, 0, st>>>(S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
+            hpq_launch(k_pc_norms<R>, dim3(blocks_for(nxy, 256, 148 * 4)), dim3(256), 0, st, S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
             HPQ_LAUNCH_CHECK();
-            k_pc_iter_factor<<<1, 1, 0, st>>>(ctl, tol, maxit);
+            hpq_launch(k_pc_iter_factor, dim3(1), dim3(1), 0, st, ctl, tol, maxit);
             HPQ_LAUNCH_CHECK();
-            k_pc_mix<R><<<blocks_for((long long)S.cstride, 256), 256, 0, st>>>(S, ctl, cfg.predcorr_B_mixing_factor, tol, maxit);
+            hpq_launch(k_pc_mix<R>, dim3(blocks_for((long long)S.cstride, 256)), dim3(256), 0, st, S, ctl, cfg.predcorr_B_mixing_factor, tol, maxit);
             HPQ_LAUNCH_CHECK();
-            k_pc_after_mix<<<1, 1, 0, st>>>(ctl, tol, maxit);
+            hpq_launch(k_pc_after_mix, dim3(1), dim3(1), 0, st, ctl, tol, maxit);
             HPQ_LAUNCH_CHECK();
         }
     }
     void deposit_beam_if(int b) {
-        k_beam_deposit<R><<<148 * 2, 256, 0, st>>>(bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1);
+        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1);
         HPQ_LAUNCH_CHECK();
     }
 

@@ -143,19 +143,37 @@ def test_graph_replay_equals_kernel_launches():
         assert rel_l2(a, b) <= 1e-10
 
 
-def test_mixed_precision_error_vs_oracle():
-    """FP32 fields/plasma/multigrid, FP64 beam: relative L2 of Ez, Psi, jz vs the FP64 oracle."""
-    from cases import EXPLICIT_FFT
-    text = EXPLICIT_FFT.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-4")
+def mixed_errors(text, comps=("Ez", "Psi", "jz_beam", "Bx")):
     g = hp.Hipace(text, precision=hp.MIXED)
     g.init_data()
     o = Oracle(text)
     o.set_beam(0, g.get_beam(0))
-    comps = ["Ez", "Psi", "jz_beam", "Bx"]
-    g.set_diag(comps)
-    o.set_diag(comps)
+    g.set_diag(list(comps))
+    o.set_diag(list(comps))
     g.step(0)
     o.step(0)
-    errs = {k: rel_l2(g.get_diag(k), o.get_diag(k)) for k in comps}
-    print("mixed precision rel L2:", errs)
-    assert errs["Ez"] <= 1e-4 and errs["Psi"] <= 1e-4 and errs["jz_beam"] <= 1e-5
+    return {k: rel_l2(g.get_diag(k), o.get_diag(k)) for k in comps}
+
+
+# Stated error bounds of the mixed path (FP32 plasma, fields and multigrid, FP64 beam) against
+# the FP64 oracle after one full step (all slices), relative L2 over the 3-D arrays.
+MIXED_BOUNDS_WEAK = {"Ez": 1e-4, "Psi": 1e-4, "jz_beam": 1e-5, "Bx": 1e-3}
+MIXED_BOUNDS_BLOWOUT = {"Ez": 5e-3, "Psi": 1e-3, "jz_beam": 1e-5, "Bx": 1e-2}
+
+
+@pytest.mark.parametrize("regime", ["weak", "blowout"])
+def test_mixed_precision_error_vs_oracle(regime):
+    """Mixed path vs the FP64 oracle on the 63x63x48 explicit case (FFT Poisson path).
+
+    weak: driver peak density 0.05 (linear wake); blowout: peak density 5, where plasma electrons
+    cross and rounding differences grow along the slice march.
+    """
+    from cases import EXPLICIT_FFT
+    text = EXPLICIT_FFT.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-5")
+    if regime == "weak":
+        text = text.replace("beam.density = 5.", "beam.density = 0.05")
+    errs = mixed_errors(text)
+    print("mixed precision rel L2 (%s):" % regime, errs)
+    bounds = MIXED_BOUNDS_WEAK if regime == "weak" else MIXED_BOUNDS_BLOWOUT
+    for k, b in bounds.items():
+        assert errs[k] <= b, (k, errs[k], b)
