@@ -75,6 +75,13 @@ struct Ctl {
     // predictor-corrector
     double pc_err, pc_err_prev, pc_sum[2], pc_w[2], pc_mix;
     int pc_iter, pc_go, pc_mixnow, pc_pad;
+    // persistent multigrid solve (one cooperative launch): |rhs| max, residual norms by
+    // iteration parity and the grid barrier {arrivals, generation}, cleared before every solve;
+    // the barrier's timeout flag, cleared when a step begins
+    double mgp_rhsnorm, mgp_norm[2];
+    unsigned int mgp_bar[2];
+    int mgp_bar_err, mgp_pad;
+    int tc_err, tc_pad;  // error code of the tensor-core DST kernels (a timed-out wait)
 };
 
 struct Geo {

@@ -13,6 +13,12 @@
 // a CUDA graph with a conditional while node.
 #pragma once
 
+#include <algorithm>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -46,18 +52,26 @@ __device__ __forceinline__ R mg_lap(const MGLev& L, int i, int j, R pc, R pim, R
     return l;
 }
 
+// Gauss-Seidel point update (gs1, HpMultiGrid.cpp:265-294) split in two: the inverse of the
+// diagonal, which depends only on the coefficient and the position, is computed once per point
+// and reused by every colour sweep.
 template <class R, bool CELL>
-__device__ __forceinline__ R mg_gs(const MGLev& L, int i, int j, R pim, R pip, R pjm, R pjp, R rhs, R a, R facx,
-                                   R facy) {
-    R l;
+__device__ __forceinline__ R mg_diag_inv(const MGLev& L, int i, int j, R a, R facx, R facy) {
     R c0 = -(a + R(2.) * (facx + facy));
-    if (CELL && i == 0) { l = facx * R(4. / 3.) * pip; c0 -= R(2.) * facx; }
-    else if (CELL && i == L.w - 1) { l = facx * R(4. / 3.) * pim; c0 -= R(2.) * facx; }
+    if (CELL && (i == 0 || i == L.w - 1)) c0 -= R(2.) * facx;
+    if (CELL && (j == 0 || j == L.h - 1)) c0 -= R(2.) * facy;
+    return R(1.) / c0;
+}
+template <class R, bool CELL>
+__device__ __forceinline__ R mg_gs_inv(const MGLev& L, int i, int j, R pim, R pip, R pjm, R pjp, R rhs, R c0_inv,
+                                       R facx, R facy) {
+    R l;
+    if (CELL && i == 0) l = facx * R(4. / 3.) * pip;
+    else if (CELL && i == L.w - 1) l = facx * R(4. / 3.) * pim;
     else l = facx * (pim + pip);
-    if (CELL && j == 0) { l += facy * R(4. / 3.) * pjp; c0 -= R(2.) * facy; }
-    else if (CELL && j == L.h - 1) { l += facy * R(4. / 3.) * pjm; c0 -= R(2.) * facy; }
+    if (CELL && j == 0) l += facy * R(4. / 3.) * pjp;
+    else if (CELL && j == L.h - 1) l += facy * R(4. / 3.) * pjm;
     else l += facy * (pjm + pjp);
-    const R c0_inv = R(1.) / c0;
     return (rhs - l) * c0_inv;
 }
 
@@ -175,33 +189,40 @@ struct SmoothSmem {
     static constexpr int E = T + 2 * H;
     static constexpr int Q = T + 2;
     template <class R>
-    static constexpr size_t bytes() { return (size_t)(5 * E * E + 2 * Q * Q) * sizeof(R); }
+    static constexpr size_t bytes() { return (size_t)(6 * E * E + 2 * Q * Q) * sizeof(R); }
 };
 
+// One T x T tile (tile coordinates bx, by) of the fused smoother. `swap` selects in2/out2 for
+// in/out. The tile's residual and |rhs| max norms are folded into the caller's bmax / brhs.
 template <class R, bool CELL, int T, int INIT, bool RES, bool RESTR, int NORM, int NSW>
-__global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
-    HPQ_PDL_ENTRY();
+__device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, int by, bool swap,
+                                               unsigned char* smem_raw, double& bmax, double& brhs) {
     using SM = SmoothSmem<T, NSW>;
     constexpr int H = SM::H;
     constexpr int E = SM::E;
     constexpr int Q = SM::Q;  // residual tile with its ring
-    extern __shared__ unsigned char smem_raw[];
+    constexpr int NT = 256;   // threads of every smoother launch
     R (*sp)[E * E] = reinterpret_cast<R (*)[E * E]>(smem_raw);                 // phi, 2 comps
     R (*srh)[E * E] = reinterpret_cast<R (*)[E * E]>(smem_raw + 2 * E * E * sizeof(R));  // rhs
     R* sa = reinterpret_cast<R*>(smem_raw + 4 * E * E * sizeof(R));             // coefficient
-    R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 5 * E * E * sizeof(R));   // residual
-    __shared__ double wmax[8], wrhs[8];
+    R* sinv = reinterpret_cast<R*>(smem_raw + 5 * E * E * sizeof(R));           // 1 / diagonal
+    R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 6 * E * E * sizeof(R));   // residual
     const MGLev& L = A.L;
-    const int t0i = L.vlo + blockIdx.x * T, t0j = L.vlo + blockIdx.y * T;
+    const int t0i = L.vlo + bx * T, t0j = L.vlo + by * T;
     const int ti0 = t0i - H, tj0 = t0j - H;
-    const bool swap = A.pingpong && (A.ctl->mg_iter & 1);
     const MV<R> vin = swap ? A.in2 : A.in;
     const MV<R> vout = swap ? A.out2 : A.out;
-    // every global read of the block happens here, all in flight together
-    for (int e = threadIdx.x; e < E * E; e += blockDim.x) {
+    __syncthreads();  // shared memory of the previous tile of this block
+    // every global read of the tile happens here, all in flight together
+#pragma unroll
+    for (int e0 = 0; e0 < E * E; e0 += NT) {
+        const int e = e0 + threadIdx.x;
+        if (e >= E * E) break;
         const int i = ti0 + e % E, j = tj0 + e / E;
         const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
-        sa[e] = v ? A.acf(i, j, 0) : R(0);
+        const R av = v ? A.acf(i, j, 0) : R(0);
+        sa[e] = av;
+        sinv[e] = v ? mg_diag_inv<R, CELL>(L, i, j, av, A.facx, A.facy) : R(0);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             R val = R(0);
@@ -215,24 +236,26 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
     }
     __syncthreads();
     for (int s = 0; s < NSW; ++s) {
-        for (int e = threadIdx.x; e < E * E; e += blockDim.x) {
+#pragma unroll
+        for (int e0 = 0; e0 < E * E; e0 += NT) {
+            const int e = e0 + threadIdx.x;
+            if (e >= E * E) break;
             const int li = e % E, lj = e / E;
             if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1) continue;
             const int i = ti0 + li, j = tj0 + lj;
             if (((i + j + s) & 1) != 0) continue;
             if (i < L.vlo || i > L.vhi_i || j < L.vlo || j > L.vhi_j) continue;
-            const R a = sa[e];
+            const R inv = sinv[e];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const R* q = sp[c];
-                sp[c][e] = mg_gs<R, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], a, A.facx, A.facy);
+                sp[c][e] = mg_gs_inv<R, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], inv, A.facx, A.facy);
             }
         }
         __syncthreads();
     }
-    double bmax = 0, brhs = 0;
     if (RES) {
-        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+        for (int e = threadIdx.x; e < Q * Q; e += NT) {
             const int ri = e % Q, rj = e / Q;
             const int i = t0i - 1 + ri, j = t0j - 1 + rj;
             const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
@@ -254,7 +277,7 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
             }
         }
     }
-    for (int e = threadIdx.x; e < T * T; e += blockDim.x) {
+    for (int e = threadIdx.x; e < T * T; e += NT) {
         const int li = e % T, lj = e / T;
         const int i = t0i + li, j = t0j + lj;
         if (i > L.vhi_i || j > L.vhi_j) continue;
@@ -270,7 +293,7 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
         const int ci1 = min(C.vhi_i, (t0i + T - 1) >> 1), cj1 = min(C.vhi_j, (t0j + T - 1) >> 1);
         const int cw = ci1 - ci0 + 1, ch = cj1 - cj0 + 1;
         if (cw > 0 && ch > 0) {
-            for (int e = threadIdx.x; e < cw * ch; e += blockDim.x) {
+            for (int e = threadIdx.x; e < cw * ch; e += NT) {
                 const int I = ci0 + e % cw, J = cj0 + e / cw;
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
@@ -289,16 +312,35 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
             }
         }
     }
+}
+
+// max over the block of two per-thread values; the result is valid in thread 0
+__device__ __forceinline__ void block_max2(double& a, double& b) {
+    __shared__ double wa[32], wb[32];
+    for (int d = 16; d > 0; d >>= 1) {
+        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, d));
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, d));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) { wa[warp] = a; wb[warp] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { a = fmax(a, wa[w]); b = fmax(b, wb[w]); }
+}
+
+// one tile per block; with NORM the last block to finish takes the convergence decision of
+// solve_doit (:1340-1398) and sets the graph condition
+template <class R, bool CELL, int T, int INIT, bool RES, bool RESTR, int NORM, int NSW>
+__global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
+    HPQ_PDL_ENTRY();
+    extern __shared__ unsigned char smem_raw[];
+    double bmax = 0, brhs = 0;
+    const bool swap = A.pingpong && (A.ctl->mg_iter & 1);
+    mg_smooth_tile<R, CELL, T, INIT, RES, RESTR, NORM, NSW>(A, blockIdx.x, blockIdx.y, swap, smem_raw, bmax, brhs);
     if (NORM != MG_NORM_NONE) {
-        for (int d = 16; d > 0; d >>= 1) {
-            bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, d));
-            brhs = fmax(brhs, __shfl_xor_sync(0xffffffffu, brhs, d));
-        }
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) { wmax[warp] = bmax; wrhs[warp] = brhs; }
-        __syncthreads();
+        block_max2(bmax, brhs);
         if (threadIdx.x == 0) {
-            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { bmax = fmax(bmax, wmax[w]); brhs = fmax(brhs, wrhs[w]); }
             Ctl* ctl = A.ctl;
             atomic_max_nonneg(&ctl->mg_norm, bmax);
             if (NORM == MG_NORM_FIRST) atomic_max_nonneg(&ctl->mg_maxnorm, brhs);
@@ -331,7 +373,7 @@ struct MGCoarse {
 };
 
 template <class R, bool CELL>
-__device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* acf, const R* res, R* cor, int nsweeps, R facx,
+__device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* dinv, const R* res, R* cor, int nsweeps, R facx,
                                            R facy) {
     const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
     const int plane = L.w * L.h;
@@ -342,28 +384,30 @@ __device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* acf, const R
             const int id = j * L.w + i;
             const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
             const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-            const R a = acf[id];
+            const R inv = dinv[id];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 R* p = cor + c * plane;
-                p[id] = mg_gs<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], res[c * plane + id], a, facx, facy);
+                p[id] = mg_gs_inv<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], res[c * plane + id], inv, facx, facy);
             }
         }
         __syncthreads();
     }
 }
 
+// The global arrays are plain (not restrict/read-only) pointers: in the persistent solve other
+// blocks write them earlier in the same launch.
 template <class R, bool CELL>
-__global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restrict__ res_g, const R* __restrict__ acf_g,
-                                                    R* __restrict__ cor_g, R facx0, R facy0) {
-    HPQ_PDL_ENTRY();
-    extern __shared__ unsigned char smem_raw[];
+__device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
+                                                R facy0, unsigned char* smem_raw) {
+    __syncthreads();  // the block may have used the shared memory just before
     R* arena = reinterpret_cast<R*>(smem_raw);
-    // level l: cor (2n), res (2n), rescor (2n), acf (n)
+    // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
     auto cor = [&](int l) { return arena + M.off[l]; };
     auto res = [&](int l) { return arena + M.off[l] + 2 * (size_t)M.L[l].w * M.L[l].h; };
     auto rsc = [&](int l) { return arena + M.off[l] + 4 * (size_t)M.L[l].w * M.L[l].h; };
     auto acf = [&](int l) { return arena + M.off[l] + 6 * (size_t)M.L[l].w * M.L[l].h; };
+    auto dinv = [&](int l) { return arena + M.off[l] + 7 * (size_t)M.L[l].w * M.L[l].h; };
     {
         const int n0 = M.L[0].w * M.L[0].h;
         for (int k = threadIdx.x; k < n0; k += blockDim.x) {
@@ -373,7 +417,7 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
         }
         for (int l = 1; l < M.nl; ++l) {
             const int n = M.L[l].w * M.L[l].h;
-            for (int k = threadIdx.x; k < 7 * n; k += blockDim.x) cor(l)[k] = R(0);
+            for (int k = threadIdx.x; k < 8 * n; k += blockDim.x) cor(l)[k] = R(0);
         }
         __syncthreads();
         // coefficient hierarchy below sb
@@ -388,6 +432,18 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
             }
             __syncthreads();
         }
+        R fx = facx0, fy = facy0;
+        for (int l = 0; l < M.nl; ++l) {
+            const MGLev& L = M.L[l];
+            const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
+            for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
+                const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+                dinv(l)[j * L.w + i] = mg_diag_inv<R, CELL>(L, i, j, acf(l)[j * L.w + i], fx, fy);
+            }
+            fx *= R(0.25);
+            fy *= R(0.25);
+        }
+        __syncthreads();
     }
     R facx = facx0, facy = facy0;
     for (int l = 0; l < M.nl; ++l) {
@@ -396,10 +452,10 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
         for (int k = threadIdx.x; k < 2 * plane; k += blockDim.x) cor(l)[k] = R(0);
         __syncthreads();
         if (l == M.nl - 1) {
-            blk_sweeps<R, CELL>(L, acf(l), res(l), cor(l), 16, facx, facy);
+            blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 16, facx, facy);
             break;
         }
-        blk_sweeps<R, CELL>(L, acf(l), res(l), cor(l), 4, facx, facy);
+        blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
         const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
         for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
             const int i = L.vlo + k % vw, j = L.vlo + k / vw;
@@ -441,10 +497,18 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
             for (int c = 0; c < 2; ++c) cor(l)[c * plane + j * L.w + i] += mg_interp1<R, CELL>(crse, i, j, c);
         }
         __syncthreads();
-        blk_sweeps<R, CELL>(L, acf(l), res(l), cor(l), 4, facx, facy);
+        blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
     }
     const int n0 = 2 * M.L[0].w * M.L[0].h;
     for (int k = threadIdx.x; k < n0; k += blockDim.x) cor_g[k] = cor(0)[k];
+}
+
+template <class R, bool CELL>
+__global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restrict__ res_g, const R* __restrict__ acf_g,
+                                                    R* __restrict__ cor_g, R facx0, R facy0) {
+    HPQ_PDL_ENTRY();
+    extern __shared__ unsigned char smem_raw[];
+    mg_bottom_block<R, CELL>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw);
 }
 
 template <class R>
@@ -456,6 +520,445 @@ __global__ void k_mg_copy_out(MGLev L, MV<R> sol, MV<R> cor_even, MV<R> cor_odd,
         const int i = L.vlo + (int)(k % vw), j = L.vlo + (int)(k / vw);
         sol(i, j, 0) = cor(i, j, 0);
         sol(i, j, 1) = cor(i, j, 1);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent solve: the whole of solve_doit (first smoothing, every V-cycle, the convergence
+// decisions and the copy into the solution) in ONE cooperative launch. Each phase of the
+// multi-kernel V-cycle above becomes a loop over its tiles, separated by grid barriers; the
+// arithmetic per point is the same device code, so both forms give identical results.
+// ------------------------------------------------------------------------------------------
+constexpr int kMGMaxLevels = 16;
+constexpr long long kBarrierSpins = 1ll << 24;  // >= ~1 s of polling before giving up
+
+template <class R>
+struct MGSolveArgs {
+    int nl, sb;
+    MGLev lev[kMGMaxLevels];
+    R facx[kMGMaxLevels], facy[kMGMaxLevels];
+    MV<R> sol, rhs, a0;  // level-0 views into the slice arrays
+    R* acf[kMGMaxLevels];
+    R* res[kMGMaxLevels];
+    R* cor[kMGMaxLevels];
+    R* up[kMGMaxLevels];
+    MGCoarse coarse;
+    Ctl* ctl;
+    double tol_rel, tol_abs;
+    int maxiter;
+    // single precision: level-0 solution in FP64 and the FP32 right-hand side of the level-0
+    // correction equation, two slots each (by iteration parity)
+    double* x64[2];
+    R* r32[2];
+    // optional phase trace (HPQ_MG_TRACE): block 0 records the global timer after each barrier
+    unsigned long long* trace;
+};
+
+__device__ __forceinline__ unsigned long long tc_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier for a cooperative launch (all blocks co-resident). Bounded: a block that
+// polls longer than kBarrierSpins, or sees the error flag, sets the flag and returns false;
+// every block then leaves the kernel at its next barrier.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, int* err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 1;
+        volatile int* verr = err;
+        const unsigned int g = *gen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (*verr) break;
+                if (++it > kBarrierSpins) { atomicExch(err, 1); break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = (*verr == 0);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <class R>
+__device__ __forceinline__ MV<R> mg_own(R* const* v, const MGLev* lev, int l, int ncomp = 2) {
+    const size_t n = (size_t)lev[l].w * lev[l].h;
+    return {{v[l], ncomp > 1 ? v[l] + n : v[l]}, lev[l].w, 0};
+}
+
+// ------------------------------------------------------------------------------------------
+// Level 0 of the single-precision solve with FP64 iterative refinement. The solution x is held
+// in FP64; the colour sweeps run in FP32 on the correction d of the level-0 correction equation
+// (Lap - a) d = r, whose right-hand side r = rhs + a x - Lap(x) is recomputed in FP64 from x.
+// Because every smoothing step is affine and keeps the exact solution fixed, sweeping d from
+// zero (or from the coarse-grid correction) with right-hand side r and then adding d to x gives
+// the same iterates as sweeping x itself (the reference's form), up to FP32 rounding of d; the
+// residual, its norm and the stopping test are FP64, so the solve converges to tolerances that
+// an all-FP32 multigrid cannot reach.
+//   FIRST: x = initial guess (the slice arrays), r from x, 4 sweeps on d from zero.
+//   else:  x, r from the previous iteration, d from the interpolated coarse correction, 8 sweeps
+//          (the up-sweep of this V-cycle and the down-sweep of the next).
+// Both end with x += d, the new FP64 residual on the tile and its ring, its max norm, the FP32
+// residual of the tile (next right-hand side) and its restriction to level 1.
+// ------------------------------------------------------------------------------------------
+template <int T, int NSW>
+struct RefineSmem {
+    static constexpr int H = NSW + 2;
+    static constexpr int E = T + 2 * H;
+    static constexpr int Q = T + 2;
+    static constexpr size_t bytes() { return (size_t)2 * E * E * sizeof(double) + (size_t)(6 * E * E + 2 * Q * Q) * sizeof(float); }
+};
+
+template <bool CELL, bool FIRST, int NSW>
+__device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int slot_in, int bx, int by,
+                                               unsigned char* smem_raw, double& bmax, double& brhs) {
+    constexpr int T = 16, NT = 256;
+    using SM = RefineSmem<T, NSW>;
+    constexpr int H = SM::H, E = SM::E, Q = SM::Q;
+    double (*sx)[E * E] = reinterpret_cast<double (*)[E * E]>(smem_raw);                     // x, 2 comps
+    float* fbase = reinterpret_cast<float*>(smem_raw + 2 * E * E * sizeof(double));
+    float (*sd)[E * E] = reinterpret_cast<float (*)[E * E]>(fbase);                          // d
+    float (*srh)[E * E] = reinterpret_cast<float (*)[E * E]>(fbase + 2 * E * E);             // r (rhs of d)
+    float* sa = fbase + 4 * E * E;                                                            // coefficient
+    float* sinv = fbase + 5 * E * E;                                                          // 1 / diagonal
+    float (*sr)[Q * Q] = reinterpret_cast<float (*)[Q * Q]>(fbase + 6 * E * E);              // new residual
+    const MGLev& L = P.lev[0];
+    const float facx = P.facx[0], facy = P.facy[0];
+    const double dfx = (double)facx, dfy = (double)facy;
+    const int t0i = L.vlo + bx * T, t0j = L.vlo + by * T;
+    const int ti0 = t0i - H, tj0 = t0j - H;
+    const MV<float> crse = (P.sb == 1) ? MV<float>{{P.cor[1], P.cor[1] + (size_t)P.lev[1].w * P.lev[1].h}, P.lev[1].w, 0}
+                                       : MV<float>{{P.up[1], P.up[1] + (size_t)P.lev[1].w * P.lev[1].h}, P.lev[1].w, 0};
+    const size_t n0 = (size_t)L.w * L.h;
+    const double* xin = P.x64[slot_in];
+    const float* rin = P.r32[slot_in];
+    double* xout = P.x64[slot_in ^ (FIRST ? 0 : 1)];
+    float* rout = P.r32[slot_in ^ (FIRST ? 0 : 1)];
+    auto inside = [&](int i, int j) { return i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j; };
+    __syncthreads();
+#pragma unroll
+    for (int e0 = 0; e0 < E * E; e0 += NT) {
+        const int e = e0 + threadIdx.x;
+        if (e >= E * E) break;
+        const int i = ti0 + e % E, j = tj0 + e / E;
+        const bool v = inside(i, j);
+        const float av = v ? P.a0(i, j, 0) : 0.f;
+        sa[e] = av;
+        sinv[e] = v ? mg_diag_inv<float, CELL>(L, i, j, av, facx, facy) : 0.f;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (FIRST) {
+                sx[c][e] = v ? (double)P.sol(i, j, c) : 0.0;
+                sd[c][e] = 0.f;
+                srh[c][e] = v ? P.rhs(i, j, c) : 0.f;  // f for now, r below
+            } else {
+                const size_t id = (size_t)j * L.w + i;
+                sx[c][e] = v ? xin[c * n0 + id] : 0.0;
+                sd[c][e] = v ? mg_interp1<float, CELL>(crse, i, j, c) : 0.f;
+                srh[c][e] = v ? rin[c * n0 + id] : 0.f;
+            }
+        }
+    }
+    __syncthreads();
+    if (FIRST) {
+        // r = f + a x - Lap(x) in FP64 wherever the sweeps read it (all but the outer ring)
+        float rr[(E * E + NT - 1) / NT][2];
+#pragma unroll
+        for (int e0 = 0, q = 0; e0 < E * E; e0 += NT, ++q) {
+            const int e = e0 + threadIdx.x;
+            rr[q][0] = rr[q][1] = 0.f;
+            if (e >= E * E) break;
+            const int li = e % E, lj = e / E;
+            const int i = ti0 + li, j = tj0 + lj;
+            if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1 || !inside(i, j)) continue;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const double* x = sx[c];
+                const double r = (double)srh[c][e] + (double)sa[e] * x[e] -
+                                 mg_lap<double, CELL>(L, i, j, x[e], x[e - 1], x[e + 1], x[e - E], x[e + E], dfx, dfy);
+                rr[q][c] = (float)r;
+                if (li >= H && li < H + T && lj >= H && lj < H + T) brhs = fmax(brhs, fabs((double)srh[c][e]));
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e0 = 0, q = 0; e0 < E * E; e0 += NT, ++q) {
+            const int e = e0 + threadIdx.x;
+            if (e >= E * E) break;
+            srh[0][e] = rr[q][0];
+            srh[1][e] = rr[q][1];
+        }
+        __syncthreads();
+    }
+    for (int s = 0; s < NSW; ++s) {
+#pragma unroll
+        for (int e0 = 0; e0 < E * E; e0 += NT) {
+            const int e = e0 + threadIdx.x;
+            if (e >= E * E) break;
+            const int li = e % E, lj = e / E;
+            if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1) continue;
+            const int i = ti0 + li, j = tj0 + lj;
+            if (((i + j + s) & 1) != 0) continue;
+            if (!inside(i, j)) continue;
+            const float inv = sinv[e];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float* q = sd[c];
+                sd[c][e] = mg_gs_inv<float, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], inv, facx, facy);
+            }
+        }
+        __syncthreads();
+    }
+    // x += d where d is exact (distance >= NSW from the edge of the loaded region)
+#pragma unroll
+    for (int e0 = 0; e0 < E * E; e0 += NT) {
+        const int e = e0 + threadIdx.x;
+        if (e >= E * E) break;
+        const int li = e % E, lj = e / E;
+        if (li < NSW || lj < NSW || li >= E - NSW || lj >= E - NSW) continue;
+        sx[0][e] += (double)sd[0][e];
+        sx[1][e] += (double)sd[1][e];
+    }
+    __syncthreads();
+    // FP64 residual of the new x with the original right-hand side f on the tile and its ring
+    for (int e = threadIdx.x; e < Q * Q; e += NT) {
+        const int ri = e % Q, rj = e / Q;
+        const int i = t0i - 1 + ri, j = t0j - 1 + rj;
+        const bool v = inside(i, j);
+        const bool in_tile = ri >= 1 && ri <= T && rj >= 1 && rj <= T;
+        const int k = (rj + H - 1) * E + (ri + H - 1);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            float rf = 0.f;
+            if (v) {
+                const double* x = sx[c];
+                const double f = (double)P.rhs(i, j, c);
+                const double r = f + (double)sa[k] * x[k] -
+                                 mg_lap<double, CELL>(L, i, j, x[k], x[k - 1], x[k + 1], x[k - E], x[k + E], dfx, dfy);
+                if (in_tile) bmax = fmax(bmax, fabs(r));
+                rf = (float)r;
+            }
+            sr[c][e] = rf;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < T * T; e += NT) {
+        const int li = e % T, lj = e / T;
+        const int i = t0i + li, j = t0j + lj;
+        if (i > L.vhi_i || j > L.vhi_j) continue;
+        const int k = (lj + H) * E + (li + H);
+        const size_t id = (size_t)j * L.w + i;
+        const int kr = (lj + 1) * Q + (li + 1);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            xout[c * n0 + id] = sx[c][k];
+            rout[c * n0 + id] = sr[c][kr];
+        }
+    }
+    {
+        const MGLev& C = P.lev[1];
+        MV<float> cres{{P.res[1], P.res[1] + (size_t)C.w * C.h}, C.w, 0};
+        const int ci0 = max(C.vlo, (t0i + 1) >> 1), cj0 = max(C.vlo, (t0j + 1) >> 1);
+        const int ci1 = min(C.vhi_i, (t0i + T - 1) >> 1), cj1 = min(C.vhi_j, (t0j + T - 1) >> 1);
+        const int cw = ci1 - ci0 + 1, ch = cj1 - cj0 + 1;
+        if (cw > 0 && ch > 0) {
+            for (int e = threadIdx.x; e < cw * ch; e += NT) {
+                const int I = ci0 + e % cw, J = cj0 + e / cw;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    auto f = [&](int i, int j) -> float { return sr[c][(j - t0j + 1) * Q + (i - t0i + 1)]; };
+                    float v;
+                    if (CELL) {
+                        v = 0.25f * (f(2 * I, 2 * J) + f(2 * I + 1, 2 * J) + f(2 * I, 2 * J + 1) + f(2 * I + 1, 2 * J + 1));
+                    } else {
+                        v = (1.f / 16.f) * (f(2 * I - 1, 2 * J - 1) + 2.f * f(2 * I, 2 * J - 1) + f(2 * I + 1, 2 * J - 1) +
+                                            2.f * f(2 * I - 1, 2 * J) + 4.f * f(2 * I, 2 * J) + 2.f * f(2 * I + 1, 2 * J) +
+                                            f(2 * I - 1, 2 * J + 1) + 2.f * f(2 * I, 2 * J + 1) + f(2 * I + 1, 2 * J + 1));
+                    }
+                    cres(I, J, c) = v;
+                }
+            }
+        }
+    }
+}
+
+template <class R, bool CELL>
+__global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
+    HPQ_PDL_ENTRY();
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ int s_go;
+    __shared__ double s_target, s_maxn;
+    constexpr bool kRefine = std::is_same<R, float>::value;
+    Ctl* ctl = P.ctl;
+    unsigned int* bar = ctl->mgp_bar;
+    int* err = &ctl->mgp_bar_err;
+    const int nb = gridDim.x;
+    int nstamp = 0;
+    auto stamp = [&]() {
+        if (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && nstamp < 255) P.trace[1 + nstamp++] = tc_clock_ns();
+    };
+    stamp();
+    auto base = [&](int l) {
+        SmoothArgs<R> a{};
+        a.L = P.lev[l];
+        if (l + 1 < P.nl) a.Lc = P.lev[l + 1];
+        a.facx = P.facx[l];
+        a.facy = P.facy[l];
+        a.ctl = ctl;
+        return a;
+    };
+    auto ntiles = [&](int l, int& ntx) {
+        const MGLev& L = P.lev[l];
+        ntx = (L.vhi_i - L.vlo + 16) / 16;
+        return ntx * ((L.vhi_j - L.vlo + 16) / 16);
+    };
+    // coefficient of level l from level l-1 (average_down_acoef), grid-stride
+    auto restrict_acf = [&](int l) {
+        const MGLev& C = P.lev[l];
+        MV<R> fine = (l == 1) ? P.a0 : mg_own<R>(P.acf, P.lev, l - 1, 1);
+        MV<R> crse = mg_own<R>(P.acf, P.lev, l, 1);
+        const int vw = C.vhi_i - C.vlo + 1, vh = C.vhi_j - C.vlo + 1;
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < vw * vh; k += nb * blockDim.x) {
+            const int i = C.vlo + k % vw, j = C.vlo + k / vw;
+            crse(i, j, 0) = mg_restrict1<R, CELL>(fine, i, j, 0);
+        }
+    };
+    double bmax = 0, brhs = 0;
+    // ---- first smoothing of level 0 (residual, restriction, norms) and the level-1 coefficient
+    {
+        SmoothArgs<R> a = base(0);
+        a.out = mg_own<R>(P.cor, P.lev, 0); a.rhs = P.rhs; a.acf = P.a0; a.in = P.sol;
+        a.crse_res = mg_own<R>(P.res, P.lev, 1);
+        int ntx;
+        const int nt = ntiles(0, ntx);
+        for (int t = blockIdx.x; t < nt; t += nb) {
+            if constexpr (kRefine)
+                mg_refine_tile<CELL, true, 4>(P, 0, t % ntx, t / ntx, smem_raw, bmax, brhs);
+            else
+                mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, true, true, MG_NORM_FIRST, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+        }
+        restrict_acf(1);
+        block_max2(bmax, brhs);
+        if (threadIdx.x == 0) {
+            atomic_max_nonneg(&ctl->mgp_norm[0], bmax);
+            atomic_max_nonneg(&ctl->mgp_rhsnorm, brhs);
+        }
+    }
+    if (!grid_barrier(bar, err)) return;
+    stamp();
+    if (threadIdx.x == 0) {
+        const double r0 = atomic_read(&ctl->mgp_norm[0]), m0 = atomic_read(&ctl->mgp_rhsnorm);
+        s_maxn = (m0 >= r0) ? m0 : r0;
+        s_target = fmax(P.tol_abs, fmax(P.tol_rel, 1.e-16) * s_maxn);
+        s_go = !(r0 <= s_target);
+        if (blockIdx.x == 0) { ctl->mg_target = s_target; ctl->mg_maxnorm = s_maxn; }
+    }
+    __syncthreads();
+    int it = 0;
+    while (s_go) {
+        // down: levels 1 .. sb-1 (zero initial guess), residual restricted to the next level
+        for (int l = 1; l < P.sb; ++l) {
+            SmoothArgs<R> a = base(l);
+            a.out = mg_own<R>(P.cor, P.lev, l); a.rhs = mg_own<R>(P.res, P.lev, l);
+            a.acf = mg_own<R>(P.acf, P.lev, l, 1); a.crse_res = mg_own<R>(P.res, P.lev, l + 1);
+            int ntx;
+            const int nt = ntiles(l, ntx);
+            for (int t = blockIdx.x; t < nt; t += nb)
+                mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+            if (it == 0) restrict_acf(l + 1);
+            if (!grid_barrier(bar, err)) return;
+            stamp();
+        }
+        // levels sb .. nl-1 in block 0
+        if (blockIdx.x == 0)
+            mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw);
+        if (!grid_barrier(bar, err)) return;
+        stamp();
+        // up: levels sb-1 .. 1, interpolation of the coarser correction + 4 sweeps
+        for (int l = P.sb - 1; l >= 1; --l) {
+            SmoothArgs<R> a = base(l);
+            a.out = mg_own<R>(P.up, P.lev, l); a.rhs = mg_own<R>(P.res, P.lev, l);
+            a.acf = mg_own<R>(P.acf, P.lev, l, 1); a.in = mg_own<R>(P.cor, P.lev, l);
+            a.crse_in = (l + 1 == P.sb) ? mg_own<R>(P.cor, P.lev, P.sb) : mg_own<R>(P.up, P.lev, l + 1);
+            int ntx;
+            const int nt = ntiles(l, ntx);
+            for (int t = blockIdx.x; t < nt; t += nb)
+                mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+            if (!grid_barrier(bar, err)) return;
+            stamp();
+        }
+        // level 0: up-sweep and the next down-sweep (8 colour sweeps), residual, restriction,
+        // norm; the solution alternates between cor[0] and up[0] by iteration parity
+        {
+            SmoothArgs<R> a = base(0);
+            a.in = mg_own<R>(P.cor, P.lev, 0); a.out = mg_own<R>(P.up, P.lev, 0);
+            a.in2 = mg_own<R>(P.up, P.lev, 0); a.out2 = mg_own<R>(P.cor, P.lev, 0);
+            a.rhs = P.rhs; a.acf = P.a0;
+            a.crse_in = (P.sb == 1) ? mg_own<R>(P.cor, P.lev, 1) : mg_own<R>(P.up, P.lev, 1);
+            a.crse_res = mg_own<R>(P.res, P.lev, 1);
+            int ntx;
+            const int nt = ntiles(0, ntx);
+            bmax = 0;
+            for (int t = blockIdx.x; t < nt; t += nb) {
+                if constexpr (kRefine)
+                    mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
+                else
+                    mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
+            }
+            block_max2(bmax, brhs);
+            if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
+        }
+        if (!grid_barrier(bar, err)) return;
+        stamp();
+        ++it;
+        if (threadIdx.x == 0) {
+            const double norm = atomic_read(&ctl->mgp_norm[it & 1]);
+            int go = 1, status = 0;
+            if (norm <= s_target) go = 0;
+            else if (norm > 1.e20 * s_maxn) { go = 0; status = 2; }
+            else if (it >= P.maxiter) { go = 0; status = 1; }
+            s_go = go;
+            if (blockIdx.x == 0) {
+                ctl->mgp_norm[(it + 1) & 1] = 0;  // read by every block at the previous decision
+                ctl->mg_total_iters += 1;
+                if (status && !ctl->mg_status) ctl->mg_status = status;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->mg_iter = it;
+        ctl->mg_go = 0;
+        if (P.trace) P.trace[0] = nstamp;
+    }
+    // solution: the last level-0 output (cor[0] after an even number of cycles, else up[0]; the
+    // FP64 solution slot it & 1 in single precision)
+    const MV<R> fin = (it & 1) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
+    const MGLev& L = P.lev[0];
+    const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
+    const size_t n0 = (size_t)L.w * L.h;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < vw * vh; k += nb * blockDim.x) {
+        const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+        if constexpr (kRefine) {
+            const double* x = P.x64[it & 1];
+            P.sol(i, j, 0) = (R)x[(size_t)j * L.w + i];
+            P.sol(i, j, 1) = (R)x[n0 + (size_t)j * L.w + i];
+        } else {
+            P.sol(i, j, 0) = fin(i, j, 0);
+            P.sol(i, j, 1) = fin(i, j, 1);
+        }
     }
 }
 
@@ -494,7 +997,7 @@ public:
         // single-block levels: from the first level (>= 1) whose hierarchy fits 160 KB of shared memory
         auto smem_from = [&](int s0) {
             size_t tot = 0;
-            for (int l = s0; l < nl; ++l) tot += 7 * (size_t)lev[l].w * lev[l].h;
+            for (int l = s0; l < nl; ++l) tot += 8 * (size_t)lev[l].w * lev[l].h;
             return tot * sizeof(R);
         };
         sb = nl - 1;
@@ -506,7 +1009,7 @@ public:
         for (int l = sb; l < nl; ++l) {
             coarse.L[l - sb] = lev[l];
             coarse.off[l - sb] = off;
-            off += 7 * (size_t)lev[l].w * lev[l].h;
+            off += 8 * (size_t)lev[l].w * lev[l].h;
         }
         acf.assign(nl, nullptr); res.assign(nl, nullptr); cor.assign(nl, nullptr); up.assign(nl, nullptr);
         for (int l = 0; l < nl; ++l) {
@@ -526,6 +1029,105 @@ public:
         HPQ_CUDA(cudaMemset(counter, 0, sizeof(unsigned int)));
         if (cell) HPQ_CUDA(cudaFuncSetAttribute(k_mg_bottom<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bottom_smem));
         else HPQ_CUDA(cudaFuncSetAttribute(k_mg_bottom<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bottom_smem));
+        if (cell) setup_persistent<true>(); else setup_persistent<false>();
+    }
+
+    // persistent solve: one cooperative launch with as many co-resident blocks as there are
+    // level-0 tiles, at most (HPQ_MG=kernels in the environment selects the multi-kernel form)
+    bool coop_ok = false;
+    int coop_blocks = 0;
+    size_t coop_smem = 0;
+    double* x64[2] = {nullptr, nullptr};  // single precision: FP64 level-0 solution (refinement)
+    R* r32[2] = {nullptr, nullptr};
+    unsigned long long* trace = nullptr;  // HPQ_MG_TRACE=1: phase timestamps of the last solve
+
+    // Prints the phase durations of the last persistent solve (microseconds) to stderr.
+    void print_trace() const {
+        if (!trace) return;
+        std::vector<unsigned long long> h(256);
+        if (cudaMemcpy(h.data(), trace, 256 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+        const int n = (int)std::min<unsigned long long>(h[0], 255);
+        std::string line = "hpmg phases (us):";
+        for (int k = 1; k < n; ++k) {
+            char buf[32];
+            snprintf(buf, sizeof(buf), " %.2f", (double)(h[1 + k] - h[k]) / 1000.0);
+            line += buf;
+        }
+        fprintf(stderr, "%s\n", line.c_str());
+    }
+
+    template <bool CELL>
+    void setup_persistent() {
+        coop_ok = false;
+        const char* e = getenv("HPQ_MG");
+        if (e && std::string(e) == "kernels") return;
+        if (nl > kMGMaxLevels) return;
+        coop_smem = std::max({SmoothSmem<16, 8>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
+        if (const char* t = getenv("HPQ_MG_TRACE")) {
+            if (t[0] == '1') {
+                HPQ_CUDA(cudaMalloc(&trace, 256 * sizeof(unsigned long long)));
+                HPQ_CUDA(cudaMemset(trace, 0, 256 * sizeof(unsigned long long)));
+            }
+        }
+        if (std::is_same<R, float>::value) {
+            coop_smem = std::max({coop_smem, RefineSmem<16, 8>::bytes(), RefineSmem<16, 4>::bytes()});
+            const size_t n0 = (size_t)lev[0].w * lev[0].h;
+            for (int k = 0; k < 2; ++k) {
+                HPQ_CUDA(cudaMalloc(&x64[k], 2 * n0 * sizeof(double)));
+                HPQ_CUDA(cudaMalloc(&r32[k], 2 * n0 * sizeof(R)));
+                HPQ_CUDA(cudaMemset(x64[k], 0, 2 * n0 * sizeof(double)));
+                HPQ_CUDA(cudaMemset(r32[k], 0, 2 * n0 * sizeof(R)));
+            }
+        }
+        auto kern = k_mg_solve<R, CELL>;
+        HPQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem));
+        int dev = 0, sms = 0, coop = 0, per = 0;
+        HPQ_CUDA(cudaGetDevice(&dev));
+        HPQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        HPQ_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, coop_smem));
+        const MGLev& L = lev[0];
+        const int nt0 = ((L.vhi_i - L.vlo + 16) / 16) * ((L.vhi_j - L.vlo + 16) / 16);
+        coop_blocks = std::min(per * sms, nt0);
+        coop_ok = coop && per > 0 && coop_blocks > 0;
+    }
+
+    template <bool CELL>
+    void solve_persistent(cudaStream_t st, const Slab<R>& S, Ctl* ctl, double tol_rel, double tol_abs, int maxiter) {
+        MGSolveArgs<R> P{};
+        P.nl = nl;
+        P.sb = sb;
+        for (int l = 0; l < nl; ++l) {
+            P.lev[l] = lev[l];
+            P.facx[l] = (R)fac(l, dx);
+            P.facy[l] = (R)fac(l, dy);
+            P.acf[l] = acf[l]; P.res[l] = res[l]; P.cor[l] = cor[l]; P.up[l] = up[l];
+        }
+        P.sol = slab_view(S, C_BX, C_BY);
+        P.rhs = slab_view(S, C_SY, C_SX);
+        P.a0 = slab_view(S, C_CHI, C_CHI);
+        P.coarse = coarse;
+        P.ctl = ctl;
+        P.tol_rel = tol_rel; P.tol_abs = tol_abs; P.maxiter = maxiter;
+        P.x64[0] = x64[0]; P.x64[1] = x64[1];
+        P.r32[0] = r32[0]; P.r32[1] = r32[1];
+        P.trace = trace;
+        // norms and barrier state; the timeout flag stays set until the step ends, so that after
+        // a timeout the remaining solves of the step leave at their first barrier
+        static_assert(offsetof(Ctl, mgp_bar_err) - offsetof(Ctl, mgp_rhsnorm) == 32, "Ctl layout");
+        HPQ_CUDA(cudaMemsetAsync(&ctl->mgp_rhsnorm, 0, 32, st));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(coop_blocks);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = coop_smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        HPQ_CUDA(cudaLaunchKernelEx(&cfg, k_mg_solve<R, CELL>, P));
+        HPQ_LAUNCH_CHECK();
     }
     void release() {
         for (int l = 0; l < nl; ++l) {
@@ -534,6 +1136,13 @@ public:
         }
         if (counter) cudaFree(counter);
         counter = nullptr;
+        if (trace) cudaFree(trace);
+        trace = nullptr;
+        for (int k = 0; k < 2; ++k) {
+            if (x64[k]) cudaFree(x64[k]);
+            if (r32[k]) cudaFree(r32[k]);
+            x64[k] = nullptr; r32[k] = nullptr;
+        }
         lev.clear(); nl = 0;
     }
     MV<R> own(std::vector<R*>& v, int l, int ncomp = 2) const {

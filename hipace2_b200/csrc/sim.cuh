@@ -685,6 +685,9 @@ public:
         if (ctl_h->mg_status && !st_host.mg_status) st_host.mg_status = ctl_h->mg_status;
         st_host.slices += nz;
         for (auto& p : pl) st_host.plasma_pushes += p.n * nz;
+        if (cfg.explicit_solver) mg.print_trace();
+        if (ctl_h->tc_err) throw CudaError("tensor-core DST: a pipeline wait timed out (code " + std::to_string(ctl_h->tc_err) + ")");
+        if (ctl_h->mgp_bar_err) throw CudaError("hpmg: grid barrier of the persistent multigrid solve timed out");
         if (st_host.mg_status == 1) throw CudaError("hpmg: failed to converge within the iteration limit");
         if (st_host.mg_status == 2) throw CudaError("hpmg: diverged");
     }
@@ -733,6 +736,11 @@ public:
     }
     template <bool CELL>
     void mg_solve_t() {
+        if (mg.coop_ok) {
+            // the whole solve, iterations and decisions included, is one cooperative kernel
+            mg.template solve_persistent<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters);
+            return;
+        }
         if (capturing) {
             // inside the slice graph: a conditional WHILE node repeats the V-cycle body for as
             // long as the device-side decision (k_mg_init_decide / k_mg_decide) says so

@@ -162,6 +162,32 @@ MIXED_BOUNDS_BLOWOUT = {"Ez": 5e-3, "Psi": 1e-3, "jz_beam": 1e-5, "Bx": 1e-2}
 
 
 @pytest.mark.parametrize("regime", ["weak", "blowout"])
+def test_persistent_multigrid_equals_multi_kernel_form():
+    """One cooperative launch per multigrid solve vs one launch per V-cycle phase (HPQ_MG=kernels)."""
+    from cases import EXPLICIT_FFT, EXPLICIT_MOVING
+    for text in (EXPLICIT_FFT, EXPLICIT_MOVING):
+        out, cycles = [], []
+        for mode in ("persistent", "kernels"):
+            old = os.environ.pop("HPQ_MG", None)
+            if mode == "kernels":
+                os.environ["HPQ_MG"] = "kernels"
+            try:
+                g = hp.Hipace(text, graphs=True)
+                g.init_data()
+            finally:
+                os.environ.pop("HPQ_MG", None)
+                if old is not None:
+                    os.environ["HPQ_MG"] = old
+            g.set_diag(["Bx", "By", "Ez"])
+            for s in range(2):
+                g.step(s)
+            out.append([g.get_diag(k) for k in ("Bx", "By", "Ez")])
+            cycles.append(g.counters()["mg_vcycles"])
+        assert cycles[0] > 0 and abs(cycles[0] - cycles[1]) <= max(1, cycles[1] // 100), cycles
+        for a, b in zip(*out):
+            assert rel_l2(a, b) <= 1e-10
+
+
 def test_mixed_precision_error_vs_oracle(regime):
     """Mixed path vs the FP64 oracle on the 63x63x48 explicit case (FFT Poisson path).
 
