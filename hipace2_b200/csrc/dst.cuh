@@ -12,8 +12,11 @@
 // are both plain row-major GEMMs on the same buffer.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fftdst.cuh"
+#include "tcdst.cuh"
 
 namespace hpq {
 
@@ -105,18 +108,39 @@ class PoissonDST {
 public:
     int nx = 0, ny = 0, nrhs_max = 0;
     R *sx = nullptr, *sy = nullptr, *eig = nullptr, *stage = nullptr, *work = nullptr;
-    bool use_fft = false;
+    R* stage_simt = nullptr;  // the stage of the SIMT-GEMM and FFT forms
+    bool use_fft = false, use_tc = false;
     FastDST<R> fast;
+    TcDST tcd;  // tensor-core form, single precision only
+    double dx_ = 0, dy_ = 0;
     // stage element (rhs k, row j, column i) is stage[k * sk + j * sj + i]
     int sk = 0, sj = 0;
     void set_mode(bool fft) {
+        use_tc = false;
+        stage = stage_simt;
         use_fft = fft && FastDST<R>::supported(nx, ny);
         if (use_fft) { sk = nx * ny; sj = nx; }
         else { sk = nx; sj = nrhs_max * nx; }
     }
+    // tensor-core sine GEMMs (TF32x3) for the single-precision path; err receives the kernels'
+    // error code
+    void set_tensor_mode(int* err) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (!TcDST::supported(nx, ny)) return;
+            if (!tcd.stage) tcd.init(nx, ny, dx_, dy_, nrhs_max, err);
+            use_tc = true;
+            use_fft = false;
+            stage = tcd.stage;
+            sk = ny * tcd.px;
+            sj = tcd.px;
+        } else {
+            (void)err;
+        }
+    }
 
     void init(int nx_, int ny_, double dx, double dy, int nrhs_max_) {
         nx = nx_; ny = ny_; nrhs_max = nrhs_max_;
+        dx_ = dx; dy_ = dy;
         std::vector<R> hx((size_t)nx * nx), hy((size_t)ny * ny), he((size_t)nx * ny);
         const double pi = 3.14159265358979323846;
         for (int i = 0; i < nx; ++i)
@@ -134,7 +158,8 @@ public:
         HPQ_CUDA(cudaMalloc(&sx, hx.size() * sizeof(R)));
         HPQ_CUDA(cudaMalloc(&sy, hy.size() * sizeof(R)));
         HPQ_CUDA(cudaMalloc(&eig, he.size() * sizeof(R)));
-        HPQ_CUDA(cudaMalloc(&stage, (size_t)nx * ny * nrhs_max * sizeof(R)));
+        HPQ_CUDA(cudaMalloc(&stage_simt, (size_t)nx * ny * nrhs_max * sizeof(R)));
+        stage = stage_simt;
         HPQ_CUDA(cudaMalloc(&work, (size_t)nx * ny * nrhs_max * sizeof(R)));
         HPQ_CUDA(cudaMemcpy(sx, hx.data(), hx.size() * sizeof(R), cudaMemcpyHostToDevice));
         HPQ_CUDA(cudaMemcpy(sy, hy.data(), hy.size() * sizeof(R), cudaMemcpyHostToDevice));
@@ -143,9 +168,10 @@ public:
         set_mode(true);
     }
     void release() {
-        for (R* p : {sx, sy, eig, stage, work}) if (p) cudaFree(p);
-        sx = sy = eig = stage = work = nullptr;
+        for (R* p : {sx, sy, eig, stage_simt, work}) if (p) cudaFree(p);
+        sx = sy = eig = stage = stage_simt = work = nullptr;
         fast.release();
+        tcd.release();
     }
 
     template <class Epi>
@@ -159,6 +185,12 @@ public:
     // Solve for `nrhs` right-hand sides already in `stage` ([j][k][i]); results go to field
     // components comps[k] of the slab (interior only).
     void solve(cudaStream_t st, int nrhs, R* base, size_t cstride, int pitch, const int* comps) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (use_tc) {
+                tcd.solve(st, nrhs, base, cstride, pitch, comps);
+                return;
+            }
+        }
         if (use_fft) {
             fast.solve(st, nrhs, stage, work, eig, base, cstride, pitch, comps);
             return;

@@ -54,6 +54,12 @@ struct BeamDev {
 template <class R>
 struct PlasmaDev {
     R *x, *y, *w, *ux, *uy, *psi, *xp, *yp, *uxh, *uyh, *psih;
+    // Single precision only: the particle's lattice point in cell units (exact in FP32, e.g.
+    // 130.5). x, y, xp, yp then hold the displacement from that point and psi, psih hold psi - 1,
+    // so the cell fraction that the shape factors use and the deviation of psi from 1 keep full
+    // FP32 precision instead of the precision of |x| and of 1. Null in double precision, where
+    // x, y and psi are stored as they are.
+    const float *ru, *rv;
     uint8_t* valid;
     long long n;
     double charge, mass, qsa_max;
@@ -133,11 +139,13 @@ __global__ void k_plasma_reset(PlasmaDev<R> P, const double* __restrict__ x0, co
         double v[3] = {x, y, c_t};
         const double w = density.eval(v) * scale;
         const double psi = sqrt(1. + ux0 * ux0 + uy0 * uy0 + uz0 * uz0) - uz0;
-        P.x[i] = (R)x; P.y[i] = (R)y; P.xp[i] = (R)x; P.yp[i] = (R)y;
+        const R xs = P.ru ? R(0) : (R)x, ys = P.ru ? R(0) : (R)y;
+        P.x[i] = xs; P.y[i] = ys; P.xp[i] = xs; P.yp[i] = ys;
         P.w[i] = (R)w;
         P.ux[i] = (R)(ux0 * clight); P.uy[i] = (R)(uy0 * clight);
         P.uxh[i] = (R)(ux0 * clight); P.uyh[i] = (R)(uy0 * clight);
-        P.psi[i] = (R)psi; P.psih[i] = (R)psi;
+        const R psis = P.ru ? (R)(psi - 1.0) : (R)psi;
+        P.psi[i] = psis; P.psih[i] = psis;
         P.valid[i] = 1;
     }
 }
@@ -157,6 +165,27 @@ __device__ __forceinline__ void addc(R* base, int pitch, int i, int j, R v) {
     atomicAdd(base + (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc), v);
 }
 
+// Cell-unit coordinate of a plasma position along one axis as base + t: with a reference lattice
+// coordinate (single precision) t = frac(u0) + x * dxi is a small number and the integer part
+// goes to `base`; without one, base = 0 and t = (x - off) * dxi. Clamped to [-1, n] like clamp_mid.
+template <class R>
+__device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R off, R dxi, int n, int& base) {
+    if (ref == nullptr) {
+        base = 0;
+        return clamp_mid<R>((x - off) * dxi, n);
+    }
+    const float u0 = ref[ip];
+    const float fb = floorf(u0);
+    const R t = (R)(u0 - fb) + x * dxi;
+    const R tot = (R)fb + t;
+    if (!(tot >= R(-1) && tot <= R(n))) {
+        base = 0;
+        return clamp_mid<R>(tot, n);
+    }
+    base = (int)fb;
+    return t;
+}
+
 template <class R>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
                                                         const int* gate) {
@@ -170,14 +199,21 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
     const R qsa = (R)P.qsa_max;
     for (long long ip = gtid(); ip < P.n; ip += gstride()) {
         if (!P.valid[ip]) continue;
-        const R psi_inv = R(1) / P.psi[ip];
+        const R psis = P.psi[ip];
+        const R psi_inv = P.ru ? R(1) / (R(1) + psis) : R(1) / psis;
         const R vx_c = P.ux[ip] * psi_inv;
         const R vy_c = P.uy[ip] * psi_inv;
         const R q_invvol = charge_invvol * P.w[ip];
-        const R xmid = clamp_mid<R>((P.x[ip] - xoff) * dxi, g.nx);
-        const R ymid = clamp_mid<R>((P.y[ip] - yoff) * dyi, g.ny);
+        int bx, by;
+        const R xmid = plasma_mid<R>(P.ru, ip, P.x[ip], xoff, dxi, g.nx, bx);
+        const R ymid = plasma_mid<R>(P.rv, ip, P.y[ip], yoff, dyi, g.ny, by);
         const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
                                       vy_c * vy_c * clightinv * clightinv + R(1));
+        // gamma/psi - 1; with psi - 1 stored, (1/psi)^2 - 1 = -(psi - 1)(psi + 1)/psi^2 avoids the
+        // cancellation of two numbers close to 1
+        const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                        vy_c * vy_c * clightinv * clightinv)
+                            : gamma_psi - R(1);
         if (gamma_psi < R(0) || gamma_psi > qsa || psi_inv < R(0)) {
             P.w[ip] = R(0);
             P.valid[ip] = 0;
@@ -185,7 +221,10 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
         }
         Sh<R> sx[3], sy[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k); }
+        for (int k = 0; k < 3; ++k) {
+            sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k);
+            sx[k].cell += bx; sy[k].cell += by;
+        }
 #pragma unroll
         for (int iy = 0; iy < 3; ++iy)
 #pragma unroll
@@ -193,7 +232,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 const R cd = q_invvol * sx[ix].s * sy[iy].s;
                 if (o.jx) { addc(o.jx, o.pitch, i, j, cd * vx_c); addc(o.jy, o.pitch, i, j, cd * vy_c); }
-                if (o.jz) addc(o.jz, o.pitch, i, j, cd * (gamma_psi - R(1)) * clight);
+                if (o.jz) addc(o.jz, o.pitch, i, j, cd * gpm1 * clight);
                 if (o.rho) addc(o.rho, o.pitch, i, j, cd * gamma_psi);
                 if (o.chi) addc(o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
                 if (o.rhomjz) addc(o.rhomjz, o.pitch, i, j, cd);
@@ -218,15 +257,25 @@ __global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R
     constexpr int NS = 3 + DT;
     for (long long ip = gtid(); ip < P.n; ip += gstride()) {
         if (!P.valid[ip]) continue;
-        const R psi_inv = R(1) / P.psi[ip];
+        const R psis = P.psi[ip];
+        const R psi_inv = P.ru ? R(1) / (R(1) + psis) : R(1) / psis;
         const R vx = P.ux[ip] * psi_inv * clight_inv;
         const R vy = P.uy[ip] * psi_inv * clight_inv;
         const R cdm = charge_invvol_mu0 * P.w[ip];
-        const R xmid = clamp_mid<R>((P.x[ip] - xoff) * dxi, g.nx), ymid = clamp_mid<R>((P.y[ip] - yoff) * dyi, g.ny);
+        int bx, by;
+        const R xmid = plasma_mid<R>(P.ru, ip, P.x[ip], xoff, dxi, g.nx, bx);
+        const R ymid = plasma_mid<R>(P.rv, ip, P.y[ip], yoff, dyi, g.ny, by);
         const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx * vx + vy * vy + R(1));
+        // gamma/psi - 1 - v_y^2 and gamma/psi - 1 - v_x^2 (see k_plasma_deposit for psi - 1)
+        const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx * vx + vy * vy) : R(0);
+        const R gmy = P.ru ? gpm1 - vy * vy : gamma_psi - vy * vy - R(1);
+        const R gmx = P.ru ? gpm1 - vx * vx : gamma_psi - vx * vx - R(1);
         DSh<R> sx[NS], sy[NS];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) { sx[k] = dshape2<R, DT>(xmid, k); sy[k] = dshape2<R, DT>(ymid, k); }
+        for (int k = 0; k < NS; ++k) {
+            sx[k] = dshape2<R, DT>(xmid, k); sy[k] = dshape2<R, DT>(ymid, k);
+            sx[k].cell += bx; sy[k].cell += by;
+        }
 #pragma unroll
         for (int iy = 0; iy < NS; ++iy)
 #pragma unroll
@@ -236,9 +285,9 @@ __global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R
                 const R Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = Ex(i, j), EypBx_v = Ey(i, j);
                 const R sxs = sx[ix].s, sys = sy[iy].s, sxd = sx[ix].ds, syd = sy[iy].ds;
                 const R vsy = cdm * (-sxs * sys * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * clight_inv) * q_mass_ratio * psi_inv +
-                                     (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * (gamma_psi - vy * vy - R(1))) * a_clight);
+                                     (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * gmy) * a_clight);
                 const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
-                                     (+sxd * sys * dxi * (gamma_psi - vx * vx - R(1)) + sxs * syd * dyi * (-vx * vy)) * a_clight);
+                                     (+sxd * sys * dxi * gmx + sxs * syd * dyi * (-vx * vy)) * a_clight);
                 addc(Sy, S.pitch, i, j, vsy);
                 addc(Sx, S.pitch, i, j, vsx);
             }
@@ -248,15 +297,18 @@ __global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R
 // ------------------------------------------------------------------------------------------
 // Field gather (FieldGather.H:45-96, derivative type 1, 4x4 stencil)
 // ------------------------------------------------------------------------------------------
+// x, y in cell units, as base + fraction (bx, by integer)
 template <class R, class T>
-__device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T yp, T& ExmBy, T& EypBx, T& Ez,
-                                       T& Bx, T& By, T& Bz) {
+__device__ __forceinline__ void gather_mid(const Slab<R>& S, const Geo& g, T x, T y, int bx, int by, T& ExmBy,
+                                           T& EypBx, T& Ez, T& Bx, T& By, T& Bz) {
     const T dxi = (T)g.dxi[0], dyi = (T)g.dxi[1];
-    const T x = clamp_mid<T>((xp - (T)g.xoff) * dxi, g.nx), y = clamp_mid<T>((yp - (T)g.yoff) * dyi, g.ny);
     const F2<R> Psi = S.c(C_PSI), FEz = S.c(C_EZ), FBx = S.c(C_BX), FBy = S.c(C_BY), FBz = S.c(C_BZ);
     DSh<T> sx[4], sy[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) { sx[k] = dshape_nodal2<T>(x, k); sy[k] = dshape_nodal2<T>(y, k); }
+    for (int k = 0; k < 4; ++k) {
+        sx[k] = dshape_nodal2<T>(x, k); sy[k] = dshape_nodal2<T>(y, k);
+        sx[k].cell += bx; sy[k].cell += by;
+    }
 #pragma unroll
     for (int iy = 0; iy < 4; iy++)
 #pragma unroll
@@ -271,6 +323,13 @@ __device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T y
             By += s * (T)FBy(i, j);
             Bz += s * (T)FBz(i, j);
         }
+}
+
+template <class R, class T>
+__device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T yp, T& ExmBy, T& EypBx, T& Ez,
+                                       T& Bx, T& By, T& Bz) {
+    const T x = clamp_mid<T>((xp - (T)g.xoff) * (T)g.dxi[0], g.nx), y = clamp_mid<T>((yp - (T)g.yoff) * (T)g.dxi[1], g.ny);
+    gather_mid<R, T>(S, g, x, y, 0, 0, ExmBy, EypBx, Ez, Bx, By, Bz);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -317,11 +376,17 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
         for (int isc = 0; isc < nsubc; ++isc) {
             R xp = P.xp[ip], yp = P.yp[ip];
             R Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
-            gather<R, R>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
+            {
+                int bx, by;
+                const R xm = plasma_mid<R>(P.ru, ip, xp, (R)g.xoff, (R)g.dxi[0], g.nx, bx);
+                const R ym = plasma_mid<R>(P.rv, ip, yp, (R)g.yoff, (R)g.dxi[1], g.ny, by);
+                gather_mid<R, R>(S, g, xm, ym, bx, by, Ex, Ey, Ez, Bx, By, Bz);
+            }
             Bx *= clight; By *= clight;
             R ux = P.uxh[ip], uy = P.uyh[ip], psi = P.psih[ip];
+            const R pb = P.ru ? R(1) : R(0);  // psi = pb + stored value
             auto substep = [&]() {
-                const R pi = R(1) / psi;
+                const R pi = R(1) / (pb + psi);
                 R d0, d1, d2;
                 plasma_rhs<R>(ux, uy, pi, Ex, Ey, Ez, Bx, By, Bz, ci, qmc, d0, d1, d2);
                 Du<R> e0, e1, e2;
@@ -332,9 +397,17 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
             };
 #pragma unroll
             for (int k = 0; k < 4; ++k) substep();
-            xp += dzs * ci * (ux * (R(1) / psi));
-            yp += dzs * ci * (uy * (R(1) / psi));
-            if (!enforce_bc<R>(g, xp, yp, ux, uy)) { P.w[ip] = R(0); P.valid[ip] = 0; break; }
+            xp += dzs * ci * (ux * (R(1) / (pb + psi)));
+            yp += dzs * ci * (uy * (R(1) / (pb + psi)));
+            if (P.ru) {
+                // displacements: the boundary test needs the absolute position
+                const R x0 = (R)(g.xoff + (double)P.ru[ip] * g.dx[0]), y0 = (R)(g.yoff + (double)P.rv[ip] * g.dx[1]);
+                R xa = x0 + xp, ya = y0 + yp;
+                const R xa0 = xa, ya0 = ya;
+                if (!enforce_bc<R>(g, xa, ya, ux, uy)) { P.w[ip] = R(0); P.valid[ip] = 0; break; }
+                if (xa != xa0) xp = xa - x0;
+                if (ya != ya0) yp = ya - y0;
+            } else if (!enforce_bc<R>(g, xp, yp, ux, uy)) { P.w[ip] = R(0); P.valid[ip] = 0; break; }
             P.x[ip] = xp; P.y[ip] = yp;
             if (!temp) {
                 P.uxh[ip] = ux; P.uyh[ip] = uy; P.psih[ip] = psi;

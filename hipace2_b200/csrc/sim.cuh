@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "config.hpp"
 #include "dst.cuh"
+#include <type_traits>
 #include "kernels.cuh"
 #include "mg.cuh"
 #include "rng.hpp"
@@ -189,6 +190,7 @@ public:
     Multigrid<R> mg;
     std::vector<PlasmaDev<R>> pl;
     std::vector<double*> px0, py0;
+    std::vector<std::vector<double>> hx0, hy0;  // lattice points on the host (output of displacements)
     std::vector<BeamDev> bm;
     std::vector<HostBeam> pending_beams;
     std::vector<bool> beam_set;
@@ -291,9 +293,11 @@ public:
         mg.release();
         for (auto& p : pl)
             for (void* q : {(void*)p.x, (void*)p.y, (void*)p.w, (void*)p.ux, (void*)p.uy, (void*)p.psi, (void*)p.xp,
-                            (void*)p.yp, (void*)p.uxh, (void*)p.uyh, (void*)p.psih, (void*)p.valid})
+                            (void*)p.yp, (void*)p.uxh, (void*)p.uyh, (void*)p.psih, (void*)p.valid, (void*)p.ru,
+                            (void*)p.rv})
                 if (q) cudaFree(q);
         pl.clear();
+        hx0.clear(); hy0.clear();
         for (auto* q : px0) cudaFree(q);
         for (auto* q : py0) cudaFree(q);
         px0.clear(); py0.clear();
@@ -345,15 +349,18 @@ public:
         HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * C_NCOMP * sizeof(R)));
         dst.init(nx, ny, g.dx[0], g.dx[1], 3);
         if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
-        // HPQ_DST=gemm selects the sine-matrix GEMM path on every grid (cross-checks)
-        if (const char* e = getenv("HPQ_DST")) {
-            if (std::string(e) == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
-        }
         if (cfg.explicit_solver) mg.init(nx, ny, g.dx[0], g.dx[1]);
         HPQ_CUDA(cudaMalloc(&ctl, sizeof(Ctl)));
         HPQ_CUDA(cudaMemset(ctl, 0, sizeof(Ctl)));
         HPQ_CUDA(cudaMallocHost(&ctl_h, sizeof(Ctl)));
         std::memset(ctl_h, 0, sizeof(Ctl));
+        // Poisson form: HPQ_DST=gemm (SIMT sine GEMMs on every grid, cross-checks), fft, or tc
+        // (tensor-core sine GEMMs, single precision only)
+        if (const char* e = getenv("HPQ_DST")) {
+            const std::string m(e);
+            if (m == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
+            else if (m == "tc") { dst.set_tensor_mode(&ctl->tc_err); pc_dst.set_tensor_mode(&ctl->tc_err); }
+        }
         init_plasma_lattices();
         // beams: fixed_ppc generated here, fixed_weight drawn from the seeded generator unless
         // the caller provides particles with set_beam before the first step
@@ -418,8 +425,24 @@ public:
                 HPQ_CUDA(cudaMemcpy(dx0, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice));
                 HPQ_CUDA(cudaMemcpy(dy0, hy.data(), hy.size() * sizeof(double), cudaMemcpyHostToDevice));
             }
+            d.ru = d.rv = nullptr;
+            if (std::is_same<R, float>::value) {
+                // lattice points in cell units (exact in FP32); positions become displacements
+                std::vector<float> hu(nb, 0.f), hv(nb, 0.f);
+                for (size_t i = 0; i < hx.size(); ++i) {
+                    hu[i] = (float)((hx[i] - g.xoff) * g.dxi[0]);
+                    hv[i] = (float)((hy[i] - g.yoff) * g.dxi[1]);
+                }
+                float *du, *dv;
+                HPQ_CUDA(cudaMalloc(&du, nb * sizeof(float)));
+                HPQ_CUDA(cudaMalloc(&dv, nb * sizeof(float)));
+                HPQ_CUDA(cudaMemcpy(du, hu.data(), nb * sizeof(float), cudaMemcpyHostToDevice));
+                HPQ_CUDA(cudaMemcpy(dv, hv.data(), nb * sizeof(float), cudaMemcpyHostToDevice));
+                d.ru = du; d.rv = dv;
+            }
             pl.push_back(d);
             px0.push_back(dx0); py0.push_back(dy0);
+            hx0.push_back(std::move(hx)); hy0.push_back(std::move(hy));
         }
     }
 
@@ -987,7 +1010,13 @@ public:
         std::vector<R> tmp(n);
         for (int k = 0; k < 11; ++k) {
             HPQ_CUDA(cudaMemcpy(tmp.data(), arr[k], n * sizeof(R), cudaMemcpyDeviceToHost));
-            for (size_t i = 0; i < n; ++i) out12[k * n + i] = (double)tmp[i];
+            // x, y, xp, yp are displacements from the lattice point, psi, psih are psi - 1 when
+            // p.ru is set
+            const std::vector<double>* ref = nullptr;
+            if (p.ru && (k == 0 || k == 6)) ref = &hx0.at(sp);
+            if (p.ru && (k == 1 || k == 7)) ref = &hy0.at(sp);
+            const double off = (p.ru && (k == 5 || k == 10)) ? 1.0 : 0.0;
+            for (size_t i = 0; i < n; ++i) out12[k * n + i] = (double)tmp[i] + (ref ? (*ref)[i] : 0.0) + off;
         }
         std::vector<uint8_t> v(n);
         HPQ_CUDA(cudaMemcpy(v.data(), p.valid, n, cudaMemcpyDeviceToHost));

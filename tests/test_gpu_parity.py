@@ -143,25 +143,6 @@ def test_graph_replay_equals_kernel_launches():
         assert rel_l2(a, b) <= 1e-10
 
 
-def mixed_errors(text, comps=("Ez", "Psi", "jz_beam", "Bx")):
-    g = hp.Hipace(text, precision=hp.MIXED)
-    g.init_data()
-    o = Oracle(text)
-    o.set_beam(0, g.get_beam(0))
-    g.set_diag(list(comps))
-    o.set_diag(list(comps))
-    g.step(0)
-    o.step(0)
-    return {k: rel_l2(g.get_diag(k), o.get_diag(k)) for k in comps}
-
-
-# Stated error bounds of the mixed path (FP32 plasma, fields and multigrid, FP64 beam) against
-# the FP64 oracle after one full step (all slices), relative L2 over the 3-D arrays.
-MIXED_BOUNDS_WEAK = {"Ez": 1e-4, "Psi": 1e-4, "jz_beam": 1e-5, "Bx": 1e-3}
-MIXED_BOUNDS_BLOWOUT = {"Ez": 5e-3, "Psi": 1e-3, "jz_beam": 1e-5, "Bx": 1e-2}
-
-
-@pytest.mark.parametrize("regime", ["weak", "blowout"])
 def test_persistent_multigrid_equals_multi_kernel_form():
     """One cooperative launch per multigrid solve vs one launch per V-cycle phase (HPQ_MG=kernels)."""
     from cases import EXPLICIT_FFT, EXPLICIT_MOVING
@@ -188,6 +169,85 @@ def test_persistent_multigrid_equals_multi_kernel_form():
             assert rel_l2(a, b) <= 1e-10
 
 
+def head_slices(text, env, nslices, comps=("Psi", "Ez", "Bz", "Bx")):
+    """Fields of the first `nslices` slices of step 0 (mixed precision) under the given HPQ_* env."""
+    saved = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        g = hp.Hipace(text, precision=hp.MIXED, graphs=False)
+        g.init_data()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    g.begin_step(0)
+    nz = g.n_cell[2]
+    out = {k: [] for k in comps}
+    for s in range(nz - 1, nz - 1 - nslices, -1):
+        g.solve_one_slice(s)
+        for k in comps:
+            out[k].append(g.get_field(k))
+    g.end_step()
+    return {k: np.array(v) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("grid", ["63 63", "64 48", "255 255"])
+def test_tensor_core_dst_matches_fft_and_oracle(grid):
+    """TF32x3 sine GEMMs on tcgen05 vs the FP32 FFT (or SIMT GEMM) form and the FP64 oracle.
+
+    The first slices after the head of the box carry the driver's own field with an undisturbed
+    plasma, so differences are those of the Poisson solves, not of the slice march.
+    """
+    from cases import EXPLICIT_FFT
+    text = EXPLICIT_FFT.replace("amr.n_cell = 63 63 48", "amr.n_cell = %s 48" % grid)
+    text = text.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-10")
+    text = text.replace("beam.position_mean = 0. 0. 0.", "beam.position_mean = 0. 0. 2.5")
+    n = 6
+    tc = head_slices(text, {"HPQ_DST": "tc"}, n)
+    ref = head_slices(text, {"HPQ_DST": "fft" if grid != "64 48" else "gemm"}, n)
+    o = Oracle(text)
+    g = hp.Hipace(text, graphs=False)
+    g.init_data()
+    o.set_beam(0, g.get_beam(0))
+    comps = ["Psi", "Ez", "Bz", "Bx"]
+    o.set_diag(comps)
+    assert o.step(0) == 0
+    nz = g.n_cell[2]
+    for k in comps:
+        want = o.get_diag(k)[nz - n:][::-1]
+        e_tc, e_ref = rel_l2(tc[k], want), rel_l2(ref[k], want)
+        print(grid, k, "tc vs oracle", e_tc, "fp32 reference form vs oracle", e_ref, "tc vs it", rel_l2(tc[k], ref[k]))
+        if k in ("Bz", "Bx"):
+            # sources built from the plasma current: a cancellation at the FP32 noise level in
+            # these slices; the tensor-core form must do as well as the FP32 reference form
+            assert e_tc <= max(1e-5, 2 * e_ref), (k, e_tc, e_ref)
+        else:
+            assert e_tc <= 1e-5, (k, e_tc)
+            assert rel_l2(tc[k], ref[k]) <= 1e-5, k
+
+
+def mixed_errors(text, comps=("Ez", "Psi", "jz_beam", "Bx")):
+    g = hp.Hipace(text, precision=hp.MIXED)
+    g.init_data()
+    o = Oracle(text)
+    o.set_beam(0, g.get_beam(0))
+    g.set_diag(list(comps))
+    o.set_diag(list(comps))
+    g.step(0)
+    o.step(0)
+    return {k: rel_l2(g.get_diag(k), o.get_diag(k)) for k in comps}
+
+
+# Stated error bounds of the mixed path (FP32 plasma, fields and multigrid smoothing, FP64
+# multigrid residuals and beam) against the FP64 oracle after one full step (all slices),
+# relative L2 over the 3-D arrays.
+MIXED_BOUNDS_WEAK = {"Ez": 1e-4, "Psi": 1e-4, "jz_beam": 1e-5, "Bx": 1e-3}
+MIXED_BOUNDS_BLOWOUT = {"Ez": 5e-3, "Psi": 1e-3, "jz_beam": 1e-5, "Bx": 1e-2}
+
+
+@pytest.mark.parametrize("regime", ["weak", "blowout"])
 def test_mixed_precision_error_vs_oracle(regime):
     """Mixed path vs the FP64 oracle on the 63x63x48 explicit case (FFT Poisson path).
 
@@ -195,7 +255,7 @@ def test_mixed_precision_error_vs_oracle(regime):
     cross and rounding differences grow along the slice march.
     """
     from cases import EXPLICIT_FFT
-    text = EXPLICIT_FFT.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-5")
+    text = EXPLICIT_FFT.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-10")
     if regime == "weak":
         text = text.replace("beam.density = 5.", "beam.density = 0.05")
     errs = mixed_errors(text)
