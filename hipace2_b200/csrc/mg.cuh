@@ -372,15 +372,29 @@ struct MGCoarse {
     size_t off[16];  // level offsets (elements) in the shared-memory arena
 };
 
+// 2-D loops over the valid points of a level (threads as 16 columns x blockDim/16 rows, no
+// integer division), all points or those of one colour ((i + j + s) even)
+template <class F>
+__device__ __forceinline__ void for_valid(const MGLev& L, F f) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4, nty = blockDim.x >> 4;
+    for (int j = L.vlo + ty; j <= L.vhi_j; j += nty)
+        for (int i = L.vlo + tx; i <= L.vhi_i; i += 16) f(i, j);
+}
+template <class F>
+__device__ __forceinline__ void for_colour(const MGLev& L, int s, F f) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4, nty = blockDim.x >> 4;
+    for (int j = L.vlo + ty; j <= L.vhi_j; j += nty) {
+        const int i0 = L.vlo + ((L.vlo + j + s) & 1);
+        for (int i = i0 + 2 * tx; i <= L.vhi_i; i += 32) f(i, j);
+    }
+}
+
 template <class R, bool CELL>
 __device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* dinv, const R* res, R* cor, int nsweeps, R facx,
                                            R facy) {
-    const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
     const int plane = L.w * L.h;
     for (int s = 0; s < nsweeps; ++s) {
-        for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
-            const int i = L.vlo + k % vw, j = L.vlo + k / vw;
-            if (((i + j + s) & 1) != 0) continue;
+        for_colour(L, s, [&](int i, int j) {
             const int id = j * L.w + i;
             const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
             const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
@@ -390,16 +404,19 @@ __device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* dinv, const 
                 R* p = cor + c * plane;
                 p[id] = mg_gs_inv<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], res[c * plane + id], inv, facx, facy);
             }
-        }
+        });
         __syncthreads();
     }
 }
 
-// The global arrays are plain (not restrict/read-only) pointers: in the persistent solve other
-// blocks write them earlier in the same launch.
+// The coarse levels in one block. With `init` the coefficient hierarchy and the inverse
+// diagonals are built in the arena; without it they are the ones of an earlier call of the same
+// solve, still resident in this block's shared memory. The global arrays are plain (not
+// restrict/read-only) pointers: in the persistent solve other blocks write them earlier in the
+// same launch.
 template <class R, bool CELL>
 __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
-                                                R facy0, unsigned char* smem_raw) {
+                                                R facy0, unsigned char* smem_raw, bool init) {
     __syncthreads();  // the block may have used the shared memory just before
     R* arena = reinterpret_cast<R*>(smem_raw);
     // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
@@ -408,57 +425,52 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     auto rsc = [&](int l) { return arena + M.off[l] + 4 * (size_t)M.L[l].w * M.L[l].h; };
     auto acf = [&](int l) { return arena + M.off[l] + 6 * (size_t)M.L[l].w * M.L[l].h; };
     auto dinv = [&](int l) { return arena + M.off[l] + 7 * (size_t)M.L[l].w * M.L[l].h; };
-    {
-        const int n0 = M.L[0].w * M.L[0].h;
-        for (int k = threadIdx.x; k < n0; k += blockDim.x) {
-            res(0)[k] = res_g[k];
-            res(0)[n0 + k] = res_g[n0 + k];
-            acf(0)[k] = acf_g[k];
-        }
-        for (int l = 1; l < M.nl; ++l) {
+    const int n0 = M.L[0].w * M.L[0].h;
+    if (init) {
+        for (int l = 0; l < M.nl; ++l) {
             const int n = M.L[l].w * M.L[l].h;
             for (int k = threadIdx.x; k < 8 * n; k += blockDim.x) cor(l)[k] = R(0);
         }
         __syncthreads();
+        for (int k = threadIdx.x; k < n0; k += blockDim.x) acf(0)[k] = acf_g[k];
+        __syncthreads();
         // coefficient hierarchy below sb
         for (int l = 1; l < M.nl; ++l) {
             const MGLev& C = M.L[l];
-            const MGLev& F = M.L[l - 1];
-            MV<R> fine{{acf(l - 1), acf(l - 1)}, F.w, 0};
-            const int cw = C.vhi_i - C.vlo + 1, ch = C.vhi_j - C.vlo + 1;
-            for (int k = threadIdx.x; k < cw * ch; k += blockDim.x) {
-                const int i = C.vlo + k % cw, j = C.vlo + k / cw;
-                acf(l)[j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, 0);
-            }
+            MV<R> fine{{acf(l - 1), acf(l - 1)}, M.L[l - 1].w, 0};
+            for_valid(C, [&](int i, int j) { acf(l)[j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, 0); });
             __syncthreads();
         }
         R fx = facx0, fy = facy0;
         for (int l = 0; l < M.nl; ++l) {
             const MGLev& L = M.L[l];
-            const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
-            for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
-                const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+            for_valid(L, [&](int i, int j) {
                 dinv(l)[j * L.w + i] = mg_diag_inv<R, CELL>(L, i, j, acf(l)[j * L.w + i], fx, fy);
-            }
+            });
             fx *= R(0.25);
             fy *= R(0.25);
         }
-        __syncthreads();
+    } else {
+        for (int l = 0; l < M.nl; ++l) {
+            const int n = M.L[l].w * M.L[l].h;
+            for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) cor(l)[k] = R(0);
+        }
     }
+    for (int k = threadIdx.x; k < n0; k += blockDim.x) {
+        res(0)[k] = res_g[k];
+        res(0)[n0 + k] = res_g[n0 + k];
+    }
+    __syncthreads();
     R facx = facx0, facy = facy0;
     for (int l = 0; l < M.nl; ++l) {
         const MGLev& L = M.L[l];
         const int plane = L.w * L.h;
-        for (int k = threadIdx.x; k < 2 * plane; k += blockDim.x) cor(l)[k] = R(0);
-        __syncthreads();
         if (l == M.nl - 1) {
             blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 16, facx, facy);
             break;
         }
         blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
-        const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
-        for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
-            const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+        for_valid(L, [&](int i, int j) {
             const int id = j * L.w + i;
             const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
             const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
@@ -468,17 +480,15 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
                 rsc(l)[c * plane + id] = res(l)[c * plane + id] + acf(l)[id] * p[id] -
                                          mg_lap<R, CELL>(L, i, j, p[id], p[im], p[ip], p[jm], p[jp], facx, facy);
             }
-        }
+        });
         __syncthreads();
         const MGLev& C = M.L[l + 1];
-        const int cw = C.vhi_i - C.vlo + 1, ch = C.vhi_j - C.vlo + 1;
         MV<R> fine{{rsc(l), rsc(l) + plane}, L.w, 0};
         const int cplane = C.w * C.h;
-        for (int k = threadIdx.x; k < cw * ch; k += blockDim.x) {
-            const int i = C.vlo + k % cw, j = C.vlo + k / cw;
+        for_valid(C, [&](int i, int j) {
 #pragma unroll
             for (int c = 0; c < 2; ++c) res(l + 1)[c * cplane + j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, c);
-        }
+        });
         __syncthreads();
         facx *= R(0.25);
         facy *= R(0.25);
@@ -490,17 +500,14 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         const MGLev& C = M.L[l + 1];
         const int plane = L.w * L.h;
         MV<R> crse{{cor(l + 1), cor(l + 1) + C.w * C.h}, C.w, 0};
-        const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
-        for (int k = threadIdx.x; k < vw * vh; k += blockDim.x) {
-            const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+        for_valid(L, [&](int i, int j) {
 #pragma unroll
             for (int c = 0; c < 2; ++c) cor(l)[c * plane + j * L.w + i] += mg_interp1<R, CELL>(crse, i, j, c);
-        }
+        });
         __syncthreads();
         blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
     }
-    const int n0 = 2 * M.L[0].w * M.L[0].h;
-    for (int k = threadIdx.x; k < n0; k += blockDim.x) cor_g[k] = cor(0)[k];
+    for (int k = threadIdx.x; k < 2 * n0; k += blockDim.x) cor_g[k] = cor(0)[k];
 }
 
 template <class R, bool CELL>
@@ -508,7 +515,7 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
                                                     R* __restrict__ cor_g, R facx0, R facy0) {
     HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
-    mg_bottom_block<R, CELL>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw);
+    mg_bottom_block<R, CELL>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw, true);
 }
 
 template <class R>
@@ -560,31 +567,35 @@ __device__ __forceinline__ unsigned long long tc_clock_ns() {
     return t;
 }
 
-// Grid-wide barrier for a cooperative launch (all blocks co-resident). Bounded: a block that
+// Grid-wide barrier for a cooperative launch (all blocks co-resident). Arrival is one
+// acquire-release atomic per block; the last block to arrive resets the counter and bumps the
+// generation word with a release, the others poll it with acquire loads. Bounded: a block that
 // polls longer than kBarrierSpins, or sees the error flag, sets the flag and returns false;
 // every block then leaves the kernel at its next barrier.
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool grid_barrier(unsigned int* bar, int* err) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int* gen = bar + 1;
         volatile int* verr = err;
-        const unsigned int g = *gen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
+        const unsigned int g = ld_acquire(bar + 1);
+        unsigned int arrived;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
         if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
         } else {
             long long it = 0;
-            while (*gen == g) {
+            while (ld_acquire(bar + 1) == g) {
                 if (*verr) break;
                 if (++it > kBarrierSpins) { atomicExch(err, 1); break; }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
-        __threadfence();
         s_ok = (*verr == 0);
     }
     __syncthreads();
@@ -818,6 +829,10 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         a.ctl = ctl;
         return a;
     };
+    // block 0 runs the coarse levels and keeps them resident in its shared memory; the tiles
+    // go to the other blocks
+    const int tb = (nb > 1) ? (int)blockIdx.x - 1 : 0, ntb = (nb > 1) ? nb - 1 : 1;
+    const bool tile_block = (nb == 1) || blockIdx.x > 0;
     auto ntiles = [&](int l, int& ntx) {
         const MGLev& L = P.lev[l];
         ntx = (L.vhi_i - L.vlo + 16) / 16;
@@ -842,7 +857,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         a.crse_res = mg_own<R>(P.res, P.lev, 1);
         int ntx;
         const int nt = ntiles(0, ntx);
-        for (int t = blockIdx.x; t < nt; t += nb) {
+        for (int t = tb; tile_block && t < nt; t += ntb) {
             if constexpr (kRefine)
                 mg_refine_tile<CELL, true, 4>(P, 0, t % ntx, t / ntx, smem_raw, bmax, brhs);
             else
@@ -874,7 +889,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             a.acf = mg_own<R>(P.acf, P.lev, l, 1); a.crse_res = mg_own<R>(P.res, P.lev, l + 1);
             int ntx;
             const int nt = ntiles(l, ntx);
-            for (int t = blockIdx.x; t < nt; t += nb)
+            for (int t = tb; tile_block && t < nt; t += ntb)
                 mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (it == 0) restrict_acf(l + 1);
             if (!grid_barrier(bar, err)) return;
@@ -882,7 +897,8 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         }
         // levels sb .. nl-1 in block 0
         if (blockIdx.x == 0)
-            mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw);
+            mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
+                                     it == 0 || nb == 1);
         if (!grid_barrier(bar, err)) return;
         stamp();
         // up: levels sb-1 .. 1, interpolation of the coarser correction + 4 sweeps
@@ -893,7 +909,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             a.crse_in = (l + 1 == P.sb) ? mg_own<R>(P.cor, P.lev, P.sb) : mg_own<R>(P.up, P.lev, l + 1);
             int ntx;
             const int nt = ntiles(l, ntx);
-            for (int t = blockIdx.x; t < nt; t += nb)
+            for (int t = tb; tile_block && t < nt; t += ntb)
                 mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (!grid_barrier(bar, err)) return;
             stamp();
@@ -910,7 +926,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             int ntx;
             const int nt = ntiles(0, ntx);
             bmax = 0;
-            for (int t = blockIdx.x; t < nt; t += nb) {
+            for (int t = tb; tile_block && t < nt; t += ntb) {
                 if constexpr (kRefine)
                     mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
                 else
@@ -1088,7 +1104,7 @@ public:
         HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, coop_smem));
         const MGLev& L = lev[0];
         const int nt0 = ((L.vhi_i - L.vlo + 16) / 16) * ((L.vhi_j - L.vlo + 16) / 16);
-        coop_blocks = std::min(per * sms, nt0);
+        coop_blocks = std::min(per * sms, nt0 + 1);  // + block 0 for the coarse levels
         coop_ok = coop && per > 0 && coop_blocks > 0;
     }
 
