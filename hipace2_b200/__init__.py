@@ -23,7 +23,7 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_init", "hpq_set_beam", "hpq_beam_count", "hpq_get_beam", "hpq_step",
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
            "hpq_get_diag", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
-           "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
+           "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
            "hpq_get_profile", "hpq_poisson_dirichlet_noalloc")
 
 _lib = None
@@ -67,6 +67,7 @@ def load_library(path=None):
         "hpq_plasma_count": ([vp, i32, lp], i32),
         "hpq_get_plasma": ([vp, i32, dp], i32),
         "hpq_set_graphs": ([vp, i32], i32),
+        "hpq_set_deterministic": ([vp, i32], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
         "hpq_get_counters": ([vp, lp, lp, lp, lp], i32),
@@ -98,7 +99,7 @@ PLASMA_ATTRS = ("x", "y", "w", "ux", "uy", "psi", "x_prev", "y_prev", "ux_half_s
 class Hipace:
     """One simulation on one GPU, driven through libhpq."""
 
-    def __init__(self, input_text, precision=PLAIN_FP64, graphs=True):
+    def __init__(self, input_text, precision=PLAIN_FP64, graphs=True, deterministic=False):
         self.L = load_library()
         h = ctypes.c_void_p()
         rc = self.L.hpq_create(input_text.encode(), ctypes.byref(h))
@@ -107,6 +108,7 @@ class Hipace:
         self.h = h
         self._check(self.L.hpq_set_precision(self.h, precision))
         self._check(self.L.hpq_set_graphs(self.h, int(bool(graphs))))
+        self._check(self.L.hpq_set_deterministic(self.h, int(bool(deterministic))))
         self.n_cell = _n_cell(input_text)
         self.max_step = _scalar(input_text, "max_step", 0)
         self._diag = []
@@ -190,6 +192,10 @@ class Hipace:
 
     def stream(self):
         return self.L.hpq_stream(self.h)
+
+    def set_deterministic(self, on):
+        """Bit-identical results run to run (fixed-point deposition, fixed-order reductions)."""
+        self._check(self.L.hpq_set_deterministic(self.h, int(bool(on))))
 
     def set_profiling(self, on):
         self._check(self.L.hpq_set_profiling(self.h, int(bool(on))))

@@ -13,6 +13,7 @@ struct hpq_handle {
     std::unique_ptr<hpq::SimBase> sim;
     int precision = HPQ_PLAIN_FP64;
     bool graphs = false;
+    bool deterministic = false;
     bool initialised = false;
     bool in_step = false;
     std::string err;
@@ -89,6 +90,7 @@ int hpq_init(hpq_handle* h) {
         else h->sim.reset(new hpq::Sim<double>(h->cfg));
         h->sim->init();
         h->sim->set_graphs(h->graphs);
+        h->sim->set_deterministic(h->deterministic);
         h->initialised = true;
         return (int)HPQ_OK;
     });
@@ -217,6 +219,15 @@ int hpq_set_graphs(hpq_handle* h, int on) {
     return guarded(h, [&] {
         h->graphs = on != 0;
         if (h->sim) h->sim->set_graphs(h->graphs);
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_set_deterministic(hpq_handle* h, int on) {
+    return guarded(h, [&] {
+        if (h->in_step) { h->err = "hpq_set_deterministic inside a step"; return (int)HPQ_ERR_STATE; }
+        h->deterministic = on != 0;
+        if (h->sim) h->sim->set_deterministic(h->deterministic);
         return (int)HPQ_OK;
     });
 }

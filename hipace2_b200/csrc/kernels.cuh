@@ -160,9 +160,36 @@ struct DepOut {
     int pitch;
 };
 
+// Deterministic deposition (hpq_set_deterministic). Floating-point atomics give sums whose last
+// bits depend on the order in which threads arrive. In deterministic mode every deposited value v
+// is split into three 64-bit fixed-point words,
+//   a = rint(v 2^10),  b = rint((v - a 2^-10) 2^50),  c = rint((v - a 2^-10 - b 2^-50) 2^90),
+// added with integer atomics into slab-shaped shadow arrays. Integer addition is associative, so
+// the totals do not depend on the arrival order, and k_det_flush turns them back into one
+// floating-point value per cell, the same on every run. Range: |sum| < 2^53; resolution 2^-91
+// per deposited value (below the FP64 rounding of any value above 1e-12).
+struct DetAcc {
+    long long* w[3];   // shadow words (null: plain floating-point atomics)
+    const void* base;  // slab base the deposited planes belong to
+};
+
 template <class R>
-__device__ __forceinline__ void addc(R* base, int pitch, int i, int j, R v) {
-    atomicAdd(base + (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc), v);
+__device__ __forceinline__ void addc(const DetAcc& d, R* base, int pitch, int i, int j, R v) {
+    const ptrdiff_t off = (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc);
+    double r = (double)v;
+    if (d.w[0] == nullptr || !isfinite(r)) {
+        atomicAdd(base + off, v);
+        return;
+    }
+    const ptrdiff_t e = (base - static_cast<const R*>(d.base)) + off;
+    const double a = rint(r * 0x1p10);
+    r -= a * 0x1p-10;
+    const double b = rint(r * 0x1p50);
+    r -= b * 0x1p-50;
+    const double c = rint(r * 0x1p90);
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.w[0] + e), (unsigned long long)(long long)a);
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.w[1] + e), (unsigned long long)(long long)b);
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.w[2] + e), (unsigned long long)(long long)c);
 }
 
 // Cell-unit coordinate of a plasma position along one axis as base + t: with a reference lattice
@@ -188,7 +215,7 @@ __device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R o
 
 template <class R>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
-                                                        const int* gate) {
+                                                        const int* gate, DetAcc det) {
     HPQ_PDL_ENTRY();
     if (gate && !*gate) return;
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
@@ -231,11 +258,11 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
             for (int ix = 0; ix < 3; ++ix) {
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 const R cd = q_invvol * sx[ix].s * sy[iy].s;
-                if (o.jx) { addc(o.jx, o.pitch, i, j, cd * vx_c); addc(o.jy, o.pitch, i, j, cd * vy_c); }
-                if (o.jz) addc(o.jz, o.pitch, i, j, cd * gpm1 * clight);
-                if (o.rho) addc(o.rho, o.pitch, i, j, cd * gamma_psi);
-                if (o.chi) addc(o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
-                if (o.rhomjz) addc(o.rhomjz, o.pitch, i, j, cd);
+                if (o.jx) { addc(det, o.jx, o.pitch, i, j, cd * vx_c); addc(det, o.jy, o.pitch, i, j, cd * vy_c); }
+                if (o.jz) addc(det, o.jz, o.pitch, i, j, cd * gpm1 * clight);
+                if (o.rho) addc(det, o.rho, o.pitch, i, j, cd * gamma_psi);
+                if (o.chi) addc(det, o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
+                if (o.rhomjz) addc(det, o.rhomjz, o.pitch, i, j, cd);
             }
     }
 }
@@ -244,7 +271,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
 // Explicit Sx/Sy deposition (ExplicitDeposition.cpp:20-265, no laser)
 // ------------------------------------------------------------------------------------------
 template <class R, int DT>
-__global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g) {
+__global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);
@@ -288,8 +315,8 @@ __global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R
                                      (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * gmy) * a_clight);
                 const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
                                      (+sxd * sys * dxi * gmx + sxs * syd * dyi * (-vx * vy)) * a_clight);
-                addc(Sy, S.pitch, i, j, vsy);
-                addc(Sx, S.pitch, i, j, vsx);
+                addc(det, Sy, S.pitch, i, j, vsy);
+                addc(det, Sx, S.pitch, i, j, vsx);
             }
     }
 }
@@ -426,7 +453,7 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
 // ------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __restrict__ ctl, int which, R* jx, R* jy,
-                                                      R* jz, R* rmj, int pitch, Geo g, int gated) {
+                                                      R* jz, R* rmj, int pitch, Geo g, int gated, DetAcc det) {
     HPQ_PDL_ENTRY();
     if (gated && !ctl->pc_go) return;
     const int s = ctl->islice - which;
@@ -455,9 +482,9 @@ __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __re
             for (int ix = 0; ix < 3; ++ix) {
                 const double S = sx[ix].s * sy[iy].s;
                 const int i = sx[ix].cell, j = sy[iy].cell;
-                if (jx) { addc<R>(jx, pitch, i, j, (R)(S * wqx)); addc<R>(jy, pitch, i, j, (R)(S * wqy)); }
-                if (jz) addc<R>(jz, pitch, i, j, (R)(S * wqz));
-                if (rmj) addc<R>(rmj, pitch, i, j, (R)(S * wqr));
+                if (jx) { addc<R>(det, jx, pitch, i, j, (R)(S * wqx)); addc<R>(det, jy, pitch, i, j, (R)(S * wqy)); }
+                if (jz) addc<R>(det, jz, pitch, i, j, (R)(S * wqz));
+                if (rmj) addc<R>(det, rmj, pitch, i, j, (R)(S * wqr));
             }
     }
 }
@@ -466,7 +493,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __re
 // non-slipped particles of this slice, jx_beam/jy_beam of the next slice from its particles.
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const Ctl* __restrict__ ctl, R* jz, R* rmj,
-                                                                R* njx, R* njy, int pitch, Geo g) {
+                                                                R* njx, R* njy, int pitch, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
     const int s = ctl->islice;
     const int par = ctl->step_parity;
@@ -496,11 +523,11 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
                 const double S = sx[ix].s * sy[iy].s;
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 if (nxt) {
-                    addc<R>(njx, pitch, i, j, (R)(S * wqx));
-                    addc<R>(njy, pitch, i, j, (R)(S * wqy));
+                    addc<R>(det, njx, pitch, i, j, (R)(S * wqx));
+                    addc<R>(det, njy, pitch, i, j, (R)(S * wqy));
                 } else {
-                    addc<R>(jz, pitch, i, j, (R)(S * wqz));
-                    if (rmj) addc<R>(rmj, pitch, i, j, (R)(S * wqr));
+                    addc<R>(det, jz, pitch, i, j, (R)(S * wqz));
+                    if (rmj) addc<R>(det, rmj, pitch, i, j, (R)(S * wqr));
                 }
             }
     }
@@ -662,6 +689,22 @@ struct CompList {
     int n;
     int c[24];
 };
+
+// deterministic deposition: listed planes += fixed-point totals (see addc), shadows cleared
+template <class R>
+__global__ void k_det_flush(Slab<R> S, DetAcc d, CompList L) {
+    HPQ_PDL_ENTRY();
+    const size_t n = S.cstride;
+    for (long long k = gtid(); k < (long long)n; k += gstride())
+        for (int q = 0; q < L.n; ++q) {
+            const size_t e = (size_t)L.c[q] * S.cstride + k;
+            const long long a = d.w[0][e], b = d.w[1][e], c = d.w[2][e];
+            if ((a | b | c) == 0) continue;
+            const double v = ((double)c * 0x1p-90 + (double)b * 0x1p-50) + (double)a * 0x1p-10;
+            S.base[e] += (R)v;
+            d.w[0][e] = 0; d.w[1][e] = 0; d.w[2][e] = 0;
+        }
+}
 
 // zero listed components over the whole allocated slice (setVal on growntilebox)
 template <class R>

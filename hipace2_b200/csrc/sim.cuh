@@ -61,6 +61,7 @@ public:
     virtual cudaStream_t stream() = 0;
     virtual Stats stats() = 0;
     virtual void set_graphs(bool on) = 0;
+    virtual void set_deterministic(bool on) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual bool get_profile(const std::string& name, double* ms, long long* n) = 0;
     virtual std::string profile_names() = 0;
@@ -103,7 +104,20 @@ __global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl
         nd += sqrt((a - c) * (a - c) + (b - d) * (b - d));
     }
     for (int o = 16; o > 0; o >>= 1) { nb += __shfl_xor_sync(0xffffffffu, nb, o); nd += __shfl_xor_sync(0xffffffffu, nd, o); }
-    if ((threadIdx.x & 31) == 0) { atomicAdd(&ctl->pc_sum[0], nb); atomicAdd(&ctl->pc_sum[1], nd); }
+    if (gridDim.x > 1) {
+        if ((threadIdx.x & 31) == 0) { atomicAdd(&ctl->pc_sum[0], nb); atomicAdd(&ctl->pc_sum[1], nd); }
+        return;
+    }
+    // one block (deterministic mode): warp sums added in warp order by one thread
+    __shared__ double wb[32], wd[32];
+    if ((threadIdx.x & 31) == 0) { wb[threadIdx.x >> 5] = nb; wd[threadIdx.x >> 5] = nd; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sb = 0, sd = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { sb += wb[w]; sd += wd[w]; }
+        ctl->pc_sum[0] += sb;
+        ctl->pc_sum[1] += sd;
+    }
 }
 // first error of a slice -> initial-guess mixing factor (InitialBfieldGuess)
 __global__ void k_pc_guess_factor(Ctl* ctl, double tol) {
@@ -303,6 +317,9 @@ public:
         px0.clear(); py0.clear();
         for (auto& b : bm) free_beam(b);
         bm.clear();
+        if (det_mem) cudaFree(det_mem);
+        det_mem = nullptr;
+        det = DetAcc{};
         if (ctl) cudaFree(ctl);
         if (ctl_h) cudaFreeHost(ctl_h);
         ctl = nullptr; ctl_h = nullptr;
@@ -685,8 +702,9 @@ public:
         for (size_t s = 0; s < pl.size(); ++s) {
             if (!pl[s].neutralize || pl[s].n == 0) continue;
             DepOut<R> o{nullptr, nullptr, nullptr, nullptr, nullptr, S.c(C_IONS).p, S.pitch};
-            hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr);
+            hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr, det);
             HPQ_LAUNCH_CHECK();
+            det_flush({C_IONS});
         }
         // control block for the slice march
         std::memset(ctl_h, 0, sizeof(Ctl));
@@ -719,14 +737,52 @@ public:
         if (pl[sp].n == 0) return;
         DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
         Scope sc(this, "plasma_deposit");
-        hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr);
+        hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det);
         HPQ_LAUNCH_CHECK();
+        det_flush_ptrs({jx, jy, jz, rho, chi, rhomjz});
     }
     void deposit_beam(int b, int which, R* jx, R* jy, R* jz, R* rmj) {
         Scope sc(this, "beam_deposit");
-        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], (const Ctl*)ctl, which, jx, jy, jz, rmj, S.pitch, g, 0);
+        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], (const Ctl*)ctl, which, jx, jy, jz, rmj, S.pitch, g, 0, det);
+        HPQ_LAUNCH_CHECK();
+        det_flush_ptrs({jx, jy, jz, rmj});
+    }
+    // ---- deterministic deposition (fixed-point shadows, see addc)
+    DetAcc det{};
+    long long* det_mem = nullptr;
+    void set_deterministic(bool on) override {
+        if (on == (det.w[0] != nullptr)) return;
+        invalidate_graph();
+        if (on) {
+            const size_t n = (size_t)C_NCOMP * S.cstride;
+            HPQ_CUDA(cudaMalloc(&det_mem, 3 * n * sizeof(long long)));
+            HPQ_CUDA(cudaMemset(det_mem, 0, 3 * n * sizeof(long long)));
+            for (int k = 0; k < 3; ++k) det.w[k] = det_mem + k * n;
+            det.base = S.base;
+        } else {
+            HPQ_CUDA(cudaDeviceSynchronize());
+            cudaFree(det_mem);
+            det_mem = nullptr;
+            det = DetAcc{};
+        }
+    }
+    void det_flush(std::initializer_list<int> comps) {
+        if (!det.w[0]) return;
+        CompList L{};
+        for (int c : comps) L.c[L.n++] = c;
+        hpq_launch(k_det_flush<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 4)), dim3(256), 0, st, S, det, L);
         HPQ_LAUNCH_CHECK();
     }
+    void det_flush_ptrs(std::initializer_list<R*> planes) {
+        if (!det.w[0]) return;
+        CompList L{};
+        for (R* p : planes)
+            if (p) L.c[L.n++] = (int)((p - S.base) / (ptrdiff_t)S.cstride);
+        if (L.n == 0) return;
+        hpq_launch(k_det_flush<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 4)), dim3(256), 0, st, S, det, L);
+        HPQ_LAUNCH_CHECK();
+    }
+
     void zero(std::initializer_list<int> comps) {
         CompList L{};
         for (int c : comps) L.c[L.n++] = c;
@@ -867,8 +923,9 @@ public:
                 const bool nj = cfg.do_beam_jx_jy_deposition;
                 hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st, 
                     bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
-                    nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g);
+                    nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det);
                 HPQ_LAUNCH_CHECK();
+                det_flush({C_JZB, C_RHOMJZB, C_NJXB, C_NJYB});
             }
         } else {
             if (cfg.deposit_rho) zero({C_EXMBY, C_EYPBX, C_JX, C_JY, C_JZ, C_RHOMJZ, C_RHO});
@@ -887,10 +944,11 @@ public:
                 if (pl[s].n == 0) continue;
                 Scope sc(this, "explicit_deposit");
                 const int nb = blocks_for(pl[s].n, 256);
-                if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
-                else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
-                else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g);
+                if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+                else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+                else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
                 HPQ_LAUNCH_CHECK();
+                det_flush({C_SX, C_SY});
             }
             mg_solve();
         } else {
@@ -933,7 +991,7 @@ public:
         const double tol = cfg.predcorr_B_error_tolerance;
         const int maxit = cfg.predcorr_max_iterations;
         HPQ_CUDA(cudaMemsetAsync(&ctl->pc_sum[0], 0, 2 * sizeof(double), st));
-        hpq_launch(k_pc_norms<R>, dim3(blocks_for(nxy, 256, 148 * 4)), dim3(256), 0, st, S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
+        hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
         HPQ_LAUNCH_CHECK();
         hpq_launch(k_pc_guess_factor, dim3(1), dim3(1), 0, st, ctl, tol);
         HPQ_LAUNCH_CHECK();
@@ -946,8 +1004,9 @@ public:
                 hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, &ctl->pc_go);
                 HPQ_LAUNCH_CHECK();
                 DepOut<R> o{S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, nullptr, nullptr, S.pitch};
-                hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go);
+                hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go, det);
                 HPQ_LAUNCH_CHECK();
+                det_flush({C_NJX, C_NJY});
             }
             if (cfg.do_beam_jx_jy_deposition)
                 for (size_t b = 0; b < bm.size(); ++b) deposit_beam_if((int)b);
@@ -955,7 +1014,7 @@ public:
             hpq_launch(k_rhs_bxby<R>, dim3(blocks_for(nxy, 256)), dim3(256), 0, st, S, g, pc_dst.stage, pc_dst.sk, pc_dst.sj);
             HPQ_LAUNCH_CHECK();
             pc_dst.solve(st, 2, S.base, S.cstride, S.pitch, comps);
-            hpq_launch(k_pc_norms<R>, dim3(blocks_for(nxy, 256, 148 * 4)), dim3(256), 0, st, S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
+            hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
             HPQ_LAUNCH_CHECK();
             hpq_launch(k_pc_iter_factor, dim3(1), dim3(1), 0, st, ctl, tol, maxit);
             HPQ_LAUNCH_CHECK();
@@ -966,8 +1025,9 @@ public:
         }
     }
     void deposit_beam_if(int b) {
-        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1);
+        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1, det);
         HPQ_LAUNCH_CHECK();
+        det_flush({C_NJX, C_NJY});
     }
 
     // ----------------------------------------------------------------------------- io

@@ -96,6 +96,13 @@ int hpq_get_plasma(hpq_handle* h, int sp, double* out);
 
 /* Capture each slice in a CUDA graph (default on) or launch kernel by kernel. */
 int hpq_set_graphs(hpq_handle* h, int on);
+/* Deterministic deposition (default off): current and charge deposits are accumulated with
+ * order-independent fixed-point integer atomics and every reduction runs in a fixed order, so
+ * two runs on the same inputs give bit-identical fields, beams and plasma. The reference deposits
+ * with floating-point atomics (PlasmaDepositCurrent.cpp:164-247, BeamDepositCurrent.cpp:130-190)
+ * and has no such mode; the values agree with the default mode to FP64 rounding. Allowed between
+ * steps. */
+int hpq_set_deterministic(hpq_handle* h, int on);
 /* Wait for all work of the handle. */
 int hpq_synchronize(hpq_handle* h);
 /* Per-kernel-class timing with CUDA events on the launching stream (kernel launch mode only).

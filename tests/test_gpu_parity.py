@@ -169,6 +169,56 @@ def test_persistent_multigrid_equals_multi_kernel_form():
             assert rel_l2(a, b) <= 1e-10
 
 
+DET_COMPS = ["Psi", "Ez", "Bx", "By", "Bz", "jx", "jy", "jz_beam", "rhomjz", "chi", "Sx", "Sy"]
+
+
+def det_run(text, precision, steps=2):
+    g = hp.Hipace(text, precision=precision, graphs=True, deterministic=True)
+    g.init_data()
+    g.set_diag(DET_COMPS)
+    for s in range(steps):
+        g.step(s)
+    return g, [g.get_diag(k) for k in DET_COMPS]
+
+
+@pytest.mark.parametrize("precision", [hp.PLAIN_FP64, hp.MIXED])
+def test_deterministic_mode_is_bit_exact_run_to_run(precision):
+    """Fixed-point deposition: two runs give identical bits (fields, beam, plasma)."""
+    from cases import EXPLICIT_MOVING
+    text = EXPLICIT_MOVING
+    if precision == hp.MIXED:
+        text = text.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-10")
+    ga, a = det_run(text, precision)
+    gb, b = det_run(text, precision)
+    for k, x, y in zip(DET_COMPS, a, b):
+        assert np.array_equal(x, y), k
+    ba, bb = ga.get_beam(0), gb.get_beam(0)
+    ia, ib = np.argsort(ba["id"], kind="stable"), np.argsort(bb["id"], kind="stable")
+    for k in ("x", "y", "z", "ux", "uy", "uz"):
+        assert np.array_equal(ba[k][ia], bb[k][ib]), k
+    pa, pb = ga.get_plasma(0), gb.get_plasma(0)
+    for k in ("x", "y", "ux", "uy", "psi"):
+        assert np.array_equal(pa[k], pb[k]), k
+
+
+def test_deterministic_mode_matches_oracle():
+    """The fixed-point accumulation keeps the FP64 parity bar (goldens and the PC solver)."""
+    for text, comps in ((golden_input("linear_wake.normalized.1Rank"), ["Ez", "Psi", "Bx", "jz_beam", "rhomjz"]),
+                        (PC_SMALL, PC_COMPS)):
+        g = hp.Hipace(text, graphs=False, deterministic=True)
+        g.init_data()
+        o = Oracle(text)
+        o.set_beam(0, g.get_beam(0))
+        g.set_diag(comps)
+        o.set_diag(comps)
+        for s in range(2):
+            g.step(s)
+            assert o.step(s) == 0
+        for k in comps:
+            e = rel_l2(g.get_diag(k), o.get_diag(k))
+            assert e <= 1e-10, (k, e)
+
+
 def head_slices(text, env, nslices, comps=("Psi", "Ez", "Bz", "Bx")):
     """Fields of the first `nslices` slices of step 0 (mixed precision) under the given HPQ_* env."""
     saved = {k: os.environ.get(k) for k in env}
