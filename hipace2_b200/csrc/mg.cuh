@@ -183,13 +183,39 @@ __device__ __forceinline__ void mg_decide_iter(Ctl* ctl, double norminf, int max
 #endif
 }
 
+// Asynchronous global -> shared copy of one element (cp.async, 4 or 8 bytes); with `valid` false
+// nothing is read and the element is zero-filled. All copies of a tile are in flight together.
+template <class R>
+__device__ __forceinline__ void cp_async_el(R* dst, const R* src, bool valid) {
+    static_assert(sizeof(R) == 4 || sizeof(R) == 8, "element size");
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if (sizeof(R) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// interpcpy (HpMultiGrid.cpp:79-120) with the coarse values read through an accessor c(ic, jc)
+template <class R, bool CELL, class C>
+__device__ __forceinline__ R mg_interp1f(const C& crse, int i, int j) {
+    const int ic = i >> 1, jc = j >> 1;
+    if (CELL) return crse(ic, jc);
+    const bool io = (ic * 2 != i), jo = (jc * 2 != j);
+    if (io && jo) return (crse(ic, jc) + crse(ic + 1, jc) + crse(ic, jc + 1) + crse(ic + 1, jc + 1)) * R(0.25);
+    if (io) return (crse(ic, jc) + crse(ic + 1, jc)) * R(0.5);
+    if (jo) return (crse(ic, jc) + crse(ic, jc + 1)) * R(0.5);
+    return crse(ic, jc);
+}
+
 template <int T, int NSW>
 struct SmoothSmem {
     static constexpr int H = NSW + 2;  // exact residual on the tile and its ring after NSW sweeps
     static constexpr int E = T + 2 * H;
     static constexpr int Q = T + 2;
+    static constexpr int EC = E / 2 + 3;  // coarse points under the loaded region (interpolation)
     template <class R>
-    static constexpr size_t bytes() { return (size_t)(6 * E * E + 2 * Q * Q) * sizeof(R); }
+    static constexpr size_t bytes() { return (size_t)(6 * E * E + 2 * Q * Q + 2 * EC * EC) * sizeof(R); }
 };
 
 // One T x T tile (tile coordinates bx, by) of the fused smoother. `swap` selects in2/out2 for
@@ -207,31 +233,56 @@ __device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, i
     R* sa = reinterpret_cast<R*>(smem_raw + 4 * E * E * sizeof(R));             // coefficient
     R* sinv = reinterpret_cast<R*>(smem_raw + 5 * E * E * sizeof(R));           // 1 / diagonal
     R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 6 * E * E * sizeof(R));   // residual
+    constexpr int EC = SM::EC;
+    R (*sc)[EC * EC] = reinterpret_cast<R (*)[EC * EC]>(smem_raw + (6 * E * E + 2 * Q * Q) * sizeof(R));  // coarse
     const MGLev& L = A.L;
     const int t0i = L.vlo + bx * T, t0j = L.vlo + by * T;
     const int ti0 = t0i - H, tj0 = t0j - H;
     const MV<R> vin = swap ? A.in2 : A.in;
     const MV<R> vout = swap ? A.out2 : A.out;
     __syncthreads();  // shared memory of the previous tile of this block
-    // every global read of the tile happens here, all in flight together
+    // every global read of the tile is an asynchronous copy issued here, all in flight together
+    // (cells outside the valid box are zero-filled)
+    const int ci0 = (ti0 >> 1) - 1, cj0 = (tj0 >> 1) - 1;  // coarse origin of the interpolation
 #pragma unroll
     for (int e0 = 0; e0 < E * E; e0 += NT) {
         const int e = e0 + threadIdx.x;
         if (e >= E * E) break;
         const int i = ti0 + e % E, j = tj0 + e / E;
         const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
-        const R av = v ? A.acf(i, j, 0) : R(0);
-        sa[e] = av;
-        sinv[e] = v ? mg_diag_inv<R, CELL>(L, i, j, av, A.facx, A.facy) : R(0);
+        cp_async_el<R>(&sa[e], v ? &A.acf(i, j, 0) : A.acf.p[0], v);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            R val = R(0);
-            if (v) {
-                if (INIT == MG_INIT_VIEW) val = vin(i, j, c);
-                else if (INIT == MG_INIT_INTERP) val = vin(i, j, c) + mg_interp1<R, CELL>(A.crse_in, i, j, c);
+            cp_async_el<R>(&srh[c][e], v ? &A.rhs(i, j, c) : A.rhs.p[c], v);
+            if (INIT == MG_INIT_ZERO) sp[c][e] = R(0);
+            else cp_async_el<R>(&sp[c][e], v ? &vin(i, j, c) : vin.p[c], v);
+        }
+    }
+    if (INIT == MG_INIT_INTERP) {
+        const MGLev& C = A.Lc;
+        for (int e = threadIdx.x; e < EC * EC; e += NT) {
+            const int ic = ci0 + e % EC, jc = cj0 + e / EC;
+            const bool v = ic >= 0 && ic < C.w && jc >= 0 && jc < C.h;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) cp_async_el<R>(&sc[c][e], v ? &A.crse_in(ic, jc, c) : A.crse_in.p[c], v);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // inverse diagonals; the interpolated coarse correction added to the initial guess
+#pragma unroll
+    for (int e0 = 0; e0 < E * E; e0 += NT) {
+        const int e = e0 + threadIdx.x;
+        if (e >= E * E) break;
+        const int i = ti0 + e % E, j = tj0 + e / E;
+        const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
+        sinv[e] = v ? mg_diag_inv<R, CELL>(L, i, j, sa[e], A.facx, A.facy) : R(0);
+        if (INIT == MG_INIT_INTERP && v) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const R* q = sc[c];
+                sp[c][e] = sp[c][e] + mg_interp1f<R, CELL>([&](int ic, int jc) { return q[(jc - cj0) * EC + (ic - ci0)]; }, i, j);
             }
-            sp[c][e] = val;
-            srh[c][e] = v ? A.rhs(i, j, c) : R(0);
         }
     }
     __syncthreads();
@@ -628,7 +679,10 @@ struct RefineSmem {
     static constexpr int H = NSW + 2;
     static constexpr int E = T + 2 * H;
     static constexpr int Q = T + 2;
-    static constexpr size_t bytes() { return (size_t)2 * E * E * sizeof(double) + (size_t)(6 * E * E + 2 * Q * Q) * sizeof(float); }
+    static constexpr int EC = E / 2 + 3;
+    static constexpr size_t bytes() {
+        return (size_t)2 * E * E * sizeof(double) + (size_t)(6 * E * E + 2 * Q * Q + 2 * EC * EC) * sizeof(float);
+    }
 };
 
 template <bool CELL, bool FIRST, int NSW>
@@ -644,6 +698,8 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
     float* sa = fbase + 4 * E * E;                                                            // coefficient
     float* sinv = fbase + 5 * E * E;                                                          // 1 / diagonal
     float (*sr)[Q * Q] = reinterpret_cast<float (*)[Q * Q]>(fbase + 6 * E * E);              // new residual
+    constexpr int EC = SM::EC;
+    float (*sc)[EC * EC] = reinterpret_cast<float (*)[EC * EC]>(fbase + 6 * E * E + 2 * Q * Q);  // coarse
     const MGLev& L = P.lev[0];
     const float facx = P.facx[0], facy = P.facy[0];
     const double dfx = (double)facx, dfy = (double)facy;
@@ -657,6 +713,39 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
     double* xout = P.x64[slot_in ^ (FIRST ? 0 : 1)];
     float* rout = P.r32[slot_in ^ (FIRST ? 0 : 1)];
     auto inside = [&](int i, int j) { return i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j; };
+    const int ci0 = (ti0 >> 1) - 1, cj0 = (tj0 >> 1) - 1;  // coarse origin of the interpolation
+    __syncthreads();
+    // asynchronous copies of everything the tile reads (zero-filled outside the valid box); in
+    // FIRST the FP32 initial guess lands in sd and is widened below
+#pragma unroll
+    for (int e0 = 0; e0 < E * E; e0 += NT) {
+        const int e = e0 + threadIdx.x;
+        if (e >= E * E) break;
+        const int i = ti0 + e % E, j = tj0 + e / E;
+        const bool v = inside(i, j);
+        const size_t id = v ? (size_t)j * L.w + i : 0;
+        cp_async_el<float>(&sa[e], v ? &P.a0(i, j, 0) : P.a0.p[0], v);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (FIRST) {
+                cp_async_el<float>(&sd[c][e], v ? &P.sol(i, j, c) : P.sol.p[c], v);
+                cp_async_el<float>(&srh[c][e], v ? &P.rhs(i, j, c) : P.rhs.p[c], v);  // f for now, r below
+            } else {
+                cp_async_el<double>(&sx[c][e], xin + c * n0 + id, v);
+                cp_async_el<float>(&srh[c][e], rin + c * n0 + id, v);
+            }
+        }
+    }
+    if (!FIRST) {
+        const MGLev& C = P.lev[1];
+        for (int e = threadIdx.x; e < EC * EC; e += NT) {
+            const int ic = ci0 + e % EC, jc = cj0 + e / EC;
+            const bool v = ic >= 0 && ic < C.w && jc >= 0 && jc < C.h;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) cp_async_el<float>(&sc[c][e], v ? &crse(ic, jc, c) : crse.p[c], v);
+        }
+    }
+    cp_async_wait_all();
     __syncthreads();
 #pragma unroll
     for (int e0 = 0; e0 < E * E; e0 += NT) {
@@ -664,20 +753,15 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
         if (e >= E * E) break;
         const int i = ti0 + e % E, j = tj0 + e / E;
         const bool v = inside(i, j);
-        const float av = v ? P.a0(i, j, 0) : 0.f;
-        sa[e] = av;
-        sinv[e] = v ? mg_diag_inv<float, CELL>(L, i, j, av, facx, facy) : 0.f;
+        sinv[e] = v ? mg_diag_inv<float, CELL>(L, i, j, sa[e], facx, facy) : 0.f;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             if (FIRST) {
-                sx[c][e] = v ? (double)P.sol(i, j, c) : 0.0;
+                sx[c][e] = (double)sd[c][e];
                 sd[c][e] = 0.f;
-                srh[c][e] = v ? P.rhs(i, j, c) : 0.f;  // f for now, r below
             } else {
-                const size_t id = (size_t)j * L.w + i;
-                sx[c][e] = v ? xin[c * n0 + id] : 0.0;
-                sd[c][e] = v ? mg_interp1<float, CELL>(crse, i, j, c) : 0.f;
-                srh[c][e] = v ? rin[c * n0 + id] : 0.f;
+                const float* q = sc[c];
+                sd[c][e] = v ? mg_interp1f<float, CELL>([&](int ic, int jc) { return q[(jc - cj0) * EC + (ic - ci0)]; }, i, j) : 0.f;
             }
         }
     }
@@ -815,9 +899,14 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     unsigned int* bar = ctl->mgp_bar;
     int* err = &ctl->mgp_bar_err;
     const int nb = gridDim.x;
-    int nstamp = 0;
+    // trace: [0] count, [1..127] block 0 after each grid barrier; [128] count, [129..255] the
+    // moment the phase's work of block 1 (tiles) or block 0 (coarse levels) is done
+    int nstamp = 0, nwork = 0;
     auto stamp = [&]() {
-        if (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && nstamp < 255) P.trace[1 + nstamp++] = tc_clock_ns();
+        if (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && nstamp < 126) P.trace[1 + nstamp++] = tc_clock_ns();
+    };
+    auto wstamp = [&](int who) {
+        if (P.trace && threadIdx.x == 0 && (int)blockIdx.x == who && nwork < 126) P.trace[129 + nwork++] = tc_clock_ns();
     };
     stamp();
     auto base = [&](int l) {
@@ -892,6 +981,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             for (int t = tb; tile_block && t < nt; t += ntb)
                 mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (it == 0) restrict_acf(l + 1);
+            wstamp(1);
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
@@ -899,6 +989,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         if (blockIdx.x == 0)
             mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
                                      it == 0 || nb == 1);
+        wstamp(1);
         if (!grid_barrier(bar, err)) return;
         stamp();
         // up: levels sb-1 .. 1, interpolation of the coarser correction + 4 sweeps
@@ -911,6 +1002,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             const int nt = ntiles(l, ntx);
             for (int t = tb; tile_block && t < nt; t += ntb)
                 mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+            wstamp(1);
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
@@ -934,6 +1026,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             }
             block_max2(bmax, brhs);
             if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
+            wstamp(1);
         }
         if (!grid_barrier(bar, err)) return;
         stamp();
@@ -959,6 +1052,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         ctl->mg_go = 0;
         if (P.trace) P.trace[0] = nstamp;
     }
+    if (P.trace && blockIdx.x == 1 && threadIdx.x == 0) P.trace[128] = nwork;
     // solution: the last level-0 output (cor[0] after an even number of cycles, else up[0]; the
     // FP64 solution slot it & 1 in single precision)
     const MV<R> fin = (it & 1) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
@@ -1062,14 +1156,22 @@ public:
         if (!trace) return;
         std::vector<unsigned long long> h(256);
         if (cudaMemcpy(h.data(), trace, 256 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) return;
-        const int n = (int)std::min<unsigned long long>(h[0], 255);
-        std::string line = "hpmg phases (us):";
+        const int n = (int)std::min<unsigned long long>(h[0], 126);
+        std::string line = "hpmg phases (us):", work = "hpmg work done at (us):";
         for (int k = 1; k < n; ++k) {
             char buf[32];
             snprintf(buf, sizeof(buf), " %.2f", (double)(h[1 + k] - h[k]) / 1000.0);
             line += buf;
         }
-        fprintf(stderr, "%s\n", line.c_str());
+        // block 1 (or block 0 for the coarse levels) finished the work of phase k at
+        // h[129 + k - 1]; relative to the start of the phase (the previous barrier)
+        const int nw = (int)std::min<unsigned long long>(h[128], 126);
+        for (int k = 1; k < n && k - 1 < nw; ++k) {
+            char buf[32];
+            snprintf(buf, sizeof(buf), " %.2f", ((double)h[129 + k - 1] - (double)h[k]) / 1000.0);
+            work += buf;
+        }
+        fprintf(stderr, "%s\n%s\n", line.c_str(), work.c_str());
     }
 
     template <bool CELL>

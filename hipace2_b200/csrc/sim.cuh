@@ -217,6 +217,28 @@ public:
     bool use_graphs = false;
     bool capturing = false;
     cudaStream_t st2 = nullptr;
+    // side stream of the two forks of a slice (beam deposit | plasma deposit, beam push and
+    // partition | plasma push and copies); not used while profiling, which times kernels serially
+    cudaStream_t sts = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t side_begin() {
+        if (profiling) return st;
+        HPQ_CUDA(cudaEventRecord(ev_fork, st));
+        HPQ_CUDA(cudaStreamWaitEvent(sts, ev_fork, 0));
+        return sts;
+    }
+    void side_end() {
+        if (profiling) return;
+        HPQ_CUDA(cudaEventRecord(ev_join, sts));
+        HPQ_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+    }
+    // launches of the enclosed code go to stream t (every launch site uses the member `st`)
+    struct OnStream {
+        Sim* s;
+        cudaStream_t old;
+        OnStream(Sim* s_, cudaStream_t t) : s(s_), old(s_->st) { s->st = t; }
+        ~OnStream() { s->st = old; }
+    };
     cudaGraph_t slice_graph = nullptr;
     cudaGraphExec_t slice_exec = nullptr;
     long long graph_nodes = 0;
@@ -333,6 +355,11 @@ public:
         invalidate_graph();
         if (st2) cudaStreamDestroy(st2);
         st2 = nullptr;
+        if (sts) cudaStreamDestroy(sts);
+        sts = nullptr;
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        ev_fork = ev_join = nullptr;
         if (st) cudaStreamDestroy(st);
         st = nullptr;
     }
@@ -357,6 +384,9 @@ public:
 
         HPQ_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         HPQ_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        HPQ_CUDA(cudaStreamCreateWithFlags(&sts, cudaStreamNonBlocking));
+        HPQ_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        HPQ_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         // slab
         S.nx = nx; S.ny = ny;
         S.pitch = ((nx + 2 * kGuardAlloc + 7) / 8) * 8;
@@ -371,12 +401,15 @@ public:
         HPQ_CUDA(cudaMemset(ctl, 0, sizeof(Ctl)));
         HPQ_CUDA(cudaMallocHost(&ctl_h, sizeof(Ctl)));
         std::memset(ctl_h, 0, sizeof(Ctl));
-        // Poisson form: HPQ_DST=gemm (SIMT sine GEMMs on every grid, cross-checks), fft, or tc
-        // (tensor-core sine GEMMs, single precision only)
-        if (const char* e = getenv("HPQ_DST")) {
-            const std::string m(e);
-            if (m == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
-            else if (m == "tc") { dst.set_tensor_mode(&ctl->tc_err); pc_dst.set_tensor_mode(&ctl->tc_err); }
+        // Poisson form: single precision uses the tensor-core sine GEMMs unless HPQ_DST=fft
+        // (FP32 FFT on 2^k - 1 grids) or gemm (SIMT sine GEMMs on every grid, cross-checks);
+        // double precision uses the FFT where the grid allows it, else the SIMT GEMMs
+        const char* env = getenv("HPQ_DST");
+        const std::string dmode = env ? env : "";
+        if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
+        else if (dmode != "fft" && std::is_same<R, float>::value) {
+            dst.set_tensor_mode(&ctl->tc_err);
+            pc_dst.set_tensor_mode(&ctl->tc_err);
         }
         init_plasma_lattices();
         // beams: fixed_ppc generated here, fixed_weight drawn from the seeded generator unless
@@ -913,20 +946,26 @@ public:
         if (ex) {
             if (cfg.deposit_rho) zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB, C_RHO});
             else zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB});
+            // beam deposits (own components) run beside the plasma deposit
+            {
+                OnStream on(this, side_begin());
+                // jz_beam of this slice and jx_beam/jy_beam of the next slice (the reference
+                // deposits the latter after the Psi/Ez/Bz solve, Hipace.cpp:656-657; the two are
+                // independent)
+                for (size_t b = 0; b < bm.size(); ++b) {
+                    Scope sc(this, "beam_deposit");
+                    const bool nj = cfg.do_beam_jx_jy_deposition;
+                    hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st,
+                        bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
+                        nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det);
+                    HPQ_LAUNCH_CHECK();
+                    det_flush({C_JZB, C_RHOMJZB, C_NJXB, C_NJYB});
+                }
+            }
             for (size_t s = 0; s < pl.size(); ++s)
                 deposit_plasma((int)s, S.c(C_JX).p, S.c(C_JY).p, nullptr, cfg.deposit_rho ? S.c(C_RHO).p : nullptr,
                                S.c(C_CHI).p, S.c(C_RHOMJZ).p);
-            // jz_beam of this slice and jx_beam/jy_beam of the next slice (the reference deposits
-            // the latter after the Psi/Ez/Bz solve, Hipace.cpp:656-657; the two are independent)
-            for (size_t b = 0; b < bm.size(); ++b) {
-                Scope sc(this, "beam_deposit");
-                const bool nj = cfg.do_beam_jx_jy_deposition;
-                hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st, 
-                    bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
-                    nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det);
-                HPQ_LAUNCH_CHECK();
-                det_flush({C_JZB, C_RHOMJZB, C_NJXB, C_NJYB});
-            }
+            side_end();
         } else {
             if (cfg.deposit_rho) zero({C_EXMBY, C_EYPBX, C_JX, C_JY, C_JZ, C_RHOMJZ, C_RHO});
             else zero({C_EXMBY, C_EYPBX, C_JX, C_JY, C_JZ, C_RHOMJZ});
@@ -958,20 +997,25 @@ public:
             hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)nx * ny * diag_list.n, 256)), dim3(256), 0, st, S, ctl, diag_list, diag_buf, nz);
             HPQ_LAUNCH_CHECK();
         }
+        // the beam push and partition (beam arrays, Ctl) run beside the plasma push and the
+        // component shifts (plasma arrays, slab planes the pushes do not read)
+        {
+            OnStream on(this, side_begin());
+            for (size_t b = 0; b < bm.size(); ++b) {
+                {
+                    Scope sc(this, "beam_push");
+                    hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, S, g, cfg.dt);
+                    HPQ_LAUNCH_CHECK();
+                }
+                Scope sc2(this, "beam_partition");
+                hpq_launch(k_beam_partition, dim3(1), dim3(1024), 0, st, bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
+                HPQ_LAUNCH_CHECK();
+            }
+        }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "plasma_push");
             hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 0, (const int*)nullptr);
-            HPQ_LAUNCH_CHECK();
-        }
-        for (size_t b = 0; b < bm.size(); ++b) {
-            {
-                Scope sc(this, "beam_push");
-                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, S, g, cfg.dt);
-                HPQ_LAUNCH_CHECK();
-            }
-            Scope sc2(this, "beam_partition");
-            hpq_launch(k_beam_partition, dim3(1), dim3(1024), 0, st, bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
             HPQ_LAUNCH_CHECK();
         }
         if (ex) {
@@ -979,6 +1023,7 @@ public:
         } else {
             copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
         }
+        side_end();
         if (bm.empty()) {
             hpq_launch(k_slice_done, dim3(1), dim3(1), 0, st, ctl);
             HPQ_LAUNCH_CHECK();

