@@ -27,23 +27,62 @@ struct DstCfg {
     static constexpr int RB = M <= 2048 ? 4 : 2;
 };
 
-template <class R, int M>
+template <class R>
+__device__ __forceinline__ Cx<R> cmul(const Cx<R>& v0, const Cx<R>& w) {
+    return {v0.re * w.re - v0.im * w.im, v0.re * w.im + v0.im * w.re};
+}
+
+// In-place radix-2 DIT FFT of nfft rows of length M held in bit-reversed order. Pairs of
+// consecutive radix-2 stages (lengths 2h and 4h) are done by one thread on 4 elements (a
+// radix-4 step with the same operations as the two radix-2 stages), so a length-2^k transform
+// needs ceil(k/2) block barriers instead of k; stage sizes are compile-time, indices are shifts.
+template <class R, int M, int LOGM>
 __device__ __forceinline__ void fft_block(Cx<R>* z, int nfft, const Cx<R>* __restrict__ tw) {
-    for (int len = 2; len <= M; len <<= 1) {
-        const int half = len >> 1, stride = M / len;
+    static_assert((1 << LOGM) == M, "M = 2^LOGM");
+    int s = 0;  // stage length 2h with h = 2^s
+    if (LOGM & 1) {
         for (int t = threadIdx.x; t < nfft * (M / 2); t += blockDim.x) {
-            const int f = t / (M / 2), b = t - f * (M / 2);
-            const int grp = b / half, pos = b - grp * half;
+            const int f = t >> (LOGM - 1), b = t & (M / 2 - 1);
             Cx<R>* zz = z + f * M;
-            const int i0 = grp * len + pos, i1 = i0 + half;
-            const Cx<R> w = tw[pos * stride];
-            const Cx<R> u = zz[i0], v0 = zz[i1];
-            const Cx<R> v{v0.re * w.re - v0.im * w.im, v0.re * w.im + v0.im * w.re};
+            const int i0 = 2 * b, i1 = i0 + 1;
+            const Cx<R> w = tw[0];
+            const Cx<R> u = zz[i0], v = cmul(zz[i1], w);
             zz[i0] = {u.re + v.re, u.im + v.im};
             zz[i1] = {u.re - v.re, u.im - v.im};
         }
         __syncthreads();
+        s = 1;
     }
+#pragma unroll
+    for (int ss = LOGM & 1; ss < LOGM; ss += 2) {
+        s = ss;
+        const int h = 1 << s;
+        for (int t = threadIdx.x; t < nfft * (M / 4); t += blockDim.x) {
+            const int f = t >> (LOGM - 2), b = t & (M / 4 - 1);
+            const int grp = b >> s, pos = b & (h - 1);
+            Cx<R>* zz = z + f * M;
+            const int i0 = grp * 4 * h + pos, i1 = i0 + h, i2 = i0 + 2 * h, i3 = i0 + 3 * h;
+            const Cx<R> wa = tw[pos * (M / (2 * h))];
+            const Cx<R> wb0 = tw[pos * (M / (4 * h))], wb1 = tw[(pos + h) * (M / (4 * h))];
+            Cx<R> x0 = zz[i0], x1 = zz[i1], x2 = zz[i2], x3 = zz[i3];
+            // stage of length 2h: (i0, i1) and (i2, i3)
+            Cx<R> v = cmul(x1, wa);
+            x1 = {x0.re - v.re, x0.im - v.im};
+            x0 = {x0.re + v.re, x0.im + v.im};
+            v = cmul(x3, wa);
+            x3 = {x2.re - v.re, x2.im - v.im};
+            x2 = {x2.re + v.re, x2.im + v.im};
+            // stage of length 4h: (i0, i2) and (i1, i3)
+            v = cmul(x2, wb0);
+            zz[i2] = {x0.re - v.re, x0.im - v.im};
+            zz[i0] = {x0.re + v.re, x0.im + v.im};
+            v = cmul(x3, wb1);
+            zz[i3] = {x1.re - v.re, x1.im - v.im};
+            zz[i1] = {x1.re + v.re, x1.im + v.im};
+        }
+        __syncthreads();
+    }
+    (void)s;
 }
 
 template <int LOGM>
@@ -83,7 +122,7 @@ __global__ void __launch_bounds__(256) k_dst_pass_t(const R* __restrict__ in, in
     const int r0 = blockIdx.x * RB;
     auto get = [&](int r, int e) -> R { const int row = r0 + r; return row < nrows ? in[(size_t)row * n + e] : R(0); };
     load_odd<R, M, LOGM>(z, RB / 2, n, get);
-    fft_block<R, M>(z, RB / 2, tw);
+    fft_block<R, M, LOGM>(z, RB / 2, tw);
     for (int t = threadIdx.x; t < RB * n; t += blockDim.x) {
         const int r = t % RB, e = t / RB;
         const int row = r0 + r;
@@ -107,7 +146,7 @@ __global__ void __launch_bounds__(256) k_dst_pass_eig(const R* __restrict__ in, 
     const int r0 = blockIdx.x * RB;
     auto get = [&](int r, int e) -> R { const int row = r0 + r; return row < nrows ? in[(size_t)row * n + e] : R(0); };
     load_odd<R, M, LOGM>(z, RB / 2, n, get);
-    fft_block<R, M>(z, RB / 2, tw);
+    fft_block<R, M, LOGM>(z, RB / 2, tw);
     for (int t = threadIdx.x; t < RB * n; t += blockDim.x) {
         const int r = t / n, e = t - r * n;
         const int row = r0 + r;
@@ -117,7 +156,7 @@ __global__ void __launch_bounds__(256) k_dst_pass_eig(const R* __restrict__ in, 
     __syncthreads();
     auto get2 = [&](int r, int e) -> R { return tmp[r * n + e]; };
     load_odd<R, M, LOGM>(z, RB / 2, n, get2);
-    fft_block<R, M>(z, RB / 2, tw);
+    fft_block<R, M, LOGM>(z, RB / 2, tw);
     for (int t = threadIdx.x; t < RB * n; t += blockDim.x) {
         const int r = t % RB, e = t / RB;
         const int row = r0 + r;
@@ -139,7 +178,7 @@ __global__ void __launch_bounds__(256) k_dst_pass_field(const R* __restrict__ in
     const int r0 = blockIdx.x * RB;
     auto get = [&](int r, int e) -> R { const int row = r0 + r; return row < nrows ? in[(size_t)row * n + e] : R(0); };
     load_odd<R, M, LOGM>(z, RB / 2, n, get);
-    fft_block<R, M>(z, RB / 2, tw);
+    fft_block<R, M, LOGM>(z, RB / 2, tw);
     for (int t = threadIdx.x; t < RB * n; t += blockDim.x) {
         const int r = t / n, e = t - r * n;
         const int row = r0 + r;
