@@ -599,6 +599,19 @@ __device__ __forceinline__ void copy_particle(const BeamBuf& d, long long di, co
     d.id[di] = s.id[si]; d.nsub[di] = nsub; d.valid[di] = 1;
 }
 
+// initial store of a beam: dst[k] = src[perm[k]] (the host's stable slice binning order)
+__global__ void k_beam_gather(BeamBuf dst, const BeamBuf src, const int* __restrict__ perm, long long n, int has_id) {
+    HPQ_PDL_ENTRY();
+    for (long long k = gtid(); k < n; k += gstride()) {
+        const int i = perm[k];
+        dst.x[k] = src.x[i]; dst.y[k] = src.y[i]; dst.z[k] = src.z[i]; dst.w[k] = src.w[i];
+        dst.ux[k] = src.ux[i]; dst.uy[k] = src.uy[i]; dst.uz[k] = src.uz[i];
+        dst.id[k] = has_id ? src.id[i] : (long long)i + 1;
+        dst.nsub[k] = 0;
+        dst.valid[k] = src.w[i] != 0.0;
+    }
+}
+
 __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, int bi, Geo g, int keep_store,
                                                          int end_slice) {
     HPQ_PDL_ENTRY();

@@ -619,15 +619,18 @@ public:
     }
 
     // BoxSort (BoxSort.cpp:14-78): slice = int((z - lo) / dz); particles outside [0, nz) are
-    // dropped; stable within a slice. Slices are stored top-down like the slice march.
-    void upload_beam(int b, const HostBeam& hb) {
+    // dropped; stable within a slice. Slices are stored top-down like the slice march. The host
+    // computes only the order (a counting sort of indices); the particle data go to the device
+    // as they are (from the caller's buffers, pinned or not) and are gathered there.
+    void upload_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
+                     const double* uy, const double* uz, const long long* id, long long nin) {
         BeamDev& d = bm[b];
         const BeamSpecies& B = cfg.beams[b];
         d.charge = B.charge; d.mass = B.mass; d.n_subcycles = B.n_subcycles; d.do_z_push = B.do_z_push;
-        std::vector<int> sl(hb.size());
+        std::vector<int> sl((size_t)nin);
         std::vector<int> cnt(nz, 0);
-        for (size_t i = 0; i < hb.size(); ++i) {
-            const int s = (int)((hb.z[i] - cfg.prob_lo[2]) * g.dxi[2]);
+        for (long long i = 0; i < nin; ++i) {
+            const int s = (int)((z[i] - cfg.prob_lo[2]) * g.dxi[2]);
             sl[i] = (s < 0 || s >= nz) ? -1 : s;
             if (sl[i] >= 0) cnt[sl[i]]++;
         }
@@ -635,11 +638,12 @@ public:
         long long acc = 0;
         for (int s = nz - 1; s >= 0; --s) { start[s] = (int)acc; acc += cnt[s]; }
         const long long n = acc;
+        if (nin > INT32_MAX) throw InputError("beam too large");
         // device buffers are kept when the new beam fits (captured slice graphs stay valid)
-        if (d.buf[0].x == nullptr || n > d.cap) {
+        if (d.buf[0].x == nullptr || nin > d.cap) {
             free_beam(d);
             invalidate_graph();
-            d.cap = std::max<long long>(n, 1);
+            d.cap = std::max<long long>(nin, 1);
             for (int q = 0; q < 2; ++q) {
                 alloc_buf(d.buf[q], d.cap);
                 alloc_buf(d.carry[q], d.cap);
@@ -647,44 +651,47 @@ public:
                 HPQ_CUDA(cudaMalloc(&d.count[q], nz * sizeof(int)));
             }
         }
+        std::vector<int> perm((size_t)std::max<long long>(n, 1));
+        {
+            std::vector<int> pos(start);
+            for (long long i = 0; i < nin; ++i)
+                if (sl[i] >= 0) perm[pos[sl[i]]++] = (int)i;
+        }
         for (int q = 0; q < 2; ++q) {
-            HPQ_CUDA(cudaMemset(d.start[q], 0, nz * sizeof(int)));
-            HPQ_CUDA(cudaMemset(d.count[q], 0, nz * sizeof(int)));
+            HPQ_CUDA(cudaMemsetAsync(d.start[q], 0, nz * sizeof(int), st));
+            HPQ_CUDA(cudaMemsetAsync(d.count[q], 0, nz * sizeof(int), st));
         }
-        std::vector<double> a[7];
-        for (auto& v : a) v.resize(n);
-        std::vector<long long> ids(n);
-        std::vector<int> nsub(n, 0);
-        std::vector<uint8_t> valid(n);
-        std::vector<int> pos(start);
-        for (size_t i = 0; i < hb.size(); ++i) {
-            if (sl[i] < 0) continue;
-            const int k = pos[sl[i]]++;
-            a[0][k] = hb.x[i]; a[1][k] = hb.y[i]; a[2][k] = hb.z[i]; a[3][k] = hb.w[i];
-            a[4][k] = hb.ux[i]; a[5][k] = hb.uy[i]; a[6][k] = hb.uz[i];
-            ids[k] = hb.id[i];
-            valid[k] = hb.w[i] != 0.0;
+        // the carry buffers are free between steps: carry[0] stages the input arrays, the sub-cycle
+        // array of carry[1] the order
+        const BeamBuf& sg = d.carry[0];
+        if (nin > 0) {
+            const double* src[7] = {x, y, z, w, ux, uy, uz};
+            double* dstp[7] = {sg.x, sg.y, sg.z, sg.w, sg.ux, sg.uy, sg.uz};
+            for (int k = 0; k < 7; ++k)
+                HPQ_CUDA(cudaMemcpyAsync(dstp[k], src[k], nin * sizeof(double), cudaMemcpyHostToDevice, st));
+            if (id) HPQ_CUDA(cudaMemcpyAsync(sg.id, id, nin * sizeof(long long), cudaMemcpyHostToDevice, st));
         }
-        const int q = parity;
-        double* dp[7] = {d.buf[q].x, d.buf[q].y, d.buf[q].z, d.buf[q].w, d.buf[q].ux, d.buf[q].uy, d.buf[q].uz};
         if (n > 0) {
-            for (int k = 0; k < 7; ++k) HPQ_CUDA(cudaMemcpy(dp[k], a[k].data(), n * sizeof(double), cudaMemcpyHostToDevice));
-            HPQ_CUDA(cudaMemcpy(d.buf[q].id, ids.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
-            HPQ_CUDA(cudaMemcpy(d.buf[q].nsub, nsub.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-            HPQ_CUDA(cudaMemcpy(d.buf[q].valid, valid.data(), n, cudaMemcpyHostToDevice));
+            HPQ_CUDA(cudaMemcpyAsync(d.carry[1].nsub, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+            hpq_launch(k_beam_gather, dim3(blocks_for(n, 256)), dim3(256), 0, st, d.buf[parity], (const BeamBuf)sg,
+                       (const int*)d.carry[1].nsub, n, id ? 1 : 0);
+            HPQ_LAUNCH_CHECK();
         }
-        HPQ_CUDA(cudaMemcpy(d.start[q], start.data(), nz * sizeof(int), cudaMemcpyHostToDevice));
-        HPQ_CUDA(cudaMemcpy(d.count[q], cnt.data(), nz * sizeof(int), cudaMemcpyHostToDevice));
+        HPQ_CUDA(cudaMemcpyAsync(d.start[parity], start.data(), nz * sizeof(int), cudaMemcpyHostToDevice, st));
+        HPQ_CUDA(cudaMemcpyAsync(d.count[parity], cnt.data(), nz * sizeof(int), cudaMemcpyHostToDevice, st));
+        HPQ_CUDA(cudaStreamSynchronize(st));  // the caller's buffers and the host vectors are released
         st_host.beam_particles = 0;
+    }
+    void upload_beam(int b, const HostBeam& hb) {
+        upload_beam(b, hb.x.data(), hb.y.data(), hb.z.data(), hb.w.data(), hb.ux.data(), hb.uy.data(), hb.uz.data(),
+                    hb.id.data(), (long long)hb.size());
     }
 
     void set_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
                   const double* uy, const double* uz, const long long* id, long long n) override {
         if (b < 0 || b >= (int)cfg.beams.size()) throw InputError("beam index out of range");
-        HostBeam hb;
-        for (long long i = 0; i < n; ++i) hb.push(x[i], y[i], z[i], w[i], ux[i], uy[i], uz[i], id ? id[i] : i + 1);
         HPQ_CUDA(cudaStreamSynchronize(st));
-        upload_beam(b, hb);
+        upload_beam(b, x, y, z, w, ux, uy, uz, id, n);
     }
 
     long long beam_count(int b) override {
@@ -704,12 +711,29 @@ public:
         HPQ_CUDA(cudaMemcpy(cnt.data(), d.count[parity], nz * sizeof(int), cudaMemcpyDeviceToHost));
         HPQ_CUDA(cudaMemcpy(start.data(), d.start[parity], nz * sizeof(int), cudaMemcpyDeviceToHost));
         const BeamBuf& s = d.buf[parity];
+        double* outs[7] = {x, y, z, w, ux, uy, uz};
+        double* ins[7] = {s.x, s.y, s.z, s.w, s.ux, s.uy, s.uz};
+        // the slices of a store are consecutive (top-down, no gaps): one copy per array
+        bool contiguous = true;
+        long long total = 0;
+        for (int sl = nz - 1; sl >= 0; --sl) {
+            if (cnt[sl] && start[sl] != start[nz - 1] + total) contiguous = false;
+            total += cnt[sl];
+        }
+        if (contiguous) {
+            if (total > 0) {
+                const size_t o = start[nz - 1];
+                for (int a = 0; a < 7; ++a)
+                    HPQ_CUDA(cudaMemcpyAsync(outs[a], ins[a] + o, total * sizeof(double), cudaMemcpyDeviceToHost, st));
+                if (id) HPQ_CUDA(cudaMemcpyAsync(id, s.id + o, total * sizeof(long long), cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaStreamSynchronize(st));
+            }
+            return;
+        }
         long long k = 0;
         for (int sl = nz - 1; sl >= 0; --sl) {
             const size_t n = cnt[sl], o = start[sl];
             if (!n) continue;
-            double* outs[7] = {x, y, z, w, ux, uy, uz};
-            double* ins[7] = {s.x, s.y, s.z, s.w, s.ux, s.uy, s.uz};
             for (int a = 0; a < 7; ++a) HPQ_CUDA(cudaMemcpy(outs[a] + k, ins[a] + o, n * sizeof(double), cudaMemcpyDeviceToHost));
             if (id) HPQ_CUDA(cudaMemcpy(id + k, s.id + o, n * sizeof(long long), cudaMemcpyDeviceToHost));
             k += n;
