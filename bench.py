@@ -317,15 +317,34 @@ def mixed_vs_fp64(text, args, torch):
     return out
 
 
-def scale_point(name, torch):
-    """One step of a larger workload in FP64 and in mixed precision (device time)."""
+def scale_point(name, torch, sample_every=64):
+    """One step of a larger workload in FP64 and in mixed precision (device time), and the mixed
+    error against the FP64 GPU path on identical inputs (step 0, every `sample_every`-th slice
+    read back through the per-slice surface; a full 3-D diagnostic would be 8 GB per component)."""
+    import numpy as np
     from cases import config
     text = config(name)
     res = {"workload": name}
+    comps = ["Ez", "Psi", "jz_beam", "Bx"]
+    samples = {}
+    beam = None
     for prec in ("fp64", "mixed"):
         sim = make_sim(text, prec, graphs=True)
+        if beam is None:
+            beam = sim.get_beam(0)
+        else:
+            sim.set_beam(0, beam)
         nz = sim.n_cell[2]
-        sim.step(0)
+        # step 0 slice by slice, sampling fields
+        got = {c: [] for c in comps}
+        sim.begin_step(0)
+        for s in range(nz - 1, -1, -1):
+            sim.solve_one_slice(s)
+            if s % sample_every == 0:
+                for c in comps:
+                    got[c].append(sim.get_field(c))
+        sim.end_step()
+        samples[prec] = {c: np.array(v) for c, v in got.items()}
         secs = time_device_steps(sim, 1, 1, torch)
         res[prec + "_slices_per_s"] = nz / secs
         res[prec + "_ms_per_step"] = secs * 1e3
@@ -334,6 +353,10 @@ def scale_point(name, torch):
             res["plasma_particles"] = int(sim.get_plasma(0)["x"].size)
         sim.close()
     res["mixed_speedup"] = res["mixed_slices_per_s"] / res["fp64_slices_per_s"]
+    for c in comps:
+        a, b = samples["mixed"][c], samples["fp64"][c]
+        res[c + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    res["error_reference"] = "FP64 GPU path, same beam, step 0, every %d-th slice" % sample_every
     return res
 
 

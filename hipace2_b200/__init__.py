@@ -22,7 +22,7 @@ ERRORS = {1: "input", 2: "cuda", 3: "state", 4: "not converged", 5: "diverged", 
 EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "hpq_set_precision",
            "hpq_init", "hpq_set_beam", "hpq_beam_count", "hpq_get_beam", "hpq_step",
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
-           "hpq_get_diag", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
+           "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
            "hpq_get_profile", "hpq_poisson_dirichlet_noalloc")
 
@@ -68,6 +68,8 @@ def load_library(path=None):
         "hpq_get_plasma": ([vp, i32, dp], i32),
         "hpq_set_graphs": ([vp, i32], i32),
         "hpq_set_deterministic": ([vp, i32], i32),
+        "hpq_insitu_size": ([vp, cp, ctypes.POINTER(ctypes.c_int64)], i32),
+        "hpq_get_insitu": ([vp, cp, dp], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
         "hpq_get_counters": ([vp, lp, lp, lp, lp], i32),
@@ -94,6 +96,25 @@ def _lp(a):
 BEAM_ATTRS = ("x", "y", "z", "w", "ux", "uy", "uz")
 PLASMA_ATTRS = ("x", "y", "w", "ux", "uy", "psi", "x_prev", "y_prev", "ux_half_step",
                 "uy_half_step", "psi_half_step", "valid")
+
+
+INSITU_BEAM = ("sum(w)", "[x]", "[x^2]", "[y]", "[y^2]", "[z]", "[z^2]", "[ux]", "[ux^2]", "[uy]", "[uy^2]",
+               "[uz]", "[uz^2]", "[x*ux]", "[y*uy]", "[z*uz]", "[x*uy]", "[y*ux]", "[ux/uz]", "[uy/uz]", "[ga]",
+               "[ga^2]")
+INSITU_FIELDS = ("[Ex^2]", "[Ey^2]", "[Ez^2]", "[Bx^2]", "[By^2]", "[Bz^2]", "[ExmBy^2]", "[EypBx^2]",
+                 "[jz_beam]", "[Ez*jz_beam]")
+
+
+def split_insitu(what, flat, nz):
+    """Flat in-situ array (hpq_get_insitu layout) -> dict of per-slice arrays and totals."""
+    names = INSITU_FIELDS if what == "fields" else INSITU_BEAM
+    d = {k: flat[i * nz:(i + 1) * nz] for i, k in enumerate(names)}
+    off = len(names) * nz
+    if what != "fields":
+        d["Np"] = flat[off:off + nz]
+        off += nz
+    d["sum"] = flat[off:]
+    return d
 
 
 class Hipace:
@@ -178,6 +199,15 @@ class Hipace:
         out = np.zeros((nz, ny, nx))
         self._check(self.L.hpq_get_diag(self.h, comp.encode(), _dp(out)))
         return out
+
+    def get_insitu(self, what):
+        """Reduced in-situ diagnostics of the last diagnostic step of a beam or of "fields" (see
+        hpq_get_insitu), split into the reference's named arrays."""
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_insitu_size(self.h, what.encode(), ctypes.byref(n)))
+        out = np.zeros(n.value)
+        self._check(self.L.hpq_get_insitu(self.h, what.encode(), _dp(out)))
+        return split_insitu(what, out, self.n_cell[2])
 
     def get_plasma(self, sp=0):
         n = ctypes.c_int64()

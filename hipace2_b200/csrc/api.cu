@@ -197,6 +197,28 @@ int hpq_get_diag(hpq_handle* h, const char* comp, double* out) {
     });
 }
 
+int hpq_insitu_size(hpq_handle* h, const char* what, int64_t* n) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!what || !n) return (int)HPQ_ERR_ARG;
+        const long long k = h->sim->insitu_size(what);
+        if (k < 0) { h->err = std::string("no in-situ diagnostic '") + what + "'"; return (int)HPQ_ERR_ARG; }
+        *n = k;
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_get_insitu(hpq_handle* h, const char* what, double* out) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!what || !out) return (int)HPQ_ERR_ARG;
+        if (h->in_step) { h->err = "hpq_get_insitu inside a step"; return (int)HPQ_ERR_STATE; }
+        if (h->sim->insitu_size(what) < 0) { h->err = std::string("no in-situ diagnostic '") + what + "'"; return (int)HPQ_ERR_ARG; }
+        if (!h->sim->get_insitu(what, out)) { h->err = "no diagnostic step has run yet"; return (int)HPQ_ERR_STATE; }
+        return (int)HPQ_OK;
+    });
+}
+
 int hpq_plasma_count(hpq_handle* h, int sp, int64_t* n) {
     return guarded(h, [&] {
         if (int r = need_init(h)) return r;

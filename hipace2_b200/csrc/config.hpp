@@ -69,6 +69,9 @@ struct BeamSpecies {
     bool do_z_push = true;
     int n_subcycles = 10;
     double min_density = 0;
+    // in-situ diagnostics (BeamParticleContainer.cpp:61-63, 476-548)
+    int insitu_period = 0;
+    double insitu_radius = 1e300;
 };
 
 struct SimConfig {
@@ -98,6 +101,7 @@ struct SimConfig {
     bool do_beam_jx_jy_deposition = true;
     bool do_beam_jz_minus_rho = false;
     bool deposit_rho = false;
+    int fields_insitu_period = 0;  // fields.insitu_period (Fields.cpp:41, 1289-1346)
     std::vector<PlasmaSpecies> plasmas;
     std::vector<BeamSpecies> beams;
     bool any_neutralize_background() const {
@@ -105,6 +109,11 @@ struct SimConfig {
         return false;
     }
 };
+
+// utils::doDiagnostics (IOUtil.cpp:75-82)
+inline bool do_diagnostics(int period, int step, int max_step, double time, double max_time) {
+    return period > 0 && (time == max_time || step == max_step || step % period == 0);
+}
 
 namespace detail {
 inline bool query_alt_str(const InputStore& in, const std::string& name, const std::string& alt,
@@ -167,6 +176,7 @@ inline SimConfig build_config(const InputStore& in) {
         throw InputError("Particle boundary must be contained within the simulation domain");
 
     in.query("max_step", c.max_step);
+    in.query("fields.insitu_period", c.fields_insitu_period);
     std::string dts;
     if (in.query_str("hipace.dt", dts)) {
         if (dts == "adaptive") throw InputError("hipace.dt = adaptive is not supported");
@@ -286,6 +296,8 @@ inline SimConfig build_config(const InputStore& in) {
         if (b.n_subcycles < 1) throw InputError("n_subcycles must be >= 1");
         in.query_bool(name + ".do_z_push", b.do_z_push);
         in.query(name + ".duz_per_uz0_dzeta", b.duz_per_uz0_dzeta);
+        query_alt(in, name, "beams", "insitu_period", b.insitu_period);
+        query_alt(in, name, "beams", "insitu_radius", b.insitu_radius);
         reject(in, name + ".do_salame", "SALAME is outside the slice loop");
         reject(in, name + ".do_spin_tracking", "spin tracking is outside the slice loop");
         reject(in, name + ".do_radiation_reaction", "radiation reaction is outside the slice loop");
@@ -369,6 +381,8 @@ inline SimConfig build_config(const InputStore& in) {
         }
         c.beams.push_back(b);
     }
+    if (c.fields_insitu_period > 0 && !c.explicit_solver)
+        throw InputError("Must use explicit solver for field insitu diagnostic");
     return c;
 }
 

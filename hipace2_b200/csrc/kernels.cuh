@@ -88,6 +88,9 @@ struct Ctl {
     unsigned int mgp_bar[2];
     int mgp_bar_err, mgp_pad;
     int tc_err, tc_pad;  // error code of the tensor-core DST kernels (a timed-out wait)
+    // in-situ reductions on this step (set when the step begins)
+    int insitu_beam[kMaxBeams];
+    int insitu_fields, insitu_pad;
 };
 
 struct Geo {
@@ -597,6 +600,81 @@ __device__ __forceinline__ void copy_particle(const BeamBuf& d, long long di, co
     d.x[di] = s.x[si]; d.y[di] = s.y[si]; d.z[di] = s.z[si]; d.w[di] = s.w[si];
     d.ux[di] = s.ux[si]; d.uy[di] = s.uy[si]; d.uz[di] = s.uz[si];
     d.id[di] = s.id[si]; d.nsub[di] = nsub; d.valid[di] = 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// In-situ reductions (BeamParticleContainer.cpp:476-548, Fields.cpp:1289-1346), one block per
+// slice so that the sums are taken in a fixed order (bit-identical run to run). Raw sums per
+// slice go to out[islice * NV + k]; the host normalises them.
+// ------------------------------------------------------------------------------------------
+template <int NV>
+__device__ __forceinline__ void block_sum_store(double (&a)[NV], double* out) {
+    __shared__ double ws[32][NV];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int d = 16; d > 0; d >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], d);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) ws[warp][k] = a[k];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+}
+
+// beam "This" slice: the slice's own particles and those that slipped in from the previous slice
+__global__ void __launch_bounds__(1024) k_beam_insitu(BeamDev B, const Ctl* __restrict__ ctl, int bi, double r2,
+                                                      double clight_inv, double* out) {
+    HPQ_PDL_ENTRY();
+    if (!ctl->insitu_beam[bi]) return;
+    const int s = ctl->islice;
+    const int par = ctl->step_parity;
+    const int start = B.start[par][s], na = B.count[par][s];
+    const int cin = (s + 1) & 1;
+    const int nc = ctl->carry_n[bi][cin];
+    double a[23];
+#pragma unroll
+    for (int k = 0; k < 23; ++k) a[k] = 0;
+    for (int k = threadIdx.x; k < na + nc; k += blockDim.x) {
+        const BeamBuf& bb = k < na ? B.buf[par] : B.carry[cin];
+        const long long ip = k < na ? start + k : k - na;
+        const double x = bb.x[ip], y = bb.y[ip];
+        if (!bb.valid[ip] || x * x + y * y > r2) continue;
+        const double z = bb.z[ip], w = bb.w[ip];
+        const double ux = bb.ux[ip] * clight_inv, uy = bb.uy[ip] * clight_inv, uz = bb.uz[ip] * clight_inv;
+        const double uz_inv = uz == 0. ? 0. : 1. / uz;
+        const double gamma = sqrt(1.0 + ux * ux + uy * uy + uz * uz);
+        a[0] += w; a[1] += w * x; a[2] += w * x * x; a[3] += w * y; a[4] += w * y * y; a[5] += w * z;
+        a[6] += w * z * z; a[7] += w * ux; a[8] += w * ux * ux; a[9] += w * uy; a[10] += w * uy * uy;
+        a[11] += w * uz; a[12] += w * uz * uz; a[13] += w * x * ux; a[14] += w * y * uy; a[15] += w * z * uz;
+        a[16] += w * x * uy; a[17] += w * y * ux; a[18] += w * ux * uz_inv; a[19] += w * uy * uz_inv;
+        a[20] += w * gamma; a[21] += w * gamma * gamma; a[22] += 1.0;
+    }
+    block_sum_store<23>(a, out + (size_t)s * 23);
+}
+
+template <class R>
+__global__ void __launch_bounds__(1024) k_field_insitu(Slab<R> S, const Ctl* __restrict__ ctl, double clight,
+                                                       double* out) {
+    HPQ_PDL_ENTRY();
+    if (!ctl->insitu_fields) return;
+    const F2<R> ex = S.c(C_EXMBY), ey = S.c(C_EYPBX), ez = S.c(C_EZ), bx = S.c(C_BX), by = S.c(C_BY), bz = S.c(C_BZ),
+                jzb = S.c(C_JZB);
+    double a[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) a[k] = 0;
+    for (int k = threadIdx.x; k < S.nx * S.ny; k += blockDim.x) {
+        const int i = k % S.nx, j = k / S.nx;
+        const double vex = ex(i, j), vey = ey(i, j), vez = ez(i, j), vbx = bx(i, j), vby = by(i, j), vbz = bz(i, j),
+                     vj = jzb(i, j);
+        const double t0 = vex + vby * clight, t1 = vey - vbx * clight;
+        a[0] += t0 * t0; a[1] += t1 * t1; a[2] += vez * vez; a[3] += vbx * vbx; a[4] += vby * vby; a[5] += vbz * vbz;
+        a[6] += vex * vex; a[7] += vey * vey; a[8] += vj; a[9] += vez * vj;
+    }
+    block_sum_store<10>(a, out + (size_t)ctl->islice * 10);
 }
 
 // initial store of a beam: dst[k] = src[perm[k]] (the host's stable slice binning order)

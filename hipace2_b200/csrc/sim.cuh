@@ -62,6 +62,9 @@ public:
     virtual Stats stats() = 0;
     virtual void set_graphs(bool on) = 0;
     virtual void set_deterministic(bool on) = 0;
+    // in-situ data of the last diagnostic step ("fields" or a beam name); size < 0: unknown name
+    virtual long long insitu_size(const std::string& what) = 0;
+    virtual bool get_insitu(const std::string& what, double* out) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual bool get_profile(const std::string& name, double* ms, long long* n) = 0;
     virtual std::string profile_names() = 0;
@@ -339,6 +342,10 @@ public:
         px0.clear(); py0.clear();
         for (auto& b : bm) free_beam(b);
         bm.clear();
+        for (double* p : insitu_beam_d) if (p) cudaFree(p);
+        insitu_beam_d.clear();
+        if (insitu_fields_d) cudaFree(insitu_fields_d);
+        insitu_fields_d = nullptr;
         if (det_mem) cudaFree(det_mem);
         det_mem = nullptr;
         det = DetAcc{};
@@ -412,6 +419,7 @@ public:
             pc_dst.set_tensor_mode(&ctl->tc_err);
         }
         init_plasma_lattices();
+        insitu_alloc();
         // beams: fixed_ppc generated here, fixed_weight drawn from the seeded generator unless
         // the caller provides particles with set_beam before the first step
         beam_set.assign(cfg.beams.size(), false);
@@ -767,6 +775,18 @@ public:
         std::memset(ctl_h, 0, sizeof(Ctl));
         ctl_h->islice = nz - 1;
         ctl_h->step_parity = parity;
+        for (size_t b = 0; b < cfg.beams.size() && b < (size_t)kMaxBeams; ++b) {
+            const bool on = insitu_beam_d[b] && do_diagnostics(cfg.beams[b].insitu_period, step, cfg.max_step,
+                                                               physical_time, cfg.max_time);
+            ctl_h->insitu_beam[b] = on;
+            if (on) insitu_beam_has[b] = 1;
+        }
+        {
+            const bool on = insitu_fields_d && do_diagnostics(cfg.fields_insitu_period, step, cfg.max_step,
+                                                              physical_time, cfg.max_time);
+            ctl_h->insitu_fields = on;
+            if (on) insitu_fields_has = true;
+        }
         HPQ_CUDA(cudaMemcpyAsync(ctl, ctl_h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
         cur_islice = nz - 1;
     }
@@ -804,6 +824,68 @@ public:
         HPQ_LAUNCH_CHECK();
         det_flush_ptrs({jx, jy, jz, rmj});
     }
+    // ---- in-situ reductions (raw per-slice sums on the device; normalised on the host)
+    std::vector<double*> insitu_beam_d;  // per beam: nz x 23
+    double* insitu_fields_d = nullptr;   // nz x 10
+    std::vector<char> insitu_beam_has;   // the last diagnostic step filled the arrays
+    bool insitu_fields_has = false;
+    void insitu_alloc() {
+        insitu_beam_d.assign(cfg.beams.size(), nullptr);
+        insitu_beam_has.assign(cfg.beams.size(), 0);
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (cfg.beams[b].insitu_period > 0) {
+                HPQ_CUDA(cudaMalloc(&insitu_beam_d[b], (size_t)nz * 23 * sizeof(double)));
+                HPQ_CUDA(cudaMemset(insitu_beam_d[b], 0, (size_t)nz * 23 * sizeof(double)));
+            }
+        if (cfg.fields_insitu_period > 0) {
+            HPQ_CUDA(cudaMalloc(&insitu_fields_d, (size_t)nz * 10 * sizeof(double)));
+            HPQ_CUDA(cudaMemset(insitu_fields_d, 0, (size_t)nz * 10 * sizeof(double)));
+        }
+    }
+    long long insitu_size(const std::string& what) override {
+        if (what == "fields") return cfg.fields_insitu_period > 0 ? 11LL * nz : -1;
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (cfg.beams[b].name == what) return cfg.beams[b].insitu_period > 0 ? 23LL * nz + 23 : -1;
+        return -1;
+    }
+    // layout of the reference's reduced diagnostics: value index outer, slice inner; beams: 22 x nz
+    // values (entry 0 the sum of weights, the others divided by it), nz counts, 22 + 1 sums over
+    // slices; fields: 10 x nz values (times dx dy dz), 10 sums
+    bool get_insitu(const std::string& what, double* out) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        if (what == "fields") {
+            if (!insitu_fields_d || !insitu_fields_has) return false;
+            std::vector<double> r((size_t)nz * 10);
+            HPQ_CUDA(cudaMemcpy(r.data(), insitu_fields_d, r.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            const double dv = g.dx[0] * g.dx[1] * g.dx[2];
+            std::vector<double> sum(10, 0.0);
+            for (int isl = nz - 1; isl >= 0; --isl)
+                for (int k = 0; k < 10; ++k) sum[k] += r[(size_t)isl * 10 + k] * dv;
+            for (int k = 0; k < 10; ++k)
+                for (int isl = 0; isl < nz; ++isl) out[(size_t)k * nz + isl] = r[(size_t)isl * 10 + k] * dv;
+            for (int k = 0; k < 10; ++k) out[(size_t)10 * nz + k] = sum[k];
+            return true;
+        }
+        for (size_t b = 0; b < cfg.beams.size(); ++b) {
+            if (cfg.beams[b].name != what) continue;
+            if (!insitu_beam_d[b] || !insitu_beam_has[b]) return false;
+            std::vector<double> r((size_t)nz * 23);
+            HPQ_CUDA(cudaMemcpy(r.data(), insitu_beam_d[b], r.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<double> sum(23, 0.0);
+            for (int isl = nz - 1; isl >= 0; --isl)
+                for (int k = 0; k < 23; ++k) sum[k] += r[(size_t)isl * 23 + k];
+            for (int isl = 0; isl < nz; ++isl) {
+                const double sw = r[(size_t)isl * 23];
+                const double inv = sw <= 0. ? 0. : 1. / sw;
+                for (int k = 0; k < 22; ++k) out[(size_t)k * nz + isl] = r[(size_t)isl * 23 + k] * (k == 0 ? 1. : inv);
+                out[(size_t)22 * nz + isl] = r[(size_t)isl * 23 + 22];
+            }
+            for (int k = 0; k < 23; ++k) out[(size_t)23 * nz + k] = sum[k];
+            return true;
+        }
+        throw InputError("unknown in-situ diagnostic '" + what + "'");
+    }
+
     // ---- deterministic deposition (fixed-point shadows, see addc)
     DetAcc det{};
     long long* det_mem = nullptr;
@@ -1021,11 +1103,23 @@ public:
             hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)nx * ny * diag_list.n, 256)), dim3(256), 0, st, S, ctl, diag_list, diag_buf, nz);
             HPQ_LAUNCH_CHECK();
         }
+        // field in-situ reductions after every field of the slice is known (Hipace.cpp:684-685)
+        if (insitu_fields_d) {
+            hpq_launch(k_field_insitu<R>, dim3(1), dim3(1024), 0, st, S, (const Ctl*)ctl, cfg.pc.c, insitu_fields_d);
+            HPQ_LAUNCH_CHECK();
+        }
         // the beam push and partition (beam arrays, Ctl) run beside the plasma push and the
         // component shifts (plasma arrays, slab planes the pushes do not read)
         {
             OnStream on(this, side_begin());
             for (size_t b = 0; b < bm.size(); ++b) {
+                // beam in-situ reductions before the push (Hipace.cpp:680-681)
+                if (insitu_beam_d[b]) {
+                    const double r = cfg.beams[b].insitu_radius;
+                    hpq_launch(k_beam_insitu, dim3(1), dim3(1024), 0, st, bm[b], (const Ctl*)ctl, (int)b,
+                               r < 1e150 ? r * r : 1e300, 1.0 / cfg.pc.c, insitu_beam_d[b]);
+                    HPQ_LAUNCH_CHECK();
+                }
                 {
                     Scope sc(this, "beam_push");
                     hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, S, g, cfg.dt);

@@ -88,6 +88,20 @@ int hpq_get_field(hpq_handle* h, const char* comp, double* out);
 int hpq_set_diag(hpq_handle* h, const char* comps);
 int hpq_get_diag(hpq_handle* h, const char* comp, double* out);
 
+/* In-situ reduced diagnostics of the last diagnostic step (keys <beam>.insitu_period,
+ * <beam>.insitu_radius, beams.insitu_*, fields.insitu_period). Replaces the per-slice reductions
+ * BeamParticleContainer::InSituComputeDiags (BeamParticleContainer.cpp:476-548) and
+ * Fields::InSituComputeDiags (Fields.cpp:1289-1346) with the arrays their InSituWriteToFile
+ * writes. `what` is a beam name or "fields". Layout, value index outer and slice inner:
+ *   beam (23 nz + 23 doubles): 22 x nz per-slice values ([0] sum of weights, [1..21] the
+ *     weighted means [x], [x^2], [y], [y^2], [z], [z^2], [ux], [ux^2], [uy], [uy^2], [uz],
+ *     [uz^2], [x*ux], [y*uy], [z*uz], [x*uy], [y*ux], [ux/uz], [uy/uz], [ga], [ga^2]), nz particle
+ *     counts, then the 22 raw sums and the particle count over all slices;
+ *   fields (11 nz doubles): 10 x nz per-slice sums times dx dy dz ([Ex^2], [Ey^2], [Ez^2],
+ *     [Bx^2], [By^2], [Bz^2], [ExmBy^2], [EypBx^2], [jz_beam], [Ez*jz_beam]), then the 10 sums. */
+int hpq_insitu_size(hpq_handle* h, const char* what, int64_t* n);
+int hpq_get_insitu(hpq_handle* h, const char* what, double* out);
+
 /* Plasma species `sp`: particle count and the 11 real attributes of PlasmaIdx
  * (src/particles/plasma/PlasmaParticleContainer.H:21-46) plus the valid flag, as 12 blocks of
  * `n` doubles: x y w ux uy psi x_prev y_prev ux_half_step uy_half_step psi_half_step valid. */

@@ -1090,6 +1090,8 @@ public:
         } else {
             pc_loop(islice);
         }
+        // in-situ reductions (after SALAME, before the beam push, Hipace.cpp:681-685)
+        insitu_compute(islice);
         // diagnostics (after all fields are known, before the pushes)
         for (auto& n : diag_names) {
             auto& d = diag[n];
@@ -1127,7 +1129,11 @@ public:
     // Hipace::Evolve per-step body (Hipace.cpp:401-492), one rank, fixed dt
     void begin_step(int step) {
         for (auto& kv : F) kv.second.zero();  // ResetAllQuantities
-        (void)step;
+        cur_step = step;
+        insitu_beam.resize(cfg.beams.size());
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (insitu_beam_on(b)) insitu_beam[b].assign((size_t)nz * 23, 0.0);
+        if (insitu_fields_on()) insitu_fields.assign((size_t)nz * 10, 0.0);
         init_plasmas();
         if (cfg.any_neutralize_background()) {
             // DepositNeutralizingBackground: rhomjz of ions with the opposite charge
@@ -1147,6 +1153,53 @@ public:
             if (!cfg.plasmas[s].neutralize_background) { plasmas[s].valid = saved[s].valid; plasmas[s].w = saved[s].w; }
     }
     void end_step() { physical_time += cfg.dt; }
+
+    // ---- in-situ diagnostics (BeamParticleContainer.cpp:476-548, Fields.cpp:1289-1346)
+    int cur_step = 0;
+    std::vector<std::vector<double>> insitu_beam;  // per beam: per slice 22 sums + Np
+    std::vector<double> insitu_fields;             // per slice 10 sums (times dx dy dz)
+    bool insitu_beam_on(size_t b) const {
+        return hpq::do_diagnostics(cfg.beams[b].insitu_period, cur_step, cfg.max_step, physical_time, cfg.max_time);
+    }
+    bool insitu_fields_on() const {
+        return hpq::do_diagnostics(cfg.fields_insitu_period, cur_step, cfg.max_step, physical_time, cfg.max_time);
+    }
+    void insitu_compute(int islice) {
+        const double cinv = 1.0 / cfg.pc.c;
+        for (size_t b = 0; b < cfg.beams.size(); ++b) {
+            if (!insitu_beam_on(b)) continue;
+            const double r2 = cfg.beams[b].insitu_radius * cfg.beams[b].insitu_radius;
+            double a[23] = {0};
+            for (const BeamParticle& q : bthis[b].p) {
+                if (!q.valid || q.x * q.x + q.y * q.y > r2) continue;
+                const double x = q.x, y = q.y, z = q.z, w = q.w;
+                const double ux = q.ux * cinv, uy = q.uy * cinv, uz = q.uz * cinv;
+                const double uz_inv = uz == 0. ? 0. : 1. / uz;
+                const double gamma = std::sqrt(1.0 + ux * ux + uy * uy + uz * uz);
+                const double v[23] = {w, w * x, w * x * x, w * y, w * y * y, w * z, w * z * z, w * ux, w * ux * ux,
+                                      w * uy, w * uy * uy, w * uz, w * uz * uz, w * x * ux, w * y * uy, w * z * uz,
+                                      w * x * uy, w * y * ux, w * ux * uz_inv, w * uy * uz_inv, w * gamma,
+                                      w * gamma * gamma, 1.0};
+                for (int k = 0; k < 23; ++k) a[k] += v[k];
+            }
+            for (int k = 0; k < 23; ++k) insitu_beam[b][(size_t)islice * 23 + k] = a[k];
+        }
+        if (insitu_fields_on()) {
+            const double c = cfg.pc.c, dv = dx * dy * dz;
+            const Field &ex = f("ExmBy"), &ey = f("EypBx"), &ez = f("Ez"), &bx = f("Bx"), &by = f("By"), &bz = f("Bz"),
+                        &jzb = f("jz_beam");
+            double a[10] = {0};
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double v[10] = {std::pow(ex(i, j) + by(i, j) * c, 2), std::pow(ey(i, j) - bx(i, j) * c, 2),
+                                          std::pow(ez(i, j), 2), std::pow(bx(i, j), 2), std::pow(by(i, j), 2),
+                                          std::pow(bz(i, j), 2), std::pow(ex(i, j), 2), std::pow(ey(i, j), 2),
+                                          jzb(i, j), ez(i, j) * jzb(i, j)};
+                    for (int k = 0; k < 10; ++k) a[k] += v[k];
+                }
+            for (int k = 0; k < 10; ++k) insitu_fields[(size_t)islice * 10 + k] = a[k] * dv;
+        }
+    }
 
     int step(int s) {
         begin_step(s);
@@ -1276,5 +1329,48 @@ int oracle_threads() {
 #endif
 }
 const char* oracle_error(OracleHandle* h) { return h->sim->error.c_str(); }
+
+// In-situ data of the last diagnostic step: "fields" or a beam name. Layout (the reference's
+// reduced-diagnostic arrays, value index outer, slice inner): beam: 22 x nz values (entry 0 the
+// sum of weights, the others divided by it), nz particle counts, 22 sums over slices, the total
+// count; fields: 10 x nz values, 10 sums.
+long long oracle_insitu_size(OracleHandle* h, const char* what) {
+    auto& s = *h->sim;
+    if (std::string(what) == "fields") return 11LL * s.nz;
+    for (size_t b = 0; b < s.cfg.beams.size(); ++b)
+        if (s.cfg.beams[b].name == what) return 23LL * s.nz + 23;
+    return -1;
+}
+int oracle_get_insitu(OracleHandle* h, const char* what, double* out) {
+    auto& s = *h->sim;
+    const int nz = s.nz;
+    if (std::string(what) == "fields") {
+        if (s.insitu_fields.empty()) return 1;
+        std::vector<double> sum(10, 0.0);
+        for (int isl = nz - 1; isl >= 0; --isl)
+            for (int k = 0; k < 10; ++k) sum[k] += s.insitu_fields[(size_t)isl * 10 + k];
+        for (int k = 0; k < 10; ++k)
+            for (int isl = 0; isl < nz; ++isl) out[(size_t)k * nz + isl] = s.insitu_fields[(size_t)isl * 10 + k];
+        for (int k = 0; k < 10; ++k) out[(size_t)10 * nz + k] = sum[k];
+        return 0;
+    }
+    for (size_t b = 0; b < s.cfg.beams.size(); ++b) {
+        if (s.cfg.beams[b].name != what) continue;
+        const auto& r = s.insitu_beam[b];
+        if (r.empty()) return 1;
+        std::vector<double> sum(23, 0.0);
+        for (int isl = nz - 1; isl >= 0; --isl)
+            for (int k = 0; k < 23; ++k) sum[k] += r[(size_t)isl * 23 + k];
+        for (int isl = 0; isl < nz; ++isl) {
+            const double sw = r[(size_t)isl * 23];
+            const double inv = sw <= 0. ? 0. : 1. / sw;
+            for (int k = 0; k < 22; ++k) out[(size_t)k * nz + isl] = r[(size_t)isl * 23 + k] * (k == 0 ? 1. : inv);
+            out[(size_t)22 * nz + isl] = r[(size_t)isl * 23 + 22];
+        }
+        for (int k = 0; k < 23; ++k) out[(size_t)23 * nz + k] = sum[k];
+        return 0;
+    }
+    return 2;
+}
 
 }  // extern "C"

@@ -42,6 +42,9 @@ def lib():
         L.oracle_get_beam.argtypes = [vp, i32] + [dp] * 7 + [lp]
         L.oracle_set_diag.argtypes = [vp, cp]
         L.oracle_get_diag.argtypes = [vp, cp, dp]
+        L.oracle_insitu_size.argtypes = [vp, cp]
+        L.oracle_insitu_size.restype = ctypes.c_longlong
+        L.oracle_get_insitu.argtypes = [vp, cp, dp]
         L.oracle_step.argtypes = [vp, i32]
         L.oracle_begin_step.argtypes = [vp, i32]
         L.oracle_solve_slice.argtypes = [vp, i32, i32]
@@ -117,6 +120,16 @@ class Oracle:
         out = np.zeros((self.nz, self.ny, self.nx))
         if self.L.oracle_get_diag(self.h, name.encode(), _dp(out)):
             raise KeyError(name)
+        return out
+
+    def get_insitu(self, what):
+        """Flat in-situ array in the layout of hpq_get_insitu."""
+        n = self.L.oracle_insitu_size(self.h, what.encode())
+        if n < 0:
+            raise KeyError(what)
+        out = np.zeros(n)
+        if self.L.oracle_get_insitu(self.h, what.encode(), _dp(out)):
+            raise KeyError(what)
         return out
 
     def step(self, s):

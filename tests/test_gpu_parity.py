@@ -169,6 +169,31 @@ def test_persistent_multigrid_equals_multi_kernel_form():
             assert rel_l2(a, b) <= 1e-10
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_insitu_diagnostics_match_oracle(graphs):
+    """In-situ beam moments and field reductions of every slice (BeamParticleContainer.cpp:476-548,
+    Fields.cpp:1289-1346) on the diagnostic steps (period 2 and the last step), against the oracle."""
+    text = EXPLICIT_MOVING + "\nbeams.insitu_period = 2\nbeam.insitu_radius = 1.5\nfields.insitu_period = 2\n"
+    g = hp.Hipace(text, graphs=graphs)
+    g.init_data()
+    o = Oracle(text)
+    o.set_beam(0, g.get_beam(0))
+    nz = g.n_cell[2]
+    for s in range(3):  # max_step = 2: diagnostics on steps 0 and 2
+        g.step(s)
+        assert o.step(s) == 0
+        if s == 1:
+            continue
+        for what in ("beam", "fields"):
+            a = g.get_insitu(what)
+            flat = np.concatenate([np.ravel(v) for v in a.values()])
+            want = o.get_insitu(what)
+            assert flat.shape == want.shape
+            e = rel_l2(flat, want)
+            assert e <= 1e-10, (what, s, e)
+        assert np.array_equal(g.get_insitu("beam")["Np"], o.get_insitu("beam")[22 * nz:23 * nz])
+
+
 DET_COMPS = ["Psi", "Ez", "Bx", "By", "Bz", "jx", "jy", "jz_beam", "rhomjz", "chi", "Sx", "Sy"]
 
 

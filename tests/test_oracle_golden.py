@@ -51,3 +51,39 @@ def test_beam_checksums(name):
     assert len(b["x"]) == gold["charge"]          # sum |q| with q = -1 per particle
     for k in ("x", "y", "z", "ux", "uy", "uz", "w"):
         assert np.abs(b[k]).sum() == pytest.approx(gold[k], rel=1e-12, abs=1e-12), k
+
+
+def synthetic_beam(n=4000, seed=5):
+    rng = np.random.default_rng(seed)
+    return {"x": rng.normal(0, 0.5, n), "y": rng.normal(0, 0.5, n), "z": rng.normal(0, 1.0, n),
+            "w": np.full(n, 0.01), "ux": rng.normal(0, 3, n), "uy": rng.normal(0, 3, n),
+            "uz": 2000 + rng.normal(0, 10, n), "id": np.arange(1, n + 1, dtype=np.int64)}
+
+
+def test_oracle_insitu_beam_moments_are_consistent():
+    """In-situ beam reductions of the oracle (BeamParticleContainer.cpp:476-548): the per-slice
+    particle counts cover the particles in the box, the totals are the sums over slices, [x] is a
+    weighted mean, and a finite insitu_radius only removes particles."""
+    from cases import EXPLICIT_MOVING
+    text = EXPLICIT_MOVING + "\nbeams.insitu_period = 1\nfields.insitu_period = 1\n"
+    beam = synthetic_beam()
+    inside = ((beam["z"] >= -8.0) & (beam["z"] < 4.0)).sum()
+    o = Oracle(text)
+    o.set_beam(0, beam)
+    assert o.step(0) == 0
+    nz = o.nz
+    flat = o.get_insitu("beam")
+    sumw, npart = flat[:nz], flat[22 * nz:23 * nz]
+    assert npart.sum() == pytest.approx(flat[23 * nz + 22])
+    # every particle is counted in its slice; a particle that slips into the next slice during
+    # the push is counted there again (the reference's "This" beam slice includes it)
+    assert inside <= npart.sum() <= inside * 1.01
+    assert flat[23 * nz] == pytest.approx(sumw.sum(), rel=1e-12)
+    xm = flat[nz:2 * nz]
+    assert np.all(np.abs(xm[npart > 0]) < 6.0)
+    fields = o.get_insitu("fields")
+    assert fields.size == 11 * nz and np.all(fields[2 * nz:3 * nz] >= 0)  # [Ez^2]
+    o2 = Oracle(text.replace("beams.insitu_period = 1", "beams.insitu_period = 1\nbeams.insitu_radius = 0.5"))
+    o2.set_beam(0, beam)
+    assert o2.step(0) == 0
+    assert o2.get_insitu("beam")[23 * nz + 22] < inside
