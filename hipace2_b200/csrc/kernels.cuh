@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
 // Explicit Sx/Sy deposition (ExplicitDeposition.cpp:20-265, no laser)
 // ------------------------------------------------------------------------------------------
 template <class R, int DT>
-__global__ void __launch_bounds__(256) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
+__global__ void __launch_bounds__(256, 2) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);

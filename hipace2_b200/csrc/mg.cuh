@@ -286,21 +286,25 @@ __device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, i
         }
     }
     __syncthreads();
+    // colour sweeps over the interior of the loaded region (its outer ring stays fixed): only
+    // the points of the sweep's colour are visited, (E-2)/2 per row
+    constexpr int HW = (E - 2) / 2;
     for (int s = 0; s < NSW; ++s) {
 #pragma unroll
-        for (int e0 = 0; e0 < E * E; e0 += NT) {
-            const int e = e0 + threadIdx.x;
-            if (e >= E * E) break;
-            const int li = e % E, lj = e / E;
-            if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1) continue;
+        for (int q0 = 0; q0 < (E - 2) * HW; q0 += NT) {
+            const int q = q0 + threadIdx.x;
+            if (q >= (E - 2) * HW) break;
+            const int lj = 1 + q / HW, k = q - (lj - 1) * HW;
+            const int par = (s + ti0 + tj0 + lj) & 1;  // parity of li for (i + j + s) even
+            const int li = (par ? 1 : 2) + 2 * k;
             const int i = ti0 + li, j = tj0 + lj;
-            if (((i + j + s) & 1) != 0) continue;
             if (i < L.vlo || i > L.vhi_i || j < L.vlo || j > L.vhi_j) continue;
+            const int e = lj * E + li;
             const R inv = sinv[e];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const R* q = sp[c];
-                sp[c][e] = mg_gs_inv<R, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], inv, A.facx, A.facy);
+                const R* qq = sp[c];
+                sp[c][e] = mg_gs_inv<R, CELL>(L, i, j, qq[e - 1], qq[e + 1], qq[e - E], qq[e + E], srh[c][e], inv, A.facx, A.facy);
             }
         }
         __syncthreads();
@@ -796,21 +800,23 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
         }
         __syncthreads();
     }
+    constexpr int HW = (E - 2) / 2;  // points of one colour per interior row
     for (int s = 0; s < NSW; ++s) {
 #pragma unroll
-        for (int e0 = 0; e0 < E * E; e0 += NT) {
-            const int e = e0 + threadIdx.x;
-            if (e >= E * E) break;
-            const int li = e % E, lj = e / E;
-            if (li == 0 || lj == 0 || li == E - 1 || lj == E - 1) continue;
+        for (int q0 = 0; q0 < (E - 2) * HW; q0 += NT) {
+            const int q = q0 + threadIdx.x;
+            if (q >= (E - 2) * HW) break;
+            const int lj = 1 + q / HW, k = q - (lj - 1) * HW;
+            const int par = (s + ti0 + tj0 + lj) & 1;
+            const int li = (par ? 1 : 2) + 2 * k;
             const int i = ti0 + li, j = tj0 + lj;
-            if (((i + j + s) & 1) != 0) continue;
             if (!inside(i, j)) continue;
+            const int e = lj * E + li;
             const float inv = sinv[e];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const float* q = sd[c];
-                sd[c][e] = mg_gs_inv<float, CELL>(L, i, j, q[e - 1], q[e + 1], q[e - E], q[e + E], srh[c][e], inv, facx, facy);
+                const float* qq = sd[c];
+                sd[c][e] = mg_gs_inv<float, CELL>(L, i, j, qq[e - 1], qq[e + 1], qq[e - E], qq[e + E], srh[c][e], inv, facx, facy);
             }
         }
         __syncthreads();
