@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
 // Explicit Sx/Sy deposition (ExplicitDeposition.cpp:20-265, no laser)
 // ------------------------------------------------------------------------------------------
 template <class R, int DT>
-__global__ void __launch_bounds__(256, 2) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);
@@ -300,20 +300,24 @@ __global__ void __launch_bounds__(256, 2) k_explicit_deposit(PlasmaDev<R> P, Sla
         const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx * vx + vy * vy) : R(0);
         const R gmy = P.ru ? gpm1 - vy * vy : gamma_psi - vy * vy - R(1);
         const R gmx = P.ru ? gpm1 - vx * vx : gamma_psi - vx * vx - R(1);
-        DSh<R> sx[NS], sy[NS];
+        DSh<R> sx[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
-            sx[k] = dshape2<R, DT>(xmid, k); sy[k] = dshape2<R, DT>(ymid, k);
-            sx[k].cell += bx; sy[k].cell += by;
+            sx[k] = dshape2<R, DT>(xmid, k);
+            sx[k].cell += bx;
         }
-#pragma unroll
-        for (int iy = 0; iy < NS; ++iy)
+        // one row of the stencil at a time (the y shape of the row is formed in the loop, which
+        // keeps the register count low enough for two blocks per SM)
+#pragma unroll 1
+        for (int iy = 0; iy < NS; ++iy) {
+            DSh<R> syr = dshape2<R, DT>(ymid, iy);
+            syr.cell += by;
 #pragma unroll
             for (int ix = 0; ix < NS; ++ix) {
                 if (DT == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
-                const int i = sx[ix].cell, j = sy[iy].cell;
+                const int i = sx[ix].cell, j = syr.cell;
                 const R Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = Ex(i, j), EypBx_v = Ey(i, j);
-                const R sxs = sx[ix].s, sys = sy[iy].s, sxd = sx[ix].ds, syd = sy[iy].ds;
+                const R sxs = sx[ix].s, sys = syr.s, sxd = sx[ix].ds, syd = syr.ds;
                 const R vsy = cdm * (-sxs * sys * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * clight_inv) * q_mass_ratio * psi_inv +
                                      (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * gmy) * a_clight);
                 const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
@@ -321,6 +325,7 @@ __global__ void __launch_bounds__(256, 2) k_explicit_deposit(PlasmaDev<R> P, Sla
                 addc(det, Sy, S.pitch, i, j, vsy);
                 addc(det, Sx, S.pitch, i, j, vsx);
             }
+        }
     }
 }
 
