@@ -24,7 +24,7 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
            "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
-           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc")
+           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad")
 
 _lib = None
 
@@ -70,6 +70,8 @@ def load_library(path=None):
         "hpq_set_deterministic": ([vp, i32], i32),
         "hpq_insitu_size": ([vp, cp, ctypes.POINTER(ctypes.c_int64)], i32),
         "hpq_get_insitu": ([vp, cp, dp], i32),
+        "hpq_adjoint_nparams": ([vp, ctypes.POINTER(i32)], i32),
+        "hpq_adjoint_grad": ([vp, dp, dp, dp], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
         "hpq_get_counters": ([vp, lp, lp, lp, lp], i32),
@@ -216,6 +218,23 @@ class Hipace:
         out = np.zeros(12 * n)
         self._check(self.L.hpq_get_plasma(self.h, sp, _dp(out)))
         return {k: out[i * n:(i + 1) * n] for i, k in enumerate(PLASMA_ATTRS)}
+
+    def adjoint_nparams(self):
+        n = ctypes.c_int()
+        self._check(self.L.hpq_adjoint_nparams(self.h, ctypes.byref(n)))
+        return n.value
+
+    def adjoint(self, knots, grad=True):
+        """Objective of the adjoint configuration for the given knots and, unless grad is False,
+        its gradient (hpq_adjoint_grad): returns J or (J, dJ/dknots)."""
+        knots = np.ascontiguousarray(knots, dtype=np.float64)
+        n = self.adjoint_nparams()
+        if knots.size != n:
+            raise ValueError("expected %d knot values, got %d" % (n, knots.size))
+        g = np.zeros(n) if grad else None
+        J = ctypes.c_double(0)
+        self._check(self.L.hpq_adjoint_grad(self.h, _dp(knots), _dp(g) if grad else None, ctypes.byref(J)))
+        return (J.value, g) if grad else J.value
 
     def synchronize(self):
         self._check(self.L.hpq_synchronize(self.h))

@@ -254,6 +254,26 @@ int hpq_set_deterministic(hpq_handle* h, int on) {
     });
 }
 
+int hpq_adjoint_nparams(hpq_handle* h, int* n) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!n) return (int)HPQ_ERR_ARG;
+        *n = h->sim->adjoint_nparams();
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_adjoint_grad(hpq_handle* h, const double* knots, double* grad, double* objective) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!knots || !objective) return (int)HPQ_ERR_ARG;
+        if (h->in_step) { h->err = "hpq_adjoint_grad inside a step"; return (int)HPQ_ERR_STATE; }
+        if (h->sim->adjoint_nparams() == 0) { h->err = "no adjoint configured (adjoint.witness)"; return (int)HPQ_ERR_INPUT; }
+        *objective = h->sim->adjoint(knots, grad);
+        return (int)HPQ_OK;
+    });
+}
+
 int hpq_synchronize(hpq_handle* h) {
     return guarded(h, [&] {
         if (int r = need_init(h)) return r;

@@ -74,6 +74,53 @@ struct BeamSpecies {
     double insitu_radius = 1e300;
 };
 
+// Adjoint of one step of the explicit slice march with respect to a beam-loading objective.
+// The reference has no adjoint; these keys belong to this library. The parameter vector is
+//   theta[0 .. n_profile)                 witness current-profile knots: the witness weights are
+//                                         multiplied by the piecewise-linear profile through
+//                                         these values at n_profile equidistant points of
+//                                         [profile_lo, profile_hi] in zeta (zero outside);
+//   theta[n_profile .. n_profile+n_density) plasma-density knots: the plasma (and neutralising
+//                                         ion) weights are multiplied by the piecewise-linear
+//                                         profile through these values over [density_lo,
+//                                         density_hi] in z = c t, clamped to the end values.
+// Objective: the current-weighted variance of Ez over the slices whose centre lies in
+// [objective_lo, objective_hi]: J = S2/S0 - (S1/S0)^2, S_n = sum jz_beam * Ez^n.
+struct AdjointConfig {
+    int witness = -1;  // beam index; -1: no adjoint configured
+    double profile_lo = -7, profile_hi = -5;
+    int n_profile = 64;
+    double density_lo = 0, density_hi = 1;
+    int n_density = 8;
+    double objective_lo = -7, objective_hi = -5;
+    int checkpoint_interval = 32;
+    int n_params() const { return n_profile + n_density; }
+};
+
+// Piecewise-linear interpolation on n equidistant knots over [lo, hi]: value = (1-f) v[k] +
+// f v[k+1]. Returns false outside [lo, hi] unless `clamp`, which then holds the end value.
+inline bool knot_interval(double z, double lo, double hi, int n, bool clamp, int& k, double& f) {
+    if (n < 1) return false;
+    if (n == 1) { k = 0; f = 0; return clamp || (z >= lo && z <= hi); }
+    if (z < lo || z > hi) {
+        if (!clamp) return false;
+        k = z < lo ? 0 : n - 2;
+        f = z < lo ? 0.0 : 1.0;
+        return true;
+    }
+    const double t = (z - lo) / (hi - lo) * (n - 1);
+    k = (int)t;
+    if (k > n - 2) k = n - 2;
+    f = t - k;
+    return true;
+}
+inline double knot_value(const double* v, double z, double lo, double hi, int n, bool clamp) {
+    int k; double f;
+    if (!knot_interval(z, lo, hi, n, clamp, k, f)) return 0.0;
+    if (n == 1) return v[0];
+    return (1.0 - f) * v[k] + f * v[k + 1];
+}
+
 struct SimConfig {
     bool normalized_units = false;
     PhysConst pc{};
@@ -102,6 +149,7 @@ struct SimConfig {
     bool do_beam_jz_minus_rho = false;
     bool deposit_rho = false;
     int fields_insitu_period = 0;  // fields.insitu_period (Fields.cpp:41, 1289-1346)
+    AdjointConfig adjoint;
     std::vector<PlasmaSpecies> plasmas;
     std::vector<BeamSpecies> beams;
     bool any_neutralize_background() const {
@@ -383,6 +431,27 @@ inline SimConfig build_config(const InputStore& in) {
     }
     if (c.fields_insitu_period > 0 && !c.explicit_solver)
         throw InputError("Must use explicit solver for field insitu diagnostic");
+    std::string witness;
+    if (in.query_str("adjoint.witness", witness)) {
+        AdjointConfig& a = c.adjoint;
+        for (size_t b = 0; b < c.beams.size(); ++b)
+            if (c.beams[b].name == witness) a.witness = (int)b;
+        if (a.witness < 0) throw InputError("adjoint.witness = " + witness + " is not in beams.names");
+        if (!c.explicit_solver) throw InputError("the adjoint needs the explicit Bx/By solver");
+        for (auto& p : c.plasmas)
+            if (p.n_subcycles != 1) throw InputError("the adjoint needs plasma n_subcycles = 1");
+        double r[2];
+        if (in.query_arr("adjoint.profile_zeta", r)) { a.profile_lo = r[0]; a.profile_hi = r[1]; }
+        if (in.query_arr("adjoint.density_z", r)) { a.density_lo = r[0]; a.density_hi = r[1]; }
+        if (in.query_arr("adjoint.objective_zeta", r)) { a.objective_lo = r[0]; a.objective_hi = r[1]; }
+        in.query("adjoint.n_profile_knots", a.n_profile);
+        in.query("adjoint.n_density_knots", a.n_density);
+        in.query("adjoint.checkpoint_interval", a.checkpoint_interval);
+        if (a.n_profile < 2 || a.n_density < 1 || a.checkpoint_interval < 1 ||
+            !(a.profile_hi > a.profile_lo) || !(a.density_hi > a.density_lo) ||
+            !(a.objective_hi >= a.objective_lo))
+            throw InputError("invalid adjoint.* ranges or knot counts");
+    }
     return c;
 }
 

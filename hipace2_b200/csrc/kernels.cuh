@@ -91,6 +91,8 @@ struct Ctl {
     // in-situ reductions on this step (set when the step begins)
     int insitu_beam[kMaxBeams];
     int insitu_fields, insitu_pad;
+    // adjoint forward: checkpoints of segment heads are written while set
+    int adj_ckpt, adj_pad;
 };
 
 struct Geo {

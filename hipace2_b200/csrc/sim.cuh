@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "common.cuh"
 #include "config.hpp"
 #include "dst.cuh"
@@ -67,6 +68,9 @@ public:
     virtual bool get_insitu(const std::string& what, double* out) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual bool get_profile(const std::string& name, double* ms, long long* n) = 0;
+    // adjoint of one step (double precision): number of parameters, objective and gradient
+    virtual int adjoint_nparams() const = 0;
+    virtual double adjoint(const double* theta, double* grad) = 0;
     virtual std::string profile_names() = 0;
     const SimConfig& config() const { return cfg; }
     SimConfig cfg;
@@ -354,6 +358,7 @@ public:
         ctl = nullptr; ctl_h = nullptr;
         if (diag_buf) cudaFree(diag_buf);
         diag_buf = nullptr;
+        adj_release();
         for (auto& kv : prof)
             for (auto& pr : kv.second.pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
         prof.clear();
@@ -689,6 +694,7 @@ public:
         HPQ_CUDA(cudaMemcpyAsync(d.count[parity], cnt.data(), nz * sizeof(int), cudaMemcpyHostToDevice, st));
         HPQ_CUDA(cudaStreamSynchronize(st));  // the caller's buffers and the host vectors are released
         st_host.beam_particles = 0;
+        ++beam_gen;
     }
     void upload_beam(int b, const HostBeam& hb) {
         upload_beam(b, hb.x.data(), hb.y.data(), hb.z.data(), hb.w.data(), hb.ux.data(), hb.uy.data(), hb.uz.data(),
@@ -758,7 +764,8 @@ public:
         for (size_t s = 0; s < pl.size(); ++s) {
             const PlasmaSpecies& P = cfg.plasmas[s];
             const int nppc = P.ppc[0] * P.ppc[1];
-            const double scale = nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc);
+            const double scale = adj_plasma_scale *
+                                 (nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc));
             if (pl[s].n == 0) continue;
             hpq_launch(k_plasma_reset<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], px0[s], py0[s], P.density, c_t, scale,
                                                                          P.u_mean[0], P.u_mean[1], P.u_mean[2], cfg.pc.c);
@@ -794,6 +801,7 @@ public:
     void end_step() override {
         physical_time += cfg.dt;
         parity = 1 - parity;
+        ++beam_gen;
         HPQ_CUDA(cudaMemcpyAsync(ctl_h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
         HPQ_CUDA(cudaStreamSynchronize(st));
         prof_collect();
@@ -950,13 +958,14 @@ public:
 
     void mg_solve() {
         Scope sc(this, "multigrid");
-        if (mg.cell) mg_solve_t<true>(); else mg_solve_t<false>();
+        if (mg.cell) mg_solve_t<true>(S); else mg_solve_t<false>(S);
     }
+    // the multigrid reads Sy, Sx, chi and writes Bx, By of slab MS
     template <bool CELL>
-    void mg_solve_t() {
+    void mg_solve_t(const Slab<R>& MS) {
         if (mg.coop_ok) {
             // the whole solve, iterations and decisions included, is one cooperative kernel
-            mg.template solve_persistent<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters);
+            mg.template solve_persistent<CELL>(st, MS, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters);
             return;
         }
         if (capturing) {
@@ -969,7 +978,7 @@ public:
             HPQ_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
             cudaGraphConditionalHandle handle;
             HPQ_CUDA(cudaGraphConditionalHandleCreate(&handle, cg, 0, cudaGraphCondAssignDefault));
-            mg.template pre<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, (unsigned long long)handle, 1);
+            mg.template pre<CELL>(st, MS, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, (unsigned long long)handle, 1);
             HPQ_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
             cudaGraphNodeParams cp{};
             cp.type = cudaGraphNodeTypeConditional;
@@ -981,26 +990,334 @@ public:
             cudaGraph_t body = cp.conditional.phGraph_out[0];
             HPQ_CUDA(cudaStreamBeginCaptureToGraph(st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
             const long long l0 = g_launches;
-            mg.template vcycle<CELL>(st2, S, ctl, cfg.mg_max_iters, (unsigned long long)handle, 1);
+            mg.template vcycle<CELL>(st2, MS, ctl, cfg.mg_max_iters, (unsigned long long)handle, 1);
             launches_body = g_launches - l0;
             body_launch_offset += launches_body;
             cudaGraph_t body_out;
             HPQ_CUDA(cudaStreamEndCapture(st2, &body_out));
             HPQ_CUDA(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
-            mg.template post<CELL>(st, S, ctl);
+            mg.template post<CELL>(st, MS, ctl);
             return;
         }
-        mg.template pre<CELL>(st, S, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, 0, 0);
+        mg.template pre<CELL>(st, MS, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, 0, 0);
         // the device decides after every V-cycle (Ctl::mg_go); without graphs the host reads
         // the decision back each cycle, like the reference's host-side max reduction
         HPQ_CUDA(cudaMemcpyAsync(&ctl_h->mg_go, &ctl->mg_go, sizeof(int), cudaMemcpyDeviceToHost, st));
         HPQ_CUDA(cudaStreamSynchronize(st));
         for (int it = 0; it < cfg.mg_max_iters && ctl_h->mg_go; ++it) {
-            mg.template vcycle<CELL>(st, S, ctl, cfg.mg_max_iters, 0, 0);
+            mg.template vcycle<CELL>(st, MS, ctl, cfg.mg_max_iters, 0, 0);
             HPQ_CUDA(cudaMemcpyAsync(&ctl_h->mg_go, &ctl->mg_go, sizeof(int), cudaMemcpyDeviceToHost, st));
             HPQ_CUDA(cudaStreamSynchronize(st));
         }
-        mg.template post<CELL>(st, S, ctl);
+        mg.template post<CELL>(st, MS, ctl);
+    }
+
+    // ------------------------------------------------------------------ adjoint (adjoint.cuh)
+    bool adj_fwd = false;           // the slice graph is the adjoint forward (hooks, no beam push)
+    double adj_plasma_scale = 1.0;  // plasma density multiplier applied when a step begins
+    long long beam_gen = 0;         // changes whenever the beam stores change
+    struct AdjBuf {
+        int K = 0, C = 0;                 // slices per segment, segments (checkpoints)
+        long long n = 0, cap = -1;        // plasma particles, witness store capacity
+        double* rec_pl[8] = {};           // K slots: x, y, ux_h, uy_h, psi_h, ux, uy, psi
+        uint8_t* rec_valid = nullptr;
+        double* rec_f[RF_N] = {};         // K slots of each recorded field plane
+        double* ck_pl[11] = {};           // C slots of the 11 plasma attributes
+        uint8_t* ck_valid = nullptr;
+        double* ck_slab = nullptr;        // C slots of the whole slab
+        Slab<double> L{}, M{};            // adjoint planes; multigrid planes of the transposed solve
+        double* lam[2][8] = {};           // adjoint of the plasma state (out / in, swapped per slice)
+        double* lw = nullptr;             // adjoint of the plasma weights (accumulated)
+        double* w_step = nullptr;         // plasma weights of the step
+        double* lwb = nullptr;            // adjoint of the witness weights (store order)
+        double* w0 = nullptr;             // witness weights before the profile
+        long long w0_gen = -1;
+        double* obj = nullptr;            // nz x 3 objective sums
+        double* ions = nullptr;           // nz ion-background terms of dJ/dsigma
+        double* knots = nullptr;          // parameters
+        double* grad = nullptr;           // profile-knot gradient
+        double* sig = nullptr;            // sum lambda_w w
+        AdjCopy<R> ck_args{}, rec_args{};
+        std::vector<void*> owned;
+    } adjb;
+
+    int adjoint_nparams() const override { return cfg.adjoint.witness < 0 ? 0 : cfg.adjoint.n_params(); }
+
+    template <class T>
+    T* adj_alloc1(size_t count) {
+        void* p = nullptr;
+        HPQ_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        HPQ_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), st));
+        adjb.owned.push_back(p);
+        return static_cast<T*>(p);
+    }
+    void adj_release() {
+        for (void* p : adjb.owned) cudaFree(p);
+        adjb = AdjBuf{};
+    }
+    // buffers of the adjoint (once per simulation; the witness arrays follow the store capacity)
+    void adj_setup() {
+        AdjBuf& a = adjb;
+        const int wb = cfg.adjoint.witness;
+        if (a.K == 0) {
+            const PlasmaDev<R>& P = pl[0];
+            a.n = P.n;
+            a.K = std::min(cfg.adjoint.checkpoint_interval, nz);
+            a.C = (nz + a.K - 1) / a.K;
+            const size_t n = (size_t)a.n, cs = S.cstride;
+            for (auto& q : a.rec_pl) q = adj_alloc1<double>(n * a.K);
+            a.rec_valid = adj_alloc1<uint8_t>(n * a.K);
+            for (auto& q : a.rec_f) q = adj_alloc1<double>(cs * a.K);
+            for (auto& q : a.ck_pl) q = adj_alloc1<double>(n * a.C);
+            a.ck_valid = adj_alloc1<uint8_t>(n * a.C);
+            a.ck_slab = adj_alloc1<double>(cs * C_NCOMP * a.C);
+            for (Slab<double>* q : {&a.L, &a.M}) {
+                q->nx = nx; q->ny = ny; q->pitch = S.pitch; q->rows = S.rows; q->cstride = cs;
+            }
+            a.L.base = adj_alloc1<double>(cs * A_NCOMP);
+            a.M.base = adj_alloc1<double>(cs * (C_BY + 1));
+            for (auto& side : a.lam)
+                for (auto& q : side) q = adj_alloc1<double>(n);
+            a.lw = adj_alloc1<double>(n);
+            a.w_step = adj_alloc1<double>(n);
+            a.obj = adj_alloc1<double>((size_t)nz * 3);
+            a.ions = adj_alloc1<double>(nz);
+            a.knots = adj_alloc1<double>(cfg.adjoint.n_params());
+            a.grad = adj_alloc1<double>(cfg.adjoint.n_profile);
+            a.sig = adj_alloc1<double>(1);
+            // checkpoint: the 11 plasma attributes, the valid flags and the whole slab
+            AdjCopy<R>& c = a.ck_args;
+            c = AdjCopy<R>{};
+            const R* src[11] = {P.x, P.y, P.w, P.ux, P.uy, P.psi, P.xp, P.yp, P.uxh, P.uyh, P.psih};
+            for (int k = 0; k < 11; ++k) { c.src[k] = src[k]; c.dst[k] = (R*)a.ck_pl[k]; c.n[k] = a.n; }
+            c.src[11] = S.base; c.dst[11] = (R*)a.ck_slab; c.n[11] = (long long)(cs * C_NCOMP);
+            c.na = 12;
+            c.vsrc = P.valid; c.vdst = a.ck_valid; c.nv = a.n;
+            c.nz = nz; c.K = a.K;
+            // record: the plasma state the reverse sweep reads and the recorded field planes
+            AdjCopy<R>& r = a.rec_args;
+            r = AdjCopy<R>{};
+            const R* rsrc[8] = {P.x, P.y, P.uxh, P.uyh, P.psih, P.ux, P.uy, P.psi};
+            for (int k = 0; k < 8; ++k) { r.src[k] = rsrc[k]; r.dst[k] = (R*)a.rec_pl[k]; r.n[k] = a.n; }
+            for (int k = 0; k < RF_N; ++k) {
+                r.src[8 + k] = S.c(kRecComp[k]).p; r.dst[8 + k] = (R*)a.rec_f[k]; r.n[8 + k] = (long long)cs;
+            }
+            r.na = 8 + RF_N;
+            r.vsrc = P.valid; r.vdst = a.rec_valid; r.nv = a.n;
+            r.nz = nz; r.K = a.K;
+        }
+        if (a.cap != bm[wb].cap) {
+            // the witness store grew: new per-particle arrays (freed with the others at release)
+            a.lwb = adj_alloc1<double>((size_t)bm[wb].cap);
+            a.w0 = adj_alloc1<double>((size_t)bm[wb].cap);
+            a.cap = bm[wb].cap;
+            a.w0_gen = -1;
+        }
+    }
+
+    // objective J (and its gradient when grad != nullptr) for the parameters theta
+    double adjoint(const double* theta, double* grad) override {
+        if constexpr (!std::is_same<R, double>::value) {
+            (void)theta; (void)grad;
+            throw InputError("the adjoint is available in double precision (hpq_set_precision HPQ_PLAIN_FP64)");
+        } else {
+            const AdjointConfig& A = cfg.adjoint;
+            if (A.witness < 0) throw InputError("no adjoint configured (adjoint.witness)");
+            if (pl.size() != 1 || pl[0].n == 0) throw InputError("the adjoint needs exactly one plasma species");
+            const int wb = A.witness;
+            adj_setup();
+            AdjBuf& a = adjb;
+            const int np = A.n_params();
+            HPQ_CUDA(cudaMemcpyAsync(a.knots, theta, np * sizeof(double), cudaMemcpyHostToDevice, st));
+            const double ct = cfg.pc.c * physical_time;
+            const double sigma = knot_value(theta + A.n_profile, ct, A.density_lo, A.density_hi, A.n_density, true);
+            if (sigma == 0.0) throw InputError("the plasma density multiplier is zero at z = c t");
+            // witness weights w0 * profile(z) in the read store
+            BeamDev& W = bm[wb];
+            if (a.w0_gen != beam_gen) {
+                HPQ_CUDA(cudaMemcpyAsync(a.w0, W.buf[parity].w, W.cap * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                a.w0_gen = beam_gen;
+            }
+            hpq_launch(k_adj_profile, dim3(8, nz), dim3(256), 0, st, W, parity, nz, (const double*)a.w0,
+                       (const double*)a.knots, A.profile_lo, A.profile_hi, A.n_profile);
+            HPQ_LAUNCH_CHECK();
+            // ---- forward: the march without the beam push, checkpoints and records. The slice
+            // graph of the adjoint forward replaces the step's graph until this call returns.
+            struct Restore {
+                Sim* s;
+                ~Restore() {
+                    cudaStreamSynchronize(s->st);
+                    s->adj_fwd = false;
+                    s->adj_plasma_scale = 1.0;
+                    s->invalidate_graph();
+                }
+            } restore{this};
+            invalidate_graph();
+            adj_fwd = true;
+            adj_plasma_scale = sigma;
+            begin_step(cur_step);
+            adj_plasma_scale = 1.0;
+            hpq_launch(k_adj_set_slice, dim3(1), dim3(1), 0, st, ctl, nz - 1, 1);
+            HPQ_LAUNCH_CHECK();
+            HPQ_CUDA(cudaMemcpyAsync(a.w_step, pl[0].w, a.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            for (int s = nz - 1; s >= 0; --s) solve_slice(s);
+            std::vector<double> obj((size_t)nz * 3);
+            HPQ_CUDA(cudaMemcpyAsync(obj.data(), a.obj, obj.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            HPQ_CUDA(cudaStreamSynchronize(st));
+            double S0 = 0, S1 = 0, S2 = 0;
+            for (int s = nz - 1; s >= 0; --s) { S0 += obj[3 * s]; S1 += obj[3 * s + 1]; S2 += obj[3 * s + 2]; }
+            const double Ebar = S0 != 0 ? S1 / S0 : 0.0;
+            const double J = S0 != 0 ? S2 / S0 - Ebar * Ebar : 0.0;
+            if (grad) {
+                adj_reverse(J, Ebar, S0);
+                std::vector<double> gp(A.n_profile), ions(nz);
+                double sig = 0;
+                HPQ_CUDA(cudaMemcpyAsync(gp.data(), a.grad, A.n_profile * sizeof(double), cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaMemcpyAsync(ions.data(), a.ions, nz * sizeof(double), cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaMemcpyAsync(&sig, a.sig, sizeof(double), cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaStreamSynchronize(st));
+                for (int k = 0; k < np; ++k) grad[k] = k < A.n_profile ? gp[k] : 0.0;
+                double dsig = sig;
+                for (int s = 0; s < nz; ++s) dsig += ions[s];
+                dsig /= sigma;
+                int kk; double fr;
+                if (knot_interval(ct, A.density_lo, A.density_hi, A.n_density, true, kk, fr)) {
+                    if (A.n_density == 1) grad[A.n_profile] += dsig;
+                    else { grad[A.n_profile + kk] += (1 - fr) * dsig; grad[A.n_profile + kk + 1] += fr * dsig; }
+                }
+            }
+            HPQ_CUDA(cudaMemcpyAsync(ctl_h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+            HPQ_CUDA(cudaStreamSynchronize(st));
+            if (ctl_h->mgp_bar_err) throw CudaError("hpmg: grid barrier of the persistent multigrid solve timed out");
+            if (ctl_h->mg_status == 1) throw CudaError("hpmg: failed to converge within the iteration limit");
+            if (ctl_h->mg_status == 2) throw CudaError("hpmg: diverged");
+            return J;
+        }
+    }
+
+    void adj_reverse(double J, double Ebar, double S0) {
+        AdjBuf& a = adjb;
+        const AdjointConfig& A = cfg.adjoint;
+        const int wb = A.witness;
+        const size_t n = (size_t)a.n;
+        for (auto* q : a.lam[0]) HPQ_CUDA(cudaMemsetAsync(q, 0, n * sizeof(double), st));
+        HPQ_CUDA(cudaMemsetAsync(a.lw, 0, n * sizeof(double), st));
+        HPQ_CUDA(cudaMemsetAsync(a.lwb, 0, a.cap * sizeof(double), st));
+        HPQ_CUDA(cudaMemsetAsync(a.ions, 0, nz * sizeof(double), st));
+        int cur = 0;
+        for (int c = a.C - 1; c >= 0; --c) {
+            const int hi = nz - 1 - c * a.K, lo = std::max(hi - a.K + 1, 0);
+            if (c != a.C - 1) {
+                // recompute the segment from its checkpoint (records only)
+                for (int k = 0; k < 11; ++k)
+                    HPQ_CUDA(cudaMemcpyAsync((void*)a.ck_args.src[k], a.ck_pl[k] + (size_t)c * n, n * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, st));
+                HPQ_CUDA(cudaMemcpyAsync(pl[0].valid, a.ck_valid + (size_t)c * n, n, cudaMemcpyDeviceToDevice, st));
+                HPQ_CUDA(cudaMemcpyAsync(S.base, a.ck_slab + (size_t)c * S.cstride * C_NCOMP,
+                                         S.cstride * C_NCOMP * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                hpq_launch(k_adj_set_slice, dim3(1), dim3(1), 0, st, ctl, hi, 0);
+                HPQ_LAUNCH_CHECK();
+                cur_islice = hi;
+                for (int s = hi; s >= lo; --s) solve_slice(s);
+            }
+            for (int s = lo; s <= hi; ++s) {
+                adj_reverse_slice(s, s - lo, cur, J, Ebar, S0);
+                cur = 1 - cur;
+            }
+        }
+        // parameters: witness profile knots and the plasma weight term of dJ/dsigma
+        hpq_launch(k_adj_knot_grad, dim3(A.n_profile), dim3(256), 0, st, bm[wb], parity, nz, (const double*)a.lwb,
+                   (const double*)a.w0, A.profile_lo, A.profile_hi, A.n_profile, a.grad);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_adj_dot, dim3(1), dim3(1024), 0, st, (const double*)a.lw, (const double*)a.w_step, a.n, a.sig);
+        HPQ_LAUNCH_CHECK();
+    }
+
+    void adj_reverse_slice(int s, int slot, int cur, double J, double Ebar, double S0) {
+        AdjBuf& a = adjb;
+        const AdjointConfig& A = cfg.adjoint;
+        const int wb = A.witness;
+        const size_t n = (size_t)a.n, cs = S.cstride;
+        const PlasmaDev<R>& P0 = pl[0];
+        AdjPlasma P{a.rec_pl[0] + slot * n, a.rec_pl[1] + slot * n, a.rec_pl[2] + slot * n, a.rec_pl[3] + slot * n,
+                    a.rec_pl[4] + slot * n, a.rec_pl[5] + slot * n, a.rec_pl[6] + slot * n, a.rec_pl[7] + slot * n,
+                    a.w_step, a.rec_valid + slot * n, a.n, P0.charge, P0.mass};
+        AdjRecF F;
+        for (int k = 0; k < RF_N; ++k) F.f[k] = F2<double>{a.rec_f[k] + slot * cs, S.pitch};
+        AdjL L;
+        for (int k = 0; k < A_NCOMP; ++k) L.f[k] = a.L.c(k);
+        const double* const* lo_ = a.lam[cur];
+        AdjLam lout{a.lam[cur][0], a.lam[cur][1], a.lam[cur][2], a.lam[cur][3], a.lam[cur][4], a.lam[cur][5],
+                    a.lam[cur][6], a.lam[cur][7]};
+        (void)lo_;
+        AdjLam lin{a.lam[1 - cur][0], a.lam[1 - cur][1], a.lam[1 - cur][2], a.lam[1 - cur][3], a.lam[1 - cur][4],
+                   a.lam[1 - cur][5], a.lam[1 - cur][6], a.lam[1 - cur][7]};
+        Geo gg = g;
+        const int nbp = blocks_for(a.n, 128);
+        HPQ_CUDA(cudaMemsetAsync(a.L.base, 0, cs * A_NCOMP * sizeof(double), st));
+        // plasma push
+        hpq_launch(k_adj_push, dim3(nbp), dim3(128), 0, st, P, lout, lin, F, L, gg);
+        HPQ_LAUNCH_CHECK();
+        // objective
+        const double zc = cfg.prob_lo[2] + (s + 0.5) * g.dx[2];
+        if (zc >= A.objective_lo && zc <= A.objective_hi && S0 != 0.0) {
+            hpq_launch(k_adj_objective, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, L, F, nx, ny, J, Ebar, S0);
+            HPQ_LAUNCH_CHECK();
+        }
+        // multigrid (transposed solve)
+        const int ncell = (int)cs;
+        hpq_launch(k_adj_mg_pre, dim3(blocks_for(ncell, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
+        HPQ_LAUNCH_CHECK();
+        if constexpr (std::is_same<R, double>::value) {
+            if (mg.cell) mg_solve_t<true>(a.M); else mg_solve_t<false>(a.M);
+        }
+        hpq_launch(k_adj_mg_post, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
+        HPQ_LAUNCH_CHECK();
+        // explicit Sx/Sy deposit
+        if (cfg.depos_derivative_type == 0) hpq_launch(k_adj_explicit<0>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
+        else if (cfg.depos_derivative_type == 1) hpq_launch(k_adj_explicit<1>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
+        else hpq_launch(k_adj_explicit<2>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
+        HPQ_LAUNCH_CHECK();
+        // beam part of Sx/Sy, -grad Psi, Poisson stage; the three solves; right-hand sides
+        if constexpr (std::is_same<R, double>::value) {
+            hpq_launch(k_adj_sxsy_stage, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny,
+                       dst.stage, dst.sk, dst.sj);
+            HPQ_LAUNCH_CHECK();
+            const int comps[3] = {A_VPSI, A_VEZ, A_VBZ};
+            dst.solve(st, 3, a.L.base, a.L.cstride, a.L.pitch, comps);
+        }
+        hpq_launch(k_adj_rhs_t, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny);
+        HPQ_LAUNCH_CHECK();
+        // plasma deposit
+        hpq_launch(k_adj_deposit, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, L, gg);
+        HPQ_LAUNCH_CHECK();
+        // ion background (scaled by the density multiplier like the plasma)
+        if (cfg.any_neutralize_background()) {
+            if constexpr (std::is_same<R, double>::value) {
+                hpq_launch(k_adj_plane_dot, dim3(1), dim3(1024), 0, st, L.f[A_RM], S.c(C_IONS), nx, ny, a.ions + s);
+                HPQ_LAUNCH_CHECK();
+            }
+        }
+        // beam deposits of the witness: jz (and rho - jz) of this slice's particles, their jx/jy
+        // (deposited one slice earlier into this slice's jx/jy), and the jx/jy of the previous and
+        // next slices' particles read by the beam part of Sx/Sy
+        const bool jxy = cfg.do_beam_jx_jy_deposition;
+        const int pitch = S.pitch;
+        hpq_launch(k_adj_beam, dim3(148), dim3(256), 0, st, bm[wb], parity, s, (const double*)L.f[A_JZB].p,
+                   cfg.do_beam_jz_minus_rho ? (const double*)L.f[A_RM].p : (const double*)nullptr,
+                   (jxy && s <= nz - 2) ? (const double*)L.f[A_JX].p : (const double*)nullptr,
+                   (const double*)L.f[A_JY].p, pitch, gg, a.lwb);
+        HPQ_LAUNCH_CHECK();
+        if (jxy && s + 1 <= nz - 2) {
+            hpq_launch(k_adj_beam, dim3(148), dim3(256), 0, st, bm[wb], parity, s + 1, (const double*)nullptr,
+                       (const double*)nullptr, (const double*)L.f[A_PJX].p, (const double*)L.f[A_PJY].p, pitch, gg, a.lwb);
+            HPQ_LAUNCH_CHECK();
+        }
+        if (jxy && s - 1 >= 0) {
+            hpq_launch(k_adj_beam, dim3(148), dim3(256), 0, st, bm[wb], parity, s - 1, (const double*)nullptr,
+                       (const double*)nullptr, (const double*)L.f[A_NJX].p, (const double*)L.f[A_NJY].p, pitch, gg, a.lwb);
+            HPQ_LAUNCH_CHECK();
+        }
     }
 
     // one slice: replay the captured graph, or launch kernel by kernel (profiling mode)
@@ -1049,6 +1366,11 @@ public:
     // Hipace::SolveOneSlice (Hipace.cpp:556-728)
     void record_slice() {
         const bool ex = cfg.explicit_solver;
+        if (adj_fwd) {
+            // adjoint forward: the state entering a segment head is checkpointed
+            hpq_launch(k_adj_checkpoint<R>, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.ck_args);
+            HPQ_LAUNCH_CHECK();
+        }
         if (ex) {
             if (cfg.deposit_rho) zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB, C_RHO});
             else zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB});
@@ -1099,6 +1421,15 @@ public:
         } else {
             pc_loop();
         }
+        if (adj_fwd) {
+            // adjoint forward: objective sums and the record of this slice (plasma state after the
+            // deposit's QSA test, the fields the reverse sweep reads)
+            hpq_launch(k_adj_objective_sums<R>, dim3(1), dim3(1024), 0, st, S, (const Ctl*)ctl, g,
+                       cfg.adjoint.objective_lo, cfg.adjoint.objective_hi, adjb.obj);
+            HPQ_LAUNCH_CHECK();
+            hpq_launch(k_adj_record<R>, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.rec_args);
+            HPQ_LAUNCH_CHECK();
+        }
         if (diag_list.n > 0) {
             hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)nx * ny * diag_list.n, 256)), dim3(256), 0, st, S, ctl, diag_list, diag_buf, nz);
             HPQ_LAUNCH_CHECK();
@@ -1110,7 +1441,9 @@ public:
         }
         // the beam push and partition (beam arrays, Ctl) run beside the plasma push and the
         // component shifts (plasma arrays, slab planes the pushes do not read)
-        {
+        // (the adjoint forward leaves the beam as it is: its push only feeds the next step)
+        const bool beams = !adj_fwd && !bm.empty();
+        if (beams) {
             OnStream on(this, side_begin());
             for (size_t b = 0; b < bm.size(); ++b) {
                 // beam in-situ reductions before the push (Hipace.cpp:680-681)
@@ -1141,8 +1474,8 @@ public:
         } else {
             copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
         }
-        side_end();
-        if (bm.empty()) {
+        if (beams) side_end();
+        else {
             hpq_launch(k_slice_done, dim3(1), dim3(1), 0, st, ctl);
             HPQ_LAUNCH_CHECK();
         }

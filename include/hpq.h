@@ -117,6 +117,24 @@ int hpq_set_graphs(hpq_handle* h, int on);
  * and has no such mode; the values agree with the default mode to FP64 rounding. Allowed between
  * steps. */
 int hpq_set_deterministic(hpq_handle* h, int on);
+/* Adjoint of one step (plain FP64 path; the reference has no adjoint). Configured with the
+ * adjoint.* input keys: the objective is the current-weighted variance of Ez over the slices
+ * whose centre lies in adjoint.objective_zeta,
+ *   J = S2/S0 - (S1/S0)^2,  S_n = sum over those slices and cells of jz_beam * Ez^n,
+ * and the parameters are n_profile + n_density knot values:
+ *   knots[0, n_profile): the witness beam (adjoint.witness) current profile, piecewise linear on
+ *     n_profile equidistant points of adjoint.profile_zeta, multiplying the witness weights
+ *     given by hpq_set_beam or the injection (zero outside the range);
+ *   knots[n_profile, n_profile + n_density): the plasma density multiplier, piecewise linear on
+ *     adjoint.density_z, evaluated at z = c t of the step (end values held outside).
+ * hpq_adjoint_grad runs the forward of the next step (without advancing time or the beam; the
+ * witness weights of the store are left multiplied by the profile) and, if grad is not NULL, the
+ * reverse sweep with checkpoints every adjoint.checkpoint_interval slices, writing dJ/dknots.
+ * The forward map replaces, for the gradient, the step of Hipace::Evolve (Hipace.cpp:393-554) and
+ * the slice loop of Hipace::SolveOneSlice (Hipace.cpp:556-728). Explicit solver, one plasma
+ * species with n_subcycles 1. */
+int hpq_adjoint_nparams(hpq_handle* h, int* n);
+int hpq_adjoint_grad(hpq_handle* h, const double* knots, double* grad, double* objective);
 /* Wait for all work of the handle. */
 int hpq_synchronize(hpq_handle* h);
 /* Per-kernel-class timing with CUDA events on the launching stream (kernel launch mode only).

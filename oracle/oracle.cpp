@@ -421,6 +421,80 @@ struct Multigrid {
 };
 
 // ------------------------------------------------------------------------------------------
+// Forward-mode tangent numbers for the adjoint: value and one directional derivative. The
+// per-particle maps (deposit, explicit deposit, gather + push) are written once for a generic
+// scalar type; the adjoint of a particle's contribution L = sum(lambda * output) with respect to
+// one input is L's tangent when that input is seeded with 1.
+// ------------------------------------------------------------------------------------------
+struct Tn { double v, d; };
+static inline Tn operator+(Tn a, Tn b) { return {a.v + b.v, a.d + b.d}; }
+static inline Tn operator-(Tn a, Tn b) { return {a.v - b.v, a.d - b.d}; }
+static inline Tn operator*(Tn a, Tn b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+static inline Tn operator/(Tn a, Tn b) { const double q = a.v / b.v; return {q, (a.d - q * b.d) / b.v}; }
+static inline Tn operator-(Tn a) { return {-a.v, -a.d}; }
+static inline Tn operator+(Tn a) { return a; }
+static inline Tn operator+(Tn a, double b) { return {a.v + b, a.d}; }
+static inline Tn operator+(double a, Tn b) { return {a + b.v, b.d}; }
+static inline Tn operator-(Tn a, double b) { return {a.v - b, a.d}; }
+static inline Tn operator-(double a, Tn b) { return {a - b.v, -b.d}; }
+static inline Tn operator*(Tn a, double b) { return {a.v * b, a.d * b}; }
+static inline Tn operator*(double a, Tn b) { return {a * b.v, a * b.d}; }
+static inline Tn operator/(Tn a, double b) { return {a.v / b, a.d / b}; }
+static inline Tn operator/(double a, Tn b) { const double q = a / b.v; return {q, -q * b.d / b.v}; }
+static inline double val(double a) { return a; }
+static inline double val(Tn a) { return a.v; }
+static inline Tn seed(double v, bool on) { return {v, on ? 1.0 : 0.0}; }
+
+template <class T> struct ShapeT { T s; int cell; };
+template <class T> struct DShapeT { T s, ds; int cell; };
+
+// shape2 / dshape2 above on a generic scalar (same expressions)
+template <class T>
+static inline ShapeT<T> shape2t(T xmid, int ix) {
+    const double xfloor = std::floor(val(xmid) + 0.5);
+    const T xint = xmid - xfloor;
+    if (ix == 0) return {0.5 * (0.5 - xint) * (0.5 - xint), (int)xfloor - 1};
+    if (ix == 1) return {0.75 - xint * xint, (int)xfloor};
+    return {0.5 * (0.5 + xint) * (0.5 + xint), (int)xfloor + 1};
+}
+template <class T>
+static inline DShapeT<T> dshape2t(int type, T xmid, int ix) {
+    if (type == 0) {
+        xmid = xmid + 0.5;
+        const double xfloor = std::floor(val(xmid));
+        const T xint = xmid - xfloor, x2 = xint * xint;
+        if (ix == 0) return {0.5 * x2 - 1.0 * xint + 0.5, -(xint - 1.0), (int)xfloor - 1 + ix};
+        if (ix == 1) return {-x2 + 1.0 * xint + 0.5, -(1.0 - 2 * xint), (int)xfloor - 1 + ix};
+        return {0.5 * x2, -xint, (int)xfloor - 1 + ix};
+    } else if (type == 1) {
+        const double xfloor = std::floor(val(xmid));
+        const T xint = xmid - xfloor, x2 = xint * xint;
+        const bool lo = val(xint) < 0.5;
+        const T zero = 0.0 * xint;
+        if (ix == 0) return {lo ? 0.5 * x2 - 0.5 * xint + 1.0 / 8.0 : zero, -(-0.5 * x2 + xint - 0.5), (int)xfloor - 1 + ix};
+        if (ix == 1) return {lo ? 0.75 - x2 : 0.5 * x2 - 1.5 * xint + 9.0 / 8.0, -(1.5 * x2 - 2 * xint), (int)xfloor - 1 + ix};
+        if (ix == 2) return {lo ? 0.5 * x2 + 0.5 * xint + 1.0 / 8.0 : -x2 + 2 * xint - 0.25, -(-1.5 * x2 + xint + 0.5), (int)xfloor - 1 + ix};
+        return {lo ? zero : 0.5 * x2 - 0.5 * xint + 1.0 / 8.0, -(0.5 * x2), (int)xfloor - 1 + ix};
+    } else {
+        xmid = xmid + 0.5;
+        const double xfloor = std::floor(val(xmid));
+        const T xint = xmid - xfloor, x2 = xint * xint;
+        const T zero = 0.0 * xint;
+        if (ix == 0) return {zero, -(-0.25 * x2 + 0.5 * xint - 0.25), (int)xfloor - 2 + ix};
+        if (ix == 1) return {0.5 * x2 - xint + 0.5, -(0.5 * x2 - 0.5 * xint - 0.25), (int)xfloor - 2 + ix};
+        if (ix == 2) return {-x2 + xint + 0.5, -(0.25 - 0.5 * xint), (int)xfloor - 2 + ix};
+        if (ix == 3) return {0.5 * x2, -(-0.5 * x2 + 0.5 * xint + 0.25), (int)xfloor - 2 + ix};
+        return {zero, -(0.25 * x2), (int)xfloor - 2 + ix};
+    }
+}
+
+// Taylor dual (value, d/dzeta) over a generic scalar, as in the plasma push
+template <class T> struct DuT { T v, e; };
+template <class T> static inline DuT<T> tadd(DuT<T> a, DuT<T> b) { return {a.v + b.v, a.e + b.e}; }
+template <class T> static inline DuT<T> tsub(DuT<T> a, DuT<T> b) { return {a.v - b.v, a.e - b.e}; }
+template <class T> static inline DuT<T> tmul(DuT<T> a, DuT<T> b) { return {a.v * b.v, a.e * b.v + a.v * b.e}; }
+
+// ------------------------------------------------------------------------------------------
 // The simulation
 // ------------------------------------------------------------------------------------------
 class Sim {
@@ -1201,6 +1275,585 @@ public:
         }
     }
 
+    // ======================================================================================
+    // Adjoint of one step (explicit solver) with respect to the witness current-profile knots
+    // and the plasma-density knots (hpq::AdjointConfig). The forward is the slice march of
+    // solve_one_slice without the beam push (the beam push of this step only feeds the next
+    // step); every slice's plasma state and fields are kept (small cases only), then the
+    // slices are swept backwards:
+    //   push            -> tangent passes of gather + push, field adjoints scattered by the
+    //                      gather shapes (gather-adjoint = deposit)
+    //   objective       -> dJ/dEz = 2 jz (Ez - Ebar)/S0, dJ/djz = ((Ez - Ebar)^2 - J)/S0
+    //   multigrid       -> one solve with the transposed operator (W A W^-1, W = 3/4 on the
+    //                      cell-centred boundary rows of the 4/3 closure, else 1); dJ/dchi = mu B
+    //   explicit Sx/Sy  -> tangent passes per particle; field adjoints in closed form
+    //   Sx/Sy beam part -> transposed centred differences
+    //   Psi, Ez, Bz     -> the DST solve is symmetric; transposed gradient/divergence/curl
+    //   deposit         -> tangent passes per particle (deposit-adjoint = gather)
+    //   beam deposits   -> linear in the witness weights
+    // ======================================================================================
+    const double* adj_theta = nullptr;  // parameters during an adjoint evaluation
+    double adj_sigma = 1.0;             // plasma density multiplier of the step
+
+    double adj_profile(double z) const {
+        const hpq::AdjointConfig& a = cfg.adjoint;
+        return hpq::knot_value(adj_theta, z, a.profile_lo, a.profile_hi, a.n_profile, false);
+    }
+
+    struct AdjSlice {
+        std::vector<Plasma> plasma;  // state entering the slice
+        Field Psi, Ez, Bz, Bx, By, ExmBy, EypBx, chi, jzb;
+    };
+
+    // one slice of the forward without the beam push (explicit solver); objective sums added
+    void adj_forward_slice(int islice, double* S) {
+        for (auto n : {"chi", "Sy", "Sx", "ExmBy", "EypBx", "jz_beam", "rhomjz", "Next.jx_beam", "Next.jy_beam", "rhomjz_beam"}) f(n).zero();
+        if (cfg.deposit_rho) f("rho").zero();
+        if (islice == nz - 1)
+            for (size_t b = 0; b < cfg.beams.size(); ++b) adj_load((int)b, islice, bthis[b]);
+        plasma_deposit(0, true, false, cfg.deposit_rho, true, true);
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            beam_deposit(bthis[b], cfg.beams[b].charge, nullptr, nullptr, &f("jz_beam"),
+                         cfg.do_beam_jz_minus_rho ? &f("rhomjz_beam") : nullptr);
+        if (cfg.any_neutralize_background()) {
+            Field& r = f("rhomjz"); const Field& ions = f("Ions.rhomjz");
+            for (size_t k = 0; k < r.a.size(); ++k) r.a[k] += ions.a[k];
+            if (cfg.deposit_rho) { Field& rr = f("rho"); for (size_t k = 0; k < rr.a.size(); ++k) rr.a[k] += ions.a[k]; }
+        }
+        solve_psi_ez_bz();
+        if (islice - 1 >= 0)
+            for (size_t b = 0; b < cfg.beams.size(); ++b) adj_load((int)b, islice - 1, bnext[b]);
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (cfg.do_beam_jx_jy_deposition && islice - 1 >= 0)
+                beam_deposit(bnext[b], cfg.beams[b].charge, &f("Next.jx_beam"), &f("Next.jy_beam"), nullptr, nullptr);
+        init_sxsy_with_beam();
+        explicit_deposit();
+        int iters = 0;
+        const int st = mg.solve(f("Bx"), f("By"), f("Sy"), f("Sx"), f("chi"), cfg.mg_tol_rel, cfg.mg_tol_abs,
+                                cfg.mg_max_iters, &iters);
+        mg_iters_total += iters;
+        if (st != 0 && mg_status == 0) mg_status = st;
+        if (adj_objective_slice(islice)) {
+            const Field& jz = f("jz_beam"); const Field& Ez = f("Ez");
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double a = jz(i, j), e = Ez(i, j);
+                    S[0] += a; S[1] += a * e; S[2] += a * e * e;
+                }
+        }
+        plasma_push(false);
+        copy(f("Prev.jx_beam"), f("jx_beam")); copy(f("Prev.jy_beam"), f("jy_beam"));
+        copy(f("jx_beam"), f("Next.jx_beam")); copy(f("jy_beam"), f("Next.jy_beam"));
+        copy(f("jx"), f("Next.jx_beam")); copy(f("jy"), f("Next.jy_beam"));
+        for (size_t b = 0; b < cfg.beams.size(); ++b) { bthis[b] = bnext[b]; bnext[b].p.clear(); bnext[b].num_nonslipped = 0; }
+    }
+    bool adj_objective_slice(int islice) const {
+        const double zc = cfg.prob_lo[2] + (islice + 0.5) * dz;
+        return zc >= cfg.adjoint.objective_lo && zc <= cfg.adjoint.objective_hi;
+    }
+    // beam slice with the witness weights multiplied by the profile
+    void adj_load(int b, int islice, BeamSlice& dst_slice) {
+        load_beam_slice(b, islice, dst_slice);
+        if (b == cfg.adjoint.witness)
+            for (auto& p : dst_slice.p) p.w *= adj_profile(p.z);
+    }
+
+    // the step's start: fields reset, plasma created and scaled by the density multiplier
+    void adj_begin(const double* theta, Field* ions0) {
+        adj_theta = theta;
+        const hpq::AdjointConfig& a = cfg.adjoint;
+        adj_sigma = hpq::knot_value(theta + a.n_profile, cfg.pc.c * physical_time, a.density_lo, a.density_hi,
+                                    a.n_density, true);
+        for (auto& kv : F) kv.second.zero();
+        init_plasmas();
+        if (cfg.any_neutralize_background()) plasma_deposit_ions();
+        if (ions0) *ions0 = f("Ions.rhomjz");
+        for (auto& pl : plasmas) for (auto& w : pl.w) w *= adj_sigma;
+        for (auto& v : f("Ions.rhomjz").a) v *= adj_sigma;
+    }
+
+    double adj_objective(const double* S) const {
+        if (S[0] == 0.0) return 0.0;
+        const double m = S[1] / S[0];
+        return S[2] / S[0] - m * m;
+    }
+
+    // forward only: the objective for parameters theta
+    double adjoint_objective(const double* theta) {
+        adj_begin(theta, nullptr);
+        double S[3] = {0, 0, 0};
+        for (int isl = nz - 1; isl >= 0; --isl) adj_forward_slice(isl, S);
+        adj_theta = nullptr;
+        return adj_objective(S);
+    }
+
+    // ---- per-particle maps on a generic scalar
+    template <class T>
+    void gather_t(T xp, T yp, T* G) {
+        const Field& Psi = f("Psi"); const Field& FEz = f("Ez");
+        const Field& FBx = f("Bx"); const Field& FBy = f("By"); const Field& FBz = f("Bz");
+        const T x = (xp - xoff) * dxi, y = (yp - yoff) * dyi;
+        for (int c = 0; c < 6; ++c) G[c] = 0.0 * x;
+        for (int iy = 0; iy <= 3; iy++)
+            for (int ix = 0; ix <= 3; ix++) {
+                DShapeT<T> sy = dshape2t(1, y, iy);
+                DShapeT<T> sx = dshape2t(1, x, ix);
+                const int i = sx.cell, j = sy.cell;
+                G[0] = G[0] + (sx.ds * sy.s) * Psi(i, j) * dxi;
+                G[1] = G[1] + (sx.s * sy.ds) * Psi(i, j) * dyi;
+                G[2] = G[2] + (sx.s * sy.s) * FEz(i, j);
+                G[3] = G[3] + (sx.s * sy.s) * FBx(i, j);
+                G[4] = G[4] + (sx.s * sy.s) * FBy(i, j);
+                G[5] = G[5] + (sx.s * sy.s) * FBz(i, j);
+            }
+        G[3] = G[3] * cfg.pc.c;
+        G[4] = G[4] * cfg.pc.c;
+    }
+    template <class T>
+    bool enforce_bc_t(T& x, T& y, T& ux, T& uy) const {
+        const double plo0 = cfg.particle_lo[0], plo1 = cfg.particle_lo[1];
+        const double phi0 = cfg.particle_hi[0], phi1 = cfg.particle_hi[1];
+        if (val(x) < plo0 || val(y) < plo1 || val(x) > phi0 || val(y) > phi1) {
+            const double lx = phi0 - plo0, ly = phi1 - plo1;
+            if (cfg.particle_bc == hpq::ParticleBC::Absorbing) return false;
+            const bool refl = cfg.particle_bc == hpq::ParticleBC::Reflecting;
+            const double px = refl ? 2 * lx : lx, py = refl ? 2 * ly : ly;
+            double m = std::fmod(val(x) - plo0, px); if (m < 0) m += px;
+            x = x + ((m + plo0) - val(x));
+            m = std::fmod(val(y) - plo1, py); if (m < 0) m += py;
+            y = y + ((m + plo1) - val(y));
+            if (refl && val(x) > phi0) { x = 2 * phi0 - x; ux = -ux; }
+            if (refl && val(y) > phi1) { y = 2 * phi1 - y; uy = -uy; }
+        }
+        return true;
+    }
+    // gather fields G (ExmBy, EypBx, Ez, c Bx, c By, Bz) given; push of one particle, n_subcycles 1.
+    // out: x, y, ux_h, uy_h, psi_h, ux, uy, psi
+    template <class T>
+    bool push_t(T x, T y, T ux, T uy, T psi, const T* G, double qmc, T* out) const {
+        const double ci = 1. / cfg.pc.c, dzs = dz;
+        const double sdz = dzs / 4;
+        auto substep = [&]() {
+            const T psi_inv = 1. / psi;
+            const T gamma_psi = 0.5 * psi_inv * psi_inv * (1.0 + ux * ux * (ci * ci) + uy * uy * (ci * ci)) + 0.5;
+            const T d_ux = qmc * (gamma_psi * G[0] + G[4] + (uy * G[5]) * psi_inv);
+            const T d_uy = qmc * (gamma_psi * G[1] - G[3] - (ux * G[5]) * psi_inv);
+            const T d_psi = qmc * ci * ((ux * G[0] + uy * G[1]) * ci * psi_inv - G[2]);
+            const T zero = 0.0 * psi;
+            DuT<T> dx_{ux, d_ux}, dy_{uy, d_uy}, dp{psi_inv, -psi_inv * psi_inv * d_psi};
+            const DuT<T> c2{zero + ci * ci, zero}, one{zero + 1.0, zero}, half{zero + 0.5, zero};
+            const DuT<T> q{zero + qmc, zero}, cc{zero + ci, zero};
+            const DuT<T> E0{G[0], zero}, E1{G[1], zero}, E2{G[2], zero}, B0{G[3], zero}, B1{G[4], zero}, B2{G[5], zero};
+            DuT<T> t = tadd(tadd(one, tmul(tmul(dx_, dx_), c2)), tmul(tmul(dy_, dy_), c2));
+            DuT<T> gp = tadd(tmul(tmul(tmul(half, dp), dp), t), half);
+            DuT<T> dux = tmul(q, tadd(tadd(tmul(gp, E0), B1), tmul(tmul(dy_, B2), dp)));
+            DuT<T> duy = tmul(q, tsub(tsub(tmul(gp, E1), B0), tmul(tmul(dx_, B2), dp)));
+            DuT<T> dps = tmul(tmul(q, cc), tsub(tmul(tmul(tadd(tmul(dx_, E0), tmul(dy_, E1)), cc), dp), E2));
+            ux = ux + sdz * d_ux + 0.5 * sdz * sdz * dux.e;
+            uy = uy + sdz * d_uy + 0.5 * sdz * sdz * duy.e;
+            psi = psi + sdz * d_psi + 0.5 * sdz * sdz * dps.e;
+        };
+        for (int k = 0; k < 4; ++k) substep();
+        x = x + dzs * ci * (ux * (1. / psi));
+        y = y + dzs * ci * (uy * (1. / psi));
+        if (!enforce_bc_t(x, y, ux, uy)) return false;
+        out[0] = x; out[1] = y; out[2] = ux; out[3] = uy; out[4] = psi;
+        for (int k = 0; k < 2; ++k) substep();
+        out[5] = ux; out[6] = uy; out[7] = psi;
+        return true;
+    }
+
+    struct AdjFields {
+        Field Psi, Ez, Bz, Bx, By, ExmBy, EypBx, Sx, Sy, chi, jx, jy, rm, jzb, Pjx, Pjy, Njx, Njy;
+        void init(const Grid& g) {
+            for (Field* q : {&Psi, &Ez, &Bz, &Bx, &By, &ExmBy, &EypBx, &Sx, &Sy, &chi, &jx, &jy, &rm, &jzb, &Pjx, &Pjy, &Njx, &Njy}) q->init(g);
+        }
+        void zero() {
+            for (Field* q : {&Psi, &Ez, &Bz, &Bx, &By, &ExmBy, &EypBx, &Sx, &Sy, &chi, &jx, &jy, &rm, &jzb, &Pjx, &Pjy, &Njx, &Njy}) q->zero();
+        }
+    };
+    struct PlasmaAdj { std::vector<double> x, y, uhx, uhy, psih, ux, uy, psi, w; };
+
+    static void zero_outside_interior(Field& q, int nx_, int ny_) {
+        const int g = q.gr.g;
+        for (int j = -g; j < ny_ + g; ++j)
+            for (int i = -g; i < nx_ + g; ++i)
+                if (i < 0 || j < 0 || i >= nx_ || j >= ny_) q(i, j) = 0.0;
+    }
+
+    // adjoint of the beam deposits of beam slice k of the witness: dJ/dw_eff per particle
+    void adj_beam(int k, const Field* ljz, const Field* lrm, const Field* ljx, const Field* ljy,
+                  std::vector<std::vector<double>>& lw) {
+        if (k < 0 || k >= nz) return;
+        const int b = cfg.adjoint.witness;
+        const BeamSlice& bs = store[b][k];
+        const double invvol = cfg.normalized_units ? 1.0 : dxi * dyi * dzi;
+        const double ci = 1.0 / cfg.pc.c, ci2 = ci * ci;
+        const double q = cfg.beams[b].charge;
+        for (size_t ip = 0; ip < bs.p.size(); ++ip) {
+            const BeamParticle& p = bs.p[ip];
+            if (!p.valid) continue;
+            const double gaminv = 1.0 / std::sqrt(1.0 + p.ux * p.ux * ci2 + p.uy * p.uy * ci2 + p.uz * p.uz * ci2);
+            const double vx = p.ux * gaminv, vy = p.uy * gaminv, vz = p.uz * gaminv;
+            const double xmid = (p.x - xoff) * dxi, ymid = (p.y - yoff) * dyi;
+            double acc = 0;
+            for (int iy = 0; iy <= 2; ++iy)
+                for (int ix = 0; ix <= 2; ++ix) {
+                    Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);
+                    const double S = sx.s * sy.s;
+                    const int i = sx.cell, j = sy.cell;
+                    double l = 0;
+                    if (ljz) l += vz * (*ljz)(i, j);
+                    if (lrm) l += (1. - vz * ci) * (*lrm)(i, j);
+                    if (ljx) l += vx * (*ljx)(i, j) + vy * (*ljy)(i, j);
+                    acc += S * l;
+                }
+            lw[k][ip] += q * invvol * acc;
+        }
+    }
+
+    // gradient of the objective; returns J
+    double adjoint_grad(const double* theta, double* grad) {
+        const hpq::AdjointConfig& A = cfg.adjoint;
+        Field ions0; ions0.init(gr);
+        adj_begin(theta, &ions0);
+        double S[3] = {0, 0, 0};
+        std::vector<AdjSlice> rec(nz);
+        std::vector<std::vector<double>> w0(plasmas.size());
+        for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+            w0[sp] = plasmas[sp].w;
+            for (auto& w : w0[sp]) w = adj_sigma != 0 ? w / adj_sigma : 0.0;
+        }
+        for (int isl = nz - 1; isl >= 0; --isl) {
+            rec[isl].plasma = plasmas;
+            adj_forward_slice(isl, S);
+            AdjSlice& r = rec[isl];
+            r.Psi = f("Psi"); r.Ez = f("Ez"); r.Bz = f("Bz"); r.Bx = f("Bx"); r.By = f("By");
+            r.ExmBy = f("ExmBy"); r.EypBx = f("EypBx"); r.chi = f("chi"); r.jzb = f("jz_beam");
+        }
+        const double J = adj_objective(S);
+        const double S0 = S[0], Ebar = S0 != 0 ? S[1] / S0 : 0.0;
+        const double mu0 = cfg.pc.mu0, ep0 = cfg.pc.ep0, cl = cfg.pc.c, ci = 1. / cl;
+        const double hx = 0.5 * dxi, hy = 0.5 * dyi;
+        // adjoint state
+        AdjFields L; L.init(gr);
+        std::vector<PlasmaAdj> lp(plasmas.size());
+        for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+            const size_t n = plasmas[sp].n();
+            for (auto* v : {&lp[sp].x, &lp[sp].y, &lp[sp].uhx, &lp[sp].uhy, &lp[sp].psih, &lp[sp].ux, &lp[sp].uy, &lp[sp].psi, &lp[sp].w})
+                v->assign(n, 0.0);
+        }
+        std::vector<std::vector<double>> lwb(nz);
+        const int wb = A.witness;
+        for (int k = 0; k < nz; ++k) lwb[k].assign(store[wb][k].p.size(), 0.0);
+        double dsigma_ions = 0;
+        Field sol[2], rhs[2];
+        for (int c = 0; c < 2; ++c) { sol[c].init(gr); rhs[c].init(gr); }
+
+        for (int isl = 0; isl < nz; ++isl) {
+            AdjSlice& r = rec[isl];
+            // the forward fields of this slice become current (gather/explicit read them)
+            f("Psi") = r.Psi; f("Ez") = r.Ez; f("Bz") = r.Bz; f("Bx") = r.Bx; f("By") = r.By;
+            f("ExmBy") = r.ExmBy; f("EypBx") = r.EypBx;
+            L.zero();
+            std::vector<PlasmaAdj> lin(plasmas.size());
+            for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+                const size_t n = plasmas[sp].n();
+                for (auto* v : {&lin[sp].x, &lin[sp].y, &lin[sp].uhx, &lin[sp].uhy, &lin[sp].psih, &lin[sp].ux, &lin[sp].uy, &lin[sp].psi})
+                    v->assign(n, 0.0);
+            }
+            // (1) plasma push
+            for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+                const hpq::PlasmaSpecies& P = cfg.plasmas[sp];
+                const Plasma& pl = r.plasma[sp];
+                const PlasmaAdj& lo = lp[sp];
+                const double qmc = P.charge / (P.mass * cl);
+                for (size_t ip = 0; ip < pl.n(); ++ip) {
+                    if (!pl.valid[ip] || !adj_alive(P, pl, ip)) continue;
+                    const double lout[8] = {lo.x[ip], lo.y[ip], lo.uhx[ip], lo.uhy[ip], lo.psih[ip], lo.ux[ip], lo.uy[ip], lo.psi[ip]};
+                    bool any = false;
+                    for (double v : lout) any = any || v != 0.0;
+                    if (!any) continue;
+                    const double in[5] = {pl.x_prev[ip], pl.y_prev[ip], pl.ux_h[ip], pl.uy_h[ip], pl.psi_h[ip]};
+                    double dl[5];
+                    bool alive = true;
+                    for (int k = 0; k < 5 && alive; ++k) {
+                        Tn t[5];
+                        for (int m = 0; m < 5; ++m) t[m] = seed(in[m], m == k);
+                        Tn G[6], out[8];
+                        gather_t(t[0], t[1], G);
+                        alive = push_t(t[0], t[1], t[2], t[3], t[4], G, qmc, out);
+                        double d = 0;
+                        for (int o = 0; o < 8; ++o) d += lout[o] * out[o].d;
+                        dl[k] = d;
+                    }
+                    if (!alive) continue;
+                    double Gv[6];
+                    gather_t(in[0], in[1], Gv);
+                    double lG[6];
+                    for (int c = 0; c < 6; ++c) {
+                        Tn t[5], G[6], out[8];
+                        for (int m = 0; m < 5; ++m) t[m] = seed(in[m], false);
+                        for (int m = 0; m < 6; ++m) G[m] = seed(Gv[m], m == c);
+                        push_t(t[0], t[1], t[2], t[3], t[4], G, qmc, out);
+                        double d = 0;
+                        for (int o = 0; o < 8; ++o) d += lout[o] * out[o].d;
+                        lG[c] = d;
+                    }
+                    PlasmaAdj& li = lin[sp];
+                    li.x[ip] += dl[0]; li.y[ip] += dl[1]; li.uhx[ip] += dl[2]; li.uhy[ip] += dl[3]; li.psih[ip] += dl[4];
+                    // gather adjoint: scatter by the gather shapes
+                    const double x = (in[0] - xoff) * dxi, y = (in[1] - yoff) * dyi;
+                    for (int iy = 0; iy <= 3; iy++)
+                        for (int ix = 0; ix <= 3; ix++) {
+                            DShape sy = dshape2(1, y, iy), sx = dshape2(1, x, ix);
+                            const int i = sx.cell, j = sy.cell;
+                            const double Sv = sx.s * sy.s;
+                            L.Psi(i, j) += lG[0] * sx.ds * sy.s * dxi + lG[1] * sx.s * sy.ds * dyi;
+                            L.Ez(i, j) += lG[2] * Sv;
+                            L.Bx(i, j) += lG[3] * cl * Sv;
+                            L.By(i, j) += lG[4] * cl * Sv;
+                            L.Bz(i, j) += lG[5] * Sv;
+                        }
+                }
+            }
+            // (2) objective
+            if (adj_objective_slice(isl) && S0 != 0) {
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        const double jz = r.jzb(i, j), e = r.Ez(i, j) - Ebar;
+                        L.Ez(i, j) += 2 * jz * e / S0;
+                        L.jzb(i, j) += (e * e - J) / S0;
+                    }
+            }
+            // (3) multigrid: mu = W A^-1 W^-1 lambda_B
+            for (Field* q : {&L.Bx, &L.By}) zero_outside_interior(*q, nx, ny);
+            const bool cellc = mg.cell;
+            auto wgt = [&](int i, int j) {
+                double w = 1;
+                if (cellc && (i == 0 || i == nx - 1)) w *= 0.75;
+                if (cellc && (j == 0 || j == ny - 1)) w *= 0.75;
+                return w;
+            };
+            for (int c = 0; c < 2; ++c) { sol[c].zero(); rhs[c].zero(); }
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    rhs[0](i, j) = L.Bx(i, j) / wgt(i, j);
+                    rhs[1](i, j) = L.By(i, j) / wgt(i, j);
+                }
+            {
+                int iters = 0;
+                mg.solve(sol[0], sol[1], rhs[0], rhs[1], r.chi, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, &iters);
+            }
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double mx = sol[0](i, j) * wgt(i, j), my = sol[1](i, j) * wgt(i, j);
+                    L.Sy(i, j) = mx;
+                    L.Sx(i, j) = my;
+                    L.chi(i, j) += mx * r.Bx(i, j) + my * r.By(i, j);
+                }
+            // (4) explicit deposit
+            adj_explicit(r, L, lin);
+            // (5) Sx/Sy beam part (Hipace.cpp:744-790)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double ly_ = L.Sy(i, j), lx_ = L.Sx(i, j);
+                    L.jzb(i, j + 1) += -mu0 / (2 * dy) * ly_;
+                    L.jzb(i, j - 1) += mu0 / (2 * dy) * ly_;
+                    L.jzb(i + 1, j) += mu0 / (2 * dx) * lx_;
+                    L.jzb(i - 1, j) += -mu0 / (2 * dx) * lx_;
+                    L.Pjy(i, j) += mu0 / (2 * dz) * ly_;
+                    L.Njy(i, j) += -mu0 / (2 * dz) * ly_;
+                    L.Pjx(i, j) += -mu0 / (2 * dz) * lx_;
+                    L.Njx(i, j) += mu0 / (2 * dz) * lx_;
+                }
+            // (6) ExmBy, EypBx = -grad Psi on [-1, n]
+            for (int j = -1; j <= ny; ++j)
+                for (int i = -1; i <= nx; ++i) {
+                    const double a = L.ExmBy(i, j), b = L.EypBx(i, j);
+                    L.Psi(i + 1, j) += -a * hx; L.Psi(i - 1, j) += a * hx;
+                    L.Psi(i, j + 1) += -b * hy; L.Psi(i, j - 1) += b * hy;
+                }
+            // (7) Poisson solves (symmetric), then transposed right-hand sides
+            std::vector<double> st((size_t)nx * ny);
+            auto solve_from = [&](const Field& q) {
+                for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) st[(size_t)j * nx + i] = q(i, j);
+                dst.solve(st);
+            };
+            solve_from(L.Psi);
+            for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) L.rm(i, j) += -1. / ep0 * st[(size_t)j * nx + i];
+            const double fe = 1. / (ep0 * cl);
+            solve_from(L.Ez);
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double v = st[(size_t)j * nx + i];
+                    L.jx(i + 1, j) += fe * hx * v; L.jx(i - 1, j) -= fe * hx * v;
+                    L.jy(i, j + 1) += fe * hy * v; L.jy(i, j - 1) -= fe * hy * v;
+                }
+            solve_from(L.Bz);
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double v = st[(size_t)j * nx + i];
+                    L.jx(i, j + 1) += mu0 * hy * v; L.jx(i, j - 1) -= mu0 * hy * v;
+                    L.jy(i + 1, j) -= mu0 * hx * v; L.jy(i - 1, j) += mu0 * hx * v;
+                }
+            // (8) plasma deposit
+            adj_deposit(r, L, lin);
+            // ions and beam
+            for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) dsigma_ions += L.rm(i, j) * ions0(i, j);
+            adj_beam(isl, &L.jzb, cfg.do_beam_jz_minus_rho ? &L.rm : nullptr,
+                     (cfg.do_beam_jx_jy_deposition && isl <= nz - 2) ? &L.jx : nullptr, &L.jy, lwb);
+            if (cfg.do_beam_jx_jy_deposition) {
+                if (isl + 1 <= nz - 2) adj_beam(isl + 1, nullptr, nullptr, &L.Pjx, &L.Pjy, lwb);
+                if (isl - 1 >= 0) adj_beam(isl - 1, nullptr, nullptr, &L.Njx, &L.Njy, lwb);
+            }
+            for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+                PlasmaAdj& a = lp[sp];
+                a.x = lin[sp].x; a.y = lin[sp].y; a.uhx = lin[sp].uhx; a.uhy = lin[sp].uhy; a.psih = lin[sp].psih;
+                a.ux = lin[sp].ux; a.uy = lin[sp].uy; a.psi = lin[sp].psi;
+                for (size_t ip = 0; ip < a.w.size(); ++ip) a.w[ip] += lin[sp].w.empty() ? 0.0 : lin[sp].w[ip];
+            }
+        }
+        // parameters
+        const int np = A.n_params();
+        for (int k = 0; k < np; ++k) grad[k] = 0;
+        for (int k = 0; k < nz; ++k) {
+            const BeamSlice& bs = store[wb][k];
+            for (size_t ip = 0; ip < bs.p.size(); ++ip) {
+                if (!bs.p[ip].valid || lwb[k][ip] == 0.0) continue;
+                int kk; double fr;
+                if (!hpq::knot_interval(bs.p[ip].z, A.profile_lo, A.profile_hi, A.n_profile, false, kk, fr)) continue;
+                const double g = lwb[k][ip] * bs.p[ip].w;
+                grad[kk] += (1 - fr) * g;
+                grad[kk + 1] += fr * g;
+            }
+        }
+        double dsigma = dsigma_ions;
+        for (size_t sp = 0; sp < plasmas.size(); ++sp)
+            for (size_t ip = 0; ip < w0[sp].size(); ++ip) dsigma += lp[sp].w[ip] * w0[sp][ip];
+        {
+            int kk; double fr;
+            if (hpq::knot_interval(cfg.pc.c * physical_time, A.density_lo, A.density_hi, A.n_density, true, kk, fr)) {
+                if (A.n_density == 1) grad[A.n_profile] += dsigma;
+                else { grad[A.n_profile + kk] += (1 - fr) * dsigma; grad[A.n_profile + kk + 1] += fr * dsigma; }
+            }
+        }
+        adj_theta = nullptr;
+        return J;
+    }
+
+    // the deposit's QSA test (PlasmaDepositCurrent.cpp:164-247) on the stored state
+    bool adj_alive(const hpq::PlasmaSpecies& P, const Plasma& pl, size_t ip) const {
+        const double psi_inv = 1.0 / pl.psi[ip];
+        const double ci = 1.0 / cfg.pc.c;
+        const double vx = pl.ux[ip] * psi_inv * ci, vy = pl.uy[ip] * psi_inv * ci;
+        const double gamma_psi = 0.5 * (psi_inv * psi_inv + vx * vx + vy * vy + 1.0);
+        return !(gamma_psi < 0.0 || gamma_psi > P.max_qsa_weighting_factor || psi_inv < 0.0);
+    }
+
+    template <class T>
+    T dep_L(const hpq::PlasmaSpecies& P, T x, T y, T ux, T uy, T psi, double w, const AdjFields& L) const {
+        const double invvol = cfg.normalized_units ? dx * dy * dxi * dyi : dxi * dyi * dzi;
+        const double clightinv = 1.0 / cfg.pc.c;
+        const double q_invvol = P.charge * invvol * w;
+        const double qm = P.charge * cfg.pc.mu0 / P.mass;
+        const T psi_inv = 1.0 / psi;
+        const T vx_c = ux * psi_inv, vy_c = uy * psi_inv;
+        (void)clightinv;
+        const T xmid = (x - xoff) * dxi, ymid = (y - yoff) * dyi;
+        T acc = 0.0 * x;
+        for (int iy = 0; iy <= 2; ++iy)
+            for (int ix = 0; ix <= 2; ++ix) {
+                ShapeT<T> sx = shape2t(xmid, ix), sy = shape2t(ymid, iy);
+                const int i = sx.cell, j = sy.cell;
+                const T cd = q_invvol * sx.s * sy.s;
+                acc = acc + cd * (vx_c * L.jx(i, j) + vy_c * L.jy(i, j) + qm * psi_inv * L.chi(i, j) + L.rm(i, j));
+            }
+        return acc;
+    }
+    void adj_deposit(const AdjSlice& r, const AdjFields& L, std::vector<PlasmaAdj>& lin) {
+        for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[sp];
+            const Plasma& pl = r.plasma[sp];
+            PlasmaAdj& li = lin[sp];
+            if (li.w.empty()) li.w.assign(pl.n(), 0.0);
+            for (size_t ip = 0; ip < pl.n(); ++ip) {
+                if (!pl.valid[ip] || !adj_alive(P, pl, ip)) continue;
+                const double in[5] = {pl.x[ip], pl.y[ip], pl.ux[ip], pl.uy[ip], pl.psi[ip]};
+                double d[5];
+                for (int k = 0; k < 5; ++k) {
+                    Tn t[5];
+                    for (int m = 0; m < 5; ++m) t[m] = seed(in[m], m == k);
+                    d[k] = dep_L(P, t[0], t[1], t[2], t[3], t[4], pl.w[ip], L).d;
+                }
+                li.x[ip] += d[0]; li.y[ip] += d[1]; li.ux[ip] += d[2]; li.uy[ip] += d[3]; li.psi[ip] += d[4];
+                li.w[ip] += dep_L(P, in[0], in[1], in[2], in[3], in[4], 1.0, L);
+            }
+        }
+    }
+
+    template <class T>
+    T ex_L(const hpq::PlasmaSpecies& P, T x, T y, T ux, T uy, T psi, double w, const AdjFields& L,
+           AdjFields* scatter) {
+        const int dt = cfg.depos_derivative_type;
+        const int ns = 2 + dt;
+        const Field& Bz = f("Bz"); const Field& Ez = f("Ez");
+        const Field& ExmBy = f("ExmBy"); const Field& EypBx = f("EypBx");
+        const double invvol = cfg.normalized_units ? dx * dy * dxi * dyi : dxi * dyi * dzi;
+        const double a_clight = cfg.pc.c, ci = 1. / cfg.pc.c;
+        const double cdm = P.charge * invvol * cfg.pc.mu0 * w;
+        const double qm = P.charge / P.mass;
+        const T psi_inv = 1. / psi;
+        const T vx = ux * psi_inv * ci, vy = uy * psi_inv * ci;
+        const T xmid = (x - xoff) * dxi, ymid = (y - yoff) * dyi;
+        const T gamma_psi = 0.5 * (psi_inv * psi_inv + vx * vx + vy * vy + 1.);
+        T acc = 0.0 * x;
+        for (int iy = 0; iy <= ns; ++iy)
+            for (int ix = 0; ix <= ns; ++ix) {
+                if (dt == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                DShapeT<T> sy = dshape2t(dt, ymid, iy);
+                DShapeT<T> sx = dshape2t(dt, xmid, ix);
+                const int i = sx.cell, j = sy.cell;
+                const double Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = ExmBy(i, j), EypBx_v = EypBx(i, j);
+                const T Sy_c = cdm * (-sx.s * sy.s * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * ci) * qm * psi_inv +
+                                      (-sx.ds * sy.s * dxi * (-vx * vy) - sx.s * sy.ds * dyi * (gamma_psi - vy * vy - 1.)) * a_clight);
+                const T Sx_c = cdm * (+sx.s * sy.s * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * ci) * qm * psi_inv +
+                                      (+sx.ds * sy.s * dxi * (gamma_psi - vx * vx - 1.) + sx.s * sy.ds * dyi * (-vx * vy)) * a_clight);
+                const double lSy = L.Sy(i, j), lSx = L.Sx(i, j);
+                acc = acc + lSy * Sy_c + lSx * Sx_c;
+                if (scatter) {
+                    const double K = val(cdm * sx.s * sy.s * qm * psi_inv);
+                    const double vxv = val(vx), vyv = val(vy), gp = val(gamma_psi);
+                    scatter->Bz(i, j) += lSy * K * vxv + lSx * K * vyv;
+                    scatter->Ez(i, j) += -lSy * K * vyv * ci + lSx * K * vxv * ci;
+                    scatter->ExmBy(i, j) += lSy * K * vxv * vyv * ci + lSx * K * (gp - vxv * vxv) * ci;
+                    scatter->EypBx(i, j) += -lSy * K * (gp - vyv * vyv) * ci - lSx * K * vxv * vyv * ci;
+                }
+            }
+        return acc;
+    }
+    void adj_explicit(const AdjSlice& r, AdjFields& L, std::vector<PlasmaAdj>& lin) {
+        for (size_t sp = 0; sp < plasmas.size(); ++sp) {
+            const hpq::PlasmaSpecies& P = cfg.plasmas[sp];
+            const Plasma& pl = r.plasma[sp];
+            PlasmaAdj& li = lin[sp];
+            if (li.w.empty()) li.w.assign(pl.n(), 0.0);
+            for (size_t ip = 0; ip < pl.n(); ++ip) {
+                if (!pl.valid[ip] || !adj_alive(P, pl, ip)) continue;
+                const double in[5] = {pl.x[ip], pl.y[ip], pl.ux[ip], pl.uy[ip], pl.psi[ip]};
+                double d[5];
+                for (int k = 0; k < 5; ++k) {
+                    Tn t[5];
+                    for (int m = 0; m < 5; ++m) t[m] = seed(in[m], m == k);
+                    d[k] = ex_L(P, t[0], t[1], t[2], t[3], t[4], pl.w[ip], L, nullptr).d;
+                }
+                li.x[ip] += d[0]; li.y[ip] += d[1]; li.ux[ip] += d[2]; li.uy[ip] += d[3]; li.psi[ip] += d[4];
+                li.w[ip] += ex_L(P, in[0], in[1], in[2], in[3], in[4], 1.0, L, nullptr);
+                ex_L(P, in[0], in[1], in[2], in[3], in[4], pl.w[ip], L, &L);
+            }
+        }
+    }
+
     int step(int s) {
         begin_step(s);
         for (int isl = nz - 1; isl >= 0; --isl) solve_one_slice(isl, s);
@@ -1334,6 +1987,17 @@ const char* oracle_error(OracleHandle* h) { return h->sim->error.c_str(); }
 // reduced-diagnostic arrays, value index outer, slice inner): beam: 22 x nz values (entry 0 the
 // sum of weights, the others divided by it), nz particle counts, 22 sums over slices, the total
 // count; fields: 10 x nz values, 10 sums.
+int oracle_adjoint_nparams(OracleHandle* h) {
+    return h->sim->cfg.adjoint.witness < 0 ? 0 : h->sim->cfg.adjoint.n_params();
+}
+// objective (and its gradient when grad != NULL) for parameters theta; 0 on success
+int oracle_adjoint(OracleHandle* h, const double* theta, double* grad, double* J) {
+    oracle::Sim& s = *h->sim;
+    if (s.cfg.adjoint.witness < 0) return 1;
+    for (size_t b = 0; b < s.cfg.beams.size(); ++b) if (!s.store_valid[b]) return 2;
+    *J = grad ? s.adjoint_grad(theta, grad) : s.adjoint_objective(theta);
+    return s.mg_status;
+}
 long long oracle_insitu_size(OracleHandle* h, const char* what) {
     auto& s = *h->sim;
     if (std::string(what) == "fields") return 11LL * s.nz;

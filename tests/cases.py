@@ -68,6 +68,72 @@ plasma.element = electron
 """
 
 
+# adjoint of one step: driver + witness ("can" profile on [-7, -5]), objective on the witness
+# slices, 16 witness-profile knots and 4 plasma-density knots; moderate driver so that no plasma
+# particle crosses the QSA filter (the objective is then differentiable in every parameter)
+ADJOINT_SMALL = """
+amr.n_cell = 32 32 64
+hipace.normalized_units = 1
+max_step = 0
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -6. -6. -10.
+geometry.prob_hi =  6.  6.  4.
+beams.names = driver witness
+driver.injection_type = fixed_weight
+driver.num_particles = 20000
+driver.position_mean = 0. 0. 0.
+driver.position_std = 0.3 0.3 1.0
+driver.density = 1.
+driver.u_mean = 0. 0. 2000.
+driver.u_std = 0.0333 0.0333 0.
+witness.injection_type = fixed_weight
+witness.profile = can
+witness.zmin = -7.
+witness.zmax = -5.
+witness.num_particles = 5000
+witness.position_mean = 0. 0. -6.
+witness.position_std = 0.1 0.1 1.
+witness.density = 5.
+witness.u_mean = 0. 0. 2000.
+random_seed = 11
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+hipace.MG_tolerance_rel = 1e-13
+adjoint.witness = witness
+adjoint.profile_zeta = -7. -5.
+adjoint.n_profile_knots = 16
+adjoint.density_z = -10. 10.
+adjoint.n_density_knots = 4
+adjoint.objective_zeta = -7. -5.
+adjoint.checkpoint_interval = 16
+"""
+
+
+def adjoint_beams(seed=1):
+    """Seeded driver and witness particles for ADJOINT_SMALL (same arrays for oracle and GPU)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n, m = 20000, 5000
+    driver = {"x": rng.normal(0, 0.3, n), "y": rng.normal(0, 0.3, n), "z": rng.normal(0, 1.0, n),
+              "w": np.full(n, 0.05), "ux": rng.normal(0, 0.0333, n), "uy": rng.normal(0, 0.0333, n),
+              "uz": np.full(n, 2000.), "id": np.arange(1, n + 1, dtype=np.int64)}
+    witness = {"x": rng.normal(0, 0.1, m), "y": rng.normal(0, 0.1, m), "z": rng.uniform(-7., -5., m),
+               "w": np.full(m, 0.01), "ux": np.zeros(m), "uy": np.zeros(m), "uz": np.full(m, 2000.),
+               "id": np.arange(1, m + 1, dtype=np.int64)}
+    return driver, witness
+
+
+def adjoint_knots(seed=4321, n_profile=16, n_density=4):
+    """Witness knots 0.5 +- 10 % seeded noise, density knots 1."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.concatenate([0.5 * (1 + 0.1 * rng.uniform(-1, 1, n_profile)), np.ones(n_density)])
+
+
 def config(name):
     """The five benchmark workloads, restated in reference keys (seeded synthetic beams)."""
     if name == "linear_wake_64":
@@ -144,6 +210,49 @@ plasmas.names = plasma
 plasma.density(x,y,z) = 1. + 0.05*(x*x+y*y)
 plasma.ppc = 2 2
 plasma.element = electron
+"""
+    if name == "beam_loading_255":
+        # adjoint workload: the blowout grid extended to 512 slices, driver plus a witness whose
+        # current profile is set by 64 knots on [-7, -5], 8 plasma-density knots, objective on
+        # the witness slices, checkpoints every 32 slices
+        return """
+amr.n_cell = 255 255 512
+hipace.normalized_units = 1
+max_step = 0
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -6. -6. -10.
+geometry.prob_hi =  6.  6.  4.
+beams.names = driver witness
+driver.injection_type = fixed_weight
+driver.num_particles = 1000000
+driver.position_mean = 0. 0. 0.
+driver.position_std = 0.3 0.3 1.0
+driver.density = 10.
+driver.u_mean = 0. 0. 2000.
+driver.u_std = 0.0333333333333 0.0333333333333 0.
+witness.injection_type = fixed_weight
+witness.profile = can
+witness.zmin = -7.
+witness.zmax = -5.
+witness.num_particles = 500000
+witness.position_mean = 0. 0. -6.
+witness.position_std = 0.1 0.1 1.
+witness.density = 5.
+witness.u_mean = 0. 0. 2000.
+random_seed = 1234
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+adjoint.witness = witness
+adjoint.profile_zeta = -7. -5.
+adjoint.n_profile_knots = 64
+adjoint.density_z = -100. 100.
+adjoint.n_density_knots = 8
+adjoint.objective_zeta = -7. -5.
+adjoint.checkpoint_interval = 32
 """
     raise KeyError(name)
 

@@ -56,6 +56,9 @@ def lib():
         L.oracle_mg_iterations.argtypes = [vp]
         L.oracle_mg_iterations.restype = ctypes.c_longlong
         L.oracle_threads.restype = i32
+        L.oracle_adjoint_nparams.argtypes = [vp]
+        L.oracle_adjoint_nparams.restype = i32
+        L.oracle_adjoint.argtypes = [vp, dp, dp, dp]
         L.oracle_error.argtypes = [vp]
         L.oracle_error.restype = cp
         _lib = L
@@ -155,6 +158,18 @@ class Oracle:
         out = np.zeros(12 * n)
         self.L.oracle_get_plasma(self.h, sp, _dp(out))
         return {k: out[i * n:(i + 1) * n] for i, k in enumerate(PLASMA_ATTRS)}
+
+    def adjoint(self, theta, grad=True):
+        """Objective (and gradient) of the adjoint configuration for parameters theta."""
+        n = self.L.oracle_adjoint_nparams(self.h)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        assert theta.size == n, (theta.size, n)
+        g = np.zeros(n) if grad else None
+        J = ctypes.c_double(0)
+        rc = self.L.oracle_adjoint(self.h, _dp(theta), _dp(g) if grad else None, ctypes.byref(J))
+        if rc != 0:
+            raise RuntimeError("oracle_adjoint failed: %d" % rc)
+        return (J.value, g) if grad else J.value
 
     def mg_iterations(self):
         return self.L.oracle_mg_iterations(self.h)
