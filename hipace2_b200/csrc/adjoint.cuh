@@ -167,8 +167,9 @@ __device__ __forceinline__ void a_gather(const AdjRecF& F, const Geo& g, T xp, T
 }
 
 // EnforceBC on a generic scalar: the wrap is a shift by a constant, the reflection flips signs
+// (bit 0/1 of *reflected: x/y reflected)
 template <class T>
-__device__ __forceinline__ bool a_enforce_bc(const Geo& g, T& x, T& y, T& ux, T& uy) {
+__device__ __forceinline__ bool a_enforce_bc(const Geo& g, T& x, T& y, T& ux, T& uy, int* reflected = nullptr) {
     const double plo0 = g.plo_p[0], plo1 = g.plo_p[1], phi0 = g.phi_p[0], phi1 = g.phi_p[1];
     if (val(x) < plo0 || val(y) < plo1 || val(x) > phi0 || val(y) > phi1) {
         if (g.bc != 0 && g.bc != 1) return false;
@@ -181,46 +182,48 @@ __device__ __forceinline__ bool a_enforce_bc(const Geo& g, T& x, T& y, T& ux, T&
         m = fmod(val(y) - plo1, py);
         if (m < 0) m += py;
         y = y + ((m + plo1) - val(y));
-        if (refl && val(x) > phi0) { x = 2 * phi0 - x; ux = -ux; }
-        if (refl && val(y) > phi1) { y = 2 * phi1 - y; uy = -uy; }
+        int r = 0;
+        if (refl && val(x) > phi0) { x = 2 * phi0 - x; ux = -ux; r |= 1; }
+        if (refl && val(y) > phi1) { y = 2 * phi1 - y; uy = -uy; r |= 2; }
+        if (reflected) *reflected = r;
     }
     return true;
 }
 
-template <class T> struct ADu { T v, e; };
-template <class T> __device__ __forceinline__ ADu<T> operator+(ADu<T> a, ADu<T> b) { return {a.v + b.v, a.e + b.e}; }
-template <class T> __device__ __forceinline__ ADu<T> operator-(ADu<T> a, ADu<T> b) { return {a.v - b.v, a.e - b.e}; }
-template <class T> __device__ __forceinline__ ADu<T> operator*(ADu<T> a, ADu<T> b) { return {a.v * b.v, a.e * b.v + a.v * b.e}; }
-
 // plasma push of one particle (n_subcycles 1) with gathered fields G. out: x, y, ux_h, uy_h,
-// psi_h, ux, uy, psi. Returns false if the particle is absorbed.
+// psi_h, ux, uy, psi. Returns false if the particle is absorbed. Each sub-step is
+//   u += h f(u) + h^2/2 (Df(u) f(u)),
+// f the momentum right-hand side of k_plasma_push and Df f its derivative along the trajectory
+// (the dual-number term of the forward, written out: the fields are constant along it).
 template <class T>
-__device__ __forceinline__ bool a_push(const Geo& g, double qmc, T x, T y, T ux, T uy, T psi, const T* G, T* out) {
-    const double ci = 1. / g.c, dzs = g.dx[2];
-    const double sdz = dzs / 4;
+__device__ __forceinline__ bool a_push(const Geo& g, double qmc, T x, T y, T ux, T uy, T psi, const T* G, T* out,
+                                       int* reflected = nullptr) {
+    const double ci = 1. / g.c, c2 = ci * ci, dzs = g.dx[2];
+    const double sdz = dzs / 4, hh = 0.5 * sdz * sdz;
     auto substep = [&]() {
         const T pi = 1.0 / psi;
-        const T gp = 0.5 * pi * pi * (1.0 + ux * ux * (ci * ci) + uy * uy * (ci * ci)) + 0.5;
+        const T a2 = 1.0 + (ux * ux + uy * uy) * c2;
+        const T gp = 0.5 * pi * pi * a2 + 0.5;
+        const T ue = ux * G[0] + uy * G[1];
         const T d0 = qmc * (gp * G[0] + G[4] + (uy * G[5]) * pi);
         const T d1 = qmc * (gp * G[1] - G[3] - (ux * G[5]) * pi);
-        const T d2 = qmc * ci * ((ux * G[0] + uy * G[1]) * ci * pi - G[2]);
-        const T z = 0.0 * psi;
-        const ADu<T> dux{ux, d0}, duy{uy, d1}, dpi{pi, -pi * pi * d2};
-        const ADu<T> c2{z + ci * ci, z}, one{z + 1.0, z}, half{z + 0.5, z}, q{z + qmc, z}, cc{z + ci, z};
-        const ADu<T> E0{G[0], z}, E1{G[1], z}, E2{G[2], z}, B0{G[3], z}, B1{G[4], z}, B2{G[5], z};
-        const ADu<T> gpd = half * dpi * dpi * (one + dux * dux * c2 + duy * duy * c2) + half;
-        const ADu<T> e0 = q * (gpd * E0 + B1 + (duy * B2) * dpi);
-        const ADu<T> e1 = q * (gpd * E1 - B0 - (dux * B2) * dpi);
-        const ADu<T> e2 = q * cc * ((dux * E0 + duy * E1) * cc * dpi - E2);
-        ux = ux + sdz * d0 + 0.5 * sdz * sdz * e0.e;
-        uy = uy + sdz * d1 + 0.5 * sdz * sdz * e1.e;
-        psi = psi + sdz * d2 + 0.5 * sdz * sdz * e2.e;
+        const T d2 = qmc * ci * (ue * ci * pi - G[2]);
+        // derivatives along (d0, d1, d2): dpi = -pi^2 d2
+        const T dpi = -(pi * pi) * d2;
+        const T dgp = pi * dpi * a2 + pi * pi * c2 * (ux * d0 + uy * d1);
+        const T e0 = qmc * (dgp * G[0] + G[5] * (d1 * pi + uy * dpi));
+        const T e1 = qmc * (dgp * G[1] - G[5] * (d0 * pi + ux * dpi));
+        const T e2 = qmc * c2 * ((d0 * G[0] + d1 * G[1]) * pi + ue * dpi);
+        ux = ux + sdz * d0 + hh * e0;
+        uy = uy + sdz * d1 + hh * e1;
+        psi = psi + sdz * d2 + hh * e2;
     };
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) substep();
     x = x + dzs * ci * (ux * (1.0 / psi));
     y = y + dzs * ci * (uy * (1.0 / psi));
-    if (!a_enforce_bc(g, x, y, ux, uy)) return false;
+    if (reflected) *reflected = 0;
+    if (!a_enforce_bc(g, x, y, ux, uy, reflected)) return false;
     out[0] = x; out[1] = y; out[2] = ux; out[3] = uy; out[4] = psi;
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) substep();
@@ -380,75 +383,78 @@ struct AdjL {
     F2<double> f[A_NCOMP];
 };
 
-// plasma push: lin(x, y, ux_h, uy_h, psi_h) = J^T lout; lin(ux, uy, psi) = 0; field adjoints
-// scattered by the gather shapes
-__global__ void __launch_bounds__(128) k_adj_push(AdjPlasma P, AdjLam lout, AdjLam lin, AdjRecF F, AdjL L, Geo g) {
+// plasma push: lin += J^T lout for (x, y, ux_h, uy_h, psi_h) (lin zeroed before); field
+// adjoints scattered by the gather shapes. One thread per (particle, seed): seeds 0-2
+// differentiate the push with respect to ux_h, uy_h, psi_h, seeds 3-8 with respect to the six
+// gathered values G. The positions enter the push only through G and the position update
+// x' = x + dz ux/(c psi) (+-1 under a reflection), so dL/dx = sum_c dL/dG_c dG_c/dx + lout_x' (+-1):
+// the thread of G_c adds its term (gather shapes differentiated in x and y) and deposits dL/dG_c
+// on the plane of G_c (the adjoint of a gather is a deposit).
+constexpr int kPushSeeds = 9;
+__global__ void __launch_bounds__(256) k_adj_push(AdjPlasma P, AdjLam lout, AdjLam lin, AdjRecF F, AdjL L, Geo g) {
     HPQ_PDL_ENTRY();
     const double qmc = P.charge / (P.mass * g.c);
-    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
-        lin.ux[ip] = 0; lin.uy[ip] = 0; lin.psi[ip] = 0;
-        double lo[8] = {lout.x[ip], lout.y[ip], lout.uxh[ip], lout.uyh[ip], lout.psih[ip],
-                        lout.ux[ip], lout.uy[ip], lout.psi[ip]};
+    const long long total = P.n * kPushSeeds;
+    for (long long t = gtid(); t < total; t += gstride()) {
+        const long long ip = t / kPushSeeds;
+        const int k = (int)(t - ip * kPushSeeds);
+        const double lo[8] = {lout.x[ip], lout.y[ip], lout.uxh[ip], lout.uyh[ip], lout.psih[ip],
+                              lout.ux[ip], lout.uy[ip], lout.psi[ip]};
         bool any = false;
 #pragma unroll
         for (int o = 0; o < 8; ++o) any = any || lo[o] != 0.0;
-        if (!P.valid[ip] || !any) {
-            lin.x[ip] = 0; lin.y[ip] = 0; lin.uxh[ip] = 0; lin.uyh[ip] = 0; lin.psih[ip] = 0;
-            continue;
-        }
+        if (!P.valid[ip] || !any) continue;
         const double in[5] = {P.x[ip], P.y[ip], P.uxh[ip], P.uyh[ip], P.psih[ip]};
-        double d[5];
-        bool alive = true;
-#pragma unroll 1
-        for (int k = 0; k < 5 && alive; ++k) {
-            Tn t[5], G[6], out[8];
-#pragma unroll
-            for (int m = 0; m < 5; ++m) t[m] = tseed(in[m], m == k);
-            a_gather<Tn>(F, g, t[0], t[1], G);
-            alive = a_push<Tn>(g, qmc, t[0], t[1], t[2], t[3], t[4], G, out);
-            double s = 0;
-#pragma unroll
-            for (int o = 0; o < 8; ++o) s += lo[o] * out[o].d;
-            d[k] = s;
-        }
-        if (!alive) {
-            lin.x[ip] = 0; lin.y[ip] = 0; lin.uxh[ip] = 0; lin.uyh[ip] = 0; lin.psih[ip] = 0;
-            continue;
-        }
         double Gv[6];
         a_gather<double>(F, g, in[0], in[1], Gv);
-        double lG[6];
-#pragma unroll 1
-        for (int c = 0; c < 6; ++c) {
-            Tn G[6], out[8];
+        Tn G[6], out[8];
 #pragma unroll
-            for (int m = 0; m < 6; ++m) G[m] = tseed(Gv[m], m == c);
-            a_push<Tn>(g, qmc, tseed(in[0], false), tseed(in[1], false), tseed(in[2], false), tseed(in[3], false),
-                       tseed(in[4], false), G, out);
-            double s = 0;
+        for (int m = 0; m < 6; ++m) G[m] = tseed(Gv[m], m == k - 3);
+        int refl = 0;
+        const bool alive = a_push<Tn>(g, qmc, tseed(in[0], false), tseed(in[1], false), tseed(in[2], k == 0),
+                                      tseed(in[3], k == 1), tseed(in[4], k == 2), G, out, &refl);
+        if (!alive) continue;
+        double sum = 0;
 #pragma unroll
-            for (int o = 0; o < 8; ++o) s += lo[o] * out[o].d;
-            lG[c] = s;
+        for (int o = 0; o < 8; ++o) sum += lo[o] * out[o].d;
+        if (k < 3) {
+            double* const lk = k == 0 ? lin.uxh : k == 1 ? lin.uyh : lin.psih;
+            lk[ip] += sum;
+            if (k == 0) {
+                atomicAdd(lin.x + ip, (refl & 1) ? -lo[0] : lo[0]);
+                atomicAdd(lin.y + ip, (refl & 2) ? -lo[1] : lo[1]);
+            }
+            continue;
         }
-        lin.x[ip] = d[0]; lin.y[ip] = d[1]; lin.uxh[ip] = d[2]; lin.uyh[ip] = d[3]; lin.psih[ip] = d[4];
-        // adjoint of the gather: a deposit with the gather shapes
-        const double x = a_clamp((in[0] - g.xoff) * g.dxi[0], g.nx), y = a_clamp((in[1] - g.yoff) * g.dxi[1], g.ny);
+        if (sum == 0.0) continue;
+        const int c = k - 3;
+        const F2<double> dstp = L.f[c <= 1 ? A_PSI : c == 2 ? A_EZ : c == 3 ? A_BX : c == 4 ? A_BY : A_BZ];
+        const F2<double> src = F.f[c <= 1 ? RF_PSI : c == 2 ? RF_EZ : c == 3 ? RF_BX : c == 4 ? RF_BY : RF_BZ];
+        const double fac = (c == 3 || c == 4) ? g.c : 1.0;
         const double dxi = g.dxi[0], dyi = g.dxi[1];
+        // cell coordinates with their derivatives d/dx (x pass) and d/dy (y pass)
+        const Tn xm = a_clamp((tseed(in[0], true) - g.xoff) * dxi, g.nx);
+        const Tn ym = a_clamp((tseed(in[1], true) - g.yoff) * dyi, g.ny);
+        double gx = 0, gy = 0;
 #pragma unroll 1
         for (int iy = 0; iy < 4; iy++) {
-            const ADSh<double> sy = a_dshape2<double>(1, y, iy);
+            const ADSh<Tn> sy = a_dshape2<Tn>(1, ym, iy);
 #pragma unroll
             for (int ix = 0; ix < 4; ix++) {
-                const ADSh<double> sx = a_dshape2<double>(1, x, ix);
+                const ADSh<Tn> sx = a_dshape2<Tn>(1, xm, ix);
                 const int i = sx.cell, j = sy.cell;
-                const double s = sx.s * sy.s;
-                atomicAdd(L.f[A_PSI].ptr(i, j), lG[0] * sx.ds * sy.s * dxi + lG[1] * sx.s * sy.ds * dyi);
-                atomicAdd(L.f[A_EZ].ptr(i, j), lG[2] * s);
-                atomicAdd(L.f[A_BX].ptr(i, j), lG[3] * g.c * s);
-                atomicAdd(L.f[A_BY].ptr(i, j), lG[4] * g.c * s);
-                atomicAdd(L.f[A_BZ].ptr(i, j), lG[5] * s);
+                double w, wx, wy;
+                if (c == 0) { w = sx.ds.v * sy.s.v * dxi; wx = sx.ds.d * sy.s.v * dxi; wy = sx.ds.v * sy.s.d * dxi; }
+                else if (c == 1) { w = sx.s.v * sy.ds.v * dyi; wx = sx.s.d * sy.ds.v * dyi; wy = sx.s.v * sy.ds.d * dyi; }
+                else { w = sx.s.v * sy.s.v; wx = sx.s.d * sy.s.v; wy = sx.s.v * sy.s.d; }
+                const double f = src(i, j);
+                gx += wx * f;
+                gy += wy * f;
+                atomicAdd(dstp.ptr(i, j), sum * fac * w);
             }
         }
+        atomicAdd(lin.x + ip, sum * fac * gx);
+        atomicAdd(lin.y + ip, sum * fac * gy);
     }
 }
 
@@ -470,7 +476,8 @@ __device__ __forceinline__ double adj_mg_weight(int i, int j, int nx, int ny, in
     return w;
 }
 
-// multigrid slab for the transposed solve: chi, rhs = W^-1 lambda_B (interior), zero guess
+// multigrid slab for the transposed solve: chi, rhs = W^-1 lambda_B (interior), zero initial guess (the
+// previous slice's solution is a worse start: lambda_B changes its pattern from slice to slice)
 __global__ void k_adj_mg_pre(Slab<double> M, AdjL L, AdjRecF F, int cellc) {
     HPQ_PDL_ENTRY();
     const int ax = M.nx + 2 * kGuardAlloc;
@@ -498,68 +505,106 @@ __global__ void k_adj_mg_post(Slab<double> M, AdjL L, AdjRecF F, int cellc) {
     }
 }
 
-// explicit Sx/Sy deposit: lambda of the particle (+=) and of Bz, Ez, ExmBy, EypBx (scattered)
-template <class T, int DT>
-__device__ __forceinline__ T a_explicit_L(const AdjRecF& F, const AdjL& L, const Geo& g, double charge, double mass,
-                                          double w, T x, T y, T ux, T uy, T psi, bool scatter) {
-    const double invvol = g.normalized ? g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1] : g.dxi[0] * g.dxi[1] * g.dxi[2];
-    const double a_clight = g.c, ci = 1. / g.c;
-    const double cdm = charge * invvol * g.mu0 * w;
-    const double qm = charge / mass;
-    const double dxi = g.dxi[0], dyi = g.dxi[1];
-    const T pi = 1.0 / psi;
-    const T vx = ux * pi * ci, vy = uy * pi * ci;
-    const T xmid = a_clamp((x - g.xoff) * dxi, g.nx), ymid = a_clamp((y - g.yoff) * dyi, g.ny);
-    const T gp = 0.5 * (pi * pi + vx * vx + vy * vy + 1.0);
+// explicit Sx/Sy deposit. With a = lambda_Sx, b = lambda_Sy, S = sx sy, Dx = sx' sy, Dy = sx sy'
+// (shape and derivative shape) and the node fields, the particle's contribution to the adjoint
+// objective is cdm * Phi with
+//   Phi = qm pi [vy m1 + ci vx m2 + ci (gp - vx^2) m3 - ci vx vy m4 + vx m5 - ci vy m6
+//                + ci vx vy m7 - ci (gp - vy^2) m8]
+//       + c [dxi (gp - vx^2 - 1) d1 + dxi vx vy d2 - dyi vx vy d3 - dyi (gp - vy^2 - 1) d4],
+//   m1..m4 = sum S a (Bz, Ez, ExmBy, EypBx), m5..m8 = sum S b (...), d1 = sum Dx a, d2 = sum Dx b,
+//   d3 = sum Dy a, d4 = sum Dy b
+// (the expression of k_explicit_deposit regrouped). Phi is linear in the 12 stencil moments, so
+// dPhi/dx is Phi of the moments' x-derivatives (one pass with the shapes differentiated in x),
+// likewise y; the velocity variables enter Phi only through (pi, vx, vy, gp).
+template <class V, class M>
+__device__ __forceinline__ V a_explicit_phi(const Geo& g, double qm, V pi, V vx, V vy, V gp, const M* m) {
+    const double ci = 1. / g.c, dxi = g.dxi[0], dyi = g.dxi[1];
+    return qm * pi * (vy * m[0] + ci * vx * m[1] + ci * (gp - vx * vx) * m[2] - ci * vx * vy * m[3] + vx * m[4] -
+                      ci * vy * m[5] + ci * vx * vy * m[6] - ci * (gp - vy * vy) * m[7]) +
+           g.c * (dxi * (gp - vx * vx - 1.0) * m[8] + dxi * vx * vy * m[9] - dyi * vx * vy * m[10] -
+                  dyi * (gp - vy * vy - 1.0) * m[11]);
+}
+template <int DT>
+__device__ __forceinline__ void a_explicit_moments(const AdjRecF& F, const AdjL& L, const Geo& g, Tn xm, Tn ym,
+                                                   Tn* m) {
+#pragma unroll
+    for (int q = 0; q < 12; ++q) m[q] = Tn{0.0, 0.0};
     constexpr int NS = 3 + DT;
-    T acc = 0.0 * x;
 #pragma unroll 1
     for (int iy = 0; iy < NS; ++iy) {
-        const ADSh<T> sy = a_dshape2<T>(DT, ymid, iy);
+        const ADSh<Tn> sy = a_dshape2<Tn>(DT, ym, iy);
 #pragma unroll 1
         for (int ix = 0; ix < NS; ++ix) {
             if (DT == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
-            const ADSh<T> sx = a_dshape2<T>(DT, xmid, ix);
+            const ADSh<Tn> sx = a_dshape2<Tn>(DT, xm, ix);
             const int i = sx.cell, j = sy.cell;
+            const double a = L.f[A_SX](i, j), b = L.f[A_SY](i, j);
+            if (a == 0.0 && b == 0.0) continue;
+            const Tn S = sx.s * sy.s, Dx = sx.ds * sy.s, Dy = sx.s * sy.ds;
             const double Bz = F.f[RF_BZ](i, j), Ez = F.f[RF_EZ](i, j), Ex = F.f[RF_EXMBY](i, j), Ey = F.f[RF_EYPBX](i, j);
-            const double lsy = L.f[A_SY](i, j), lsx = L.f[A_SX](i, j);
-            if (lsy == 0.0 && lsx == 0.0) continue;
-            const T ss = sx.s * sy.s;
-            const T vsy = cdm * (-ss * (-Bz * vx + (Ez * vy + Ex * (-vx * vy) + Ey * (gp - vy * vy)) * ci) * qm * pi +
-                                 (-sx.ds * sy.s * dxi * (-vx * vy) - sx.s * sy.ds * dyi * (gp - vy * vy - 1.0)) * a_clight);
-            const T vsx = cdm * (ss * (Bz * vy + (Ez * vx + Ex * (gp - vx * vx) + Ey * (-vx * vy)) * ci) * qm * pi +
-                                 (sx.ds * sy.s * dxi * (gp - vx * vx - 1.0) + sx.s * sy.ds * dyi * (-vx * vy)) * a_clight);
-            acc = acc + lsy * vsy + lsx * vsx;
-            if (scatter) {
-                const double K = val(ss * pi) * cdm * qm;
-                const double a = val(vx), b = val(vy), gpv = val(gp);
-                atomicAdd(L.f[A_BZ].ptr(i, j), lsy * K * a + lsx * K * b);
-                atomicAdd(L.f[A_EZ].ptr(i, j), -lsy * K * b * ci + lsx * K * a * ci);
-                atomicAdd(L.f[A_EXMBY].ptr(i, j), lsy * K * a * b * ci + lsx * K * (gpv - a * a) * ci);
-                atomicAdd(L.f[A_EYPBX].ptr(i, j), -lsy * K * (gpv - b * b) * ci - lsx * K * a * b * ci);
-            }
+            const Tn Sa = S * a, Sb = S * b;
+            m[0] = m[0] + Sa * Bz; m[1] = m[1] + Sa * Ez; m[2] = m[2] + Sa * Ex; m[3] = m[3] + Sa * Ey;
+            m[4] = m[4] + Sb * Bz; m[5] = m[5] + Sb * Ez; m[6] = m[6] + Sb * Ex; m[7] = m[7] + Sb * Ey;
+            m[8] = m[8] + Dx * a; m[9] = m[9] + Dx * b; m[10] = m[10] + Dy * a; m[11] = m[11] + Dy * b;
         }
     }
-    return acc;
 }
 
 template <int DT>
-__global__ void __launch_bounds__(128) k_adj_explicit(AdjPlasma P, AdjLam lin, double* lw, AdjRecF F, AdjL L, Geo g) {
+__global__ void __launch_bounds__(256) k_adj_explicit(AdjPlasma P, AdjLam lin, double* lw, AdjRecF F, AdjL L, Geo g) {
     HPQ_PDL_ENTRY();
+    const double invvol = g.normalized ? g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1] : g.dxi[0] * g.dxi[1] * g.dxi[2];
+    const double ci = 1. / g.c, dxi = g.dxi[0], dyi = g.dxi[1];
+    const double cdm1 = P.charge * invvol * g.mu0;  // cdm per unit weight
+    const double qm = P.charge / P.mass;
     for (long long ip = gtid(); ip < P.n; ip += gstride()) {
         if (!P.valid[ip]) continue;
-        const double in[5] = {P.x[ip], P.y[ip], P.ux[ip], P.uy[ip], P.psi[ip]};
-        double d[5];
-#pragma unroll 1
-        for (int k = 0; k < 5; ++k) {
-            Tn t[5];
+        const double x = P.x[ip], y = P.y[ip], ux = P.ux[ip], uy = P.uy[ip], psi = P.psi[ip], w = P.w[ip];
+        const double cdm = cdm1 * w;
+        Tn mx[12], my[12];
+        a_explicit_moments<DT>(F, L, g, a_clamp((tseed(x, true) - g.xoff) * dxi, g.nx),
+                               a_clamp((tseed(y, false) - g.yoff) * dyi, g.ny), mx);
+        a_explicit_moments<DT>(F, L, g, a_clamp((tseed(x, false) - g.xoff) * dxi, g.nx),
+                               a_clamp((tseed(y, true) - g.yoff) * dyi, g.ny), my);
+        double mv[12], mdx[12], mdy[12];
 #pragma unroll
-            for (int m = 0; m < 5; ++m) t[m] = tseed(in[m], m == k);
-            d[k] = a_explicit_L<Tn, DT>(F, L, g, P.charge, P.mass, P.w[ip], t[0], t[1], t[2], t[3], t[4], false).d;
+        for (int q = 0; q < 12; ++q) { mv[q] = mx[q].v; mdx[q] = mx[q].d; mdy[q] = my[q].d; }
+        const double pi = 1.0 / psi, vx = ux * pi * ci, vy = uy * pi * ci;
+        const double gp = 0.5 * (pi * pi + vx * vx + vy * vy + 1.0);
+        lin.x[ip] += cdm * a_explicit_phi<double, double>(g, qm, pi, vx, vy, gp, mdx);
+        lin.y[ip] += cdm * a_explicit_phi<double, double>(g, qm, pi, vx, vy, gp, mdy);
+        double dv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const Tn tux = tseed(ux, k == 0), tuy = tseed(uy, k == 1), tps = tseed(psi, k == 2);
+            const Tn tpi = 1.0 / tps, tvx = tux * tpi * ci, tvy = tuy * tpi * ci;
+            const Tn tgp = 0.5 * (tpi * tpi + tvx * tvx + tvy * tvy + 1.0);
+            dv[k] = a_explicit_phi<Tn, double>(g, qm, tpi, tvx, tvy, tgp, mv).d;
         }
-        lin.x[ip] += d[0]; lin.y[ip] += d[1]; lin.ux[ip] += d[2]; lin.uy[ip] += d[3]; lin.psi[ip] += d[4];
-        lw[ip] += a_explicit_L<double, DT>(F, L, g, P.charge, P.mass, 1.0, in[0], in[1], in[2], in[3], in[4], false);
-        a_explicit_L<double, DT>(F, L, g, P.charge, P.mass, P.w[ip], in[0], in[1], in[2], in[3], in[4], true);
+        lin.ux[ip] += cdm * dv[0];
+        lin.uy[ip] += cdm * dv[1];
+        lin.psi[ip] += cdm * dv[2];
+        lw[ip] += cdm1 * a_explicit_phi<double, double>(g, qm, pi, vx, vy, gp, mv);
+        // field adjoints (closed form per node)
+        const double xm = a_clamp((x - g.xoff) * dxi, g.nx), ym = a_clamp((y - g.yoff) * dyi, g.ny);
+        constexpr int NS = 3 + DT;
+#pragma unroll 1
+        for (int iy = 0; iy < NS; ++iy) {
+            const ADSh<double> sy = a_dshape2<double>(DT, ym, iy);
+#pragma unroll 1
+            for (int ix = 0; ix < NS; ++ix) {
+                if (DT == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                const ADSh<double> sx = a_dshape2<double>(DT, xm, ix);
+                const int i = sx.cell, j = sy.cell;
+                const double lsx = L.f[A_SX](i, j), lsy = L.f[A_SY](i, j);
+                if (lsx == 0.0 && lsy == 0.0) continue;
+                const double K = sx.s * sy.s * pi * cdm * qm;
+                atomicAdd(L.f[A_BZ].ptr(i, j), lsy * K * vx + lsx * K * vy);
+                atomicAdd(L.f[A_EZ].ptr(i, j), -lsy * K * vy * ci + lsx * K * vx * ci);
+                atomicAdd(L.f[A_EXMBY].ptr(i, j), lsy * K * vx * vy * ci + lsx * K * (gp - vx * vx) * ci);
+                atomicAdd(L.f[A_EYPBX].ptr(i, j), -lsy * K * (gp - vy * vy) * ci - lsx * K * vx * vy * ci);
+            }
+        }
     }
 }
 
@@ -607,46 +652,56 @@ __global__ void k_adj_rhs_t(AdjL L, Geo g, int nx, int ny) {
     }
 }
 
-// plasma deposit (jx, jy, chi, rho - jz): lambda of the particle (+=)
-template <class T>
-__device__ __forceinline__ T a_deposit_L(const AdjL& L, const Geo& g, double charge, double mass, double w, T x, T y,
-                                         T ux, T uy, T psi) {
-    const double invvol = g.normalized ? g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1] : g.dxi[0] * g.dxi[1] * g.dxi[2];
-    const double q_invvol = charge * invvol * w;
-    const double qm = charge * g.mu0 / mass;
-    const T pi = 1.0 / psi;
-    const T vx = ux * pi, vy = uy * pi;
-    const T xmid = a_clamp((x - g.xoff) * g.dxi[0], g.nx), ymid = a_clamp((y - g.yoff) * g.dxi[1], g.ny);
-    T acc = 0.0 * x;
+// plasma deposit (jx, jy, chi, rho - jz). The particle's contribution to the adjoint objective is
+// q_invvol * (vx m0 + vy m1 + qm pi m2 + m3) with vx = ux pi, vy = uy pi, pi = 1/psi and the
+// moments m = sum S (lambda_jx, lambda_jy, lambda_chi, lambda_rhomjz) over the 3x3 stencil;
+// x and y derivatives from the moments of the differentiated shapes.
+__device__ __forceinline__ void a_deposit_moments(const AdjL& L, Tn xm, Tn ym, Tn* m) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) m[q] = Tn{0.0, 0.0};
 #pragma unroll
     for (int iy = 0; iy < 3; ++iy) {
-        const ASh<T> sy = a_shape2<T>(ymid, iy);
+        const ASh<Tn> sy = a_shape2<Tn>(ym, iy);
 #pragma unroll
         for (int ix = 0; ix < 3; ++ix) {
-            const ASh<T> sx = a_shape2<T>(xmid, ix);
+            const ASh<Tn> sx = a_shape2<Tn>(xm, ix);
             const int i = sx.cell, j = sy.cell;
-            const T cd = q_invvol * sx.s * sy.s;
-            acc = acc + cd * (vx * L.f[A_JX](i, j) + vy * L.f[A_JY](i, j) + qm * pi * L.f[A_CHI](i, j) + L.f[A_RM](i, j));
+            const Tn S = sx.s * sy.s;
+            m[0] = m[0] + S * L.f[A_JX](i, j);
+            m[1] = m[1] + S * L.f[A_JY](i, j);
+            m[2] = m[2] + S * L.f[A_CHI](i, j);
+            m[3] = m[3] + S * L.f[A_RM](i, j);
         }
     }
-    return acc;
+}
+template <class V, class M>
+__device__ __forceinline__ V a_deposit_phi(double qm, V ux, V uy, V psi, const M* m) {
+    const V pi = 1.0 / psi;
+    return ux * pi * m[0] + uy * pi * m[1] + qm * pi * m[2] + m[3];
 }
 
-__global__ void __launch_bounds__(128) k_adj_deposit(AdjPlasma P, AdjLam lin, double* lw, AdjL L, Geo g) {
+__global__ void __launch_bounds__(256) k_adj_deposit(AdjPlasma P, AdjLam lin, double* lw, AdjL L, Geo g) {
     HPQ_PDL_ENTRY();
+    const double invvol = g.normalized ? g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1] : g.dxi[0] * g.dxi[1] * g.dxi[2];
+    const double q1 = P.charge * invvol;  // q_invvol per unit weight
+    const double qm = P.charge * g.mu0 / P.mass;
+    const double dxi = g.dxi[0], dyi = g.dxi[1];
     for (long long ip = gtid(); ip < P.n; ip += gstride()) {
         if (!P.valid[ip]) continue;
-        const double in[5] = {P.x[ip], P.y[ip], P.ux[ip], P.uy[ip], P.psi[ip]};
-        double d[5];
-#pragma unroll 1
-        for (int k = 0; k < 5; ++k) {
-            Tn t[5];
+        const double x = P.x[ip], y = P.y[ip], ux = P.ux[ip], uy = P.uy[ip], psi = P.psi[ip];
+        const double qw = q1 * P.w[ip];
+        Tn mx[4], my[4];
+        a_deposit_moments(L, a_clamp((tseed(x, true) - g.xoff) * dxi, g.nx), a_clamp((tseed(y, false) - g.yoff) * dyi, g.ny), mx);
+        a_deposit_moments(L, a_clamp((tseed(x, false) - g.xoff) * dxi, g.nx), a_clamp((tseed(y, true) - g.yoff) * dyi, g.ny), my);
+        double mv[4], mdx[4], mdy[4];
 #pragma unroll
-            for (int m = 0; m < 5; ++m) t[m] = tseed(in[m], m == k);
-            d[k] = a_deposit_L<Tn>(L, g, P.charge, P.mass, P.w[ip], t[0], t[1], t[2], t[3], t[4]).d;
-        }
-        lin.x[ip] += d[0]; lin.y[ip] += d[1]; lin.ux[ip] += d[2]; lin.uy[ip] += d[3]; lin.psi[ip] += d[4];
-        lw[ip] += a_deposit_L<double>(L, g, P.charge, P.mass, 1.0, in[0], in[1], in[2], in[3], in[4]);
+        for (int q = 0; q < 4; ++q) { mv[q] = mx[q].v; mdx[q] = mx[q].d; mdy[q] = my[q].d; }
+        lin.x[ip] += qw * a_deposit_phi<double, double>(qm, ux, uy, psi, mdx);
+        lin.y[ip] += qw * a_deposit_phi<double, double>(qm, ux, uy, psi, mdy);
+        lin.ux[ip] += qw * a_deposit_phi<Tn, double>(qm, tseed(ux, true), tseed(uy, false), tseed(psi, false), mv).d;
+        lin.uy[ip] += qw * a_deposit_phi<Tn, double>(qm, tseed(ux, false), tseed(uy, true), tseed(psi, false), mv).d;
+        lin.psi[ip] += qw * a_deposit_phi<Tn, double>(qm, tseed(ux, false), tseed(uy, false), tseed(psi, true), mv).d;
+        lw[ip] += q1 * a_deposit_phi<double, double>(qm, ux, uy, psi, mv);
     }
 }
 

@@ -371,33 +371,10 @@ __device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T y
 
 // ------------------------------------------------------------------------------------------
 // Plasma push (PlasmaParticleAdvance.cpp:29-217; PlasmaMomentumPush PushPlasmaParticles.H:39-75)
-// Leapfrog in zeta: 4 Taylor sub-steps (second order through a dual-number derivative) for
-// u and psi from -1/2 to +1/2, full position step, 2 more sub-steps to the slice.
+// Leapfrog in zeta: 4 Taylor sub-steps (second order through the derivative of the right-hand
+// side along the trajectory) for u and psi from -1/2 to +1/2, full position step, 2 more
+// sub-steps to the slice.
 // ------------------------------------------------------------------------------------------
-template <class R>
-struct Du { R v, e; };
-template <class R> __device__ __forceinline__ Du<R> operator+(Du<R> a, Du<R> b) { return {a.v + b.v, a.e + b.e}; }
-template <class R> __device__ __forceinline__ Du<R> operator-(Du<R> a, Du<R> b) { return {a.v - b.v, a.e - b.e}; }
-template <class R> __device__ __forceinline__ Du<R> operator*(Du<R> a, Du<R> b) { return {a.v * b.v, a.e * b.v + a.v * b.e}; }
-
-template <class T>
-__device__ __forceinline__ void plasma_rhs(const T& ux, const T& uy, const T& pi, T ExmBy, T EypBx, T Ez, T Bxc, T Byc,
-                                           T Bz, T ci, T qmc, T& dux, T& duy, T& dpsi) {
-    const T gp = T(0.5) * pi * pi * (T(1.0) + ux * ux * T(ci * ci) + uy * uy * T(ci * ci)) + T(0.5);
-    dux = T(qmc) * (gp * T(ExmBy) + T(Byc) + (uy * T(Bz)) * pi);
-    duy = T(qmc) * (gp * T(EypBx) - T(Bxc) - (ux * T(Bz)) * pi);
-    dpsi = T(qmc) * T(ci) * ((ux * T(ExmBy) + uy * T(EypBx)) * T(ci) * pi - T(Ez));
-}
-template <class R>
-__device__ __forceinline__ void plasma_rhs_dual(Du<R> ux, Du<R> uy, Du<R> pi, R ExmBy, R EypBx, R Ez, R Bxc, R Byc,
-                                                R Bz, R ci, R qmc, Du<R>& dux, Du<R>& duy, Du<R>& dpsi) {
-    const Du<R> c2{ci * ci, 0};
-    const Du<R> gp = Du<R>{R(0.5), 0} * pi * pi * (Du<R>{R(1.0), 0} + ux * ux * c2 + uy * uy * c2) + Du<R>{R(0.5), 0};
-    dux = Du<R>{qmc, 0} * (gp * Du<R>{ExmBy, 0} + Du<R>{Byc, 0} + (uy * Du<R>{Bz, 0}) * pi);
-    duy = Du<R>{qmc, 0} * (gp * Du<R>{EypBx, 0} - Du<R>{Bxc, 0} - (ux * Du<R>{Bz, 0}) * pi);
-    dpsi = Du<R>{qmc, 0} * Du<R>{ci, 0} * ((ux * Du<R>{ExmBy, 0} + uy * Du<R>{EypBx, 0}) * Du<R>{ci, 0} * pi - Du<R>{Ez, 0});
-}
-
 template <class R>
 __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, Geo g, int temp,
                                                      const int* gate) {
@@ -422,15 +399,26 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
             Bx *= clight; By *= clight;
             R ux = P.uxh[ip], uy = P.uyh[ip], psi = P.psih[ip];
             const R pb = P.ru ? R(1) : R(0);  // psi = pb + stored value
+            // u += h f(u) + h^2/2 Df(u) f(u): the second-order term is the derivative of the
+            // right-hand side along the trajectory (the reference evaluates it with dual numbers,
+            // PushPlasmaParticles.H:39-75; the fields are constant along it, so it is written out)
+            const R c2 = ci * ci, hh = R(0.5) * sdz * sdz;
             auto substep = [&]() {
                 const R pi = R(1) / (pb + psi);
-                R d0, d1, d2;
-                plasma_rhs<R>(ux, uy, pi, Ex, Ey, Ez, Bx, By, Bz, ci, qmc, d0, d1, d2);
-                Du<R> e0, e1, e2;
-                plasma_rhs_dual<R>({ux, d0}, {uy, d1}, {pi, -pi * pi * d2}, Ex, Ey, Ez, Bx, By, Bz, ci, qmc, e0, e1, e2);
-                ux += sdz * d0 + R(0.5) * sdz * sdz * e0.e;
-                uy += sdz * d1 + R(0.5) * sdz * sdz * e1.e;
-                psi += sdz * d2 + R(0.5) * sdz * sdz * e2.e;
+                const R a2 = R(1) + (ux * ux + uy * uy) * c2;
+                const R gp = R(0.5) * pi * pi * a2 + R(0.5);
+                const R ue = ux * Ex + uy * Ey;
+                const R d0 = qmc * (gp * Ex + By + (uy * Bz) * pi);
+                const R d1 = qmc * (gp * Ey - Bx - (ux * Bz) * pi);
+                const R d2 = qmc * ci * (ue * ci * pi - Ez);
+                const R dpi = -(pi * pi) * d2;
+                const R dgp = pi * dpi * a2 + pi * pi * c2 * (ux * d0 + uy * d1);
+                const R e0 = qmc * (dgp * Ex + Bz * (d1 * pi + uy * dpi));
+                const R e1 = qmc * (dgp * Ey - Bz * (d0 * pi + ux * dpi));
+                const R e2 = qmc * c2 * ((d0 * Ex + d1 * Ey) * pi + ue * dpi);
+                ux += sdz * d0 + hh * e0;
+                uy += sdz * d1 + hh * e1;
+                psi += sdz * d2 + hh * e2;
             };
 #pragma unroll
             for (int k = 0; k < 4; ++k) substep();

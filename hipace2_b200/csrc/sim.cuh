@@ -1204,9 +1204,17 @@ public:
         HPQ_CUDA(cudaMemsetAsync(a.lw, 0, n * sizeof(double), st));
         HPQ_CUDA(cudaMemsetAsync(a.lwb, 0, a.cap * sizeof(double), st));
         HPQ_CUDA(cudaMemsetAsync(a.ions, 0, nz * sizeof(double), st));
+        HPQ_CUDA(cudaMemsetAsync(a.M.base, 0, a.M.cstride * (C_BY + 1) * sizeof(double), st));
+        // slices behind the first objective slice do not influence J: their adjoints are zero
+        int smin = nz;
+        for (int s = 0; s < nz; ++s) {
+            const double zc = cfg.prob_lo[2] + (s + 0.5) * g.dx[2];
+            if (zc >= A.objective_lo && zc <= A.objective_hi) { smin = s; break; }
+        }
         int cur = 0;
         for (int c = a.C - 1; c >= 0; --c) {
-            const int hi = nz - 1 - c * a.K, lo = std::max(hi - a.K + 1, 0);
+            const int hi = nz - 1 - c * a.K, lo_seg = std::max(hi - a.K + 1, 0), lo = std::max(lo_seg, smin);
+            if (hi < lo) continue;
             if (c != a.C - 1) {
                 // recompute the segment from its checkpoint (records only)
                 for (int k = 0; k < 11; ++k)
@@ -1221,7 +1229,7 @@ public:
                 for (int s = hi; s >= lo; --s) solve_slice(s);
             }
             for (int s = lo; s <= hi; ++s) {
-                adj_reverse_slice(s, s - lo, cur, J, Ebar, S0);
+                adj_reverse_slice(s, s - lo_seg, cur, J, Ebar, S0);
                 cur = 1 - cur;
             }
         }
@@ -1253,10 +1261,12 @@ public:
         AdjLam lin{a.lam[1 - cur][0], a.lam[1 - cur][1], a.lam[1 - cur][2], a.lam[1 - cur][3], a.lam[1 - cur][4],
                    a.lam[1 - cur][5], a.lam[1 - cur][6], a.lam[1 - cur][7]};
         Geo gg = g;
-        const int nbp = blocks_for(a.n, 128);
+        const int nbp = blocks_for(a.n * kPushSeeds, 256), nbd = blocks_for(a.n, 256);
         HPQ_CUDA(cudaMemsetAsync(a.L.base, 0, cs * A_NCOMP * sizeof(double), st));
+        for (int k = 0; k < 8; ++k) HPQ_CUDA(cudaMemsetAsync(a.lam[1 - cur][k], 0, n * sizeof(double), st));
         // plasma push
-        hpq_launch(k_adj_push, dim3(nbp), dim3(128), 0, st, P, lout, lin, F, L, gg);
+        Scope sc_push(this, "adj_push");
+        hpq_launch(k_adj_push, dim3(nbp), dim3(256), 0, st, P, lout, lin, F, L, gg);
         HPQ_LAUNCH_CHECK();
         // objective
         const double zc = cfg.prob_lo[2] + (s + 0.5) * g.dx[2];
@@ -1265,6 +1275,7 @@ public:
             HPQ_LAUNCH_CHECK();
         }
         // multigrid (transposed solve)
+        Scope sc_mg(this, "adj_multigrid");
         const int ncell = (int)cs;
         hpq_launch(k_adj_mg_pre, dim3(blocks_for(ncell, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
         HPQ_LAUNCH_CHECK();
@@ -1274,11 +1285,13 @@ public:
         hpq_launch(k_adj_mg_post, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
         HPQ_LAUNCH_CHECK();
         // explicit Sx/Sy deposit
-        if (cfg.depos_derivative_type == 0) hpq_launch(k_adj_explicit<0>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
-        else if (cfg.depos_derivative_type == 1) hpq_launch(k_adj_explicit<1>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
-        else hpq_launch(k_adj_explicit<2>, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, F, L, gg);
+        Scope sc_ex(this, "adj_explicit");
+        if (cfg.depos_derivative_type == 0) hpq_launch(k_adj_explicit<0>, dim3(nbd), dim3(256), 0, st, P, lin, a.lw, F, L, gg);
+        else if (cfg.depos_derivative_type == 1) hpq_launch(k_adj_explicit<1>, dim3(nbd), dim3(256), 0, st, P, lin, a.lw, F, L, gg);
+        else hpq_launch(k_adj_explicit<2>, dim3(nbd), dim3(256), 0, st, P, lin, a.lw, F, L, gg);
         HPQ_LAUNCH_CHECK();
         // beam part of Sx/Sy, -grad Psi, Poisson stage; the three solves; right-hand sides
+        Scope sc_f(this, "adj_fields");
         if constexpr (std::is_same<R, double>::value) {
             hpq_launch(k_adj_sxsy_stage, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny,
                        dst.stage, dst.sk, dst.sj);
@@ -1289,7 +1302,8 @@ public:
         hpq_launch(k_adj_rhs_t, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny);
         HPQ_LAUNCH_CHECK();
         // plasma deposit
-        hpq_launch(k_adj_deposit, dim3(nbp), dim3(128), 0, st, P, lin, a.lw, L, gg);
+        Scope sc_dep(this, "adj_deposit");
+        hpq_launch(k_adj_deposit, dim3(nbd), dim3(256), 0, st, P, lin, a.lw, L, gg);
         HPQ_LAUNCH_CHECK();
         // ion background (scaled by the density multiplier like the plasma)
         if (cfg.any_neutralize_background()) {
@@ -1301,6 +1315,7 @@ public:
         // beam deposits of the witness: jz (and rho - jz) of this slice's particles, their jx/jy
         // (deposited one slice earlier into this slice's jx/jy), and the jx/jy of the previous and
         // next slices' particles read by the beam part of Sx/Sy
+        Scope sc_b(this, "adj_beam");
         const bool jxy = cfg.do_beam_jx_jy_deposition;
         const int pitch = S.pitch;
         hpq_launch(k_adj_beam, dim3(148), dim3(256), 0, st, bm[wb], parity, s, (const double*)L.f[A_JZB].p,
