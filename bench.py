@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     p.add_argument("--scale-config", default="channel_1023",
                    help="larger workload timed for FP64 vs mixed (one step each); '' to skip")
+    p.add_argument("--adjoint-config", default="beam_loading_255",
+                   help="workload of the adjoint timing (time per gradient); '' to skip")
     return p.parse_args()
 
 
@@ -266,6 +268,8 @@ def run_ours(args):
         line["mixed"] = mixed_vs_fp64(text, args, torch)
         if args.scale_config:
             line["scale_point"] = scale_point(args.scale_config, torch)
+    if rank == 0 and args.adjoint_config and args.precision == "fp64":
+        line["adjoint"] = adjoint_point(args.adjoint_config, torch)
     if rank == 0:
         print(json.dumps(line))
     sim.close()
@@ -358,6 +362,79 @@ def scale_point(name, torch, sample_every=64):
         res[c + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     res["error_reference"] = "FP64 GPU path, same beam, step 0, every %d-th slice" % sample_every
     return res
+
+
+def adjoint_point(name, torch, reps=3):
+    """Adjoint of one step (hpq_adjoint_grad) on the beam-loading workload: device-synchronised
+    wall time per gradient (forward with checkpoints, recomputation, reverse sweep), per forward
+    of the same step (no reverse) and per plain step (hpq_step, beam push included), plus a
+    central-difference check of two witness-profile knots (FP64 forward, step 1e-4 relative)."""
+    import numpy as np
+    import hipace2_b200 as hp
+    from cases import adjoint_knots, config
+    text = config(name)
+    sim = hp.Hipace(text, graphs=True)
+    sim.init_data()
+    nz = sim.n_cell[2]
+    n_profile = int(_key(text, "adjoint.n_profile_knots"))
+    n_density = int(_key(text, "adjoint.n_density_knots"))
+    theta = adjoint_knots(n_profile=n_profile, n_density=n_density)
+
+    def timed(f, n):
+        f()
+        sim.synchronize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            r = f()
+        sim.synchronize()
+        return (time.perf_counter() - t0) / n, r
+
+    t_fwd, J = timed(lambda: sim.adjoint(theta, grad=False), reps)
+    t_grad, (J2, g) = timed(lambda: sim.adjoint(theta), reps)
+    fd = {}
+    scale = float(np.abs(g).max())
+    k0 = n_profile // 2
+    for k in (k0 - 8, k0 + 8):
+        h = 1e-4 * abs(theta[k])
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        d = (sim.adjoint(tp, grad=False) - sim.adjoint(tm, grad=False)) / (2 * h)
+        fd[str(k)] = {"adjoint": float(g[k]), "central_difference": d,
+                      "err_rel_to_max_grad": abs(float(g[k]) - d) / scale}
+    step = [0]
+
+    def plain():
+        sim.step(step[0])
+        step[0] += 1
+
+    t_step, _ = timed(plain, 2)
+    sim.close()
+    return {"workload": name, "grid": [int(v) for v in _n_cell(text)], "params": int(theta.size),
+            "checkpoint_interval": int(_key(text, "adjoint.checkpoint_interval")),
+            "seconds_per_gradient": t_grad, "seconds_forward": t_fwd, "seconds_plain_step": t_step,
+            "gradient_over_plain_step": t_grad / t_step, "gradient_over_forward": t_grad / t_fwd,
+            "objective": J, "max_abs_grad": scale, "fd_check": fd, "dtype": "f64",
+            "timing": "wall time between device synchronisations"}
+
+
+def _key(text, key):
+    for line in text.splitlines():
+        if line.strip().startswith(key + " ") or line.strip().startswith(key + "="):
+            return line.split("=", 1)[1].split()[0]
+    raise KeyError(key)
+
+
+def _n_cell(text):
+    return [int(v) for v in _key_all(text, "amr.n_cell")]
+
+
+def _key_all(text, key):
+    for line in text.splitlines():
+        if line.strip().startswith(key):
+            return line.split("=", 1)[1].split()
+    raise KeyError(key)
 
 
 def cpu_baseline(text, args):
