@@ -46,7 +46,7 @@ struct PlasmaSpecies {
     bool prevent_centered_particle = false;
 };
 
-enum class BeamInjection : int { FixedPPC = 0, FixedWeight = 1 };
+enum class BeamInjection : int { FixedPPC = 0, FixedWeight = 1, FixedWeightPDF = 2 };
 enum class BeamProfile : int { Gaussian = 0, Flattop = 1, Can = 2 };
 
 struct BeamSpecies {
@@ -72,6 +72,13 @@ struct BeamSpecies {
     // in-situ diagnostics (BeamParticleContainer.cpp:61-63, 476-548)
     int insitu_period = 0;
     double insitu_radius = 1e300;
+    // fixed_weight_pdf (BeamParticleContainer.cpp:200-249): longitudinal pdf(z); mean x, mean y,
+    // std x, std y of z; u_mean x y z and u_std x y z of z; pdf sub-slices per slice
+    Expr pdf;
+    Expr pdf_pos[4];
+    Expr pdf_u[6];
+    int pdf_ref_ratio = 4;
+    bool peak_density_specified = false;
 };
 
 // Adjoint of one step of the explicit slice march with respect to a beam-loading objective.
@@ -351,10 +358,48 @@ inline SimConfig build_config(const InputStore& in) {
         reject(in, name + ".do_radiation_reaction", "radiation reaction is outside the slice loop");
         reject(in, name + ".external_E(x,y,z,t)", "external fields are not implemented");
         reject(in, name + ".external_B(x,y,z,t)", "external fields are not implemented");
-        in.query_arr(name + ".u_mean", b.u_mean);
-        in.query_arr(name + ".u_std", b.u_std);
+        if (inj != "fixed_weight_pdf") {
+            in.query_arr(name + ".u_mean", b.u_mean);
+            in.query_arr(name + ".u_std", b.u_std);
+        }
         std::string profile;
-        if (inj == "fixed_ppc") {
+        if (inj == "fixed_weight_pdf") {
+            // BeamParticleContainer.cpp:200-249: every profile quantity is a function of z
+            b.injection = BeamInjection::FixedWeightPDF;
+            std::string pdf;
+            if (!in.query_str(name + ".pdf", pdf)) throw InputError("missing required input '" + name + ".pdf'");
+            b.pdf = in.function(pdf, {"z"});
+            auto funcs = [&](const std::string& key, Expr* out, size_t n) {
+                const std::vector<std::string> v = in.query_strs(name + "." + key);
+                if (v.size() != n)
+                    throw InputError("input '" + name + "." + key + "' expects " + std::to_string(n) + " values");
+                for (size_t i = 0; i < n; ++i) out[i] = in.function(v[i], {"z"});
+            };
+            Expr pm[2], ps[2], um[3], us[3];
+            funcs("position_mean", pm, 2);
+            funcs("position_std", ps, 2);
+            funcs("u_mean", um, 3);
+            funcs("u_std", us, 3);
+            b.pdf_pos[0] = pm[0]; b.pdf_pos[1] = pm[1]; b.pdf_pos[2] = ps[0]; b.pdf_pos[3] = ps[1];
+            for (int i = 0; i < 3; ++i) { b.pdf_u[i] = um[i]; b.pdf_u[i + 3] = us[i]; }
+            in.get(name + ".num_particles", b.num_particles);
+            in.query(name + ".radius", b.radius);
+            in.query(name + ".z_foc", b.z_foc);
+            in.query_bool(name + ".do_symmetrize", b.do_symmetrize);
+            in.query(name + ".pdf_ref_ratio", b.pdf_ref_ratio);
+            if (b.pdf_ref_ratio < 1) throw InputError(name + ".pdf_ref_ratio must be >= 1");
+            if (b.do_symmetrize && b.num_particles % 4 != 0)
+                throw InputError("To symmetrize the beam, please specify a beam particle number divisible by 4.");
+            const bool has_q = in.query(name + ".total_charge", b.total_charge);
+            const bool has_n = in.query(name + ".density", b.density);
+            if (has_q && c.normalized_units)
+                throw InputError("The option 'beam.total_charge' is only valid in SI units.");
+            if ((int)has_q + (int)has_n != 1)
+                throw InputError("Please specify exlusively either total_charge or density of the beam");
+            b.peak_density_specified = has_n;
+            b.density = std::fabs(b.density);
+            b.total_charge = std::fabs(b.total_charge);
+        } else if (inj == "fixed_ppc") {
             b.injection = BeamInjection::FixedPPC;
             in.query_arr(name + ".ppc", b.ppc);
             in.get(name + ".zmin", b.zmin);
@@ -425,7 +470,7 @@ inline SimConfig build_config(const InputStore& in) {
             if (c.normalized_units) b.total_charge *= 1.0 / (c.dx[0] * c.dx[1] * c.dx[2]);
         } else {
             throw InputError(name + ".injection_type = " + inj +
-                             " is not supported (fixed_ppc, fixed_weight)");
+                             " is not supported (fixed_ppc, fixed_weight, fixed_weight_pdf)");
         }
         c.beams.push_back(b);
     }

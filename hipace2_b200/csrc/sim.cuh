@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -431,7 +432,10 @@ public:
         pending_beams.assign(cfg.beams.size(), HostBeam{});
         bm.resize(cfg.beams.size());
         for (size_t b = 0; b < cfg.beams.size(); ++b) {
-            HostBeam hb = cfg.beams[b].injection == BeamInjection::FixedPPC ? make_fixed_ppc((int)b) : make_fixed_weight((int)b);
+            const BeamInjection inj = cfg.beams[b].injection;
+            HostBeam hb = inj == BeamInjection::FixedPPC      ? make_fixed_ppc((int)b)
+                          : inj == BeamInjection::FixedWeight ? make_fixed_weight((int)b)
+                                                              : make_fixed_weight_pdf((int)b);
             upload_beam((int)b, hb);
         }
     }
@@ -583,6 +587,99 @@ public:
                 double xp = cx + sx * x, yp = cy + sy * y, uxp = sx * u[0] * cfg.pc.c, uyp = sy * u[1] * cfg.pc.c;
                 const bool ok = host_bc(xp, yp, uxp, uyp) && valid;
                 hb.push(xp, yp, zc, ok ? std::fabs(weight) : 0.0, uxp, uyp, u[2] * cfg.pc.c, pid++);
+            }
+        }
+        return hb;
+    }
+
+    // fixed_weight_pdf (InitBeamFixedWeightPDF3D and InitBeamFixedWeightPDFSlice,
+    // BeamParticleContainerInit.cpp:479-678): particle counts per pdf sub-slice drawn from Poisson
+    // distributions with the pdf's means (redrawn on the remainder until the total is exact), z
+    // inside a sub-slice from the inverse of the trapezoidal pdf, Gaussian x, y, u with z-dependent
+    // means and widths, constant weights. The random streams are this library's (std::mt19937_64
+    // for the counts, Philox for the particles), not AMReX's.
+    HostBeam make_fixed_weight_pdf(int b) {
+        const BeamSpecies& B = cfg.beams[b];
+        HostBeam hb;
+        if (B.num_particles <= 0) return hb;
+        const long long nadd = B.do_symmetrize ? B.num_particles / 4 : B.num_particles;
+        const int ref = B.pdf_ref_ratio;
+        const int nsl = nz * ref;
+        const double z0 = cfg.prob_lo[2], zs = g.dx[2] / ref;
+        const double pi = 3.14159265358979323846;
+        auto fz = [](const Expr& e, double z) { return e.eval(&z); };
+        std::vector<double> lw(nsl);
+        double integral = 0, maxd = 0;
+        for (int s = nsl - 1; s >= 0; --s) {
+            const double zmin = z0 + s * zs, zmax = z0 + (s + 1) * zs, zmid = 0.5 * (zmin + zmax);
+            const double a = fz(B.pdf, zmin), c = fz(B.pdf, zmax);
+            if (!(a >= 0 && c >= 0)) throw InputError("PDF must be >= 0 everywhere");
+            lw[s] = 0.5 * (a + c);
+            if (B.peak_density_specified)
+                maxd = std::max(maxd, lw[s] / (zs * fz(B.pdf_pos[2], zmid) * fz(B.pdf_pos[3], zmid) * 2.0 * pi));
+            integral += lw[s];
+        }
+        if (!(integral > 0)) throw InputError("the pdf of beam " + B.name + " is zero over the box");
+        double total_weight = B.peak_density_specified ? B.density * integral / maxd : B.total_charge / std::fabs(B.charge);
+        if (cfg.normalized_units) total_weight *= g.dxi[0] * g.dxi[1] * g.dxi[2];
+        const uint64_t seed = (uint64_t)(cfg.has_random_seed ? cfg.random_seed : 0) * 1000003ull + (uint64_t)b * 7919ull + 54321ull;
+        std::mt19937_64 gen(seed);
+        std::vector<long long> cnt(nsl, 0);
+        long long added = 0;
+        while (added != nadd) {
+            const long long now = nadd - added;
+            for (int s = nsl - 1; s >= 0; --s) {
+                const double mean = (double)now * lw[s] / integral;
+                if (mean > 0) {
+                    const long long n = std::poisson_distribution<long long>(mean)(gen);
+                    cnt[s] += n;
+                    added += n;
+                } else if (mean < 0) {
+                    const long long n = std::min(std::poisson_distribution<long long>(-mean)(gen), cnt[s]);
+                    cnt[s] -= n;
+                    added -= n;
+                }
+            }
+        }
+        const double weight = total_weight / B.num_particles;
+        const Philox rng(seed ^ 0x9e3779b97f4a7c15ull);
+        constexpr int kTries = 1000;  // transverse redraws inside the radius (the reference loops until one fits)
+        long long idx = 0, pid = 1;
+        for (int s = nsl - 1; s >= 0; --s) {
+            if (cnt[s] == 0) continue;
+            const double zmin = z0 + s * zs, zmax = z0 + (s + 1) * zs;
+            const double lo = fz(B.pdf, zmin), hi = fz(B.pdf, zmax);
+            // the exact inverse is ill-conditioned for lo close to hi: Taylor form within 10 %
+            const bool taylor = std::min(lo, hi) * 1.1 > std::max(lo, hi);
+            const double inv = taylor ? 1.0 / (hi + lo) : 1.0 / (hi - lo);
+            for (long long q = 0; q < cnt[s]; ++q, ++idx) {
+                const uint64_t ctr = (uint64_t)idx * 1024;
+                const double w = rng.uniform(ctr, 0);
+                const double z = zmin + (taylor ? zs * (w - w * (w - 1.0) * (hi - lo) * inv)
+                                                : zs * ((std::sqrt(lo * lo + w * (hi * hi - lo * lo)) - lo) * inv));
+                const double xm = fz(B.pdf_pos[0], z), ym = fz(B.pdf_pos[1], z);
+                const double xs = fz(B.pdf_pos[2], z), ys = fz(B.pdf_pos[3], z);
+                double x = 0, y = 0, nrm[4];
+                bool valid = false;
+                for (int t = 0; t < kTries; ++t) {
+                    rng.normals(ctr + t, nrm);
+                    x = xs * nrm[0];
+                    y = ys * nrm[1];
+                    valid = x * x + y * y <= B.radius * B.radius;
+                    if (valid || B.peak_density_specified) break;
+                }
+                rng.normals(ctr + 1023, nrm);
+                double u[3];
+                for (int d = 0; d < 3; ++d) u[d] = fz(B.pdf_u[d], z) + fz(B.pdf_u[d + 3], z) * nrm[d];
+                x -= B.z_foc * u[0] / u[2];
+                y -= B.z_foc * u[1] / u[2];
+                const int ncopy = B.do_symmetrize ? 4 : 1;
+                for (int k = 0; k < ncopy; ++k) {
+                    const double sx = (k & 1) ? -1 : 1, sy = (k & 2) ? -1 : 1;
+                    double xp = xm + sx * x, yp = ym + sy * y, uxp = sx * u[0] * cfg.pc.c, uyp = sy * u[1] * cfg.pc.c;
+                    const bool ok = host_bc(xp, yp, uxp, uyp) && valid;
+                    hb.push(xp, yp, z, ok ? std::fabs(weight) : 0.0, uxp, uyp, u[2] * cfg.pc.c, pid++);
+                }
             }
         }
         return hb;

@@ -113,6 +113,35 @@ adjoint.checkpoint_interval = 16
 """
 
 
+# fixed_weight_pdf witness (BeamParticleContainer.cpp:200-249): trapezoidal current profile on
+# [-7, -5], tilted centroid, z-dependent width and energy chirp
+PDF_BEAM = """
+amr.n_cell = 32 32 64
+hipace.normalized_units = 1
+max_step = 1
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -6. -6. -10.
+geometry.prob_hi =  6.  6.  4.
+beams.names = wit
+wit.injection_type = fixed_weight_pdf
+wit.pdf = "(z<-5)*(z>-7)*(1+0.3*(z+6))"
+wit.position_mean = "0.1*(z+6)" "0."
+wit.position_std = "0.1+0.02*(z+6)" "0.1"
+wit.u_mean = "0." "0." "2000.*(1+0.01*(z+6))"
+wit.u_std = "1." "1." "5."
+wit.num_particles = 200000
+wit.density = 5.
+random_seed = 3
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+hipace.MG_tolerance_rel = 1e-12
+"""
+
+
 def adjoint_beams(seed=1):
     """Seeded driver and witness particles for ADJOINT_SMALL (same arrays for oracle and GPU)."""
     import numpy as np
@@ -210,6 +239,48 @@ plasmas.names = plasma
 plasma.density(x,y,z) = 1. + 0.05*(x*x+y*y)
 plasma.ppc = 2 2
 plasma.element = electron
+"""
+    if name == "large_2047":
+        # large forward (and adjoint) workload: 2047^2 x 2048 slices, 4.2M plasma particles,
+        # 1e7 driver and a 2e6 witness with the knot parameterisation of beam_loading_255
+        return """
+amr.n_cell = 2047 2047 2048
+hipace.normalized_units = 1
+max_step = 0
+hipace.dt = 20
+boundary.field = Dirichlet
+boundary.particle = Reflecting
+geometry.prob_lo = -10. -10. -12.
+geometry.prob_hi =  10.  10.   4.
+beams.names = driver witness
+driver.injection_type = fixed_weight
+driver.num_particles = 10000000
+driver.position_mean = 0. 0. 0.
+driver.position_std = 0.3 0.3 1.0
+driver.density = 10.
+driver.u_mean = 0. 0. 2000.
+driver.u_std = 0.0333333333333 0.0333333333333 0.
+witness.injection_type = fixed_weight
+witness.profile = can
+witness.zmin = -7.
+witness.zmax = -5.
+witness.num_particles = 2000000
+witness.position_mean = 0. 0. -6.
+witness.position_std = 0.1 0.1 1.
+witness.density = 5.
+witness.u_mean = 0. 0. 2000.
+random_seed = 1234
+plasmas.names = plasma
+plasma.density(x,y,z) = 1.
+plasma.ppc = 1 1
+plasma.element = electron
+adjoint.witness = witness
+adjoint.profile_zeta = -7. -5.
+adjoint.n_profile_knots = 64
+adjoint.density_z = -100. 100.
+adjoint.n_density_knots = 8
+adjoint.objective_zeta = -7. -5.
+adjoint.checkpoint_interval = 64
 """
     if name == "beam_loading_255":
         # adjoint workload: the blowout grid extended to 512 slices, driver plus a witness whose

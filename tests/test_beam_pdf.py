@@ -1,0 +1,84 @@
+"""fixed_weight_pdf beam injection (BeamParticleContainerInit.cpp:479-678) against a numpy
+restatement of the reference's total weight and per-sub-slice expectation, and the slice loop on
+such a beam against the oracle. The random streams are this library's, so the particle sets are
+compared statistically (counts per slice within 5 sigma of the Poisson expectation, moments per
+z bin within 5 standard errors)."""
+import numpy as np
+import pytest
+
+from cases import PDF_BEAM
+
+pytestmark = pytest.mark.gpu
+
+N = 200000
+ZLO, DZ, NZ, REF = -10.0, 14.0 / 64, 64, 4
+
+
+def pdf(z):
+    return ((z < -5) & (z > -7)) * (1 + 0.3 * (z + 6))
+
+
+def sx(z):
+    return 0.1 + 0.02 * (z + 6)
+
+
+def expectations(density=5.0, dx=12.0 / 32, dy=12.0 / 32):
+    """InitBeamFixedWeightPDF3D (BeamParticleContainerInit.cpp:479-582): trapezoid weights per
+    pdf sub-slice, total weight from the peak density, normalised units."""
+    zs = DZ / REF
+    zmin = ZLO + np.arange(NZ * REF) * zs
+    lw = 0.5 * (pdf(zmin) + pdf(zmin + zs))
+    zmid = zmin + 0.5 * zs
+    maxd = np.max(lw / (zs * sx(zmid) * 0.1 * 2 * np.pi))
+    total = density * lw.sum() / maxd / (dx * dy * DZ)
+    return total / N, lw / lw.sum()
+
+
+def test_pdf_beam_counts_weights_and_moments():
+    import hipace2_b200 as hp
+    sim = hp.Hipace(PDF_BEAM)
+    sim.init_data()
+    b = sim.get_beam(0)
+    sim.close()
+    assert b["x"].size == N
+    weight, frac = expectations()
+    assert np.allclose(b["w"], weight, rtol=1e-12, atol=0)
+    z = b["z"]
+    # z is drawn from the trapezoid through the pdf at the ends of each pdf sub-slice, so the
+    # sub-slices that straddle the support's edges reach one sub-slice beyond it
+    zs = DZ / REF
+    assert z.min() >= -7.0 - zs and z.max() <= -5.0 + zs
+    # particles per slice: sum of the Poisson expectations of the slice's sub-slices
+    sl = np.floor((z - ZLO) / DZ).astype(int)
+    obs = np.bincount(sl, minlength=NZ)
+    exp = N * frac.reshape(NZ, REF).sum(axis=1)
+    assert np.all(np.abs(obs - exp) <= 5 * np.sqrt(exp) + 1), np.max(np.abs(obs - exp) / np.sqrt(exp + 1))
+    # moments in four z bins: tilted centroid, growing width, energy chirp
+    for lo in (-6.9, -6.5, -6.0, -5.5):
+        m = (z >= lo) & (z < lo + 0.4)
+        n = m.sum()
+        zb = z[m].mean()
+        assert abs(b["x"][m].mean() - 0.1 * (zb + 6)) < 5 * sx(zb) / np.sqrt(n) + 0.01 * 0.5
+        assert b["x"][m].std() == pytest.approx(np.sqrt(np.mean(sx(z[m]) ** 2) + np.var(0.1 * (z[m] + 6))), rel=0.03)
+        assert b["y"][m].std() == pytest.approx(0.1, rel=0.03)
+        assert abs(b["uz"][m].mean() - 2000 * (1 + 0.01 * (zb + 6))) < 5 * 5 / np.sqrt(n) + 2000 * 0.01 * 0.3
+        assert b["ux"][m].std() == pytest.approx(1.0, rel=0.03)
+
+
+def test_pdf_beam_slice_loop_matches_oracle():
+    import hipace2_b200 as hp
+    from oracle_lib import Oracle
+    text = PDF_BEAM.replace("wit.num_particles = 200000", "wit.num_particles = 20000")
+    g = hp.Hipace(text, graphs=False)
+    g.init_data()
+    o = Oracle(text)
+    o.set_beam(0, g.get_beam(0))
+    comps = ["Ez", "Psi", "Bx", "jz_beam", "Sy"]
+    g.set_diag(comps)
+    o.set_diag(comps)
+    g.step(0)
+    o.step(0)
+    for c in comps:
+        a, r = g.get_diag(c), o.get_diag(c)
+        assert np.linalg.norm(a - r) <= 1e-10 * np.linalg.norm(r), c
+    g.close()
