@@ -24,7 +24,7 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
            "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
-           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad")
+           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad", "hpq_n_cell")
 
 _lib = None
 
@@ -71,6 +71,7 @@ def load_library(path=None):
         "hpq_insitu_size": ([vp, cp, ctypes.POINTER(ctypes.c_int64)], i32),
         "hpq_get_insitu": ([vp, cp, dp], i32),
         "hpq_adjoint_nparams": ([vp, ctypes.POINTER(i32)], i32),
+        "hpq_n_cell": ([vp, ctypes.POINTER(i32)], i32),
         "hpq_adjoint_grad": ([vp, dp, dp, dp], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
@@ -132,8 +133,11 @@ class Hipace:
         self._check(self.L.hpq_set_precision(self.h, precision))
         self._check(self.L.hpq_set_graphs(self.h, int(bool(graphs))))
         self._check(self.L.hpq_set_deterministic(self.h, int(bool(deterministic))))
-        self.n_cell = _n_cell(input_text)
+        nc = (ctypes.c_int * 3)()
+        self._check(self.L.hpq_n_cell(self.h, nc))
+        self.n_cell = [nc[0], nc[1], nc[2]]
         self.max_step = _scalar(input_text, "max_step", 0)
+        self.diag_type = _string(input_text, "diagnostic.diag_type", "xyz")
         self._diag = []
 
     def _check(self, rc):
@@ -197,8 +201,10 @@ class Hipace:
         self._check(self.L.hpq_set_diag(self.h, " ".join(comps).encode()))
 
     def get_diag(self, comp):
+        """3-D diagnostic of the last step: (nz, ny, nx), or (nz, nx) / (nz, ny) for
+        diagnostic.diag_type = xz / yz."""
         nx, ny, nz = self.n_cell
-        out = np.zeros((nz, ny, nx))
+        out = np.zeros(_diag_shape(self.diag_type, nx, ny, nz))
         self._check(self.L.hpq_get_diag(self.h, comp.encode(), _dp(out)))
         return out
 
@@ -270,10 +276,14 @@ def _scalar(text, key, default):
     return v
 
 
-def _n_cell(text):
-    n = None
+def _string(text, key, default):
+    v = default
     for line in text.splitlines():
         line = line.split("#")[0]
-        if "=" in line and line.split("=")[0].strip() == "amr.n_cell":
-            n = [int(float(v)) for v in line.split("=", 1)[1].split()]
-    return n
+        if "=" in line and line.split("=")[0].strip() == key:
+            v = line.split("=", 1)[1].strip().strip('"')
+    return v
+
+
+def _diag_shape(diag_type, nx, ny, nz):
+    return {"xyz": (nz, ny, nx), "xz": (nz, nx), "yz": (nz, ny)}[diag_type]

@@ -74,6 +74,12 @@ void hpq_destroy(hpq_handle* h) { delete h; }
 
 const char* hpq_last_error(const hpq_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+int hpq_n_cell(const hpq_handle* h, int n_cell[3]) {
+    if (!h || !n_cell) return HPQ_ERR_ARG;
+    for (int d = 0; d < 3; ++d) n_cell[d] = h->cfg.n_cell[d];
+    return HPQ_OK;
+}
+
 int hpq_set_precision(hpq_handle* h, int mode) {
     return guarded(h, [&] {
         if (h->initialised) { h->err = "hpq_set_precision must come before hpq_init"; return (int)HPQ_ERR_STATE; }

@@ -156,6 +156,7 @@ struct SimConfig {
     bool do_beam_jz_minus_rho = false;
     bool deposit_rho = false;
     int fields_insitu_period = 0;  // fields.insitu_period (Fields.cpp:41, 1289-1346)
+    int diag_type = 0;             // diagnostic.diag_type: 0 xyz, 1 xz, 2 yz (see mid_plane)
     AdjointConfig adjoint;
     std::vector<PlasmaSpecies> plasmas;
     std::vector<BeamSpecies> beams;
@@ -164,6 +165,15 @@ struct SimConfig {
         return false;
     }
 };
+
+// diagnostic.diag_type (Diagnostic.cpp:51-61): 0 xyz (whole slices), 1 xz (the plane y = domain
+// centre), 2 yz (x = domain centre). The plane value is Fields::Copy's order-1 interpolation
+// (Fields.cpp:413-533) at the centre of n cells: the middle cell for odd n, the mean of the two
+// middle cells for even n.
+inline void mid_plane(int n, int& lo, int& hi, double& wlo, double& whi) {
+    if (n % 2) { lo = hi = (n - 1) / 2; wlo = 1.0; whi = 0.0; }
+    else { lo = n / 2 - 1; hi = n / 2; wlo = 0.5; whi = 0.5; }
+}
 
 // utils::doDiagnostics (IOUtil.cpp:75-82)
 inline bool do_diagnostics(int period, int step, int max_step, double time, double max_time) {
@@ -232,6 +242,15 @@ inline SimConfig build_config(const InputStore& in) {
 
     in.query("max_step", c.max_step);
     in.query("fields.insitu_period", c.fields_insitu_period);
+    {
+        std::string dt;
+        if (in.query_str("diagnostic.diag_type", dt)) {
+            if (dt == "xyz") c.diag_type = 0;
+            else if (dt == "xz") c.diag_type = 1;
+            else if (dt == "yz") c.diag_type = 2;
+            else throw InputError("Unknown diagnostics type: must be xyz, xz or yz.");
+        }
+    }
     std::string dts;
     if (in.query_str("hipace.dt", dts)) {
         if (dts == "adaptive") throw InputError("hipace.dt = adaptive is not supported");

@@ -918,16 +918,26 @@ __global__ void k_rhs_bxby(Slab<R> S, Geo g, R* __restrict__ stage, int sk, int 
 
 // copy interior of listed components into the 3-D diagnostic buffer at the current slice
 // out layout: [q][nz][ny][nx]
+// diagnostic plane of a slice: the whole slice (type 0), or the row (type 1, xz) / column
+// (type 2, yz) at the domain centre, interpolated between cells lo and hi with weights wlo, whi
+struct DiagSel {
+    int type, lo, hi;
+    double wlo, whi;
+};
 template <class R>
-__global__ void k_diag_copy(Slab<R> S, const Ctl* ctl, CompList L, double* __restrict__ out, int nz) {
+__global__ void k_diag_copy(Slab<R> S, const Ctl* ctl, CompList L, double* __restrict__ out, int nz, DiagSel d) {
     HPQ_PDL_ENTRY();
     const int s = ctl->islice;
-    const long long nxy = (long long)S.nx * S.ny;
-    for (long long k = gtid(); k < nxy * L.n; k += gstride()) {
-        const int q = (int)(k / nxy);
-        const long long r = k % nxy;
-        const int i = (int)(r % S.nx), j = (int)(r / S.nx);
-        out[((size_t)q * nz + s) * nxy + r] = (double)S.c(L.c[q])(i, j);
+    const long long np = d.type == 0 ? (long long)S.nx * S.ny : d.type == 1 ? S.nx : S.ny;
+    for (long long k = gtid(); k < np * L.n; k += gstride()) {
+        const int q = (int)(k / np);
+        const long long r = k % np;
+        const F2<R> f = S.c(L.c[q]);
+        double v;
+        if (d.type == 0) v = (double)f((int)(r % S.nx), (int)(r / S.nx));
+        else if (d.type == 1) v = d.wlo * (double)f((int)r, d.lo) + d.whi * (double)f((int)r, d.hi);
+        else v = d.wlo * (double)f(d.lo, (int)r) + d.whi * (double)f(d.hi, (int)r);
+        out[((size_t)q * nz + s) * np + r] = v;
     }
 }
 

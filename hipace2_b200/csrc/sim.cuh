@@ -1543,7 +1543,8 @@ public:
             HPQ_LAUNCH_CHECK();
         }
         if (diag_list.n > 0) {
-            hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)nx * ny * diag_list.n, 256)), dim3(256), 0, st, S, ctl, diag_list, diag_buf, nz);
+            hpq_launch(k_diag_copy<R>, dim3(blocks_for((long long)diag_plane() * diag_list.n, 256)), dim3(256), 0, st, S, ctl,
+                       diag_list, diag_buf, nz, diag_sel());
             HPQ_LAUNCH_CHECK();
         }
         // field in-situ reductions after every field of the slice is known (Hipace.cpp:684-685)
@@ -1647,6 +1648,13 @@ public:
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i) out[(size_t)j * nx + i] = (double)tmp[(size_t)(j + kGuardAlloc) * S.pitch + i + kGuardAlloc];
     }
+    long long diag_plane() const { return cfg.diag_type == 0 ? (long long)nx * ny : cfg.diag_type == 1 ? nx : ny; }
+    DiagSel diag_sel() const {
+        DiagSel d{cfg.diag_type, 0, 0, 1.0, 0.0};
+        if (cfg.diag_type == 1) mid_plane(ny, d.lo, d.hi, d.wlo, d.whi);
+        if (cfg.diag_type == 2) mid_plane(nx, d.lo, d.hi, d.wlo, d.whi);
+        return d;
+    }
     void set_diag(const std::vector<std::string>& names) override {
         if (names.size() > 24) throw InputError("at most 24 diagnostic components");
         synchronize();
@@ -1656,7 +1664,7 @@ public:
         for (auto& n : names) diag_list.c[diag_list.n++] = comp_from_name(n, cfg.explicit_solver);
         if (diag_buf) { cudaFree(diag_buf); diag_buf = nullptr; }
         if (!names.empty()) {
-            const size_t n = (size_t)names.size() * nx * ny * nz;
+            const size_t n = (size_t)names.size() * diag_plane() * nz;
             HPQ_CUDA(cudaMalloc(&diag_buf, n * sizeof(double)));
             HPQ_CUDA(cudaMemset(diag_buf, 0, n * sizeof(double)));
         }
@@ -1665,7 +1673,7 @@ public:
         auto it = std::find(diag_names.begin(), diag_names.end(), name);
         if (it == diag_names.end()) throw InputError("component '" + name + "' is not in the diagnostic list");
         const size_t q = it - diag_names.begin();
-        const size_t n = (size_t)nx * ny * nz;
+        const size_t n = (size_t)diag_plane() * nz;
         HPQ_CUDA(cudaStreamSynchronize(st));
         HPQ_CUDA(cudaMemcpy(out, diag_buf + q * n, n * sizeof(double), cudaMemcpyDeviceToHost));
     }

@@ -41,6 +41,9 @@ enum { HPQ_PLAIN_FP64 = 0, HPQ_MIXED = 1 };
 int hpq_create(const char* input_text, hpq_handle** out);
 void hpq_destroy(hpq_handle* h);
 const char* hpq_last_error(const hpq_handle* h);
+/* Grid size (amr.n_cell, after my_constants and expressions are evaluated), valid after
+ * hpq_create (Hipace.cpp:176-230 reads the same key). */
+int hpq_n_cell(const hpq_handle* h, int n_cell[3]);
 /* Text of the last hpq_create failure (no handle exists then). */
 const char* hpq_create_error(void);
 

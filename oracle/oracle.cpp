@@ -1170,8 +1170,18 @@ public:
         for (auto& n : diag_names) {
             auto& d = diag[n];
             const Field& src = f(n.c_str());
-            for (int j = 0; j < ny; ++j)
-                for (int i = 0; i < nx; ++i) d[((size_t)islice * ny + j) * nx + i] = src(i, j);
+            int lo, hi;
+            double wlo, whi;
+            if (cfg.diag_type == 0) {
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) d[((size_t)islice * ny + j) * nx + i] = src(i, j);
+            } else if (cfg.diag_type == 1) {
+                hpq::mid_plane(ny, lo, hi, wlo, whi);
+                for (int i = 0; i < nx; ++i) d[(size_t)islice * nx + i] = wlo * src(i, lo) + whi * src(i, hi);
+            } else {
+                hpq::mid_plane(nx, lo, hi, wlo, whi);
+                for (int j = 0; j < ny; ++j) d[(size_t)islice * ny + j] = wlo * src(lo, j) + whi * src(hi, j);
+            }
         }
         plasma_push(false);
         for (size_t b = 0; b < cfg.beams.size(); ++b) {
@@ -1214,7 +1224,8 @@ public:
             std::vector<hpq::PlasmaSpecies> saved = cfg.plasmas;
             plasma_deposit_ions();
         }
-        for (auto& n : diag_names) diag[n].assign((size_t)nx * ny * nz, 0.0);
+        const size_t plane = cfg.diag_type == 0 ? (size_t)nx * ny : cfg.diag_type == 1 ? (size_t)nx : (size_t)ny;
+        for (auto& n : diag_names) diag[n].assign(plane * nz, 0.0);
     }
     void plasma_deposit_ions() {
         // only species with neutralize_background deposit (MultiPlasma.cpp:103-115)
@@ -1987,6 +1998,10 @@ const char* oracle_error(OracleHandle* h) { return h->sim->error.c_str(); }
 // reduced-diagnostic arrays, value index outer, slice inner): beam: 22 x nz values (entry 0 the
 // sum of weights, the others divided by it), nz particle counts, 22 sums over slices, the total
 // count; fields: 10 x nz values, 10 sums.
+int oracle_n_cell(OracleHandle* h, int* n) {
+    for (int d = 0; d < 3; ++d) n[d] = h->sim->cfg.n_cell[d];
+    return 0;
+}
 int oracle_adjoint_nparams(OracleHandle* h) {
     return h->sim->cfg.adjoint.witness < 0 ? 0 : h->sim->cfg.adjoint.n_params();
 }

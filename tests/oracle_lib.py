@@ -56,6 +56,7 @@ def lib():
         L.oracle_mg_iterations.argtypes = [vp]
         L.oracle_mg_iterations.restype = ctypes.c_longlong
         L.oracle_threads.restype = i32
+        L.oracle_n_cell.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.oracle_adjoint_nparams.argtypes = [vp]
         L.oracle_adjoint_nparams.restype = i32
         L.oracle_adjoint.argtypes = [vp, dp, dp, dp]
@@ -88,7 +89,11 @@ class Oracle:
         if rc != 0:
             raise ValueError(err.value.decode())
         self.h = h
-        self.nx, self.ny, self.nz = _n_cell(input_text)
+        nc = (ctypes.c_int * 3)()
+        L.oracle_n_cell(h, nc)
+        self.nx, self.ny, self.nz = nc[0], nc[1], nc[2]
+        import hipace2_b200 as hp
+        self.diag_type = hp._string(input_text, "diagnostic.diag_type", "xyz")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -120,7 +125,8 @@ class Oracle:
             raise KeyError(names)
 
     def get_diag(self, name):
-        out = np.zeros((self.nz, self.ny, self.nx))
+        import hipace2_b200 as hp
+        out = np.zeros(hp._diag_shape(self.diag_type, self.nx, self.ny, self.nz))
         if self.L.oracle_get_diag(self.h, name.encode(), _dp(out)):
             raise KeyError(name)
         return out
@@ -174,11 +180,3 @@ class Oracle:
     def mg_iterations(self):
         return self.L.oracle_mg_iterations(self.h)
 
-
-def _n_cell(text):
-    n = None
-    for line in text.splitlines():
-        line = line.split("#")[0]
-        if "=" in line and line.split("=")[0].strip() == "amr.n_cell":
-            n = [int(float(v)) for v in line.split("=", 1)[1].split()]
-    return n

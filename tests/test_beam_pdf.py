@@ -82,3 +82,40 @@ def test_pdf_beam_slice_loop_matches_oracle():
         a, r = g.get_diag(c), o.get_diag(c)
         assert np.linalg.norm(a - r) <= 1e-10 * np.linalg.norm(r), c
     g.close()
+
+
+# field checksums of the transverse benchmark that carry the wake signal; the others (Bx, Bz,
+# EypBx, jy, Sy on the y = 0 plane) vanish for a symmetric beam up to the beam's shot noise, so
+# they depend on the random stream
+SIGNAL = ("By", "ExmBy", "Ez", "Psi", "chi", "jx", "jz_beam", "rhomjz", "Sx")
+
+
+def test_transverse_benchmark_golden():
+    """The reference's transverse_benchmark.1Rank regression test (1023^2 x 1000 slices,
+    fixed_weight_pdf Gaussian beam of 10.5M particles, xz diagnostic). The beam checksums that do
+    not depend on the random stream are exact: particle count, total weight (the pdf normalisation
+    of InitBeamFixedWeightPDF3D) and uz of the cold beam; the field checksums of the y = 0 plane
+    agree statistically."""
+    import hipace2_b200 as hp
+    from cases import GOLDEN
+    case = GOLDEN["transverse_benchmark.1Rank"]
+    sim = hp.Hipace(case["input"])
+    sim.init_data()
+    b = sim.get_beam(0)
+    gold = case["beam"]
+    assert b["x"].size == gold["charge"]
+    assert np.abs(b["w"]).sum() == pytest.approx(gold["w"], rel=1e-9)
+    assert np.abs(b["uz"]).sum() == pytest.approx(gold["uz"], rel=1e-12)
+    for k in ("x", "y", "z"):
+        assert np.abs(b[k]).sum() == pytest.approx(gold[k], rel=2e-3), k
+    comps = sorted(case["fields"])
+    sim.set_diag(comps)
+    sim.step(0)
+    dev = {}
+    for k in comps:
+        got = np.abs(sim.get_diag(k)).sum()
+        dev[k] = got / case["fields"][k] - 1 if case["fields"][k] else got
+    sim.close()
+    print("transverse_benchmark field checksum deviations:", {k: round(v, 5) for k, v in dev.items()})
+    for k in SIGNAL:
+        assert abs(dev[k]) < 0.03, (k, dev[k])

@@ -13,7 +13,9 @@ import pytest
 from oracle_lib import Oracle
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = json.load(open(os.path.join(HERE, "golden", "golden_cases.json")))
+# deterministic cases only: the statistical ones draw their beam from a random stream
+CASES = {k: v for k, v in json.load(open(os.path.join(HERE, "golden", "golden_cases.json"))).items()
+         if not v.get("statistical")}
 
 
 def _max_step(text):
