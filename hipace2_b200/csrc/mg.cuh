@@ -132,7 +132,9 @@ __global__ void k_mg_interp(MGLev F, MV<R> out, MV<R> fin, MV<R> crse) {
 // A cell at distance d from the edge of the loaded region is exact after 4 colour sweeps when
 // d >= 4, so the residual is exact on the tile and its ring with a halo of 6.
 // ------------------------------------------------------------------------------------------
-enum { MG_INIT_ZERO = 0, MG_INIT_VIEW = 1, MG_INIT_INTERP = 2 };
+// initial guess of a smoothing pass: zero, the input view, the input view plus the interpolated
+// coarse correction, or zero plus the interpolated coarse correction
+enum { MG_INIT_ZERO = 0, MG_INIT_VIEW = 1, MG_INIT_INTERP = 2, MG_INIT_INTERP0 = 3 };
 enum { MG_NORM_NONE = 0, MG_NORM_ITER = 1, MG_NORM_FIRST = 2 };
 
 template <class R>
@@ -254,11 +256,11 @@ __device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, i
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             cp_async_el<R>(&srh[c][e], v ? &A.rhs(i, j, c) : A.rhs.p[c], v);
-            if (INIT == MG_INIT_ZERO) sp[c][e] = R(0);
+            if (INIT == MG_INIT_ZERO || INIT == MG_INIT_INTERP0) sp[c][e] = R(0);
             else cp_async_el<R>(&sp[c][e], v ? &vin(i, j, c) : vin.p[c], v);
         }
     }
-    if (INIT == MG_INIT_INTERP) {
+    if (INIT == MG_INIT_INTERP || INIT == MG_INIT_INTERP0) {
         const MGLev& C = A.Lc;
         for (int e = threadIdx.x; e < EC * EC; e += NT) {
             const int ic = ci0 + e % EC, jc = cj0 + e / EC;
@@ -277,7 +279,7 @@ __device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, i
         const int i = ti0 + e % E, j = tj0 + e / E;
         const bool v = i >= L.vlo && i <= L.vhi_i && j >= L.vlo && j <= L.vhi_j;
         sinv[e] = v ? mg_diag_inv<R, CELL>(L, i, j, sa[e], A.facx, A.facy) : R(0);
-        if (INIT == MG_INIT_INTERP && v) {
+        if ((INIT == MG_INIT_INTERP || INIT == MG_INIT_INTERP0) && v) {
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const R* q = sc[c];
@@ -614,6 +616,11 @@ struct MGSolveArgs {
     R* r32[2];
     // optional phase trace (HPQ_MG_TRACE): block 0 records the global timer after each barrier
     unsigned long long* trace;
+    // level 0 of a V-cycle as two phases of 4 sweeps (interpolation + up-sweeps, then the next
+    // down-sweeps + residual) instead of one phase of 8: each 16^2 tile then sweeps a 28^2
+    // region 4 + 4 times instead of a 36^2 region 8 times (40 % fewer point updates, one more
+    // grid barrier). Same sweeps in the same order, so the same results.
+    int split0;
 };
 
 __device__ __forceinline__ unsigned long long tc_clock_ns() {
@@ -689,7 +696,9 @@ struct RefineSmem {
     }
 };
 
-template <bool CELL, bool FIRST, int NSW>
+// DIN: the correction d starts from P.up[0] (the first 4 sweeps of the split level-0 phase)
+// instead of the interpolated coarse correction
+template <bool CELL, bool FIRST, int NSW, bool DIN = false>
 __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int slot_in, int bx, int by,
                                                unsigned char* smem_raw, double& bmax, double& brhs) {
     constexpr int T = 16, NT = 256;
@@ -737,10 +746,11 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
             } else {
                 cp_async_el<double>(&sx[c][e], xin + c * n0 + id, v);
                 cp_async_el<float>(&srh[c][e], rin + c * n0 + id, v);
+                if (DIN) cp_async_el<float>(&sd[c][e], P.up[0] + c * n0 + id, v);
             }
         }
     }
-    if (!FIRST) {
+    if (!FIRST && !DIN) {
         const MGLev& C = P.lev[1];
         for (int e = threadIdx.x; e < EC * EC; e += NT) {
             const int ic = ci0 + e % EC, jc = cj0 + e / EC;
@@ -763,7 +773,7 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
             if (FIRST) {
                 sx[c][e] = (double)sd[c][e];
                 sd[c][e] = 0.f;
-            } else {
+            } else if (!DIN) {
                 const float* q = sc[c];
                 sd[c][e] = v ? mg_interp1f<float, CELL>([&](int ic, int jc) { return q[(jc - cj0) * EC + (ic - ci0)]; }, i, j) : 0.f;
             }
@@ -1012,6 +1022,55 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
+        // level 0, split form (double precision on large grids): interpolation + 4 up-sweeps
+        // from cor[0] into up[0], barrier, 4 down-sweeps + residual + restriction + norm from
+        // up[0] back into cor[0]
+        // (single precision: the first 4 sweeps of the correction d, from the interpolated coarse
+        // correction with the FP32 residual as right-hand side, go to up[0]; the second pass
+        // reloads d, sweeps 4 more times, adds it to the FP64 solution and forms the residual)
+        if (P.split0) {
+            {
+                SmoothArgs<R> a = base(0);
+                a.crse_in = (P.sb == 1) ? mg_own<R>(P.cor, P.lev, 1) : mg_own<R>(P.up, P.lev, 1);
+                a.out = mg_own<R>(P.up, P.lev, 0);
+                a.acf = P.a0;
+                int ntx;
+                const int nt = ntiles(0, ntx);
+                if constexpr (kRefine) {
+                    const size_t n0 = (size_t)P.lev[0].w * P.lev[0].h;
+                    a.rhs = MV<R>{{P.r32[it & 1], P.r32[it & 1] + n0}, P.lev[0].w, 0};
+                    for (int t = tb; tile_block && t < nt; t += ntb)
+                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP0, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                } else {
+                    a.in = mg_own<R>(P.cor, P.lev, 0);
+                    a.rhs = P.rhs;
+                    for (int t = tb; tile_block && t < nt; t += ntb)
+                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                }
+                wstamp(1);
+            }
+            if (!grid_barrier(bar, err)) return;
+            stamp();
+            {
+                int ntx;
+                const int nt = ntiles(0, ntx);
+                bmax = 0;
+                if constexpr (kRefine) {
+                    for (int t = tb; tile_block && t < nt; t += ntb)
+                        mg_refine_tile<CELL, false, 4, true>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
+                } else {
+                    SmoothArgs<R> a = base(0);
+                    a.in = mg_own<R>(P.up, P.lev, 0); a.out = mg_own<R>(P.cor, P.lev, 0);
+                    a.rhs = P.rhs; a.acf = P.a0;
+                    a.crse_res = mg_own<R>(P.res, P.lev, 1);
+                    for (int t = tb; tile_block && t < nt; t += ntb)
+                        mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, true, true, MG_NORM_ITER, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                }
+                block_max2(bmax, brhs);
+                if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
+                wstamp(1);
+            }
+        } else
         // level 0: up-sweep and the next down-sweep (8 colour sweeps), residual, restriction,
         // norm; the solution alternates between cor[0] and up[0] by iteration parity
         {
@@ -1061,7 +1120,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     if (P.trace && blockIdx.x == 1 && threadIdx.x == 0) P.trace[128] = nwork;
     // solution: the last level-0 output (cor[0] after an even number of cycles, else up[0]; the
     // FP64 solution slot it & 1 in single precision)
-    const MV<R> fin = (it & 1) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
+    const MV<R> fin = ((it & 1) && !P.split0) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
     const MGLev& L = P.lev[0];
     const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
     const size_t n0 = (size_t)L.w * L.h;
@@ -1156,6 +1215,7 @@ public:
     double* x64[2] = {nullptr, nullptr};  // single precision: FP64 level-0 solution (refinement)
     R* r32[2] = {nullptr, nullptr};
     unsigned long long* trace = nullptr;  // HPQ_MG_TRACE=1: phase timestamps of the last solve
+    bool split0 = false;                  // level-0 phase split in two (MGSolveArgs::split0)
 
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
@@ -1214,6 +1274,10 @@ public:
         const int nt0 = ((L.vhi_i - L.vlo + 16) / 16) * ((L.vhi_j - L.vlo + 16) / 16);
         coop_blocks = std::min(per * sms, nt0 + 1);  // + block 0 for the coarse levels
         coop_ok = coop && per > 0 && coop_blocks > 0;
+        // split level-0 phase once every tile block sweeps at least 4 tiles (HPQ_MG_SPLIT=0/1
+        // in the environment forces either form)
+        const char* es = getenv("HPQ_MG_SPLIT");
+        split0 = es ? (es[0] == '1') : (nt0 >= 4 * std::max(coop_blocks - 1, 1));
     }
 
     template <bool CELL>
@@ -1236,6 +1300,7 @@ public:
         P.x64[0] = x64[0]; P.x64[1] = x64[1];
         P.r32[0] = r32[0]; P.r32[1] = r32[1];
         P.trace = trace;
+        P.split0 = split0 ? 1 : 0;
         // norms and barrier state; the timeout flag stays set until the step ends, so that after
         // a timeout the remaining solves of the step leave at their first barrier
         static_assert(offsetof(Ctl, mgp_bar_err) - offsetof(Ctl, mgp_rhsnorm) == 32, "Ctl layout");

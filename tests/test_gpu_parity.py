@@ -169,6 +169,35 @@ def test_persistent_multigrid_equals_multi_kernel_form():
             assert rel_l2(a, b) <= 1e-10
 
 
+@pytest.mark.parametrize("precision", [hp.PLAIN_FP64, hp.MIXED])
+def test_split_level0_phase_equals_merged(precision):
+    """The level-0 phase of a V-cycle as one 8-sweep tile pass or two 4-sweep passes
+    (HPQ_MG_SPLIT): the same colour sweeps in the same order, so the same fields and V-cycles
+    (node-centred 33^2 and 63^2 grids), bit for bit with deterministic deposition."""
+    from cases import EXPLICIT_FFT, EXPLICIT_MOVING
+    for text in (EXPLICIT_MOVING, EXPLICIT_FFT):
+        out, cycles = [], []
+        for split in ("0", "1"):
+            old = os.environ.get("HPQ_MG_SPLIT")
+            os.environ["HPQ_MG_SPLIT"] = split
+            try:
+                g = hp.Hipace(text, precision=precision, graphs=True, deterministic=True)
+                g.init_data()
+            finally:
+                os.environ.pop("HPQ_MG_SPLIT", None)
+                if old is not None:
+                    os.environ["HPQ_MG_SPLIT"] = old
+            g.set_diag(["Bx", "By", "Ez"])
+            for s in range(2):
+                g.step(s)
+            out.append([g.get_diag(k) for k in ("Bx", "By", "Ez")])
+            cycles.append(g.counters()["mg_vcycles"])
+            g.close()
+        assert cycles[0] == cycles[1] > 0, cycles
+        for a, b in zip(*out):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("graphs", [False, True])
 def test_insitu_diagnostics_match_oracle(graphs):
     """In-situ beam moments and field reductions of every slice (BeamParticleContainer.cpp:476-548,
