@@ -21,11 +21,13 @@ struct Cx {
     R re, im;
 };
 
-// rows per block by transform length (shared memory: RB/2 complex arrays of M elements)
+// rows per block by transform length (shared memory: RB/2 complex arrays of M elements); passes
+// with fewer than 2 blocks per SM at that size run 2 rows per block instead
 template <int M>
 struct DstCfg {
     static constexpr int RB = M <= 2048 ? 4 : 2;
 };
+constexpr int kDstSmallRows = 2 * 148 * 4;  // rows below which a pass uses 2 rows per block
 
 template <class R>
 __device__ __forceinline__ Cx<R> cmul(const Cx<R>& v0, const Cx<R>& w) {
@@ -112,11 +114,10 @@ __device__ __forceinline__ R dst_val(const Cx<R>* z, int r, int e) {
 
 // Pass over rows: out(row, e) = DST-I(in row)[e]; written transposed:
 // out[(row / rows_per_plane) * n * rows_per_plane + e * rows_per_plane + row % rows_per_plane]
-template <class R, int M, int LOGM>
+template <class R, int M, int LOGM, int RB>
 __global__ void __launch_bounds__(256) k_dst_pass_t(const R* __restrict__ in, int nrows, int n, int rows_per_plane,
                                                     R* __restrict__ out, const Cx<R>* __restrict__ tw) {
     HPQ_PDL_ENTRY();
-    constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
     const int r0 = blockIdx.x * RB;
@@ -134,12 +135,11 @@ __global__ void __launch_bounds__(256) k_dst_pass_t(const R* __restrict__ in, in
 
 // y-pass, eigenvalue multiply, y-pass; rows are (plane, i) of length n = ny; eig is [j][i] with
 // row length nxe; written transposed back to [plane][j][i]
-template <class R, int M, int LOGM>
+template <class R, int M, int LOGM, int RB>
 __global__ void __launch_bounds__(256) k_dst_pass_eig(const R* __restrict__ in, int nrows, int n, int rows_per_plane,
                                                       const R* __restrict__ eig, R* __restrict__ out,
                                                       const Cx<R>* __restrict__ tw) {
     HPQ_PDL_ENTRY();
-    constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
     R* tmp = reinterpret_cast<R*>(z + (RB / 2) * M);
@@ -167,12 +167,11 @@ __global__ void __launch_bounds__(256) k_dst_pass_eig(const R* __restrict__ in, 
 }
 
 // final x-pass: rows are (plane k, j) of length nx; result scattered into field component comp[k]
-template <class R, int M, int LOGM>
+template <class R, int M, int LOGM, int RB>
 __global__ void __launch_bounds__(256) k_dst_pass_field(const R* __restrict__ in, int nrows, int n, int ny, R* base,
                                                         size_t cstride, int pitch, int c0, int c1, int c2,
                                                         const Cx<R>* __restrict__ tw) {
     HPQ_PDL_ENTRY();
-    constexpr int RB = DstCfg<M>::RB;
     extern __shared__ unsigned char smem_raw[];
     Cx<R>* z = reinterpret_cast<Cx<R>*>(smem_raw);
     const int r0 = blockIdx.x * RB;
@@ -224,37 +223,55 @@ public:
         if (twy) cudaFree(twy);
         twx = twy = nullptr;
     }
-    template <int M>
-    static size_t smem_fft() { return (size_t)(DstCfg<M>::RB / 2) * M * sizeof(Cx<R>); }
-    template <int M>
-    static size_t smem_eig(int n) { return smem_fft<M>() + (size_t)DstCfg<M>::RB * n * sizeof(R); }
+    template <int M, int RB>
+    static size_t smem_fft() { return (size_t)(RB / 2) * M * sizeof(Cx<R>); }
+    template <int M, int RB>
+    static size_t smem_eig(int n) { return smem_fft<M, RB>() + (size_t)RB * n * sizeof(R); }
+    template <int M, int LOGM, int RB>
+    static void set_attrs_rb() {
+        const int big = 200 * 1024;
+        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_t<R, M, LOGM, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_eig<R, M, LOGM, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_field<R, M, LOGM, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    }
     template <int M, int LOGM>
     static void set_attrs() {
-        const int big = 200 * 1024;
-        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_t<R, M, LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_eig<R, M, LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        HPQ_CUDA(cudaFuncSetAttribute(k_dst_pass_field<R, M, LOGM>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        set_attrs_rb<M, LOGM, DstCfg<M>::RB>();
+        if (DstCfg<M>::RB != 2) set_attrs_rb<M, LOGM, 2>();
     }
 
+    template <int M, int LOGM, int RB>
+    void pass_t_rb(cudaStream_t st, const R* in, int nrows, int n, int rpp, R* out, const Cx<R>* tw) {
+        hpq_launch(k_dst_pass_t<R, M, LOGM, RB>, dim3((nrows + RB - 1) / RB), dim3(256), smem_fft<M, RB>(), st, in, nrows, n, rpp, out, tw);
+        HPQ_LAUNCH_CHECK();
+    }
     template <int M, int LOGM>
     void pass_t(cudaStream_t st, const R* in, int nrows, int n, int rpp, R* out, const Cx<R>* tw) {
-        const int rb = DstCfg<M>::RB;
-        hpq_launch(k_dst_pass_t<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_fft<M>(), st, in, nrows, n, rpp, out, tw);
+        if (nrows < kDstSmallRows) pass_t_rb<M, LOGM, 2>(st, in, nrows, n, rpp, out, tw);
+        else pass_t_rb<M, LOGM, DstCfg<M>::RB>(st, in, nrows, n, rpp, out, tw);
+    }
+    template <int M, int LOGM, int RB>
+    void pass_eig_rb(cudaStream_t st, const R* in, int nrows, int n, int rpp, const R* eig, R* out, const Cx<R>* tw) {
+        hpq_launch(k_dst_pass_eig<R, M, LOGM, RB>, dim3((nrows + RB - 1) / RB), dim3(256), smem_eig<M, RB>(n), st, in, nrows, n, rpp, eig, out, tw);
         HPQ_LAUNCH_CHECK();
     }
     template <int M, int LOGM>
     void pass_eig(cudaStream_t st, const R* in, int nrows, int n, int rpp, const R* eig, R* out, const Cx<R>* tw) {
-        const int rb = DstCfg<M>::RB;
-        hpq_launch(k_dst_pass_eig<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_eig<M>(n), st, in, nrows, n, rpp, eig, out, tw);
+        if (nrows < kDstSmallRows) pass_eig_rb<M, LOGM, 2>(st, in, nrows, n, rpp, eig, out, tw);
+        else pass_eig_rb<M, LOGM, DstCfg<M>::RB>(st, in, nrows, n, rpp, eig, out, tw);
+    }
+    template <int M, int LOGM, int RB>
+    void pass_field_rb(cudaStream_t st, const R* in, int nrows, int n, R* base, size_t cs, int pitch, const int* comps,
+                       int nrhs, const Cx<R>* tw) {
+        hpq_launch(k_dst_pass_field<R, M, LOGM, RB>, dim3((nrows + RB - 1) / RB), dim3(256), smem_fft<M, RB>(), st,
+            in, nrows, n, ny, base, cs, pitch, comps[0], nrhs > 1 ? comps[1] : comps[0], nrhs > 2 ? comps[2] : comps[0], tw);
         HPQ_LAUNCH_CHECK();
     }
     template <int M, int LOGM>
     void pass_field(cudaStream_t st, const R* in, int nrows, int n, R* base, size_t cs, int pitch, const int* comps,
                     int nrhs, const Cx<R>* tw) {
-        const int rb = DstCfg<M>::RB;
-        hpq_launch(k_dst_pass_field<R, M, LOGM>, dim3((nrows + rb - 1) / rb), dim3(256), smem_fft<M>(), st, 
-            in, nrows, n, ny, base, cs, pitch, comps[0], nrhs > 1 ? comps[1] : comps[0], nrhs > 2 ? comps[2] : comps[0], tw);
-        HPQ_LAUNCH_CHECK();
+        if (nrows < kDstSmallRows) pass_field_rb<M, LOGM, 2>(st, in, nrows, n, base, cs, pitch, comps, nrhs, tw);
+        else pass_field_rb<M, LOGM, DstCfg<M>::RB>(st, in, nrows, n, base, cs, pitch, comps, nrhs, tw);
     }
 
 #define HPQ_DST_DISPATCH(Mval, CALL)                       \

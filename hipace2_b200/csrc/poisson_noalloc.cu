@@ -76,10 +76,10 @@ cudaError_t pass_t(cudaStream_t st, const double* in, int nrows, int n, int rpp,
                    const hpq::Cx<double>* tw) {
     const int rb = hpq::DstCfg<M>::RB;
     const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>);
-    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_t<double, M, LOGM>,
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_t<double, M, LOGM, hpq::DstCfg<M>::RB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    hpq::k_dst_pass_t<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, out, tw);
+    hpq::k_dst_pass_t<double, M, LOGM, hpq::DstCfg<M>::RB><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, out, tw);
     return cudaGetLastError();
 }
 
@@ -88,10 +88,10 @@ cudaError_t pass_eig(cudaStream_t st, const double* in, int nrows, int n, int rp
                      double* out, const hpq::Cx<double>* tw) {
     const int rb = hpq::DstCfg<M>::RB;
     const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>) + (size_t)rb * n * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_eig<double, M, LOGM>,
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_eig<double, M, LOGM, hpq::DstCfg<M>::RB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    hpq::k_dst_pass_eig<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, eig, out, tw);
+    hpq::k_dst_pass_eig<double, M, LOGM, hpq::DstCfg<M>::RB><<<(nrows + rb - 1) / rb, 256, smem, st>>>(in, nrows, n, rpp, eig, out, tw);
     return cudaGetLastError();
 }
 
@@ -102,12 +102,12 @@ cudaError_t pass_plane(cudaStream_t st, const double* in, int nrows, int n, int 
                        const hpq::Cx<double>* tw) {
     const int rb = hpq::DstCfg<M>::RB;
     const size_t smem = (size_t)(rb / 2) * M * sizeof(hpq::Cx<double>);
-    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_field<double, M, LOGM>,
+    cudaError_t e = cudaFuncSetAttribute(hpq::k_dst_pass_field<double, M, LOGM, hpq::DstCfg<M>::RB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int G = hpq::kGuardAlloc;
     double* base = out - ((ptrdiff_t)G * n + G);  // element (i, j) -> out[j * n + i]
-    hpq::k_dst_pass_field<double, M, LOGM><<<(nrows + rb - 1) / rb, 256, smem, st>>>(
+    hpq::k_dst_pass_field<double, M, LOGM, hpq::DstCfg<M>::RB><<<(nrows + rb - 1) / rb, 256, smem, st>>>(
         in, nrows, n, ny, base, 0, n, 0, 0, 0, tw);
     return cudaGetLastError();
 }
