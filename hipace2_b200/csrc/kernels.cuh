@@ -533,14 +533,17 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
 
 // ------------------------------------------------------------------------------------------
 // Beam push (BeamParticleAdvance.cpp:19-336; FP64 throughout). Pushes the non-slipped
-// particles of this slice and the particles that slipped in from the previous slice, resuming
-// at their sub-cycle count; a particle stops when it leaves the slice (z < slice lower edge).
+// particles of slice ctl->islice + lag and the particles that slipped in from the slice before
+// it, resuming at their sub-cycle count; a particle stops when it leaves the slice (z < slice
+// lower edge). S holds that slice's fields (the slice driver runs the push of a slice beside the
+// next slice's solve, on a saved copy of the fields); lag 1 beyond the box head does nothing.
 // ------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restrict__ ctl, int bi, Slab<R> S, Geo g,
-                                                   double dt) {
+                                                   double dt, int lag) {
     HPQ_PDL_ENTRY();
-    const int s = ctl->islice;
+    const int s = ctl->islice + lag;
+    if (s < 0 || s >= g.nz) return;
     const int par = ctl->step_parity;
     const int start = B.start[par][s], na = B.count[par][s];
     const int cin = (s + 1) & 1;
@@ -587,9 +590,10 @@ __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restr
 
 // ------------------------------------------------------------------------------------------
 // Slice partition after the beam push (SliceSort.cpp:13-64 with the MultiBuffer hand-off,
-// MultiBuffer.cpp:806-926): invalid particles are dropped, particles still on this slice are
-// appended to the next step's store (sub-cycle count reset), slipped particles go to the carry
-// buffer of the next slice. One block; stable order via block-wide prefix sums.
+// MultiBuffer.cpp:806-926) of slice ctl->islice + lag: invalid particles are dropped, particles
+// still on the slice are appended to the next step's store (sub-cycle count reset), slipped
+// particles go to the carry buffer of the next slice. One block; stable order via block-wide
+// prefix sums.
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void copy_particle(const BeamBuf& d, long long di, const BeamBuf& s, long long si, int nsub) {
     d.x[di] = s.x[si]; d.y[di] = s.y[si]; d.z[di] = s.z[si]; d.w[di] = s.w[si];
@@ -622,10 +626,11 @@ __device__ __forceinline__ void block_sum_store(double (&a)[NV], double* out) {
 
 // beam "This" slice: the slice's own particles and those that slipped in from the previous slice
 __global__ void __launch_bounds__(1024) k_beam_insitu(BeamDev B, const Ctl* __restrict__ ctl, int bi, double r2,
-                                                      double clight_inv, double* out) {
+                                                      double clight_inv, double* out, int lag, int nz) {
     HPQ_PDL_ENTRY();
     if (!ctl->insitu_beam[bi]) return;
-    const int s = ctl->islice;
+    const int s = ctl->islice + lag;
+    if (s < 0 || s >= nz) return;
     const int par = ctl->step_parity;
     const int start = B.start[par][s], na = B.count[par][s];
     const int cin = (s + 1) & 1;
@@ -685,13 +690,13 @@ __global__ void k_beam_gather(BeamBuf dst, const BeamBuf src, const int* __restr
     }
 }
 
-__global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, int bi, Geo g, int keep_store,
-                                                         int end_slice) {
+__global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, int bi, Geo g, int keep_store, int lag) {
     HPQ_PDL_ENTRY();
     constexpr int IT = 8;  // consecutive particles per thread and round
     __shared__ int sst[32], ssl[32];
     __shared__ int base_stay, base_slip;
-    const int s = ctl->islice;
+    const int s = ctl->islice + lag;
+    if (s < 0 || s >= g.nz) return;
     const int par = ctl->step_parity;
     const int start = B.start[par][s], na = B.count[par][s];
     const int cin = (s + 1) & 1, cout = s & 1;
@@ -764,7 +769,6 @@ __global__ void __launch_bounds__(1024) k_beam_partition(BeamDev B, Ctl* ctl, in
         B.count[1 - par][s] = keep_store ? base_stay : 0;
         if (keep_store) ctl->cursor[bi] = cursor + base_stay;
         ctl->carry_n[bi][cout] = base_slip;
-        if (end_slice) ctl->islice = s - 1;
     }
 }
 

@@ -229,6 +229,23 @@ public:
     // partition | plasma push and copies); not used while profiling, which times kernels serially
     cudaStream_t sts = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // second side stream: the beam push and partition of slice s run beside the solve of slice
+    // s - 1 (their results only feed the next step), on a copy SB of slice s's gathered fields
+    // (planes C_EZ .. C_PSI); the last slice's beam work runs when the step ends
+    cudaStream_t stb = nullptr;
+    cudaEvent_t ev_bfork = nullptr, ev_bjoin = nullptr;
+    Slab<R> SB;
+    cudaStream_t beam_begin() {
+        if (profiling) return st;
+        HPQ_CUDA(cudaEventRecord(ev_bfork, st));
+        HPQ_CUDA(cudaStreamWaitEvent(stb, ev_bfork, 0));
+        return stb;
+    }
+    void beam_end() {
+        if (profiling) return;
+        HPQ_CUDA(cudaEventRecord(ev_bjoin, stb));
+        HPQ_CUDA(cudaStreamWaitEvent(st, ev_bjoin, 0));
+    }
     cudaStream_t side_begin() {
         if (profiling) return st;
         HPQ_CUDA(cudaEventRecord(ev_fork, st));
@@ -332,6 +349,8 @@ public:
         if (st) cudaStreamSynchronize(st);
         if (S.base) cudaFree(S.base);
         S.base = nullptr;
+        if (SB.base) cudaFree(SB.base);
+        SB.base = nullptr;
         dst.release();
         pc_dst.release();
         mg.release();
@@ -373,6 +392,11 @@ public:
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         ev_fork = ev_join = nullptr;
+        if (stb) cudaStreamDestroy(stb);
+        stb = nullptr;
+        if (ev_bfork) cudaEventDestroy(ev_bfork);
+        if (ev_bjoin) cudaEventDestroy(ev_bjoin);
+        ev_bfork = ev_bjoin = nullptr;
         if (st) cudaStreamDestroy(st);
         st = nullptr;
     }
@@ -400,6 +424,9 @@ public:
         HPQ_CUDA(cudaStreamCreateWithFlags(&sts, cudaStreamNonBlocking));
         HPQ_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         HPQ_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        HPQ_CUDA(cudaStreamCreateWithFlags(&stb, cudaStreamNonBlocking));
+        HPQ_CUDA(cudaEventCreateWithFlags(&ev_bfork, cudaEventDisableTiming));
+        HPQ_CUDA(cudaEventCreateWithFlags(&ev_bjoin, cudaEventDisableTiming));
         // slab
         S.nx = nx; S.ny = ny;
         S.pitch = ((nx + 2 * kGuardAlloc + 7) / 8) * 8;
@@ -407,6 +434,9 @@ public:
         S.cstride = (size_t)S.pitch * S.rows;
         HPQ_CUDA(cudaMalloc(&S.base, S.cstride * C_NCOMP * sizeof(R)));
         HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * C_NCOMP * sizeof(R)));
+        SB = S;
+        HPQ_CUDA(cudaMalloc(&SB.base, S.cstride * (C_PSI + 1) * sizeof(R)));
+        HPQ_CUDA(cudaMemset(SB.base, 0, S.cstride * (C_PSI + 1) * sizeof(R)));
         dst.init(nx, ny, g.dx[0], g.dx[1], 3);
         if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
         if (cfg.explicit_solver) mg.init(nx, ny, g.dx[0], g.dx[1]);
@@ -896,6 +926,12 @@ public:
     }
 
     void end_step() override {
+        if (!bm.empty()) {
+            // beam work of the last slice (slice 0: the counter stands at -1)
+            const long long l0 = g_launches;
+            beam_work(1);
+            launches_total += g_launches - l0;
+        }
         physical_time += cfg.dt;
         parity = 1 - parity;
         ++beam_gen;
@@ -1476,12 +1512,41 @@ public:
     }
 
     // Hipace::SolveOneSlice (Hipace.cpp:556-728)
+    // beam in-situ reductions, push and partition of slice ctl->islice + lag (Hipace.cpp:680-700)
+    void beam_work(int lag) {
+        for (size_t b = 0; b < bm.size(); ++b) {
+            // beam in-situ reductions before the push (Hipace.cpp:680-681)
+            if (insitu_beam_d[b]) {
+                const double r = cfg.beams[b].insitu_radius;
+                hpq_launch(k_beam_insitu, dim3(1), dim3(1024), 0, st, bm[b], (const Ctl*)ctl, (int)b,
+                           r < 1e150 ? r * r : 1e300, 1.0 / cfg.pc.c, insitu_beam_d[b], lag, nz);
+                HPQ_LAUNCH_CHECK();
+            }
+            {
+                Scope sc(this, "beam_push");
+                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, SB, g, cfg.dt, lag);
+                HPQ_LAUNCH_CHECK();
+            }
+            Scope sc2(this, "beam_partition");
+            hpq_launch(k_beam_partition, dim3(1), dim3(1024), 0, st, bm[b], ctl, (int)b, g, 1, lag);
+            HPQ_LAUNCH_CHECK();
+        }
+    }
+
     void record_slice() {
         const bool ex = cfg.explicit_solver;
         if (adj_fwd) {
             // adjoint forward: the state entering a segment head is checkpointed
             hpq_launch(k_adj_checkpoint<R>, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.ck_args);
             HPQ_LAUNCH_CHECK();
+        }
+        // (the adjoint forward leaves the beam as it is: its push only feeds the next step)
+        const bool beams = !adj_fwd && !bm.empty();
+        if (beams) {
+            // the previous slice's beam push and partition, beside this slice's solve (nothing
+            // at the head of the box)
+            OnStream on(this, beam_begin());
+            beam_work(1);
         }
         if (ex) {
             if (cfg.deposit_rho) zero({C_CHI, C_SY, C_SX, C_EXMBY, C_EYPBX, C_JZB, C_RHOMJZ, C_NJXB, C_NJYB, C_RHOMJZB, C_RHO});
@@ -1554,27 +1619,12 @@ public:
         }
         // the beam push and partition (beam arrays, Ctl) run beside the plasma push and the
         // component shifts (plasma arrays, slab planes the pushes do not read)
-        // (the adjoint forward leaves the beam as it is: its push only feeds the next step)
-        const bool beams = !adj_fwd && !bm.empty();
         if (beams) {
-            OnStream on(this, side_begin());
-            for (size_t b = 0; b < bm.size(); ++b) {
-                // beam in-situ reductions before the push (Hipace.cpp:680-681)
-                if (insitu_beam_d[b]) {
-                    const double r = cfg.beams[b].insitu_radius;
-                    hpq_launch(k_beam_insitu, dim3(1), dim3(1024), 0, st, bm[b], (const Ctl*)ctl, (int)b,
-                               r < 1e150 ? r * r : 1e300, 1.0 / cfg.pc.c, insitu_beam_d[b]);
-                    HPQ_LAUNCH_CHECK();
-                }
-                {
-                    Scope sc(this, "beam_push");
-                    hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, S, g, cfg.dt);
-                    HPQ_LAUNCH_CHECK();
-                }
-                Scope sc2(this, "beam_partition");
-                hpq_launch(k_beam_partition, dim3(1), dim3(1024), 0, st, bm[b], ctl, (int)b, g, 1, b + 1 == bm.size());
-                HPQ_LAUNCH_CHECK();
-            }
+            // this slice's gathered fields for its beam push (behind the previous slice's beam
+            // work on the same side stream, beside the plasma push)
+            OnStream on(this, beam_begin());
+            HPQ_CUDA(cudaMemcpyAsync(SB.c(C_EZ).p, S.c(C_EZ).p, (size_t)(C_PSI - C_EZ + 1) * S.cstride * sizeof(R),
+                                     cudaMemcpyDeviceToDevice, st));
         }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
@@ -1587,11 +1637,9 @@ public:
         } else {
             copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
         }
-        if (beams) side_end();
-        else {
-            hpq_launch(k_slice_done, dim3(1), dim3(1), 0, st, ctl);
-            HPQ_LAUNCH_CHECK();
-        }
+        if (beams) beam_end();
+        hpq_launch(k_slice_done, dim3(1), dim3(1), 0, st, ctl);
+        HPQ_LAUNCH_CHECK();
     }
 
     // Hipace::PredictorCorrectorLoopToSolveBxBy (Hipace.cpp:935-1031)
