@@ -1626,6 +1626,12 @@ public:
             HPQ_CUDA(cudaMemcpyAsync(SB.c(C_EZ).p, S.c(C_EZ).p, (size_t)(C_PSI - C_EZ + 1) * S.cstride * sizeof(R),
                                      cudaMemcpyDeviceToDevice, st));
         }
+        if (ex) {
+            // ShiftSlices (Fields.cpp:588-604) beside the plasma push: the push reads Psi, Ez, Bx,
+            // By, Bz, none of the shifted planes
+            OnStream on(this, side_begin());
+            copies({{C_PJXB, C_JXB}, {C_PJYB, C_JYB}, {C_JXB, C_NJXB}, {C_JYB, C_NJYB}, {C_JX, C_NJXB}, {C_JY, C_NJYB}});
+        }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "plasma_push");
@@ -1633,7 +1639,7 @@ public:
             HPQ_LAUNCH_CHECK();
         }
         if (ex) {
-            copies({{C_PJXB, C_JXB}, {C_PJYB, C_JYB}, {C_JXB, C_NJXB}, {C_JYB, C_NJYB}, {C_JX, C_NJXB}, {C_JY, C_NJYB}});
+            side_end();
         } else {
             copies({{C_PCPBX, C_PBX}, {C_PCPBY, C_PBY}, {C_PBX, C_BX}, {C_PBY, C_BY}, {C_PJX, C_JX}, {C_PJY, C_JY}});
         }
