@@ -191,13 +191,16 @@ def run_ours(args):
     nb = beam["x"].size
     pinned = {key: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for key, v in beam.items()}
     host = {key: v.numpy() for key, v in pinned.items()}
+    # the pushed beam is read back into pinned arrays reused from step to step
+    res_pinned = {key: torch.empty(v.shape, dtype=v.dtype).pin_memory() for key, v in pinned.items()}
+    res_host = {key: v.numpy() for key, v in res_pinned.items()}
     torch.cuda.synchronize()
     sim.synchronize()
     t0 = time.perf_counter()
     for s in range(w + k, w + 2 * k):
         sim.set_beam(0, host)
         sim.step(s)
-        out = sim.get_beam(0)
+        out = sim.get_beam(0, out=res_host)
     sim.synchronize()
     e2e_secs = time.perf_counter() - t0
     h2d = nb * (7 * 8 + 8)

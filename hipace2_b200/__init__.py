@@ -181,14 +181,20 @@ class Hipace:
         self._check(self.L.hpq_set_beam(self.h, b, *[_dp(a) for a in arrs],
                                         _lp(ids) if ids is not None else None, len(arrs[0])))
 
-    def get_beam(self, b=0):
+    def get_beam(self, b=0, out=None):
+        """Beam particles of species b (hpq_get_beam). `out`, optional, is a dict of contiguous
+        arrays (float64, "id" int64) at least as long as the beam, e.g. in pinned memory that is
+        reused from step to step; the result is then views of its first entries."""
         n = ctypes.c_int64()
         self._check(self.L.hpq_beam_count(self.h, b, ctypes.byref(n)))
-        out = {k: np.zeros(n.value) for k in BEAM_ATTRS}
-        out["id"] = np.zeros(n.value, dtype=np.int64)
-        self._check(self.L.hpq_get_beam(self.h, b, *[_dp(out[k]) for k in BEAM_ATTRS],
-                                        _lp(out["id"])))
-        return out
+        n = n.value
+        if out is not None and all(out[k].size >= n and out[k].flags.c_contiguous for k in BEAM_ATTRS + ("id",)):
+            res = {k: out[k][:n] for k in BEAM_ATTRS + ("id",)}
+        else:
+            res = {k: np.empty(n) for k in BEAM_ATTRS}
+            res["id"] = np.empty(n, dtype=np.int64)
+        self._check(self.L.hpq_get_beam(self.h, b, *[_dp(res[k]) for k in BEAM_ATTRS], _lp(res["id"])))
+        return res
 
     def get_field(self, comp):
         nx, ny, _ = self.n_cell

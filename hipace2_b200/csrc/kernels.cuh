@@ -677,9 +677,123 @@ __global__ void __launch_bounds__(1024) k_field_insitu(Slab<R> S, const Ctl* __r
     block_sum_store<10>(a, out + (size_t)ctl->islice * 10);
 }
 
-// initial store of a beam: dst[k] = src[perm[k]] (the host's stable slice binning order)
-__global__ void k_beam_gather(BeamBuf dst, const BeamBuf src, const int* __restrict__ perm, long long n, int has_id) {
+// ------------------------------------------------------------------------------------------
+// Slice binning of an uploaded beam (BoxSort.cpp:14-78): slice = int((z - plo_z) dzi), particles
+// outside [0, nz) dropped, slices stored top-down (nz-1 first), input order kept within a slice.
+// A stable counting sort in four launches: per-chunk histograms, per-slice scans across chunks,
+// the scan over slices, and a scatter in which one warp walks its chunk in order, ranking equal
+// slices within each group of 32 with __match_any_sync.
+// ------------------------------------------------------------------------------------------
+constexpr int kBinChunk = 8192;  // particles per chunk (one block of the histogram and scatter)
+
+// key[i] = slice of particle i or -1; hist[k * nb + b] = particles of chunk b in slice k
+__global__ void __launch_bounds__(256) k_bin_hist(const double* __restrict__ z, long long n, double plo, double dzi,
+                                                  int nz, int* __restrict__ key, int* __restrict__ hist, int nb) {
     HPQ_PDL_ENTRY();
+    extern __shared__ int sh[];
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+    const long long i0 = (long long)blockIdx.x * kBinChunk;
+    const long long i1 = i0 + kBinChunk < n ? i0 + kBinChunk : n;
+    for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int s = (int)((z[i] - plo) * dzi);
+        const int k = (s < 0 || s >= nz) ? -1 : s;
+        key[i] = k;
+        if (k >= 0) atomicAdd(&sh[k], 1);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) hist[(size_t)k * nb + blockIdx.x] = sh[k];
+}
+
+// one block per slice: exclusive prefix of the slice's chunk counts (in place) and its total
+__global__ void __launch_bounds__(256) k_bin_scan_chunks(int* __restrict__ hist, int nb, int* __restrict__ count) {
+    HPQ_PDL_ENTRY();
+    __shared__ int ws[8];
+    __shared__ int carry;
+    int* h = hist + (size_t)blockIdx.x * nb;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b0 = 0; b0 < nb; b0 += blockDim.x) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < nb ? h[b] : 0;
+        int x = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += t;
+        }
+        if (lane == 31) ws[warp] = x;
+        __syncthreads();
+        int wsum = 0;
+        for (int w = 0; w < warp; ++w) wsum += ws[w];
+        const int base = carry;
+        if (b < nb) h[b] = base + wsum + x - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = base + wsum + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[blockIdx.x] = carry;
+}
+
+// one block: start of every slice, top slice first
+__global__ void __launch_bounds__(1024) k_bin_scan_slices(const int* __restrict__ count, int nz, int* __restrict__ start,
+                                                          long long* __restrict__ total) {
+    HPQ_PDL_ENTRY();
+    __shared__ int ws[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r0 = 0; r0 < nz; r0 += blockDim.x) {
+        const int r = r0 + threadIdx.x;  // rank from the top: slice nz-1-r
+        const int v = r < nz ? count[nz - 1 - r] : 0;
+        int x = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += t;
+        }
+        if (lane == 31) ws[warp] = x;
+        __syncthreads();
+        int wsum = 0;
+        for (int w = 0; w < warp; ++w) wsum += ws[w];
+        const int base = carry;
+        if (r < nz) start[nz - 1 - r] = base + wsum + x - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = base + wsum + x;
+        __syncthreads();
+        (void)nw;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// one warp per chunk, in input order: perm[start[k] + hist[k][b] + rank] = i
+__global__ void __launch_bounds__(32) k_bin_scatter(const int* __restrict__ key, long long n, const int* __restrict__ hist,
+                                                    int nb, const int* __restrict__ start, int nz, int* __restrict__ perm) {
+    HPQ_PDL_ENTRY();
+    extern __shared__ int cnt[];
+    const int b = blockIdx.x, lane = threadIdx.x;
+    for (int k = lane; k < nz; k += 32) cnt[k] = start[k] + hist[(size_t)k * nb + b];
+    __syncwarp();
+    const long long i0 = (long long)b * kBinChunk;
+    const long long i1 = i0 + kBinChunk < n ? i0 + kBinChunk : n;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long g0 = i0; g0 < i1; g0 += 32) {
+        const long long i = g0 + lane;
+        const int k = i < i1 ? key[i] : -2;
+        const unsigned m = __match_any_sync(0xffffffffu, k);
+        const int rank = __popc(m & lt);
+        if (k >= 0) perm[cnt[k] + rank] = (int)i;
+        __syncwarp();
+        if (k >= 0 && (m & lt) == 0) cnt[k] += __popc(m);
+        __syncwarp();
+    }
+}
+
+// initial store of a beam: dst[k] = src[perm[k]] for k < *n (stable slice binning order)
+__global__ void k_beam_gather(BeamBuf dst, const BeamBuf src, const int* __restrict__ perm, const long long* n_dev,
+                              int has_id) {
+    HPQ_PDL_ENTRY();
+    const long long n = *n_dev;
     for (long long k = gtid(); k < n; k += gstride()) {
         const int i = perm[k];
         dst.x[k] = src.x[i]; dst.y[k] = src.y[i]; dst.z[k] = src.z[i]; dst.w[k] = src.w[i];

@@ -351,6 +351,12 @@ public:
         S.base = nullptr;
         if (SB.base) cudaFree(SB.base);
         SB.base = nullptr;
+        if (bin_key) cudaFree(bin_key);
+        if (bin_hist) cudaFree(bin_hist);
+        if (bin_total) cudaFree(bin_total);
+        bin_key = bin_hist = nullptr;
+        bin_total = nullptr;
+        bin_key_cap = bin_hist_cap = 0;
         dst.release();
         pc_dst.release();
         mg.release();
@@ -762,22 +768,17 @@ public:
     // dropped; stable within a slice. Slices are stored top-down like the slice march. The host
     // computes only the order (a counting sort of indices); the particle data go to the device
     // as they are (from the caller's buffers, pinned or not) and are gathered there.
+    // scratch of the device slice binning: keys, per-chunk histograms, the in-box count
+    int* bin_key = nullptr;
+    int* bin_hist = nullptr;
+    long long* bin_total = nullptr;
+    long long bin_key_cap = 0, bin_hist_cap = 0;
+
     void upload_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
                      const double* uy, const double* uz, const long long* id, long long nin) {
         BeamDev& d = bm[b];
         const BeamSpecies& B = cfg.beams[b];
         d.charge = B.charge; d.mass = B.mass; d.n_subcycles = B.n_subcycles; d.do_z_push = B.do_z_push;
-        std::vector<int> sl((size_t)nin);
-        std::vector<int> cnt(nz, 0);
-        for (long long i = 0; i < nin; ++i) {
-            const int s = (int)((z[i] - cfg.prob_lo[2]) * g.dxi[2]);
-            sl[i] = (s < 0 || s >= nz) ? -1 : s;
-            if (sl[i] >= 0) cnt[sl[i]]++;
-        }
-        std::vector<int> start(nz, 0);
-        long long acc = 0;
-        for (int s = nz - 1; s >= 0; --s) { start[s] = (int)acc; acc += cnt[s]; }
-        const long long n = acc;
         if (nin > INT32_MAX) throw InputError("beam too large");
         // device buffers are kept when the new beam fits (captured slice graphs stay valid)
         if (d.buf[0].x == nullptr || nin > d.cap) {
@@ -791,12 +792,18 @@ public:
                 HPQ_CUDA(cudaMalloc(&d.count[q], nz * sizeof(int)));
             }
         }
-        std::vector<int> perm((size_t)std::max<long long>(n, 1));
-        {
-            std::vector<int> pos(start);
-            for (long long i = 0; i < nin; ++i)
-                if (sl[i] >= 0) perm[pos[sl[i]]++] = (int)i;
+        const int nb = (int)std::max<long long>((nin + kBinChunk - 1) / kBinChunk, 1);
+        if (bin_key_cap < nin || !bin_key) {
+            if (bin_key) cudaFree(bin_key);
+            bin_key_cap = std::max<long long>(nin, 1);
+            HPQ_CUDA(cudaMalloc(&bin_key, bin_key_cap * sizeof(int)));
         }
+        if (bin_hist_cap < (long long)nz * nb || !bin_hist) {
+            if (bin_hist) cudaFree(bin_hist);
+            bin_hist_cap = (long long)nz * nb;
+            HPQ_CUDA(cudaMalloc(&bin_hist, bin_hist_cap * sizeof(int)));
+        }
+        if (!bin_total) HPQ_CUDA(cudaMalloc(&bin_total, sizeof(long long)));
         for (int q = 0; q < 2; ++q) {
             HPQ_CUDA(cudaMemsetAsync(d.start[q], 0, nz * sizeof(int), st));
             HPQ_CUDA(cudaMemsetAsync(d.count[q], 0, nz * sizeof(int), st));
@@ -810,16 +817,27 @@ public:
             for (int k = 0; k < 7; ++k)
                 HPQ_CUDA(cudaMemcpyAsync(dstp[k], src[k], nin * sizeof(double), cudaMemcpyHostToDevice, st));
             if (id) HPQ_CUDA(cudaMemcpyAsync(sg.id, id, nin * sizeof(long long), cudaMemcpyHostToDevice, st));
-        }
-        if (n > 0) {
-            HPQ_CUDA(cudaMemcpyAsync(d.carry[1].nsub, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
-            hpq_launch(k_beam_gather, dim3(blocks_for(n, 256)), dim3(256), 0, st, d.buf[parity], (const BeamBuf)sg,
-                       (const int*)d.carry[1].nsub, n, id ? 1 : 0);
+            // slice binning on the device (stable counting sort, top slice first)
+            const size_t ksm = (size_t)nz * sizeof(int);
+            if (ksm > 48 * 1024) {
+                HPQ_CUDA(cudaFuncSetAttribute(k_bin_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksm));
+                HPQ_CUDA(cudaFuncSetAttribute(k_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksm));
+            }
+            hpq_launch(k_bin_hist, dim3(nb), dim3(256), ksm, st, (const double*)sg.z, nin, cfg.prob_lo[2], g.dxi[2], nz,
+                       bin_key, bin_hist, nb);
+            HPQ_LAUNCH_CHECK();
+            hpq_launch(k_bin_scan_chunks, dim3(nz), dim3(256), 0, st, bin_hist, nb, d.count[parity]);
+            HPQ_LAUNCH_CHECK();
+            hpq_launch(k_bin_scan_slices, dim3(1), dim3(1024), 0, st, (const int*)d.count[parity], nz, d.start[parity], bin_total);
+            HPQ_LAUNCH_CHECK();
+            hpq_launch(k_bin_scatter, dim3(nb), dim3(32), ksm, st, (const int*)bin_key, nin, (const int*)bin_hist, nb,
+                       (const int*)d.start[parity], nz, d.carry[1].nsub);
+            HPQ_LAUNCH_CHECK();
+            hpq_launch(k_beam_gather, dim3(blocks_for(nin, 256)), dim3(256), 0, st, d.buf[parity], (const BeamBuf)sg,
+                       (const int*)d.carry[1].nsub, (const long long*)bin_total, id ? 1 : 0);
             HPQ_LAUNCH_CHECK();
         }
-        HPQ_CUDA(cudaMemcpyAsync(d.start[parity], start.data(), nz * sizeof(int), cudaMemcpyHostToDevice, st));
-        HPQ_CUDA(cudaMemcpyAsync(d.count[parity], cnt.data(), nz * sizeof(int), cudaMemcpyHostToDevice, st));
-        HPQ_CUDA(cudaStreamSynchronize(st));  // the caller's buffers and the host vectors are released
+        HPQ_CUDA(cudaStreamSynchronize(st));  // the caller's buffers are released
         st_host.beam_particles = 0;
         ++beam_gen;
     }
