@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(1024) k_bin_scan_slices(const int* __restrict_
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int r0 = 0; r0 < nz; r0 += blockDim.x) {
         const int r = r0 + threadIdx.x;  // rank from the top: slice nz-1-r
         const int v = r < nz ? count[nz - 1 - r] : 0;
@@ -761,7 +761,6 @@ __global__ void __launch_bounds__(1024) k_bin_scan_slices(const int* __restrict_
         __syncthreads();
         if (threadIdx.x == blockDim.x - 1) carry = base + wsum + x;
         __syncthreads();
-        (void)nw;
     }
     if (threadIdx.x == 0) *total = carry;
 }

@@ -1405,10 +1405,8 @@ public:
         for (int k = 0; k < RF_N; ++k) F.f[k] = F2<double>{a.rec_f[k] + slot * cs, S.pitch};
         AdjL L;
         for (int k = 0; k < A_NCOMP; ++k) L.f[k] = a.L.c(k);
-        const double* const* lo_ = a.lam[cur];
         AdjLam lout{a.lam[cur][0], a.lam[cur][1], a.lam[cur][2], a.lam[cur][3], a.lam[cur][4], a.lam[cur][5],
                     a.lam[cur][6], a.lam[cur][7]};
-        (void)lo_;
         AdjLam lin{a.lam[1 - cur][0], a.lam[1 - cur][1], a.lam[1 - cur][2], a.lam[1 - cur][3], a.lam[1 - cur][4],
                    a.lam[1 - cur][5], a.lam[1 - cur][6], a.lam[1 - cur][7]};
         Geo gg = g;

@@ -105,3 +105,16 @@ def test_adjoint_through_torch_autograd_and_step_after():
     sim.step(0)
     assert np.isfinite(sim.get_beam(1)["x"]).all()
     sim.close()
+
+
+def test_oracle_adjoint_node_centred_grid():
+    """Odd grid: node-centred multigrid levels, whose operator is symmetric (W = 1); density knots
+    bracketing z = c t through the plasma and ion weights."""
+    text = ADJOINT_SMALL.replace("amr.n_cell = 32 32 64", "amr.n_cell = 33 33 48")
+    o = oracle_with_beams(text)
+    theta = adjoint_knots()
+    J, g = o.adjoint(theta)
+    scale = np.abs(g).max()
+    for k in (5, 10, 17, 18):
+        fd = central_difference(lambda t: o.adjoint(t, grad=False), theta, k)
+        assert abs(g[k] - fd) <= FD_TOL * scale, (k, g[k], fd)
