@@ -594,6 +594,7 @@ __global__ void k_mg_copy_out(MGLev L, MV<R> sol, MV<R> cor_even, MV<R> cor_odd,
 // arithmetic per point is the same device code, so both forms give identical results.
 // ------------------------------------------------------------------------------------------
 constexpr int kMGMaxLevels = 16;
+constexpr double kRefineTol = 1e-5;  // relative tolerance below which single precision refines in FP64
 constexpr long long kBarrierSpins = 1ll << 24;  // >= ~1 s of polling before giving up
 
 template <class R>
@@ -616,6 +617,8 @@ struct MGSolveArgs {
     R* r32[2];
     // optional phase trace (HPQ_MG_TRACE): block 0 records the global timer after each barrier
     unsigned long long* trace;
+    // single precision: 1 = level 0 with FP64 iterative refinement, 0 = plain FP32 V-cycles
+    int refine;
     // level 0 of a V-cycle as two phases of 4 sweeps (interpolation + up-sweeps, then the next
     // down-sweeps + residual) instead of one phase of 8: each 16^2 tile then sweeps a 28^2
     // region 4 + 4 times instead of a 36^2 region 8 times (40 % fewer point updates, one more
@@ -910,7 +913,8 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ int s_go;
     __shared__ double s_target, s_maxn;
-    constexpr bool kRefine = std::is_same<R, float>::value;
+    constexpr bool kFloat = std::is_same<R, float>::value;
+    const bool refine = kFloat && P.refine != 0;  // FP64 refinement of level 0 (tight tolerances)
     Ctl* ctl = P.ctl;
     unsigned int* bar = ctl->mgp_bar;
     int* err = &ctl->mgp_bar_err;
@@ -963,9 +967,11 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         int ntx;
         const int nt = ntiles(0, ntx);
         for (int t = tb; tile_block && t < nt; t += ntb) {
-            if constexpr (kRefine)
-                mg_refine_tile<CELL, true, 4>(P, 0, t % ntx, t / ntx, smem_raw, bmax, brhs);
-            else
+            bool done = false;
+            if constexpr (kFloat) {
+                if (refine) { mg_refine_tile<CELL, true, 4>(P, 0, t % ntx, t / ntx, smem_raw, bmax, brhs); done = true; }
+            }
+            if (!done)
                 mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, true, true, MG_NORM_FIRST, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
         }
         restrict_acf(1);
@@ -1036,7 +1042,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                 a.acf = P.a0;
                 int ntx;
                 const int nt = ntiles(0, ntx);
-                if constexpr (kRefine) {
+                if (refine) {
                     const size_t n0 = (size_t)P.lev[0].w * P.lev[0].h;
                     a.rhs = MV<R>{{P.r32[it & 1], P.r32[it & 1] + n0}, P.lev[0].w, 0};
                     for (int t = tb; tile_block && t < nt; t += ntb)
@@ -1055,10 +1061,15 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                 int ntx;
                 const int nt = ntiles(0, ntx);
                 bmax = 0;
-                if constexpr (kRefine) {
-                    for (int t = tb; tile_block && t < nt; t += ntb)
-                        mg_refine_tile<CELL, false, 4, true>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
-                } else {
+                bool done = false;
+                if constexpr (kFloat) {
+                    if (refine) {
+                        for (int t = tb; tile_block && t < nt; t += ntb)
+                            mg_refine_tile<CELL, false, 4, true>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
+                        done = true;
+                    }
+                }
+                if (!done) {
                     SmoothArgs<R> a = base(0);
                     a.in = mg_own<R>(P.up, P.lev, 0); a.out = mg_own<R>(P.cor, P.lev, 0);
                     a.rhs = P.rhs; a.acf = P.a0;
@@ -1084,9 +1095,11 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             const int nt = ntiles(0, ntx);
             bmax = 0;
             for (int t = tb; tile_block && t < nt; t += ntb) {
-                if constexpr (kRefine)
-                    mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
-                else
+                bool done = false;
+                if constexpr (kFloat) {
+                    if (refine) { mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs); done = true; }
+                }
+                if (!done)
                     mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
             }
             block_max2(bmax, brhs);
@@ -1126,7 +1139,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     const size_t n0 = (size_t)L.w * L.h;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < vw * vh; k += nb * blockDim.x) {
         const int i = L.vlo + k % vw, j = L.vlo + k / vw;
-        if constexpr (kRefine) {
+        if (refine) {
             const double* x = P.x64[it & 1];
             P.sol(i, j, 0) = (R)x[(size_t)j * L.w + i];
             P.sol(i, j, 1) = (R)x[n0 + (size_t)j * L.w + i];
@@ -1216,6 +1229,7 @@ public:
     R* r32[2] = {nullptr, nullptr};
     unsigned long long* trace = nullptr;  // HPQ_MG_TRACE=1: phase timestamps of the last solve
     bool split0 = false;                  // level-0 phase split in two (MGSolveArgs::split0)
+    int refine_force = -1;                // single precision: -1 by tolerance, 0 plain FP32, 1 FP64 refinement
 
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
@@ -1278,6 +1292,9 @@ public:
         // in the environment forces either form)
         const char* es = getenv("HPQ_MG_SPLIT");
         split0 = es ? (es[0] == '1') : (nt0 >= 4 * std::max(coop_blocks - 1, 1));
+        // single precision: HPQ_MG_REFINE=0/1 forces plain FP32 V-cycles or FP64 refinement
+        const char* er = getenv("HPQ_MG_REFINE");
+        refine_force = er ? (er[0] == '1' ? 1 : 0) : -1;
     }
 
     template <bool CELL>
@@ -1301,6 +1318,9 @@ public:
         P.r32[0] = r32[0]; P.r32[1] = r32[1];
         P.trace = trace;
         P.split0 = split0 ? 1 : 0;
+        // single precision refines level 0 in FP64 only where the tolerance asks for it: an FP32
+        // V-cycle reaches relative residuals well below kRefineTol on its own
+        P.refine = std::is_same<R, float>::value && (refine_force >= 0 ? refine_force == 1 : tol_rel < kRefineTol);
         // norms and barrier state; the timeout flag stays set until the step ends, so that after
         // a timeout the remaining solves of the step leave at their first barrier
         static_assert(offsetof(Ctl, mgp_bar_err) - offsetof(Ctl, mgp_rhsnorm) == 32, "Ctl layout");
