@@ -7,6 +7,7 @@ sm_100a. This module binds it with ctypes and mirrors the reference's driver sur
 the library or a CUDA device is missing.
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -24,7 +25,8 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_begin_step", "hpq_solve_slice", "hpq_end_step", "hpq_get_field", "hpq_set_diag",
            "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
-           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad", "hpq_n_cell")
+           "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad", "hpq_n_cell",
+           "hpq_max_step", "hpq_time", "hpq_diag_count", "hpq_beam_name")
 
 _lib = None
 
@@ -72,6 +74,10 @@ def load_library(path=None):
         "hpq_get_insitu": ([vp, cp, dp], i32),
         "hpq_adjoint_nparams": ([vp, ctypes.POINTER(i32)], i32),
         "hpq_n_cell": ([vp, ctypes.POINTER(i32)], i32),
+        "hpq_max_step": ([vp, ctypes.POINTER(i32)], i32),
+        "hpq_time": ([vp, dp], i32),
+        "hpq_diag_count": ([vp, lp], i32),
+        "hpq_beam_name": ([vp, i32], cp),
         "hpq_adjoint_grad": ([vp, dp, dp, dp], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
@@ -136,7 +142,9 @@ class Hipace:
         nc = (ctypes.c_int * 3)()
         self._check(self.L.hpq_n_cell(self.h, nc))
         self.n_cell = [nc[0], nc[1], nc[2]]
-        self.max_step = _scalar(input_text, "max_step", 0)
+        ms = ctypes.c_int()
+        self._check(self.L.hpq_max_step(self.h, ctypes.byref(ms)))
+        self.max_step = ms.value
         self.diag_type = _string(input_text, "diagnostic.diag_type", "xyz")
         self._diag = []
 
@@ -157,9 +165,19 @@ class Hipace:
         self._check(self.L.hpq_init(self.h))
 
     def evolve(self, first_step=0, last_step=None):
+        """Steps first_step .. last_step (default max_step), leaving the loop after the step
+        at hipace.max_time like Hipace::Evolve (Hipace.cpp:401-419)."""
         last = self.max_step if last_step is None else last_step
         for s in range(first_step, last + 1):
+            if math.isinf(self.time()):
+                break
             self.step(s)
+
+    def time(self):
+        """Physical time at which the next step starts (+inf after the step at max_time)."""
+        t = ctypes.c_double()
+        self._check(self.L.hpq_time(self.h, ctypes.byref(t)))
+        return t.value
 
     def step(self, step):
         self._check(self.L.hpq_step(self.h, step))
@@ -211,6 +229,9 @@ class Hipace:
         diagnostic.diag_type = xz / yz."""
         nx, ny, nz = self.n_cell
         out = np.zeros(_diag_shape(self.diag_type, nx, ny, nz))
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_diag_count(self.h, ctypes.byref(n)))
+        assert n.value == out.size, (n.value, out.shape)
         self._check(self.L.hpq_get_diag(self.h, comp.encode(), _dp(out)))
         return out
 
@@ -271,15 +292,6 @@ class Hipace:
         self._check(self.L.hpq_get_counters(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
                                             ctypes.byref(d)))
         return {"mg_vcycles": a.value, "slices": b.value, "plasma_pushes": c.value, "kernel_launches": d.value}
-
-
-def _scalar(text, key, default):
-    v = default
-    for line in text.splitlines():
-        line = line.split("#")[0]
-        if "=" in line and line.split("=")[0].strip() == key:
-            v = int(float(line.split("=", 1)[1].split()[0]))
-    return v
 
 
 def _string(text, key, default):

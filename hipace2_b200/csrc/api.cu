@@ -1,5 +1,6 @@
 // C ABI of the slice loop (declared in include/hpq.h). All exceptions stop here and turn into
 // status codes plus a message kept on the handle.
+#include <cmath>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -80,6 +81,33 @@ int hpq_n_cell(const hpq_handle* h, int n_cell[3]) {
     return HPQ_OK;
 }
 
+const char* hpq_beam_name(const hpq_handle* h, int beam) {
+    if (!h || beam < 0 || beam >= (int)h->cfg.beams.size()) return nullptr;
+    return h->cfg.beams[(size_t)beam].name.c_str();
+}
+
+int hpq_max_step(const hpq_handle* h, int* max_step) {
+    if (!h || !max_step) return HPQ_ERR_ARG;
+    *max_step = h->cfg.max_step;
+    return HPQ_OK;
+}
+
+int hpq_time(hpq_handle* h, double* t) {
+    return guarded(h, [&] {
+        if (!t) return (int)HPQ_ERR_ARG;
+        *t = h->sim ? h->sim->time() : 0.0;
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_diag_count(const hpq_handle* h, int64_t* n) {
+    if (!h || !n) return HPQ_ERR_ARG;
+    const hpq::SimConfig& c = h->cfg;
+    const int64_t plane = c.diag_type == 0 ? (int64_t)c.n_cell[0] * c.n_cell[1] : c.diag_type == 1 ? c.n_cell[0] : c.n_cell[1];
+    *n = plane * c.n_cell[2];
+    return HPQ_OK;
+}
+
 int hpq_set_precision(hpq_handle* h, int mode) {
     return guarded(h, [&] {
         if (h->initialised) { h->err = "hpq_set_precision must come before hpq_init"; return (int)HPQ_ERR_STATE; }
@@ -136,6 +164,10 @@ int hpq_begin_step(hpq_handle* h, int step) {
     return guarded(h, [&] {
         if (int r = need_init(h)) return r;
         if (h->in_step) { h->err = "hpq_begin_step inside a step"; return (int)HPQ_ERR_STATE; }
+        if (std::isinf(h->sim->time())) {
+            h->err = "the step at hipace.max_time has run; the simulation has ended";
+            return (int)HPQ_ERR_STATE;
+        }
         h->sim->begin_step(step);
         h->in_step = true;
         return (int)HPQ_OK;

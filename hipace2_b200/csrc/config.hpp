@@ -11,6 +11,7 @@
 // beams) are rejected with an explicit error instead of being silently ignored.
 #pragma once
 
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -173,6 +174,18 @@ struct SimConfig {
 inline void mid_plane(int n, int& lo, int& hi, double& wlo, double& whi) {
     if (n % 2) { lo = hi = (n - 1) / 2; wlo = 1.0; whi = 0.0; }
     else { lo = n / 2 - 1; hi = n / 2; wlo = 0.5; whi = 0.5; }
+}
+
+// Time step of the step that starts at time t (Hipace::Evolve, Hipace.cpp:424-435): a step that
+// starts at max_time is a last step with dt = 0, after which the time is infinite and the step
+// loop ends (Hipace.cpp:413-419); a step that would cross max_time is shortened to end on it.
+struct StepTime {
+    double dt, next;
+};
+inline StepTime step_time(double t, double dt, double max_time) {
+    if (t == max_time) return {0.0, std::numeric_limits<double>::infinity()};
+    if ((t + dt >= max_time && t < max_time) || (t + dt <= max_time && t > max_time)) return {max_time - t, max_time};
+    return {dt, t + dt};
 }
 
 // utils::doDiagnostics (IOUtil.cpp:75-82)

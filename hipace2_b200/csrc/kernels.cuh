@@ -93,6 +93,8 @@ struct Ctl {
     int insitu_fields, insitu_pad;
     // adjoint forward: checkpoints of segment heads are written while set
     int adj_ckpt, adj_pad;
+    // beam time step of this step (hipace.dt, shortened to end on hipace.max_time)
+    double beam_dt;
 };
 
 struct Geo {
@@ -540,7 +542,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
 // ------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restrict__ ctl, int bi, Slab<R> S, Geo g,
-                                                   double dt, int lag) {
+                                                   int lag) {
     HPQ_PDL_ENTRY();
     const int s = ctl->islice + lag;
     if (s < 0 || s >= g.nz) return;
@@ -551,7 +553,7 @@ __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restr
     const BeamBuf a = B.buf[par];
     const BeamBuf c = B.carry[cin];
     const int nsubc = B.n_subcycles;
-    const double dtb = dt / nsubc;
+    const double dtb = ctl->beam_dt / nsubc;
     const double clight = g.c, inv_c2 = 1. / (g.c * g.c);
     const double cmr = B.charge / B.mass;
     const double min_z = g.plo[2] + s * g.dx[2];

@@ -73,6 +73,8 @@ public:
     virtual int adjoint_nparams() const = 0;
     virtual double adjoint(const double* theta, double* grad) = 0;
     virtual std::string profile_names() = 0;
+    // physical time at which the next step starts (infinite once the step at max_time ran)
+    virtual double time() const = 0;
     const SimConfig& config() const { return cfg; }
     SimConfig cfg;
 };
@@ -222,6 +224,7 @@ public:
     int cur_step = 0;
     int cur_islice = 0;
     double physical_time = 0;
+    double next_time = 0;  // physical time after the current step (step_time)
     bool use_graphs = false;
     bool capturing = false;
     cudaStream_t st2 = nullptr;
@@ -328,6 +331,8 @@ public:
         *n = it->second.n;
         return true;
     }
+    double time() const override { return physical_time; }
+
     std::string profile_names() override {
         std::string r;
         for (auto& kv : prof) r += kv.first + " ";
@@ -927,6 +932,9 @@ public:
         std::memset(ctl_h, 0, sizeof(Ctl));
         ctl_h->islice = nz - 1;
         ctl_h->step_parity = parity;
+        const StepTime T = step_time(physical_time, cfg.dt, cfg.max_time);
+        ctl_h->beam_dt = T.dt;
+        next_time = T.next;
         for (size_t b = 0; b < cfg.beams.size() && b < (size_t)kMaxBeams; ++b) {
             const bool on = insitu_beam_d[b] && do_diagnostics(cfg.beams[b].insitu_period, step, cfg.max_step,
                                                                physical_time, cfg.max_time);
@@ -950,7 +958,7 @@ public:
             beam_work(1);
             launches_total += g_launches - l0;
         }
-        physical_time += cfg.dt;
+        physical_time = next_time;
         parity = 1 - parity;
         ++beam_gen;
         HPQ_CUDA(cudaMemcpyAsync(ctl_h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
@@ -1540,7 +1548,7 @@ public:
             }
             {
                 Scope sc(this, "beam_push");
-                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, SB, g, cfg.dt, lag);
+                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, SB, g, lag);
                 HPQ_LAUNCH_CHECK();
             }
             Scope sc2(this, "beam_partition");

@@ -44,6 +44,17 @@ const char* hpq_last_error(const hpq_handle* h);
 /* Grid size (amr.n_cell, after my_constants and expressions are evaluated), valid after
  * hpq_create (Hipace.cpp:176-230 reads the same key). */
 int hpq_n_cell(const hpq_handle* h, int n_cell[3]);
+/* max_step of the input (the last step of Hipace::Evolve's loop, Hipace.cpp:401). */
+int hpq_max_step(const hpq_handle* h, int* max_step);
+/* Physical time at which the next step starts (0 before the first step). Steps follow the
+ * reference's max_time rule (Hipace.cpp:413-435): a step that would cross hipace.max_time is
+ * shortened to end on it, the step that starts on it runs with dt = 0, after which the time is
+ * +infinity and hpq_begin_step / hpq_step return HPQ_ERR_STATE (the reference leaves its step
+ * loop there). */
+int hpq_time(hpq_handle* h, double* t);
+/* Number of doubles hpq_get_diag writes per component: nz*ny*nx (diagnostic.diag_type = xyz),
+ * nz*nx (xz) or nz*ny (yz). */
+int hpq_diag_count(const hpq_handle* h, int64_t* n);
 /* Text of the last hpq_create failure (no handle exists then). */
 const char* hpq_create_error(void);
 
@@ -64,6 +75,8 @@ int hpq_init(hpq_handle* h);
 int hpq_set_beam(hpq_handle* h, int beam, const double* x, const double* y, const double* z,
                  const double* w, const double* ux, const double* uy, const double* uz,
                  const int64_t* id, int64_t n);
+/* Name of beam `beam` (beams.names order), or NULL past the last beam. */
+const char* hpq_beam_name(const hpq_handle* h, int beam);
 /* Number of stored particles of a beam and a copy of them (slices from head to tail). */
 int hpq_beam_count(hpq_handle* h, int beam, int64_t* n);
 int hpq_get_beam(hpq_handle* h, int beam, double* x, double* y, double* z, double* w,

@@ -513,6 +513,7 @@ public:
     PoissonDST dst;
     Multigrid mg;
     double physical_time = 0;
+    double step_dt = 0, next_time = 0;  // this step's dt and end time (hpq::step_time)
     std::string error;
     int mg_status = 0;
     long long mg_iters_total = 0;
@@ -997,7 +998,7 @@ public:
     // BeamParticleAdvance.cpp:19-336 (no external fields, spin or radiation reaction)
     void beam_push(int b, BeamSlice& bs, int islice) {
         const hpq::BeamSpecies& B = cfg.beams[b];
-        const double dtb = cfg.dt / B.n_subcycles;
+        const double dtb = step_dt / B.n_subcycles;
         const double clight = cfg.pc.c, inv_c2 = 1. / (cfg.pc.c * cfg.pc.c);
         const double cmr = B.charge / B.mass;
         const double min_z = cfg.prob_lo[2] + (islice - 0) * dz;
@@ -1210,10 +1211,14 @@ public:
     }
 
     // -------------------------------------------------------------- one step
-    // Hipace::Evolve per-step body (Hipace.cpp:401-492), one rank, fixed dt
+    // Hipace::Evolve per-step body (Hipace.cpp:401-492), one rank, fixed dt shortened to end on
+    // max_time (Hipace.cpp:424-435)
     void begin_step(int step) {
         for (auto& kv : F) kv.second.zero();  // ResetAllQuantities
         cur_step = step;
+        const hpq::StepTime T = hpq::step_time(physical_time, cfg.dt, cfg.max_time);
+        step_dt = T.dt;
+        next_time = T.next;
         insitu_beam.resize(cfg.beams.size());
         for (size_t b = 0; b < cfg.beams.size(); ++b)
             if (insitu_beam_on(b)) insitu_beam[b].assign((size_t)nz * 23, 0.0);
@@ -1237,7 +1242,7 @@ public:
         for (size_t s = 0; s < plasmas.size(); ++s)
             if (!cfg.plasmas[s].neutralize_background) { plasmas[s].valid = saved[s].valid; plasmas[s].w = saved[s].w; }
     }
-    void end_step() { physical_time += cfg.dt; }
+    void end_step() { physical_time = next_time; }
 
     // ---- in-situ diagnostics (BeamParticleContainer.cpp:476-548, Fields.cpp:1289-1346)
     int cur_step = 0;
@@ -1962,6 +1967,7 @@ int oracle_step(OracleHandle* h, int step) { return h->sim->step(step); }
 int oracle_begin_step(OracleHandle* h, int step) { h->sim->begin_step(step); return 0; }
 int oracle_solve_slice(OracleHandle* h, int islice, int step) { h->sim->solve_one_slice(islice, step); return h->sim->mg_status; }
 int oracle_end_step(OracleHandle* h) { h->sim->end_step(); return 0; }
+double oracle_time(OracleHandle* h) { return h->sim->physical_time; }
 
 // interior nx*ny values of a slice component (current slice state)
 int oracle_get_field(OracleHandle* h, const char* name, double* out) {

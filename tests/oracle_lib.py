@@ -49,6 +49,8 @@ def lib():
         L.oracle_begin_step.argtypes = [vp, i32]
         L.oracle_solve_slice.argtypes = [vp, i32, i32]
         L.oracle_end_step.argtypes = [vp]
+        L.oracle_time.argtypes = [vp]
+        L.oracle_time.restype = ctypes.c_double
         L.oracle_get_field.argtypes = [vp, cp, dp]
         L.oracle_plasma_count.argtypes = [vp, i32]
         L.oracle_plasma_count.restype = i64
@@ -152,6 +154,9 @@ class Oracle:
 
     def end_step(self):
         self.L.oracle_end_step(self.h)
+
+    def time(self):
+        return self.L.oracle_time(self.h)
 
     def get_field(self, name):
         out = np.zeros((self.ny, self.nx))

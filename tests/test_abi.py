@@ -47,3 +47,17 @@ def test_calls_out_of_order_are_state_errors():
     with pytest.raises(hp.HpqError) as e:
         sim.step(0)
     assert e.value.code == 3
+
+
+def test_queries_without_gpu():
+    """Grid, max_step, diagnostic size, beam names and time are answered from the inputs."""
+    from cases import golden_input
+    text = golden_input("linear_wake.normalized.1Rank") + "\nmax_step = 4\ndiagnostic.diag_type = xz\n"
+    sim = hp.Hipace(text)
+    L = sim.L
+    assert sim.max_step == 4
+    nx, ny, nz = sim.n_cell
+    n = ctypes.c_int64()
+    assert L.hpq_diag_count(sim.h, ctypes.byref(n)) == 0 and n.value == nz * nx
+    assert L.hpq_beam_name(sim.h, 0) == b"beam" and L.hpq_beam_name(sim.h, 1) is None
+    assert sim.time() == 0.0
