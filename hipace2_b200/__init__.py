@@ -26,7 +26,7 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
            "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad", "hpq_n_cell",
-           "hpq_max_step", "hpq_time", "hpq_diag_count", "hpq_beam_name")
+           "hpq_max_step", "hpq_time", "hpq_diag_count", "hpq_beam_name", "hpq_salame_log")
 
 _lib = None
 
@@ -78,6 +78,7 @@ def load_library(path=None):
         "hpq_time": ([vp, dp], i32),
         "hpq_diag_count": ([vp, lp], i32),
         "hpq_beam_name": ([vp, i32], cp),
+        "hpq_salame_log": ([vp, dp, lp], i32),
         "hpq_adjoint_grad": ([vp, dp, dp, dp], i32),
         "hpq_synchronize": ([vp], i32),
         "hpq_stream": ([vp], vp),
@@ -172,6 +173,14 @@ class Hipace:
             if math.isinf(self.time()):
                 break
             self.step(s)
+
+    def salame_log(self):
+        """(slice, iteration, W) rows of every SALAME iteration since init_data."""
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_salame_log(self.h, None, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        self._check(self.L.hpq_salame_log(self.h, _dp(out), ctypes.byref(n)))
+        return out.reshape(-1, 3)
 
     def time(self):
         """Physical time at which the next step starts (+inf after the step at max_time)."""

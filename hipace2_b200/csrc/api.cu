@@ -1,5 +1,6 @@
 // C ABI of the slice loop (declared in include/hpq.h). All exceptions stop here and turn into
 // status codes plus a message kept on the handle.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <sstream>
@@ -84,6 +85,17 @@ int hpq_n_cell(const hpq_handle* h, int n_cell[3]) {
 const char* hpq_beam_name(const hpq_handle* h, int beam) {
     if (!h || beam < 0 || beam >= (int)h->cfg.beams.size()) return nullptr;
     return h->cfg.beams[(size_t)beam].name.c_str();
+}
+
+int hpq_salame_log(hpq_handle* h, double* out, int64_t* n) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!n) return (int)HPQ_ERR_ARG;
+        const std::vector<double>& v = h->sim->salame_record();
+        if (out) std::copy(v.begin(), v.end(), out);
+        *n = (int64_t)v.size();
+        return (int)HPQ_OK;
+    });
 }
 
 int hpq_max_step(const hpq_handle* h, int* max_step) {

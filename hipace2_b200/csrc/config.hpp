@@ -7,7 +7,7 @@
 //   <plasma>.*    PlasmaParticleContainer.cpp:27-187, PlasmaParticleContainer.H:151-200
 //   <beam>.*      BeamParticleContainer.cpp:41-290, BeamParticleContainer.H:206-300
 // Features that the reference has but this slice loop does not implement (mesh refinement,
-// lasers, SALAME, ionization, collisions, periodic/open field boundaries, adaptive dt, openPMD
+// lasers, ionization, collisions, periodic/open field boundaries, adaptive dt, openPMD
 // beams) are rejected with an explicit error instead of being silently ignored.
 #pragma once
 
@@ -57,6 +57,7 @@ struct BeamSpecies {
     double charge = 0, mass = 0;
     double density = 0;              // peak density (fixed_ppc: profile density)
     double zmin = -1e300, zmax = 1e300, radius = 1e300;
+    bool do_salame = false;          // <beam>.do_salame (BeamParticleContainer.cpp:66)
     double position_mean[3] = {0, 0, 0};
     double position_std[3] = {0, 0, 0};
     int ppc[3] = {1, 1, 1};
@@ -159,10 +160,19 @@ struct SimConfig {
     int fields_insitu_period = 0;  // fields.insitu_period (Fields.cpp:41, 1289-1346)
     int diag_type = 0;             // diagnostic.diag_type: 0 xyz, 1 xz, 2 yz (see mid_plane)
     AdjointConfig adjoint;
+    // SALAME beam-loading weights (Hipace.cpp:137-143, Hipace.H:284-301)
+    int salame_n_iter = 5;
+    bool salame_do_advance = true;
+    Expr salame_target;  // hipace.salame_Ez_target(zeta,zeta_initial,Ez_initial)
+    double salame_relative_tolerance = 1e-4;
     std::vector<PlasmaSpecies> plasmas;
     std::vector<BeamSpecies> beams;
     bool any_neutralize_background() const {
         for (auto& p : plasmas) if (p.neutralize_background) return true;
+        return false;
+    }
+    bool any_salame() const {
+        for (auto& b : beams) if (b.do_salame) return true;
         return false;
     }
 };
@@ -385,7 +395,7 @@ inline SimConfig build_config(const InputStore& in) {
         in.query(name + ".duz_per_uz0_dzeta", b.duz_per_uz0_dzeta);
         query_alt(in, name, "beams", "insitu_period", b.insitu_period);
         query_alt(in, name, "beams", "insitu_radius", b.insitu_radius);
-        reject(in, name + ".do_salame", "SALAME is outside the slice loop");
+        in.query_bool(name + ".do_salame", b.do_salame);
         reject(in, name + ".do_spin_tracking", "spin tracking is outside the slice loop");
         reject(in, name + ".do_radiation_reaction", "radiation reaction is outside the slice loop");
         reject(in, name + ".external_E(x,y,z,t)", "external fields are not implemented");
@@ -471,6 +481,9 @@ inline SimConfig build_config(const InputStore& in) {
                 b.profile = BeamProfile::Gaussian;
                 in.query(name + ".zmin", b.zmin);
                 in.query(name + ".zmax", b.zmax);
+                if (b.do_salame && (b.zmin <= -1e300 || b.zmax >= 1e300))
+                    throw InputError("For the SALAME algorithm it is mandatory to either use a 'can' profile or "
+                                     "'zmin' and 'zmax' with a gaussian profile");
             } else {
                 throw InputError("Only gaussian and can are supported with fixed_weight beam injection");
             }
@@ -508,6 +521,16 @@ inline SimConfig build_config(const InputStore& in) {
     }
     if (c.fields_insitu_period > 0 && !c.explicit_solver)
         throw InputError("Must use explicit solver for field insitu diagnostic");
+    in.query("hipace.salame_n_iter", c.salame_n_iter);
+    in.query_bool("hipace.salame_do_advance", c.salame_do_advance);
+    {
+        std::string t = "Ez_initial";
+        in.query_str("hipace.salame_Ez_target(zeta,zeta_initial,Ez_initial)", t);
+        c.salame_target = in.function(t, {"zeta", "zeta_initial", "Ez_initial"});
+    }
+    in.query("hipace.salame_relative_tolerance", c.salame_relative_tolerance);
+    if (c.any_salame() && !c.explicit_solver)
+        throw InputError("Cannot use SALAME algorithm with predictor-corrector solver");
     std::string witness;
     if (in.query_str("adjoint.witness", witness)) {
         AdjointConfig& a = c.adjoint;
@@ -515,6 +538,7 @@ inline SimConfig build_config(const InputStore& in) {
             if (c.beams[b].name == witness) a.witness = (int)b;
         if (a.witness < 0) throw InputError("adjoint.witness = " + witness + " is not in beams.names");
         if (!c.explicit_solver) throw InputError("the adjoint needs the explicit Bx/By solver");
+        if (c.any_salame()) throw InputError("the adjoint does not differentiate SALAME");
         for (auto& p : c.plasmas)
             if (p.n_subcycles != 1) throw InputError("the adjoint needs plasma n_subcycles = 1");
         double r[2];

@@ -15,6 +15,7 @@
 
 #include "adjoint.cuh"
 #include "common.cuh"
+#include "salame.cuh"
 #include "config.hpp"
 #include "dst.cuh"
 #include <type_traits>
@@ -75,6 +76,8 @@ public:
     virtual std::string profile_names() = 0;
     // physical time at which the next step starts (infinite once the step at max_time ran)
     virtual double time() const = 0;
+    // SALAME record: (slice, iteration, weight factor) of every iteration since hpq_init
+    virtual const std::vector<double>& salame_record() const = 0;
     const SimConfig& config() const { return cfg; }
     SimConfig cfg;
 };
@@ -211,6 +214,20 @@ public:
     Slab<R> S;
     PoissonDST<R> dst;
     PoissonDST<R> pc_dst;  // the two Bx/By solves of the predictor-corrector loop
+    PoissonDST<R> sal_dst;  // the Ez solves of the SALAME slice
+    // slab components allocated: the slice, plus the SALAME slice when a beam does SALAME
+    int ncomp_alloc = C_NCOMP;
+    // SALAME state (Hipace.H:284-301): this step runs it, the last SALAME slice, overloading,
+    // the zeta where it started, per-beam particle counts of the step's slices (host copy), the
+    // device sums of SalameGetW and a record of (slice, iteration, W)
+    bool sal_step = false;
+    int sal_last = -1;
+    bool sal_overloaded = false;
+    double sal_zeta0 = 0;
+    std::vector<std::vector<int>> sal_count;
+    double* sal_sums_d = nullptr;
+    double* sal_sums_h = nullptr;
+    std::vector<double> salame_log;
     Multigrid<R> mg;
     std::vector<PlasmaDev<R>> pl;
     std::vector<double*> px0, py0;
@@ -332,6 +349,7 @@ public:
         return true;
     }
     double time() const override { return physical_time; }
+    const std::vector<double>& salame_record() const override { return salame_log; }
 
     std::string profile_names() override {
         std::string r;
@@ -364,6 +382,11 @@ public:
         bin_key_cap = bin_hist_cap = 0;
         dst.release();
         pc_dst.release();
+        sal_dst.release();
+        if (sal_sums_d) cudaFree(sal_sums_d);
+        if (sal_sums_h) cudaFreeHost(sal_sums_h);
+        sal_sums_d = nullptr;
+        sal_sums_h = nullptr;
         mg.release();
         for (auto& p : pl)
             for (void* q : {(void*)p.x, (void*)p.y, (void*)p.w, (void*)p.ux, (void*)p.uy, (void*)p.psi, (void*)p.xp,
@@ -443,14 +466,20 @@ public:
         S.pitch = ((nx + 2 * kGuardAlloc + 7) / 8) * 8;
         S.rows = ny + 2 * kGuardAlloc;
         S.cstride = (size_t)S.pitch * S.rows;
-        HPQ_CUDA(cudaMalloc(&S.base, S.cstride * C_NCOMP * sizeof(R)));
-        HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * C_NCOMP * sizeof(R)));
+        ncomp_alloc = (cfg.explicit_solver && cfg.any_salame()) ? 2 * C_NCOMP : C_NCOMP;
+        HPQ_CUDA(cudaMalloc(&S.base, S.cstride * ncomp_alloc * sizeof(R)));
+        HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * ncomp_alloc * sizeof(R)));
         SB = S;
         HPQ_CUDA(cudaMalloc(&SB.base, S.cstride * (C_PSI + 1) * sizeof(R)));
         HPQ_CUDA(cudaMemset(SB.base, 0, S.cstride * (C_PSI + 1) * sizeof(R)));
         dst.init(nx, ny, g.dx[0], g.dx[1], 3);
         if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
         if (cfg.explicit_solver) mg.init(nx, ny, g.dx[0], g.dx[1]);
+        if (ncomp_alloc > C_NCOMP) {
+            sal_dst.init(nx, ny, g.dx[0], g.dx[1], 1);
+            HPQ_CUDA(cudaMalloc(&sal_sums_d, 4 * sizeof(double)));
+            HPQ_CUDA(cudaMallocHost(&sal_sums_h, 4 * sizeof(double)));
+        }
         HPQ_CUDA(cudaMalloc(&ctl, sizeof(Ctl)));
         HPQ_CUDA(cudaMemset(ctl, 0, sizeof(Ctl)));
         HPQ_CUDA(cudaMallocHost(&ctl_h, sizeof(Ctl)));
@@ -460,10 +489,11 @@ public:
         // double precision uses the FFT where the grid allows it, else the SIMT GEMMs
         const char* env = getenv("HPQ_DST");
         const std::string dmode = env ? env : "";
-        if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); }
+        if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); if (sal_dst.nx) sal_dst.set_mode(false); }
         else if (dmode != "fft" && std::is_same<R, float>::value) {
             dst.set_tensor_mode(&ctl->tc_err);
             pc_dst.set_tensor_mode(&ctl->tc_err);
+            if (sal_dst.nx) sal_dst.set_tensor_mode(&ctl->tc_err);
         }
         init_plasma_lattices();
         insitu_alloc();
@@ -909,7 +939,18 @@ public:
     // deposit the ion background
     void begin_step(int step) override {
         cur_step = step;
-        HPQ_CUDA(cudaMemsetAsync(S.base, 0, S.cstride * C_NCOMP * sizeof(R), st));
+        HPQ_CUDA(cudaMemsetAsync(S.base, 0, S.cstride * ncomp_alloc * sizeof(R), st));
+        // SALAME runs in step 0 only (MultiBeam::isSalameNow, MultiBeam.cpp:128-139); the host
+        // needs each SALAME beam's particle count per slice to decide slice by slice
+        sal_step = ncomp_alloc > C_NCOMP && step == 0;
+        sal_count.assign(bm.size(), {});
+        if (sal_step)
+            for (size_t b = 0; b < bm.size(); ++b) {
+                if (!cfg.beams[b].do_salame) continue;
+                sal_count[b].resize(nz);
+                HPQ_CUDA(cudaMemcpyAsync(sal_count[b].data(), bm[b].count[parity], nz * sizeof(int), cudaMemcpyDeviceToHost, st));
+            }
+        if (sal_step) HPQ_CUDA(cudaStreamSynchronize(st));
         const double c_t = cfg.pc.c * physical_time;
         for (size_t s = 0; s < pl.size(); ++s) {
             const PlasmaSpecies& P = cfg.plasmas[s];
@@ -1060,7 +1101,7 @@ public:
         if (on == (det.w[0] != nullptr)) return;
         invalidate_graph();
         if (on) {
-            const size_t n = (size_t)C_NCOMP * S.cstride;
+            const size_t n = (size_t)ncomp_alloc * S.cstride;
             HPQ_CUDA(cudaMalloc(&det_mem, 3 * n * sizeof(long long)));
             HPQ_CUDA(cudaMemset(det_mem, 0, 3 * n * sizeof(long long)));
             for (int k = 0; k < 3; ++k) det.w[k] = det_mem + k * n;
@@ -1113,6 +1154,135 @@ public:
         if (cfg.explicit_solver) hpq_launch(k_grad_psi_sxsy<R>, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, S, g);
         else hpq_launch(k_grad_psi<R>, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, S, g);
         HPQ_LAUNCH_CHECK();
+    }
+
+    // ExplicitDeposition (ExplicitDeposition.cpp:20-265): Sx, Sy += the plasma contribution
+    void explicit_deposit() {
+        for (size_t s = 0; s < pl.size(); ++s) {
+            if (pl[s].n == 0) continue;
+            Scope sc(this, "explicit_deposit");
+            const int nb = blocks_for(pl[s].n, 256);
+            if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            HPQ_LAUNCH_CHECK();
+            det_flush({C_SX, C_SY});
+        }
+    }
+
+    // ---- SALAME (Salame.cpp). The SALAME slice is slab components C_NCOMP + c (view SV).
+    bool salame_slice(int islice) const {
+        for (size_t b = 0; b < bm.size(); ++b)
+            if (cfg.beams[b].do_salame && !sal_count[b].empty() && sal_count[b][islice] > 0) return true;
+        return false;
+    }
+    Slab<R> salame_view() const {
+        Slab<R> V = S;
+        V.base = S.base + (size_t)C_NCOMP * S.cstride;
+        return V;
+    }
+    // Fields::SolvePoissonEz on the SALAME slice
+    void salame_ez(const Slab<R>& V) {
+        hpq_launch(k_sal_rhs_ez<R>, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, V, g, sal_dst.stage, sal_dst.sj);
+        HPQ_LAUNCH_CHECK();
+        const int comps[1] = {C_EZ};
+        sal_dst.solve(st, 1, V.base, V.cstride, V.pitch, comps);
+    }
+    void salame_deposit_jz(R* jz) {
+        for (size_t b = 0; b < bm.size(); ++b)
+            if (cfg.beams[b].do_salame) deposit_beam((int)b, 0, nullptr, nullptr, jz, nullptr);
+    }
+    // SalameModule (Salame.cpp:14-185), one level, no grid current; W is decided on the host
+    // like the reference's (its print of the weight factor becomes a record in salame_log)
+    void salame(int islice) {
+        constexpr int N = C_NCOMP;
+        const Slab<R> V = salame_view();
+        const double zoff = g.plo[2] + 0.5 * g.dx[2];  // GetPosOffset(2, geom, domain)
+        // the target is Ez of the first SALAME slice of a contiguous run, before SALAME (:21-29)
+        if (islice + 1 != sal_last) {
+            copies({{N + kSalEzTarget, C_EZ}});
+            sal_overloaded = false;
+            sal_zeta0 = islice * g.dx[2] + zoff;
+        }
+        sal_last = islice;
+        // the plasma part of Sx, Sy alone, kept for step 4 (:32-39)
+        zero({C_SY, C_SX});
+        explicit_deposit();
+        copies({{N + kSalSyBack, C_SY}, {N + kSalSxBack, C_SX}});
+        for (int iter = 0; iter < cfg.salame_n_iter; ++iter) {
+            const int it0 = iter;
+            // step 1: Ez of the next slice with the present weights (:43-76)
+            for (size_t s = 0; s < pl.size(); ++s) {
+                if (pl[s].n == 0) continue;
+                hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, (const int*)nullptr);
+                HPQ_LAUNCH_CHECK();
+            }
+            copies({{N + C_JX, C_NJXB}, {N + C_JY, C_NJYB}});
+            for (size_t s = 0; s < pl.size(); ++s)
+                deposit_plasma((int)s, V.c(C_JX).p, V.c(C_JY).p, nullptr, nullptr, nullptr, nullptr);
+            zero({N + C_EZ, N + C_JZB, N + C_SY, N + C_SX, N + C_BX, N + C_BY});
+            salame_ez(V);
+            copies({{N + kSalEzNoSalame, N + C_EZ}});
+            // step 2: the Ez of the next slice from the SALAME beam alone (:78-123)
+            salame_deposit_jz(V.c(C_JZB).p);
+            hpq_launch(k_sal_sxsy<R>, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, V, g);
+            HPQ_LAUNCH_CHECK();
+            copies({{N + C_CHI, C_CHI}});  // the solve takes chi of this slice
+            if (mg.cell) mg_solve_t<true>(V); else mg_solve_t<false>(V);
+            zero({N + C_EZ, N + C_JX, N + C_JY});
+            if (cfg.salame_do_advance) {
+                for (size_t s = 0; s < pl.size(); ++s) {
+                    if (pl[s].n == 0) continue;
+                    hpq_launch(k_sal_only_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], V, g);
+                    HPQ_LAUNCH_CHECK();
+                    deposit_plasma((int)s, V.c(C_JX).p, V.c(C_JY).p, nullptr, nullptr, nullptr, nullptr);
+                }
+            } else {
+                hpq_launch(k_sal_jxjy_from_b<R>, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, S, V, g);
+                HPQ_LAUNCH_CHECK();
+            }
+            salame_ez(V);
+            // step 3: the weight factor (:125-158, SalameGetW :334-400)
+            zero({N + C_JZB});
+            salame_deposit_jz(V.c(C_JZB).p);
+            hpq_launch(k_sal_sums<R>, dim3(1), dim3(1024), 0, st, V, sal_sums_d);
+            HPQ_LAUNCH_CHECK();
+            HPQ_CUDA(cudaMemcpyAsync(sal_sums_h, sal_sums_d, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            HPQ_CUDA(cudaStreamSynchronize(st));
+            const double sjz = sal_sums_h[3];
+            double s_t = sal_sums_h[0] / sjz;
+            const double s_no = sal_sums_h[1] / sjz, s_only = sal_sums_h[2] / sjz;
+            const double args[3] = {(islice - 1) * g.dx[2] + zoff, sal_zeta0, s_t};  // Ez of the next slice
+            s_t = cfg.salame_target.eval(args);
+            double W = (s_t - s_no) / s_only + 1.0;
+            if (W < 0 || sal_overloaded) {
+                W = 0;
+                iter = cfg.salame_n_iter - 1;
+                sal_overloaded = true;
+            }
+            salame_log.insert(salame_log.end(), {(double)islice, (double)it0, W});
+            if (!sal_overloaded && iter >= 1 && std::abs(W - 1.) < cfg.salame_relative_tolerance) iter = cfg.salame_n_iter - 1;
+            for (size_t b = 0; b < bm.size(); ++b) {
+                if (!cfg.beams[b].do_salame) continue;
+                hpq_launch(k_sal_weight, dim3(148), dim3(256), 0, st, bm[b], (const Ctl*)ctl, W);
+                HPQ_LAUNCH_CHECK();
+            }
+            // step 4: Bx, By of this slice with the new weights (:160-183)
+            zero({C_JZB, C_SY, C_SX});
+            for (size_t b = 0; b < bm.size(); ++b) deposit_beam((int)b, 0, nullptr, nullptr, S.c(C_JZB).p, nullptr);
+            // (recomputes ExmBy, EypBx from the unchanged Psi: the same values)
+            hpq_launch(k_grad_psi_sxsy<R>, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, S, g);
+            HPQ_LAUNCH_CHECK();
+            {
+                CopyList L{};
+                L.n = 2;
+                L.dst[0] = C_SY; L.src[0] = N + kSalSyBack;
+                L.dst[1] = C_SX; L.src[1] = N + kSalSxBack;
+                hpq_launch(k_add_comps<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 8)), dim3(256), 0, st, S, L);
+                HPQ_LAUNCH_CHECK();
+            }
+            mg_solve();
+        }
     }
 
     void mg_solve() {
@@ -1495,7 +1665,8 @@ public:
     // one slice: replay the captured graph, or launch kernel by kernel (profiling mode)
     void solve_slice(int islice) override {
         if (islice != cur_islice) throw InputError("slices must be solved from the head (nz-1) to the tail (0)");
-        if (use_graphs && !profiling) {
+        // the SALAME step runs kernel by kernel: its iterations end on host decisions
+        if (use_graphs && !profiling && !sal_step) {
             if (!slice_exec) capture_slice();
             HPQ_CUDA(cudaGraphLaunch(slice_exec, st));
             launches_total += launches_top;
@@ -1583,9 +1754,11 @@ public:
                 // independent)
                 for (size_t b = 0; b < bm.size(); ++b) {
                     Scope sc(this, "beam_deposit");
-                    const bool nj = cfg.do_beam_jx_jy_deposition;
+                    // a SALAME beam deposits only jz in the SALAME step (MultiBeam.cpp:50-56)
+                    const bool sal = sal_step && cfg.beams[b].do_salame;
+                    const bool nj = cfg.do_beam_jx_jy_deposition && !sal;
                     hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st,
-                        bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho ? S.c(C_RHOMJZB).p : nullptr,
+                        bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho && !sal ? S.c(C_RHOMJZB).p : nullptr,
                         nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det);
                     HPQ_LAUNCH_CHECK();
                     det_flush({C_JZB, C_RHOMJZB, C_NJXB, C_NJYB});
@@ -1608,17 +1781,9 @@ public:
         }
         field_solve_psi_ez_bz();
         if (ex) {
-            for (size_t s = 0; s < pl.size(); ++s) {
-                if (pl[s].n == 0) continue;
-                Scope sc(this, "explicit_deposit");
-                const int nb = blocks_for(pl[s].n, 256);
-                if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-                else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-                else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-                HPQ_LAUNCH_CHECK();
-                det_flush({C_SX, C_SY});
-            }
+            explicit_deposit();
             mg_solve();
+            if (sal_step && !capturing && salame_slice(cur_islice)) salame(cur_islice);
         } else {
             pc_loop();
         }

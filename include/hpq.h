@@ -151,6 +151,13 @@ int hpq_set_deterministic(hpq_handle* h, int on);
  * species with n_subcycles 1. */
 int hpq_adjoint_nparams(hpq_handle* h, int* n);
 int hpq_adjoint_grad(hpq_handle* h, const double* knots, double* grad, double* objective);
+/* SALAME (<beam>.do_salame, hipace.salame_*; src/salame/Salame.cpp): in step 0 the weights of
+ * the SALAME beams are rescaled slice by slice so that the current-weighted Ez of the next slice
+ * follows hipace.salame_Ez_target(zeta,zeta_initial,Ez_initial). The reference prints the weight
+ * factor W of every iteration (Salame.cpp:146-157); here they are kept as (slice, iteration, W)
+ * triples: *n receives the number of doubles (3 per iteration) and `out`, if not NULL, the
+ * values. */
+int hpq_salame_log(hpq_handle* h, double* out, int64_t* n);
 /* Wait for all work of the handle. */
 int hpq_synchronize(hpq_handle* h);
 /* Per-kernel-class timing with CUDA events on the launching stream (kernel launch mode only).

@@ -516,6 +516,11 @@ public:
     double step_dt = 0, next_time = 0;  // this step's dt and end time (hpq::step_time)
     std::string error;
     int mg_status = 0;
+    // SALAME state (Hipace.H:290-295) and a record of (slice, iteration, W) of every iteration
+    int sal_last = -1;
+    bool sal_overloaded = false;
+    double sal_zeta0 = 0;
+    std::vector<double> salame_log;
     long long mg_iters_total = 0;
     // diagnostics: requested components, 3-D arrays (nz x ny x nx) for the last solved step
     std::vector<std::string> diag_names;
@@ -541,6 +546,12 @@ public:
             "Next.jx", "Next.jy", "Prev.Bx", "Prev.By", "Prev.jx", "Prev.jy", "PCIter.Bx",
             "PCIter.By", "PCPrevIter.Bx", "PCPrevIter.By", "Ions.rhomjz"};
         if (c.explicit_solver) for (auto* n : names_explicit) F[n].init(gr);
+        // the SALAME slice (Fields.cpp:117-128)
+        if (c.explicit_solver && c.any_salame())
+            for (auto* n : {"Salame.Ez_target", "Salame.Ez_no_salame", "Salame.Ez", "Salame.jx", "Salame.jy",
+                            "Salame.jz_beam", "Salame.Bx", "Salame.By", "Salame.Sy", "Salame.Sx", "Salame.Sy_back",
+                            "Salame.Sx_back"})
+                F[n].init(gr);
         else for (auto* n : names_pc) F[n].init(gr);
         dst.init(nx, ny, dx, dy);
         if (c.explicit_solver) mg.init(nx, ny, dx, dy);
@@ -711,6 +722,7 @@ public:
             const double charge_mu0_mass_ratio = charge * cfg.pc.mu0 / P.mass;
             Field *Fjx = nullptr, *Fjy = nullptr, *Fjz = nullptr, *Frho = nullptr, *Fchi = nullptr, *Frm = nullptr;
             if (which == 2) { Frm = &f("Ions.rhomjz"); }
+            else if (which == 3) { Fjx = &f("Salame.jx"); Fjy = &f("Salame.jy"); }
             else if (cfg.explicit_solver) {
                 if (which == 0) {
                     if (jxjy) { Fjx = &f("jx"); Fjy = &f("jy"); }
@@ -1131,9 +1143,10 @@ public:
         // deposition on This
         if (ex) {
             plasma_deposit(0, true, false, cfg.deposit_rho, true, true);
+            // SALAME beams deposit only jz in step 0 (MultiBeam.cpp:50-56)
             for (size_t b = 0; b < cfg.beams.size(); ++b)
                 beam_deposit(bthis[b], cfg.beams[b].charge, nullptr, nullptr, &f("jz_beam"),
-                             cfg.do_beam_jz_minus_rho ? &f("rhomjz_beam") : nullptr);
+                             cfg.do_beam_jz_minus_rho && !is_salame(b, step) ? &f("rhomjz_beam") : nullptr);
         } else {
             plasma_deposit(0, true, true, cfg.deposit_rho, false, true);
             for (size_t b = 0; b < cfg.beams.size(); ++b)
@@ -1153,7 +1166,7 @@ public:
             for (size_t b = 0; b < cfg.beams.size(); ++b) load_beam_slice((int)b, islice - 1, bnext[b]);
         if (ex) {
             for (size_t b = 0; b < cfg.beams.size(); ++b)
-                if (cfg.do_beam_jx_jy_deposition)
+                if (cfg.do_beam_jx_jy_deposition && !is_salame(b, step))
                     beam_deposit(bnext[b], cfg.beams[b].charge, &f("Next.jx_beam"), &f("Next.jy_beam"), nullptr, nullptr);
             init_sxsy_with_beam();
             explicit_deposit();
@@ -1162,6 +1175,7 @@ public:
                                     cfg.mg_max_iters, &iters);
             mg_iters_total += iters;
             if (st != 0 && mg_status == 0) mg_status = st;
+            if (salame_now(step)) salame_module(islice);
         } else {
             pc_loop(islice);
         }
@@ -1243,6 +1257,167 @@ public:
             if (!cfg.plasmas[s].neutralize_background) { plasmas[s].valid = saved[s].valid; plasmas[s].w = saved[s].w; }
     }
     void end_step() { physical_time = next_time; }
+
+    // -------------------------------------------------------------- SALAME (Salame.cpp)
+    bool is_salame(size_t b, int step) const { return cfg.beams[b].do_salame && step == 0; }
+    // MultiBeam::isSalameNow (MultiBeam.cpp:128-139): step 0 and a SALAME beam has particles in
+    // this slice (slipped ones not counted)
+    bool salame_now(int step) const {
+        if (step != 0) return false;
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (cfg.beams[b].do_salame && bthis[b].num_nonslipped > 0) return true;
+        return false;
+    }
+    int mg_solve_fields(const char* bx, const char* by, const char* sy, const char* sx) {
+        int iters = 0;
+        const int st = mg.solve(f(bx), f(by), f(sy), f(sx), f("chi"), cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters, &iters);
+        mg_iters_total += iters;
+        if (st != 0 && mg_status == 0) mg_status = st;
+        return st;
+    }
+    // Fields::SolvePoissonEz (Fields.cpp:960-1005) on the SALAME slice
+    void salame_solve_ez() {
+        const Field& jx = f("Salame.jx"); const Field& jy = f("Salame.jy");
+        std::vector<double> st((size_t)nx * ny);
+        const double hx = 0.5 * dxi, hy = 0.5 * dyi, fe = 1. / (cfg.pc.ep0 * cfg.pc.c);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                st[(size_t)j * nx + i] = fe * ((jx(i + 1, j) - jx(i - 1, j)) * hx) + fe * ((jy(i, j + 1) - jy(i, j - 1)) * hy);
+        dst.solve(st);
+        Field& ez = f("Salame.Ez");
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) ez(i, j) = st[(size_t)j * nx + i];
+    }
+    void salame_deposit_jz(Field& jz) {
+        for (size_t b = 0; b < cfg.beams.size(); ++b)
+            if (cfg.beams[b].do_salame) beam_deposit(bthis[b], cfg.beams[b].charge, nullptr, nullptr, &jz, nullptr);
+    }
+    // SalameModule (Salame.cpp:14-185): one level, no grid current
+    void salame_module(int islice) {
+        const double zoff = cfg.prob_lo[2] + 0.5 * dz;  // GetPosOffset(2, geom, domain)
+        // always use the Ez field from before SALAME started (:21-29)
+        if (islice + 1 != sal_last) {
+            copy(f("Salame.Ez_target"), f("Ez"));
+            sal_overloaded = false;
+            sal_zeta0 = islice * dz + zoff;
+        }
+        sal_last = islice;
+        // plasma-only Sx, Sy, kept for step 4 (:32-39)
+        f("Sy").zero(); f("Sx").zero();
+        explicit_deposit();
+        copy(f("Salame.Sy_back"), f("Sy")); copy(f("Salame.Sx_back"), f("Sx"));
+        for (int iter = 0; iter < cfg.salame_n_iter; ++iter) {
+            const int it0 = iter;
+            // step 1: Ez of the next slice with the current SALAME weights (:43-76)
+            plasma_push(true);
+            copy(f("Salame.jx"), f("Next.jx_beam")); copy(f("Salame.jy"), f("Next.jy_beam"));
+            plasma_deposit(3, true, false, false, false, false);
+            for (auto n : {"Salame.Ez", "Salame.jz_beam", "Salame.Sy", "Salame.Sx", "Salame.Bx", "Salame.By"}) f(n).zero();
+            salame_solve_ez();
+            copy(f("Salame.Ez_no_salame"), f("Salame.Ez"));
+            // step 2: the Ez response to the SALAME beam alone (:78-123)
+            salame_deposit_jz(f("Salame.jz_beam"));
+            {
+                // SalameInitializeSxSyWithBeam (:189-220)
+                const Field& jzb = f("Salame.jz_beam");
+                Field& Sx = f("Salame.Sx"); Field& Sy = f("Salame.Sy");
+                const double dxih = 0.5 * dxi, dyih = 0.5 * dyi, mu0 = cfg.pc.mu0;
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        const double dx_jzb = (jzb(i + 1, j) - jzb(i - 1, j)) * dxih;
+                        const double dy_jzb = (jzb(i, j + 1) - jzb(i, j - 1)) * dyih;
+                        Sy(i, j) = mu0 * (-dy_jzb);
+                        Sx(i, j) = -mu0 * (-dx_jzb);
+                    }
+            }
+            mg_solve_fields("Salame.Bx", "Salame.By", "Salame.Sy", "Salame.Sx");
+            for (auto n : {"Salame.Ez", "Salame.jx", "Salame.jy"}) f(n).zero();
+            if (cfg.salame_do_advance) {
+                salame_only_advance();
+                plasma_deposit(3, true, false, false, false, false);
+            } else {
+                // SalameGetJxJyFromBxBy (:223-255)
+                const double dzf = 1.5 * dz, mu0_inv = 1. / cfg.pc.mu0;
+                const Field& chi = f("chi"); const Field& bx = f("Salame.Bx"); const Field& by = f("Salame.By");
+                Field& jx = f("Salame.jx"); Field& jy = f("Salame.jy");
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        jx(i, j) = dzf * chi(i, j) * by(i, j) * mu0_inv;
+                        jy(i, j) = -dzf * chi(i, j) * bx(i, j) * mu0_inv;
+                    }
+            }
+            salame_solve_ez();
+            // step 3: the weight factor (:125-158, SalameGetW :334-400)
+            f("Salame.jz_beam").zero();
+            salame_deposit_jz(f("Salame.jz_beam"));
+            double s_t = 0, s_no = 0, s_only = 0, s_jz = 0;
+            {
+                const Field& jz = f("Salame.jz_beam"); const Field& et = f("Salame.Ez_target");
+                const Field& eno = f("Salame.Ez_no_salame"); const Field& ez = f("Salame.Ez");
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        s_t += jz(i, j) * et(i, j);
+                        s_no += jz(i, j) * eno(i, j);
+                        s_only += jz(i, j) * ez(i, j);
+                        s_jz += jz(i, j);
+                    }
+            }
+            s_t /= s_jz; s_no /= s_jz; s_only /= s_jz;
+            const double zeta = (islice - 1) * dz + zoff;  // the Ez of the next slice
+            const double args[3] = {zeta, sal_zeta0, s_t};
+            s_t = cfg.salame_target.eval(args);
+            double W = (s_t - s_no) / s_only + 1.0;
+            if (W < 0 || sal_overloaded) {
+                W = 0;
+                iter = cfg.salame_n_iter - 1;
+                sal_overloaded = true;
+            }
+            salame_log.insert(salame_log.end(), {(double)islice, (double)it0, W});
+            if (!sal_overloaded && iter >= 1 && std::abs(W - 1.) < cfg.salame_relative_tolerance) iter = cfg.salame_n_iter - 1;
+            // SalameMultiplyBeamWeight (:403-437)
+            for (size_t b = 0; b < cfg.beams.size(); ++b) {
+                if (!cfg.beams[b].do_salame) continue;
+                for (size_t ip = 0; ip < bthis[b].num_nonslipped; ++ip) {
+                    BeamParticle& p = bthis[b].p[ip];
+                    if (!p.valid) continue;
+                    if (W == 0) { p.valid = false; continue; }
+                    p.w *= W;
+                }
+            }
+            // step 4: Bx, By of this slice with the new weights (:160-183)
+            f("jz_beam").zero(); f("Sy").zero(); f("Sx").zero();
+            for (size_t b = 0; b < cfg.beams.size(); ++b)
+                beam_deposit(bthis[b], cfg.beams[b].charge, nullptr, nullptr, &f("jz_beam"), nullptr);
+            init_sxsy_with_beam();
+            {
+                Field& Sy = f("Sy"); Field& Sx = f("Sx");
+                const Field& by = f("Salame.Sy_back"); const Field& bx = f("Salame.Sx_back");
+                for (size_t k = 0; k < Sy.a.size(); ++k) { Sy.a[k] += by.a[k]; Sx.a[k] += bx.a[k]; }
+            }
+            mg_solve_fields("Bx", "By", "Sy", "Sx");
+        }
+    }
+    // SalameOnlyAdvancePlasma (Salame.cpp:257-331): momenta from the SALAME-only Bx, By at the
+    // previous position
+    void salame_only_advance() {
+        const Field& FBx = f("Salame.Bx"); const Field& FBy = f("Salame.By");
+        for (size_t s = 0; s < plasmas.size(); ++s) {
+            Plasma& pl = plasmas[s];
+            const double qm = cfg.plasmas[s].charge / cfg.plasmas[s].mass;
+            for (size_t ip = 0; ip < pl.n(); ++ip) {
+                if (!pl.valid[ip]) continue;
+                const double x = (pl.x_prev[ip] - xoff) * dxi, y = (pl.y_prev[ip] - yoff) * dyi;
+                double bxp = 0, byp = 0;
+                for (int iy = 0; iy <= 2; ++iy)
+                    for (int ix = 0; ix <= 2; ++ix) {
+                        Shape sx = shape2(x, ix), sy = shape2(y, iy);
+                        bxp += sx.s * sy.s * FBx(sx.cell, sy.cell);
+                        byp += sx.s * sy.s * FBy(sx.cell, sy.cell);
+                    }
+                pl.ux[ip] = 1.5 * dz * qm * byp;
+                pl.uy[ip] = -1.5 * dz * qm * bxp;
+            }
+        }
+    }
 
     // ---- in-situ diagnostics (BeamParticleContainer.cpp:476-548, Fields.cpp:1289-1346)
     int cur_step = 0;
@@ -1968,6 +2143,12 @@ int oracle_begin_step(OracleHandle* h, int step) { h->sim->begin_step(step); ret
 int oracle_solve_slice(OracleHandle* h, int islice, int step) { h->sim->solve_one_slice(islice, step); return h->sim->mg_status; }
 int oracle_end_step(OracleHandle* h) { h->sim->end_step(); return 0; }
 double oracle_time(OracleHandle* h) { return h->sim->physical_time; }
+// SALAME record: (slice, iteration, weight factor) triples; returns the number of doubles
+long long oracle_salame_log(OracleHandle* h, double* out) {
+    const auto& v = h->sim->salame_log;
+    if (out) std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return (long long)v.size();
+}
 
 // interior nx*ny values of a slice component (current slice state)
 int oracle_get_field(OracleHandle* h, const char* name, double* out) {

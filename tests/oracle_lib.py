@@ -51,6 +51,8 @@ def lib():
         L.oracle_end_step.argtypes = [vp]
         L.oracle_time.argtypes = [vp]
         L.oracle_time.restype = ctypes.c_double
+        L.oracle_salame_log.argtypes = [vp, dp]
+        L.oracle_salame_log.restype = ctypes.c_longlong
         L.oracle_get_field.argtypes = [vp, cp, dp]
         L.oracle_plasma_count.argtypes = [vp, i32]
         L.oracle_plasma_count.restype = i64
@@ -157,6 +159,13 @@ class Oracle:
 
     def time(self):
         return self.L.oracle_time(self.h)
+
+    def salame_log(self):
+        """(slice, iteration, W) rows of every SALAME iteration so far."""
+        n = self.L.oracle_salame_log(self.h, None)
+        out = np.zeros(n)
+        self.L.oracle_salame_log(self.h, _dp(out))
+        return out.reshape(-1, 3)
 
     def get_field(self, name):
         out = np.zeros((self.ny, self.nx))
