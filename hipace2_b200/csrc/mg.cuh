@@ -907,14 +907,19 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
     }
 }
 
-template <class R, bool CELL>
+// T0: tile edge of level 0 (16, or 32 on large grids: a 4-sweep phase then loads 44^2 points per
+// 32^2 tile instead of 28^2 per 16^2, 1.6x less halo work; the sweeps give the same values). With
+// T0 = 32 level 0 always runs in the split form and without FP64 refinement.
+template <class R, bool CELL, int T0 = 16>
 __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
     __shared__ int s_go;
     __shared__ double s_target, s_maxn;
     constexpr bool kFloat = std::is_same<R, float>::value;
-    const bool refine = kFloat && P.refine != 0;  // FP64 refinement of level 0 (tight tolerances)
+    constexpr bool kRefinable = kFloat && T0 == 16;
+    const bool refine = kRefinable && P.refine != 0;  // FP64 refinement of level 0 (tight tolerances)
+    const bool split = T0 != 16 || P.split0 != 0;
     Ctl* ctl = P.ctl;
     unsigned int* bar = ctl->mgp_bar;
     int* err = &ctl->mgp_bar_err;
@@ -944,8 +949,9 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     const bool tile_block = (nb == 1) || blockIdx.x > 0;
     auto ntiles = [&](int l, int& ntx) {
         const MGLev& L = P.lev[l];
-        ntx = (L.vhi_i - L.vlo + 16) / 16;
-        return ntx * ((L.vhi_j - L.vlo + 16) / 16);
+        const int T = l == 0 ? T0 : 16;
+        ntx = (L.vhi_i - L.vlo + T) / T;
+        return ntx * ((L.vhi_j - L.vlo + T) / T);
     };
     // coefficient of level l from level l-1 (average_down_acoef), grid-stride
     auto restrict_acf = [&](int l) {
@@ -968,11 +974,11 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         const int nt = ntiles(0, ntx);
         for (int t = tb; tile_block && t < nt; t += ntb) {
             bool done = false;
-            if constexpr (kFloat) {
+            if constexpr (kRefinable) {
                 if (refine) { mg_refine_tile<CELL, true, 4>(P, 0, t % ntx, t / ntx, smem_raw, bmax, brhs); done = true; }
             }
             if (!done)
-                mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, true, true, MG_NORM_FIRST, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                mg_smooth_tile<R, CELL, T0, MG_INIT_VIEW, true, true, MG_NORM_FIRST, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
         }
         restrict_acf(1);
         block_max2(bmax, brhs);
@@ -1034,7 +1040,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
         // (single precision: the first 4 sweeps of the correction d, from the interpolated coarse
         // correction with the FP32 residual as right-hand side, go to up[0]; the second pass
         // reloads d, sweeps 4 more times, adds it to the FP64 solution and forms the residual)
-        if (P.split0) {
+        if (split) {
             {
                 SmoothArgs<R> a = base(0);
                 a.crse_in = (P.sb == 1) ? mg_own<R>(P.cor, P.lev, 1) : mg_own<R>(P.up, P.lev, 1);
@@ -1042,16 +1048,21 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                 a.acf = P.a0;
                 int ntx;
                 const int nt = ntiles(0, ntx);
-                if (refine) {
-                    const size_t n0 = (size_t)P.lev[0].w * P.lev[0].h;
-                    a.rhs = MV<R>{{P.r32[it & 1], P.r32[it & 1] + n0}, P.lev[0].w, 0};
-                    for (int t = tb; tile_block && t < nt; t += ntb)
-                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP0, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
-                } else {
+                bool done = false;
+                if constexpr (kRefinable) {
+                    if (refine) {
+                        const size_t n0 = (size_t)P.lev[0].w * P.lev[0].h;
+                        a.rhs = MV<R>{{P.r32[it & 1], P.r32[it & 1] + n0}, P.lev[0].w, 0};
+                        for (int t = tb; tile_block && t < nt; t += ntb)
+                            mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP0, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                        done = true;
+                    }
+                }
+                if (!done) {
                     a.in = mg_own<R>(P.cor, P.lev, 0);
                     a.rhs = P.rhs;
                     for (int t = tb; tile_block && t < nt; t += ntb)
-                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                        mg_smooth_tile<R, CELL, T0, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                 }
                 wstamp(1);
             }
@@ -1062,7 +1073,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                 const int nt = ntiles(0, ntx);
                 bmax = 0;
                 bool done = false;
-                if constexpr (kFloat) {
+                if constexpr (kRefinable) {
                     if (refine) {
                         for (int t = tb; tile_block && t < nt; t += ntb)
                             mg_refine_tile<CELL, false, 4, true>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs);
@@ -1075,7 +1086,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                     a.rhs = P.rhs; a.acf = P.a0;
                     a.crse_res = mg_own<R>(P.res, P.lev, 1);
                     for (int t = tb; tile_block && t < nt; t += ntb)
-                        mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, true, true, MG_NORM_ITER, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                        mg_smooth_tile<R, CELL, T0, MG_INIT_VIEW, true, true, MG_NORM_ITER, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                 }
                 block_max2(bmax, brhs);
                 if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
@@ -1096,11 +1107,13 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
             bmax = 0;
             for (int t = tb; tile_block && t < nt; t += ntb) {
                 bool done = false;
-                if constexpr (kFloat) {
+                if constexpr (kRefinable) {
                     if (refine) { mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs); done = true; }
                 }
-                if (!done)
-                    mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
+                if constexpr (T0 == 16) {
+                    if (!done)
+                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
+                }
             }
             block_max2(bmax, brhs);
             if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
@@ -1133,7 +1146,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     if (P.trace && blockIdx.x == 1 && threadIdx.x == 0) P.trace[128] = nwork;
     // solution: the last level-0 output (cor[0] after an even number of cycles, else up[0]; the
     // FP64 solution slot it & 1 in single precision)
-    const MV<R> fin = ((it & 1) && !P.split0) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
+    const MV<R> fin = ((it & 1) && !split) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
     const MGLev& L = P.lev[0];
     const int vw = L.vhi_i - L.vlo + 1, vh = L.vhi_j - L.vlo + 1;
     const size_t n0 = (size_t)L.w * L.h;
@@ -1230,6 +1243,9 @@ public:
     unsigned long long* trace = nullptr;  // HPQ_MG_TRACE=1: phase timestamps of the last solve
     bool split0 = false;                  // level-0 phase split in two (MGSolveArgs::split0)
     int refine_force = -1;                // single precision: -1 by tolerance, 0 plain FP32, 1 FP64 refinement
+    bool use32 = false;                   // level-0 tiles of 32^2 (k_mg_solve<R, CELL, 32>) for unrefined solves
+    int coop_blocks32 = 0;
+    size_t coop_smem32 = 0;
 
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
@@ -1295,6 +1311,20 @@ public:
         // single precision: HPQ_MG_REFINE=0/1 forces plain FP32 V-cycles or FP64 refinement
         const char* er = getenv("HPQ_MG_REFINE");
         refine_force = er ? (er[0] == '1' ? 1 : 0) : -1;
+        // 32^2 level-0 tiles in single precision once there are two per tile block
+        // (HPQ_MG_T0=16/32 forces either form)
+        const int nt32 = ((L.vhi_i - L.vlo + 32) / 32) * ((L.vhi_j - L.vlo + 32) / 32);
+        const char* e32 = getenv("HPQ_MG_T0");
+        use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : (std::is_same<R, float>::value && nt32 >= 2 * std::max(coop_blocks - 1, 1)));
+        if (use32) {
+            coop_smem32 = std::max({SmoothSmem<32, 4>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
+            auto k32 = k_mg_solve<R, CELL, 32>;
+            HPQ_CUDA(cudaFuncSetAttribute(k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem32));
+            int per32 = 0;
+            HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k32, 256, coop_smem32));
+            coop_blocks32 = std::min(per32 * sms, nt32 + 1);
+            use32 = coop && per32 > 0;
+        }
     }
 
     template <bool CELL>
@@ -1325,17 +1355,20 @@ public:
         // a timeout the remaining solves of the step leave at their first barrier
         static_assert(offsetof(Ctl, mgp_bar_err) - offsetof(Ctl, mgp_rhsnorm) == 32, "Ctl layout");
         HPQ_CUDA(cudaMemsetAsync(&ctl->mgp_rhsnorm, 0, 32, st));
+        const bool t32 = use32 && !P.refine;
+        if (t32) P.split0 = 1;
         cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3(coop_blocks);
+        cfg.gridDim = dim3(t32 ? coop_blocks32 : coop_blocks);
         cfg.blockDim = dim3(256);
-        cfg.dynamicSmemBytes = coop_smem;
+        cfg.dynamicSmemBytes = t32 ? coop_smem32 : coop_smem;
         cfg.stream = st;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeCooperative;
         at[0].val.cooperative = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        HPQ_CUDA(cudaLaunchKernelEx(&cfg, k_mg_solve<R, CELL>, P));
+        void (*kern)(MGSolveArgs<R>) = t32 ? k_mg_solve<R, CELL, 32> : k_mg_solve<R, CELL, 16>;
+        HPQ_CUDA(cudaLaunchKernelEx(&cfg, kern, P));
         HPQ_LAUNCH_CHECK();
     }
     void release() {

@@ -198,6 +198,39 @@ def test_split_level0_phase_equals_merged(precision):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", [hp.PLAIN_FP64, hp.MIXED])
+def test_level0_tiles_of_32_equal_16(precision):
+    """Level-0 tiles of 32^2 (HPQ_MG_T0=32; the default for single precision on large grids)
+    sweep the same points in the same colour order as tiles of 16^2: the same fields and
+    V-cycles bit for bit with deterministic deposition, at the production tolerance 1e-4 (plain
+    FP32 V-cycles in the mixed path)."""
+    from cases import EXPLICIT_FFT, EXPLICIT_MOVING
+    for text in (EXPLICIT_MOVING, EXPLICIT_FFT):
+        text = text.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-4")
+        out, cycles = [], []
+        for t0 in ("16", "32"):
+            saved = {k: os.environ.get(k) for k in ("HPQ_MG_T0", "HPQ_MG_SPLIT")}
+            os.environ["HPQ_MG_T0"] = t0
+            os.environ["HPQ_MG_SPLIT"] = "1"
+            try:
+                g = hp.Hipace(text, precision=precision, graphs=True, deterministic=True)
+                g.init_data()
+            finally:
+                for k, v in saved.items():
+                    os.environ.pop(k, None)
+                    if v is not None:
+                        os.environ[k] = v
+            g.set_diag(["Bx", "By", "Ez"])
+            for s in range(2):
+                g.step(s)
+            out.append([g.get_diag(k) for k in ("Bx", "By", "Ez")])
+            cycles.append(g.counters()["mg_vcycles"])
+            g.close()
+        assert cycles[0] == cycles[1] > 0, cycles
+        for a, b in zip(*out):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("graphs", [False, True])
 def test_insitu_diagnostics_match_oracle(graphs):
     """In-situ beam moments and field reductions of every slice (BeamParticleContainer.cpp:476-548,
