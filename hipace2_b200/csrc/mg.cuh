@@ -216,8 +216,11 @@ struct SmoothSmem {
     static constexpr int E = T + 2 * H;
     static constexpr int Q = T + 2;
     static constexpr int EC = E / 2 + 3;  // coarse points under the loaded region (interpolation)
+    // phi (2), rhs (2), coefficient, 1/diagonal, then the coarse correction (2, read before the
+    // sweeps); the residual (2 Q^2) reuses the 1/diagonal and coarse planes after the sweeps
+    static constexpr int TAIL = (E * E + 2 * EC * EC > 2 * Q * Q) ? E * E + 2 * EC * EC : 2 * Q * Q;
     template <class R>
-    static constexpr size_t bytes() { return (size_t)(6 * E * E + 2 * Q * Q + 2 * EC * EC) * sizeof(R); }
+    static constexpr size_t bytes() { return (size_t)(5 * E * E + TAIL) * sizeof(R); }
 };
 
 // One T x T tile (tile coordinates bx, by) of the fused smoother. `swap` selects in2/out2 for
@@ -234,9 +237,10 @@ __device__ __forceinline__ void mg_smooth_tile(const SmoothArgs<R>& A, int bx, i
     R (*srh)[E * E] = reinterpret_cast<R (*)[E * E]>(smem_raw + 2 * E * E * sizeof(R));  // rhs
     R* sa = reinterpret_cast<R*>(smem_raw + 4 * E * E * sizeof(R));             // coefficient
     R* sinv = reinterpret_cast<R*>(smem_raw + 5 * E * E * sizeof(R));           // 1 / diagonal
-    R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 6 * E * E * sizeof(R));   // residual
     constexpr int EC = SM::EC;
-    R (*sc)[EC * EC] = reinterpret_cast<R (*)[EC * EC]>(smem_raw + (6 * E * E + 2 * Q * Q) * sizeof(R));  // coarse
+    R (*sc)[EC * EC] = reinterpret_cast<R (*)[EC * EC]>(smem_raw + 6 * E * E * sizeof(R));  // coarse (set-up only)
+    // residual: written after the last sweep's barrier, over the 1/diagonal and coarse planes
+    R (*sr)[Q * Q] = reinterpret_cast<R (*)[Q * Q]>(smem_raw + 5 * E * E * sizeof(R));
     const MGLev& L = A.L;
     const int t0i = L.vlo + bx * T, t0j = L.vlo + by * T;
     const int ti0 = t0i - H, tj0 = t0j - H;
@@ -1315,7 +1319,8 @@ public:
         // (HPQ_MG_T0=16/32 forces either form)
         const int nt32 = ((L.vhi_i - L.vlo + 32) / 32) * ((L.vhi_j - L.vlo + 32) / 32);
         const char* e32 = getenv("HPQ_MG_T0");
-        use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : (std::is_same<R, float>::value && nt32 >= 2 * std::max(coop_blocks - 1, 1)));
+        // (the 32^2 form is taken where it keeps the blocks per SM of the 16^2 form)
+        use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : nt32 >= 2 * std::max(coop_blocks - 1, 1));
         if (use32) {
             coop_smem32 = std::max({SmoothSmem<32, 4>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
             auto k32 = k_mg_solve<R, CELL, 32>;
@@ -1323,7 +1328,7 @@ public:
             int per32 = 0;
             HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k32, 256, coop_smem32));
             coop_blocks32 = std::min(per32 * sms, nt32 + 1);
-            use32 = coop && per32 > 0;
+            use32 = per32 > 0 && (e32 || per32 >= per);
         }
     }
 
