@@ -913,9 +913,9 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
 
 // T0: tile edge of level 0 (16, or 32 on large grids: a 4-sweep phase then loads 44^2 points per
 // 32^2 tile instead of 28^2 per 16^2, 1.6x less halo work; the sweeps give the same values). With
-// T0 = 32 level 0 always runs in the split form and without FP64 refinement.
+// T0 = 32 level 0 runs without FP64 refinement, and in double precision in the split form.
 template <class R, bool CELL, int T0 = 16>
-__global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
+__global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
     HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
     __shared__ int s_go;
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
     constexpr bool kFloat = std::is_same<R, float>::value;
     constexpr bool kRefinable = kFloat && T0 == 16;
     const bool refine = kRefinable && P.refine != 0;  // FP64 refinement of level 0 (tight tolerances)
-    const bool split = T0 != 16 || P.split0 != 0;
+    const bool split = (T0 != 16 && !kFloat) || P.split0 != 0;
     Ctl* ctl = P.ctl;
     unsigned int* bar = ctl->mgp_bar;
     int* err = &ctl->mgp_bar_err;
@@ -1114,9 +1114,9 @@ __global__ void __launch_bounds__(256) k_mg_solve(MGSolveArgs<R> P) {
                 if constexpr (kRefinable) {
                     if (refine) { mg_refine_tile<CELL, false, 8>(P, it & 1, t % ntx, t / ntx, smem_raw, bmax, brhs); done = true; }
                 }
-                if constexpr (T0 == 16) {
+                if constexpr (T0 == 16 || kFloat) {
                     if (!done)
-                        mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
+                        mg_smooth_tile<R, CELL, T0, MG_INIT_INTERP, true, true, MG_NORM_ITER, 8>(a, t % ntx, t / ntx, (it & 1) != 0, smem_raw, bmax, brhs);
                 }
             }
             block_max2(bmax, brhs);
@@ -1250,6 +1250,7 @@ public:
     bool use32 = false;                   // level-0 tiles of 32^2 (k_mg_solve<R, CELL, 32>) for unrefined solves
     int coop_blocks32 = 0;
     size_t coop_smem32 = 0;
+    bool split32 = true;                  // level 0 of the 32^2 form as two 4-sweep passes
 
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
@@ -1323,6 +1324,10 @@ public:
         use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : nt32 >= 2 * std::max(coop_blocks - 1, 1));
         if (use32) {
             coop_smem32 = std::max({SmoothSmem<32, 4>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
+            // single precision may run level 0 as one 8-sweep pass of 32^2 tiles
+            if (std::is_same<R, float>::value) coop_smem32 = std::max(coop_smem32, SmoothSmem<32, 8>::template bytes<R>());
+            const char* es32 = getenv("HPQ_MG_SPLIT");
+            split32 = std::is_same<R, float>::value ? (es32 ? es32[0] == '1' : true) : true;
             auto k32 = k_mg_solve<R, CELL, 32>;
             HPQ_CUDA(cudaFuncSetAttribute(k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem32));
             int per32 = 0;
@@ -1361,7 +1366,7 @@ public:
         static_assert(offsetof(Ctl, mgp_bar_err) - offsetof(Ctl, mgp_rhsnorm) == 32, "Ctl layout");
         HPQ_CUDA(cudaMemsetAsync(&ctl->mgp_rhsnorm, 0, 32, st));
         const bool t32 = use32 && !P.refine;
-        if (t32) P.split0 = 1;
+        if (t32) P.split0 = split32 ? 1 : 0;
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(t32 ? coop_blocks32 : coop_blocks);
         cfg.blockDim = dim3(256);
