@@ -199,6 +199,14 @@ __device__ __forceinline__ void addc(const DetAcc& d, R* base, int pitch, int i,
     atomicAdd(reinterpret_cast<unsigned long long*>(d.w[2] + e), (unsigned long long)(long long)c);
 }
 
+// addc with the mode fixed at compile time: plain floating-point atomics without deterministic
+// accumulation (no per-deposit branch)
+template <bool DET, class R>
+__device__ __forceinline__ void addd(const DetAcc& d, R* base, int pitch, int i, int j, R v) {
+    if constexpr (DET) addc(d, base, pitch, i, j, v);
+    else atomicAdd(base + (ptrdiff_t)(j + kGuardAlloc) * pitch + (i + kGuardAlloc), v);
+}
+
 // Cell-unit coordinate of a plasma position along one axis as base + t: with a reference lattice
 // coordinate (single precision) t = frac(u0) + x * dxi is a small number and the integer part
 // goes to `base`; without one, base = 0 and t = (x - off) * dxi. Clamped to [-1, n] like clamp_mid.
@@ -220,7 +228,7 @@ __device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R o
     return t;
 }
 
-template <class R>
+template <class R, bool DET>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
                                                         const int* gate, DetAcc det) {
     HPQ_PDL_ENTRY();
@@ -265,11 +273,11 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
             for (int ix = 0; ix < 3; ++ix) {
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 const R cd = q_invvol * sx[ix].s * sy[iy].s;
-                if (o.jx) { addc(det, o.jx, o.pitch, i, j, cd * vx_c); addc(det, o.jy, o.pitch, i, j, cd * vy_c); }
-                if (o.jz) addc(det, o.jz, o.pitch, i, j, cd * gpm1 * clight);
-                if (o.rho) addc(det, o.rho, o.pitch, i, j, cd * gamma_psi);
-                if (o.chi) addc(det, o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
-                if (o.rhomjz) addc(det, o.rhomjz, o.pitch, i, j, cd);
+                if (o.jx) { addd<DET>(det, o.jx, o.pitch, i, j, cd * vx_c); addd<DET>(det, o.jy, o.pitch, i, j, cd * vy_c); }
+                if (o.jz) addd<DET>(det, o.jz, o.pitch, i, j, cd * gpm1 * clight);
+                if (o.rho) addd<DET>(det, o.rho, o.pitch, i, j, cd * gamma_psi);
+                if (o.chi) addd<DET>(det, o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
+                if (o.rhomjz) addd<DET>(det, o.rhomjz, o.pitch, i, j, cd);
             }
     }
 }
@@ -277,7 +285,7 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
 // ------------------------------------------------------------------------------------------
 // Explicit Sx/Sy deposition (ExplicitDeposition.cpp:20-265, no laser)
 // ------------------------------------------------------------------------------------------
-template <class R, int DT>
+template <class R, int DT, bool DET>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
@@ -326,8 +334,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposi
                                      (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * gmy) * a_clight);
                 const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
                                      (+sxd * sys * dxi * gmx + sxs * syd * dyi * (-vx * vy)) * a_clight);
-                addc(det, Sy, S.pitch, i, j, vsy);
-                addc(det, Sx, S.pitch, i, j, vsx);
+                addd<DET>(det, Sy, S.pitch, i, j, vsy);
+                addd<DET>(det, Sx, S.pitch, i, j, vsx);
             }
         }
     }

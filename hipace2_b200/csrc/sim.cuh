@@ -969,7 +969,7 @@ public:
         for (size_t s = 0; s < pl.size(); ++s) {
             if (!pl[s].neutralize || pl[s].n == 0) continue;
             DepOut<R> o{nullptr, nullptr, nullptr, nullptr, nullptr, S.c(C_IONS).p, S.pitch};
-            hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr, det);
+            hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr, det);
             HPQ_LAUNCH_CHECK();
             det_flush({C_IONS});
         }
@@ -1026,7 +1026,7 @@ public:
         if (pl[sp].n == 0) return;
         DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
         Scope sc(this, "plasma_deposit");
-        hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det);
+        hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det);
         HPQ_LAUNCH_CHECK();
         det_flush_ptrs({jx, jy, jz, rho, chi, rhomjz});
     }
@@ -1166,9 +1166,10 @@ public:
             if (pl[s].n == 0) continue;
             Scope sc(this, "explicit_deposit");
             const int nb = blocks_for(pl[s].n, 256);
-            if (cfg.depos_derivative_type == 0) hpq_launch(k_explicit_deposit<R, 0>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-            else if (cfg.depos_derivative_type == 1) hpq_launch(k_explicit_deposit<R, 1>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-            else hpq_launch(k_explicit_deposit<R, 2>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            const bool d = det.w[0] != nullptr;
+            if (cfg.depos_derivative_type == 0) hpq_launch(d ? k_explicit_deposit<R, 0, true> : k_explicit_deposit<R, 0, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            else if (cfg.depos_derivative_type == 1) hpq_launch(d ? k_explicit_deposit<R, 1, true> : k_explicit_deposit<R, 1, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            else hpq_launch(d ? k_explicit_deposit<R, 2, true> : k_explicit_deposit<R, 2, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
             HPQ_LAUNCH_CHECK();
             det_flush({C_SX, C_SY});
         }
@@ -1860,7 +1861,7 @@ public:
                 hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, &ctl->pc_go);
                 HPQ_LAUNCH_CHECK();
                 DepOut<R> o{S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, nullptr, nullptr, S.pitch};
-                hpq_launch(k_plasma_deposit<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go, det);
+                hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go, det);
                 HPQ_LAUNCH_CHECK();
                 det_flush({C_NJX, C_NJY});
             }
