@@ -211,12 +211,11 @@ __device__ __forceinline__ void addd(const DetAcc& d, R* base, int pitch, int i,
 // coordinate (single precision) t = frac(u0) + x * dxi is a small number and the integer part
 // goes to `base`; without one, base = 0 and t = (x - off) * dxi. Clamped to [-1, n] like clamp_mid.
 template <class R>
-__device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R off, R dxi, int n, int& base) {
-    if (ref == nullptr) {
+__device__ __forceinline__ R plasma_mid_v(bool has_ref, float u0, R x, R off, R dxi, int n, int& base) {
+    if (!has_ref) {
         base = 0;
         return clamp_mid<R>((x - off) * dxi, n);
     }
-    const float u0 = ref[ip];
     const float fb = floorf(u0);
     const R t = (R)(u0 - fb) + x * dxi;
     const R tot = (R)fb + t;
@@ -226,6 +225,10 @@ __device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R o
     }
     base = (int)fb;
     return t;
+}
+template <class R>
+__device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R off, R dxi, int n, int& base) {
+    return plasma_mid_v<R>(ref != nullptr, ref ? ref[ip] : 0.f, x, off, dxi, n, base);
 }
 
 template <class R, bool DET>
@@ -239,46 +242,70 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
     const R q_mu0_mass_ratio = (R)(charge * g.mu0 / P.mass);
     const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
     const R qsa = (R)P.qsa_max;
-    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
-        if (!P.valid[ip]) continue;
-        const R psis = P.psi[ip];
-        const R psi_inv = P.ru ? R(1) / (R(1) + psis) : R(1) / psis;
-        const R vx_c = P.ux[ip] * psi_inv;
-        const R vy_c = P.uy[ip] * psi_inv;
-        const R q_invvol = charge_invvol * P.w[ip];
-        int bx, by;
-        const R xmid = plasma_mid<R>(P.ru, ip, P.x[ip], xoff, dxi, g.nx, bx);
-        const R ymid = plasma_mid<R>(P.rv, ip, P.y[ip], yoff, dyi, g.ny, by);
-        const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
-                                      vy_c * vy_c * clightinv * clightinv + R(1));
-        // gamma/psi - 1; with psi - 1 stored, (1/psi)^2 - 1 = -(psi - 1)(psi + 1)/psi^2 avoids the
-        // cancellation of two numbers close to 1
-        const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
-                                        vy_c * vy_c * clightinv * clightinv)
-                            : gamma_psi - R(1);
-        if (gamma_psi < R(0) || gamma_psi > qsa || psi_inv < R(0)) {
-            P.w[ip] = R(0);
-            P.valid[ip] = 0;
-            continue;
-        }
-        Sh<R> sx[3], sy[3];
+    // the attributes of the thread's next particle are loaded before the atomics of the current
+    // one, so that two particles' loads are in flight per thread
+    struct Pt {
+        R x, y, w, ux, uy, psi;
+        float ru, rv;
+        uint8_t v;
+    };
+    auto load = [&](long long ip) {
+        Pt q;
+        q.v = P.valid[ip];
+        q.x = P.x[ip]; q.y = P.y[ip]; q.w = P.w[ip];
+        q.ux = P.ux[ip]; q.uy = P.uy[ip]; q.psi = P.psi[ip];
+        q.ru = P.ru ? P.ru[ip] : 0.f;
+        q.rv = P.rv ? P.rv[ip] : 0.f;
+        return q;
+    };
+    const long long stride = gstride();
+    long long ip = gtid();
+    Pt cur{};
+    if (ip < P.n) cur = load(ip);
+    for (; ip < P.n; ip += stride) {
+        Pt nxt{};
+        if (ip + stride < P.n) nxt = load(ip + stride);
+        if (cur.v) {
+            const R psis = cur.psi;
+            const R psi_inv = P.ru ? R(1) / (R(1) + psis) : R(1) / psis;
+            const R vx_c = cur.ux * psi_inv;
+            const R vy_c = cur.uy * psi_inv;
+            const R q_invvol = charge_invvol * cur.w;
+            int bx, by;
+            const R xmid = plasma_mid_v<R>(P.ru != nullptr, cur.ru, cur.x, xoff, dxi, g.nx, bx);
+            const R ymid = plasma_mid_v<R>(P.rv != nullptr, cur.rv, cur.y, yoff, dyi, g.ny, by);
+            const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                          vy_c * vy_c * clightinv * clightinv + R(1));
+            // gamma/psi - 1; with psi - 1 stored, (1/psi)^2 - 1 = -(psi - 1)(psi + 1)/psi^2 avoids
+            // the cancellation of two numbers close to 1
+            const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                            vy_c * vy_c * clightinv * clightinv)
+                                : gamma_psi - R(1);
+            if (gamma_psi < R(0) || gamma_psi > qsa || psi_inv < R(0)) {
+                P.w[ip] = R(0);
+                P.valid[ip] = 0;
+            } else {
+                Sh<R> sx[3], sy[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k);
-            sx[k].cell += bx; sy[k].cell += by;
-        }
+                for (int k = 0; k < 3; ++k) {
+                    sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k);
+                    sx[k].cell += bx; sy[k].cell += by;
+                }
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
+                for (int iy = 0; iy < 3; ++iy)
 #pragma unroll
-            for (int ix = 0; ix < 3; ++ix) {
-                const int i = sx[ix].cell, j = sy[iy].cell;
-                const R cd = q_invvol * sx[ix].s * sy[iy].s;
-                if (o.jx) { addd<DET>(det, o.jx, o.pitch, i, j, cd * vx_c); addd<DET>(det, o.jy, o.pitch, i, j, cd * vy_c); }
-                if (o.jz) addd<DET>(det, o.jz, o.pitch, i, j, cd * gpm1 * clight);
-                if (o.rho) addd<DET>(det, o.rho, o.pitch, i, j, cd * gamma_psi);
-                if (o.chi) addd<DET>(det, o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
-                if (o.rhomjz) addd<DET>(det, o.rhomjz, o.pitch, i, j, cd);
+                    for (int ix = 0; ix < 3; ++ix) {
+                        const int i = sx[ix].cell, j = sy[iy].cell;
+                        const R cd = q_invvol * sx[ix].s * sy[iy].s;
+                        if (o.jx) { addd<DET>(det, o.jx, o.pitch, i, j, cd * vx_c); addd<DET>(det, o.jy, o.pitch, i, j, cd * vy_c); }
+                        if (o.jz) addd<DET>(det, o.jz, o.pitch, i, j, cd * gpm1 * clight);
+                        if (o.rho) addd<DET>(det, o.rho, o.pitch, i, j, cd * gamma_psi);
+                        if (o.chi) addd<DET>(det, o.chi, o.pitch, i, j, cd * q_mu0_mass_ratio * psi_inv);
+                        if (o.rhomjz) addd<DET>(det, o.rhomjz, o.pitch, i, j, cd);
+                    }
             }
+        }
+        cur = nxt;
     }
 }
 
