@@ -273,6 +273,7 @@ def run_ours(args):
             line["scale_point"] = scale_point(args.scale_config, torch)
     if rank == 0 and args.adjoint_config and args.precision == "fp64":
         line["adjoint"] = adjoint_point(args.adjoint_config, torch)
+        line["salame_vs_adjoint"] = salame_vs_adjoint(args.adjoint_config)
     if rank == 0:
         print(json.dumps(line))
     sim.close()
@@ -420,6 +421,70 @@ def adjoint_point(name, torch, reps=3):
             "gradient_over_plain_step": t_grad / t_step, "gradient_over_forward": t_grad / t_fwd,
             "objective": J, "max_abs_grad": scale, "fd_check": fd, "dtype": "f64",
             "timing": "wall time between device synchronisations"}
+
+
+def salame_vs_adjoint(name, iters=8):
+    """The beam-loading objective J (current-weighted variance of Ez over the witness slices) of
+    the same beams with three witness current profiles: the injected one, the one SALAME makes
+    in step 0 (witness.do_salame = 1; SALAME flattens the slice-mean Ez, and removes the witness
+    where the target cannot be reached) and the one a few projected gradient-descent steps on the
+    adjoint's witness knots reach (backtracking line search; knots kept >= 0, plasma density
+    knots fixed). All three are evaluated by the same forward of hpq_adjoint_grad on the initial
+    beam positions."""
+    import numpy as np
+    import hipace2_b200 as hp
+    from cases import config
+    text = config(name)
+    sim = hp.Hipace(text, graphs=True)
+    sim.init_data()
+    drv0, wit0 = sim.get_beam(0), sim.get_beam(1)
+    n_profile = int(_key(text, "adjoint.n_profile_knots"))
+    n_density = int(_key(text, "adjoint.n_density_knots"))
+    lo, hi = [float(v) for v in _key_all(text, "adjoint.profile_zeta")[:2]]
+    ones = np.ones(n_profile + n_density)
+    J0 = sim.adjoint(ones, grad=False)
+    # SALAME on the same beams (the adjoint keys are left out: the adjoint does not cover SALAME)
+    stext = "\n".join(l for l in text.splitlines() if not l.strip().startswith("adjoint.")) + "\nwitness.do_salame = 1\n"
+    s = hp.Hipace(stext, graphs=True)
+    s.init_data()
+    s.set_beam(0, drv0)
+    s.set_beam(1, wit0)
+    s.step(0)
+    ws, log = s.get_beam(1), s.salame_log()
+    s.close()
+    # SALAME's weights (0 for the particles it removed) on the initial positions
+    w_sal = dict(zip(ws["id"].tolist(), ws["w"].tolist()))
+    wit_s = dict(wit0)
+    wit_s["w"] = np.array([w_sal.get(i, 0.0) for i in wit0["id"].tolist()])
+    sim.set_beam(1, wit_s)
+    J_sal = sim.adjoint(ones, grad=False)
+    sim.set_beam(1, wit0)
+    # projected gradient descent on the witness knots
+    theta, J, hist, lr = ones.copy(), J0, [J0], None
+    for _ in range(iters):
+        J, g = sim.adjoint(theta)
+        g[n_profile:] = 0.0
+        if lr is None:
+            lr = 0.25 / max(float(np.abs(g).max()), 1e-300)
+        for _try in range(6):
+            t = np.maximum(theta - lr * g, 0.0)
+            Jt = sim.adjoint(t, grad=False)
+            if Jt < J:
+                theta, J, lr = t, Jt, lr * 1.5
+                break
+            lr *= 0.5
+        hist.append(J)
+    knots_z = np.linspace(lo, hi, n_profile)
+    prof = np.where((wit0["z"] >= lo) & (wit0["z"] <= hi), np.interp(wit0["z"], knots_z, theta[:n_profile]), 0.0)
+    sim.close()
+    return {"workload": name, "objective": "J = S2/S0 - (S1/S0)^2, S_n = sum jz_beam Ez^n over adjoint.objective_zeta",
+            "J_injected": J0, "J_salame": J_sal, "J_adjoint_descent": hist,
+            "descent_steps": iters, "salame_iterations": int(log.shape[0]),
+            "salame_slices": int(np.unique(log[:, 0]).size) if log.size else 0,
+            # slices whose witness SALAME removed (W = 0)
+            "salame_overloaded_slices": int(np.unique(log[log[:, 2] == 0, 0]).size) if log.size else 0,
+            "witness_charge_ratio_salame": float(wit_s["w"].sum() / wit0["w"].sum()),
+            "witness_charge_ratio_adjoint": float((wit0["w"] * prof).sum() / wit0["w"].sum())}
 
 
 def _key(text, key):

@@ -900,9 +900,18 @@ public:
         for (int c : cnt) n += c;
         return n;
     }
-    // particles of the current store in slice-descending order
+    // particles of the current store in slice-descending order; invalid particles (absorbed at a
+    // boundary, removed by SALAME) are reported with weight 0, which hpq_set_beam reads back as
+    // invalid
+    std::vector<uint8_t> valid_h;
     void get_beam(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
                   long long* id) override {
+        get_beam_raw(b, x, y, z, w, ux, uy, uz, id);
+        for (long long k = 0; k < (long long)valid_h.size(); ++k)
+            if (!valid_h[k]) w[k] = 0.0;
+    }
+    void get_beam_raw(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
+                      long long* id) {
         HPQ_CUDA(cudaStreamSynchronize(st));
         BeamDev& d = bm[b];
         std::vector<int> cnt(nz), start(nz);
@@ -918,12 +927,14 @@ public:
             if (cnt[sl] && start[sl] != start[nz - 1] + total) contiguous = false;
             total += cnt[sl];
         }
+        valid_h.resize(total);
         if (contiguous) {
             if (total > 0) {
                 const size_t o = start[nz - 1];
                 for (int a = 0; a < 7; ++a)
                     HPQ_CUDA(cudaMemcpyAsync(outs[a], ins[a] + o, total * sizeof(double), cudaMemcpyDeviceToHost, st));
                 if (id) HPQ_CUDA(cudaMemcpyAsync(id, s.id + o, total * sizeof(long long), cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaMemcpyAsync(valid_h.data(), s.valid + o, total, cudaMemcpyDeviceToHost, st));
                 HPQ_CUDA(cudaStreamSynchronize(st));
             }
             return;
@@ -934,6 +945,7 @@ public:
             if (!n) continue;
             for (int a = 0; a < 7; ++a) HPQ_CUDA(cudaMemcpy(outs[a] + k, ins[a] + o, n * sizeof(double), cudaMemcpyDeviceToHost));
             if (id) HPQ_CUDA(cudaMemcpy(id + k, s.id + o, n * sizeof(long long), cudaMemcpyDeviceToHost));
+            HPQ_CUDA(cudaMemcpy(valid_h.data() + k, s.valid + o, n, cudaMemcpyDeviceToHost));
             k += n;
         }
     }

@@ -77,7 +77,9 @@ int hpq_set_beam(hpq_handle* h, int beam, const double* x, const double* y, cons
                  const int64_t* id, int64_t n);
 /* Name of beam `beam` (beams.names order), or NULL past the last beam. */
 const char* hpq_beam_name(const hpq_handle* h, int beam);
-/* Number of stored particles of a beam and a copy of them (slices from head to tail). */
+/* Number of stored particles of a beam and a copy of them (slices from head to tail). Invalid
+ * particles (absorbed at a boundary, removed by SALAME) are reported with weight 0; hpq_set_beam
+ * treats weight-0 particles as invalid, so the two round-trip. */
 int hpq_beam_count(hpq_handle* h, int beam, int64_t* n);
 int hpq_get_beam(hpq_handle* h, int beam, double* x, double* y, double* z, double* w,
                  double* ux, double* uy, double* uz, int64_t* id);

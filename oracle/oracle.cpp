@@ -2111,7 +2111,8 @@ int oracle_get_beam(OracleHandle* h, int b, double* x, double* y, double* z, dou
     int64_t k = 0;
     for (int sl = s.nz - 1; sl >= 0; --sl)
         for (auto& p : s.store[b][sl].p) {
-            x[k] = p.x; y[k] = p.y; z[k] = p.z; w[k] = p.w; ux[k] = p.ux; uy[k] = p.uy; uz[k] = p.uz;
+            // invalid particles are reported with weight 0 (as hpq_get_beam does)
+            x[k] = p.x; y[k] = p.y; z[k] = p.z; w[k] = p.valid ? p.w : 0.0; ux[k] = p.ux; uy[k] = p.uy; uz[k] = p.uz;
             if (id) id[k] = p.id;
             ++k;
         }

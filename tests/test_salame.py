@@ -115,7 +115,7 @@ def test_oracle_overloaded_witness_is_removed():
     assert all(W == 0 for s, _, W in log if s <= first_zero)
     b = o.get_beam(1)
     slices = np.floor((b["z"] + 8.0) / 0.3).astype(int)
-    assert np.all(b["w"][slices < first_zero] == 5e-4)  # invalid particles keep their weight
+    assert np.all(b["w"][slices < first_zero] == 0)  # invalid particles are reported with weight 0
 
 
 def test_salame_input_checks():
