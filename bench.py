@@ -204,7 +204,7 @@ def run_ours(args):
     sim.synchronize()
     e2e_secs = time.perf_counter() - t0
     h2d = nb * (7 * 8 + 8)
-    d2h = out["x"].size * (7 * 8 + 8)
+    d2h = out["x"].size * (7 * 8 + 8 + 1)  # 7 attributes, id, validity flag
     # ---- profiled pass (kernel launches with events) for the roofline of the dominant kernel
     sim.set_profiling(True)
     for s in range(w + 2 * k, w + 3 * k):
