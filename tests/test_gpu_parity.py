@@ -200,8 +200,8 @@ def test_split_level0_phase_equals_merged(precision):
 
 @pytest.mark.parametrize("precision", [hp.PLAIN_FP64, hp.MIXED])
 def test_level0_tiles_of_32_equal_16(precision):
-    """Level-0 tiles of 32^2 (HPQ_MG_T0=32; the default for single precision on large grids)
-    sweep the same points in the same colour order as tiles of 16^2: the same fields and
+    """Level-0 (and level-1) tiles of 32^2 (HPQ_MG_T0=32, HPQ_MG_L1=32; the default on large
+    grids) sweep the same points in the same colour order as tiles of 16^2: the same fields and
     V-cycles bit for bit with deterministic deposition, at the production tolerance 1e-4 (plain
     FP32 V-cycles in the mixed path)."""
     from cases import EXPLICIT_FFT, EXPLICIT_MOVING
@@ -211,9 +211,10 @@ def test_level0_tiles_of_32_equal_16(precision):
         # (the 8-sweep single pass of 32^2 tiles exists in single precision only)
         forms = [("16", "1"), ("32", "1")] + ([("32", "0")] if precision == hp.MIXED else [])
         for t0, split in forms:
-            saved = {k: os.environ.get(k) for k in ("HPQ_MG_T0", "HPQ_MG_SPLIT")}
+            saved = {k: os.environ.get(k) for k in ("HPQ_MG_T0", "HPQ_MG_SPLIT", "HPQ_MG_L1")}
             os.environ["HPQ_MG_T0"] = t0
             os.environ["HPQ_MG_SPLIT"] = split
+            os.environ["HPQ_MG_L1"] = t0  # level 1 in tiles of the same size
             try:
                 g = hp.Hipace(text, precision=precision, graphs=True, deterministic=True)
                 g.init_data()
