@@ -623,8 +623,8 @@ struct MGSolveArgs {
     unsigned long long* trace;
     // single precision: 1 = level 0 with FP64 iterative refinement, 0 = plain FP32 V-cycles
     int refine;
-    // 32^2 form: level 1 in 32^2 tiles as well
-    int l1_32;
+    // 32^2 form: bit l set = level l >= 1 in 32^2 tiles as well
+    unsigned int l32_mask;
     // level 0 of a V-cycle as two phases of 4 sweeps (interpolation + up-sweeps, then the next
     // down-sweeps + residual) instead of one phase of 8: each 16^2 tile then sweeps a 28^2
     // region 4 + 4 times instead of a 36^2 region 8 times (40 % fewer point updates, one more
@@ -953,11 +953,12 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
     // go to the other blocks
     const int tb = (nb > 1) ? (int)blockIdx.x - 1 : 0, ntb = (nb > 1) ? nb - 1 : 1;
     const bool tile_block = (nb == 1) || blockIdx.x > 0;
-    // level 1 also takes 32^2 tiles in the 32^2 form when there are enough of them (P.l1_32)
-    const bool l1_32 = T0 == 32 && P.l1_32 != 0;
+    // levels >= 1 also take 32^2 tiles in the 32^2 form where there are enough of them
+    // (bit l of P.l32_mask)
+    auto big = [&](int l) { return T0 == 32 && ((P.l32_mask >> l) & 1u) != 0; };
     auto ntiles = [&](int l, int& ntx) {
         const MGLev& L = P.lev[l];
-        const int T = l == 0 ? T0 : (l == 1 && l1_32) ? 32 : 16;
+        const int T = l == 0 ? T0 : big(l) ? 32 : 16;
         ntx = (L.vhi_i - L.vlo + T) / T;
         return ntx * ((L.vhi_j - L.vlo + T) / T);
     };
@@ -1016,7 +1017,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             const int nt = ntiles(l, ntx);
             bool done = false;
             if constexpr (T0 == 32) {
-                if (l == 1 && l1_32) {
+                if (big(l)) {
                     for (int t = tb; tile_block && t < nt; t += ntb)
                         mg_smooth_tile<R, CELL, 32, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                     done = true;
@@ -1047,7 +1048,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             const int nt = ntiles(l, ntx);
             bool done = false;
             if constexpr (T0 == 32) {
-                if (l == 1 && l1_32) {
+                if (big(l)) {
                     for (int t = tb; tile_block && t < nt; t += ntb)
                         mg_smooth_tile<R, CELL, 32, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                     done = true;
@@ -1273,7 +1274,7 @@ public:
     int coop_blocks32 = 0;
     size_t coop_smem32 = 0;
     bool split32 = true;                  // level 0 of the 32^2 form as two 4-sweep passes
-    bool l1_32 = false;                   // level 1 of the 32^2 form in 32^2 tiles too
+    unsigned int l32_mask = 0;            // levels >= 1 of the 32^2 form in 32^2 tiles too (bit l)
 
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
@@ -1357,13 +1358,15 @@ public:
             HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k32, 256, coop_smem32));
             coop_blocks32 = std::min(per32 * sms, nt32 + 1);
             use32 = per32 > 0 && (e32 || per32 >= per);
-            // level 1 in 32^2 tiles once they occupy at least half of the tile blocks
-            // (HPQ_MG_L1=16/32 forces either)
-            if (nl > 1) {
-                const MGLev& L1 = lev[1];
-                const int nt1 = ((L1.vhi_i - L1.vlo + 32) / 32) * ((L1.vhi_j - L1.vlo + 32) / 32);
-                const char* el1 = getenv("HPQ_MG_L1");
-                l1_32 = el1 ? std::atoi(el1) == 32 : 2 * nt1 >= coop_blocks32 - 1;
+            // levels >= 1 in 32^2 tiles once they occupy at least half of the tile blocks
+            // (HPQ_MG_L1=16/32 forces either form on level 1)
+            l32_mask = 0;
+            const char* el1 = getenv("HPQ_MG_L1");
+            for (int l = 1; l < std::min(sb, 32); ++l) {
+                const MGLev& Ll = lev[l];
+                const int ntl = ((Ll.vhi_i - Ll.vlo + 32) / 32) * ((Ll.vhi_j - Ll.vlo + 32) / 32);
+                const bool on = (l == 1 && el1) ? std::atoi(el1) == 32 : 2 * ntl >= coop_blocks32 - 1;
+                if (on) l32_mask |= 1u << l;
             }
         }
     }
@@ -1398,7 +1401,7 @@ public:
         HPQ_CUDA(cudaMemsetAsync(&ctl->mgp_rhsnorm, 0, 32, st));
         const bool t32 = use32 && !P.refine;
         if (t32) P.split0 = split32 ? 1 : 0;
-        P.l1_32 = (t32 && l1_32) ? 1 : 0;
+        P.l32_mask = t32 ? l32_mask : 0u;
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(t32 ? coop_blocks32 : coop_blocks);
         cfg.blockDim = dim3(256);
