@@ -374,6 +374,8 @@ public:
         S.base = nullptr;
         if (SB.base) cudaFree(SB.base);
         SB.base = nullptr;
+        if (quad) cudaFree(quad);
+        quad = nullptr;
         if (bin_key) cudaFree(bin_key);
         if (bin_hist) cudaFree(bin_hist);
         if (bin_total) cudaFree(bin_total);
@@ -471,6 +473,7 @@ public:
         HPQ_CUDA(cudaMemset(S.base, 0, S.cstride * ncomp_alloc * sizeof(R)));
         SB = S;
         HPQ_CUDA(cudaMalloc(&SB.base, S.cstride * (C_PSI + 1) * sizeof(R)));
+        if (cfg.explicit_solver) HPQ_CUDA(cudaMalloc(&quad, S.cstride * sizeof(Quad<R>)));
         HPQ_CUDA(cudaMemset(SB.base, 0, S.cstride * (C_PSI + 1) * sizeof(R)));
         dst.init(nx, ny, g.dx[0], g.dx[1], 3);
         if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
@@ -1172,16 +1175,25 @@ public:
         HPQ_LAUNCH_CHECK();
     }
 
-    // ExplicitDeposition (ExplicitDeposition.cpp:20-265): Sx, Sy += the plasma contribution
+    // ExplicitDeposition (ExplicitDeposition.cpp:20-265): Sx, Sy += the plasma contribution;
+    // the four fields it gathers are first packed cell by cell (Quad)
+    Quad<R>* quad = nullptr;
     void explicit_deposit() {
+        bool packed = false;
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "explicit_deposit");
+            if (!packed) {
+                hpq_launch(k_pack_explicit<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 8)), dim3(256), 0, st, S, quad);
+                HPQ_LAUNCH_CHECK();
+                packed = true;
+            }
             const int nb = blocks_for(pl[s].n, 256);
             const bool d = det.w[0] != nullptr;
-            if (cfg.depos_derivative_type == 0) hpq_launch(d ? k_explicit_deposit<R, 0, true> : k_explicit_deposit<R, 0, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-            else if (cfg.depos_derivative_type == 1) hpq_launch(d ? k_explicit_deposit<R, 1, true> : k_explicit_deposit<R, 1, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
-            else hpq_launch(d ? k_explicit_deposit<R, 2, true> : k_explicit_deposit<R, 2, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, det);
+            const Quad<R>* q = quad;
+            if (cfg.depos_derivative_type == 0) hpq_launch(d ? k_explicit_deposit<R, 0, true> : k_explicit_deposit<R, 0, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
+            else if (cfg.depos_derivative_type == 1) hpq_launch(d ? k_explicit_deposit<R, 1, true> : k_explicit_deposit<R, 1, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
+            else hpq_launch(d ? k_explicit_deposit<R, 2, true> : k_explicit_deposit<R, 2, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
             HPQ_LAUNCH_CHECK();
             det_flush({C_SX, C_SY});
         }
