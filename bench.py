@@ -64,6 +64,14 @@ def parse():
     return p.parse_args()
 
 
+def job_rate(local_secs, units_per_rank, world, reduce_max):
+    """Whole-job throughput of `world` independent replicas: the units of all ranks over the
+    slowest rank's time (reduce_max takes the maximum over ranks; every rank must call it).
+    Returns (units per second, that time)."""
+    secs = reduce_max(local_secs)
+    return units_per_rank * world / secs, secs
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -179,13 +187,16 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         secs = time_device_steps(sim, w, k, torch)
     launches_in_timed = sim.counters()["kernel_launches"] - l_before
-    if world > 1:
+
+    def reduce_max(x):
+        if world == 1:
+            return x
         import torch.distributed as dist
-        t = torch.tensor([secs], device="cuda")
+        t = torch.tensor([x], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
-    slices = nz * k * world
-    value = slices / secs
+        return float(t.item())
+
+    value, secs = job_rate(secs, nz * k, world, reduce_max)
     # ---- end to end through the C ABI with host buffers (pinned host copies every step)
     beam = sim.get_beam(0)
     nb = beam["x"].size
@@ -202,7 +213,7 @@ def run_ours(args):
         sim.step(s)
         out = sim.get_beam(0, out=res_host)
     sim.synchronize()
-    e2e_secs = time.perf_counter() - t0
+    e2e_value, _ = job_rate(time.perf_counter() - t0, nz * k, world, reduce_max)
     h2d = nb * (7 * 8 + 8)
     d2h = out["x"].size * (7 * 8 + 8 + 1)  # 7 attributes, id, validity flag
     # ---- profiled pass (kernel launches with events) for the roofline of the dominant kernel
@@ -245,7 +256,7 @@ def run_ours(args):
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 per step (beam store)",
                    "graphs": not args.no_graphs},
         "particle_updates_per_s": n_plasma * nz * k * world / secs,
-        "e2e": {"value": nz * k / e2e_secs, "unit": "slices/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": e2e_value, "unit": "slices/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": None,
         "roofline": {"bound": "hbm", "kernel": "k_mg_solve", "achieved": mg_achieved, "peak": peak,
