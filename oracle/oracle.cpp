@@ -2144,6 +2144,28 @@ int oracle_begin_step(OracleHandle* h, int step) { h->sim->begin_step(step); ret
 int oracle_solve_slice(OracleHandle* h, int islice, int step) { h->sim->solve_one_slice(islice, step); return h->sim->mg_status; }
 int oracle_end_step(OracleHandle* h) { h->sim->end_step(); return 0; }
 double oracle_time(OracleHandle* h) { return h->sim->physical_time; }
+// The Dirichlet Poisson solve of the slice loop on its own, Lap(u) = f on an nx x ny grid (x
+// fastest) with u = 0 one cell outside, by the sine transform of PoissonDST (known-answer tests)
+int oracle_poisson_dirichlet(const double* f, double* u, int nx, int ny, double dx, double dy) {
+    if (nx < 1 || ny < 1) return 1;
+    oracle::PoissonDST d;
+    d.init(nx, ny, dx, dy);
+    std::vector<double> v(f, f + (size_t)nx * ny);
+    d.solve(v);
+    std::copy(v.begin(), v.end(), u);
+    return 0;
+}
+// DST-I of length n as used by the solver: out_k = sum_i 2 sin(pi (i+1)(k+1) / (n+1)) in_i
+int oracle_dst1(const double* in, double* out, int n) {
+    if (n < 1) return 1;
+    oracle::PoissonDST d;
+    d.init(n, 1, 1.0, 1.0);
+    std::vector<double> v(in, in + n);
+    d.transform_x(v);
+    std::copy(v.begin(), v.end(), out);
+    return 0;
+}
+
 // SALAME record: (slice, iteration, weight factor) triples; returns the number of doubles
 long long oracle_salame_log(OracleHandle* h, double* out) {
     const auto& v = h->sim->salame_log;

@@ -51,6 +51,10 @@ def lib():
         L.oracle_end_step.argtypes = [vp]
         L.oracle_time.argtypes = [vp]
         L.oracle_time.restype = ctypes.c_double
+        L.oracle_poisson_dirichlet.argtypes = [dp, dp, i32, i32, ctypes.c_double, ctypes.c_double]
+        L.oracle_poisson_dirichlet.restype = i32
+        L.oracle_dst1.argtypes = [dp, dp, i32]
+        L.oracle_dst1.restype = i32
         L.oracle_salame_log.argtypes = [vp, dp]
         L.oracle_salame_log.restype = ctypes.c_longlong
         L.oracle_get_field.argtypes = [vp, cp, dp]
