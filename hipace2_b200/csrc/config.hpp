@@ -221,6 +221,13 @@ inline bool query_alt_arr(const InputStore& in, const std::string& name, const s
 inline void reject(const InputStore& in, const std::string& key, const std::string& why) {
     if (in.contains(key)) throw InputError("input '" + key + "' is not supported: " + why);
 }
+// a species key that the reference also reads under the shared prefix (queryWithParserAlt):
+// <species>.key and <alt>.key are both rejected
+inline void reject_alt(const InputStore& in, const std::string& name, const std::string& alt,
+                       const std::string& key, const std::string& why) {
+    reject(in, name + "." + key, why);
+    reject(in, alt + "." + key, why);
+}
 }  // namespace detail
 
 inline SimConfig build_config(const InputStore& in) {
@@ -346,7 +353,15 @@ inline SimConfig build_config(const InputStore& in) {
         if (p.charge == 0) throw InputError("The plasma particle charge must be specified");
         reject(in, name + ".can_ionize", "ionization is outside the slice loop");
         reject(in, name + ".ionization_product", "ionization is outside the slice loop");
-        reject(in, name + ".fine_ppc", "fine plasma patches need mesh refinement");
+        reject_alt(in, name, "plasmas", "fine_ppc", "fine plasma patches need mesh refinement");
+        reject_alt(in, name, "plasmas", "fine_patch(x,y)", "fine plasma patches need mesh refinement");
+        reject_alt(in, name, "plasmas", "fine_transition_cells", "fine plasma patches need mesh refinement");
+        reject_alt(in, name, "plasmas", "do_symmetrize", "symmetrized plasma loading is not implemented");
+        {
+            int period = 0;
+            if (query_alt(in, name, "plasmas", "insitu_period", period) && period != 0)
+                throw InputError("input '" + name + ".insitu_period' is not supported: plasma in-situ diagnostics are not implemented");
+        }
         reject(in, name + ".density_table_file", "density tables are not implemented");
         reject(in, name + ".temperature_in_ev", "use u_std instead");
         int ion_lev = -1;
@@ -396,10 +411,10 @@ inline SimConfig build_config(const InputStore& in) {
         query_alt(in, name, "beams", "insitu_period", b.insitu_period);
         query_alt(in, name, "beams", "insitu_radius", b.insitu_radius);
         in.query_bool(name + ".do_salame", b.do_salame);
-        reject(in, name + ".do_spin_tracking", "spin tracking is outside the slice loop");
-        reject(in, name + ".do_radiation_reaction", "radiation reaction is outside the slice loop");
-        reject(in, name + ".external_E(x,y,z,t)", "external fields are not implemented");
-        reject(in, name + ".external_B(x,y,z,t)", "external fields are not implemented");
+        reject_alt(in, name, "beams", "do_spin_tracking", "spin tracking is outside the slice loop");
+        reject_alt(in, name, "beams", "do_radiation_reaction", "radiation reaction is outside the slice loop");
+        reject_alt(in, name, "beams", "external_E(x,y,z,t)", "external fields are not implemented");
+        reject_alt(in, name, "beams", "external_B(x,y,z,t)", "external fields are not implemented");
         if (inj != "fixed_weight_pdf") {
             in.query_arr(name + ".u_mean", b.u_mean);
             in.query_arr(name + ".u_std", b.u_std);

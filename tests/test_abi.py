@@ -61,3 +61,20 @@ def test_queries_without_gpu():
     assert L.hpq_diag_count(sim.h, ctypes.byref(n)) == 0 and n.value == nz * nx
     assert L.hpq_beam_name(sim.h, 0) == b"beam" and L.hpq_beam_name(sim.h, 1) is None
     assert sim.time() == 0.0
+
+
+def test_shared_prefix_keys_of_unbuilt_features_are_rejected():
+    """Keys the reference also reads under beams.* / plasmas.* (queryWithParserAlt) for features
+    this build does not have are errors, not silently ignored."""
+    from cases import golden_input
+    base = golden_input("linear_wake.normalized.1Rank")
+    for extra, word in (("beams.external_E(x,y,z,t) = .5*x .5*y 0.", "external"),
+                        ("beams.external_B(x,y,z,t) = 0. 0. 1.", "external"),
+                        ("beams.do_radiation_reaction = 1", "radiation"),
+                        ("plasmas.insitu_period = 5", "in-situ"),
+                        ("plasma.do_symmetrize = 1", "symmetrized"),
+                        ("plasmas.fine_ppc = 2 2", "mesh refinement")):
+        with pytest.raises(hp.HpqError) as e:
+            hp.Hipace(base + "\n" + extra + "\n")
+        assert word in str(e.value), (extra, str(e.value))
+    hp.Hipace(base + "\nplasmas.insitu_period = 0\n")  # switched off: accepted
