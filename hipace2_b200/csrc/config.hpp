@@ -326,6 +326,11 @@ inline SimConfig build_config(const InputStore& in) {
     reject(in, "lasers.names", "laser envelope solver is outside the slice loop");
     reject(in, "hipace.collisions", "collisions are outside the slice loop");
     reject(in, "hipace.use_amrex_mlmg", "the AMReX MLMG path is not part of this build");
+    {
+        bool individual = false;
+        if (in.query_bool("hipace.deposit_rho_individual", individual) && individual)
+            throw InputError("input 'hipace.deposit_rho_individual' is not supported: per-species rho diagnostics are not implemented");
+    }
     reject(in, "fields.do_symmetrize", "field symmetrization is not implemented");
     bool bb = false;
     if (in.query_bool("hipace.interpolate_neutralizing_background", bb) && bb)

@@ -73,7 +73,8 @@ def test_shared_prefix_keys_of_unbuilt_features_are_rejected():
                         ("beams.do_radiation_reaction = 1", "radiation"),
                         ("plasmas.insitu_period = 5", "in-situ"),
                         ("plasma.do_symmetrize = 1", "symmetrized"),
-                        ("plasmas.fine_ppc = 2 2", "mesh refinement")):
+                        ("plasmas.fine_ppc = 2 2", "mesh refinement"),
+                        ("hipace.deposit_rho_individual = 1", "per-species")):
         with pytest.raises(hp.HpqError) as e:
             hp.Hipace(base + "\n" + extra + "\n")
         assert word in str(e.value), (extra, str(e.value))
