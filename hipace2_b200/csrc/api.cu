@@ -130,6 +130,13 @@ int hpq_set_precision(hpq_handle* h, int mode) {
 }
 
 int hpq_init(hpq_handle* h) {
+    if (h)
+        for (const auto& b : h->cfg.beams)
+            if (b.use_external) {
+                h->err = "input '" + b.name + ".external_E/B(x,y,z,t)' is not supported: external beam fields "
+                         "are implemented in the CPU restatement only";
+                return HPQ_ERR_INPUT;
+            }
     return guarded(h, [&] {
         if (h->initialised) { h->err = "hpq_init called twice"; return (int)HPQ_ERR_STATE; }
         if (h->precision == HPQ_MIXED) h->sim.reset(new hpq::Sim<float>(h->cfg));

@@ -58,6 +58,10 @@ struct BeamSpecies {
     double density = 0;              // peak density (fixed_ppc: profile density)
     double zmin = -1e300, zmax = 1e300, radius = 1e300;
     bool do_salame = false;          // <beam>.do_salame (BeamParticleContainer.cpp:66)
+    // external fields of the beam push, Ex Ey Ez Bx By Bz as functions of (x, y, z, t)
+    // (<beam>.external_E/B(x,y,z,t), BeamParticleContainer.cpp:72-86; CPU restatement only)
+    bool use_external = false;
+    Expr external[6];
     double position_mean[3] = {0, 0, 0};
     double position_std[3] = {0, 0, 0};
     int ppc[3] = {1, 1, 1};
@@ -418,8 +422,15 @@ inline SimConfig build_config(const InputStore& in) {
         in.query_bool(name + ".do_salame", b.do_salame);
         reject_alt(in, name, "beams", "do_spin_tracking", "spin tracking is outside the slice loop");
         reject_alt(in, name, "beams", "do_radiation_reaction", "radiation reaction is outside the slice loop");
-        reject_alt(in, name, "beams", "external_E(x,y,z,t)", "external fields are not implemented");
-        reject_alt(in, name, "beams", "external_B(x,y,z,t)", "external fields are not implemented");
+        for (int f = 0; f < 2; ++f) {
+            const std::string key = f == 0 ? "external_E(x,y,z,t)" : "external_B(x,y,z,t)";
+            std::vector<std::string> e = in.query_strs(name + "." + key);
+            if (e.empty()) e = in.query_strs("beams." + key);
+            if (!e.empty() && e.size() != 3) throw InputError(name + "." + key + " expects 3 expressions");
+            for (int d = 0; d < 3; ++d)
+                b.external[3 * f + d] = in.function(e.empty() ? std::string("0") : e[d], {"x", "y", "z", "t"});
+            if (!e.empty()) b.use_external = true;
+        }
         if (inj != "fixed_weight_pdf") {
             in.query_arr(name + ".u_mean", b.u_mean);
             in.query_arr(name + ".u_std", b.u_std);

@@ -1027,6 +1027,18 @@ public:
                 if (!enforce_bc(xp, yp, ux, uy)) { absorbed = true; break; }
                 double ExmBy = 0, EypBx = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
                 gather(xp, yp, ExmBy, EypBx, Ez, Bx, By, Bz);
+                if (B.use_external) {
+                    // ApplyExternalField (ExternalFields.H:29-56), at the step's start time
+                    const double a[4] = {xp, yp, zp, physical_time};
+                    double f[6];
+                    for (int k = 0; k < 6; ++k) f[k] = B.external[k].eval(a);
+                    ExmBy += f[0] - clight * f[4];
+                    EypBx += f[1] + clight * f[3];
+                    Ez += f[2];
+                    Bx += f[3];
+                    By += f[4];
+                    Bz += f[5];
+                }
                 const double ux_next = ux + dtb * cmr * (ExmBy + (clight - uz * gammap_inv) * By + uy * gammap_inv * Bz);
                 const double uy_next = uy + dtb * cmr * (EypBx + (uz * gammap_inv - clight) * Bx - ux * gammap_inv * Bz);
                 const double uxi = (ux_next + ux) * 0.5, uyi = (uy_next + uy) * 0.5;

@@ -40,6 +40,15 @@ CASES = {
          "geometry.prob_lo     = -10.   -10.   -6", "geometry.prob_hi     =  10.    10.    6",
          "diagnostic.field_data = all rho"],
         1e-12, []),
+    # 20 steps of a beam in vacuum focused by an external field: pins the beam push (the
+    # beam checksums are of the beam entering step 20, as the reference writes them)
+    "beam_evolution.1Rank": (
+        "examples/beam_in_vacuum/inputs_normalized",
+        ["hipace.tile_size = 8", "amr.n_cell = 32 32 10", "max_step = 20", "geometry.prob_lo = -2. -2. -2.",
+         "geometry.prob_hi =  2.  2.  2.", "hipace.dt = 3.", "diagnostic.output_period = 20",
+         "beam.density = 1.e-8", "beam.radius = 1.", "beam.ppc = 4 4 1",
+         "beams.external_E(x,y,z,t) = .5*x .5*y 0."],
+        1e-12, []),
     # 1023^2 x 1000 slices, fixed_weight_pdf Gaussian beam of 10.5M particles, xz diagnostic
     "transverse_benchmark.1Rank": (
         "examples/benchmarks/inputs_transverse_benchmark",
@@ -47,6 +56,10 @@ CASES = {
         1e-11, []),
 }
 STATISTICAL = {"transverse_benchmark.1Rank"}
+# external beam fields exist in the CPU restatement only (the library rejects them)
+ORACLE_ONLY = {"beam_evolution.1Rank"}
+# cases whose beam checksums are of the beam after this many steps (else the injected beam)
+BEAM_AFTER_STEPS = {"beam_evolution.1Rank": 20}
 
 
 def main(ref):
@@ -71,6 +84,8 @@ def main(ref):
             "beam": gold.get("beam", {}),
             "rtol_cpu": rtol,
             "statistical": name in STATISTICAL,
+            "oracle_only": name in ORACLE_ONLY,
+            "beam_after_steps": BEAM_AFTER_STEPS.get(name, 0),
         }
     with open(os.path.join(HERE, "golden_cases.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

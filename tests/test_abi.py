@@ -68,9 +68,7 @@ def test_shared_prefix_keys_of_unbuilt_features_are_rejected():
     this build does not have are errors, not silently ignored."""
     from cases import golden_input
     base = golden_input("linear_wake.normalized.1Rank")
-    for extra, word in (("beams.external_E(x,y,z,t) = .5*x .5*y 0.", "external"),
-                        ("beams.external_B(x,y,z,t) = 0. 0. 1.", "external"),
-                        ("beams.do_radiation_reaction = 1", "radiation"),
+    for extra, word in (("beams.do_radiation_reaction = 1", "radiation"),
                         ("plasmas.insitu_period = 5", "in-situ"),
                         ("plasma.do_symmetrize = 1", "symmetrized"),
                         ("plasmas.fine_ppc = 2 2", "mesh refinement"),
@@ -79,3 +77,10 @@ def test_shared_prefix_keys_of_unbuilt_features_are_rejected():
             hp.Hipace(base + "\n" + extra + "\n")
         assert word in str(e.value), (extra, str(e.value))
     hp.Hipace(base + "\nplasmas.insitu_period = 0\n")  # switched off: accepted
+    # external beam fields exist in the CPU restatement only: the library refuses them at init,
+    # before it touches the GPU
+    for extra in ("beams.external_E(x,y,z,t) = .5*x .5*y 0.", "beam.external_B(x,y,z,t) = 0. 0. 1."):
+        sim = hp.Hipace(base + "\n" + extra + "\n")
+        with pytest.raises(hp.HpqError) as e:
+            sim.init_data()
+        assert e.value.code == 1 and "CPU restatement" in str(e.value)

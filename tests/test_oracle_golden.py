@@ -45,9 +45,12 @@ def test_field_checksums(name):
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_beam_checksums(name):
+    """The injected beam, or the beam entering step n for cases written after n steps."""
     case = CASES[name]
     o = Oracle(case["input"])
     o.init_beams()
+    for s in range(case.get("beam_after_steps", 0)):
+        assert o.step(s) == 0
     b = o.get_beam(0)
     gold = case["beam"]
     assert len(b["x"]) == gold["charge"]          # sum |q| with q = -1 per particle
