@@ -130,6 +130,11 @@ int hpq_set_precision(hpq_handle* h, int mode) {
 }
 
 int hpq_init(hpq_handle* h) {
+    if (h && h->cfg.depos_order_xy != 2) {
+        h->err = "hipace.depos_order_xy = " + std::to_string(h->cfg.depos_order_xy) +
+                 " is not supported: the library deposits and gathers with order 2";
+        return HPQ_ERR_INPUT;
+    }
     if (h)
         for (const auto& b : h->cfg.beams)
             if (b.use_external) {

@@ -296,7 +296,9 @@ inline SimConfig build_config(const InputStore& in) {
     if (in.query("random_seed", c.random_seed)) c.has_random_seed = true;
 
     in.query("hipace.depos_order_xy", c.depos_order_xy);
-    if (c.depos_order_xy != 2)
+    // order 2 throughout; order 0 exists for the beam deposition of the CPU restatement only
+    // (the library refuses it at hpq_init)
+    if (c.depos_order_xy != 2 && c.depos_order_xy != 0)
         throw InputError("hipace.depos_order_xy = " + std::to_string(c.depos_order_xy) +
                          " is not supported (only 2)");
     int dz_order = 0;

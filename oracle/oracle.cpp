@@ -528,6 +528,11 @@ public:
     std::vector<double> pc_errors;
 
     explicit Sim(const SimConfig& c) : cfg(c) {
+        // deposition order 0 is restated for the beam deposition of a beam that does not move
+        // (BeamDepositCurrent.cpp with compute_shape_factor<0>, ShapeFactors.H:40-50): no plasma,
+        // dt = 0
+        if (c.depos_order_xy == 0 && (!c.plasmas.empty() || c.dt != 0.0))
+            throw hpq::InputError("the oracle restates hipace.depos_order_xy = 0 only for a beam in vacuum with dt = 0");
         nx = c.n_cell[0]; ny = c.n_cell[1]; nz = c.n_cell[2];
         dx = (c.prob_hi[0] - c.prob_lo[0]) / nx;
         dy = (c.prob_hi[1] - c.prob_lo[1]) / ny;
@@ -826,6 +831,14 @@ public:
             const double vx = p.ux * gaminv, vy = p.uy * gaminv, vz = p.uz * gaminv;
             const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
             const double xmid = (p.x - xoff) * dxi, ymid = (p.y - yoff) * dyi;
+            if (cfg.depos_order_xy == 0) {
+                // nearest cell, weight 1
+                const int i = (int)std::floor(xmid + 0.5), j = (int)std::floor(ymid + 0.5);
+                if (jx) { (*jx)(i, j) += wqx; (*jy)(i, j) += wqy; }
+                if (jz) (*jz)(i, j) += wqz;
+                if (rmj) (*rmj)(i, j) += wqr;
+                continue;
+            }
             for (int iy = 0; iy <= 2; ++iy)
                 for (int ix = 0; ix <= 2; ++ix) {
                     Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);

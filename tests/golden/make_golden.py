@@ -49,6 +49,12 @@ CASES = {
          "beam.density = 1.e-8", "beam.radius = 1.", "beam.ppc = 4 4 1",
          "beams.external_E(x,y,z,t) = .5*x .5*y 0."],
         1e-12, []),
+    # a can beam in vacuum on a 512 x 768 grid, deposition order 0, multigrid tolerance 1e-5
+    "beam_in_vacuum.normalized.1Rank": (
+        "examples/beam_in_vacuum/inputs_normalized",
+        ["hipace.tile_size = 8", "hipace.depos_order_xy=0", "diagnostic.field_data = all rho",
+         "hipace.MG_tolerance_rel = 1e-5"],
+        1e-12, []),
     # 1023^2 x 1000 slices, fixed_weight_pdf Gaussian beam of 10.5M particles, xz diagnostic
     "transverse_benchmark.1Rank": (
         "examples/benchmarks/inputs_transverse_benchmark",
@@ -56,8 +62,9 @@ CASES = {
         1e-11, []),
 }
 STATISTICAL = {"transverse_benchmark.1Rank"}
-# external beam fields exist in the CPU restatement only (the library rejects them)
-ORACLE_ONLY = {"beam_evolution.1Rank"}
+# external beam fields and deposition order 0 exist in the CPU restatement only (the library
+# rejects them)
+ORACLE_ONLY = {"beam_evolution.1Rank", "beam_in_vacuum.normalized.1Rank"}
 # cases whose beam checksums are of the beam after this many steps (else the injected beam)
 BEAM_AFTER_STEPS = {"beam_evolution.1Rank": 20}
 
