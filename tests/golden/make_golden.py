@@ -55,6 +55,27 @@ CASES = {
         ["hipace.tile_size = 8", "hipace.depos_order_xy=0", "diagnostic.field_data = all rho",
          "hipace.MG_tolerance_rel = 1e-5"],
         1e-12, []),
+    # SI-unit decks (normalized_units = 0) and the serial runs of two decks above
+    "linear_wake.SI.1Rank": (
+        "examples/linear_wake/inputs_SI",
+        ["hipace.tile_size = 8", "diagnostic.field_data = all rho"],
+        1e-11, []),
+    "gaussian_linear_wake.SI.1Rank": (
+        "examples/linear_wake/inputs_SI",
+        ["hipace.tile_size = 8", "beam.profile = gaussian", "beam.zmin = -59.e-6", "beam.zmax = 59.e-6",
+         "beam.radius = 100.e-6", "beam.position_mean = 0. 0. 0", "beam.position_std = 20.e-6 20.e-6 14.1e-6",
+         "geometry.prob_lo     = -100.e-6   -100.e-6   -60.e-6", "geometry.prob_hi     =  100.e-6    100.e-6    60.e-6",
+         "diagnostic.field_data = all rho"],
+        1e-11, []),
+    "beam_in_vacuum.SI.1Rank": (
+        "examples/beam_in_vacuum/inputs_SI",
+        ["hipace.tile_size = 8", "hipace.depos_order_xy=0", "diagnostic.field_data = all rho",
+         "hipace.MG_tolerance_rel = 1e-5"],
+        1e-12, []),
+    "beam_in_vacuum.normalized.Serial": (
+        "examples/beam_in_vacuum/inputs_normalized",
+        ["hipace.tile_size = 8", "hipace.depos_order_xy=0", "diagnostic.field_data = all rho"],
+        1e-12, []),
     # 1023^2 x 1000 slices, fixed_weight_pdf Gaussian beam of 10.5M particles, xz diagnostic
     "transverse_benchmark.1Rank": (
         "examples/benchmarks/inputs_transverse_benchmark",
@@ -64,7 +85,10 @@ CASES = {
 STATISTICAL = {"transverse_benchmark.1Rank"}
 # external beam fields and deposition order 0 exist in the CPU restatement only (the library
 # rejects them)
-ORACLE_ONLY = {"beam_evolution.1Rank", "beam_in_vacuum.normalized.1Rank"}
+ORACLE_ONLY = {"beam_evolution.1Rank", "beam_in_vacuum.normalized.1Rank", "beam_in_vacuum.SI.1Rank",
+               "beam_in_vacuum.normalized.Serial",
+               # SI decks: pinned on the oracle; the GPU golden test runs the normalized decks
+               "linear_wake.SI.1Rank", "gaussian_linear_wake.SI.1Rank"}
 # cases whose beam checksums are of the beam after this many steps (else the injected beam)
 BEAM_AFTER_STEPS = {"beam_evolution.1Rank": 20}
 

@@ -53,9 +53,16 @@ def test_beam_checksums(name):
         assert o.step(s) == 0
     b = o.get_beam(0)
     gold = case["beam"]
-    assert len(b["x"]) == gold["charge"]          # sum |q| with q = -1 per particle
+    # sum |q| over the particles: q = -1 in normalized units, -e in SI
+    normalized = any(l.split("#")[0].replace(" ", "") == "hipace.normalized_units=1" for l in case["input"].splitlines())
+    q = 1.0 if normalized else 1.602176634e-19
+    assert len(b["x"]) == pytest.approx(gold["charge"] / q, rel=1e-12)
+    # momenta are gamma*beta*c here; the reference's output holds gamma*beta (the same in
+    # normalized units, c = 1)
+    c = 1.0 if normalized else 299792458.0
     for k in ("x", "y", "z", "ux", "uy", "uz", "w"):
-        assert np.abs(b[k]).sum() == pytest.approx(gold[k], rel=1e-12, abs=1e-12), k
+        got = np.abs(b[k]).sum() / (c if k.startswith("u") else 1.0)
+        assert got == pytest.approx(gold[k], rel=1e-12, abs=1e-300), (k, got, gold[k])
 
 
 def synthetic_beam(n=4000, seed=5):
