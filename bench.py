@@ -55,7 +55,8 @@ def parse():
     p.add_argument("--config", default="blowout_255")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--no-graphs", action="store_true")
-    p.add_argument("--cpu-sample-slices", type=int, default=0)
+    p.add_argument("--cpu-sample-steps", type=int, default=2,
+                   help="whole steps of the FP64 CPU oracle timed for cpu_baseline")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     p.add_argument("--scale-config", default="channel_1023",
                    help="larger workload timed for FP64 vs mixed (one step each); '' to skip")
@@ -136,6 +137,14 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def workload_config(args, grid, n_plasma, n_beam, world):
+    """The `config` object of both arms (the same dict, so that the two lines compare)."""
+    return {"workload": args.config, "grid": [int(v) for v in grid], "plasma_particles": int(n_plasma),
+            "beam_particles": int(n_beam), "solver": "explicit+multigrid", "precision": args.precision,
+            "steps_timed": "whole steps (all slices, beam push included)",
+            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 per step (beam store)"}
+
+
 def make_sim(text, precision, graphs):
     import hipace2_b200 as hp
     sim = hp.Hipace(text, precision=hp.MIXED if precision == "mixed" else hp.PLAIN_FP64, graphs=graphs)
@@ -177,8 +186,10 @@ def run_ours(args):
     n_plasma = sim.get_plasma(0)["x"].size
     w = args.warmup
     k = args.steps
+    n_beam0 = int(sim.get_beam(0)["x"].size)
     for s in range(w):
         sim.step(s)
+    beam_w = sim.get_beam(0)  # state entering step w (input of the e2e leg)
     # ---- device-timed region (replicas: each rank runs its own independent simulation)
     if world > 1:
         import torch.distributed as dist
@@ -197,28 +208,14 @@ def run_ours(args):
         return float(t.item())
 
     value, secs = job_rate(secs, nz * k, world, reduce_max)
-    # ---- end to end through the C ABI with host buffers (pinned host copies every step)
-    beam = sim.get_beam(0)
-    nb = beam["x"].size
-    pinned = {key: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for key, v in beam.items()}
-    host = {key: v.numpy() for key, v in pinned.items()}
-    # the pushed beam is read back into pinned arrays reused from step to step
-    res_pinned = {key: torch.empty(v.shape, dtype=v.dtype).pin_memory() for key, v in pinned.items()}
-    res_host = {key: v.numpy() for key, v in res_pinned.items()}
-    torch.cuda.synchronize()
-    sim.synchronize()
-    t0 = time.perf_counter()
-    for s in range(w + k, w + 2 * k):
-        sim.set_beam(0, host)
-        sim.step(s)
-        out = sim.get_beam(0, out=res_host)
-    sim.synchronize()
-    e2e_value, _ = job_rate(time.perf_counter() - t0, nz * k, world, reduce_max)
-    h2d = nb * (7 * 8 + 8)
-    d2h = out["x"].size * (7 * 8 + 8 + 1)  # 7 attributes, id, validity flag
+    # ---- end to end through the C ABI with host buffers, on the same step indices and the same
+    # initial beam as the device-timed region: a second simulation of the same deck runs the same
+    # warm-up steps, then every timed step uploads its beam from pinned host memory, runs, and
+    # reads the pushed beam back into pinned memory, which is the next step's input
+    e2e_value, h2d, d2h = e2e_steps(text, args, beam_w, w, k, world, reduce_max, torch)
     # ---- profiled pass (kernel launches with events) for the roofline of the dominant kernel
     sim.set_profiling(True)
-    for s in range(w + 2 * k, w + 3 * k):
+    for s in range(w + k, w + 2 * k):
         sim.step(s)
     classes = ["plasma_deposit", "beam_deposit", "poisson_psi_ez_bz", "explicit_deposit", "multigrid",
                "plasma_push", "beam_push", "beam_partition"]
@@ -251,10 +248,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32 (beam f64)",
         "data": "synthetic: seeded Gaussian driver beam (Philox), lattice plasma",
-        "config": {"workload": args.config, "grid": [nx, ny, nz], "plasma_particles": n_plasma,
-                   "beam_particles": int(nb), "solver": "explicit+multigrid", "precision": args.precision,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 per step (beam store)",
-                   "graphs": not args.no_graphs},
+        "config": workload_config(args, (nx, ny, nz), n_plasma, n_beam0, world),
+        "graphs": not args.no_graphs,
         "particle_updates_per_s": n_plasma * nz * k * world / secs,
         "e2e": {"value": e2e_value, "unit": "slices/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -291,6 +286,50 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def e2e_steps(text, args, beam_w, w, k, world, reduce_max, torch):
+    """Steps w .. w+k-1 through the public C ABI with host buffers: a fresh simulation of the same
+    deck runs the warm-up steps 0 .. w-1 (untimed), then each timed step uploads its input beam
+    from pinned host memory (hpq_set_beam), runs (hpq_step) and reads the pushed beam back into
+    pinned memory (hpq_get_beam), which becomes the next step's input. The first timed step's
+    input is `beam_w`, the beam the device-timed run entered step w with, so both legs do the same
+    work. Returns (slices/s of the job, H2D bytes per step, D2H bytes per step)."""
+    import numpy as np
+    sim = make_sim(text, args.precision, graphs=not args.no_graphs)
+    nz = sim.n_cell[2]
+    for s in range(w):
+        sim.step(s)
+    cap = beam_w["x"].size
+    keys = ("x", "y", "z", "w", "ux", "uy", "uz", "id")
+
+    def pinned_set():
+        out = {}
+        for key in keys:
+            t = torch.empty(cap, dtype=torch.int64 if key == "id" else torch.float64).pin_memory()
+            out[key] = t.numpy()
+        return out
+
+    bufs = [pinned_set(), pinned_set()]
+    for key in keys:
+        bufs[0][key][:] = beam_w[key]
+    cur = {key: bufs[0][key][:cap] for key in keys}
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    sim.synchronize()
+    t0 = time.perf_counter()
+    for i, s in enumerate(range(w, w + k)):
+        n_in = cur["x"].size
+        sim.set_beam(0, cur)
+        sim.step(s)
+        cur = sim.get_beam(0, out=bufs[(i + 1) % 2])
+        h2d += n_in * (7 * 8 + 8)                 # 7 attributes + id
+        d2h += cur["x"].size * (7 * 8 + 8 + 1)   # 7 attributes + id + validity flag
+    sim.synchronize()
+    secs = time.perf_counter() - t0
+    sim.close()
+    value, _ = job_rate(secs, nz * k, world, reduce_max)
+    return value, h2d // k, d2h // k
 
 
 def mixed_vs_fp64(text, args, torch):
@@ -516,71 +555,65 @@ def _key_all(text, key):
     raise KeyError(key)
 
 
-def cpu_baseline(text, args):
-    """This build's FP64 CPU oracle on a bounded sample of the same workload."""
+def oracle_run(text, first, n_steps):
+    """Whole steps first .. first+n_steps-1 of the FP64 CPU oracle (all slices, beam push
+    included) on the beam the oracle draws itself from the deck's seed (the same Philox stream as
+    the library's beam injection; no GPU library is loaded). Returns the oracle and the seconds
+    spent in the steps."""
     from oracle_lib import Oracle
-    import hipace2_b200 as hp
     o = Oracle(text)
-    g = hp.Hipace(text, graphs=False)
-    g.init_data()
-    o.set_beam(0, g.get_beam(0))
-    g.close()
-    nz = o.nz
-    n = args.cpu_sample_slices or max(4, min(nz, 24))
-    threads = o.L.oracle_threads()
+    o.init_beams()
+    for s in range(first):
+        o.step(s)
     t0 = time.perf_counter()
-    o.begin_step(0)
-    for s in range(nz - 1, nz - 1 - n, -1):
-        o.solve_slice(s, 0)
-    dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "slices/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} slices (head of the box) of step 0 of {args.config}, FP64 oracle"}
+    for s in range(first, first + n_steps):
+        o.step(s)
+    return o, time.perf_counter() - t0
+
+
+def cpu_baseline(text, args):
+    """This build's FP64 CPU oracle on a bounded sample of the same workload: its first
+    `--cpu-sample-steps` whole steps."""
+    n = max(1, args.cpu_sample_steps)
+    o, dt = oracle_run(text, 0, n)
+    return {"value": o.nz * n / dt, "unit": "slices/s", "cores": o.L.oracle_threads(), "kind": "port",
+            "sample": f"steps 0-{n - 1} of {args.config}, every slice of each step with the beam push "
+                      "(FP64 oracle, beam drawn by the oracle from the deck's seed)"}
 
 
 def run_reference(args):
     """Reference arm: the reference's CPU implementation of the path. The reference (AMReX,
-    FFTW, MPI) cannot be built on this image, so its restatement (oracle/) runs instead with all
-    host threads, on the same workload, a bounded slice sample per step."""
+    FFTW, MPI) cannot be built on this image, so its FP64 restatement (oracle/, OpenMP, all host
+    threads) runs instead, on the same deck: W warm-up steps, then K timed whole steps (every
+    slice, beam push included), with the beam the oracle draws from the deck's seed. No GPU
+    library is loaded. Under torchrun only rank 0 runs."""
     rank, world, local = dist_env()
     if rank != 0:
         return
     from cases import config
-    from oracle_lib import Oracle, lib
+    from oracle_lib import Oracle
     text = config(args.config)
-    import hipace2_b200 as hp
-    try:
-        g = hp.Hipace(text, graphs=False)
-        g.init_data()
-        beam = g.get_beam(0)
-        g.close()
-    except Exception as e:  # no GPU: draw the same seeded beam is impossible without the library
-        print(json.dumps({"impl": "reference", "unavailable": f"beam generation needs libhpq: {e}"}))
-        return
-    o = Oracle(text)
-    o.set_beam(0, beam)
+    probe = Oracle(text)
+    probe.init_beams()
+    n_beam0 = int(probe.L.oracle_beam_count(probe.h, 0))
+    probe.begin_step(0)  # the plasma of a step is created when the step begins
+    n_plasma = int(probe.L.oracle_plasma_count(probe.h, 0))
+    grid = (probe.nx, probe.ny, probe.nz)
+    del probe
+    o, dt = oracle_run(text, args.warmup, args.steps)
     nz = o.nz
-    n = args.cpu_sample_slices or max(2, min(nz, 8))
-    for s in range(args.warmup):
-        o.begin_step(s)
-        for isl in range(nz - 1, nz - 1 - n, -1):
-            o.solve_slice(isl, s)
-    t0 = time.perf_counter()
-    for s in range(args.steps):
-        o.begin_step(s)
-        for isl in range(nz - 1, nz - 1 - n, -1):
-            o.solve_slice(isl, s)
-    dt = time.perf_counter() - t0
-    v = n * args.steps / dt
-    threads = lib().oracle_threads()
+    v = nz * args.steps / dt
+    threads = o.L.oracle_threads()
     print(json.dumps({
         "impl": "reference", "metric": "slices/s", "value": v, "unit": "slices/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded Gaussian driver beam (Philox), lattice plasma",
-        "config": {"workload": args.config, "parallelism": "cpu"},
+        "config": workload_config(args, grid, n_plasma, n_beam0, world),
         "cpu_baseline": {"value": v, "unit": "slices/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} head slices per step of {args.config}; reference binary not "
-                                   "buildable here (AMReX/FFTW/MPI absent), FP64 oracle restatement"},
+                         "sample": f"steps {args.warmup}-{args.warmup + args.steps - 1} of {args.config}, "
+                                   "every slice with the beam push; the reference binary is not buildable "
+                                   "here (AMReX/FFTW/MPI absent), so its FP64 restatement (oracle/) runs"},
         "e2e": {"value": v, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

@@ -182,13 +182,17 @@ int hpq_get_counters(hpq_handle* h, int64_t* mg_vcycles, int64_t* slices, int64_
  * allocate device memory when they solve — code running under CUDA stream capture, plugins whose
  * host framework owns the memory pool, real-time loops that must not allocate. f and u are
  * device pointers owned by the caller (u may not alias f); `stream` is a cudaStream_t (NULL =
- * default stream). Nothing is allocated: the temporaries live in a 16.1 MiB device array that
- * the library reserves at load time on every GPU that loads it, until the process exits.
- * Limit: nx, ny of the form 2^k - 1 with 31 <= n <= 1023; larger grids return
- * HPQ_ERR_TOO_LARGE, other shapes HPQ_ERR_ARG. The first call on a device looks up the device
- * address of that array (once per device, with the device current), so make the first call on
- * each device before any stream capture. All calls share the array: calls whose kernels overlap
- * on the GPU race and give wrong results; serialise them (one stream, or events). */
+ * default stream). Nothing is allocated: the temporaries live in a 16.1 MiB device array inside
+ * the library. CUDA loads the library's device code lazily, so the first call on each device
+ * commits that array's memory there (and may fail with HPQ_ERR_CUDA if the device is full); it is
+ * held until the process exits. Limit: nx, ny of the form 2^k - 1 with 31 <= n <= 1023; larger
+ * grids return HPQ_ERR_TOO_LARGE, other shapes HPQ_ERR_ARG. The first call on a device also
+ * looks up the device address of that array and sets the kernels' shared-memory limits (once per
+ * device, with the device current), so make the first call on each device before any stream
+ * capture. All calls share the array: calls whose kernels overlap on the GPU race and give wrong
+ * results; serialise them (one stream, or events). A CUDA error already pending when the call
+ * starts is not touched: the call returns HPQ_ERR_CUDA without launching anything; each of its
+ * own launches is checked as it is made. */
 int hpq_poisson_dirichlet_noalloc(const double* f, double* u, int nx, int ny, double dx, double dy,
                                   void* stream);
 

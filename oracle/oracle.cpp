@@ -22,6 +22,7 @@
 #endif
 
 #include "../hipace2_b200/csrc/config.hpp"
+#include "../hipace2_b200/csrc/rng.hpp"
 
 using hpq::SimConfig;
 
@@ -113,23 +114,143 @@ struct BeamSlice {
 };
 
 // ------------------------------------------------------------------------------------------
+// Complex DFT of any length N, out_k = sum_j in_j exp(-2 pi i j k / N), on split real/imaginary
+// arrays: iterative radix-2 (bit reversal, then butterflies) when N is a power of two, else
+// recursive mixed-radix Cooley-Tukey decimation in time over the prime factors of N (a prime
+// factor p costs O(p^2) per butterfly group). Used for the DST-I below.
+// ------------------------------------------------------------------------------------------
+struct FFTPlan {
+    int N = 0;
+    bool pow2 = false;
+    std::vector<int> f;         // prime factors of N (mixed radix)
+    std::vector<double> wr, wi;  // exp(-2 pi i t / N), t < N
+    std::vector<int> rev;       // bit reversal (radix 2)
+    int pmax = 1;
+    void init(int n) {
+        N = n;
+        pow2 = n >= 2 && (n & (n - 1)) == 0;
+        f.clear();
+        for (int m = n, p = 2; m > 1;) {
+            if (m % p == 0) { f.push_back(p); m /= p; continue; }
+            p = (p == 2) ? 3 : p + 2;
+            if ((long long)p * p > m) { f.push_back(m); break; }
+        }
+        pmax = 1;
+        for (int p : f) pmax = std::max(pmax, p);
+        wr.resize(N);
+        wi.resize(N);
+        const double pi = 3.14159265358979323846;
+        for (int t = 0; t < N; ++t) { wr[t] = std::cos(2 * pi * t / N); wi[t] = -std::sin(2 * pi * t / N); }
+        if (pow2) {
+            rev.resize(N);
+            int bits = 0;
+            while ((1 << bits) < N) ++bits;
+            for (int i = 0; i < N; ++i) {
+                int r = 0;
+                for (int k = 0; k < bits; ++k) r |= ((i >> k) & 1) << (bits - 1 - k);
+                rev[i] = r;
+            }
+        }
+    }
+    // in place on (re, im); tmp holds 2 * (N + pmax) doubles
+    void forward(double* re, double* im, double* tmp) const {
+        if (pow2) {
+            for (int i = 0; i < N; ++i)
+                if (rev[i] > i) { std::swap(re[i], re[rev[i]]); std::swap(im[i], im[rev[i]]); }
+            for (int len = 2; len <= N; len <<= 1) {
+                const int half = len >> 1, step = N / len;
+                for (int i0 = 0; i0 < N; i0 += len)
+                    for (int k = 0; k < half; ++k) {
+                        const double c = wr[k * step], s = wi[k * step];
+                        const int a = i0 + k, b = a + half;
+                        const double vr = re[b] * c - im[b] * s, vi = re[b] * s + im[b] * c;
+                        re[b] = re[a] - vr; im[b] = im[a] - vi;
+                        re[a] += vr; im[a] += vi;
+                    }
+            }
+            return;
+        }
+        double* orr = tmp;
+        double* oi = tmp + N;
+        rec(orr, oi, re, im, N, 1, 0, tmp + 2 * N);
+        std::copy(orr, orr + N, re);
+        std::copy(oi, oi + N, im);
+    }
+    void rec(double* outr, double* outi, const double* inr, const double* ini, int n, int s, int fi, double* t) const {
+        const int p = f[fi], m = n / p;
+        if (m == 1) for (int r = 0; r < p; ++r) { outr[r] = inr[(size_t)r * s]; outi[r] = ini[(size_t)r * s]; }
+        else for (int r = 0; r < p; ++r) rec(outr + (size_t)r * m, outi + (size_t)r * m, inr + (size_t)r * s, ini + (size_t)r * s, m, s * p, fi + 1, t);
+        const int sn = N / n, sp = N / p;
+        double* tr = t;
+        double* ti = t + p;
+        for (int k1 = 0; k1 < m; ++k1) {
+            for (int r = 0; r < p; ++r) {
+                const size_t w = (size_t)r * k1 * sn;  // < N
+                const double ar = outr[(size_t)r * m + k1], ai = outi[(size_t)r * m + k1];
+                tr[r] = ar * wr[w] - ai * wi[w];
+                ti[r] = ar * wi[w] + ai * wr[w];
+            }
+            for (int k2 = 0; k2 < p; ++k2) {
+                double accr = 0, acci = 0;
+                size_t w = 0;
+                const size_t dw = (size_t)k2 * sp;
+                for (int r = 0; r < p; ++r) {
+                    accr += tr[r] * wr[w] - ti[r] * wi[w];
+                    acci += tr[r] * wi[w] + ti[r] * wr[w];
+                    w += dw;
+                    if (w >= (size_t)N) w -= N;
+                }
+                outr[(size_t)k2 * m + k1] = accr;
+                outi[(size_t)k2 * m + k1] = acci;
+            }
+        }
+    }
+};
+
+// Unnormalised DST-I (FFTW RODFT00): y_k = 2 sum_j x_j sin(pi (j+1)(k+1) / (n+1)). The odd
+// extension z of length N = 2(n+1) (z_0 = z_{n+1} = 0, z_{j+1} = x_j, z_{N-1-j} = -x_j) has
+// DFT(z)_{k+1} = -i y_k. Two real rows a, b go through one complex DFT of z_a + i z_b:
+// y_a = -Im, y_b = Re.
+struct DST1 {
+    int n = 0;
+    FFTPlan plan;
+    void init(int n_) { n = n_; plan.init(2 * (n + 1)); }
+    size_t work_size() const { return (size_t)2 * plan.N + 2 * ((size_t)plan.N + plan.pmax); }
+    // rows a and b (b may be null), strided; in place
+    void apply2(double* a, double* b, size_t st, double* work) const {
+        const int N = plan.N;
+        double* re = work;
+        double* im = work + N;
+        re[0] = im[0] = re[n + 1] = im[n + 1] = 0;
+        for (int j = 0; j < n; ++j) {
+            const double va = a[(size_t)j * st], vb = b ? b[(size_t)j * st] : 0.0;
+            re[j + 1] = va; re[N - 1 - j] = -va;
+            im[j + 1] = vb; im[N - 1 - j] = -vb;
+        }
+        plan.forward(re, im, work + 2 * N);
+        for (int k = 0; k < n; ++k) {
+            a[(size_t)k * st] = -im[k + 1];
+            if (b) b[(size_t)k * st] = re[k + 1];
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------------
 // Dirichlet Poisson solver: DST-I in x and y, eigenvalue divide, DST-I back
 // (FFTPoissonSolverDirichletFast.cpp:196-328; FFTW RODFT00 in FFTPoissonSolverDirichletDirect).
-// Restated with an explicit sine matrix; normalisation 1/(4(nx+1)(ny+1)) of two unnormalised
-// RODFT00 transforms per axis is folded into the eigenvalues.
+// The transforms are the FFT-based DST-I above (O(n^2 log n) per solve, like FFTW); the
+// normalisation 1/(4(nx+1)(ny+1)) of two unnormalised RODFT00 transforms per axis is folded
+// into the eigenvalues.
 // ------------------------------------------------------------------------------------------
 struct PoissonDST {
     int nx = 0, ny = 0;
-    std::vector<double> sx, sy, eig;  // sine matrices (n x n) and eigenvalues (ny x nx)
+    DST1 tx, ty;
+    std::vector<double> eig;  // eigenvalues (ny x nx)
     void init(int nx_, int ny_, double dx, double dy) {
         nx = nx_; ny = ny_;
         const double pi = 3.14159265358979323846;
-        sx.resize((size_t)nx * nx);
-        sy.resize((size_t)ny * ny);
-        for (int i = 0; i < nx; ++i)
-            for (int k = 0; k < nx; ++k) sx[(size_t)i * nx + k] = 2.0 * std::sin(pi * (i + 1) * (k + 1) / (nx + 1));
-        for (int i = 0; i < ny; ++i)
-            for (int k = 0; k < ny; ++k) sy[(size_t)i * ny + k] = 2.0 * std::sin(pi * (i + 1) * (k + 1) / (ny + 1));
+        tx.init(nx);
+        ty.init(ny);
         const double sxf = pi / (2. * (nx + 1)), syf = pi / (2. * (ny + 1));
         const double norm = 0.5 / (2 * ((nx + 1) * (ny + 1)));
         eig.resize((size_t)nx * ny);
@@ -141,31 +262,23 @@ struct PoissonDST {
             }
     }
     // in/out: row-major ny x nx
+    // rows (x) or columns (y) in pairs, one complex DFT per pair
     void transform_x(std::vector<double>& v) const {
-        std::vector<double> out(v.size());
-#pragma omp parallel for schedule(static)
-        for (int j = 0; j < ny; ++j)
-            for (int k = 0; k < nx; ++k) {
-                double s = 0;
-                const double* row = &v[(size_t)j * nx];
-                const double* m = &sx[(size_t)k * nx];
-                for (int i = 0; i < nx; ++i) s += row[i] * m[i];
-                out[(size_t)j * nx + k] = s;
-            }
-        v.swap(out);
+#pragma omp parallel
+        {
+            std::vector<double> work(tx.work_size());
+#pragma omp for schedule(static)
+            for (int j = 0; j < ny; j += 2)
+                tx.apply2(&v[(size_t)j * nx], j + 1 < ny ? &v[(size_t)(j + 1) * nx] : nullptr, 1, work.data());
+        }
     }
     void transform_y(std::vector<double>& v) const {
-        std::vector<double> out(v.size(), 0.0);
-#pragma omp parallel for schedule(static)
-        for (int k = 0; k < ny; ++k) {
-            double* o = &out[(size_t)k * nx];
-            for (int j = 0; j < ny; ++j) {
-                const double m = sy[(size_t)k * ny + j];
-                const double* row = &v[(size_t)j * nx];
-                for (int i = 0; i < nx; ++i) o[i] += m * row[i];
-            }
+#pragma omp parallel
+        {
+            std::vector<double> work(ty.work_size());
+#pragma omp for schedule(static)
+            for (int i = 0; i < nx; i += 2) ty.apply2(&v[i], i + 1 < nx ? &v[i + 1] : nullptr, nx, work.data());
         }
-        v.swap(out);
     }
     void solve(std::vector<double>& v) const {
         transform_x(v);
@@ -558,6 +671,7 @@ public:
                             "Salame.Sx_back"})
                 F[n].init(gr);
         else for (auto* n : names_pc) F[n].init(gr);
+        g_psi = &f("Psi"); g_ez = &f("Ez"); g_bx = &f("Bx"); g_by = &f("By"); g_bz = &f("Bz");
         dst.init(nx, ny, dx, dy);
         if (c.explicit_solver) mg.init(nx, ny, dx, dy);
         store.resize(c.beams.size());
@@ -638,6 +752,59 @@ public:
         store_valid[b] = true;
     }
 
+    // InitBeamFixedWeight3D (BeamParticleContainerInit.cpp:349-476): Gaussian (or can) beam of
+    // num_particles equal weights Q / (N q). The reference draws from AMReX's random stream,
+    // which is not reproduced; this draw uses the counter-based Philox4x32-10 stream of
+    // ../hipace2_b200/csrc/rng.hpp with the seed derivation of the library's beam injection, so
+    // that the oracle and the library start from the same particles without exchanging them
+    // (per particle i: normals of counters 2i and 2i+1; z of a can beam from uniform(2i+1, 3)).
+    void init_beam_fixed_weight(int b) {
+        const hpq::BeamSpecies& B = cfg.beams[b];
+        const int64_t n = B.num_particles;
+        std::vector<double> x, y, z, w, ux, uy, uz;
+        std::vector<int64_t> id;
+        if (n > 0) {
+            const int64_t nbase = B.do_symmetrize ? n / 4 : n;
+            const uint64_t seed = (uint64_t)(cfg.has_random_seed ? cfg.random_seed : 0) * 1000003ull +
+                                  (uint64_t)b * 7919ull + 12345ull;
+            const hpq::Philox rng(seed);
+            const bool can = B.profile == hpq::BeamProfile::Can;
+            const double z_mean = can ? 0.5 * (B.zmin + B.zmax) : B.position_mean[2];
+            const double weight = B.total_charge / (B.num_particles * B.charge);
+            const int ncopy = B.do_symmetrize ? 4 : 1;
+            const size_t cap = (size_t)nbase * ncopy;
+            for (auto* v : {&x, &y, &z, &w, &ux, &uy, &uz}) v->reserve(cap);
+            id.reserve(cap);
+            int64_t pid = 1;
+            for (int64_t i = 0; i < nbase; ++i) {
+                double g[8];
+                rng.normals(2 * (uint64_t)i, g);
+                rng.normals(2 * (uint64_t)i + 1, g + 4);
+                const double zc = can ? rng.uniform(2 * (uint64_t)i + 1, 3) * (B.zmax - B.zmin) + B.zmin
+                                      : z_mean + B.position_std[2] * g[0];
+                double px = B.position_std[0] * g[1], py = B.position_std[1] * g[2];
+                double u[3] = {B.u_mean[0] + B.u_std[0] * g[3], B.u_mean[1] + B.u_std[1] * g[4],
+                               B.u_mean[2] + B.u_std[2] * g[5]};
+                u[2] += (zc - z_mean) * B.duz_per_uz0_dzeta * B.u_mean[2];
+                const bool inside = !(zc < B.zmin || zc > B.zmax || px * px + py * py > B.radius * B.radius);
+                px -= B.z_foc * u[0] / u[2];
+                py -= B.z_foc * u[1] / u[2];
+                for (int q = 0; q < ncopy; ++q) {
+                    const double sx = (q & 1) ? -1 : 1, sy = (q & 2) ? -1 : 1;
+                    double xp = B.position_mean[0] + sx * px, yp = B.position_mean[1] + sy * py;
+                    double uxp = sx * u[0] * cfg.pc.c, uyp = sy * u[1] * cfg.pc.c;
+                    const bool ok = enforce_bc(xp, yp, uxp, uyp) && inside;
+                    x.push_back(xp); y.push_back(yp); z.push_back(zc);
+                    w.push_back(ok ? std::fabs(weight) : 0.0);
+                    ux.push_back(uxp); uy.push_back(uyp); uz.push_back(u[2] * cfg.pc.c);
+                    id.push_back(pid++);
+                }
+            }
+        }
+        set_beam(b, x.data(), y.data(), z.data(), w.data(), ux.data(), uy.data(), uz.data(), id.data(),
+                 (int64_t)x.size());
+    }
+
     // EnforceBC (GetAndSetPosition.H:29-99); returns false if the particle is absorbed
     bool enforce_bc(double& x, double& y, double& ux, double& uy) const {
         const double plo0 = cfg.particle_lo[0], plo1 = cfg.particle_lo[1];
@@ -714,6 +881,35 @@ public:
         }
     }
 
+    // -------------------------------------------------------------- threaded deposition
+    // The deposits run over the particles grouped in bands of kBand cell rows (by the row of
+    // the particle's position). A deposit stencil reaches at most 3 rows from that row, so the
+    // bands of one parity touch disjoint rows: the even bands deposit in parallel, then the odd
+    // ones. Within a band the particles keep their order, so the sums do not depend on the number
+    // of threads. (The reference's OpenMP build tiles its deposition in the same spirit,
+    // PlasmaDepositCurrent.cpp:90-130.)
+    static constexpr int kBand = 8;
+    template <class Body>
+    void for_particles_banded(const Plasma& pl, const std::vector<double>& ypos, Body body) {
+        const size_t n = pl.n();
+        const int nb = (gr.ny + 2 * gr.g) / kBand + 2;
+        std::vector<int> band(n);
+        std::vector<size_t> start(nb + 1, 0);
+        for (size_t ip = 0; ip < n; ++ip) {
+            const int row = (int)std::floor((ypos[ip] - yoff) * dyi) + gr.g;
+            band[ip] = std::min(std::max(row / kBand, 0), nb - 1);
+            ++start[band[ip] + 1];
+        }
+        for (int b = 0; b < nb; ++b) start[b + 1] += start[b];
+        std::vector<size_t> idx(n), fill(start.begin(), start.end() - 1);
+        for (size_t ip = 0; ip < n; ++ip) idx[fill[band[ip]]++] = ip;
+        for (int parity = 0; parity < 2; ++parity) {
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int b = parity; b < nb; b += 2)
+                for (size_t k = start[b]; k < start[b + 1]; ++k) body(idx[k]);
+        }
+    }
+
     // -------------------------------------------------------------- plasma deposition
     // PlasmaDepositCurrent.cpp:22-259, order 2. `which`: 0 = This, 1 = Next, 2 = ions.
     void plasma_deposit(int which, bool jxjy, bool jz, bool rho, bool chi, bool rhomjz) {
@@ -745,8 +941,8 @@ public:
                     if (jxjy) { Fjx = &f("Next.jx"); Fjy = &f("Next.jy"); }
                 }
             }
-            for (size_t ip = 0; ip < pl.n(); ++ip) {
-                if (!pl.valid[ip]) continue;
+            for_particles_banded(pl, pl.y, [&](size_t ip) {
+                if (!pl.valid[ip]) return;
                 const double psi_inv = 1.0 / pl.psi[ip];
                 const double xp = pl.x[ip], yp = pl.y[ip];
                 const double vx_c = pl.ux[ip] * psi_inv;
@@ -761,7 +957,7 @@ public:
                 if (gamma_psi < 0.0 || gamma_psi > P.max_qsa_weighting_factor || psi_inv < 0.0) {
                     pl.w[ip] = 0.0;
                     pl.valid[ip] = 0;
-                    continue;
+                    return;
                 }
                 for (int iy = 0; iy <= 2; ++iy)
                     for (int ix = 0; ix <= 2; ++ix) {
@@ -774,7 +970,7 @@ public:
                         if (Fchi) (*Fchi)(i, j) += cd * q_mu0_mass_ratio * psi_inv;
                         if (Frm) (*Frm)(i, j) += cd;
                     }
-            }
+            });
         }
     }
 
@@ -793,8 +989,8 @@ public:
             const double a_clight = cfg.pc.c, clight_inv = 1. / cfg.pc.c;
             const double charge_invvol_mu0 = P.charge * invvol * cfg.pc.mu0;
             const double q_mass_ratio = P.charge / P.mass;
-            for (size_t ip = 0; ip < pl.n(); ++ip) {
-                if (!pl.valid[ip]) continue;
+            for_particles_banded(pl, pl.y, [&](size_t ip) {
+                if (!pl.valid[ip]) return;
                 const double psi_inv = 1. / pl.psi[ip];
                 const double xp = pl.x[ip], yp = pl.y[ip];
                 const double vx = pl.ux[ip] * psi_inv * clight_inv;
@@ -802,11 +998,13 @@ public:
                 const double cdm = charge_invvol_mu0 * pl.w[ip];
                 const double xmid = (xp - xoff) * dxi, ymid = (yp - yoff) * dyi;
                 const double gamma_psi = 0.5 * ((1. + 0.5 * 0.0) * psi_inv * psi_inv + vx * vx + vy * vy + 1.);
+                DShape shx[5], shy[5];
+                for (int k = 0; k <= ns; ++k) { shx[k] = dshape2(dt, xmid, k); shy[k] = dshape2(dt, ymid, k); }
                 for (int iy = 0; iy <= ns; ++iy)
                     for (int ix = 0; ix <= ns; ++ix) {
                         if (dt == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
-                        DShape sy = dshape2(dt, ymid, iy);
-                        DShape sx = dshape2(dt, xmid, ix);
+                        const DShape& sy = shy[iy];
+                        const DShape& sx = shx[ix];
                         const int i = sx.cell, j = sy.cell;
                         const double Bz_v = Bz(i, j), Ez_v = Ez(i, j), ExmBy_v = ExmBy(i, j), EypBx_v = EypBx(i, j);
                         Sy(i, j) += cdm * (-sx.s * sy.s * (-Bz_v * vx + (Ez_v * vy + ExmBy_v * (-vx * vy) + EypBx_v * (gamma_psi - vy * vy)) * clight_inv - 0.25 * 0.0 * q_mass_ratio * psi_inv) * q_mass_ratio * psi_inv +
@@ -814,7 +1012,7 @@ public:
                         Sx(i, j) += cdm * (+sx.s * sy.s * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv - 0.25 * 0.0 * q_mass_ratio * psi_inv) * q_mass_ratio * psi_inv +
                                            (+sx.ds * sy.s * dxi * (gamma_psi - vx * vx - 1.) + sx.s * sy.ds * dyi * (-vx * vy)) * a_clight);
                     }
-            }
+            });
         }
     }
 
@@ -956,14 +1154,18 @@ public:
         dpsi = dmul(dmul(Dual{qmc, 0}, Dual{ci, 0}), dsub(dmul(dmul(dadd(dmul(ux, Dual{ExmBy, 0}), dmul(uy, Dual{EypBx, 0})), Dual{ci, 0}), pi), Dual{Ez, 0}));
     }
 
+    // the gathered planes, looked up once (std::map nodes do not move)
+    const Field *g_psi = nullptr, *g_ez = nullptr, *g_bx = nullptr, *g_by = nullptr, *g_bz = nullptr;
     void gather(double xp, double yp, double& ExmBy, double& EypBx, double& Ez, double& Bx, double& By, double& Bz) {
-        const Field& Psi = f("Psi"); const Field& FEz = f("Ez");
-        const Field& FBx = f("Bx"); const Field& FBy = f("By"); const Field& FBz = f("Bz");
+        const Field& Psi = *g_psi; const Field& FEz = *g_ez;
+        const Field& FBx = *g_bx; const Field& FBy = *g_by; const Field& FBz = *g_bz;
         const double x = (xp - xoff) * dxi, y = (yp - yoff) * dyi;
+        DShape shx[4], shy[4];
+        for (int k = 0; k <= 3; k++) { shx[k] = dshape2(1, x, k); shy[k] = dshape2(1, y, k); }
         for (int iy = 0; iy <= 3; iy++)
             for (int ix = 0; ix <= 3; ix++) {
-                DShape sy = dshape2(1, y, iy);
-                DShape sx = dshape2(1, x, ix);
+                const DShape& sy = shy[iy];
+                const DShape& sx = shx[ix];
                 const int i = sx.cell, j = sy.cell;
                 ExmBy += (sx.ds * sy.s) * Psi(i, j) * dxi;
                 EypBx += (sx.s * sy.ds) * Psi(i, j) * dyi;
@@ -1027,7 +1229,9 @@ public:
         const double clight = cfg.pc.c, inv_c2 = 1. / (cfg.pc.c * cfg.pc.c);
         const double cmr = B.charge / B.mass;
         const double min_z = cfg.prob_lo[2] + (islice - 0) * dz;
-        for (auto& p : bs.p) {
+#pragma omp parallel for schedule(static) if (bs.p.size() > 2048)
+        for (size_t ip = 0; ip < bs.p.size(); ++ip) {
+            BeamParticle& p = bs.p[ip];
             if (!p.valid) continue;
             double xp = p.x, yp = p.y, zp = p.z, ux = p.ux, uy = p.uy, uz = p.uz;
             int i = p.nsub;
@@ -2110,7 +2314,9 @@ int oracle_init_beams(OracleHandle* h) {
     auto& s = *h->sim;
     for (size_t b = 0; b < s.cfg.beams.size(); ++b) {
         if (s.cfg.beams[b].injection == hpq::BeamInjection::FixedPPC) s.init_beam_fixed_ppc((int)b);
-        else if (!s.store_valid[b]) return 2;  // fixed_weight beams must be provided
+        else if (s.store_valid[b]) continue;  // particles given with oracle_set_beam
+        else if (s.cfg.beams[b].injection == hpq::BeamInjection::FixedWeight) s.init_beam_fixed_weight((int)b);
+        else return 2;  // fixed_weight_pdf beams must be provided
     }
     return 0;
 }
@@ -2208,7 +2414,11 @@ int oracle_get_field(OracleHandle* h, const char* name, double* out) {
     return 0;
 }
 
-int64_t oracle_plasma_count(OracleHandle* h, int sp) { return (int64_t)h->sim->plasmas[sp].n(); }
+// particles of plasma species sp in the current step (0 before the first step begins)
+int64_t oracle_plasma_count(OracleHandle* h, int sp) {
+    const auto& p = h->sim->plasmas;
+    return (sp >= 0 && sp < (int)p.size()) ? (int64_t)p[sp].n() : 0;
+}
 // attributes: x y w ux uy psi x_prev y_prev ux_half uy_half psi_half valid
 int oracle_get_plasma(OracleHandle* h, int sp, double* out12) {
     auto& pl = h->sim->plasmas[sp];

@@ -1,6 +1,6 @@
 """Generate the golden fixtures from the reference's own regression tests.
 
-Reads, from a HiPACE++ source tree (default /root/reference):
+Reads, from a HiPACE++ source tree (the path given on the command line):
   * the example input decks named by each regression test script,
   * the command-line overrides that script passes (tests/<name>.sh),
   * the checksum goldens (tests/checksum/benchmarks_json/<name>.json),
@@ -14,7 +14,7 @@ Cases marked "statistical" draw their beam from a random stream (AMReX's in the 
 library's here): their beam checksums that do not depend on the stream (particle count, total
 weight, uz of a cold beam) pin the injection exactly, the field checksums only statistically.
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>
 """
 import json
 import os
@@ -130,4 +130,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference_root>")
+    main(sys.argv[1])

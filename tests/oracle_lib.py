@@ -21,7 +21,8 @@ def build(force=False):
 def _newest_source():
     srcs = [os.path.join(ROOT, "oracle", "oracle.cpp"),
             os.path.join(ROOT, "hipace2_b200", "csrc", "config.hpp"),
-            os.path.join(ROOT, "hipace2_b200", "csrc", "inputs.hpp")]
+            os.path.join(ROOT, "hipace2_b200", "csrc", "inputs.hpp"),
+            os.path.join(ROOT, "hipace2_b200", "csrc", "rng.hpp")]
     return max(os.path.getmtime(s) for s in srcs)
 
 
@@ -111,7 +112,7 @@ class Oracle:
     def init_beams(self):
         rc = self.L.oracle_init_beams(self.h)
         if rc:
-            raise RuntimeError("fixed_weight beams must be set with set_beam before init")
+            raise RuntimeError("fixed_weight_pdf beams must be set with set_beam before init")
 
     def set_beam(self, b, beam):
         arrs = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in BEAM_ATTRS]

@@ -72,10 +72,6 @@ def test_explicit_moving_beam_matches_oracle():
         e = rel_l2(bg[k][ig], bo[k][io])
         assert e <= 1e-10, (k, e)
     pg, po = g.get_plasma(0), o.get_plasma(0)
-    out = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
-    if os.path.isdir(out):
-        np.savez(os.path.join(out, "plasma_parity.npz"), **{"g_" + k: v for k, v in pg.items()},
-                 **{"o_" + k: v for k, v in po.items()})
     # particles invalidated by the QSA test (a runaway with psi < 0 here) freeze at chaotic
     # values; the valid flags must agree and only valid particles are compared
     assert np.array_equal(pg["valid"], po["valid"])

@@ -57,3 +57,32 @@ def test_noalloc_poisson_rejects_sizes_beyond_the_limit():
     dummy = ctypes.c_void_p(16)
     assert L.hpq_poisson_dirichlet_noalloc(dummy, dummy, 2047, 2047, 0.1, 0.1, None) == 7
     assert L.hpq_poisson_dirichlet_noalloc(dummy, dummy, 100, 100, 0.1, 0.1, None) == 6
+
+
+@pytest.mark.parametrize("nx,ny", [(127, 63), (127, 255), (1023, 1023)])
+def test_noalloc_poisson_matches_oracle_on_rectangular_and_largest_grids(nx, ny):
+    """Non-square grids (the x and y twiddle tables and transform lengths differ) and the
+    largest grid the scratch array holds, against the CPU oracle's DST-I solve; two calls in a
+    row with different right-hand sides, so the second one runs on the first one's leftovers."""
+    import torch
+    from oracle_lib import lib
+
+    L = hp.load_library()
+    O = lib()
+    rng = np.random.default_rng(nx * 7 + ny)
+    dx, dy = 0.05, 0.07
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        f = rng.standard_normal((ny, nx))
+        want = np.zeros_like(f)
+        assert O.oracle_poisson_dirichlet(f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          want.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          nx, ny, dx, dy) == 0
+        fd = torch.from_numpy(f).cuda()
+        u = torch.full_like(fd, float("nan"))
+        rc = L.hpq_poisson_dirichlet_noalloc(ctypes.c_void_p(fd.data_ptr()), ctypes.c_void_p(u.data_ptr()),
+                                             nx, ny, dx, dy, ctypes.c_void_p(stream.cuda_stream))
+        assert rc == 0
+        torch.cuda.synchronize()
+        got = u.cpu().numpy()
+        assert rel_l2(got, want) <= 1e-10, rel_l2(got, want)
