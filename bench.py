@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--cpu-sample-steps", type=int, default=2,
                    help="whole steps of the FP64 CPU oracle timed for cpu_baseline")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--scale-config", default="channel_1023",
                    help="larger workload timed for FP64 vs mixed (one step each); '' to skip")
     p.add_argument("--adjoint-config", default="beam_loading_255",
@@ -271,7 +272,8 @@ def run_ours(args):
     }
     if rank == 0:
         line["gpu_launches"] = launches_in_timed
-        line["cpu_baseline"] = cpu_baseline(text, args)
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(text, args)
     sim.close()
     if rank == 0 and not args.no_mixed and args.precision == "fp64":
         line["mixed"] = mixed_vs_fp64(text, args, torch)

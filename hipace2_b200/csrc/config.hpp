@@ -45,6 +45,11 @@ struct PlasmaSpecies {
     int n_subcycles = 1;
     bool neutralize_background = true;
     bool prevent_centered_particle = false;
+    bool thermal = false;     // u_std != 0: momenta drawn every step (rng.hpp plasma_thermal_u)
+    // reorder by cell every reorder_period slices (PlasmaParticleContainer.cpp:197-208), binned
+    // to cells (0) or nodes (1) per axis
+    int reorder_period = 0;
+    int reorder_idx_type[2] = {0, 0};
 };
 
 enum class BeamInjection : int { FixedPPC = 0, FixedWeight = 1, FixedWeightPDF = 2 };
@@ -374,7 +379,7 @@ inline SimConfig build_config(const InputStore& in) {
                 throw InputError("input '" + name + ".insitu_period' is not supported: plasma in-situ diagnostics are not implemented");
         }
         reject(in, name + ".density_table_file", "density tables are not implemented");
-        reject(in, name + ".temperature_in_ev", "use u_std instead");
+
         int ion_lev = -1;
         if (in.query(name + ".initial_ion_level", ion_lev)) p.charge *= ion_lev;
         query_alt(in, name, "plasmas", "n_subcycles", p.n_subcycles);
@@ -392,10 +397,26 @@ inline SimConfig build_config(const InputStore& in) {
         if (!query_alt_arr(in, name, "plasmas", "ppc", p.ppc))
             throw InputError("missing required input '" + name + ".ppc'");
         in.query_arr(name + ".u_mean", p.u_mean);
-        in.query_arr(name + ".u_std", p.u_std);
+        const bool has_u_std = in.query_arr(name + ".u_std", p.u_std);
+        double temperature_ev = 0;
+        const bool has_t = in.query(name + ".temperature_in_ev", temperature_ev);
+        if (has_u_std && has_t)
+            throw InputError("Please specify exlusively either a temperature or the thermal momentum");
+        if (has_t) {
+            // PlasmaParticleContainer.cpp:135-144: u_std = sqrt(T e / (m c^2)) in SI
+            const double q_e_si = 1.602176634e-19, m_e_si = 9.1093837015e-31, c_si = 299792458.0;
+            const double m_si = p.mass * (m_e_si / pc.m_e);
+            for (int d = 0; d < 3; ++d) p.u_std[d] = std::sqrt(temperature_ev * q_e_si / (m_si * c_si * c_si));
+        }
+        p.thermal = p.u_std[0] != 0 || p.u_std[1] != 0 || p.u_std[2] != 0;
         query_alt(in, name, "plasmas", "prevent_centered_particle", p.prevent_centered_particle);
-        int reorder = 0;
-        query_alt(in, name, "plasmas", "reorder_period", reorder);  // cache locality only
+        query_alt(in, name, "plasmas", "reorder_period", p.reorder_period);
+        if (p.reorder_period < 0) throw InputError(name + ".reorder_period must be >= 0");
+        p.reorder_idx_type[0] = p.reorder_idx_type[1] = c.depos_order_xy % 2;
+        query_alt_arr(in, name, "plasmas", "reorder_idx_type", p.reorder_idx_type);
+        for (int d = 0; d < 2; ++d)
+            if (p.reorder_idx_type[d] != 0 && p.reorder_idx_type[d] != 1)
+                throw InputError(name + ".reorder_idx_type must be 0 (cells) or 1 (nodes) per axis");
         c.plasmas.push_back(p);
     }
     // ---------------- beams

@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "inputs.hpp"
+#include "rng.hpp"
 
 namespace hpq {
 
@@ -59,7 +60,7 @@ struct PlasmaDev {
     // so the cell fraction that the shape factors use and the deviation of psi from 1 keep full
     // FP32 precision instead of the precision of |x| and of 1. Null in double precision, where
     // x, y and psi are stored as they are.
-    const float *ru, *rv;
+    float *ru, *rv;
     uint8_t* valid;
     long long n;
     double charge, mass, qsa_max;
@@ -136,24 +137,173 @@ __device__ __forceinline__ bool enforce_bc(const Geo& g, T& x, T& y, T& ux, T& u
 // species is fixed on the host (lattice positions that pass the domain/radius tests); the
 // kernel evaluates the density expression at c*t and resets all attributes.
 // ------------------------------------------------------------------------------------------
+// Thermal momenta (u_std != 0) are drawn per particle from the counter-based stream of rng.hpp
+// (plasma_thermal_u), keyed by the particle's lattice index and the step. Particles are put back
+// in lattice order (a reorder during the previous step permuted them), including their lattice
+// points in cell units in single precision.
+struct PlasmaMomenta {
+    double mean[3], stdv[3];
+    uint64_t seed;
+    int step;
+    int thermal;
+};
 template <class R>
 __global__ void k_plasma_reset(PlasmaDev<R> P, const double* __restrict__ x0, const double* __restrict__ y0,
-                               Expr density, double c_t, double scale, double ux0, double uy0, double uz0,
-                               double clight) {
+                               Expr density, double c_t, double scale, PlasmaMomenta m, double clight, double xoff,
+                               double dxi, double yoff, double dyi) {
     HPQ_PDL_ENTRY();
+    const Philox rng(m.seed);
     for (long long i = gtid(); i < P.n; i += gstride()) {
         const double x = x0[i], y = y0[i];
         double v[3] = {x, y, c_t};
         const double w = density.eval(v) * scale;
-        const double psi = sqrt(1. + ux0 * ux0 + uy0 * uy0 + uz0 * uz0) - uz0;
+        double u[3] = {m.mean[0], m.mean[1], m.mean[2]};
+        if (m.thermal) plasma_thermal_u(rng, m.step, i, m.mean, m.stdv, u);
+        const double psi = sqrt(1. + u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) - u[2];
         const R xs = P.ru ? R(0) : (R)x, ys = P.ru ? R(0) : (R)y;
         P.x[i] = xs; P.y[i] = ys; P.xp[i] = xs; P.yp[i] = ys;
+        if (P.ru) {
+            P.ru[i] = (float)((x - xoff) * dxi);
+            P.rv[i] = (float)((y - yoff) * dyi);
+        }
         P.w[i] = (R)w;
-        P.ux[i] = (R)(ux0 * clight); P.uy[i] = (R)(uy0 * clight);
-        P.uxh[i] = (R)(ux0 * clight); P.uyh[i] = (R)(uy0 * clight);
+        P.ux[i] = (R)(u[0] * clight); P.uy[i] = (R)(u[1] * clight);
+        P.uxh[i] = (R)(u[0] * clight); P.uyh[i] = (R)(u[1] * clight);
         const R psis = P.ru ? (R)(psi - 1.0) : (R)psi;
         P.psi[i] = psis; P.psih[i] = psis;
         P.valid[i] = 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Plasma reorder (PlasmaParticleContainer::ReorderParticles, PlasmaParticleContainer.cpp:197-208):
+// every reorder_period slices the particles are sorted by the cell (or node) they sit in, which
+// gives the deposit's atomics cell locality once the plasma response has scattered them. The
+// sort is a stable counting sort, so that runs are reproducible: keys and per-bin counts, an
+// exclusive scan over the bins, a scatter into the bins, each bin's indices put back in
+// ascending order (bins hold a few particles), then a gather of every attribute into scratch
+// arrays and a copy back (the slice graph keeps the attribute pointers).
+// Bin of a particle: cell centres sit at integer t = (x - xoff) / dx, so the cell is
+// floor(t + 1/2) in [0, n-1] and the nearest node floor(t + 1) in [0, n]; key = j (nx + 1) + i.
+// ------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ int reorder_bin(bool has_ref, float r0, R x, double off, double dxi, int n, int node) {
+    const double t = has_ref ? (double)r0 + (double)x * dxi : ((double)x - off) * dxi;
+    const double f = floor(t + (node ? 1.0 : 0.5));
+    const int hi = node ? n : n - 1;
+    return f < 0 ? 0 : (f > hi ? hi : (int)f);
+}
+
+template <class R>
+__global__ void k_reorder_keys(PlasmaDev<R> P, Geo g, int node_x, int node_y, int* __restrict__ key,
+                               int* __restrict__ cnt) {
+    HPQ_PDL_ENTRY();
+    for (long long i = gtid(); i < P.n; i += gstride()) {
+        const int bi = reorder_bin<R>(P.ru != nullptr, P.ru ? P.ru[i] : 0.f, P.x[i], g.xoff, g.dxi[0], g.nx, node_x);
+        const int bj = reorder_bin<R>(P.rv != nullptr, P.rv ? P.rv[i] : 0.f, P.y[i], g.yoff, g.dxi[1], g.ny, node_y);
+        const int k = bj * (g.nx + 1) + bi;
+        key[i] = k;
+        atomicAdd(&cnt[k], 1);
+    }
+}
+
+// exclusive scan of n ints in three launches: per-block scans (1024 per block) with block
+// totals, the scan of the block totals (one block), and the block offsets added (also written to
+// `fill`, the scatter cursors)
+__device__ __forceinline__ int block_exclusive_scan_1024(int v, int& total) {
+    __shared__ int ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    __syncthreads();
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        if (w < warp) before += ws[w];
+        total += ws[w];
+    }
+    return before + x - v;
+}
+__global__ void __launch_bounds__(1024) k_scan_blocks(const int* __restrict__ in, int* __restrict__ out,
+                                                      int* __restrict__ bsum, long long n) {
+    HPQ_PDL_ENTRY();
+    const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+    int total;
+    const int e = block_exclusive_scan_1024(i < n ? in[i] : 0, total);
+    if (i < n) out[i] = e;
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(1024) k_scan_totals(int* __restrict__ bsum, int nb) {
+    HPQ_PDL_ENTRY();
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < nb; b0 += 1024) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < nb ? bsum[b] : 0;
+        int total;
+        const int e = block_exclusive_scan_1024(v, total);
+        const int base = carry;
+        if (b < nb) bsum[b] = base + e;
+        __syncthreads();
+        if (threadIdx.x == 0) carry = base + total;
+        __syncthreads();
+    }
+}
+__global__ void k_scan_add(int* __restrict__ out, const int* __restrict__ bsum, int* __restrict__ fill, long long n) {
+    HPQ_PDL_ENTRY();
+    for (long long i = gtid(); i < n; i += gstride()) {
+        const int v = out[i] + bsum[i / 1024];
+        out[i] = v;
+        fill[i] = v;
+    }
+}
+
+__global__ void k_reorder_scatter(const int* __restrict__ key, long long n, int* __restrict__ fill, int* __restrict__ perm) {
+    HPQ_PDL_ENTRY();
+    for (long long i = gtid(); i < n; i += gstride()) perm[atomicAdd(&fill[key[i]], 1)] = (int)i;
+}
+
+// one thread per bin: insertion sort of the bin's particle indices (ascending = stable)
+__global__ void k_reorder_bins(const int* __restrict__ start, const int* __restrict__ cnt, long long nbins,
+                               int* __restrict__ perm) {
+    HPQ_PDL_ENTRY();
+    for (long long b = gtid(); b < nbins; b += gstride()) {
+        const int s0 = start[b], m = cnt[b];
+        for (int a = 1; a < m; ++a) {
+            const int v = perm[s0 + a];
+            int c = a - 1;
+            while (c >= 0 && perm[s0 + c] > v) {
+                perm[s0 + c + 1] = perm[s0 + c];
+                --c;
+            }
+            perm[s0 + c + 1] = v;
+        }
+    }
+}
+
+// dst[k] = src[perm[k]] for every attribute (to = 1), or the copy back src[k] = dst[k] (to = 0)
+template <class R>
+__global__ void k_reorder_move(PlasmaDev<R> P, PlasmaDev<R> T, const int* __restrict__ perm, int to) {
+    HPQ_PDL_ENTRY();
+    for (long long k = gtid(); k < P.n; k += gstride()) {
+        if (to) {
+            const int i = perm[k];
+            T.x[k] = P.x[i]; T.y[k] = P.y[i]; T.w[k] = P.w[i]; T.ux[k] = P.ux[i]; T.uy[k] = P.uy[i];
+            T.psi[k] = P.psi[i]; T.xp[k] = P.xp[i]; T.yp[k] = P.yp[i]; T.uxh[k] = P.uxh[i]; T.uyh[k] = P.uyh[i];
+            T.psih[k] = P.psih[i]; T.valid[k] = P.valid[i];
+            if (P.ru) { T.ru[k] = P.ru[i]; T.rv[k] = P.rv[i]; }
+        } else {
+            P.x[k] = T.x[k]; P.y[k] = T.y[k]; P.w[k] = T.w[k]; P.ux[k] = T.ux[k]; P.uy[k] = T.uy[k];
+            P.psi[k] = T.psi[k]; P.xp[k] = T.xp[k]; P.yp[k] = T.yp[k]; P.uxh[k] = T.uxh[k]; P.uyh[k] = T.uyh[k];
+            P.psih[k] = T.psih[k]; P.valid[k] = T.valid[k];
+            if (P.ru) { P.ru[k] = T.ru[k]; P.rv[k] = T.rv[k]; }
+        }
     }
 }
 

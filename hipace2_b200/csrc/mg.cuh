@@ -475,9 +475,20 @@ __device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* dinv, const 
 // solve, still resident in this block's shared memory. The global arrays are plain (not
 // restrict/read-only) pointers: in the persistent solve other blocks write them earlier in the
 // same launch.
+__device__ __forceinline__ unsigned long long tc_clock_ns();
+
+// bt (tracing only): thread 0 records the global timer at the start, after the set-up, after each
+// level of the down sweep, after the coarsest level, after each level of the up sweep and at the
+// end: bt[0] = count, bt[1..]
 template <class R, bool CELL>
 __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
-                                                R facy0, unsigned char* smem_raw, bool init) {
+                                                R facy0, unsigned char* smem_raw, bool init,
+                                                unsigned long long* bt = nullptr) {
+    int nbt = 0;
+    auto bstamp = [&]() {
+        if (bt && threadIdx.x == 0 && nbt < 60) bt[1 + nbt++] = tc_clock_ns();
+    };
+    bstamp();
     __syncthreads();  // the block may have used the shared memory just before
     R* arena = reinterpret_cast<R*>(smem_raw);
     // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
@@ -522,12 +533,14 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         res(0)[n0 + k] = res_g[n0 + k];
     }
     __syncthreads();
+    bstamp();
     R facx = facx0, facy = facy0;
     for (int l = 0; l < M.nl; ++l) {
         const MGLev& L = M.L[l];
         const int plane = L.w * L.h;
         if (l == M.nl - 1) {
             blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 16, facx, facy);
+            bstamp();
             break;
         }
         blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
@@ -551,6 +564,7 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
             for (int c = 0; c < 2; ++c) res(l + 1)[c * cplane + j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, c);
         });
         __syncthreads();
+        bstamp();
         facx *= R(0.25);
         facy *= R(0.25);
     }
@@ -567,8 +581,11 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         });
         __syncthreads();
         blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
+        bstamp();
     }
     for (int k = threadIdx.x; k < 2 * n0; k += blockDim.x) cor_g[k] = cor(0)[k];
+    bstamp();
+    if (bt && threadIdx.x == 0) bt[0] = nbt;
 }
 
 template <class R, bool CELL>
@@ -1034,7 +1051,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
         // levels sb .. nl-1 in block 0
         if (blockIdx.x == 0)
             mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
-                                     it == 0 || nb == 1);
+                                     it == 0 || nb == 1, P.trace ? P.trace + 256 : nullptr);
         wstamp(1);
         if (!grid_barrier(bar, err)) return;
         stamp();
@@ -1279,8 +1296,8 @@ public:
     // Prints the phase durations of the last persistent solve (microseconds) to stderr.
     void print_trace() const {
         if (!trace) return;
-        std::vector<unsigned long long> h(256);
-        if (cudaMemcpy(h.data(), trace, 256 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+        std::vector<unsigned long long> h(320);
+        if (cudaMemcpy(h.data(), trace, 320 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) return;
         const int n = (int)std::min<unsigned long long>(h[0], 126);
         std::string line = "hpmg phases (us):", work = "hpmg work done at (us):";
         for (int k = 1; k < n; ++k) {
@@ -1288,15 +1305,23 @@ public:
             snprintf(buf, sizeof(buf), " %.2f", (double)(h[1 + k] - h[k]) / 1000.0);
             line += buf;
         }
-        // block 1 (or block 0 for the coarse levels) finished the work of phase k at
-        // h[129 + k - 1]; relative to the start of the phase (the previous barrier)
+        // block 1 finished the work of phase w + 2 (the first smoothing, phase 1, has no stamp)
+        // at h[129 + w]; relative to the start of that phase (the barrier before it)
         const int nw = (int)std::min<unsigned long long>(h[128], 126);
-        for (int k = 1; k < n && k - 1 < nw; ++k) {
+        for (int w = 0; w < nw && w + 2 < n; ++w) {
             char buf[32];
-            snprintf(buf, sizeof(buf), " %.2f", ((double)h[129 + k - 1] - (double)h[k]) / 1000.0);
+            snprintf(buf, sizeof(buf), " %.2f", ((double)h[129 + w] - (double)h[w + 2]) / 1000.0);
             work += buf;
         }
-        fprintf(stderr, "%s\n%s\n", line.c_str(), work.c_str());
+        // the last coarse-level solve: set-up, each level down, coarsest, each level up, store
+        std::string bot = "hpmg bottom steps (us):";
+        const int nb = (int)std::min<unsigned long long>(h[256], 60);
+        for (int k = 1; k < nb; ++k) {
+            char buf[32];
+            snprintf(buf, sizeof(buf), " %.2f", (double)(h[257 + k] - h[256 + k]) / 1000.0);
+            bot += buf;
+        }
+        fprintf(stderr, "%s\n%s\n%s\n", line.c_str(), work.c_str(), bot.c_str());
     }
 
     template <bool CELL>
@@ -1308,8 +1333,8 @@ public:
         coop_smem = std::max({SmoothSmem<16, 8>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
         if (const char* t = getenv("HPQ_MG_TRACE")) {
             if (t[0] == '1') {
-                HPQ_CUDA(cudaMalloc(&trace, 256 * sizeof(unsigned long long)));
-                HPQ_CUDA(cudaMemset(trace, 0, 256 * sizeof(unsigned long long)));
+                HPQ_CUDA(cudaMalloc(&trace, 320 * sizeof(unsigned long long)));
+                HPQ_CUDA(cudaMemset(trace, 0, 320 * sizeof(unsigned long long)));
             }
         }
         if (std::is_same<R, float>::value) {

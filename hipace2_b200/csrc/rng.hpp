@@ -1,18 +1,25 @@
-// Counter-based random numbers for seeded beam initialisation: Philox4x32-10 (Salmon, Moraes,
-// Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11), uniforms with 53 random
-// bits and Box-Muller normals. Counter = (particle index, sub-stream); key = seed.
+// Counter-based random numbers for seeded initialisation (beams on the host, thermal plasma
+// momenta on the device): Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers:
+// as easy as 1, 2, 3", SC'11), uniforms with 53 random bits and Box-Muller normals.
+// Counter = (particle index, sub-stream); key = seed. Usable from host and device code.
 #pragma once
 
-#include <cmath>
-#include <cstdint>
+#include <math.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define HPQ_RNG_HD __host__ __device__
+#else
+#define HPQ_RNG_HD
+#endif
 
 namespace hpq {
 
 class Philox {
 public:
-    explicit Philox(uint64_t seed) : k0_((uint32_t)seed), k1_((uint32_t)(seed >> 32)) {}
+    HPQ_RNG_HD explicit Philox(uint64_t seed) : k0_((uint32_t)seed), k1_((uint32_t)(seed >> 32)) {}
 
-    void block(uint64_t ctr, uint32_t sub, uint32_t out[4]) const {
+    HPQ_RNG_HD void block(uint64_t ctr, uint32_t sub, uint32_t out[4]) const {
         uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), sub, 0x5eedu};
         uint32_t k0 = k0_, k1 = k1_;
         for (int r = 0; r < 10; ++r) {
@@ -30,31 +37,45 @@ public:
         for (int i = 0; i < 4; ++i) out[i] = c[i];
     }
     // two uniforms in [0, 1) from one block
-    void uniforms2(uint64_t ctr, uint32_t sub, double u[2]) const {
+    HPQ_RNG_HD void uniforms2(uint64_t ctr, uint32_t sub, double u[2]) const {
         uint32_t r[4];
         block(ctr, sub, r);
         u[0] = ((r[0] >> 5) * 67108864.0 + (r[1] >> 6)) * (1.0 / 9007199254740992.0);
         u[1] = ((r[2] >> 5) * 67108864.0 + (r[3] >> 6)) * (1.0 / 9007199254740992.0);
     }
-    double uniform(uint64_t ctr, uint32_t k) const {
+    HPQ_RNG_HD double uniform(uint64_t ctr, uint32_t k) const {
         double u[2];
         uniforms2(ctr, 2 + k, u);
         return u[0];
     }
     // four standard normals (two Box-Muller pairs)
-    void normals(uint64_t ctr, double out[4]) const {
+    HPQ_RNG_HD void normals(uint64_t ctr, double out[4]) const {
         for (uint32_t s = 0; s < 2; ++s) {
             double u[2];
             uniforms2(ctr, s, u);
-            const double r = std::sqrt(-2.0 * std::log(1.0 - u[0]));
+            const double r = ::sqrt(-2.0 * ::log(1.0 - u[0]));
             const double t = 6.283185307179586476925 * u[1];
-            out[2 * s] = r * std::cos(t);
-            out[2 * s + 1] = r * std::sin(t);
+            out[2 * s] = r * ::cos(t);
+            out[2 * s + 1] = r * ::sin(t);
         }
     }
 
 private:
     uint32_t k0_, k1_;
 };
+
+// Thermal momentum draw of the plasma (PlasmaParticleContainerInit.cpp:282,
+// ParticleUtil.H:113-124: u = u_mean + u_std * N(0, 1) per component). The plasma is created
+// anew every step, so the draw has a stream per (species, step): key from the deck's seed and the
+// species, counter = (step << 40) | index of the particle in the species' lattice order.
+HPQ_RNG_HD inline uint64_t plasma_thermal_seed(uint64_t random_seed, int species) {
+    return random_seed * 1000003ull + (uint64_t)species * 7919ull + 424242ull;
+}
+HPQ_RNG_HD inline void plasma_thermal_u(const Philox& rng, int step, long long i, const double mean[3],
+                                        const double stdv[3], double u[3]) {
+    double g[4];
+    rng.normals(((uint64_t)(uint32_t)step << 40) | (uint64_t)i, g);
+    for (int d = 0; d < 3; ++d) u[d] = mean[d] + stdv[d] * g[d];
+}
 
 }  // namespace hpq

@@ -230,6 +230,13 @@ public:
     std::vector<double> salame_log;
     Multigrid<R> mg;
     std::vector<PlasmaDev<R>> pl;
+    // plasma reorder (allocated at the first reorder): attribute scratch, keys, permutation and
+    // per-bin counts, starts and cursors, scan block totals
+    PlasmaDev<R> ro_tmp{};
+    int *ro_key = nullptr, *ro_perm = nullptr, *ro_cnt = nullptr, *ro_start = nullptr, *ro_fill = nullptr,
+        *ro_bsum = nullptr;
+    long long ro_cap = 0, ro_bins = 0;
+    std::vector<bool> reordered;  // species reordered since its last reset (lattice order lost)
     std::vector<double*> px0, py0;
     std::vector<std::vector<double>> hx0, hy0;  // lattice points on the host (output of displacements)
     std::vector<BeamDev> bm;
@@ -396,6 +403,7 @@ public:
                             (void*)p.rv})
                 if (q) cudaFree(q);
         pl.clear();
+        release_reorder();
         hx0.clear(); hy0.clear();
         for (auto* q : px0) cudaFree(q);
         for (auto* q : py0) cudaFree(q);
@@ -535,8 +543,6 @@ public:
                 ihi = std::min(ihi, (int)std::round((P.radius - cfg.prob_lo[0]) / g.dx[0] + 2));
                 jhi = std::min(jhi, (int)std::round((P.radius - cfg.prob_lo[1]) / g.dx[1] + 2));
             }
-            if (P.u_std[0] != 0 || P.u_std[1] != 0 || P.u_std[2] != 0)
-                throw InputError(P.name + ".u_std != 0 (thermal plasma) is not supported");
             // particles whose density is below min_density at t=0 are dropped; the density of a
             // kept particle is re-evaluated at c*t every step
             for (int ip = 0; ip < nppc; ++ip) {
@@ -977,9 +983,15 @@ public:
             const double scale = adj_plasma_scale *
                                  (nppc <= 0 ? 0. : (cfg.normalized_units ? 1. / nppc : g.dx[0] * g.dx[1] * g.dx[2] / nppc));
             if (pl[s].n == 0) continue;
+            PlasmaMomenta m{};
+            for (int d = 0; d < 3; ++d) { m.mean[d] = P.u_mean[d]; m.stdv[d] = P.u_std[d]; }
+            m.thermal = P.thermal ? 1 : 0;
+            m.seed = plasma_thermal_seed((uint64_t)(cfg.has_random_seed ? cfg.random_seed : 0), (int)s);
+            m.step = step;
             hpq_launch(k_plasma_reset<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], px0[s], py0[s], P.density, c_t, scale,
-                                                                         P.u_mean[0], P.u_mean[1], P.u_mean[2], cfg.pc.c);
+                       m, cfg.pc.c, g.xoff, g.dxi[0], g.yoff, g.dxi[1]);
             HPQ_LAUNCH_CHECK();
+            if (s < reordered.size()) reordered[s] = false;
         }
         for (size_t s = 0; s < pl.size(); ++s) {
             if (!pl[s].neutralize || pl[s].n == 0) continue;
@@ -1691,9 +1703,81 @@ public:
         }
     }
 
+    // Stable sort of species sp by bin (k_reorder_* in kernels.cuh), on the library's stream.
+    void reorder_plasma(int sp) {
+        PlasmaDev<R>& P = pl[sp];
+        if (P.n == 0) return;
+        const long long bins = (long long)(nx + 1) * (ny + 1);
+        if (ro_cap < P.n || ro_bins < bins) {
+            release_reorder();
+            ro_cap = 0;
+            for (auto& q : pl) ro_cap = std::max(ro_cap, q.n);
+            ro_bins = bins;
+            const size_t n = (size_t)ro_cap;
+            R** arrs[] = {&ro_tmp.x, &ro_tmp.y, &ro_tmp.w, &ro_tmp.ux, &ro_tmp.uy, &ro_tmp.psi, &ro_tmp.xp, &ro_tmp.yp,
+                          &ro_tmp.uxh, &ro_tmp.uyh, &ro_tmp.psih};
+            for (R** a : arrs) HPQ_CUDA(cudaMalloc(a, n * sizeof(R)));
+            HPQ_CUDA(cudaMalloc(&ro_tmp.valid, n));
+            if (std::is_same<R, float>::value) {
+                HPQ_CUDA(cudaMalloc(&ro_tmp.ru, n * sizeof(float)));
+                HPQ_CUDA(cudaMalloc(&ro_tmp.rv, n * sizeof(float)));
+            }
+            HPQ_CUDA(cudaMalloc(&ro_key, n * sizeof(int)));
+            HPQ_CUDA(cudaMalloc(&ro_perm, n * sizeof(int)));
+            HPQ_CUDA(cudaMalloc(&ro_cnt, (size_t)bins * sizeof(int)));
+            HPQ_CUDA(cudaMalloc(&ro_start, (size_t)bins * sizeof(int)));
+            HPQ_CUDA(cudaMalloc(&ro_fill, (size_t)bins * sizeof(int)));
+            HPQ_CUDA(cudaMalloc(&ro_bsum, (size_t)((bins + 1023) / 1024) * sizeof(int)));
+        }
+        PlasmaDev<R> T = ro_tmp;
+        T.n = P.n;
+        if (!P.ru) T.ru = T.rv = nullptr;
+        const PlasmaSpecies& S_ = cfg.plasmas[sp];
+        const int nblk = (int)((bins + 1023) / 1024);
+        const unsigned pb = blocks_for(P.n, 256);
+        HPQ_CUDA(cudaMemsetAsync(ro_cnt, 0, (size_t)bins * sizeof(int), st));
+        hpq_launch(k_reorder_keys<R>, dim3(pb), dim3(256), 0, st, P, g, S_.reorder_idx_type[0], S_.reorder_idx_type[1],
+                   ro_key, ro_cnt);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_scan_blocks, dim3(nblk), dim3(1024), 0, st, (const int*)ro_cnt, ro_start, ro_bsum, bins);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_scan_totals, dim3(1), dim3(1024), 0, st, ro_bsum, nblk);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_scan_add, dim3(blocks_for(bins, 256)), dim3(256), 0, st, ro_start, (const int*)ro_bsum, ro_fill, bins);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_reorder_scatter, dim3(pb), dim3(256), 0, st, (const int*)ro_key, P.n, ro_fill, ro_perm);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_reorder_bins, dim3(blocks_for(bins, 256)), dim3(256), 0, st, (const int*)ro_start,
+                   (const int*)ro_cnt, bins, ro_perm);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_reorder_move<R>, dim3(pb), dim3(256), 0, st, P, T, (const int*)ro_perm, 1);
+        HPQ_LAUNCH_CHECK();
+        hpq_launch(k_reorder_move<R>, dim3(pb), dim3(256), 0, st, P, T, (const int*)ro_perm, 0);
+        HPQ_LAUNCH_CHECK();
+        if (reordered.size() < pl.size()) reordered.resize(pl.size(), false);
+        reordered[sp] = true;
+    }
+    void release_reorder() {
+        for (void* q : {(void*)ro_tmp.x, (void*)ro_tmp.y, (void*)ro_tmp.w, (void*)ro_tmp.ux, (void*)ro_tmp.uy,
+                        (void*)ro_tmp.psi, (void*)ro_tmp.xp, (void*)ro_tmp.yp, (void*)ro_tmp.uxh, (void*)ro_tmp.uyh,
+                        (void*)ro_tmp.psih, (void*)ro_tmp.valid, (void*)ro_tmp.ru, (void*)ro_tmp.rv, (void*)ro_key,
+                        (void*)ro_perm, (void*)ro_cnt, (void*)ro_start, (void*)ro_fill, (void*)ro_bsum})
+            if (q) cudaFree(q);
+        ro_tmp = PlasmaDev<R>{};
+        ro_key = ro_perm = ro_cnt = ro_start = ro_fill = ro_bsum = nullptr;
+        ro_cap = ro_bins = 0;
+    }
+
     // one slice: replay the captured graph, or launch kernel by kernel (profiling mode)
     void solve_slice(int islice) override {
         if (islice != cur_islice) throw InputError("slices must be solved from the head (nz-1) to the tail (0)");
+        // ReorderParticles(islice) at the start of SolveOneSlice (Hipace.cpp:594-595); not in the
+        // adjoint forward, whose reverse sweep follows particles by index from slice to slice
+        if (!adj_fwd)
+            for (size_t sp = 0; sp < pl.size(); ++sp) {
+                const int period = cfg.plasmas[sp].reorder_period;
+                if (period > 0 && islice % period == 0) reorder_plasma((int)sp);
+            }
         // the SALAME step runs kernel by kernel: its iterations end on host decisions
         if (use_graphs && !profiling && !sal_step) {
             if (!slice_exec) capture_slice();
@@ -1956,13 +2040,26 @@ public:
         const size_t n = p.n;
         const R* arr[11] = {p.x, p.y, p.w, p.ux, p.uy, p.psi, p.xp, p.yp, p.uxh, p.uyh, p.psih};
         std::vector<R> tmp(n);
+        // lattice points of the particles in their current order: the host copy, or, after a
+        // reorder, the points in cell units carried by the particles
+        std::vector<double> lx, ly;
+        const bool perm = p.ru && sp < (int)reordered.size() && reordered[sp];
+        if (perm) {
+            std::vector<float> f(n);
+            lx.resize(n);
+            ly.resize(n);
+            HPQ_CUDA(cudaMemcpy(f.data(), p.ru, n * sizeof(float), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) lx[i] = g.xoff + (double)f[i] * g.dx[0];
+            HPQ_CUDA(cudaMemcpy(f.data(), p.rv, n * sizeof(float), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) ly[i] = g.yoff + (double)f[i] * g.dx[1];
+        }
         for (int k = 0; k < 11; ++k) {
             HPQ_CUDA(cudaMemcpy(tmp.data(), arr[k], n * sizeof(R), cudaMemcpyDeviceToHost));
             // x, y, xp, yp are displacements from the lattice point, psi, psih are psi - 1 when
             // p.ru is set
             const std::vector<double>* ref = nullptr;
-            if (p.ru && (k == 0 || k == 6)) ref = &hx0.at(sp);
-            if (p.ru && (k == 1 || k == 7)) ref = &hy0.at(sp);
+            if (p.ru && (k == 0 || k == 6)) ref = perm ? &lx : &hx0.at(sp);
+            if (p.ru && (k == 1 || k == 7)) ref = perm ? &ly : &hy0.at(sp);
             const double off = (p.ru && (k == 5 || k == 10)) ? 1.0 : 0.0;
             for (size_t i = 0; i < n; ++i) out12[k * n + i] = (double)tmp[i] + (ref ? (*ref)[i] : 0.0) + off;
         }

@@ -850,6 +850,7 @@ public:
                 ihi = std::min(ihi, (int)std::round((P.radius - cfg.prob_lo[0]) / dx + 2));
                 jhi = std::min(jhi, (int)std::round((P.radius - cfg.prob_lo[1]) / dy + 2));
             }
+            const hpq::Philox rng(hpq::plasma_thermal_seed((uint64_t)(cfg.has_random_seed ? cfg.random_seed : 0), (int)s));
             for (int ip = 0; ip < nppc; ++ip) {
                 const int ixp = ip % P.ppc[0], iyp = ip / P.ppc[0];
                 const double r0 = (0.5 + ixp) / P.ppc[0], r1 = (0.5 + iyp) / P.ppc[1];
@@ -863,10 +864,12 @@ public:
                             y < cfg.particle_lo[1] || rsq > P.radius * P.radius ||
                             rsq < P.hollow_core_radius * P.hollow_core_radius || P.density.eval(v) <= P.min_density)
                             continue;
-                        const double u0 = P.u_mean[0], u1 = P.u_mean[1], u2 = P.u_mean[2];
-                        if (P.u_std[0] != 0 || P.u_std[1] != 0 || P.u_std[2] != 0) {
-                            error = "plasma u_std != 0 needs a random stream; not restated in the oracle";
-                        }
+                        // get_gaussian_random_momentum (ParticleUtil.H:113-124) from the
+                        // counter-based stream shared with the library (rng.hpp); the counter is
+                        // the particle's index in this lattice order and the step
+                        double u[3] = {P.u_mean[0], P.u_mean[1], P.u_mean[2]};
+                        if (P.thermal) hpq::plasma_thermal_u(rng, cur_step, (long long)pl.x.size(), P.u_mean, P.u_std, u);
+                        const double u0 = u[0], u1 = u[1], u2 = u[2];
                         pl.x.push_back(x); pl.y.push_back(y);
                         pl.w.push_back(P.density.eval(v) * scale);
                         pl.ux.push_back(u0 * cfg.pc.c); pl.uy.push_back(u1 * cfg.pc.c);
@@ -1358,8 +1361,43 @@ public:
 
     // -------------------------------------------------------------- one slice
     // Hipace::SolveOneSlice (Hipace.cpp:556-728), level 0 only
+    // PlasmaParticleContainer::ReorderParticles (PlasmaParticleContainer.cpp:197-208; the CPU
+    // build's SortParticlesByCell): a stable sort of the particles by the cell (index type 0) or
+    // nearest node (1) they sit in. Cell centres sit at integer t = (x - xoff) / dx, so the cell is
+    // floor(t + 1/2) in [0, n-1], the node floor(t + 1) in [0, n]; key = j (nx + 1) + i.
+    void reorder_plasma(int s) {
+        Plasma& pl = plasmas[s];
+        const hpq::PlasmaSpecies& P = cfg.plasmas[s];
+        const size_t n = pl.n();
+        auto bin = [](double t, int node, int nc) {
+            const double f = std::floor(t + (node ? 1.0 : 0.5));
+            const int hi = node ? nc : nc - 1;
+            return f < 0 ? 0 : (f > hi ? hi : (int)f);
+        };
+        std::vector<long long> key(n);
+        for (size_t i = 0; i < n; ++i)
+            key[i] = (long long)bin((pl.y[i] - yoff) * dyi, P.reorder_idx_type[1], ny) * (nx + 1) +
+                     bin((pl.x[i] - xoff) * dxi, P.reorder_idx_type[0], nx);
+        std::vector<size_t> perm(n);
+        for (size_t i = 0; i < n; ++i) perm[i] = i;
+        std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return key[a] < key[b]; });
+        for (auto* v : {&pl.x, &pl.y, &pl.w, &pl.ux, &pl.uy, &pl.psi, &pl.x_prev, &pl.y_prev, &pl.ux_h, &pl.uy_h, &pl.psi_h}) {
+            std::vector<double> t(n);
+            for (size_t k = 0; k < n; ++k) t[k] = (*v)[perm[k]];
+            v->swap(t);
+        }
+        std::vector<uint8_t> t(n);
+        for (size_t k = 0; k < n; ++k) t[k] = pl.valid[perm[k]];
+        pl.valid.swap(t);
+    }
+
     void solve_one_slice(int islice, int step) {
         const bool ex = cfg.explicit_solver;
+        // ReorderParticles(islice) at the start of SolveOneSlice (Hipace.cpp:594-595)
+        for (size_t s = 0; s < plasmas.size(); ++s) {
+            const int period = cfg.plasmas[s].reorder_period;
+            if (period > 0 && islice % period == 0) reorder_plasma((int)s);
+        }
         if (islice == nz - 1)
             for (size_t b = 0; b < cfg.beams.size(); ++b) load_beam_slice((int)b, islice, bthis[b]);
         // InitializeSlices (Fields.cpp:535-586)

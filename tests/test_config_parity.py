@@ -109,7 +109,10 @@ def test_blowout_255_whole_step_matches_oracle():
 def test_channel_1023_head_slices_match_oracle():
     g, o = pair("channel_1023")
     nz = g.n_cell[2]
-    comps = ["Psi", "Ez", "ExmBy", "Bx", "By", "jz_beam", "rhomjz", "chi"]
+    # rhomjz is left out here: ahead of the wake the electrons' charge cancels the ion background
+    # to ~1e-6, so its relative error measures that cancellation (it is compared over a whole
+    # step in the blowout test); Psi, solved from it, is compared
+    comps = ["Psi", "Ez", "ExmBy", "Bx", "By", "jz_beam", "chi"]
     g.begin_step(0)
     o.begin_step(0)
     checked = 0
