@@ -26,7 +26,8 @@ EXPORTS = ("hpq_create", "hpq_destroy", "hpq_last_error", "hpq_create_error", "h
            "hpq_get_diag", "hpq_insitu_size", "hpq_get_insitu", "hpq_plasma_count", "hpq_get_plasma", "hpq_set_graphs",
            "hpq_set_deterministic", "hpq_synchronize", "hpq_stream", "hpq_get_counters", "hpq_set_profiling",
            "hpq_get_profile", "hpq_poisson_dirichlet_noalloc", "hpq_adjoint_nparams", "hpq_adjoint_grad", "hpq_n_cell",
-           "hpq_max_step", "hpq_time", "hpq_diag_count", "hpq_beam_name", "hpq_salame_log")
+           "hpq_max_step", "hpq_time", "hpq_diag_count", "hpq_beam_name", "hpq_salame_log",
+           "hpq_beam_slice_count", "hpq_get_beam_slice", "hpq_put_beam_slice", "hpq_set_time")
 
 _lib = None
 
@@ -86,6 +87,10 @@ def load_library(path=None):
         "hpq_set_profiling": ([vp, i32], i32),
         "hpq_get_profile": ([vp, cp, dp, lp], i32),
         "hpq_poisson_dirichlet_noalloc": ([vp, vp, i32, i32, ctypes.c_double, ctypes.c_double, vp], i32),
+        "hpq_beam_slice_count": ([vp, i32, i32, lp], i32),
+        "hpq_get_beam_slice": ([vp, i32, i32] + [dp] * 7 + [lp], i32),
+        "hpq_put_beam_slice": ([vp, i32, i32] + [dp] * 7 + [lp, i64], i32),
+        "hpq_set_time": ([vp, ctypes.c_double], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -222,6 +227,25 @@ class Hipace:
             res["id"] = np.empty(n, dtype=np.int64)
         self._check(self.L.hpq_get_beam(self.h, b, *[_dp(res[k]) for k in BEAM_ATTRS], _lp(res["id"])))
         return res
+
+    # ---- time-step pipeline hand-off (hipace2_b200/pipeline.py)
+    def get_beam_slice(self, b, islice):
+        """Particles that slice `islice` of the current (or last) step hands to the next step."""
+        n = ctypes.c_int64()
+        self._check(self.L.hpq_beam_slice_count(self.h, b, islice, ctypes.byref(n)))
+        res = {k: np.empty(n.value) for k in BEAM_ATTRS}
+        res["id"] = np.empty(n.value, dtype=np.int64)
+        self._check(self.L.hpq_get_beam_slice(self.h, b, islice, *[_dp(res[k]) for k in BEAM_ATTRS], _lp(res["id"])))
+        return res
+
+    def put_beam_slice(self, b, islice, beam):
+        """Particles of slice `islice` of the current step, received from the previous step."""
+        arrs = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in BEAM_ATTRS]
+        ids = np.ascontiguousarray(beam["id"], dtype=np.int64)
+        self._check(self.L.hpq_put_beam_slice(self.h, b, islice, *[_dp(a) for a in arrs], _lp(ids), len(ids)))
+
+    def set_time(self, t):
+        self._check(self.L.hpq_set_time(self.h, float(t)))
 
     def get_field(self, comp):
         nx, ny, _ = self.n_cell

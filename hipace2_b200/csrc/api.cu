@@ -135,13 +135,6 @@ int hpq_init(hpq_handle* h) {
                  " is not supported: the library deposits and gathers with order 2";
         return HPQ_ERR_INPUT;
     }
-    if (h)
-        for (const auto& b : h->cfg.beams)
-            if (b.use_external) {
-                h->err = "input '" + b.name + ".external_E/B(x,y,z,t)' is not supported: external beam fields "
-                         "are implemented in the CPU restatement only";
-                return HPQ_ERR_INPUT;
-            }
     return guarded(h, [&] {
         if (h->initialised) { h->err = "hpq_init called twice"; return (int)HPQ_ERR_STATE; }
         if (h->precision == HPQ_MIXED) h->sim.reset(new hpq::Sim<float>(h->cfg));
@@ -180,6 +173,51 @@ int hpq_get_beam(hpq_handle* h, int beam, double* x, double* y, double* z, doubl
         if (int r = need_init(h)) return r;
         if (beam < 0 || beam >= (int)h->cfg.beams.size()) return (int)HPQ_ERR_ARG;
         h->sim->get_beam(beam, x, y, z, w, ux, uy, uz, (long long*)id);
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_beam_slice_count(hpq_handle* h, int beam, int islice, int64_t* n) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (!n || beam < 0 || beam >= (int)h->cfg.beams.size() || islice < 0 || islice >= h->cfg.n_cell[2])
+            return (int)HPQ_ERR_ARG;
+        *n = h->sim->beam_slice_count(beam, islice);
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_get_beam_slice(hpq_handle* h, int beam, int islice, double* x, double* y, double* z, double* w, double* ux,
+                       double* uy, double* uz, int64_t* id) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (beam < 0 || beam >= (int)h->cfg.beams.size() || islice < 0 || islice >= h->cfg.n_cell[2])
+            return (int)HPQ_ERR_ARG;
+        h->sim->get_beam_slice(beam, islice, x, y, z, w, ux, uy, uz, (long long*)id);
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_put_beam_slice(hpq_handle* h, int beam, int islice, const double* x, const double* y, const double* z,
+                       const double* w, const double* ux, const double* uy, const double* uz, const int64_t* id,
+                       int64_t n) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (beam < 0 || beam >= (int)h->cfg.beams.size() || islice < 0 || islice >= h->cfg.n_cell[2] || n < 0 ||
+            (n > 0 && (!x || !y || !z || !w || !ux || !uy || !uz || !id)))
+            return (int)HPQ_ERR_ARG;
+        if (!h->in_step) { h->err = "hpq_put_beam_slice outside a step"; return (int)HPQ_ERR_STATE; }
+        h->sim->put_beam_slice(beam, islice, x, y, z, w, ux, uy, uz, (const long long*)id, n);
+        return (int)HPQ_OK;
+    });
+}
+
+int hpq_set_time(hpq_handle* h, double t) {
+    return guarded(h, [&] {
+        if (int r = need_init(h)) return r;
+        if (h->in_step) { h->err = "hpq_set_time inside a step"; return (int)HPQ_ERR_STATE; }
+        if (!std::isfinite(t)) return (int)HPQ_ERR_ARG;
+        h->sim->set_time(t);
         return (int)HPQ_OK;
     });
 }

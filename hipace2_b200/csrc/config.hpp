@@ -64,7 +64,7 @@ struct BeamSpecies {
     double zmin = -1e300, zmax = 1e300, radius = 1e300;
     bool do_salame = false;          // <beam>.do_salame (BeamParticleContainer.cpp:66)
     // external fields of the beam push, Ex Ey Ez Bx By Bz as functions of (x, y, z, t)
-    // (<beam>.external_E/B(x,y,z,t), BeamParticleContainer.cpp:72-86; CPU restatement only)
+    // (<beam>.external_E/B(x,y,z,t), BeamParticleContainer.cpp:72-86)
     bool use_external = false;
     Expr external[6];
     double position_mean[3] = {0, 0, 0};

@@ -50,6 +50,9 @@ struct BeamDev {
     int n_subcycles;
     int do_z_push;
     long long cap;
+    // external fields Ex Ey Ez Bx By Bz (x, y, z, t) of the beam push in device memory, or null
+    // (<beam>.external_E/B(x,y,z,t), BeamParticleContainer.cpp:72-86)
+    const Expr* ext;
 };
 
 template <class R>
@@ -96,6 +99,8 @@ struct Ctl {
     int adj_ckpt, adj_pad;
     // beam time step of this step (hipace.dt, shortened to end on hipace.max_time)
     double beam_dt;
+    // physical time at the start of this step (external beam fields)
+    double phys_time;
 };
 
 struct Geo {
@@ -775,6 +780,20 @@ __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restr
             if (!enforce_bc<double>(g, xp, yp, ux, uy)) { absorbed = true; break; }
             double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
             gather<R, double>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
+            if (B.ext) {
+                // ApplyExternalField (ExternalFields.H:29-56) at the step's start time; Ex, Ey
+                // here are ExmBy, EypBx
+                const double at[4] = {xp, yp, zp, ctl->phys_time};
+                double f[6];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) f[q] = B.ext[q].eval(at);
+                Ex += f[0] - clight * f[4];
+                Ey += f[1] + clight * f[3];
+                Ez += f[2];
+                Bx += f[3];
+                By += f[4];
+                Bz += f[5];
+            }
             const double uxn = ux + dtb * cmr * (Ex + (clight - uz * gpi) * By + uy * gpi * Bz);
             const double uyn = uy + dtb * cmr * (Ey + (uz * gpi - clight) * Bx - ux * gpi * Bz);
             const double uxi = (uxn + ux) * 0.5, uyi = (uyn + uy) * 0.5;
@@ -990,6 +1009,15 @@ __global__ void __launch_bounds__(32) k_bin_scatter(const int* __restrict__ key,
         __syncwarp();
         if (k >= 0 && (m & lt) == 0) cnt[k] += __popc(m);
         __syncwarp();
+    }
+}
+
+// particles received for one slice (time-step pipeline): sub-cycle count 0, valid where w != 0
+__global__ void k_beam_slice_flags(BeamBuf dst, long long c0, long long n) {
+    HPQ_PDL_ENTRY();
+    for (long long k = gtid(); k < n; k += gstride()) {
+        dst.nsub[c0 + k] = 0;
+        dst.valid[c0 + k] = dst.w[c0 + k] != 0.0;
     }
 }
 

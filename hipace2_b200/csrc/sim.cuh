@@ -50,6 +50,16 @@ public:
     virtual void set_beam(int b, const double* x, const double* y, const double* z, const double* w, const double* ux,
                           const double* uy, const double* uz, const long long* id, long long n) = 0;
     virtual long long beam_count(int b) = 0;
+    // time-step pipeline hand-off (MultiBuffer.cpp:181-430): the particles that slice islice of
+    // the current (or last) step hands to the next step, and the particles of slice islice of the
+    // current step received from the rank that ran the previous step
+    virtual long long beam_slice_count(int b, int islice) = 0;
+    virtual void get_beam_slice(int b, int islice, double* x, double* y, double* z, double* w, double* ux, double* uy,
+                                double* uz, long long* id) = 0;
+    virtual void put_beam_slice(int b, int islice, const double* x, const double* y, const double* z, const double* w,
+                                const double* ux, const double* uy, const double* uz, const long long* id,
+                                long long n) = 0;
+    virtual void set_time(double t) = 0;
     virtual void get_beam(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
                           long long* id) = 0;
     virtual void begin_step(int step) = 0;
@@ -804,6 +814,8 @@ public:
         std::memset(&b, 0, sizeof(b));
     }
     static void free_beam(BeamDev& d) {
+        if (d.ext) cudaFree(const_cast<Expr*>(d.ext));
+        d.ext = nullptr;
         for (int q = 0; q < 2; ++q) {
             free_buf(d.buf[q]); free_buf(d.carry[q]);
             if (d.start[q]) cudaFree(d.start[q]);
@@ -832,6 +844,12 @@ public:
         if (d.buf[0].x == nullptr || nin > d.cap) {
             free_beam(d);
             invalidate_graph();
+            if (B.use_external) {
+                Expr* e = nullptr;
+                HPQ_CUDA(cudaMalloc(&e, 6 * sizeof(Expr)));
+                HPQ_CUDA(cudaMemcpy(e, B.external, 6 * sizeof(Expr), cudaMemcpyHostToDevice));
+                d.ext = e;
+            }
             d.cap = std::max<long long>(nin, 1);
             for (int q = 0; q < 2; ++q) {
                 alloc_buf(d.buf[q], d.cap);
@@ -901,6 +919,67 @@ public:
         upload_beam(b, x, y, z, w, ux, uy, uz, id, n);
     }
 
+    // ---- time-step pipeline hand-off
+    // out_par: parity of the store the current (or last) step writes for the next step
+    int out_par = 1;
+    std::vector<long long> put_cursor;
+    long long beam_slice_count(int b, int islice) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        int n = 0;
+        HPQ_CUDA(cudaMemcpy(&n, bm.at(b).count[out_par] + islice, sizeof(int), cudaMemcpyDeviceToHost));
+        return n;
+    }
+    void get_beam_slice(int b, int islice, double* x, double* y, double* z, double* w, double* ux, double* uy,
+                        double* uz, long long* id) override {
+        HPQ_CUDA(cudaStreamSynchronize(st));
+        const BeamDev& d = bm.at(b);
+        int n = 0, s0 = 0;
+        HPQ_CUDA(cudaMemcpy(&n, d.count[out_par] + islice, sizeof(int), cudaMemcpyDeviceToHost));
+        HPQ_CUDA(cudaMemcpy(&s0, d.start[out_par] + islice, sizeof(int), cudaMemcpyDeviceToHost));
+        if (n == 0) return;
+        const BeamBuf& src = d.buf[out_par];
+        double* outs[7] = {x, y, z, w, ux, uy, uz};
+        const double* ins[7] = {src.x, src.y, src.z, src.w, src.ux, src.uy, src.uz};
+        for (int a = 0; a < 7; ++a)
+            HPQ_CUDA(cudaMemcpy(outs[a], ins[a] + s0, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+        HPQ_CUDA(cudaMemcpy(id, src.id + s0, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost));
+    }
+    // Appends the particles of slice islice to the store the current step reads. Slices come from
+    // the head down; the first one of a step (nz - 1) empties the store. Each must arrive before
+    // the slice graph that reads it: slice islice is read by the solves of slices islice + 1 (its
+    // jx/jy beam deposit) and islice.
+    void put_beam_slice(int b, int islice, const double* x, const double* y, const double* z, const double* w,
+                        const double* ux, const double* uy, const double* uz, const long long* id,
+                        long long n) override {
+        BeamDev& d = bm.at(b);
+        if (put_cursor.size() < bm.size()) put_cursor.resize(bm.size(), 0);
+        if (islice == nz - 1) {
+            put_cursor[b] = 0;
+            HPQ_CUDA(cudaMemsetAsync(d.count[parity], 0, nz * sizeof(int), st));
+            HPQ_CUDA(cudaMemsetAsync(d.start[parity], 0, nz * sizeof(int), st));
+        }
+        const long long c0 = put_cursor[b];
+        if (c0 + n > d.cap)
+            throw InputError("hpq_put_beam_slice: the received particles exceed the beam's store (" +
+                             std::to_string(d.cap) + ")");
+        const BeamBuf& dst = d.buf[parity];
+        if (n > 0) {
+            const double* ins[7] = {x, y, z, w, ux, uy, uz};
+            double* outs[7] = {dst.x, dst.y, dst.z, dst.w, dst.ux, dst.uy, dst.uz};
+            for (int a = 0; a < 7; ++a)
+                HPQ_CUDA(cudaMemcpyAsync(outs[a] + c0, ins[a], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+            HPQ_CUDA(cudaMemcpyAsync(dst.id + c0, id, (size_t)n * sizeof(long long), cudaMemcpyHostToDevice, st));
+            hpq_launch(k_beam_slice_flags, dim3(blocks_for(n, 256)), dim3(256), 0, st, dst, c0, n);
+            HPQ_LAUNCH_CHECK();
+        }
+        const int s0 = (int)c0, cnt = (int)n;
+        HPQ_CUDA(cudaMemcpyAsync(d.start[parity] + islice, &s0, sizeof(int), cudaMemcpyHostToDevice, st));
+        HPQ_CUDA(cudaMemcpyAsync(d.count[parity] + islice, &cnt, sizeof(int), cudaMemcpyHostToDevice, st));
+        put_cursor[b] = c0 + n;
+        HPQ_CUDA(cudaStreamSynchronize(st));  // the caller's buffers (and s0, cnt) are released
+    }
+    void set_time(double t) override { physical_time = t; }
+
     long long beam_count(int b) override {
         HPQ_CUDA(cudaStreamSynchronize(st));
         std::vector<int> cnt(nz);
@@ -964,6 +1043,7 @@ public:
     // deposit the ion background
     void begin_step(int step) override {
         cur_step = step;
+        out_par = 1 - parity;
         HPQ_CUDA(cudaMemsetAsync(S.base, 0, S.cstride * ncomp_alloc * sizeof(R), st));
         // SALAME runs in step 0 only (MultiBeam::isSalameNow, MultiBeam.cpp:128-139); the host
         // needs each SALAME beam's particle count per slice to decide slice by slice
@@ -1006,6 +1086,7 @@ public:
         ctl_h->step_parity = parity;
         const StepTime T = step_time(physical_time, cfg.dt, cfg.max_time);
         ctl_h->beam_dt = T.dt;
+        ctl_h->phys_time = physical_time;
         next_time = T.next;
         for (size_t b = 0; b < cfg.beams.size() && b < (size_t)kMaxBeams; ++b) {
             const bool on = insitu_beam_d[b] && do_diagnostics(cfg.beams[b].insitu_period, step, cfg.max_step,

@@ -84,6 +84,28 @@ int hpq_beam_count(hpq_handle* h, int beam, int64_t* n);
 int hpq_get_beam(hpq_handle* h, int beam, double* x, double* y, double* z, double* w,
                  double* ux, double* uy, double* uz, int64_t* id);
 
+/* Time-step pipeline across processes (one GPU each): rank r runs steps r, r+N, ... and hands
+ * each finished beam slice to rank r+1, which replaces the reference's MultiBuffer transfers
+ * (src/utils/MultiBuffer.cpp:181-430, put_data/get_data around SolveOneSlice,
+ * src/Hipace.cpp:581-583, 700-705). The transport is the caller's (hipace2_b200/pipeline.py).
+ * hpq_beam_slice_count / hpq_get_beam_slice: the particles that slice `islice` of the current
+ *   (or last) step hands to the next step, after the slice's beam push and slip bookkeeping;
+ *   final once slice islice - 1 has been solved (hpq_solve_slice), or after hpq_end_step for
+ *   slice 0.
+ * hpq_put_beam_slice: inside a step, the particles of slice `islice` of this step received
+ *   from the rank that ran the previous step (the step's own beam is replaced). Slices are put
+ *   from the head (nz-1) down, nz-1 first, and slice islice must be put before
+ *   hpq_solve_slice(islice + 1) (its jx/jy beam deposit reads it). Weight-0 particles are
+ *   invalid. HPQ_ERR_INPUT if the particles exceed the beam's store.
+ * hpq_set_time: physical time at which the next step starts (each rank runs every N-th step). */
+int hpq_beam_slice_count(hpq_handle* h, int beam, int islice, int64_t* n);
+int hpq_get_beam_slice(hpq_handle* h, int beam, int islice, double* x, double* y, double* z, double* w,
+                       double* ux, double* uy, double* uz, int64_t* id);
+int hpq_put_beam_slice(hpq_handle* h, int beam, int islice, const double* x, const double* y,
+                       const double* z, const double* w, const double* ux, const double* uy,
+                       const double* uz, const int64_t* id, int64_t n);
+int hpq_set_time(hpq_handle* h, double t);
+
 /* One full time step (all slices, head to tail); replaces the body of the step loop of
  * Hipace::Evolve (src/Hipace.cpp:401-492). */
 int hpq_step(hpq_handle* h, int step);

@@ -2367,6 +2367,35 @@ int oracle_set_beam(OracleHandle* h, int b, const double* x, const double* y, co
     return 0;
 }
 
+// Time-step pipeline hand-off (MultiBuffer.cpp:181-430): after slice islice of a step, store
+// slice islice holds what it hands to the next step; a rank that runs the next step puts the
+// received particles there (slices from the head down, nz-1 first, which empties the store).
+int64_t oracle_beam_slice_count(OracleHandle* h, int b, int islice) {
+    return (int64_t)h->sim->store.at(b).at(islice).p.size();
+}
+int oracle_get_beam_slice(OracleHandle* h, int b, int islice, double* x, double* y, double* z, double* w, double* ux,
+                          double* uy, double* uz, int64_t* id) {
+    const auto& v = h->sim->store.at(b).at(islice).p;
+    for (size_t k = 0; k < v.size(); ++k) {
+        x[k] = v[k].x; y[k] = v[k].y; z[k] = v[k].z; w[k] = v[k].w;
+        ux[k] = v[k].ux; uy[k] = v[k].uy; uz[k] = v[k].uz; id[k] = v[k].id;
+    }
+    return 0;
+}
+int oracle_put_beam_slice(OracleHandle* h, int b, int islice, const double* x, const double* y, const double* z,
+                          const double* w, const double* ux, const double* uy, const double* uz, const int64_t* id,
+                          int64_t n) {
+    auto& st = h->sim->store.at(b);
+    if (islice == (int)st.size() - 1)
+        for (auto& sl : st) { sl.p.clear(); sl.num_nonslipped = 0; }
+    auto& sl = st.at(islice);
+    sl.p.clear();
+    for (int64_t k = 0; k < n; ++k) sl.p.push_back({x[k], y[k], z[k], w[k], ux[k], uy[k], uz[k], id[k], 0, w[k] != 0.0});
+    sl.num_nonslipped = sl.p.size();
+    return 0;
+}
+void oracle_set_time(OracleHandle* h, double t) { h->sim->physical_time = t; }
+
 // number of stored particles of beam b (all slices), and a copy in slice-descending order
 int64_t oracle_beam_count(OracleHandle* h, int b) {
     auto& s = *h->sim;

@@ -69,6 +69,11 @@ def lib():
         L.oracle_adjoint_nparams.argtypes = [vp]
         L.oracle_adjoint_nparams.restype = i32
         L.oracle_adjoint.argtypes = [vp, dp, dp, dp]
+        L.oracle_beam_slice_count.argtypes = [vp, i32, i32]
+        L.oracle_beam_slice_count.restype = i64
+        L.oracle_get_beam_slice.argtypes = [vp, i32, i32] + [dp] * 7 + [lp]
+        L.oracle_put_beam_slice.argtypes = [vp, i32, i32] + [dp] * 7 + [lp, i64]
+        L.oracle_set_time.argtypes = [vp, ctypes.c_double]
         L.oracle_error.argtypes = [vp]
         L.oracle_error.restype = cp
         _lib = L
@@ -121,6 +126,21 @@ class Oracle:
         n = len(arrs[0])
         self.L.oracle_set_beam(self.h, b, *[_dp(a) for a in arrs],
                                _lp(ids) if ids is not None else None, n)
+
+    def get_beam_slice(self, b, islice):
+        n = self.L.oracle_beam_slice_count(self.h, b, islice)
+        out = {k: np.zeros(n) for k in BEAM_ATTRS}
+        out["id"] = np.zeros(n, dtype=np.int64)
+        self.L.oracle_get_beam_slice(self.h, b, islice, *[_dp(out[k]) for k in BEAM_ATTRS], _lp(out["id"]))
+        return out
+
+    def put_beam_slice(self, b, islice, beam):
+        arrs = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in BEAM_ATTRS]
+        ids = np.ascontiguousarray(beam["id"], dtype=np.int64)
+        self.L.oracle_put_beam_slice(self.h, b, islice, *[_dp(a) for a in arrs], _lp(ids), len(ids))
+
+    def set_time(self, t):
+        self.L.oracle_set_time(self.h, float(t))
 
     def get_beam(self, b):
         n = self.L.oracle_beam_count(self.h, b)
