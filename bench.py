@@ -334,53 +334,159 @@ def e2e_steps(text, args, beam_w, w, k, world, reduce_max, torch):
     return value, h2d // k, d2h // k
 
 
+def make_sim_env(text, precision, env=None, deterministic=False):
+    """make_sim with environment switches read by the library at set-up (HPQ_DST, HPQ_MG_REFINE)."""
+    import hipace2_b200 as hp
+    env = env or {}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        sim = hp.Hipace(text, precision=hp.MIXED if precision == "mixed" else hp.PLAIN_FP64, graphs=True,
+                        deterministic=deterministic)
+        sim.init_data()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    return sim
+
+
+def rel_l2(a, b):
+    import numpy as np
+    n = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / n if n > 0 else float(np.linalg.norm(a - b))
+
+
+def beam_moment_errors(m, d):
+    """Per-slice beam centroid and normalized emittance of two in-situ records (a run and its FP64
+    reference; BeamParticleContainer.cpp:476-548 moments): the centroid error as the weighted L2
+    of the centroid difference over the weighted L2 of the rms size, the emittance error as a
+    relative weighted L2, over the slices holding particles; and the projected emittance error."""
+    import numpy as np
+    out = {}
+    w = d["sum(w)"]
+    sel = w > 0
+    for ax, u in (("x", "ux"), ("y", "uy")):
+        def emit(r):
+            vx = r["[%s^2]" % ax] - r["[%s]" % ax] ** 2
+            vu = r["[%s^2]" % u] - r["[%s]" % u] ** 2
+            cx = r["[%s*%s]" % (ax, u)] - r["[%s]" % ax] * r["[%s]" % u]
+            return np.sqrt(np.maximum(vx * vu - cx * cx, 0.0)), np.sqrt(np.maximum(vx, 0.0))
+        em, sm = emit(m)
+        ed, sd = emit(d)
+        ww = w[sel]
+        out["centroid_%s_err_over_rms_size" % ax] = float(
+            np.sqrt(np.sum(ww * (m["[%s]" % ax][sel] - d["[%s]" % ax][sel]) ** 2) / np.sum(ww * sd[sel] ** 2)))
+        out["emittance_%s_rel_l2" % ax] = float(np.sqrt(np.sum(ww * (em[sel] - ed[sel]) ** 2) / np.sum(ww * ed[sel] ** 2)))
+
+        def proj(r):
+            t = r["sum"]
+            names = hp_insitu_names()
+            g = {k: t[i] for i, k in enumerate(names)}
+            vx = g["[%s^2]" % ax] - g["[%s]" % ax] ** 2
+            vu = g["[%s^2]" % u] - g["[%s]" % u] ** 2
+            cx = g["[%s*%s]" % (ax, u)] - g["[%s]" % ax] * g["[%s]" % u]
+            return np.sqrt(max(vx * vu - cx * cx, 0.0))
+        pm, pd = proj(m), proj(d)
+        out["projected_emittance_%s_rel" % ax] = abs(pm - pd) / pd if pd > 0 else None
+    return out
+
+
+def hp_insitu_names():
+    import hipace2_b200 as hp
+    return hp.INSITU_BEAM
+
+
+def precision_errors(text, precision, beam, comps, env=None, deterministic=False, ref=None, steps=2):
+    """Fields of step 0 and the beam moments entering step 1 (after one push) of one run, and
+    their errors against `ref` (an earlier result of this function) when given."""
+    sim = make_sim_env(text, precision, env, deterministic)
+    sim.set_beam(0, beam)
+    sim.set_diag(comps)
+    sim.step(0)
+    fields = {c: sim.get_diag(c) for c in comps}
+    sim.step(1)
+    moments = sim.get_insitu("beam")
+    sim.close()
+    res = {"fields": fields, "moments": moments}
+    if ref is not None:
+        err = {c + "_rel_l2": rel_l2(fields[c], ref["fields"][c]) for c in comps}
+        err.update(beam_moment_errors(moments, ref["moments"]))
+        res["errors"] = err
+    return res
+
+
 def mixed_vs_fp64(text, args, torch):
     """The same workload in mixed precision (FP32 plasma, fields and multigrid; FP64 beam) against
-    the FP64 path on identical inputs: throughput and the relative L2 error of Ez, Psi and jz
-    over every slice of one step. The FP64 GPU path stands in for the FP64 oracle here (it
-    matches the oracle to <= 1e-10 in the parity tests; the oracle is too slow at this size)."""
+    the FP64 path on identical inputs: throughput, the relative L2 error of Ez, Psi, jz_beam and
+    Bx over every slice of step 0, and the beam's per-slice centroid and emittance entering step
+    1 (after one push in the mixed fields). The FP64 GPU path stands in for the FP64 oracle (it
+    matches the oracle to <= 1e-10 over a whole step of this workload in the parity tests).
+    Beside it: the FP64 noise floor (FP64 with floating-point atomics against FP64 in
+    deterministic mode, and FP64 with the beam's x displaced by 1e-7 of its rms size), and the
+    mixed path with one stage changed (the FP32 FFT instead of the tensor-core DST; FP64
+    residual refinement of the multigrid), and a weak-wake version of the workload (the driver's
+    weights scaled to a peak density of 0.5), where the plasma response is closer to linear."""
     import numpy as np
-    import hipace2_b200 as hp
     comps = ["Ez", "Psi", "jz_beam", "Bx"]
     out = {}
     ref = make_sim(text, "fp64", graphs=True)
     beam = ref.get_beam(0)
+    ref.close()
     mix = make_sim(text, "mixed", graphs=True)
     mix.set_beam(0, beam)
-    nz = ref.n_cell[2]
+    nz = mix.n_cell[2]
     # speed: warm-up steps then timed steps, like the FP64 headline
     w, k = max(1, args.warmup), max(1, args.steps)
     for s in range(w):
         mix.step(s)
     secs = time_device_steps(mix, w, k, torch)
+    mix.close()
     out["value"] = nz * k / secs
     out["unit"] = "slices/s"
     out["ms_per_step"] = secs / k * 1e3
-    # error: one step from identical state (fresh simulations, same beam)
-    ref.close()
-    mix.close()
-    ref = make_sim(text, "fp64", graphs=True)
-    ref.set_beam(0, beam)
-    mix = make_sim(text, "mixed", graphs=True)
-    mix.set_beam(0, beam)
-    ref.set_diag(comps)
-    mix.set_diag(comps)
-    ref.step(0)
-    mix.step(0)
-    for c in comps:
-        a, b = mix.get_diag(c), ref.get_diag(c)
-        out[c + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    out["error_reference"] = "FP64 GPU path, same inputs, step 0 (all slices)"
+    tdiag = text + "\nbeams.insitu_period = 1\n"
+    d64 = precision_errors(tdiag, "fp64", beam, comps, deterministic=True)
+    out.update(precision_errors(tdiag, "mixed", beam, comps, ref=d64)["errors"])
+    out["error_reference"] = ("FP64 GPU path in deterministic mode, same beam: fields of step 0 (all slices), "
+                              "beam moments entering step 1")
     out["dtype"] = "f32 plasma/fields/multigrid, f64 beam"
-    ref.close()
-    mix.close()
+    floor = {}
+    floor["fp64_atomics_vs_deterministic"] = precision_errors(tdiag, "fp64", beam, comps, ref=d64)["errors"]
+    shifted = dict(beam)
+    shifted["x"] = beam["x"] + 1e-7 * float(np.std(beam["x"]))
+    floor["fp64_beam_x_displaced_1e-7_rms"] = precision_errors(tdiag, "fp64", shifted, comps, deterministic=True,
+                                                              ref=d64)["errors"]
+    out["fp64_noise_floor"] = floor
+    abl = {}
+    for name, env in (("fp32_fft_dst", {"HPQ_DST": "fft"}), ("fp64_multigrid_refinement", {"HPQ_MG_REFINE": "1"})):
+        r = precision_errors(tdiag, "mixed", beam, comps, env=env, ref=d64)["errors"]
+        sim = make_sim_env(text, "mixed", env)
+        sim.set_beam(0, beam)
+        sim.step(0)
+        r["slices_per_s"] = nz / time_device_steps(sim, 1, 1, torch)
+        sim.close()
+        abl[name] = r
+    out["ablation"] = abl
+    # weak wake: the same particles with weights scaled to a peak density of 0.5
+    weak = tdiag
+    wbeam = dict(beam)
+    wbeam["w"] = beam["w"] * (0.5 / 10.0)
+    w64 = precision_errors(weak, "fp64", wbeam, comps, deterministic=True)
+    out["weak_wake"] = {"driver_density": 0.5,
+                        "mixed": precision_errors(weak, "mixed", wbeam, comps, ref=w64)["errors"],
+                        "fp64_atomics_vs_deterministic": precision_errors(weak, "fp64", wbeam, comps, ref=w64)["errors"]}
     return out
 
 
 def scale_point(name, torch, sample_every=64):
-    """One step of a larger workload in FP64 and in mixed precision (device time), and the mixed
-    error against the FP64 GPU path on identical inputs (step 0, every `sample_every`-th slice
-    read back through the per-slice surface; a full 3-D diagnostic would be 8 GB per component)."""
+    """The larger workload over its configured 5 steps in FP64 and in mixed precision: steps 1-3
+    device-timed, steps 0 and 4 run slice by slice with every `sample_every`-th slice's fields
+    read back (a full 3-D diagnostic would be 8 GB per component), and the mixed error against
+    the FP64 GPU path on identical inputs for both; plus the FP64 noise floor of step 0 (FP64
+    with floating-point atomics against FP64 in deterministic mode)."""
     import numpy as np
     from cases import config
     text = config(name)
@@ -388,35 +494,48 @@ def scale_point(name, torch, sample_every=64):
     comps = ["Ez", "Psi", "jz_beam", "Bx"]
     samples = {}
     beam = None
-    for prec in ("fp64", "mixed"):
-        sim = make_sim(text, prec, graphs=True)
-        if beam is None:
-            beam = sim.get_beam(0)
-        else:
-            sim.set_beam(0, beam)
-        nz = sim.n_cell[2]
-        # step 0 slice by slice, sampling fields
+
+    def sampled_step(sim, step):
         got = {c: [] for c in comps}
-        sim.begin_step(0)
-        for s in range(nz - 1, -1, -1):
+        sim.begin_step(step)
+        for s in range(sim.n_cell[2] - 1, -1, -1):
             sim.solve_one_slice(s)
             if s % sample_every == 0:
                 for c in comps:
                     got[c].append(sim.get_field(c))
         sim.end_step()
-        samples[prec] = {c: np.array(v) for c, v in got.items()}
-        secs = time_device_steps(sim, 1, 1, torch)
-        res[prec + "_slices_per_s"] = nz / secs
-        res[prec + "_ms_per_step"] = secs * 1e3
+        return {c: np.array(v) for c, v in got.items()}
+
+    for prec, det in (("fp64", True), ("fp64", False), ("mixed", False)):
+        sim = make_sim_env(text, prec, deterministic=det)
+        if beam is None:
+            beam = sim.get_beam(0)
+        else:
+            sim.set_beam(0, beam)
+        nz = sim.n_cell[2]
+        key = prec + ("_det" if det else "")
+        first = sampled_step(sim, 0)
+        if det:
+            samples[key] = {0: first}
+            sim.close()
+            continue
+        secs = time_device_steps(sim, 1, 3, torch)
+        last = sampled_step(sim, 4)
+        samples[key] = {0: first, 4: last}
+        res[prec + "_slices_per_s"] = 3 * nz / secs
+        res[prec + "_ms_per_step"] = secs / 3 * 1e3
         if prec == "fp64":
             res["grid"] = sim.n_cell
             res["plasma_particles"] = int(sim.get_plasma(0)["x"].size)
         sim.close()
     res["mixed_speedup"] = res["mixed_slices_per_s"] / res["fp64_slices_per_s"]
-    for c in comps:
-        a, b = samples["mixed"][c], samples["fp64"][c]
-        res[c + "_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    res["error_reference"] = "FP64 GPU path, same beam, step 0, every %d-th slice" % sample_every
+    for step in (0, 4):
+        for c in comps:
+            res["step%d_%s_rel_l2" % (step, c)] = rel_l2(samples["mixed"][step][c], samples["fp64"][step][c])
+    res["fp64_noise_floor_step0"] = {c + "_rel_l2": rel_l2(samples["fp64"][0][c], samples["fp64_det"][0][c])
+                                     for c in comps}
+    res["steps"] = "5 (0-4): steps 1-3 timed, steps 0 and 4 sampled"
+    res["error_reference"] = "FP64 GPU path, same beam, every %d-th slice of steps 0 and 4" % sample_every
     return res
 
 

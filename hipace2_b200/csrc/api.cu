@@ -130,11 +130,6 @@ int hpq_set_precision(hpq_handle* h, int mode) {
 }
 
 int hpq_init(hpq_handle* h) {
-    if (h && h->cfg.depos_order_xy != 2) {
-        h->err = "hipace.depos_order_xy = " + std::to_string(h->cfg.depos_order_xy) +
-                 " is not supported: the library deposits and gathers with order 2";
-        return HPQ_ERR_INPUT;
-    }
     return guarded(h, [&] {
         if (h->initialised) { h->err = "hpq_init called twice"; return (int)HPQ_ERR_STATE; }
         if (h->precision == HPQ_MIXED) h->sim.reset(new hpq::Sim<float>(h->cfg));

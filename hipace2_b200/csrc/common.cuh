@@ -140,11 +140,119 @@ __device__ __forceinline__ DSh<R> dshape2(R xmid, int ix) {
     }
 }
 
-// Position in cell units clamped to [-1, n]: identity for particles inside the domain
-// (xmid in [-0.5, n-0.5]); keeps NaN/inf positions from indexing outside the guard cells.
+// Shape factors of any transverse order 0..3 (ShapeFactors.H:130-197 for the deposits,
+// :212-468 for the derivative shapes of the gather and the explicit deposition): the quadratic
+// ones are the functions above, the others the B-splines of order 0, 1 and 3 and their
+// derivative forms (analytic, nodal, centred). Stencil points: ORD + 1 for shapeN,
+// ORD + TYPE + 1 for dshapeN (ORD + 3 for the centred type 2).
+template <class R, int ORD>
+__device__ __forceinline__ Sh<R> shapeN(R xmid, int ix) {
+    if constexpr (ORD == 2) {
+        return shape2<R>(xmid, ix);
+    } else if constexpr (ORD == 0) {
+        return {R(1), (int)floor(xmid + R(0.5))};
+    } else if constexpr (ORD == 1) {
+        const R xf = floor(xmid), xi = xmid - xf;
+        return {ix == 0 ? R(1) - xi : xi, (int)xf + ix};
+    } else {
+        const R xf = floor(xmid), xi = xmid - xf, xm = R(1) - xi;
+        const int c = (int)xf - 1 + ix;
+        if (ix == 0) return {R(1.0 / 6.0) * xm * xm * xm, c};
+        if (ix == 1) return {R(2.0 / 3.0) - xi * xi * (R(1) - xi / R(2)), c};
+        if (ix == 2) return {R(2.0 / 3.0) - xm * xm * (R(1) - R(0.5) * xm), c};
+        return {R(1.0 / 6.0) * xi * xi * xi, c};
+    }
+}
+template <int TYPE, int ORD>
+__host__ __device__ constexpr int dshape_points() { return TYPE == 2 ? ORD + 3 : ORD + TYPE + 1; }
+
+template <class R, int TYPE, int ORD>
+__device__ __forceinline__ DSh<R> dshapeN(R xmid, int ix) {
+    if constexpr (ORD == 2) {
+        return dshape2<R, TYPE>(xmid, ix);
+    } else if constexpr (TYPE == 0) {  // analytic derivative
+        if constexpr (ORD == 0) {
+            return {R(1), R(0), (int)floor(xmid + R(0.5))};
+        } else if constexpr (ORD == 1) {
+            const R xf = floor(xmid), xi = xmid - xf;
+            return ix == 0 ? DSh<R>{R(1) - xi, R(1), (int)xf} : DSh<R>{xi, R(-1), (int)xf + 1};
+        } else {
+            const R xf = floor(xmid), xi = xmid - xf, x2 = xi * xi, x3 = x2 * xi;
+            const int c = (int)xf - 1 + ix;
+            if (ix == 0) return {R(-1.0 / 6.0) * x3 + R(0.5) * x2 - R(0.5) * xi + R(1.0 / 6.0), -(R(-0.5) * x2 + xi - R(0.5)), c};
+            if (ix == 1) return {R(0.5) * x3 - x2 + R(2.0 / 3.0), -(R(1.5) * x2 - R(2) * xi), c};
+            if (ix == 2) return {R(-0.5) * x3 + R(0.5) * x2 + R(0.5) * xi + R(1.0 / 6.0), -(R(-1.5) * x2 + xi + R(0.5)), c};
+            return {R(1.0 / 6.0) * x3, -(R(0.5) * x2), c};
+        }
+    } else if constexpr (TYPE == 1) {  // nodal derivative
+        if constexpr (ORD == 0) {
+            const R xf = floor(xmid), xi = xmid - xf;
+            const bool lo = xi < R(0.5);
+            return ix == 0 ? DSh<R>{lo ? R(1) : R(0), R(1), (int)xf} : DSh<R>{lo ? R(0) : R(1), R(-1), (int)xf + 1};
+        } else if constexpr (ORD == 1) {
+            const R xm = xmid + R(0.5), xf = floor(xm), xi = xm - xf;
+            const bool lo = xi < R(0.5);
+            const int c = (int)xf - 1 + ix;
+            if (ix == 0) return {lo ? R(0.5) - xi : R(0), -(xi - R(1)), c};
+            if (ix == 1) return {lo ? xi + R(0.5) : R(1.5) - xi, -(R(1) - R(2) * xi), c};
+            return {lo ? R(0) : xi - R(0.5), -xi, c};
+        } else {
+            const R xm = xmid + R(0.5), xf = floor(xm), xi = xm - xf, x2 = xi * xi, x3 = x2 * xi;
+            const bool lo = xi < R(0.5);
+            const int c = (int)xf - 2 + ix;
+            if (ix == 0)
+                return {lo ? R(-1.0 / 6.0) * x3 + R(0.25) * x2 - R(0.125) * xi + R(1.0 / 48.0) : R(0),
+                        -(R(1.0 / 6.0) * x3 - R(0.5) * x2 + R(0.5) * xi - R(1.0 / 6.0)), c};
+            if (ix == 1)
+                return {lo ? R(0.5) * x3 - R(0.25) * x2 - R(0.625) * xi + R(23.0 / 48.0)
+                           : R(-1.0 / 6.0) * x3 + R(0.75) * x2 - R(1.125) * xi + R(9.0 / 16.0),
+                        -(R(-2.0 / 3.0) * x3 + R(1.5) * x2 - R(0.5) * xi - R(0.5)), c};
+            if (ix == 2)
+                return {lo ? R(-0.5) * x3 - R(0.25) * x2 + R(0.625) * xi + R(23.0 / 48.0)
+                           : R(0.5) * x3 - R(1.75) * x2 + R(1.375) * xi + R(17.0 / 48.0),
+                        -(x3 - R(1.5) * x2 - R(0.5) * xi + R(0.5)), c};
+            if (ix == 3)
+                return {lo ? R(1.0 / 6.0) * x3 + R(0.25) * x2 + R(0.125) * xi + R(1.0 / 48.0)
+                           : R(-0.5) * x3 + R(1.25) * x2 - R(0.375) * xi + R(5.0 / 48.0),
+                        -(R(-2.0 / 3.0) * x3 + R(0.5) * x2 + R(0.5) * xi + R(1.0 / 6.0)), c};
+            return {lo ? R(0) : R(1.0 / 6.0) * x3 - R(0.25) * x2 + R(0.125) * xi - R(1.0 / 48.0), -(R(1.0 / 6.0) * x3), c};
+        }
+    } else {  // centred derivative
+        if constexpr (ORD == 0) {
+            const R xf = floor(xmid + R(0.5));
+            const int c = (int)xf - 1 + ix;
+            if (ix == 0) return {R(0), R(0.5), c};
+            if (ix == 1) return {R(1), R(0), c};
+            return {R(0), R(-0.5), c};
+        } else if constexpr (ORD == 1) {
+            const R xf = floor(xmid), xi = xmid - xf;
+            const int c = (int)xf - 1 + ix;
+            if (ix == 0) return {R(0), -(R(0.5) * xi - R(0.5)), c};
+            if (ix == 1) return {R(1) - xi, -(R(-0.5) * xi), c};
+            if (ix == 2) return {xi, -(R(0.5) - R(0.5) * xi), c};
+            return {R(0), -(R(0.5) * xi), c};
+        } else {
+            const R xf = floor(xmid), xi = xmid - xf, x2 = xi * xi, x3 = x2 * xi;
+            const int c = (int)xf - 2 + ix;
+            if (ix == 0) return {R(0), -(R(1.0 / 12.0) * x3 - R(0.25) * x2 + R(0.25) * xi - R(1.0 / 12.0)), c};
+            if (ix == 1)
+                return {R(-1.0 / 6.0) * x3 + R(0.5) * x2 - R(0.5) * xi + R(1.0 / 6.0), -(R(-0.25) * x3 + R(0.5) * x2 - R(1.0 / 3.0)), c};
+            if (ix == 2) return {R(0.5) * x3 - x2 + R(2.0 / 3.0), -(R(1.0 / 6.0) * x3 - R(0.5) * xi), c};
+            if (ix == 3)
+                return {R(-0.5) * x3 + R(0.5) * x2 + R(0.5) * xi + R(1.0 / 6.0), -(R(1.0 / 6.0) * x3 - R(0.5) * x2 + R(1.0 / 3.0)), c};
+            if (ix == 4)
+                return {R(1.0 / 6.0) * x3, -(R(-0.25) * x3 + R(0.25) * x2 + R(0.25) * xi + R(1.0 / 12.0)), c};
+            return {R(0), -(R(1.0 / 12.0) * x3), c};
+        }
+    }
+}
+
+// Position in cell units clamped to [-1, n - 1/2]: identity for particles inside the domain
+// (xmid in [-0.5, n-0.5]); keeps NaN/inf positions from indexing outside the three guard cells
+// with any stencil of order <= 3.
 template <class R>
 __device__ __forceinline__ R clamp_mid(R xmid, int n) {
-    return fmin(fmax(xmid, R(-1)), R(n));
+    return fmin(fmax(xmid, R(-1)), R(n) - R(0.5));
 }
 
 // grid-stride loop helpers

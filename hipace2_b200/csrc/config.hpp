@@ -301,11 +301,9 @@ inline SimConfig build_config(const InputStore& in) {
     if (in.query("random_seed", c.random_seed)) c.has_random_seed = true;
 
     in.query("hipace.depos_order_xy", c.depos_order_xy);
-    // order 2 throughout; order 0 exists for the beam deposition of the CPU restatement only
-    // (the library refuses it at hpq_init)
-    if (c.depos_order_xy != 2 && c.depos_order_xy != 0)
+    if (c.depos_order_xy < 0 || c.depos_order_xy > 3)
         throw InputError("hipace.depos_order_xy = " + std::to_string(c.depos_order_xy) +
-                         " is not supported (only 2)");
+                         " is not supported (0, 1, 2 or 3)");
     int dz_order = 0;
     in.query("hipace.depos_order_z", dz_order);
     if (dz_order != 0) throw InputError("hipace.depos_order_z must be 0");
@@ -593,6 +591,8 @@ inline SimConfig build_config(const InputStore& in) {
         if (a.witness < 0) throw InputError("adjoint.witness = " + witness + " is not in beams.names");
         if (!c.explicit_solver) throw InputError("the adjoint needs the explicit Bx/By solver");
         if (c.any_salame()) throw InputError("the adjoint does not differentiate SALAME");
+        if (c.depos_order_xy != 2)
+            throw InputError("the adjoint is written for the quadratic shapes (hipace.depos_order_xy = 2)");
         for (auto& p : c.plasmas)
             if (p.n_subcycles != 1) throw InputError("the adjoint needs plasma n_subcycles = 1");
         double r[2];

@@ -364,7 +364,8 @@ __device__ __forceinline__ void addd(const DetAcc& d, R* base, int pitch, int i,
 
 // Cell-unit coordinate of a plasma position along one axis as base + t: with a reference lattice
 // coordinate (single precision) t = frac(u0) + x * dxi is a small number and the integer part
-// goes to `base`; without one, base = 0 and t = (x - off) * dxi. Clamped to [-1, n] like clamp_mid.
+// goes to `base`; without one, base = 0 and t = (x - off) * dxi. Clamped to [-1, n - 1/2] like
+// clamp_mid.
 template <class R>
 __device__ __forceinline__ R plasma_mid_v(bool has_ref, float u0, R x, R off, R dxi, int n, int& base) {
     if (!has_ref) {
@@ -374,7 +375,7 @@ __device__ __forceinline__ R plasma_mid_v(bool has_ref, float u0, R x, R off, R 
     const float fb = floorf(u0);
     const R t = (R)(u0 - fb) + x * dxi;
     const R tot = (R)fb + t;
-    if (!(tot >= R(-1) && tot <= R(n))) {
+    if (!(tot >= R(-1) && tot <= R(n) - R(0.5))) {
         base = 0;
         return clamp_mid<R>(tot, n);
     }
@@ -386,7 +387,7 @@ __device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R o
     return plasma_mid_v<R>(ref != nullptr, ref ? ref[ip] : 0.f, x, off, dxi, n, base);
 }
 
-template <class R, bool DET>
+template <class R, bool DET, int ORD = 2>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
                                                         const int* gate, DetAcc det) {
     HPQ_PDL_ENTRY();
@@ -440,16 +441,17 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
                 P.w[ip] = R(0);
                 P.valid[ip] = 0;
             } else {
-                Sh<R> sx[3], sy[3];
+                constexpr int NP = ORD + 1;
+                Sh<R> sx[NP], sy[NP];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    sx[k] = shape2<R>(xmid, k); sy[k] = shape2<R>(ymid, k);
+                for (int k = 0; k < NP; ++k) {
+                    sx[k] = shapeN<R, ORD>(xmid, k); sy[k] = shapeN<R, ORD>(ymid, k);
                     sx[k].cell += bx; sy[k].cell += by;
                 }
 #pragma unroll
-                for (int iy = 0; iy < 3; ++iy)
+                for (int iy = 0; iy < NP; ++iy)
 #pragma unroll
-                    for (int ix = 0; ix < 3; ++ix) {
+                    for (int ix = 0; ix < NP; ++ix) {
                         const int i = sx[ix].cell, j = sy[iy].cell;
                         const R cd = q_invvol * sx[ix].s * sy[iy].s;
                         if (o.jx) { addd<DET>(det, o.jx, o.pitch, i, j, cd * vx_c); addd<DET>(det, o.jy, o.pitch, i, j, cd * vy_c); }
@@ -483,7 +485,7 @@ __global__ void k_pack_explicit(Slab<R> S, Quad<R>* __restrict__ q) {
     for (long long k = gtid(); k < (long long)S.cstride; k += gstride()) q[k] = Quad<R>{bz[k], ez[k], ex[k], ey[k]};
 }
 
-template <class R, int DT, bool DET>
+template <class R, int DT, bool DET, int ORD = 2>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g,
                                                                                     const Quad<R>* __restrict__ quad,
                                                                                     DetAcc det) {
@@ -495,7 +497,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposi
     const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
     R* Sx = S.c(C_SX).p;
     R* Sy = S.c(C_SY).p;
-    constexpr int NS = 3 + DT;
+    constexpr int NS = dshape_points<DT, ORD>();
     for (long long ip = gtid(); ip < P.n; ip += gstride()) {
         if (!P.valid[ip]) continue;
         const R psis = P.psi[ip];
@@ -514,18 +516,18 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposi
         DSh<R> sx[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
-            sx[k] = dshape2<R, DT>(xmid, k);
+            sx[k] = dshapeN<R, DT, ORD>(xmid, k);
             sx[k].cell += bx;
         }
         // one row of the stencil at a time (the y shape of the row is formed in the loop, which
         // keeps the register count low enough for two blocks per SM)
 #pragma unroll 1
         for (int iy = 0; iy < NS; ++iy) {
-            DSh<R> syr = dshape2<R, DT>(ymid, iy);
+            DSh<R> syr = dshapeN<R, DT, ORD>(ymid, iy);
             syr.cell += by;
 #pragma unroll
             for (int ix = 0; ix < NS; ++ix) {
-                if (DT == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                if (DT == 2 && (ix == 0 || ix == NS - 1) && (iy == 0 || iy == NS - 1)) continue;
                 const int i = sx[ix].cell, j = syr.cell;
                 const Quad<R> fq = quad[(ptrdiff_t)(j + kGuardAlloc) * S.pitch + (i + kGuardAlloc)];
                 const R Bz_v = fq.bz, Ez_v = fq.ez, ExmBy_v = fq.ex, EypBx_v = fq.ey;
@@ -542,24 +544,25 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposi
 }
 
 // ------------------------------------------------------------------------------------------
-// Field gather (FieldGather.H:45-96, derivative type 1, 4x4 stencil)
+// Field gather (FieldGather.H:45-96, derivative type 1: (ORD + 2)^2 stencil, 4x4 at order 2)
 // ------------------------------------------------------------------------------------------
 // x, y in cell units, as base + fraction (bx, by integer)
-template <class R, class T>
+template <class R, class T, int ORD = 2>
 __device__ __forceinline__ void gather_mid(const Slab<R>& S, const Geo& g, T x, T y, int bx, int by, T& ExmBy,
                                            T& EypBx, T& Ez, T& Bx, T& By, T& Bz) {
     const T dxi = (T)g.dxi[0], dyi = (T)g.dxi[1];
     const F2<R> Psi = S.c(C_PSI), FEz = S.c(C_EZ), FBx = S.c(C_BX), FBy = S.c(C_BY), FBz = S.c(C_BZ);
-    DSh<T> sx[4], sy[4];
+    constexpr int NG = ORD + 2;
+    DSh<T> sx[NG], sy[NG];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        sx[k] = dshape_nodal2<T>(x, k); sy[k] = dshape_nodal2<T>(y, k);
+    for (int k = 0; k < NG; ++k) {
+        sx[k] = dshapeN<T, 1, ORD>(x, k); sy[k] = dshapeN<T, 1, ORD>(y, k);
         sx[k].cell += bx; sy[k].cell += by;
     }
 #pragma unroll
-    for (int iy = 0; iy < 4; iy++)
+    for (int iy = 0; iy < NG; iy++)
 #pragma unroll
-        for (int ix = 0; ix < 4; ix++) {
+        for (int ix = 0; ix < NG; ix++) {
             const int i = sx[ix].cell, j = sy[iy].cell;
             const T psi = (T)Psi(i, j);
             ExmBy += (sx[ix].ds * sy[iy].s) * psi * dxi;
@@ -572,11 +575,11 @@ __device__ __forceinline__ void gather_mid(const Slab<R>& S, const Geo& g, T x, 
         }
 }
 
-template <class R, class T>
+template <class R, class T, int ORD = 2>
 __device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T yp, T& ExmBy, T& EypBx, T& Ez,
                                        T& Bx, T& By, T& Bz) {
     const T x = clamp_mid<T>((xp - (T)g.xoff) * (T)g.dxi[0], g.nx), y = clamp_mid<T>((yp - (T)g.yoff) * (T)g.dxi[1], g.ny);
-    gather_mid<R, T>(S, g, x, y, 0, 0, ExmBy, EypBx, Ez, Bx, By, Bz);
+    gather_mid<R, T, ORD>(S, g, x, y, 0, 0, ExmBy, EypBx, Ez, Bx, By, Bz);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -585,7 +588,7 @@ __device__ __forceinline__ void gather(const Slab<R>& S, const Geo& g, T xp, T y
 // side along the trajectory) for u and psi from -1/2 to +1/2, full position step, 2 more
 // sub-steps to the slice.
 // ------------------------------------------------------------------------------------------
-template <class R>
+template <class R, int ORD = 2>
 __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, Geo g, int temp,
                                                      const int* gate) {
     HPQ_PDL_ENTRY();
@@ -604,7 +607,7 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
                 int bx, by;
                 const R xm = plasma_mid<R>(P.ru, ip, xp, (R)g.xoff, (R)g.dxi[0], g.nx, bx);
                 const R ym = plasma_mid<R>(P.rv, ip, yp, (R)g.yoff, (R)g.dxi[1], g.ny, by);
-                gather_mid<R, R>(S, g, xm, ym, bx, by, Ex, Ey, Ez, Bx, By, Bz);
+                gather_mid<R, R, ORD>(S, g, xm, ym, bx, by, Ex, Ey, Ez, Bx, By, Bz);
             }
             Bx *= clight; By *= clight;
             R ux = P.uxh[ip], uy = P.uyh[ip], psi = P.psih[ip];
@@ -659,7 +662,7 @@ __global__ void __launch_bounds__(256) k_plasma_push(PlasmaDev<R> P, Slab<R> S, 
 // Beam deposition (BeamDepositCurrent.cpp:21-196): the non-slipped particles of slice
 // `ctl->islice - which` of the current store.
 // ------------------------------------------------------------------------------------------
-template <class R>
+template <class R, int ORD = 2>
 __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __restrict__ ctl, int which, R* jx, R* jy,
                                                       R* jz, R* rmj, int pitch, Geo g, int gated, DetAcc det) {
     HPQ_PDL_ENTRY();
@@ -681,13 +684,14 @@ __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __re
         const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
         const double xmid = clamp_mid<double>((b.x[ip] - g.xoff) * g.dxi[0], g.nx);
         const double ymid = clamp_mid<double>((b.y[ip] - g.yoff) * g.dxi[1], g.ny);
-        Sh<double> sx[3], sy[3];
+        constexpr int NP = ORD + 1;
+        Sh<double> sx[NP], sy[NP];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) { sx[q] = shape2<double>(xmid, q); sy[q] = shape2<double>(ymid, q); }
+        for (int q = 0; q < NP; ++q) { sx[q] = shapeN<double, ORD>(xmid, q); sy[q] = shapeN<double, ORD>(ymid, q); }
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
+        for (int iy = 0; iy < NP; ++iy)
 #pragma unroll
-            for (int ix = 0; ix < 3; ++ix) {
+            for (int ix = 0; ix < NP; ++ix) {
                 const double S = sx[ix].s * sy[iy].s;
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 if (jx) { addc<R>(det, jx, pitch, i, j, (R)(S * wqx)); addc<R>(det, jy, pitch, i, j, (R)(S * wqy)); }
@@ -699,7 +703,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit(BeamDev B, const Ctl* __re
 
 // Both beam depositions of the explicit solver in one launch: jz_beam (and rhomjz_beam) from the
 // non-slipped particles of this slice, jx_beam/jy_beam of the next slice from its particles.
-template <class R>
+template <class R, int ORD = 2>
 __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const Ctl* __restrict__ ctl, R* jz, R* rmj,
                                                                 R* njx, R* njy, int pitch, Geo g, DetAcc det) {
     HPQ_PDL_ENTRY();
@@ -721,13 +725,14 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
         const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
         const double xmid = clamp_mid<double>((b.x[ip] - g.xoff) * g.dxi[0], g.nx);
         const double ymid = clamp_mid<double>((b.y[ip] - g.yoff) * g.dxi[1], g.ny);
-        Sh<double> sx[3], sy[3];
+        constexpr int NP = ORD + 1;
+        Sh<double> sx[NP], sy[NP];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) { sx[q] = shape2<double>(xmid, q); sy[q] = shape2<double>(ymid, q); }
+        for (int q = 0; q < NP; ++q) { sx[q] = shapeN<double, ORD>(xmid, q); sy[q] = shapeN<double, ORD>(ymid, q); }
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
+        for (int iy = 0; iy < NP; ++iy)
 #pragma unroll
-            for (int ix = 0; ix < 3; ++ix) {
+            for (int ix = 0; ix < NP; ++ix) {
                 const double S = sx[ix].s * sy[iy].s;
                 const int i = sx[ix].cell, j = sy[iy].cell;
                 if (nxt) {
@@ -748,7 +753,7 @@ __global__ void __launch_bounds__(256) k_beam_deposit_this_next(BeamDev B, const
 // lower edge). S holds that slice's fields (the slice driver runs the push of a slice beside the
 // next slice's solve, on a saved copy of the fields); lag 1 beyond the box head does nothing.
 // ------------------------------------------------------------------------------------------
-template <class R>
+template <class R, int ORD = 2>
 __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restrict__ ctl, int bi, Slab<R> S, Geo g,
                                                    int lag) {
     HPQ_PDL_ENTRY();
@@ -779,7 +784,7 @@ __global__ void __launch_bounds__(256) k_beam_push(BeamDev B, const Ctl* __restr
             yp += dtb * 0.5 * uy * gpi;
             if (!enforce_bc<double>(g, xp, yp, ux, uy)) { absorbed = true; break; }
             double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
-            gather<R, double>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
+            gather<R, double, ORD>(S, g, xp, yp, Ex, Ey, Ez, Bx, By, Bz);
             if (B.ext) {
                 // ApplyExternalField (ExternalFields.H:29-56) at the step's start time; Ex, Ey
                 // here are ExmBy, EypBx

@@ -60,9 +60,9 @@ __global__ void k_sal_jxjy_from_b(Slab<R> S, Slab<R> V, Geo g) {
 }
 
 // SalameOnlyAdvancePlasma (Salame.cpp:257-331): the plasma momenta from the SALAME-only Bx, By
-// gathered (order-2 shape, doBxByGatherShapeN, FieldGather.H:183-216) at the previous position:
-// ux = 1.5 dz q/m By, uy = -1.5 dz q/m Bx.
-template <class R>
+// gathered (deposit shape of order ORD, doBxByGatherShapeN, FieldGather.H:183-216) at the
+// previous position: ux = 1.5 dz q/m By, uy = -1.5 dz q/m Bx.
+template <class R, int ORD = 2>
 __global__ void __launch_bounds__(256) k_sal_only_push(PlasmaDev<R> P, Slab<R> V, Geo g) {
     HPQ_PDL_ENTRY();
     const F2<R> FBx = V.c(C_BX), FBy = V.c(C_BY);
@@ -72,17 +72,18 @@ __global__ void __launch_bounds__(256) k_sal_only_push(PlasmaDev<R> P, Slab<R> V
         int bx, by;
         const R xm = plasma_mid<R>(P.ru, ip, P.xp[ip], (R)g.xoff, (R)g.dxi[0], g.nx, bx);
         const R ym = plasma_mid<R>(P.rv, ip, P.yp[ip], (R)g.yoff, (R)g.dxi[1], g.ny, by);
-        Sh<R> sx[3], sy[3];
+        constexpr int NP = ORD + 1;
+        Sh<R> sx[NP], sy[NP];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            sx[q] = shape2<R>(xm, q); sy[q] = shape2<R>(ym, q);
+        for (int q = 0; q < NP; ++q) {
+            sx[q] = shapeN<R, ORD>(xm, q); sy[q] = shapeN<R, ORD>(ym, q);
             sx[q].cell += bx; sy[q].cell += by;
         }
         R bxp = 0, byp = 0;
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
+        for (int iy = 0; iy < NP; ++iy)
 #pragma unroll
-            for (int ix = 0; ix < 3; ++ix) {
+            for (int ix = 0; ix < NP; ++ix) {
                 const R s = sx[ix].s * sy[iy].s;
                 bxp += s * FBx(sx[ix].cell, sy[iy].cell);
                 byp += s * FBy(sx[ix].cell, sy[iy].cell);

@@ -919,6 +919,18 @@ public:
         upload_beam(b, x, y, z, w, ux, uy, uz, id, n);
     }
 
+    // calls f(std::integral_constant<int, ORD>{}) for the deck's transverse shape order
+    // (hipace.depos_order_xy, 0..3): the deposits, gathers and pushes are compiled per order
+    template <class F>
+    void with_order(F&& f) const {
+        switch (cfg.depos_order_xy) {
+            case 0: f(std::integral_constant<int, 0>{}); break;
+            case 1: f(std::integral_constant<int, 1>{}); break;
+            case 3: f(std::integral_constant<int, 3>{}); break;
+            default: f(std::integral_constant<int, 2>{}); break;
+        }
+    }
+
     // ---- time-step pipeline hand-off
     // out_par: parity of the store the current (or last) step writes for the next step
     int out_par = 1;
@@ -1076,7 +1088,7 @@ public:
         for (size_t s = 0; s < pl.size(); ++s) {
             if (!pl[s].neutralize || pl[s].n == 0) continue;
             DepOut<R> o{nullptr, nullptr, nullptr, nullptr, nullptr, S.c(C_IONS).p, S.pitch};
-            hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr, det);
+            with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(det.w[0] ? k_plasma_deposit<R, true, ORD> : k_plasma_deposit<R, false, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, -pl[s].charge, (const int*)nullptr, det); });
             HPQ_LAUNCH_CHECK();
             det_flush({C_IONS});
         }
@@ -1134,13 +1146,13 @@ public:
         if (pl[sp].n == 0) return;
         DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
         Scope sc(this, "plasma_deposit");
-        hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det);
+        with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(det.w[0] ? k_plasma_deposit<R, true, ORD> : k_plasma_deposit<R, false, ORD>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det); });
         HPQ_LAUNCH_CHECK();
         det_flush_ptrs({jx, jy, jz, rho, chi, rhomjz});
     }
     void deposit_beam(int b, int which, R* jx, R* jy, R* jz, R* rmj) {
         Scope sc(this, "beam_deposit");
-        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], (const Ctl*)ctl, which, jx, jy, jz, rmj, S.pitch, g, 0, det);
+        with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_beam_deposit<R, ORD>, dim3(148 * 2), dim3(256), 0, st, bm[b], (const Ctl*)ctl, which, jx, jy, jz, rmj, S.pitch, g, 0, det); });
         HPQ_LAUNCH_CHECK();
         det_flush_ptrs({jx, jy, jz, rmj});
     }
@@ -1284,9 +1296,9 @@ public:
             const int nb = blocks_for(pl[s].n, 256);
             const bool d = det.w[0] != nullptr;
             const Quad<R>* q = quad;
-            if (cfg.depos_derivative_type == 0) hpq_launch(d ? k_explicit_deposit<R, 0, true> : k_explicit_deposit<R, 0, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
-            else if (cfg.depos_derivative_type == 1) hpq_launch(d ? k_explicit_deposit<R, 1, true> : k_explicit_deposit<R, 1, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
-            else hpq_launch(d ? k_explicit_deposit<R, 2, true> : k_explicit_deposit<R, 2, false>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det);
+            if (cfg.depos_derivative_type == 0) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 0, true, ORD> : k_explicit_deposit<R, 0, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
+            else if (cfg.depos_derivative_type == 1) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 1, true, ORD> : k_explicit_deposit<R, 1, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
+            else with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 2, true, ORD> : k_explicit_deposit<R, 2, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
             HPQ_LAUNCH_CHECK();
             det_flush({C_SX, C_SY});
         }
@@ -1336,7 +1348,7 @@ public:
             // step 1: Ez of the next slice with the present weights (:43-76)
             for (size_t s = 0; s < pl.size(); ++s) {
                 if (pl[s].n == 0) continue;
-                hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, (const int*)nullptr);
+                with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_plasma_push<R, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, (const int*)nullptr); });
                 HPQ_LAUNCH_CHECK();
             }
             copies({{N + C_JX, C_NJXB}, {N + C_JY, C_NJYB}});
@@ -1355,7 +1367,10 @@ public:
             if (cfg.salame_do_advance) {
                 for (size_t s = 0; s < pl.size(); ++s) {
                     if (pl[s].n == 0) continue;
-                    hpq_launch(k_sal_only_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], V, g);
+                    with_order([&](auto o_) {
+                        constexpr int ORD = decltype(o_)::value;
+                        hpq_launch(k_sal_only_push<R, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], V, g);
+                    });
                     HPQ_LAUNCH_CHECK();
                     deposit_plasma((int)s, V.c(C_JX).p, V.c(C_JY).p, nullptr, nullptr, nullptr, nullptr);
                 }
@@ -1913,7 +1928,7 @@ public:
             }
             {
                 Scope sc(this, "beam_push");
-                hpq_launch(k_beam_push<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, SB, g, lag);
+                with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_beam_push<R, ORD>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, (int)b, SB, g, lag); });
                 HPQ_LAUNCH_CHECK();
             }
             Scope sc2(this, "beam_partition");
@@ -1951,9 +1966,9 @@ public:
                     // a SALAME beam deposits only jz in the SALAME step (MultiBeam.cpp:50-56)
                     const bool sal = sal_step && cfg.beams[b].do_salame;
                     const bool nj = cfg.do_beam_jx_jy_deposition && !sal;
-                    hpq_launch(k_beam_deposit_this_next<R>, dim3(148 * 2), dim3(256), 0, st,
+                    with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_beam_deposit_this_next<R, ORD>, dim3(148 * 2), dim3(256), 0, st,
                         bm[b], ctl, S.c(C_JZB).p, cfg.do_beam_jz_minus_rho && !sal ? S.c(C_RHOMJZB).p : nullptr,
-                        nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det);
+                        nj ? S.c(C_NJXB).p : nullptr, nj ? S.c(C_NJYB).p : nullptr, S.pitch, g, det); });
                     HPQ_LAUNCH_CHECK();
                     det_flush({C_JZB, C_RHOMJZB, C_NJXB, C_NJYB});
                 }
@@ -2018,7 +2033,7 @@ public:
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "plasma_push");
-            hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 0, (const int*)nullptr);
+            with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_plasma_push<R, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 0, (const int*)nullptr); });
             HPQ_LAUNCH_CHECK();
         }
         if (ex) {
@@ -2047,10 +2062,10 @@ public:
             // iterations after convergence are predicated off on the device (Ctl::pc_go)
             for (size_t s = 0; s < pl.size(); ++s) {
                 if (pl[s].n == 0) continue;
-                hpq_launch(k_plasma_push<R>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, &ctl->pc_go);
+                with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_plasma_push<R, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], S, g, 1, &ctl->pc_go); });
                 HPQ_LAUNCH_CHECK();
                 DepOut<R> o{S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, nullptr, nullptr, S.pitch};
-                hpq_launch(det.w[0] ? k_plasma_deposit<R, true> : k_plasma_deposit<R, false>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go, det);
+                with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(det.w[0] ? k_plasma_deposit<R, true, ORD> : k_plasma_deposit<R, false, ORD>, dim3(blocks_for(pl[s].n, 256)), dim3(256), 0, st, pl[s], o, g, pl[s].charge, &ctl->pc_go, det); });
                 HPQ_LAUNCH_CHECK();
                 det_flush({C_NJX, C_NJY});
             }
@@ -2071,7 +2086,7 @@ public:
         }
     }
     void deposit_beam_if(int b) {
-        hpq_launch(k_beam_deposit<R>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1, det);
+        with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(k_beam_deposit<R, ORD>, dim3(148 * 2), dim3(256), 0, st, bm[b], ctl, 1, S.c(C_NJX).p, S.c(C_NJY).p, nullptr, nullptr, S.pitch, g, 1, det); });
         HPQ_LAUNCH_CHECK();
         det_flush({C_NJX, C_NJY});
     }

@@ -74,6 +74,81 @@ static inline DShape dshape2(int type, double xmid, int ix) {
     }
 }
 
+// Orders 0..3 (ShapeFactors.H:130-197 compute_single_shape_factor, :212-468
+// single_derivative_shape_factor): B-splines of order 0, 1, 3 and their analytic (type 0), nodal
+// (1) and centred (2) derivative forms; order 2 is shape2 / dshape2 above.
+static inline Shape shapeN(int ord, double xmid, int ix) {
+    if (ord == 2) return shape2(xmid, ix);
+    if (ord == 0) return {1.0, (int)std::floor(xmid + 0.5)};
+    const double xfloor = std::floor(xmid), xint = xmid - xfloor;
+    if (ord == 1) return {ix == 0 ? 1.0 - xint : xint, (int)xfloor + ix};
+    const int c = (int)xfloor - 1 + ix;
+    if (ix == 0) return {1.0 / 6.0 * (1.0 - xint) * (1.0 - xint) * (1.0 - xint), c};
+    if (ix == 1) return {2.0 / 3.0 - xint * xint * (1.0 - xint / 2.0), c};
+    if (ix == 2) return {2.0 / 3.0 - (1.0 - xint) * (1.0 - xint) * (1.0 - 0.5 * (1.0 - xint)), c};
+    return {1.0 / 6.0 * xint * xint * xint, c};
+}
+static inline int dshape_points(int type, int ord) { return type == 2 ? ord + 3 : ord + type + 1; }
+static inline DShape dshapeN(int type, int ord, double xmid, int ix) {
+    if (ord == 2) return dshape2(type, xmid, ix);
+    if (type == 0) {
+        if (ord == 0) return {1.0, 0.0, (int)std::floor(xmid + 0.5)};
+        const double xfloor = std::floor(xmid), x = xmid - xfloor, x2 = x * x, x3 = x2 * x;
+        if (ord == 1) return ix == 0 ? DShape{1.0 - x, 1.0, (int)xfloor} : DShape{x, -1.0, (int)xfloor + 1};
+        const int c = (int)xfloor - 1 + ix;
+        if (ix == 0) return {-1.0 / 6.0 * x3 + 0.5 * x2 - 0.5 * x + 1.0 / 6.0, -(-0.5 * x2 + x - 0.5), c};
+        if (ix == 1) return {0.5 * x3 - x2 + 2.0 / 3.0, -(1.5 * x2 - 2 * x), c};
+        if (ix == 2) return {-0.5 * x3 + 0.5 * x2 + 0.5 * x + 1.0 / 6.0, -(-1.5 * x2 + x + 0.5), c};
+        return {1.0 / 6.0 * x3, -(0.5 * x2), c};
+    }
+    if (type == 1) {
+        if (ord == 0) {
+            const double xfloor = std::floor(xmid), x = xmid - xfloor;
+            const bool lo = x < 0.5;
+            return ix == 0 ? DShape{lo ? 1.0 : 0.0, 1.0, (int)xfloor} : DShape{lo ? 0.0 : 1.0, -1.0, (int)xfloor + 1};
+        }
+        const double xm = xmid + 0.5, xfloor = std::floor(xm), x = xm - xfloor, x2 = x * x, x3 = x2 * x;
+        const bool lo = x < 0.5;
+        if (ord == 1) {
+            const int c = (int)xfloor - 1 + ix;
+            if (ix == 0) return {lo ? 0.5 - x : 0.0, -(x - 1), c};
+            if (ix == 1) return {lo ? x + 0.5 : 1.5 - x, -(1 - 2 * x), c};
+            return {lo ? 0.0 : x - 0.5, -x, c};
+        }
+        const int c = (int)xfloor - 2 + ix;
+        if (ix == 0) return {lo ? -1.0 / 6.0 * x3 + 0.25 * x2 - 0.125 * x + 1.0 / 48.0 : 0.0,
+                             -(1.0 / 6.0 * x3 - 0.5 * x2 + 0.5 * x - 1.0 / 6.0), c};
+        if (ix == 1) return {lo ? 0.5 * x3 - 0.25 * x2 - 0.625 * x + 23.0 / 48.0 : -1.0 / 6.0 * x3 + 0.75 * x2 - 1.125 * x + 9.0 / 16.0,
+                             -(-2.0 / 3.0 * x3 + 1.5 * x2 - 0.5 * x - 0.5), c};
+        if (ix == 2) return {lo ? -0.5 * x3 - 0.25 * x2 + 0.625 * x + 23.0 / 48.0 : 0.5 * x3 - 1.75 * x2 + 1.375 * x + 17.0 / 48.0,
+                             -(x3 - 1.5 * x2 - 0.5 * x + 0.5), c};
+        if (ix == 3) return {lo ? 1.0 / 6.0 * x3 + 0.25 * x2 + 0.125 * x + 1.0 / 48.0 : -0.5 * x3 + 1.25 * x2 - 0.375 * x + 5.0 / 48.0,
+                             -(-2.0 / 3.0 * x3 + 0.5 * x2 + 0.5 * x + 1.0 / 6.0), c};
+        return {lo ? 0.0 : 1.0 / 6.0 * x3 - 0.25 * x2 + 0.125 * x - 1.0 / 48.0, -(1.0 / 6.0 * x3), c};
+    }
+    if (ord == 0) {
+        const int c = (int)std::floor(xmid + 0.5) - 1 + ix;
+        if (ix == 0) return {0.0, 0.5, c};
+        if (ix == 1) return {1.0, 0.0, c};
+        return {0.0, -0.5, c};
+    }
+    const double xfloor = std::floor(xmid), x = xmid - xfloor, x2 = x * x, x3 = x2 * x;
+    if (ord == 1) {
+        const int c = (int)xfloor - 1 + ix;
+        if (ix == 0) return {0.0, -(0.5 * x - 0.5), c};
+        if (ix == 1) return {1 - x, -(-0.5 * x), c};
+        if (ix == 2) return {x, -(0.5 - 0.5 * x), c};
+        return {0.0, -(0.5 * x), c};
+    }
+    const int c = (int)xfloor - 2 + ix;
+    if (ix == 0) return {0.0, -(1.0 / 12.0 * x3 - 0.25 * x2 + 0.25 * x - 1.0 / 12.0), c};
+    if (ix == 1) return {-1.0 / 6.0 * x3 + 0.5 * x2 - 0.5 * x + 1.0 / 6.0, -(-0.25 * x3 + 0.5 * x2 - 1.0 / 3.0), c};
+    if (ix == 2) return {0.5 * x3 - x2 + 2.0 / 3.0, -(1.0 / 6.0 * x3 - 0.5 * x), c};
+    if (ix == 3) return {-0.5 * x3 + 0.5 * x2 + 0.5 * x + 1.0 / 6.0, -(1.0 / 6.0 * x3 - 0.5 * x2 + 1.0 / 3.0), c};
+    if (ix == 4) return {1.0 / 6.0 * x3, -(-0.25 * x3 + 0.25 * x2 + 0.25 * x + 1.0 / 12.0), c};
+    return {0.0, -(1.0 / 12.0 * x3), c};
+}
+
 // ------------------------------------------------------------------------------------------
 // Slice field storage: nx x ny interior plus guard cells (the reference uses
 // (depos_order+1)/2+1 = 2 guards, Fields.cpp:63; one more is allocated so that stencils that
@@ -641,11 +716,6 @@ public:
     std::vector<double> pc_errors;
 
     explicit Sim(const SimConfig& c) : cfg(c) {
-        // deposition order 0 is restated for the beam deposition of a beam that does not move
-        // (BeamDepositCurrent.cpp with compute_shape_factor<0>, ShapeFactors.H:40-50): no plasma,
-        // dt = 0
-        if (c.depos_order_xy == 0 && (!c.plasmas.empty() || c.dt != 0.0))
-            throw hpq::InputError("the oracle restates hipace.depos_order_xy = 0 only for a beam in vacuum with dt = 0");
         nx = c.n_cell[0]; ny = c.n_cell[1]; nz = c.n_cell[2];
         dx = (c.prob_hi[0] - c.prob_lo[0]) / nx;
         dy = (c.prob_hi[1] - c.prob_lo[1]) / ny;
@@ -962,9 +1032,10 @@ public:
                     pl.valid[ip] = 0;
                     return;
                 }
-                for (int iy = 0; iy <= 2; ++iy)
-                    for (int ix = 0; ix <= 2; ++ix) {
-                        Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);
+                const int ord = cfg.depos_order_xy;
+                for (int iy = 0; iy <= ord; ++iy)
+                    for (int ix = 0; ix <= ord; ++ix) {
+                        Shape sx = shapeN(ord, xmid, ix), sy = shapeN(ord, ymid, iy);
                         const int i = sx.cell, j = sy.cell;
                         const double cd = q_invvol * sx.s * sy.s;
                         if (Fjx) { (*Fjx)(i, j) += cd * vx_c; (*Fjy)(i, j) += cd * vy_c; }
@@ -981,7 +1052,8 @@ public:
     // ExplicitDeposition.cpp:20-265 (no laser): Sx, Sy += plasma contribution
     void explicit_deposit() {
         const int dt = cfg.depos_derivative_type;
-        const int ns = 2 + dt;  // stencil extent - 1
+        const int ord = cfg.depos_order_xy;
+        const int ns = dshape_points(dt, ord) - 1;  // stencil extent - 1
         Field& Sx = f("Sx"); Field& Sy = f("Sy");
         const Field& Bz = f("Bz"); const Field& Ez = f("Ez");
         const Field& ExmBy = f("ExmBy"); const Field& EypBx = f("EypBx");
@@ -1001,11 +1073,11 @@ public:
                 const double cdm = charge_invvol_mu0 * pl.w[ip];
                 const double xmid = (xp - xoff) * dxi, ymid = (yp - yoff) * dyi;
                 const double gamma_psi = 0.5 * ((1. + 0.5 * 0.0) * psi_inv * psi_inv + vx * vx + vy * vy + 1.);
-                DShape shx[5], shy[5];
-                for (int k = 0; k <= ns; ++k) { shx[k] = dshape2(dt, xmid, k); shy[k] = dshape2(dt, ymid, k); }
+                DShape shx[6], shy[6];
+                for (int k = 0; k <= ns; ++k) { shx[k] = dshapeN(dt, ord, xmid, k); shy[k] = dshapeN(dt, ord, ymid, k); }
                 for (int iy = 0; iy <= ns; ++iy)
                     for (int ix = 0; ix <= ns; ++ix) {
-                        if (dt == 2 && (ix == 0 || ix == 4) && (iy == 0 || iy == 4)) continue;
+                        if (dt == 2 && (ix == 0 || ix == ns) && (iy == 0 || iy == ns)) continue;
                         const DShape& sy = shy[iy];
                         const DShape& sx = shx[ix];
                         const int i = sx.cell, j = sy.cell;
@@ -1032,17 +1104,10 @@ public:
             const double vx = p.ux * gaminv, vy = p.uy * gaminv, vz = p.uz * gaminv;
             const double wqx = wq * vx, wqy = wq * vy, wqz = wq * vz, wqr = wq * (1. - vz * clightinv);
             const double xmid = (p.x - xoff) * dxi, ymid = (p.y - yoff) * dyi;
-            if (cfg.depos_order_xy == 0) {
-                // nearest cell, weight 1
-                const int i = (int)std::floor(xmid + 0.5), j = (int)std::floor(ymid + 0.5);
-                if (jx) { (*jx)(i, j) += wqx; (*jy)(i, j) += wqy; }
-                if (jz) (*jz)(i, j) += wqz;
-                if (rmj) (*rmj)(i, j) += wqr;
-                continue;
-            }
-            for (int iy = 0; iy <= 2; ++iy)
-                for (int ix = 0; ix <= 2; ++ix) {
-                    Shape sx = shape2(xmid, ix), sy = shape2(ymid, iy);
+            const int ord = cfg.depos_order_xy;
+            for (int iy = 0; iy <= ord; ++iy)
+                for (int ix = 0; ix <= ord; ++ix) {
+                    Shape sx = shapeN(ord, xmid, ix), sy = shapeN(ord, ymid, iy);
                     const double S = sx.s * sy.s;
                     const int i = sx.cell, j = sy.cell;
                     if (jx) { (*jx)(i, j) += S * wqx; (*jy)(i, j) += S * wqy; }
@@ -1163,10 +1228,11 @@ public:
         const Field& Psi = *g_psi; const Field& FEz = *g_ez;
         const Field& FBx = *g_bx; const Field& FBy = *g_by; const Field& FBz = *g_bz;
         const double x = (xp - xoff) * dxi, y = (yp - yoff) * dyi;
-        DShape shx[4], shy[4];
-        for (int k = 0; k <= 3; k++) { shx[k] = dshape2(1, x, k); shy[k] = dshape2(1, y, k); }
-        for (int iy = 0; iy <= 3; iy++)
-            for (int ix = 0; ix <= 3; ix++) {
+        const int ord = cfg.depos_order_xy;
+        DShape shx[5], shy[5];
+        for (int k = 0; k <= ord + 1; k++) { shx[k] = dshapeN(1, ord, x, k); shy[k] = dshapeN(1, ord, y, k); }
+        for (int iy = 0; iy <= ord + 1; iy++)
+            for (int ix = 0; ix <= ord + 1; ix++) {
                 const DShape& sy = shy[iy];
                 const DShape& sx = shx[ix];
                 const int i = sx.cell, j = sy.cell;
@@ -1674,9 +1740,10 @@ public:
                 if (!pl.valid[ip]) continue;
                 const double x = (pl.x_prev[ip] - xoff) * dxi, y = (pl.y_prev[ip] - yoff) * dyi;
                 double bxp = 0, byp = 0;
-                for (int iy = 0; iy <= 2; ++iy)
-                    for (int ix = 0; ix <= 2; ++ix) {
-                        Shape sx = shape2(x, ix), sy = shape2(y, iy);
+                const int ord = cfg.depos_order_xy;
+                for (int iy = 0; iy <= ord; ++iy)
+                    for (int ix = 0; ix <= ord; ++ix) {
+                        Shape sx = shapeN(ord, x, ix), sy = shapeN(ord, y, iy);
                         bxp += sx.s * sy.s * FBx(sx.cell, sy.cell);
                         byp += sx.s * sy.s * FBy(sx.cell, sy.cell);
                     }
@@ -2461,6 +2528,20 @@ int oracle_dst1(const double* in, double* out, int n) {
     std::vector<double> v(in, in + n);
     d.transform_x(v);
     std::copy(v.begin(), v.end(), out);
+    return 0;
+}
+
+// One shape factor of the restated ShapeFactors.H: type -1 the deposit shape of order `ord`,
+// types 0/1/2 the derivative shapes (known-answer tests)
+int oracle_shape_factor(int type, int ord, double xmid, int ix, double* sv, double* dsv, int* cell) {
+    if (ord < 0 || ord > 3 || type < -1 || type > 2) return 1;
+    if (type < 0) {
+        const oracle::Shape r = oracle::shapeN(ord, xmid, ix);
+        *sv = r.s; *dsv = 0; *cell = r.cell;
+    } else {
+        const oracle::DShape r = oracle::dshapeN(type, ord, xmid, ix);
+        *sv = r.s; *dsv = r.ds; *cell = r.cell;
+    }
     return 0;
 }
 

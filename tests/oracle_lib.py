@@ -74,6 +74,8 @@ def lib():
         L.oracle_get_beam_slice.argtypes = [vp, i32, i32] + [dp] * 7 + [lp]
         L.oracle_put_beam_slice.argtypes = [vp, i32, i32] + [dp] * 7 + [lp, i64]
         L.oracle_set_time.argtypes = [vp, ctypes.c_double]
+        L.oracle_shape_factor.argtypes = [i32, i32, ctypes.c_double, i32, dp, dp, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_shape_factor.restype = i32
         L.oracle_error.argtypes = [vp]
         L.oracle_error.restype = cp
         _lib = L
