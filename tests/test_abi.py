@@ -77,10 +77,7 @@ def test_shared_prefix_keys_of_unbuilt_features_are_rejected():
             hp.Hipace(base + "\n" + extra + "\n")
         assert word in str(e.value), (extra, str(e.value))
     hp.Hipace(base + "\nplasmas.insitu_period = 0\n")  # switched off: accepted
-    # deposition orders other than 2 exist in the CPU restatement only: the library refuses them
-    # at init, before it touches the GPU
-    for extra, word in (("hipace.depos_order_xy = 0", "order 2"),):
-        sim = hp.Hipace(base + "\n" + extra + "\n")
-        with pytest.raises(hp.HpqError) as e:
-            sim.init_data()
-        assert e.value.code == 1 and word in str(e.value), str(e.value)
+    # orders outside 0..3 are rejected when the deck is read
+    with pytest.raises(hp.HpqError) as e:
+        hp.Hipace(base + "\nhipace.depos_order_xy = 4\n")
+    assert "0, 1, 2 or 3" in str(e.value)
