@@ -429,9 +429,11 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
 // ------------------------------------------------------------------------------------------
 struct MGCoarse {
     int nl;
+    int lw;          // first level run by one warp (levels of at most kWarpLevelPoints points)
     MGLev L[16];
     size_t off[16];  // level offsets (elements) in the shared-memory arena
 };
+constexpr int kWarpLevelPoints = 128;
 
 // 2-D loops over the valid points of a level (threads as 16 columns x blockDim/16 rows, no
 // integer division), all points or those of one colour ((i + j + s) even)
@@ -450,31 +452,109 @@ __device__ __forceinline__ void for_colour(const MGLev& L, int s, F f) {
     }
 }
 
-template <class R, bool CELL>
-__device__ __forceinline__ void blk_sweeps(const MGLev& L, const R* dinv, const R* res, R* cor, int nsweeps, R facx,
-                                           R facy) {
-    const int plane = L.w * L.h;
-    for (int s = 0; s < nsweeps; ++s) {
-        for_colour(L, s, [&](int i, int j) {
-            const int id = j * L.w + i;
-            const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
-            const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-            const R inv = dinv[id];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                R* p = cor + c * plane;
-                p[id] = mg_gs_inv<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], res[c * plane + id], inv, facx, facy);
-            }
-        });
-        __syncthreads();
-    }
-}
 
 // The coarse levels in one block. With `init` the coefficient hierarchy and the inverse
 // diagonals are built in the arena; without it they are the ones of an earlier call of the same
 // solve, still resident in this block's shared memory. The global arrays are plain (not
 // restrict/read-only) pointers: in the persistent solve other blocks write them earlier in the
 // same launch.
+// Thread groups of the coarse levels: the whole block (loops over 16 columns x blockDim/16 rows,
+// block barriers), or warp 0 alone for the smallest levels (lane-strided loops, warp barriers:
+// a level of a few dozen points is then a handful of instructions per step instead of a block
+// barrier). A colour sweep updates points of one colour from the other colour only, so the
+// order of the points, and the group, do not change the result.
+struct BlockGroup {
+    __device__ static void sync() { __syncthreads(); }
+    template <class F>
+    __device__ static void valid(const MGLev& L, F f) { for_valid(L, f); }
+    template <class F>
+    __device__ static void colour(const MGLev& L, int s, F f) { for_colour(L, s, f); }
+};
+struct WarpGroup {
+    __device__ static void sync() { __syncwarp(); }
+    template <class F>
+    __device__ static void valid(const MGLev& L, F f) {
+        const int vw = L.vhi_i - L.vlo + 1, n = vw * (L.vhi_j - L.vlo + 1);
+        for (int k = threadIdx.x & 31; k < n; k += 32) f(L.vlo + k % vw, L.vlo + k / vw);
+    }
+    template <class F>
+    __device__ static void colour(const MGLev& L, int s, F f) {
+        valid(L, [&](int i, int j) {
+            if (((i + j + s) & 1) == 0) f(i, j);
+        });
+    }
+};
+
+// one coarse level in the shared-memory arena: correction, right-hand side, residual,
+// coefficient, inverse diagonal (two components each for the first three)
+template <class R>
+struct CoarseLevel {
+    MGLev L;
+    R *cor, *res, *rsc, *acf, *dinv;
+    R facx, facy;
+};
+
+template <class G, class R, bool CELL>
+__device__ __forceinline__ void coarse_sweeps(const CoarseLevel<R>& A, int nsweeps) {
+    const MGLev& L = A.L;
+    const int plane = L.w * L.h;
+    for (int s = 0; s < nsweeps; ++s) {
+        G::colour(L, s, [&](int i, int j) {
+            const int id = j * L.w + i;
+            const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
+            const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
+            const R inv = A.dinv[id];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                R* p = A.cor + c * plane;
+                p[id] = mg_gs_inv<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], A.res[c * plane + id], inv, A.facx, A.facy);
+            }
+        });
+        G::sync();
+    }
+}
+
+// 4 sweeps, the residual, and its restriction into the next level's right-hand side
+template <class G, class R, bool CELL>
+__device__ __forceinline__ void coarse_down(const CoarseLevel<R>& A, const CoarseLevel<R>& C) {
+    coarse_sweeps<G, R, CELL>(A, 4);
+    const MGLev& L = A.L;
+    const int plane = L.w * L.h;
+    G::valid(L, [&](int i, int j) {
+        const int id = j * L.w + i;
+        const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
+        const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const R* p = A.cor + c * plane;
+            A.rsc[c * plane + id] = A.res[c * plane + id] + A.acf[id] * p[id] -
+                                    mg_lap<R, CELL>(L, i, j, p[id], p[im], p[ip], p[jm], p[jp], A.facx, A.facy);
+        }
+    });
+    G::sync();
+    MV<R> fine{{A.rsc, A.rsc + plane}, L.w, 0};
+    const int cplane = C.L.w * C.L.h;
+    G::valid(C.L, [&](int i, int j) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) C.res[c * cplane + j * C.L.w + i] = mg_restrict1<R, CELL>(fine, i, j, c);
+    });
+    G::sync();
+}
+
+// interpolation of the coarser correction, then 4 sweeps
+template <class G, class R, bool CELL>
+__device__ __forceinline__ void coarse_up(const CoarseLevel<R>& A, const CoarseLevel<R>& C) {
+    const MGLev& L = A.L;
+    const int plane = L.w * L.h;
+    MV<R> crse{{C.cor, C.cor + C.L.w * C.L.h}, C.L.w, 0};
+    G::valid(L, [&](int i, int j) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) A.cor[c * plane + j * L.w + i] += mg_interp1<R, CELL>(crse, i, j, c);
+    });
+    G::sync();
+    coarse_sweeps<G, R, CELL>(A, 4);
+}
+
 __device__ __forceinline__ unsigned long long tc_clock_ns();
 
 // bt (tracing only): thread 0 records the global timer at the start, after the set-up, after each
@@ -534,53 +614,34 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     }
     __syncthreads();
     bstamp();
-    R facx = facx0, facy = facy0;
-    for (int l = 0; l < M.nl; ++l) {
-        const MGLev& L = M.L[l];
-        const int plane = L.w * L.h;
-        if (l == M.nl - 1) {
-            blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 16, facx, facy);
-            bstamp();
-            break;
+    // down to the first warp level (block-wide), the smallest levels by warp 0 alone (down,
+    // coarsest, up: no block barrier between their short steps), then the block-wide up-sweep
+    const int lw = M.lw < M.nl ? M.lw : M.nl;
+    auto fac = [&](int l, R f0) {
+        for (int k = 0; k < l; ++k) f0 *= R(0.25);
+        return f0;
+    };
+    auto arena_level = [&](int l) {
+        return CoarseLevel<R>{M.L[l], cor(l), res(l), rsc(l), acf(l), dinv(l), fac(l, facx0), fac(l, facy0)};
+    };
+    for (int l = 0; l < lw && l < M.nl - 1; ++l) {
+        coarse_down<BlockGroup, R, CELL>(arena_level(l), arena_level(l + 1));
+        bstamp();
+    }
+    if (lw >= M.nl - 1 && lw == M.nl) {
+        coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), 16);
+        bstamp();
+    } else {
+        if (threadIdx.x < 32) {
+            for (int l = lw; l < M.nl - 1; ++l) coarse_down<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
+            coarse_sweeps<WarpGroup, R, CELL>(arena_level(M.nl - 1), 16);
+            for (int l = M.nl - 2; l >= lw; --l) coarse_up<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
         }
-        blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
-        for_valid(L, [&](int i, int j) {
-            const int id = j * L.w + i;
-            const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
-            const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const R* p = cor(l) + c * plane;
-                rsc(l)[c * plane + id] = res(l)[c * plane + id] + acf(l)[id] * p[id] -
-                                         mg_lap<R, CELL>(L, i, j, p[id], p[im], p[ip], p[jm], p[jp], facx, facy);
-            }
-        });
-        __syncthreads();
-        const MGLev& C = M.L[l + 1];
-        MV<R> fine{{rsc(l), rsc(l) + plane}, L.w, 0};
-        const int cplane = C.w * C.h;
-        for_valid(C, [&](int i, int j) {
-#pragma unroll
-            for (int c = 0; c < 2; ++c) res(l + 1)[c * cplane + j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, c);
-        });
         __syncthreads();
         bstamp();
-        facx *= R(0.25);
-        facy *= R(0.25);
     }
-    for (int l = M.nl - 2; l >= 0; --l) {
-        facx *= R(4.);
-        facy *= R(4.);
-        const MGLev& L = M.L[l];
-        const MGLev& C = M.L[l + 1];
-        const int plane = L.w * L.h;
-        MV<R> crse{{cor(l + 1), cor(l + 1) + C.w * C.h}, C.w, 0};
-        for_valid(L, [&](int i, int j) {
-#pragma unroll
-            for (int c = 0; c < 2; ++c) cor(l)[c * plane + j * L.w + i] += mg_interp1<R, CELL>(crse, i, j, c);
-        });
-        __syncthreads();
-        blk_sweeps<R, CELL>(L, dinv(l), res(l), cor(l), 4, facx, facy);
+    for (int l = (lw < M.nl ? lw : M.nl - 1) - 1; l >= 0; --l) {
+        coarse_up<BlockGroup, R, CELL>(arena_level(l), arena_level(l + 1));
         bstamp();
     }
     for (int k = threadIdx.x; k < 2 * n0; k += blockDim.x) cor_g[k] = cor(0)[k];
@@ -617,6 +678,7 @@ __global__ void k_mg_copy_out(MGLev L, MV<R> sol, MV<R> cor_even, MV<R> cor_odd,
 constexpr int kMGMaxLevels = 16;
 constexpr double kRefineTol = 1e-5;  // relative tolerance below which single precision refines in FP64
 constexpr long long kBarrierSpins = 1ll << 24;  // >= ~1 s of polling before giving up
+constexpr long long kBarrierFastSpins = 256;    // polls without a sleep in between
 
 template <class R>
 struct MGSolveArgs {
@@ -677,11 +739,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, int* err) {
             asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
             asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
         } else {
+            // poll without sleeping first (a barrier is released within a few microseconds),
+            // then with short sleeps
             long long it = 0;
             while (ld_acquire(bar + 1) == g) {
                 if (*verr) break;
                 if (++it > kBarrierSpins) { atomicExch(err, 1); break; }
-                __nanosleep(32);
+                if (it > kBarrierFastSpins) __nanosleep(32);
             }
         }
         s_ok = (*verr == 0);
@@ -1250,6 +1314,12 @@ public:
         if (nl - sb > 16) sb = nl - 16;
         bottom_smem = smem_from(sb);
         coarse.nl = nl - sb;
+        // HPQ_MG_WARP=0 in the environment keeps every coarse level block-wide
+        const char* ew = getenv("HPQ_MG_WARP");
+        coarse.lw = coarse.nl;
+        if (!(ew && ew[0] == '0'))
+            for (int l = sb; l < nl; ++l)
+                if ((long long)lev[l].w * lev[l].h <= kWarpLevelPoints) { coarse.lw = l - sb; break; }
         size_t off = 0;
         for (int l = sb; l < nl; ++l) {
             coarse.L[l - sb] = lev[l];
