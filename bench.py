@@ -63,6 +63,8 @@ def parse():
                    help="larger workload timed for FP64 vs mixed (one step each); '' to skip")
     p.add_argument("--adjoint-config", default="beam_loading_255",
                    help="workload of the adjoint timing (time per gradient); '' to skip")
+    p.add_argument("--large-config", default="large_2047",
+                   help="largest workload: one mixed-precision step and one adjoint gradient; '' to skip")
     return p.parse_args()
 
 
@@ -282,6 +284,10 @@ def run_ours(args):
     if rank == 0 and args.adjoint_config and args.precision == "fp64":
         line["adjoint"] = adjoint_point(args.adjoint_config, torch)
         line["salame_vs_adjoint"] = salame_vs_adjoint(args.adjoint_config)
+    if rank == 0 and args.precision == "fp64" and args.config == "blowout_255" and not args.no_mixed:
+        line["linear_wake_64"] = linear_wake_point(torch, args.no_cpu)
+        if args.large_config:
+            line["large"] = large_point(args.large_config, torch)
     if rank == 0:
         print(json.dumps(line))
     sim.close()
@@ -426,7 +432,7 @@ def mixed_vs_fp64(text, args, torch):
     matches the oracle to <= 1e-10 over a whole step of this workload in the parity tests).
     Beside it: the FP64 noise floor (FP64 with floating-point atomics against FP64 in
     deterministic mode, and FP64 with the beam's x displaced by 1e-7 of its rms size), and the
-    mixed path with one stage changed (the FP32 FFT instead of the tensor-core DST; FP64
+    mixed path with one stage changed (the TF32x3 tensor-core DST instead of the FP32 FFT; FP64
     residual refinement of the multigrid), and a weak-wake version of the workload (the driver's
     weights scaled to a peak density of 0.5), where the plasma response is closer to linear."""
     import numpy as np
@@ -461,7 +467,7 @@ def mixed_vs_fp64(text, args, torch):
                                                               ref=d64)["errors"]
     out["fp64_noise_floor"] = floor
     abl = {}
-    for name, env in (("fp32_fft_dst", {"HPQ_DST": "fft"}), ("fp64_multigrid_refinement", {"HPQ_MG_REFINE": "1"})):
+    for name, env in (("tf32x3_tensor_core_dst", {"HPQ_DST": "tc"}), ("fp64_multigrid_refinement", {"HPQ_MG_REFINE": "1"})):
         r = precision_errors(tdiag, "mixed", beam, comps, env=env, ref=d64)["errors"]
         sim = make_sim_env(text, "mixed", env)
         sim.set_beam(0, beam)
@@ -536,6 +542,69 @@ def scale_point(name, torch, sample_every=64):
                                      for c in comps}
     res["steps"] = "5 (0-4): steps 1-3 timed, steps 0 and 4 sampled"
     res["error_reference"] = "FP64 GPU path, same beam, every %d-th slice of steps 0 and 4" % sample_every
+    return res
+
+
+def linear_wake_point(torch, no_cpu=False):
+    """The CPU-runnable workload (64 x 64 x 100, predictor-corrector Bx/By with 3 iterations, 1e5
+    driver particles): all 11 steps (0-10) on the GPU in FP64 (device time) and, unless skipped,
+    in the FP64 CPU oracle on the same seeded beam (all host threads)."""
+    from cases import config
+    text = config("linear_wake_64")
+    sim = make_sim(text, "fp64", graphs=True)
+    nz = sim.n_cell[2]
+    sim.step(0)  # graph capture and warm-up (step 0 again below on a fresh simulation)
+    sim.close()
+    sim = make_sim(text, "fp64", graphs=True)
+    secs = time_device_steps(sim, 0, 11, torch)
+    sim.close()
+    res = {"workload": "linear_wake_64", "grid": [64, 64, nz], "steps": 11, "gpu_slices_per_s": 11 * nz / secs,
+           "gpu_ms_per_step": secs / 11 * 1e3}
+    if not no_cpu:
+        o, dt = oracle_run(text, 0, 11)
+        res["cpu_oracle_slices_per_s"] = 11 * nz / dt
+        res["cpu_oracle_threads"] = o.L.oracle_threads()
+        res["gpu_over_cpu"] = res["gpu_slices_per_s"] / res["cpu_oracle_slices_per_s"]
+    return res
+
+
+def large_point(name, torch):
+    """The largest workload (2047 x 2047 x 2048, 4.2M plasma particles, 1.2e7 beam particles): one
+    mixed-precision step (device time) and one adjoint gradient with its forward (FP64, wall time
+    between device synchronisations), with the device memory in use."""
+    import numpy as np
+    import hipace2_b200 as hp
+    from cases import adjoint_knots, config
+    text = config(name)
+    res = {"workload": name, "grid": [int(v) for v in _n_cell(text)]}
+    sim = make_sim(text, "mixed", graphs=True)
+    nz = sim.n_cell[2]
+    sim.step(0)
+    secs = time_device_steps(sim, 1, 1, torch)
+    res["mixed_slices_per_s"] = nz / secs
+    res["mixed_ms_per_step"] = secs * 1e3
+    sim.close()
+    sim = hp.Hipace(text, graphs=True)
+    sim.init_data()
+    theta = adjoint_knots(n_profile=int(_key(text, "adjoint.n_profile_knots")),
+                          n_density=int(_key(text, "adjoint.n_density_knots")))
+    sim.adjoint(theta, grad=False)  # allocation of the records and checkpoints, graph capture
+    sim.synchronize()
+    t0 = time.perf_counter()
+    sim.adjoint(theta, grad=False)
+    sim.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J, g = sim.adjoint(theta)
+    sim.synchronize()
+    t_grad = time.perf_counter() - t0
+    free, total = torch.cuda.mem_get_info()
+    sim.close()
+    res.update({"adjoint_seconds_forward": t_fwd, "adjoint_seconds_per_gradient": t_grad,
+                "gradient_over_forward": t_grad / t_fwd, "adjoint_dtype": "f64",
+                "device_memory_in_use_gb_at_gradient": (total - free) / 1e9,
+                "objective": J, "max_abs_grad": float(np.abs(g).max()),
+                "checkpoint_interval": int(_key(text, "adjoint.checkpoint_interval"))})
     return res
 
 

@@ -505,15 +505,15 @@ public:
         HPQ_CUDA(cudaMemset(ctl, 0, sizeof(Ctl)));
         HPQ_CUDA(cudaMallocHost(&ctl_h, sizeof(Ctl)));
         std::memset(ctl_h, 0, sizeof(Ctl));
-        // Poisson form: single precision uses the tensor-core sine GEMMs (O(n^3)) up to 1023^2 and
-        // the FP32 FFT (O(n^2 log n)) on larger 2^k - 1 grids, where it is faster (2047^2: 266 vs
-        // 249 slices/s; 1023^2: 582 vs 608); HPQ_DST=tc / fft / gemm (SIMT sine GEMMs on every
-        // grid, cross-checks) forces a form; double precision uses the FFT where the grid allows
-        // it, else the SIMT GEMMs
+        // Poisson form: single precision uses the radix-2 FP32 FFT on 2^k - 1 grids (at 255^2 as
+        // fast as the tensor-core GEMMs, 3438 vs 3429 slices/s, with 2.5x less error in Ez: 5.2e-4
+        // vs 1.3e-3 of FP64 in the blowout; at 2047^2 faster, 266 vs 249; at 1023^2 4 % slower,
+        // 582 vs 608) and the tensor-core sine GEMMs (TF32x3) on other grids up to 1023^2;
+        // HPQ_DST=tc / fft / gemm (SIMT sine GEMMs on every grid, cross-checks) forces a form;
+        // double precision uses the FFT (radix 2, or Bluestein for other lengths)
         const char* env = getenv("HPQ_DST");
         std::string dmode = env ? env : "";
-        if (dmode.empty() && std::is_same<R, float>::value && FastDST<R>::supported(nx, ny) && std::max(nx, ny) >= 2047)
-            dmode = "fft";
+        if (dmode.empty() && std::is_same<R, float>::value && FastDST<R>::radix2(nx, ny)) dmode = "fft";
         if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); if (sal_dst.nx) sal_dst.set_mode(false); }
         else if (dmode != "fft" && std::is_same<R, float>::value) {
             dst.set_tensor_mode(&ctl->tc_err);

@@ -428,3 +428,30 @@ def test_mixed_loose_tolerance_plain_fp32_multigrid():
     assert errs["Ez"] <= 1e-4 and errs["Psi"] <= 1e-4, errs
     assert errs["Bx"] <= 1e-3, errs
     assert v_mix <= 1.5 * v_ref + 8, (v_mix, v_ref)
+
+
+@pytest.mark.parametrize("name", sorted(k for k in GOLDEN if GOLDEN[k].get("oracle_only")
+                                         and not GOLDEN[k].get("beam_after_steps")))
+def test_remaining_goldens_on_gpu(name):
+    """The goldens first pinned on the oracle alone: SI units, deposition order 0 on a 512 x 768
+    grid (both transverse lengths go through the Bluestein DST), the serial blowout deck (made by
+    the reference with the AB5 pusher, checked at that test's own tolerance)."""
+    case = GOLDEN[name]
+    comps = sorted(case["fields"])
+    g, o = run_pair(case["input"], comps, 1)
+    rtol = max(1e-7, case["rtol_cpu"])
+    for k in comps:
+        a, b = g.get_diag(k), o.get_diag(k)
+        assert rel_l2(a, b) <= 1e-10, (k, rel_l2(a, b))
+        assert np.abs(a).sum() == pytest.approx(case["fields"][k], rel=rtol, abs=1e-300), k
+
+
+def test_bluestein_dst_on_odd_grids_matches_oracle():
+    """Grids whose 2(n + 1) is not a power of two (100 x 72 and 45 x 33) take the Bluestein FFT
+    DST in FP64; the whole slice march must match the oracle."""
+    for shape in ("100 72 24", "45 33 24"):
+        text = EXPLICIT_MOVING.replace("amr.n_cell = 33 33 40", "amr.n_cell = " + shape)
+        g, o = run_pair(text, EXPLICIT_COMPS, 2)
+        for k in EXPLICIT_COMPS:
+            e = rel_l2(g.get_diag(k), o.get_diag(k))
+            assert e <= 1e-10, (shape, k, e)
