@@ -320,6 +320,7 @@ template <class R>
 struct DepOut {
     R *jx, *jy, *jz, *rho, *chi, *rhomjz;
     int pitch;
+    int merge;  // order 2, floating-point atomics: warp-merged stencils (plasma_deposit_merged)
 };
 
 // Deterministic deposition (hpq_set_deterministic). Floating-point atomics give sums whose last
@@ -387,6 +388,97 @@ __device__ __forceinline__ R plasma_mid(const float* ref, long long ip, R x, R o
     return plasma_mid_v<R>(ref != nullptr, ref ? ref[ip] : 0.f, x, off, dxi, n, base);
 }
 
+// Warp-merged order-2 plasma deposition. The lanes of a warp hold consecutive particles; in a
+// plasma still in lattice (or reorder) order, lane l + 1 sits one cell to the right of lane l in
+// the same row, and their 3 x 3 stencils share two columns. Each lane then deposits its centre
+// column with the right column of lane l - 1 and the left column of lane l + 1 added in (their
+// shapes and weights come by shuffle); a lane deposits its own left/right column only where it has
+// no such neighbour. Lattice-ordered rows need a third of the atomics of the plain deposit; the
+// sums per cell are the same terms in another order.
+template <class R>
+__device__ __forceinline__ void plasma_deposit_merged(const PlasmaDev<R>& P, const DepOut<R>& o, const Geo& g,
+                                                      R charge_invvol, R q_mu0_mass_ratio) {
+    const R clight = (R)g.c, clightinv = (R)(1.0 / g.c);
+    const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
+    const R qsa = (R)P.qsa_max;
+    const int lane = threadIdx.x & 31;
+    const long long stride = gstride();
+    const DetAcc nodet{};
+    for (long long base = gtid() - lane; base < P.n; base += stride) {
+        const long long ip = base + lane;
+        bool act = ip < P.n && P.valid[ip];
+        R qv = 0, f[5] = {0, 0, 0, 0, 0}, sxs[3] = {0, 0, 0}, sys[3] = {0, 0, 0};
+        int cx = 0, cy = 0;
+        if (act) {
+            const R psis = P.psi[ip];
+            const R psi_inv = P.ru ? R(1) / (R(1) + psis) : R(1) / psis;
+            const R vx_c = P.ux[ip] * psi_inv, vy_c = P.uy[ip] * psi_inv;
+            int bx, by;
+            const R xmid = plasma_mid<R>(P.ru, ip, P.x[ip], xoff, dxi, g.nx, bx);
+            const R ymid = plasma_mid<R>(P.rv, ip, P.y[ip], yoff, dyi, g.ny, by);
+            const R gamma_psi = R(0.5) * (psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                          vy_c * vy_c * clightinv * clightinv + R(1));
+            const R gpm1 = P.ru ? R(0.5) * (-psis * (R(2) + psis) * psi_inv * psi_inv + vx_c * vx_c * clightinv * clightinv +
+                                            vy_c * vy_c * clightinv * clightinv)
+                                : gamma_psi - R(1);
+            if (gamma_psi < R(0) || gamma_psi > qsa || psi_inv < R(0)) {
+                P.w[ip] = R(0);
+                P.valid[ip] = 0;
+                act = false;
+            } else {
+                qv = charge_invvol * P.w[ip];
+                f[0] = vx_c; f[1] = vy_c; f[2] = gpm1 * clight; f[3] = gamma_psi; f[4] = q_mu0_mass_ratio * psi_inv;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const Sh<R> a = shape2<R>(xmid, k), b = shape2<R>(ymid, k);
+                    sxs[k] = a.s; sys[k] = b.s;
+                    if (k == 1) { cx = a.cell + bx; cy = b.cell + by; }
+                }
+            }
+        }
+        // links to the right neighbour, and from the left one
+        const int cxn = __shfl_down_sync(0xffffffffu, cx, 1), cyn = __shfl_down_sync(0xffffffffu, cy, 1);
+        const bool actn = __shfl_down_sync(0xffffffffu, act, 1);
+        const bool right = act && lane < 31 && actn && cyn == cy && cxn == cx + 1;
+        const bool left = __shfl_up_sync(0xffffffffu, right, 1) && lane > 0;
+        // the neighbours' weights: right lane's left column, left lane's right column
+        const R qn = __shfl_down_sync(0xffffffffu, qv * sxs[0], 1), qp = __shfl_up_sync(0xffffffffu, qv * sxs[2], 1);
+        R syn[3], syp[3], fn[5], fp[5];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            syn[k] = __shfl_down_sync(0xffffffffu, sys[k], 1);
+            syp[k] = __shfl_up_sync(0xffffffffu, sys[k], 1);
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            fn[k] = __shfl_down_sync(0xffffffffu, f[k], 1);
+            fp[k] = __shfl_up_sync(0xffffffffu, f[k], 1);
+        }
+        if (!act) continue;
+        R* planes[5] = {o.jx, o.jy, o.jz, o.rho, o.chi};
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            const int j = cy - 1 + iy;
+            const R wc = qv * sxs[1] * sys[iy];
+            const R wr = right ? qn * syn[iy] : R(0);
+            const R wl = left ? qp * syp[iy] : R(0);
+            const R w0 = qv * sxs[0] * sys[iy], w2 = qv * sxs[2] * sys[iy];
+#pragma unroll
+            for (int p = 0; p < 5; ++p) {
+                if (!planes[p]) continue;
+                addd<false>(nodet, planes[p], o.pitch, cx, j, wc * f[p] + wr * fn[p] + wl * fp[p]);
+                if (!left) addd<false>(nodet, planes[p], o.pitch, cx - 1, j, w0 * f[p]);
+                if (!right) addd<false>(nodet, planes[p], o.pitch, cx + 1, j, w2 * f[p]);
+            }
+            if (o.rhomjz) {
+                addd<false>(nodet, o.rhomjz, o.pitch, cx, j, wc + wr + wl);
+                if (!left) addd<false>(nodet, o.rhomjz, o.pitch, cx - 1, j, w0);
+                if (!right) addd<false>(nodet, o.rhomjz, o.pitch, cx + 1, j, w2);
+            }
+        }
+    }
+}
+
 template <class R, bool DET, int ORD = 2>
 __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R> o, Geo g, double charge,
                                                         const int* gate, DetAcc det) {
@@ -398,6 +490,12 @@ __global__ void __launch_bounds__(256) k_plasma_deposit(PlasmaDev<R> P, DepOut<R
     const R q_mu0_mass_ratio = (R)(charge * g.mu0 / P.mass);
     const R xoff = (R)g.xoff, yoff = (R)g.yoff, dxi = (R)g.dxi[0], dyi = (R)g.dxi[1];
     const R qsa = (R)P.qsa_max;
+    if constexpr (!DET && ORD == 2) {
+        if (o.merge) {
+            plasma_deposit_merged<R>(P, o, g, charge_invvol, q_mu0_mass_ratio);
+            return;
+        }
+    }
     // the attributes of the thread's next particle are loaded before the atomics of the current
     // one, so that two particles' loads are in flight per thread
     struct Pt {

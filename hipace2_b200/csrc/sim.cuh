@@ -1142,9 +1142,16 @@ public:
         if (st_host.mg_status == 2) throw CudaError("hpmg: diverged");
     }
 
+    // warp-merged order-2 plasma deposit (plasma_deposit_merged); HPQ_DEPOSIT_MERGE=1/0 in the
+    // environment switches it on/off
+    int deposit_merge = -1;
     void deposit_plasma(int sp, R* jx, R* jy, R* jz, R* rho, R* chi, R* rhomjz) {
         if (pl[sp].n == 0) return;
-        DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch};
+        if (deposit_merge < 0) {
+            const char* e = getenv("HPQ_DEPOSIT_MERGE");
+            deposit_merge = (e && e[0] == '1') ? 1 : 0;
+        }
+        DepOut<R> o{jx, jy, jz, rho, chi, rhomjz, S.pitch, deposit_merge};
         Scope sc(this, "plasma_deposit");
         with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(det.w[0] ? k_plasma_deposit<R, true, ORD> : k_plasma_deposit<R, false, ORD>, dim3(blocks_for(pl[sp].n, 256)), dim3(256), 0, st, pl[sp], o, g, pl[sp].charge, (const int*)nullptr, det); });
         HPQ_LAUNCH_CHECK();
