@@ -467,7 +467,8 @@ def mixed_vs_fp64(text, args, torch):
                                                               ref=d64)["errors"]
     out["fp64_noise_floor"] = floor
     abl = {}
-    for name, env in (("tf32x3_tensor_core_dst", {"HPQ_DST": "tc"}), ("fp64_multigrid_refinement", {"HPQ_MG_REFINE": "1"})):
+    for name, env in (("tf32x3_tensor_core_dst", {"HPQ_DST": "tc"}), ("bf16x3_tensor_core_dst", {"HPQ_DST": "tc_bf16"}),
+                      ("fp64_multigrid_refinement", {"HPQ_MG_REFINE": "1"})):
         r = precision_errors(tdiag, "mixed", beam, comps, env=env, ref=d64)["errors"]
         sim = make_sim_env(text, "mixed", env)
         sim.set_beam(0, beam)

@@ -122,12 +122,13 @@ public:
         if (use_fft) { sk = nx * ny; sj = nx; }
         else { sk = nx; sj = nrhs_max * nx; }
     }
-    // tensor-core sine GEMMs (TF32x3) for the single-precision path; err receives the kernels'
-    // error code
-    void set_tensor_mode(int* err) {
+    // tensor-core sine GEMMs (TF32x3, or BF16x3 with bf16) for the single-precision path; err
+    // receives the kernels' error code
+    void set_tensor_mode(int* err, bool bf16 = false) {
         if constexpr (std::is_same<R, float>::value) {
             if (!TcDST::supported(nx, ny)) return;
-            if (!tcd.stage) tcd.init(nx, ny, dx_, dy_, nrhs_max, err);
+            if (tcd.stage && tcd.bf16 != bf16) tcd.release();
+            if (!tcd.stage) tcd.init(nx, ny, dx_, dy_, nrhs_max, err, bf16);
             use_tc = true;
             use_fft = false;
             stage = tcd.stage;

@@ -509,16 +509,18 @@ public:
         // fast as the tensor-core GEMMs, 3438 vs 3429 slices/s, with 2.5x less error in Ez: 5.2e-4
         // vs 1.3e-3 of FP64 in the blowout; at 2047^2 faster, 266 vs 249; at 1023^2 4 % slower,
         // 582 vs 608) and the tensor-core sine GEMMs (TF32x3) on other grids up to 1023^2;
-        // HPQ_DST=tc / fft / gemm (SIMT sine GEMMs on every grid, cross-checks) forces a form;
+        // HPQ_DST=tc / tc_bf16 (BF16x3 tensor-core GEMMs) / fft / gemm (SIMT sine GEMMs on every
+        // grid, cross-checks) forces a form;
         // double precision uses the FFT (radix 2, or Bluestein for other lengths)
         const char* env = getenv("HPQ_DST");
         std::string dmode = env ? env : "";
         if (dmode.empty() && std::is_same<R, float>::value && FastDST<R>::radix2(nx, ny)) dmode = "fft";
         if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); if (sal_dst.nx) sal_dst.set_mode(false); }
         else if (dmode != "fft" && std::is_same<R, float>::value) {
-            dst.set_tensor_mode(&ctl->tc_err);
-            pc_dst.set_tensor_mode(&ctl->tc_err);
-            if (sal_dst.nx) sal_dst.set_tensor_mode(&ctl->tc_err);
+            const bool bf16 = dmode == "tc_bf16";
+            dst.set_tensor_mode(&ctl->tc_err, bf16);
+            pc_dst.set_tensor_mode(&ctl->tc_err, bf16);
+            if (sal_dst.nx) sal_dst.set_tensor_mode(&ctl->tc_err, bf16);
         }
         init_plasma_lattices();
         insitu_alloc();

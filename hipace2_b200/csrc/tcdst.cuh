@@ -154,6 +154,39 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 __host__ __device__ __forceinline__ uint32_t tf32_bits(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
 
 
+// one row's 16 consecutive output columns nb0 .. nb0+15 of a tile, through the epilogue mode
+__device__ __forceinline__ void epilogue16(const Epi& epi, int r, int k, int a, int nb0, float (&v)[16]) {
+    if (epi.mode == EPI_ROW || epi.mode == EPI_EIG) {
+        if (epi.mode == EPI_EIG) {
+            const float* e = epi.eigT + (size_t)a * epi.lde + nb0;
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                if (nb0 + q < epi.nb) v[q] *= e[q];
+        }
+        float* o = epi.out + (size_t)r * epi.ldo + nb0;
+        if (nb0 + 16 <= epi.nb) {
+#pragma unroll
+            for (int q = 0; q < 16; q += 4)
+                *reinterpret_cast<float4*>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                if (nb0 + q < epi.nb) o[q] = v[q];
+        }
+    } else if (epi.mode == EPI_TRANS) {
+        float* o = epi.out + ((size_t)k * epi.nb + nb0) * epi.ldo + a;
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+            if (nb0 + q < epi.nb) o[(size_t)q * epi.ldo] = v[q];
+    } else {
+        float* o = epi.base + (size_t)epi.comp[k] * epi.cstride + (size_t)(a + kGuardAlloc) * epi.pitch +
+                   kGuardAlloc + nb0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+            if (nb0 + q < epi.nb) o[q] = v[q];
+    }
+}
+
 template <int BN, int ST>
 struct Smem {
     static constexpr int A_BYTES = BM * BK * 4;
@@ -307,40 +340,218 @@ __global__ void __launch_bounds__(kThreads, 1)
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
                 if (!rv) continue;
-                const int nb0 = n0 + c;
-                if (epi.mode == EPI_ROW || epi.mode == EPI_EIG) {
-                    if (epi.mode == EPI_EIG) {
-                        const float* e = epi.eigT + (size_t)a * epi.lde + nb0;
-#pragma unroll
-                        for (int q = 0; q < 16; ++q)
-                            if (nb0 + q < epi.nb) v[q] *= e[q];
-                    }
-                    float* o = epi.out + (size_t)r * epi.ldo + nb0;
-                    if (nb0 + 16 <= epi.nb) {
-#pragma unroll
-                        for (int q = 0; q < 16; q += 4)
-                            *reinterpret_cast<float4*>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 16; ++q)
-                            if (nb0 + q < epi.nb) o[q] = v[q];
-                    }
-                } else if (epi.mode == EPI_TRANS) {
-                    float* o = epi.out + ((size_t)k * epi.nb + nb0) * epi.ldo + a;
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (nb0 + q < epi.nb) o[(size_t)q * epi.ldo] = v[q];
-                } else {
-                    float* o = epi.base + (size_t)epi.comp[k] * epi.cstride + (size_t)(a + kGuardAlloc) * epi.pitch +
-                               kGuardAlloc + nb0;
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (nb0 + q < epi.nb) o[q] = v[q];
-                }
+                epilogue16(epi, r, k, a, n0 + c, v);
             }
         }
     }
     // ---------------- teardown: every MMA has completed before the tensor memory is freed
+    if (warp == 5 && lane == 0) mbar_wait(accf, 0, nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// BF16x3 variant of the same GEMM: a = a_hi + a_lo with a_hi = bf16(a), a_lo = bf16(a - a_hi),
+// D = A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 by tcgen05.mma kind::f16 (both
+// operands bf16). A k-block is 64 elements: two FP32 TMA boxes of 128 x 32 land in shared memory
+// and the converter warps write the bf16 hi and lo tiles (128 x 64, one 128-byte row per tile
+// row, in the same 128-byte swizzle: 16-byte chunk c of row r at chunk c ^ (r % 8)); B hi/lo are
+// bf16 on the host and arrive by TMA. 4 MMAs of K = 16 per product and k-block.
+// Relative error per product ~2^-16 (TF32x3: ~2^-20), at twice the tensor rate of TF32.
+// ------------------------------------------------------------------------------------------
+constexpr int BK16 = 64;  // bf16 per 128-byte swizzled row
+
+// instruction descriptor: D f32, A and B bf16 (kind::f16), both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+// round-to-nearest-even bf16 of an fp32 bit pattern (finite inputs)
+__host__ __device__ __forceinline__ uint32_t bf16_bits(uint32_t b) { return (b + 0x7FFFu + ((b >> 16) & 1u)) >> 16; }
+__device__ __forceinline__ uint32_t bf16_hi_lo(float a, uint32_t& lo) {
+    const uint32_t h = bf16_bits(__float_as_uint(a));
+    const float r = a - __uint_as_float(h << 16);
+    lo = bf16_bits(__float_as_uint(r));
+    return h;
+}
+
+template <int BN, int ST>
+struct Smem16 {
+    static constexpr int F_BYTES = BM * 32 * 4;                    // one fp32 TMA box (128 x 32)
+    static constexpr int A_BYTES = BM * BK16 * 2;                  // one bf16 A tile (128 x 64)
+    static constexpr int B_BYTES = BN * BK16 * 2;                  // one bf16 B tile
+    static constexpr int STAGE = 2 * F_BYTES + 2 * A_BYTES + 2 * B_BYTES;  // F0, F1, A_hi, A_lo, B_hi, B_lo
+    static constexpr int BAR_OFF = ST * STAGE;
+    static constexpr int NBAR = 3 * ST + 2;
+    static constexpr int TOTAL = BAR_OFF + 8 * NBAR + 16 + 1024;
+};
+
+template <int BN, int ST>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_gemm_bf16(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mBh,
+                   const __grid_constant__ CUtensorMap mBl, int M, int num_kb, Epi epi, int* err) {
+    HPQ_PDL_ENTRY();
+    using L = Smem16<BN, ST>;
+    extern __shared__ unsigned char smem_dyn[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + L::BAR_OFF);
+    uint64_t* conv = full + ST;
+    uint64_t* empty = conv + ST;
+    uint64_t* accf = empty + ST;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(full + L::NBAR);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(conv + s, 4);
+            mbar_init(empty + s, 1);
+        }
+        mbar_init(accf, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    auto raise = [&](int code) {
+        *abort = 1;
+        atomicExch(err, code);
+    };
+
+    if (warp == 4) {
+        // ---------------- TMA producer: two fp32 boxes of A, the bf16 B hi/lo tiles
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < num_kb; ++kb) {
+                const int s = kb % ST;
+                const uint32_t ph = (uint32_t)(kb / ST) & 1u;
+                if (kb >= ST && !mbar_wait(empty + s, ph ^ 1u, abort)) {
+                    if (!*abort) raise(11);
+                    break;
+                }
+                unsigned char* st = sm + s * L::STAGE;
+                mbar_expect_tx(full + s, (uint32_t)(2 * L::F_BYTES + 2 * L::B_BYTES));
+                tma_load_2d(st, &mA, full + s, kb * BK16, m0);
+                tma_load_2d(st + L::F_BYTES, &mA, full + s, kb * BK16 + 32, m0);
+                unsigned char* bst = st + 2 * L::F_BYTES + 2 * L::A_BYTES;
+                tma_load_2d(bst, &mBh, full + s, kb * BK16, n0);
+                tma_load_2d(bst + L::B_BYTES, &mBl, full + s, kb * BK16, n0);
+                issued = kb + 1;
+            }
+            for (int kb = (issued > ST ? issued - ST : 0); kb < issued; ++kb)
+                mbar_wait(full + kb % ST, (uint32_t)(kb / ST) & 1u, nullptr);
+        }
+    } else if (warp == 5) {
+        // ---------------- MMA issue (one thread)
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(BM, BN);
+            for (int kb = 0; kb < num_kb; ++kb) {
+                const int s = kb % ST;
+                const uint32_t ph = (uint32_t)(kb / ST) & 1u;
+                if (!mbar_wait(conv + s, ph, abort)) {
+                    if (!*abort) raise(12);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ah = smem_u32(sm + s * L::STAGE + 2 * L::F_BYTES);
+                const uint32_t al = ah + L::A_BYTES;
+                const uint32_t bh = ah + 2 * L::A_BYTES;
+                const uint32_t bl = bh + L::B_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < BK16 / 16; ++kk) {
+                    const uint32_t o = 32u * kk;
+                    mma_bf16(tmem, desc_sw128(ah + o), desc_sw128(bh + o), idesc, (kb | kk) != 0 ? 1u : 0u);
+                    mma_bf16(tmem, desc_sw128(ah + o), desc_sw128(bl + o), idesc, 1u);
+                    mma_bf16(tmem, desc_sw128(al + o), desc_sw128(bh + o), idesc, 1u);
+                }
+                mma_commit(empty + s);
+            }
+            mma_commit(accf);
+        }
+    } else {
+        // ---------------- warps 0-3: fp32 boxes -> bf16 hi/lo tiles, then the epilogue
+        bool ok = true;
+        for (int kb = 0; kb < num_kb && ok; ++kb) {
+            const int s = kb % ST;
+            const uint32_t ph = (uint32_t)(kb / ST) & 1u;
+            ok = mbar_wait(full + s, ph, abort);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0 && !*abort) raise(13);
+                ok = false;
+                break;
+            }
+            const unsigned char* f = sm + s * L::STAGE;
+            unsigned char* hi = sm + s * L::STAGE + 2 * L::F_BYTES;
+            unsigned char* lo = hi + L::A_BYTES;
+            // output chunk (r, c): bf16 k = 8c .. 8c+7 of row r, from fp32 box c / 4, fp32 chunks
+            // 2 (c % 4) and 2 (c % 4) + 1 of that row
+#pragma unroll 2
+            for (int e = threadIdx.x; e < BM * 8; e += 128) {
+                const int r = e >> 3, c = e & 7;
+                const int sw = r & 7;
+                const unsigned char* box = f + (c >> 2) * L::F_BYTES + r * 128;
+                const int q0 = 2 * (c & 3);
+                const float4 v0 = *reinterpret_cast<const float4*>(box + ((q0 ^ sw) << 4));
+                const float4 v1 = *reinterpret_cast<const float4*>(box + (((q0 + 1) ^ sw) << 4));
+                const float a[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+                uint32_t h[8], l[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) h[t] = bf16_hi_lo(a[t], l[t]);
+                const uint4 hv = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+                const uint4 lv = make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16), l[6] | (l[7] << 16));
+                *reinterpret_cast<uint4*>(hi + r * 128 + ((c ^ sw) << 4)) = hv;
+                *reinterpret_cast<uint4*>(lo + r * 128 + ((c ^ sw) << 4)) = lv;
+            }
+            // generic-proxy writes become visible to the tensor core's reads; the MMA waits for
+            // the arrivals of all four converter warps
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(conv + s);
+        }
+        if (ok) {
+            ok = mbar_wait(accf, 0, abort);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0 && !*abort) raise(14);
+                ok = false;
+            }
+        }
+        if (ok) {
+            tc_fence_after();
+            const int r = m0 + warp * 32 + lane;
+            const bool rv = r < M;
+            const int k = rv ? r / epi.na : 0, a = rv ? r - k * epi.na : 0;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+                if (!rv) continue;
+                epilogue16(epi, r, k, a, n0 + c, v);
+            }
+        }
+    }
     if (warp == 5 && lane == 0) mbar_wait(accf, 0, nullptr);
     tc_fence_before();
     __syncthreads();
@@ -356,6 +567,20 @@ inline float host_tf32(double x) {
     uint32_t b;
     std::memcpy(&b, &f, 4);
     b = tf32_bits(b);
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+// bf16 of a double, rounded to nearest even through fp32
+inline uint16_t host_bf16(double x) {
+    const float f = (float)x;
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    return (uint16_t)bf16_bits(b);
+}
+inline double bf16_value(uint16_t h) {
+    const uint32_t b = (uint32_t)h << 16;
+    float f;
     std::memcpy(&f, &b, 4);
     return f;
 }
@@ -392,6 +617,22 @@ inline CUtensorMap make_map(const float* ptr, int inner, int rows, int box_rows)
     return m;
 }
 
+// row-major bf16 matrix `rows` x `inner` (inner = row pitch, a multiple of 8), tiles of
+// box_rows x 64 in the 128-byte swizzle; reads outside the matrix return zeros
+inline CUtensorMap make_map16(const uint16_t* ptr, int inner, int rows, int box_rows) {
+    if (inner % 8 || (reinterpret_cast<uintptr_t>(ptr) & 15)) throw CudaError("tensor map: unaligned operand");
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)inner * sizeof(uint16_t)};
+    const cuuint32_t box[2] = {(cuuint32_t)BK16, (cuuint32_t)box_rows};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t*>(ptr), dims,
+                                      strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
 }  // namespace tc
 
 // Host side of the tensor-core DST solve (single precision). Buffers: stage [k][j][i] (pitch px),
@@ -405,11 +646,15 @@ public:
     int* err = nullptr;  // device error code of the last failing CTA (0 = none)
     CUtensorMap m_stage{}, m_w1{}, m_w2{}, m_w3{}, m_sxh{}, m_sxl{}, m_syh{}, m_syl{};
     int bn = 128;
+    // BF16x3 form (kind::f16 MMAs on bf16 hi/lo splits): the sines are bf16 tables with row
+    // pitches padded to multiples of 8 (16-byte TMA strides)
+    bool bf16 = false;
+    uint16_t *bxh = nullptr, *bxl = nullptr, *byh = nullptr, *byl = nullptr;
 
     static bool supported(int nx, int ny) { return nx >= 16 && ny >= 16; }
 
-    void init(int nx_, int ny_, double dx, double dy, int nrhs_, int* err_dev) {
-        nx = nx_; ny = ny_; nrhs = nrhs_; err = err_dev;
+    void init(int nx_, int ny_, double dx, double dy, int nrhs_, int* err_dev, bool bf16_ = false) {
+        nx = nx_; ny = ny_; nrhs = nrhs_; err = err_dev; bf16 = bf16_;
         px = (nx + 3) & ~3;
         py = (ny + 3) & ~3;
         const double pi = 3.14159265358979323846;
@@ -424,9 +669,22 @@ public:
                     lo[(size_t)a * p + b] = tc::host_tf32(v - (double)h);
                 }
         };
+        auto sine16 = [&](int n, int p, std::vector<uint16_t>& hi, std::vector<uint16_t>& lo) {
+            hi.assign((size_t)p * p, 0);
+            lo.assign((size_t)p * p, 0);
+            for (int a = 0; a < n; ++a)
+                for (int b = 0; b < n; ++b) {
+                    const double v = sin(pi * (double)(a + 1) * (b + 1) / (n + 1));
+                    const uint16_t h = tc::host_bf16(v);
+                    hi[(size_t)a * p + b] = h;
+                    lo[(size_t)a * p + b] = tc::host_bf16(v - tc::bf16_value(h));
+                }
+        };
         std::vector<float> hxh, hxl, hyh, hyl;
-        sine(nx, px, hxh, hxl);
-        sine(ny, py, hyh, hyl);
+        if (!bf16) {
+            sine(nx, px, hxh, hxl);
+            sine(ny, py, hyh, hyl);
+        }
         std::vector<float> he((size_t)nx * py, 0.f);
         const double sxf = pi / (2. * (nx + 1)), syf = pi / (2. * (ny + 1));
         const double norm = (2.0 / (nx + 1)) * (2.0 / (ny + 1));
@@ -440,7 +698,19 @@ public:
             HPQ_CUDA(cudaMalloc(&d, h.size() * sizeof(float)));
             HPQ_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
         };
-        upload(sxh, hxh); upload(sxl, hxl); upload(syh, hyh); upload(syl, hyl); upload(eigT, he);
+        upload(eigT, he);
+        if (!bf16) {
+            upload(sxh, hxh); upload(sxl, hxl); upload(syh, hyh); upload(syl, hyl);
+        } else {
+            const int qx = (nx + 7) & ~7, qy = (ny + 7) & ~7;
+            auto upload16 = [&](uint16_t*& d, const std::vector<uint16_t>& h) {
+                HPQ_CUDA(cudaMalloc(&d, h.size() * sizeof(uint16_t)));
+                HPQ_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+            };
+            std::vector<uint16_t> h, l;
+            sine16(nx, qx, h, l); upload16(bxh, h); upload16(bxl, l);
+            sine16(ny, qy, h, l); upload16(byh, h); upload16(byl, l);
+        }
         auto zeros = [&](float*& d, size_t n) {
             HPQ_CUDA(cudaMalloc(&d, n * sizeof(float)));
             HPQ_CUDA(cudaMemset(d, 0, n * sizeof(float)));
@@ -459,16 +729,36 @@ public:
         m_w1 = tc::make_map(w1, py, nrhs * nx, tc::BM);
         m_w2 = tc::make_map(w2, py, nrhs * nx, tc::BM);
         m_w3 = tc::make_map(w3, px, nrhs * ny, tc::BM);
-        m_sxh = tc::make_map(sxh, px, px, bn);
-        m_sxl = tc::make_map(sxl, px, px, bn);
-        m_syh = tc::make_map(syh, py, py, bn);
-        m_syl = tc::make_map(syl, py, py, bn);
-        set_attrs<128, 3>();
-        set_attrs<64, 4>();
+        if (!bf16) {
+            m_sxh = tc::make_map(sxh, px, px, bn);
+            m_sxl = tc::make_map(sxl, px, px, bn);
+            m_syh = tc::make_map(syh, py, py, bn);
+            m_syl = tc::make_map(syl, py, py, bn);
+            set_attrs<128, 3>();
+            set_attrs<64, 4>();
+        } else {
+            const int qx = (nx + 7) & ~7, qy = (ny + 7) & ~7;
+            m_sxh = tc::make_map16(bxh, qx, qx, bn);
+            m_sxl = tc::make_map16(bxl, qx, qx, bn);
+            m_syh = tc::make_map16(byh, qy, qy, bn);
+            m_syl = tc::make_map16(byl, qy, qy, bn);
+            set_attrs16<128, 2>();
+            set_attrs16<64, 2>();
+        }
     }
     void release() {
         for (float* p : {stage, w1, w2, w3, sxh, sxl, syh, syl, eigT}) if (p) cudaFree(p);
+        for (uint16_t* p : {bxh, bxl, byh, byl}) if (p) cudaFree(p);
         stage = w1 = w2 = w3 = sxh = sxl = syh = syl = eigT = nullptr;
+        bxh = bxl = byh = byl = nullptr;
+    }
+    template <int BN, int ST>
+    static void set_attrs16() {
+        static bool done = false;
+        if (done) return;
+        HPQ_CUDA(cudaFuncSetAttribute(tc::k_tc_gemm_bf16<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      tc::Smem16<BN, ST>::TOTAL));
+        done = true;
     }
 
     template <int BN, int ST>
@@ -482,6 +772,20 @@ public:
 
     void gemm(cudaStream_t st, const CUtensorMap& a, const CUtensorMap& bh, const CUtensorMap& bl, int M, int N, int K,
               const tc::Epi& e) {
+        if (bf16) {
+            const int nkb = (K + tc::BK16 - 1) / tc::BK16;
+            if (bn == 128) {
+                dim3 grid((M + tc::BM - 1) / tc::BM, (N + 127) / 128);
+                hpq_launch(tc::k_tc_gemm_bf16<128, 2>, grid, dim3(tc::kThreads), (size_t)tc::Smem16<128, 2>::TOTAL, st,
+                           a, bh, bl, M, nkb, e, err);
+            } else {
+                dim3 grid((M + tc::BM - 1) / tc::BM, (N + 63) / 64);
+                hpq_launch(tc::k_tc_gemm_bf16<64, 2>, grid, dim3(tc::kThreads), (size_t)tc::Smem16<64, 2>::TOTAL, st,
+                           a, bh, bl, M, nkb, e, err);
+            }
+            HPQ_LAUNCH_CHECK();
+            return;
+        }
         const int nkb = (K + tc::BK - 1) / tc::BK;
         if (bn == 128) {
             dim3 grid((M + tc::BM - 1) / tc::BM, (N + 127) / 128);

@@ -331,19 +331,24 @@ def head_slices(text, env, nslices, comps=("Psi", "Ez", "Bz", "Bx")):
     return {k: np.array(v) for k, v in out.items()}
 
 
+@pytest.mark.parametrize("form", ["tc", "tc_bf16"])
 @pytest.mark.parametrize("grid", ["63 63", "64 48", "255 255"])
-def test_tensor_core_dst_matches_fft_and_oracle(grid):
-    """TF32x3 sine GEMMs on tcgen05 vs the FP32 FFT (or SIMT GEMM) form and the FP64 oracle.
+def test_tensor_core_dst_matches_fft_and_oracle(grid, form):
+    """TF32x3 (tc) and BF16x3 (tc_bf16) sine GEMMs on tcgen05 vs the FP32 FFT (or SIMT GEMM) form
+    and the FP64 oracle.
 
     The first slices after the head of the box carry the driver's own field with an undisturbed
-    plasma, so differences are those of the Poisson solves, not of the slice march.
+    plasma, so differences are those of the Poisson solves, not of the slice march. BF16x3 drops
+    the lo x lo product of two 8-bit-mantissa splits (~2^-18 per product against ~2^-22 for
+    TF32x3), so its bound is ten times wider.
     """
     from cases import EXPLICIT_FFT
     text = EXPLICIT_FFT.replace("amr.n_cell = 63 63 48", "amr.n_cell = %s 48" % grid)
     text = text.replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-10")
     text = text.replace("beam.position_mean = 0. 0. 0.", "beam.position_mean = 0. 0. 2.5")
     n = 6
-    tc = head_slices(text, {"HPQ_DST": "tc"}, n)
+    tc = head_slices(text, {"HPQ_DST": form}, n)
+    tol = 1e-5 if form == "tc" else 1e-4
     ref = head_slices(text, {"HPQ_DST": "fft" if grid != "64 48" else "gemm"}, n)
     o = Oracle(text)
     g = hp.Hipace(text, graphs=False)
@@ -360,10 +365,10 @@ def test_tensor_core_dst_matches_fft_and_oracle(grid):
         if k in ("Bz", "Bx"):
             # sources built from the plasma current, a cancellation at the FP32 noise level in
             # these slices (both FP32 forms land between 1e-7 and 3e-5 here)
-            assert e_tc <= 1e-4, (k, e_tc, e_ref)
+            assert e_tc <= 10 * tol, (k, e_tc, e_ref)
         else:
-            assert e_tc <= 1e-5, (k, e_tc)
-            assert rel_l2(tc[k], ref[k]) <= 1e-5, k
+            assert e_tc <= tol, (k, e_tc)
+            assert rel_l2(tc[k], ref[k]) <= tol, k
 
 
 def mixed_errors(text, comps=("Ez", "Psi", "jz_beam", "Bx")):
