@@ -430,6 +430,7 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
 struct MGCoarse {
     int nl;
     int lw;          // first level run by one warp (levels of at most kWarpLevelPoints points)
+    int ns_bottom;   // sweeps of the coarsest level: max(16, its longest side rounded up to even)
     MGLev L[16];
     size_t off[16];  // level offsets (elements) in the shared-memory arena
 };
@@ -629,12 +630,12 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         bstamp();
     }
     if (lw >= M.nl - 1 && lw == M.nl) {
-        coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), 16);
+        coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
         bstamp();
     } else {
         if (threadIdx.x < 32) {
             for (int l = lw; l < M.nl - 1; ++l) coarse_down<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
-            coarse_sweeps<WarpGroup, R, CELL>(arena_level(M.nl - 1), 16);
+            coarse_sweeps<WarpGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
             for (int l = M.nl - 2; l >= lw; --l) coarse_up<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
         }
         __syncthreads();
@@ -1314,6 +1315,10 @@ public:
         if (nl - sb > 16) sb = nl - 16;
         bottom_smem = smem_from(sb);
         coarse.nl = nl - sb;
+        // the bottom solve of HpMultiGrid's CPU build (HpMultiGrid.cpp:1584-1592): 16 sweeps, or
+        // the longest side of the coarsest level rounded up to an even count when that is more
+        // (grids that stop coarsening early, e.g. 100 x 72 -> 25 x 18)
+        coarse.ns_bottom = std::max(16, (std::max(lev[nl - 1].w, lev[nl - 1].h) + 1) / 2 * 2);
         // HPQ_MG_WARP=1 in the environment runs the smallest coarse levels on one warp (measured
         // slower at 255^2: 10.8 us instead of 7.0 for levels 9^2 and 5^2, so off by default)
         const char* ew = getenv("HPQ_MG_WARP");
