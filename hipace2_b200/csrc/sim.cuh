@@ -536,6 +536,11 @@ public:
                                                               : make_fixed_weight_pdf((int)b);
             upload_beam((int)b, hb);
         }
+        // the set-up above zeroes and fills buffers with synchronous cudaMemset / cudaMemcpy calls
+        // on the legacy default stream, which the library's non-blocking streams do not wait
+        // for (a memset returns before it runs, a pageable upload before its DMA lands): finish
+        // them before the first launch on those streams
+        HPQ_CUDA(cudaDeviceSynchronize());
     }
 
     void init_plasma_lattices() {
@@ -849,7 +854,7 @@ public:
             if (B.use_external) {
                 Expr* e = nullptr;
                 HPQ_CUDA(cudaMalloc(&e, 6 * sizeof(Expr)));
-                HPQ_CUDA(cudaMemcpy(e, B.external, 6 * sizeof(Expr), cudaMemcpyHostToDevice));
+                HPQ_CUDA(cudaMemcpyAsync(e, B.external, 6 * sizeof(Expr), cudaMemcpyHostToDevice, st));
                 d.ext = e;
             }
             d.cap = std::max<long long>(nin, 1);
@@ -1236,7 +1241,7 @@ public:
         if (on) {
             const size_t n = (size_t)ncomp_alloc * S.cstride;
             HPQ_CUDA(cudaMalloc(&det_mem, 3 * n * sizeof(long long)));
-            HPQ_CUDA(cudaMemset(det_mem, 0, 3 * n * sizeof(long long)));
+            HPQ_CUDA(cudaMemsetAsync(det_mem, 0, 3 * n * sizeof(long long), st));
             for (int k = 0; k < 3; ++k) det.w[k] = det_mem + k * n;
             det.base = S.base;
         } else {
@@ -2127,7 +2132,8 @@ public:
         if (!names.empty()) {
             const size_t n = (size_t)names.size() * diag_plane() * nz;
             HPQ_CUDA(cudaMalloc(&diag_buf, n * sizeof(double)));
-            HPQ_CUDA(cudaMemset(diag_buf, 0, n * sizeof(double)));
+            // on the library's stream, ahead of the slices that fill it
+            HPQ_CUDA(cudaMemsetAsync(diag_buf, 0, n * sizeof(double), st));
         }
     }
     void get_diag(const std::string& name, double* out) override {
