@@ -458,6 +458,174 @@ __global__ void __launch_bounds__(256) k_adj_push(AdjPlasma P, AdjLam lout, AdjL
     }
 }
 
+// The same map in reverse mode, one thread per particle: the forward push in double keeping the
+// state entering each of the 6 sub-steps, then the adjoint of each sub-step in reverse order
+// (a_substep_rev: the sub-step's expressions differentiated by hand, last operation first), of the
+// boundary condition (a reflection flips x and u) and of the position update. All nine input
+// adjoints (u_h, and the six gathered values) come out of one pass, where the forward-mode form
+// re-runs the push nine times. Same results as k_adj_push up to the order of the sums.
+struct SubstepC {
+    double qmc, ci, c2, sdz, hh;
+};
+__device__ __forceinline__ void a_substep_fwd(const SubstepC& k, const double* G, double& ux, double& uy,
+                                              double& psi) {
+    const double pi = 1.0 / psi;
+    const double a2 = 1.0 + (ux * ux + uy * uy) * k.c2;
+    const double gp = 0.5 * pi * pi * a2 + 0.5;
+    const double ue = ux * G[0] + uy * G[1];
+    const double d0 = k.qmc * (gp * G[0] + G[4] + (uy * G[5]) * pi);
+    const double d1 = k.qmc * (gp * G[1] - G[3] - (ux * G[5]) * pi);
+    const double d2 = k.qmc * k.ci * (ue * k.ci * pi - G[2]);
+    const double dpi = -(pi * pi) * d2;
+    const double dgp = pi * dpi * a2 + pi * pi * k.c2 * (ux * d0 + uy * d1);
+    const double e0 = k.qmc * (dgp * G[0] + G[5] * (d1 * pi + uy * dpi));
+    const double e1 = k.qmc * (dgp * G[1] - G[5] * (d0 * pi + ux * dpi));
+    const double e2 = k.qmc * k.c2 * ((d0 * G[0] + d1 * G[1]) * pi + ue * dpi);
+    ux = ux + k.sdz * d0 + k.hh * e0;
+    uy = uy + k.sdz * d1 + k.hh * e1;
+    psi = psi + k.sdz * d2 + k.hh * e2;
+}
+// (ux, uy, psi): the state entering the sub-step; (lux, luy, lpsi): the adjoint of the state
+// after it on entry, of the state before it on exit; lG accumulates the field adjoints
+__device__ __forceinline__ void a_substep_rev(const SubstepC& k, const double* G, double ux, double uy, double psi,
+                                              double& lux, double& luy, double& lpsi, double* lG) {
+    const double pi = 1.0 / psi;
+    const double a2 = 1.0 + (ux * ux + uy * uy) * k.c2;
+    const double gp = 0.5 * pi * pi * a2 + 0.5;
+    const double ue = ux * G[0] + uy * G[1];
+    const double d0 = k.qmc * (gp * G[0] + G[4] + (uy * G[5]) * pi);
+    const double d1 = k.qmc * (gp * G[1] - G[3] - (ux * G[5]) * pi);
+    const double d2 = k.qmc * k.ci * (ue * k.ci * pi - G[2]);
+    const double dpi = -(pi * pi) * d2;
+    const double dgp = pi * dpi * a2 + pi * pi * k.c2 * (ux * d0 + uy * d1);
+    // u' = u + sdz d + hh e
+    double ld0 = k.sdz * lux, ld1 = k.sdz * luy, ld2 = k.sdz * lpsi;
+    const double le0 = k.hh * lux, le1 = k.hh * luy, le2 = k.hh * lpsi;
+    double lpi = 0, lue = 0, ldpi = 0, ldgp = 0, lgp = 0, la2 = 0;
+    // e2 = qmc c2 ((d0 G0 + d1 G1) pi + ue dpi)
+    const double k2 = k.qmc * k.c2 * le2;
+    ld0 += k2 * G[0] * pi; lG[0] += k2 * d0 * pi;
+    ld1 += k2 * G[1] * pi; lG[1] += k2 * d1 * pi;
+    lpi += k2 * (d0 * G[0] + d1 * G[1]); lue += k2 * dpi; ldpi += k2 * ue;
+    // e1 = qmc (dgp G1 - G5 (d0 pi + ux dpi))
+    const double k1 = k.qmc * le1;
+    ldgp += k1 * G[1]; lG[1] += k1 * dgp; lG[5] -= k1 * (d0 * pi + ux * dpi);
+    ld0 -= k1 * G[5] * pi; lpi -= k1 * G[5] * d0; lux -= k1 * G[5] * dpi; ldpi -= k1 * G[5] * ux;
+    // e0 = qmc (dgp G0 + G5 (d1 pi + uy dpi))
+    const double k0 = k.qmc * le0;
+    ldgp += k0 * G[0]; lG[0] += k0 * dgp; lG[5] += k0 * (d1 * pi + uy * dpi);
+    ld1 += k0 * G[5] * pi; lpi += k0 * G[5] * d1; luy += k0 * G[5] * dpi; ldpi += k0 * G[5] * uy;
+    // dgp = pi dpi a2 + pi^2 c2 (ux d0 + uy d1)
+    const double pp = pi * pi * k.c2;
+    lpi += ldgp * (dpi * a2 + 2.0 * pi * k.c2 * (ux * d0 + uy * d1));
+    ldpi += ldgp * pi * a2; la2 += ldgp * pi * dpi;
+    lux += ldgp * pp * d0; ld0 += ldgp * pp * ux;
+    luy += ldgp * pp * d1; ld1 += ldgp * pp * uy;
+    // dpi = -pi^2 d2
+    lpi -= ldpi * 2.0 * pi * d2; ld2 -= ldpi * pi * pi;
+    // d2 = qmc ci (ue ci pi - G2)
+    const double kd2 = k.qmc * k.ci * ld2;
+    lue += kd2 * k.ci * pi; lpi += kd2 * ue * k.ci; lG[2] -= kd2;
+    // d1 = qmc (gp G1 - G3 - ux G5 pi)
+    const double kd1 = k.qmc * ld1;
+    lgp += kd1 * G[1]; lG[1] += kd1 * gp; lG[3] -= kd1;
+    lux -= kd1 * G[5] * pi; lG[5] -= kd1 * ux * pi; lpi -= kd1 * ux * G[5];
+    // d0 = qmc (gp G0 + G4 + uy G5 pi)
+    const double kd0 = k.qmc * ld0;
+    lgp += kd0 * G[0]; lG[0] += kd0 * gp; lG[4] += kd0;
+    luy += kd0 * G[5] * pi; lG[5] += kd0 * uy * pi; lpi += kd0 * uy * G[5];
+    // ue = ux G0 + uy G1; gp = pi^2 a2 / 2 + 1/2; a2 = 1 + (ux^2 + uy^2) c2; pi = 1/psi
+    lux += lue * G[0]; lG[0] += lue * ux; luy += lue * G[1]; lG[1] += lue * uy;
+    lpi += lgp * pi * a2; la2 += lgp * 0.5 * pi * pi;
+    lux += la2 * 2.0 * ux * k.c2; luy += la2 * 2.0 * uy * k.c2;
+    lpsi -= lpi * pi * pi;
+}
+
+__global__ void __launch_bounds__(256) k_adj_push_rev(AdjPlasma P, AdjLam lout, AdjLam lin, AdjRecF F, AdjL L, Geo g) {
+    HPQ_PDL_ENTRY();
+    SubstepC k;
+    k.qmc = P.charge / (P.mass * g.c);
+    k.ci = 1. / g.c;
+    k.c2 = k.ci * k.ci;
+    const double dzs = g.dx[2];
+    k.sdz = dzs / 4;
+    k.hh = 0.5 * k.sdz * k.sdz;
+    const double dxi = g.dxi[0], dyi = g.dxi[1];
+    for (long long ip = gtid(); ip < P.n; ip += gstride()) {
+        const double lo[8] = {lout.x[ip], lout.y[ip], lout.uxh[ip], lout.uyh[ip], lout.psih[ip],
+                              lout.ux[ip], lout.uy[ip], lout.psi[ip]};
+        bool any = false;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) any = any || lo[o] != 0.0;
+        if (!P.valid[ip] || !any) continue;
+        const double x0 = P.x[ip], y0 = P.y[ip];
+        double G[6];
+        a_gather<double>(F, g, x0, y0, G);
+        // forward, keeping the state entering each sub-step
+        double su[6], sv[6], sp[6];
+        double ux = P.uxh[ip], uy = P.uyh[ip], psi = P.psih[ip];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { su[q] = ux; sv[q] = uy; sp[q] = psi; a_substep_fwd(k, G, ux, uy, psi); }
+        const double ux4 = ux, uy4 = uy, psi4 = psi;
+        double x = x0 + dzs * k.ci * (ux * (1.0 / psi));
+        double y = y0 + dzs * k.ci * (uy * (1.0 / psi));
+        int refl = 0;
+        if (!a_enforce_bc<double>(g, x, y, ux, uy, &refl)) continue;
+#pragma unroll
+        for (int q = 4; q < 6; ++q) { su[q] = ux; sv[q] = uy; sp[q] = psi; a_substep_fwd(k, G, ux, uy, psi); }
+        // reverse
+        double lux = lo[5], luy = lo[6], lpsi = lo[7];
+        double lG[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 5; q >= 4; --q) a_substep_rev(k, G, su[q], sv[q], sp[q], lux, luy, lpsi, lG);
+        lux += lo[2]; luy += lo[3]; lpsi += lo[4];
+        double lx = lo[0], ly = lo[1];
+        if (refl & 1) { lx = -lx; lux = -lux; }
+        if (refl & 2) { ly = -ly; luy = -luy; }
+        // x' = x + dz ux / (c psi), y' likewise, at the state after 4 sub-steps
+        const double pinv = 1.0 / psi4, f = dzs * k.ci;
+        lux += lx * f * pinv;
+        luy += ly * f * pinv;
+        lpsi -= (lx * ux4 + ly * uy4) * f * pinv * pinv;
+#pragma unroll
+        for (int q = 3; q >= 0; --q) a_substep_rev(k, G, su[q], sv[q], sp[q], lux, luy, lpsi, lG);
+        lin.uxh[ip] += lux;
+        lin.uyh[ip] += luy;
+        lin.psih[ip] += lpsi;
+        // field adjoints by the gather shapes, and the positions' share through the gathered values
+        lG[3] *= g.c;
+        lG[4] *= g.c;
+        const Tn xm = a_clamp((tseed(x0, true) - g.xoff) * dxi, g.nx);
+        const Tn ym = a_clamp((tseed(y0, true) - g.yoff) * dyi, g.ny);
+        double gx = 0, gy = 0;
+#pragma unroll 1
+        for (int iy = 0; iy < 4; iy++) {
+            const ADSh<Tn> sy = a_dshape2<Tn>(1, ym, iy);
+#pragma unroll
+            for (int ix = 0; ix < 4; ix++) {
+                const ADSh<Tn> sx = a_dshape2<Tn>(1, xm, ix);
+                const int i = sx.cell, j = sy.cell;
+                const double w = sx.s.v * sy.s.v, wx = sx.s.d * sy.s.v, wy = sx.s.v * sy.s.d;
+                // Psi through ExmBy (x derivative shape) and EypBx (y derivative shape)
+                const double wp = lG[0] * sx.ds.v * sy.s.v * dxi + lG[1] * sx.s.v * sy.ds.v * dyi;
+                const double wpx = lG[0] * sx.ds.d * sy.s.v * dxi + lG[1] * sx.s.d * sy.ds.v * dyi;
+                const double wpy = lG[0] * sx.ds.v * sy.s.d * dxi + lG[1] * sx.s.v * sy.ds.d * dyi;
+                const double fpsi = F.f[RF_PSI](i, j), fez = F.f[RF_EZ](i, j), fbx = F.f[RF_BX](i, j),
+                             fby = F.f[RF_BY](i, j), fbz = F.f[RF_BZ](i, j);
+                gx += wpx * fpsi + wx * (lG[2] * fez + lG[3] * fbx + lG[4] * fby + lG[5] * fbz);
+                gy += wpy * fpsi + wy * (lG[2] * fez + lG[3] * fbx + lG[4] * fby + lG[5] * fbz);
+                if (wp != 0.0) atomicAdd(L.f[A_PSI].ptr(i, j), wp);
+                if (lG[2] != 0.0) atomicAdd(L.f[A_EZ].ptr(i, j), lG[2] * w);
+                if (lG[3] != 0.0) atomicAdd(L.f[A_BX].ptr(i, j), lG[3] * w);
+                if (lG[4] != 0.0) atomicAdd(L.f[A_BY].ptr(i, j), lG[4] * w);
+                if (lG[5] != 0.0) atomicAdd(L.f[A_BZ].ptr(i, j), lG[5] * w);
+            }
+        }
+        lin.x[ip] += lx + gx;
+        lin.y[ip] += ly + gy;
+    }
+}
+
 // objective: lambda_Ez += 2 jz (Ez - Ebar)/S0, lambda_jz += ((Ez - Ebar)^2 - J)/S0 (interior)
 __global__ void k_adj_objective(AdjL L, AdjRecF F, int nx, int ny, double J, double Ebar, double S0) {
     HPQ_PDL_ENTRY();

@@ -1493,6 +1493,13 @@ public:
     }
 
     // ------------------------------------------------------------------ adjoint (adjoint.cuh)
+    static bool adj_push_tangent() {
+        static const bool on = [] {
+            const char* e = getenv("HPQ_ADJ_PUSH");
+            return e && std::string(e) == "tangent";
+        }();
+        return on;
+    }
     bool adj_fwd = false;           // the slice graph is the adjoint forward (hooks, no beam push)
     double adj_plasma_scale = 1.0;  // plasma density multiplier applied when a step begins
     long long beam_gen = 0;         // changes whenever the beam stores change
@@ -1742,9 +1749,12 @@ public:
         const int nbp = blocks_for(a.n * kPushSeeds, 256), nbd = blocks_for(a.n, 256);
         HPQ_CUDA(cudaMemsetAsync(a.L.base, 0, cs * A_NCOMP * sizeof(double), st));
         for (int k = 0; k < 8; ++k) HPQ_CUDA(cudaMemsetAsync(a.lam[1 - cur][k], 0, n * sizeof(double), st));
-        // plasma push
+        // plasma push: reverse mode, one thread per particle (HPQ_ADJ_PUSH=tangent in the
+        // environment selects the forward-mode form, one thread per particle and seed, for
+        // cross-checks)
         Scope sc_push(this, "adj_push");
-        hpq_launch(k_adj_push, dim3(nbp), dim3(256), 0, st, P, lout, lin, F, L, gg);
+        if (adj_push_tangent()) hpq_launch(k_adj_push, dim3(nbp), dim3(256), 0, st, P, lout, lin, F, L, gg);
+        else hpq_launch(k_adj_push_rev, dim3(nbd), dim3(256), 0, st, P, lout, lin, F, L, gg);
         HPQ_LAUNCH_CHECK();
         // objective
         const double zc = cfg.prob_lo[2] + (s + 0.5) * g.dx[2];

@@ -72,6 +72,35 @@ def test_gpu_adjoint_matches_oracle_and_finite_differences(interval):
 
 
 @pytest.mark.gpu
+def test_reverse_mode_push_adjoint_equals_forward_mode(tmp_path):
+    """The push adjoint in reverse mode (one thread per particle, the default) and in forward
+    mode (HPQ_ADJ_PUSH=tangent: one thread per particle and seed) compute the same products of
+    the same derivatives in another order: the gradients agree to rounding."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, 'tests'); import hipace2_b200 as hp;"
+        "from cases import ADJOINT_SMALL, adjoint_beams, adjoint_knots;"
+        "s = hp.Hipace(ADJOINT_SMALL); s.init_data(); d, w = adjoint_beams(); s.set_beam(0, d); s.set_beam(1, w);"
+        "J, g = s.adjoint(adjoint_knots()); np.save(sys.argv[1], np.concatenate([[J], g]))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for mode in ("reverse", "tangent"):
+        env = dict(os.environ)
+        env.pop("HPQ_ADJ_PUSH", None)
+        if mode == "tangent":
+            env["HPQ_ADJ_PUSH"] = "tangent"
+        path = str(tmp_path / ("adj_%s.npy" % mode))
+        subprocess.run([sys.executable, "-c", code, path], cwd=root, env=env, check=True, timeout=600)
+        out[mode] = np.load(path)
+    a, b = out["reverse"], out["tangent"]
+    assert a[0] == pytest.approx(b[0], rel=1e-13)
+    scale = np.abs(b[1:]).max()
+    assert np.abs(a[1:] - b[1:]).max() <= 1e-10 * scale, np.abs(a[1:] - b[1:]).max() / scale
+
+
+@pytest.mark.gpu
 def test_adjoint_through_torch_autograd_and_step_after():
     """A thin torch.autograd.Function over hpq_adjoint_grad (harness only): backward returns the
     adjoint gradient; a normal step runs after the adjoint calls."""
