@@ -627,14 +627,14 @@ def adjoint_point(name, torch, reps=3):
     n_density = int(_key(text, "adjoint.n_density_knots"))
     theta = adjoint_knots(n_profile=n_profile, n_density=n_density)
 
-    def timed(f, n):
+    def timed(f, n, s=sim):
         f()
-        sim.synchronize()
+        s.synchronize()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(n):
             r = f()
-        sim.synchronize()
+        s.synchronize()
         return (time.perf_counter() - t0) / n, r
 
     t_fwd, J = timed(lambda: sim.adjoint(theta, grad=False), reps)
@@ -658,11 +658,31 @@ def adjoint_point(name, torch, reps=3):
 
     t_step, _ = timed(plain, 2)
     sim.close()
+    # the same gradient with the single-precision forward (FP64 reverse sweep), same beams
+    mix = hp.Hipace(text, precision=hp.MIXED, graphs=True)
+    mix.init_data()
+    tm_fwd, Jm = timed(lambda: mix.adjoint(theta, grad=False), reps, mix)
+    tm_grad, (Jm2, gm) = timed(lambda: mix.adjoint(theta), reps, mix)
+    mstep = [0]
+
+    def mplain():
+        mix.step(mstep[0])
+        mstep[0] += 1
+
+    tm_step, _ = timed(mplain, 2, mix)
+    mix.close()
+    mixed = {"seconds_per_gradient": tm_grad, "seconds_forward": tm_fwd, "seconds_plain_step": tm_step,
+             "gradient_over_forward": tm_grad / tm_fwd, "gradient_over_plain_step": tm_grad / tm_step,
+             "objective_rel_diff_from_f64": abs(Jm - J) / abs(J),
+             "grad_max_abs_diff_over_max_grad": float(np.abs(gm - g).max()) / scale,
+             "grad_rel_l2_from_f64": float(np.linalg.norm(gm - g) / np.linalg.norm(g)),
+             "dtype": "f32 forward (beam f64), f64 reverse"}
     return {"workload": name, "grid": [int(v) for v in _n_cell(text)], "params": int(theta.size),
             "checkpoint_interval": int(_key(text, "adjoint.checkpoint_interval")),
             "seconds_per_gradient": t_grad, "seconds_forward": t_fwd, "seconds_plain_step": t_step,
             "gradient_over_plain_step": t_grad / t_step, "gradient_over_forward": t_grad / t_fwd,
             "objective": J, "max_abs_grad": scale, "fd_check": fd, "dtype": "f64",
+            "mixed_precision_forward": mixed,
             "timing": "wall time between device synchronisations"}
 
 

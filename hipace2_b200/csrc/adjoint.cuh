@@ -275,6 +275,51 @@ __global__ void k_adj_record(const Ctl* __restrict__ ctl, AdjCopy<R> a) {
     for (long long i = gtid(); i < a.nv; i += gstride()) a.vdst[slot * a.nv + i] = a.vsrc[i];
 }
 
+// record of a single-precision forward, widened to double for the reverse sweep: positions as
+// the particle's lattice point plus its stored displacement, psi as 1 + the stored psi - 1, the
+// field planes converted
+struct AdjRecMixed {
+    const float* pl[8];  // x, y, ux_h, uy_h, psi_h, ux, uy, psi (displacements, psi - 1)
+    const float* ru;
+    const float* rv;
+    double xoff, yoff, dx, dy;
+    double* dst[8];
+    const float* f[RF_N];
+    double* fdst[RF_N];
+    long long n, cs;
+    const uint8_t* vsrc;
+    uint8_t* vdst;
+    int nz, K;
+};
+__global__ void k_adj_record_mixed(const Ctl* __restrict__ ctl, AdjRecMixed a) {
+    HPQ_PDL_ENTRY();
+    const int s = ctl->islice;
+    const int c = (a.nz - 1 - s) / a.K;
+    const int hi = a.nz - 1 - c * a.K;
+    const int lo = hi - a.K + 1 > 0 ? hi - a.K + 1 : 0;
+    const long long slot = s - lo;
+    for (long long i = gtid(); i < a.n; i += gstride()) {
+        const size_t o = slot * a.n + i;
+        a.dst[0][o] = a.xoff + (double)a.ru[i] * a.dx + (double)a.pl[0][i];
+        a.dst[1][o] = a.yoff + (double)a.rv[i] * a.dy + (double)a.pl[1][i];
+        a.dst[2][o] = (double)a.pl[2][i];
+        a.dst[3][o] = (double)a.pl[3][i];
+        a.dst[4][o] = 1.0 + (double)a.pl[4][i];
+        a.dst[5][o] = (double)a.pl[5][i];
+        a.dst[6][o] = (double)a.pl[6][i];
+        a.dst[7][o] = 1.0 + (double)a.pl[7][i];
+        a.vdst[o] = a.vsrc[i];
+    }
+    for (int k = 0; k < RF_N; ++k)
+        for (long long i = gtid(); i < a.cs; i += gstride()) a.fdst[k][slot * a.cs + i] = (double)a.f[k][i];
+}
+// dst = src in double
+template <class R>
+__global__ void k_adj_widen(const R* __restrict__ src, double* __restrict__ dst, long long n) {
+    HPQ_PDL_ENTRY();
+    for (long long i = gtid(); i < n; i += gstride()) dst[i] = (double)src[i];
+}
+
 // objective sums S0 = sum jz_beam, S1 = sum jz_beam Ez, S2 = sum jz_beam Ez^2 over the interior of
 // an objective slice (zero elsewhere); one block, fixed order
 template <class R>
@@ -366,12 +411,13 @@ __global__ void __launch_bounds__(1024) k_adj_dot(const double* __restrict__ a, 
 }
 
 // interior dot product of two planes (the ion background term); one block
-__global__ void __launch_bounds__(1024) k_adj_plane_dot(F2<double> a, F2<double> b, int nx, int ny, double* out) {
+template <class R>
+__global__ void __launch_bounds__(1024) k_adj_plane_dot(F2<double> a, F2<R> b, int nx, int ny, double* out) {
     HPQ_PDL_ENTRY();
     double s[1] = {0};
     for (long long k = threadIdx.x; k < (long long)nx * ny; k += blockDim.x) {
         const int i = (int)(k % nx), j = (int)(k / nx);
-        s[0] += a(i, j) * b(i, j);
+        s[0] += a(i, j) * (double)b(i, j);
     }
     block_sum_store<1>(s, out);
 }

@@ -1442,7 +1442,9 @@ public:
     }
     // the multigrid reads Sy, Sx, chi and writes Bx, By of slab MS
     template <bool CELL>
-    void mg_solve_t(const Slab<R>& MS) {
+    void mg_solve_t(const Slab<R>& MS) { mg_run<CELL>(mg, MS); }
+    template <bool CELL, class MGT, class RS>
+    void mg_run(MGT& mg, const Slab<RS>& MS) {
         if (mg.coop_ok) {
             // the whole solve, iterations and decisions included, is one cooperative kernel
             mg.template solve_persistent<CELL>(st, MS, ctl, cfg.mg_tol_rel, cfg.mg_tol_abs, cfg.mg_max_iters);
@@ -1525,8 +1527,12 @@ public:
         double* grad = nullptr;           // profile-knot gradient
         double* sig = nullptr;            // sum lambda_w w
         AdjCopy<R> ck_args{}, rec_args{};
+        AdjRecMixed rec_mixed{};          // single precision: the record widened to double
         std::vector<void*> owned;
     } adjb;
+    // single precision: the reverse sweep runs in double with its own multigrid and DST
+    Multigrid<double>* mg64 = nullptr;
+    PoissonDST<double>* dst64 = nullptr;
 
     int adjoint_nparams() const override { return cfg.adjoint.witness < 0 ? 0 : cfg.adjoint.n_params(); }
 
@@ -1541,6 +1547,8 @@ public:
     void adj_release() {
         for (void* p : adjb.owned) cudaFree(p);
         adjb = AdjBuf{};
+        if (mg64) { mg64->release(); delete mg64; mg64 = nullptr; }
+        if (dst64) { dst64->release(); delete dst64; dst64 = nullptr; }
     }
     // buffers of the adjoint (once per simulation; the witness arrays follow the store capacity)
     void adj_setup() {
@@ -1592,6 +1600,24 @@ public:
             r.na = 8 + RF_N;
             r.vsrc = P.valid; r.vdst = a.rec_valid; r.nv = a.n;
             r.nz = nz; r.K = a.K;
+            if constexpr (std::is_same<R, float>::value) {
+                AdjRecMixed& m = a.rec_mixed;
+                m = AdjRecMixed{};
+                for (int k = 0; k < 8; ++k) { m.pl[k] = rsrc[k]; m.dst[k] = a.rec_pl[k]; }
+                m.ru = P.ru; m.rv = P.rv;
+                m.xoff = g.xoff; m.yoff = g.yoff; m.dx = g.dx[0]; m.dy = g.dx[1];
+                for (int k = 0; k < RF_N; ++k) { m.f[k] = S.c(kRecComp[k]).p; m.fdst[k] = a.rec_f[k]; }
+                m.n = a.n; m.cs = (long long)cs;
+                m.vsrc = P.valid; m.vdst = a.rec_valid;
+                m.nz = nz; m.K = a.K;
+                // the transposed multigrid and the Poisson solves of the reverse sweep, in double
+                mg64 = new Multigrid<double>();
+                mg64->init(nx, ny, g.dx[0], g.dx[1]);
+                dst64 = new PoissonDST<double>();
+                dst64->init(nx, ny, g.dx[0], g.dx[1], 3);
+            }
+            // the set-up above ran synchronous copies on the legacy stream
+            HPQ_CUDA(cudaDeviceSynchronize());
         }
         if (a.cap != bm[wb].cap) {
             // the witness store grew: new per-particle arrays (freed with the others at release)
@@ -1603,11 +1629,11 @@ public:
     }
 
     // objective J (and its gradient when grad != nullptr) for the parameters theta
+    // In single precision the forward (and the recomputation of each segment) runs in FP32 and
+    // records its state widened to double; the reverse sweep, the objective sums and the knot
+    // reductions are FP64.
     double adjoint(const double* theta, double* grad) override {
-        if constexpr (!std::is_same<R, double>::value) {
-            (void)theta; (void)grad;
-            throw InputError("the adjoint is available in double precision (hpq_set_precision HPQ_PLAIN_FP64)");
-        } else {
+        {
             const AdjointConfig& A = cfg.adjoint;
             if (A.witness < 0) throw InputError("no adjoint configured (adjoint.witness)");
             if (pl.size() != 1 || pl[0].n == 0) throw InputError("the adjoint needs exactly one plasma species");
@@ -1646,7 +1672,13 @@ public:
             adj_plasma_scale = 1.0;
             hpq_launch(k_adj_set_slice, dim3(1), dim3(1), 0, st, ctl, nz - 1, 1);
             HPQ_LAUNCH_CHECK();
-            HPQ_CUDA(cudaMemcpyAsync(a.w_step, pl[0].w, a.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if constexpr (std::is_same<R, double>::value) {
+                HPQ_CUDA(cudaMemcpyAsync(a.w_step, pl[0].w, a.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            } else {
+                hpq_launch(k_adj_widen<R>, dim3(blocks_for(a.n, 256, 148 * 4)), dim3(256), 0, st, (const R*)pl[0].w,
+                           a.w_step, a.n);
+                HPQ_LAUNCH_CHECK();
+            }
             for (int s = nz - 1; s >= 0; --s) solve_slice(s);
             std::vector<double> obj((size_t)nz * 3);
             HPQ_CUDA(cudaMemcpyAsync(obj.data(), a.obj, obj.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1705,11 +1737,11 @@ public:
             if (c != a.C - 1) {
                 // recompute the segment from its checkpoint (records only)
                 for (int k = 0; k < 11; ++k)
-                    HPQ_CUDA(cudaMemcpyAsync((void*)a.ck_args.src[k], a.ck_pl[k] + (size_t)c * n, n * sizeof(double),
+                    HPQ_CUDA(cudaMemcpyAsync((void*)a.ck_args.src[k], (const R*)a.ck_pl[k] + (size_t)c * n, n * sizeof(R),
                                              cudaMemcpyDeviceToDevice, st));
                 HPQ_CUDA(cudaMemcpyAsync(pl[0].valid, a.ck_valid + (size_t)c * n, n, cudaMemcpyDeviceToDevice, st));
-                HPQ_CUDA(cudaMemcpyAsync(S.base, a.ck_slab + (size_t)c * S.cstride * C_NCOMP,
-                                         S.cstride * C_NCOMP * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                HPQ_CUDA(cudaMemcpyAsync(S.base, (const R*)a.ck_slab + (size_t)c * S.cstride * C_NCOMP,
+                                         S.cstride * C_NCOMP * sizeof(R), cudaMemcpyDeviceToDevice, st));
                 hpq_launch(k_adj_set_slice, dim3(1), dim3(1), 0, st, ctl, hi, 0);
                 HPQ_LAUNCH_CHECK();
                 cur_islice = hi;
@@ -1768,7 +1800,9 @@ public:
         hpq_launch(k_adj_mg_pre, dim3(blocks_for(ncell, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
         HPQ_LAUNCH_CHECK();
         if constexpr (std::is_same<R, double>::value) {
-            if (mg.cell) mg_solve_t<true>(a.M); else mg_solve_t<false>(a.M);
+            if (mg.cell) mg_run<true>(mg, a.M); else mg_run<false>(mg, a.M);
+        } else {
+            if (mg64->cell) mg_run<true>(*mg64, a.M); else mg_run<false>(*mg64, a.M);
         }
         hpq_launch(k_adj_mg_post, dim3(blocks_for((long long)nx * ny, 256)), dim3(256), 0, st, a.M, L, F, (int)mg.cell);
         HPQ_LAUNCH_CHECK();
@@ -1780,12 +1814,15 @@ public:
         HPQ_LAUNCH_CHECK();
         // beam part of Sx/Sy, -grad Psi, Poisson stage; the three solves; right-hand sides
         Scope sc_f(this, "adj_fields");
-        if constexpr (std::is_same<R, double>::value) {
+        {
+            PoissonDST<double>* d64 = nullptr;
+            if constexpr (std::is_same<R, double>::value) d64 = &dst;
+            else d64 = dst64;
             hpq_launch(k_adj_sxsy_stage, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny,
-                       dst.stage, dst.sk, dst.sj);
+                       d64->stage, d64->sk, d64->sj);
             HPQ_LAUNCH_CHECK();
             const int comps[3] = {A_VPSI, A_VEZ, A_VBZ};
-            dst.solve(st, 3, a.L.base, a.L.cstride, a.L.pitch, comps);
+            d64->solve(st, 3, a.L.base, a.L.cstride, a.L.pitch, comps);
         }
         hpq_launch(k_adj_rhs_t, dim3(blocks_for((long long)(nx + 2) * (ny + 2), 256)), dim3(256), 0, st, L, gg, nx, ny);
         HPQ_LAUNCH_CHECK();
@@ -1795,10 +1832,8 @@ public:
         HPQ_LAUNCH_CHECK();
         // ion background (scaled by the density multiplier like the plasma)
         if (cfg.any_neutralize_background()) {
-            if constexpr (std::is_same<R, double>::value) {
-                hpq_launch(k_adj_plane_dot, dim3(1), dim3(1024), 0, st, L.f[A_RM], S.c(C_IONS), nx, ny, a.ions + s);
-                HPQ_LAUNCH_CHECK();
-            }
+            hpq_launch(k_adj_plane_dot<R>, dim3(1), dim3(1024), 0, st, L.f[A_RM], S.c(C_IONS), nx, ny, a.ions + s);
+            HPQ_LAUNCH_CHECK();
         }
         // beam deposits of the witness: jz (and rho - jz) of this slice's particles, their jx/jy
         // (deposited one slice earlier into this slice's jx/jy), and the jx/jy of the previous and
@@ -2026,7 +2061,10 @@ public:
             hpq_launch(k_adj_objective_sums<R>, dim3(1), dim3(1024), 0, st, S, (const Ctl*)ctl, g,
                        cfg.adjoint.objective_lo, cfg.adjoint.objective_hi, adjb.obj);
             HPQ_LAUNCH_CHECK();
-            hpq_launch(k_adj_record<R>, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.rec_args);
+            if constexpr (std::is_same<R, double>::value)
+                hpq_launch(k_adj_record<R>, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.rec_args);
+            else
+                hpq_launch(k_adj_record_mixed, dim3(148 * 4), dim3(256), 0, st, (const Ctl*)ctl, adjb.rec_mixed);
             HPQ_LAUNCH_CHECK();
         }
         if (diag_list.n > 0) {

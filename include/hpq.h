@@ -157,7 +157,9 @@ int hpq_set_graphs(hpq_handle* h, int on);
  * and has no such mode; the values agree with the default mode to FP64 rounding. Allowed between
  * steps. */
 int hpq_set_deterministic(hpq_handle* h, int on);
-/* Adjoint of one step (plain FP64 path; the reference has no adjoint). Configured with the
+/* Adjoint of one step (the reference has no adjoint). In plain FP64 everything runs in double;
+ * with HPQ_MIXED the forward and its segment recomputations run in single precision and record
+ * their state widened to double, and the reverse sweep is FP64. Configured with the
  * adjoint.* input keys: the objective is the current-weighted variance of Ez over the slices
  * whose centre lies in adjoint.objective_zeta,
  *   J = S2/S0 - (S1/S0)^2,  S_n = sum over those slices and cells of jz_beam * Ez^n,

@@ -147,3 +147,34 @@ def test_oracle_adjoint_node_centred_grid():
     for k in (5, 10, 17, 18):
         fd = central_difference(lambda t: o.adjoint(t, grad=False), theta, k)
         assert abs(g[k] - fd) <= FD_TOL * scale, (k, g[k], fd)
+
+
+@pytest.mark.gpu
+def test_single_precision_forward_adjoint_against_fp64():
+    """hpq_adjoint_grad in mixed precision: FP32 forward (and segment recomputation) recorded in
+    double, FP64 reverse sweep. Against the FP64 oracle's gradient and central differences of
+    the FP64 forward; the difference is the FP32 rounding of the recorded trajectory (measured
+    on a B200: objective 2.0e-5, gradient 3.6e-5 of its largest entry)."""
+    import hipace2_b200 as hp
+    sim = hp.Hipace(ADJOINT_SMALL, precision=hp.MIXED)
+    sim.init_data()
+    d, w = adjoint_beams()
+    sim.set_beam(0, d)
+    sim.set_beam(1, w)
+    theta = adjoint_knots()
+    J, g = sim.adjoint(theta)
+    o = oracle_with_beams()
+    Jo, go = o.adjoint(theta)
+    scale = np.abs(go).max()
+    err = np.abs(g - go).max() / scale
+    print("mixed adjoint: J rel", abs(J - Jo) / abs(Jo), "grad max diff / max", err)
+    assert J == pytest.approx(Jo, rel=1e-4)
+    assert err <= 1e-4, err
+    for k in FD_KNOTS:
+        fd = central_difference(lambda t: o.adjoint(t, grad=False), theta, k)
+        assert abs(g[k] - fd) <= 2e-4 * scale, (k, g[k], fd)
+    # the forward alone repeats the objective (up to the order of the FP32 atomic sums), and a
+    # plain step still runs after the adjoint
+    assert sim.adjoint(theta, grad=False) == pytest.approx(J, rel=1e-5)
+    sim.step(0)
+    sim.close()
