@@ -431,10 +431,14 @@ struct MGCoarse {
     int nl;
     int lw;          // first level run by one warp (levels of at most kWarpLevelPoints points)
     int ns_bottom;   // sweeps of the coarsest level: max(16, its longest side rounded up to even)
+    // arena of the coarse levels in global memory when they do not fit in shared memory (grids
+    // that stop coarsening at a large level, e.g. 300^2 -> 75^2), else null
+    void* garena;
     MGLev L[16];
     size_t off[16];  // level offsets (elements) in the shared-memory arena
 };
 constexpr int kWarpLevelPoints = 128;
+constexpr size_t kBottomSmemMax = 200 * 1024;  // shared memory of the single-block bottom solve
 
 // 2-D loops over the valid points of a level (threads as 16 columns x blockDim/16 rows, no
 // integer division), all points or those of one colour ((i + j + s) even)
@@ -571,7 +575,7 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     };
     bstamp();
     __syncthreads();  // the block may have used the shared memory just before
-    R* arena = reinterpret_cast<R*>(smem_raw);
+    R* arena = M.garena ? static_cast<R*>(M.garena) : reinterpret_cast<R*>(smem_raw);
     // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
     auto cor = [&](int l) { return arena + M.off[l]; };
     auto res = [&](int l) { return arena + M.off[l] + 2 * (size_t)M.L[l].w * M.L[l].h; };
@@ -1314,6 +1318,14 @@ public:
         for (int l = 1; l < nl; ++l) if (smem_from(l) <= 160 * 1024 && (long long)lev[l].w * lev[l].h <= 4096) { sb = l; break; }
         if (nl - sb > 16) sb = nl - 16;
         bottom_smem = smem_from(sb);
+        coarse.garena = nullptr;
+        if (bottom_smem > kBottomSmemMax) {
+            // the coarsest level alone is too large for shared memory: the bottom block works on
+            // the same arena in global memory (L2-resident), with the same arithmetic
+            HPQ_CUDA(cudaMalloc(&coarse.garena, bottom_smem));
+            HPQ_CUDA(cudaMemset(coarse.garena, 0, bottom_smem));
+            bottom_smem = 0;
+        }
         coarse.nl = nl - sb;
         // the bottom solve of HpMultiGrid's CPU build (HpMultiGrid.cpp:1584-1592): 16 sweeps, or
         // the longest side of the coarsest level rounded up to an even count when that is more
@@ -1524,6 +1536,8 @@ public:
         }
         if (counter) cudaFree(counter);
         counter = nullptr;
+        if (coarse.garena) cudaFree(coarse.garena);
+        coarse.garena = nullptr;
         if (trace) cudaFree(trace);
         trace = nullptr;
         for (int k = 0; k < 2; ++k) {

@@ -511,10 +511,16 @@ public:
         // 582 vs 608) and the tensor-core sine GEMMs (TF32x3) on other grids up to 1023^2;
         // HPQ_DST=tc / tc_bf16 (BF16x3 tensor-core GEMMs) / fft / gemm (SIMT sine GEMMs on every
         // grid, cross-checks) forces a form;
-        // double precision uses the FFT (radix 2, or Bluestein for other lengths)
+        // double precision uses the radix-2 FFT on 2^k - 1 grids, the SIMT sine GEMMs on other
+        // grids up to 1024 (measured whole steps on a B200 against the Bluestein FFT: equal or
+        // faster from 48 to 1000, e.g. 13.8 vs 20.0 ms at 128^2 x 40 slices, 20.9 vs 29.0 at 256^2,
+        // 102.6 vs 110.2 at 600^2 x 16, the linear-wake predictor-corrector case at 64^2 3053 vs
+        // 1912 slices/s; up to 7 % slower on explicit decks below 128) and the Bluestein FFT beyond
         const char* env = getenv("HPQ_DST");
         std::string dmode = env ? env : "";
         if (dmode.empty() && std::is_same<R, float>::value && FastDST<R>::radix2(nx, ny)) dmode = "fft";
+        if (dmode.empty() && std::is_same<R, double>::value && !FastDST<R>::radix2(nx, ny) && std::max(nx, ny) <= 1024)
+            dmode = "gemm";
         if (dmode == "gemm") { dst.set_mode(false); pc_dst.set_mode(false); if (sal_dst.nx) sal_dst.set_mode(false); }
         else if (dmode != "fft" && std::is_same<R, float>::value) {
             const bool bf16 = dmode == "tc_bf16";

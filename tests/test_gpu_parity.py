@@ -451,7 +451,7 @@ def test_remaining_goldens_on_gpu(name):
         assert np.abs(a).sum() == pytest.approx(case["fields"][k], rel=rtol, abs=1e-300), k
 
 
-def test_bluestein_dst_on_odd_grids_matches_oracle():
+def test_bluestein_dst_on_odd_grids_matches_oracle(monkeypatch):
     """Grids whose 2(n + 1) is not a power of two (100 x 72 and 45 x 33) take the Bluestein FFT
     DST in FP64; the whole slice march must match the oracle (weak driver: the DST's rounding,
     a few 1e-14 relative, is not amplified by a strongly nonlinear plasma response).
@@ -459,7 +459,9 @@ def test_bluestein_dst_on_odd_grids_matches_oracle():
     These grids also stop coarsening early (100 x 72 -> 25 x 18), so the multigrid's bottom level
     takes more than 16 sweeps (HpMultiGrid's CPU rule, which the oracle restates); with 16 the
     V-cycles differ and Bz, the curl of a nearly curl-free current in this weak wake, ends 4e-10
-    from the oracle."""
+    from the oracle. The library's default on these grids is the sine-GEMM form (faster below
+    1024 cells); HPQ_DST=fft selects the Bluestein FFT."""
+    monkeypatch.setenv("HPQ_DST", "fft")
     for shape in ("100 72 24", "45 33 24"):
         text = (EXPLICIT_MOVING.replace("amr.n_cell = 33 33 40", "amr.n_cell = " + shape)
                 .replace("beam.density = 5.", "beam.density = 0.5"))
@@ -467,6 +469,19 @@ def test_bluestein_dst_on_odd_grids_matches_oracle():
         for k in EXPLICIT_COMPS:
             e = rel_l2(g.get_diag(k), o.get_diag(k))
             assert e <= 1e-10, (shape, k, e)
+
+
+def test_large_coarsest_multigrid_level_matches_oracle():
+    """150 x 100 cells coarsen only once (to 75 x 50): the coarsest multigrid level's arrays do
+    not fit in shared memory, so the bottom solve works on an arena in global memory (76 sweeps
+    of the 75 x 50 level, HpMultiGrid's CPU rule). Fields and beam vs the oracle."""
+    text = (EXPLICIT_MOVING.replace("amr.n_cell = 33 33 40", "amr.n_cell = 150 100 8")
+            .replace("beam.density = 5.", "beam.density = 0.5")
+            .replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-6"))
+    g, o = run_pair(text, EXPLICIT_COMPS, 2)
+    for k in EXPLICIT_COMPS:
+        e = rel_l2(g.get_diag(k), o.get_diag(k))
+        assert e <= 1e-10, (k, e)
 
 
 def test_warp_merged_plasma_deposit_matches_oracle(monkeypatch):
