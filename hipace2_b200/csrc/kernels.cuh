@@ -85,6 +85,7 @@ struct Ctl {
     // predictor-corrector
     double pc_err, pc_err_prev, pc_sum[2], pc_w[2], pc_mix;
     int pc_iter, pc_go, pc_mixnow, pc_pad;
+    unsigned int pc_cnt[2];  // arrivals of the blocks of the norm and mix kernels (last block decides)
     // persistent multigrid solve (one cooperative launch): |rhs| max, residual norms by
     // iteration parity and the grid barrier {arrivals, generation}, cleared before every solve;
     // the barrier's timeout flag, cleared when a step begins

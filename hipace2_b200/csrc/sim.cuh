@@ -114,8 +114,37 @@ inline int comp_from_name(const std::string& n, bool explicit_solver) {
 // ------------------------------------------------------------------------------------------
 // PC helper kernels (Fields.cpp:1149-1286)
 // ------------------------------------------------------------------------------------------
+// first error of a slice -> initial-guess mixing factor (InitialBfieldGuess)
+__device__ __forceinline__ void pc_guess_factor(Ctl* ctl, double tol) {
+    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
+    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
+    ctl->pc_mix = exp(-0.5 * pow(err / (2.5 * tol), 2));
+    ctl->pc_iter = 0;
+    ctl->pc_err = 1.0;
+    ctl->pc_err_prev = 1.0;
+    ctl->pc_go = 1.0 > tol;
+}
+// error of one iteration -> mixing weights and whether to continue (MixAndShiftBfields)
+__device__ __forceinline__ void pc_iter_factor(Ctl* ctl) {
+    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
+    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
+    ctl->pc_iter += 1;
+    double prev = ctl->pc_err_prev;
+    if (ctl->pc_iter == 1) prev = err;
+    double wi, wp;
+    if (err != 0. || prev != 0.) { wi = prev / (err + prev); wp = err / (err + prev); }
+    else { wi = 0.5; wp = 0.5; }
+    ctl->pc_w[0] = wi; ctl->pc_w[1] = wp;
+    ctl->pc_err = err;
+    ctl->pc_err_prev = err;
+    ctl->pc_mixnow = 1;
+}
+
+// Norms of (B) and (B - B_iter) summed over the interior into Ctl::pc_sum; the last block to
+// finish turns them into the guess factor (gated == 0, the first norms of a slice) or the
+// iteration weights (gated == 1, skipped with the whole kernel once the loop has stopped)
 template <class R>
-__global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl, int gated) {
+__global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl, int gated, double tol) {
     HPQ_PDL_ENTRY();
     if (gated && !ctl->pc_go) return;
     const F2<R> Bx = S.c(bx), By = S.c(by), Bxi = S.c(bxi), Byi = S.c(byi);
@@ -127,31 +156,33 @@ __global__ void k_pc_norms(Slab<R> S, int bx, int by, int bxi, int byi, Ctl* ctl
         nd += sqrt((a - c) * (a - c) + (b - d) * (b - d));
     }
     for (int o = 16; o > 0; o >>= 1) { nb += __shfl_xor_sync(0xffffffffu, nb, o); nd += __shfl_xor_sync(0xffffffffu, nd, o); }
+    __shared__ double wb[32], wd[32];
+    __shared__ int last;
     if (gridDim.x > 1) {
         if ((threadIdx.x & 31) == 0) { atomicAdd(&ctl->pc_sum[0], nb); atomicAdd(&ctl->pc_sum[1], nd); }
-        return;
-    }
-    // one block (deterministic mode): warp sums added in warp order by one thread
-    __shared__ double wb[32], wd[32];
-    if ((threadIdx.x & 31) == 0) { wb[threadIdx.x >> 5] = nb; wd[threadIdx.x >> 5] = nd; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last = atomicAdd(&ctl->pc_cnt[0], 1u) == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (!last || threadIdx.x != 0) return;
+        __threadfence();
+        ctl->pc_sum[0] = atomic_read(&ctl->pc_sum[0]);
+        ctl->pc_sum[1] = atomic_read(&ctl->pc_sum[1]);
+        ctl->pc_cnt[0] = 0;
+    } else {
+        // one block (deterministic mode): warp sums added in warp order by one thread
+        if ((threadIdx.x & 31) == 0) { wb[threadIdx.x >> 5] = nb; wd[threadIdx.x >> 5] = nd; }
+        __syncthreads();
+        if (threadIdx.x != 0) return;
         double sb = 0, sd = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { sb += wb[w]; sd += wd[w]; }
         ctl->pc_sum[0] += sb;
         ctl->pc_sum[1] += sd;
     }
-}
-// first error of a slice -> initial-guess mixing factor (InitialBfieldGuess)
-__global__ void k_pc_guess_factor(Ctl* ctl, double tol) {
-    HPQ_PDL_ENTRY();
-    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
-    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
-    ctl->pc_mix = exp(-0.5 * pow(err / (2.5 * tol), 2));
-    ctl->pc_iter = 0;
-    ctl->pc_err = 1.0;
-    ctl->pc_err_prev = 1.0;
-    ctl->pc_go = 1.0 > tol;
+    if (gated) pc_iter_factor(ctl);
+    else pc_guess_factor(ctl, tol);
 }
 template <class R>
 __global__ void k_pc_guess(Slab<R> S, const Ctl* ctl) {
@@ -167,23 +198,8 @@ __global__ void k_pc_guess(Slab<R> S, const Ctl* ctl) {
         PCP[k] = bx; PCPy[k] = by;
     }
 }
-// error of one iteration -> mixing weights and whether to continue (MixAndShiftBfields)
-__global__ void k_pc_iter_factor(Ctl* ctl, double tol, int maxit) {
-    HPQ_PDL_ENTRY();
-    if (!ctl->pc_go) return;
-    const double err = ctl->pc_sum[0] > 0 ? ctl->pc_sum[1] / ctl->pc_sum[0] : 0.0;
-    ctl->pc_sum[0] = ctl->pc_sum[1] = 0;
-    ctl->pc_iter += 1;
-    double prev = ctl->pc_err_prev;
-    if (ctl->pc_iter == 1) prev = err;
-    double wi, wp;
-    if (err != 0. || prev != 0.) { wi = prev / (err + prev); wp = err / (err + prev); }
-    else { wi = 0.5; wp = 0.5; }
-    ctl->pc_w[0] = wi; ctl->pc_w[1] = wp;
-    ctl->pc_err = err;
-    ctl->pc_err_prev = err;
-    ctl->pc_mixnow = 1;
-}
+// B = (1 - a) B + a (wi B_iter + wp B_previter); the last block to finish ends the iteration
+// (clears the mix flag, decides whether the loop goes on)
 template <class R>
 __global__ void k_pc_mix(Slab<R> S, Ctl* ctl, double a, double tol, int maxit) {
     HPQ_PDL_ENTRY();
@@ -200,10 +216,15 @@ __global__ void k_pc_mix(Slab<R> S, Ctl* ctl, double a, double tol, int maxit) {
         PCP[k] = PCI[k]; PCPy[k] = PCIy[k];
         NJX[k] = 0; NJY[k] = 0;
     }
-}
-__global__ void k_pc_after_mix(Ctl* ctl, double tol, int maxit) {
-    HPQ_PDL_ENTRY();
-    if (!ctl->pc_mixnow) return;
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&ctl->pc_cnt[1], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    ctl->pc_cnt[1] = 0;
     ctl->pc_mixnow = 0;
     ctl->pc_go = (ctl->pc_err > tol) && (ctl->pc_iter < maxit);
 }
@@ -2120,9 +2141,7 @@ public:
         const double tol = cfg.predcorr_B_error_tolerance;
         const int maxit = cfg.predcorr_max_iterations;
         HPQ_CUDA(cudaMemsetAsync(&ctl->pc_sum[0], 0, 2 * sizeof(double), st));
-        hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0);
-        HPQ_LAUNCH_CHECK();
-        hpq_launch(k_pc_guess_factor, dim3(1), dim3(1), 0, st, ctl, tol);
+        hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_PBX, C_PBY, C_PCPBX, C_PCPBY, ctl, 0, tol);
         HPQ_LAUNCH_CHECK();
         hpq_launch(k_pc_guess<R>, dim3(blocks_for((long long)S.cstride, 256)), dim3(256), 0, st, S, ctl);
         HPQ_LAUNCH_CHECK();
@@ -2143,13 +2162,9 @@ public:
             hpq_launch(k_rhs_bxby<R>, dim3(blocks_for(nxy, 256)), dim3(256), 0, st, S, g, pc_dst.stage, pc_dst.sk, pc_dst.sj);
             HPQ_LAUNCH_CHECK();
             pc_dst.solve(st, 2, S.base, S.cstride, S.pitch, comps);
-            hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1);
-            HPQ_LAUNCH_CHECK();
-            hpq_launch(k_pc_iter_factor, dim3(1), dim3(1), 0, st, ctl, tol, maxit);
+            hpq_launch(k_pc_norms<R>, dim3(det.w[0] ? 1 : blocks_for(nxy, 256, 148 * 4)), dim3(det.w[0] ? 1024 : 256), 0, st, S, C_BX, C_BY, C_PCIBX, C_PCIBY, ctl, 1, tol);
             HPQ_LAUNCH_CHECK();
             hpq_launch(k_pc_mix<R>, dim3(blocks_for((long long)S.cstride, 256)), dim3(256), 0, st, S, ctl, cfg.predcorr_B_mixing_factor, tol, maxit);
-            HPQ_LAUNCH_CHECK();
-            hpq_launch(k_pc_after_mix, dim3(1), dim3(1), 0, st, ctl, tol, maxit);
             HPQ_LAUNCH_CHECK();
         }
     }
