@@ -714,6 +714,9 @@ struct MGSolveArgs {
     // region 4 + 4 times instead of a 36^2 region 8 times (40 % fewer point updates, one more
     // grid barrier). Same sweeps in the same order, so the same results.
     int split0;
+    // the coarsest level (sb = nl - 1) is too large for one block's shared memory: its sweeps run
+    // as grid-wide tile phases instead of in the bottom block
+    int tile_bottom;
 };
 
 __device__ __forceinline__ unsigned long long tc_clock_ns() {
@@ -1117,10 +1120,38 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
-        // levels sb .. nl-1 in block 0
-        if (blockIdx.x == 0)
+        if (P.tile_bottom) {
+            // the coarsest level: ns_bottom sweeps from a zero guess as grid-wide phases of 4
+            // sweeps (the last of 2 when ns_bottom is not a multiple of 4) on 16^2 tiles with
+            // their halos, alternating between up and cor so that the last phase writes cor
+            const int l = P.sb;
+            const MGLev& L = P.lev[l];
+            const int ns = P.coarse.ns_bottom, n2 = (ns % 4) ? 1 : 0, nph = ns / 4 + n2;
+            const int ntx = (L.vhi_i - L.vlo + 16) / 16, nt = ntx * ((L.vhi_j - L.vlo + 16) / 16);
+            for (int ph = 0; ph < nph; ++ph) {
+                const bool to_cor = ((nph - 1 - ph) & 1) == 0;
+                SmoothArgs<R> a = base(l);
+                a.rhs = mg_own<R>(P.res, P.lev, l);
+                a.acf = mg_own<R>(P.acf, P.lev, l, 1);
+                a.out = to_cor ? mg_own<R>(P.cor, P.lev, l) : mg_own<R>(P.up, P.lev, l);
+                a.in = to_cor ? mg_own<R>(P.up, P.lev, l) : mg_own<R>(P.cor, P.lev, l);
+                const bool two = n2 && ph == nph - 1;
+                for (int t = tb; tile_block && t < nt; t += ntb) {
+                    if (ph == 0) {
+                        if (two) mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, false, false, MG_NORM_NONE, 2>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                        else mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                    } else {
+                        if (two) mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, false, false, MG_NORM_NONE, 2>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                        else mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
+                    }
+                }
+                if (ph + 1 < nph && !grid_barrier(bar, err)) return;
+            }
+        } else if (blockIdx.x == 0) {
+            // levels sb .. nl-1 in block 0
             mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
                                      it == 0 || nb == 1, P.trace ? P.trace + 256 : nullptr);
+        }
         wstamp(1);
         if (!grid_barrier(bar, err)) return;
         stamp();
@@ -1505,6 +1536,7 @@ public:
         P.r32[0] = r32[0]; P.r32[1] = r32[1];
         P.trace = trace;
         P.split0 = split0 ? 1 : 0;
+        P.tile_bottom = coarse.garena != nullptr && sb == nl - 1 ? 1 : 0;
         // single precision refines level 0 in FP64 only where the tolerance asks for it: an FP32
         // V-cycle reaches relative residuals well below kRefineTol on its own
         P.refine = std::is_same<R, float>::value && (refine_force >= 0 ? refine_force == 1 : tol_rel < kRefineTol);
