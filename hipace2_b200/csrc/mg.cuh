@@ -508,12 +508,17 @@ __device__ __forceinline__ void coarse_sweeps(const CoarseLevel<R>& A, int nswee
             const int id = j * L.w + i;
             const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
             const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
+            // every load of both components before either store: a colour sweep reads only the
+            // other colour, so the two update chains are independent and overlap
             const R inv = A.dinv[id];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                R* p = A.cor + c * plane;
-                p[id] = mg_gs_inv<R, CELL>(L, i, j, p[im], p[ip], p[jm], p[jp], A.res[c * plane + id], inv, A.facx, A.facy);
-            }
+            const R* p0 = A.cor;
+            const R* p1 = A.cor + plane;
+            const R a0 = p0[im], b0 = p0[ip], c0 = p0[jm], d0 = p0[jp], r0 = A.res[id];
+            const R a1 = p1[im], b1 = p1[ip], c1 = p1[jm], d1 = p1[jp], r1 = A.res[plane + id];
+            const R v0 = mg_gs_inv<R, CELL>(L, i, j, a0, b0, c0, d0, r0, inv, A.facx, A.facy);
+            const R v1 = mg_gs_inv<R, CELL>(L, i, j, a1, b1, c1, d1, r1, inv, A.facx, A.facy);
+            A.cor[id] = v0;
+            A.cor[plane + id] = v1;
         });
         G::sync();
     }
@@ -529,19 +534,23 @@ __device__ __forceinline__ void coarse_down(const CoarseLevel<R>& A, const Coars
         const int id = j * L.w + i;
         const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
         const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const R* p = A.cor + c * plane;
-            A.rsc[c * plane + id] = A.res[c * plane + id] + A.acf[id] * p[id] -
-                                    mg_lap<R, CELL>(L, i, j, p[id], p[im], p[ip], p[jm], p[jp], A.facx, A.facy);
-        }
+        const R a = A.acf[id];
+        const R* p0 = A.cor;
+        const R* p1 = A.cor + plane;
+        const R e0 = p0[id], a0 = p0[im], b0 = p0[ip], c0 = p0[jm], d0 = p0[jp], r0 = A.res[id];
+        const R e1 = p1[id], a1 = p1[im], b1 = p1[ip], c1 = p1[jm], d1 = p1[jp], r1 = A.res[plane + id];
+        const R q0 = r0 + a * e0 - mg_lap<R, CELL>(L, i, j, e0, a0, b0, c0, d0, A.facx, A.facy);
+        const R q1 = r1 + a * e1 - mg_lap<R, CELL>(L, i, j, e1, a1, b1, c1, d1, A.facx, A.facy);
+        A.rsc[id] = q0;
+        A.rsc[plane + id] = q1;
     });
     G::sync();
     MV<R> fine{{A.rsc, A.rsc + plane}, L.w, 0};
     const int cplane = C.L.w * C.L.h;
     G::valid(C.L, [&](int i, int j) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c) C.res[c * cplane + j * C.L.w + i] = mg_restrict1<R, CELL>(fine, i, j, c);
+        const R q0 = mg_restrict1<R, CELL>(fine, i, j, 0), q1 = mg_restrict1<R, CELL>(fine, i, j, 1);
+        C.res[j * C.L.w + i] = q0;
+        C.res[cplane + j * C.L.w + i] = q1;
     });
     G::sync();
 }
@@ -553,8 +562,11 @@ __device__ __forceinline__ void coarse_up(const CoarseLevel<R>& A, const CoarseL
     const int plane = L.w * L.h;
     MV<R> crse{{C.cor, C.cor + C.L.w * C.L.h}, C.L.w, 0};
     G::valid(L, [&](int i, int j) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c) A.cor[c * plane + j * L.w + i] += mg_interp1<R, CELL>(crse, i, j, c);
+        const int id = j * L.w + i;
+        const R u0 = A.cor[id] + mg_interp1<R, CELL>(crse, i, j, 0);
+        const R u1 = A.cor[plane + id] + mg_interp1<R, CELL>(crse, i, j, 1);
+        A.cor[id] = u0;
+        A.cor[plane + id] = u1;
     });
     G::sync();
     coarse_sweeps<G, R, CELL>(A, 4);
@@ -565,7 +577,7 @@ __device__ __forceinline__ unsigned long long tc_clock_ns();
 // bt (tracing only): thread 0 records the global timer at the start, after the set-up, after each
 // level of the down sweep, after the coarsest level, after each level of the up sweep and at the
 // end: bt[0] = count, bt[1..]
-template <class R, bool CELL>
+template <class R, bool CELL, bool GA = false>
 __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
                                                 R facy0, unsigned char* smem_raw, bool init,
                                                 unsigned long long* bt = nullptr) {
@@ -575,7 +587,8 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     };
     bstamp();
     __syncthreads();  // the block may have used the shared memory just before
-    R* arena = M.garena ? static_cast<R*>(M.garena) : reinterpret_cast<R*>(smem_raw);
+    // GA: the arena in global memory (M.garena), else in shared memory, known at compile time
+    R* arena = GA ? static_cast<R*>(M.garena) : reinterpret_cast<R*>(smem_raw);
     // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
     auto cor = [&](int l) { return arena + M.off[l]; };
     auto res = [&](int l) { return arena + M.off[l] + 2 * (size_t)M.L[l].w * M.L[l].h; };
@@ -634,7 +647,8 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         bstamp();
     }
     if (lw >= M.nl - 1 && lw == M.nl) {
-        coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
+        if (M.ns_bottom == 16) coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), 16);
+        else coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
         bstamp();
     } else {
         if (threadIdx.x < 32) {
@@ -659,7 +673,8 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(MGCoarse M, const R* __restr
                                                     R* __restrict__ cor_g, R facx0, R facy0) {
     HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
-    mg_bottom_block<R, CELL>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw, true);
+    if (M.garena) mg_bottom_block<R, CELL, true>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw, true);
+    else mg_bottom_block<R, CELL, false>(M, res_g, acf_g, cor_g, facx0, facy0, smem_raw, true);
 }
 
 template <class R>
@@ -714,9 +729,6 @@ struct MGSolveArgs {
     // region 4 + 4 times instead of a 36^2 region 8 times (40 % fewer point updates, one more
     // grid barrier). Same sweeps in the same order, so the same results.
     int split0;
-    // the coarsest level (sb = nl - 1) is too large for one block's shared memory: its sweeps run
-    // as grid-wide tile phases instead of in the bottom block
-    int tile_bottom;
 };
 
 __device__ __forceinline__ unsigned long long tc_clock_ns() {
@@ -1005,7 +1017,10 @@ __device__ __forceinline__ void mg_refine_tile(const MGSolveArgs<float>& P, int 
 // T0: tile edge of level 0 (16, or 32 on large grids: a 4-sweep phase then loads 44^2 points per
 // 32^2 tile instead of 28^2 per 16^2, 1.6x less halo work; the sweeps give the same values). With
 // T0 = 32 level 0 runs without FP64 refinement, and in double precision in the split form.
-template <class R, bool CELL, int T0 = 16>
+// TB: the coarsest level is too large for one block's shared memory (Multigrid::tile_bottom) and
+// its sweeps run as grid-wide tile phases; a separate instance, so that the common one keeps its
+// register allocation.
+template <class R, bool CELL, int T0 = 16, bool TB = false>
 __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
     HPQ_PDL_ENTRY();
     extern __shared__ unsigned char smem_raw[];
@@ -1120,7 +1135,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
-        if (P.tile_bottom) {
+        if constexpr (TB) {
             // the coarsest level: ns_bottom sweeps from a zero guess as grid-wide phases of 4
             // sweeps (the last of 2 when ns_bottom is not a multiple of 4) on 16^2 tiles with
             // their halos, alternating between up and cor so that the last phase writes cor
@@ -1149,7 +1164,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             }
         } else if (blockIdx.x == 0) {
             // levels sb .. nl-1 in block 0
-            mg_bottom_block<R, CELL>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
+            mg_bottom_block<R, CELL, false>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
                                      it == 0 || nb == 1, P.trace ? P.trace + 256 : nullptr);
         }
         wstamp(1);
@@ -1407,6 +1422,7 @@ public:
     bool split0 = false;                  // level-0 phase split in two (MGSolveArgs::split0)
     int refine_force = -1;                // single precision: -1 by tolerance, 0 plain FP32, 1 FP64 refinement
     bool use32 = false;                   // level-0 tiles of 32^2 (k_mg_solve<R, CELL, 32>) for unrefined solves
+    bool tile_bottom = false;             // the coarsest level's sweeps as grid-wide tile phases (TB)
     int coop_blocks32 = 0;
     size_t coop_smem32 = 0;
     bool split32 = true;                  // level 0 of the 32^2 form as two 4-sweep passes
@@ -1466,7 +1482,13 @@ public:
                 HPQ_CUDA(cudaMemset(r32[k], 0, 2 * n0 * sizeof(R)));
             }
         }
-        auto kern = k_mg_solve<R, CELL>;
+        // a global-memory arena only ever holds the coarsest level alone (sb == nl - 1): the
+        // persistent kernel then sweeps it as grid-wide tile phases, and otherwise its bottom block
+        // works in shared memory
+        if (coarse.garena != nullptr && sb != nl - 1)
+            throw CudaError("hpmg: coarse levels exceed shared memory below the coarsest level");
+        tile_bottom = coarse.garena != nullptr;
+        auto kern = tile_bottom ? k_mg_solve<R, CELL, 16, true> : k_mg_solve<R, CELL, 16, false>;
         HPQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem));
         int dev = 0, sms = 0, coop = 0, per = 0;
         HPQ_CUDA(cudaGetDevice(&dev));
@@ -1496,7 +1518,7 @@ public:
             if (std::is_same<R, float>::value) coop_smem32 = std::max(coop_smem32, SmoothSmem<32, 8>::template bytes<R>());
             const char* es32 = getenv("HPQ_MG_SPLIT");
             split32 = std::is_same<R, float>::value ? (es32 ? es32[0] == '1' : true) : true;
-            auto k32 = k_mg_solve<R, CELL, 32>;
+            auto k32 = tile_bottom ? k_mg_solve<R, CELL, 32, true> : k_mg_solve<R, CELL, 32, false>;
             HPQ_CUDA(cudaFuncSetAttribute(k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem32));
             int per32 = 0;
             HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k32, 256, coop_smem32));
@@ -1536,7 +1558,6 @@ public:
         P.r32[0] = r32[0]; P.r32[1] = r32[1];
         P.trace = trace;
         P.split0 = split0 ? 1 : 0;
-        P.tile_bottom = coarse.garena != nullptr && sb == nl - 1 ? 1 : 0;
         // single precision refines level 0 in FP64 only where the tolerance asks for it: an FP32
         // V-cycle reaches relative residuals well below kRefineTol on its own
         P.refine = std::is_same<R, float>::value && (refine_force >= 0 ? refine_force == 1 : tol_rel < kRefineTol);
@@ -1557,7 +1578,8 @@ public:
         at[0].val.cooperative = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        void (*kern)(MGSolveArgs<R>) = t32 ? k_mg_solve<R, CELL, 32> : k_mg_solve<R, CELL, 16>;
+        void (*kern)(MGSolveArgs<R>) = tile_bottom ? (t32 ? k_mg_solve<R, CELL, 32, true> : k_mg_solve<R, CELL, 16, true>)
+                                                   : (t32 ? k_mg_solve<R, CELL, 32, false> : k_mg_solve<R, CELL, 16, false>);
         HPQ_CUDA(cudaLaunchKernelEx(&cfg, kern, P));
         HPQ_LAUNCH_CHECK();
     }
