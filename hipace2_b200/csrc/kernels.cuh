@@ -584,12 +584,10 @@ __global__ void k_pack_explicit(Slab<R> S, Quad<R>* __restrict__ q) {
     for (long long k = gtid(); k < (long long)S.cstride; k += gstride()) q[k] = Quad<R>{bz[k], ez[k], ex[k], ey[k]};
 }
 
-// sxy (single precision, floating-point atomics only, else null): an interleaved (Sx, Sy) plane
-// receiving both sums of a cell with one two-component atomic (k_add_sxy folds it into Sx, Sy)
 template <class R, int DT, bool DET, int ORD = 2>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposit(PlasmaDev<R> P, Slab<R> S, Geo g,
                                                                                     const Quad<R>* __restrict__ quad,
-                                                                                    DetAcc det, R* sxy) {
+                                                                                    DetAcc det) {
     HPQ_PDL_ENTRY();
     const R invvol = g.normalized ? (R)(g.dx[0] * g.dx[1] * g.dxi[0] * g.dxi[1]) : (R)(g.dxi[0] * g.dxi[1] * g.dxi[2]);
     const R a_clight = (R)g.c, clight_inv = (R)(1.0 / g.c);
@@ -637,34 +635,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_explicit_deposi
                                      (-sxd * sys * dxi * (-vx * vy) - sxs * syd * dyi * gmy) * a_clight);
                 const R vsx = cdm * (+sxs * sys * (+Bz_v * vy + (Ez_v * vx + ExmBy_v * (gamma_psi - vx * vx) + EypBx_v * (-vx * vy)) * clight_inv) * q_mass_ratio * psi_inv +
                                      (+sxd * sys * dxi * gmx + sxs * syd * dyi * (-vx * vy)) * a_clight);
-                if constexpr (!DET && std::is_same<R, float>::value) {
-                    if (sxy) {
-                        const ptrdiff_t c = (ptrdiff_t)(j + kGuardAlloc) * S.pitch + (i + kGuardAlloc);
-                        atomicAdd(reinterpret_cast<float2*>(sxy) + c, make_float2(vsx, vsy));
-                        continue;
-                    }
-                }
                 addd<DET>(det, Sy, S.pitch, i, j, vsy);
                 addd<DET>(det, Sx, S.pitch, i, j, vsx);
             }
-        }
-    }
-}
-
-// Sx += sxy.x, Sy += sxy.y over the whole slice, and the interleaved plane cleared for the next
-// deposit
-template <class R>
-__global__ void k_add_sxy(Slab<R> S, R* __restrict__ sxy) {
-    HPQ_PDL_ENTRY();
-    R* Sx = S.c(C_SX).p;
-    R* Sy = S.c(C_SY).p;
-    for (long long k = gtid(); k < (long long)S.cstride; k += gstride()) {
-        const R a = sxy[2 * k], b = sxy[2 * k + 1];
-        if (a != R(0) || b != R(0)) {
-            Sx[k] += a;
-            Sy[k] += b;
-            sxy[2 * k] = R(0);
-            sxy[2 * k + 1] = R(0);
         }
     }
 }

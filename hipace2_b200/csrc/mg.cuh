@@ -435,7 +435,9 @@ struct MGCoarse {
     // that stop coarsening at a large level, e.g. 300^2 -> 75^2), else null
     void* garena;
     MGLev L[16];
-    size_t off[16];  // level offsets (elements) in the shared-memory arena
+    // level l starts (3 NC + 2) poff[l] elements into the arena, poff[l] = the points of the
+    // levels before it (NC: components per bottom block)
+    size_t poff[16];
 };
 constexpr int kWarpLevelPoints = 128;
 constexpr size_t kBottomSmemMax = 200 * 1024;  // shared memory of the single-block bottom solve
@@ -499,7 +501,10 @@ struct CoarseLevel {
     R facx, facy;
 };
 
-template <class G, class R, bool CELL>
+// NC: the components one group carries (2, or 1 when the two components of the coarse levels
+// are solved by two blocks side by side); every load of a point's components comes before
+// any of its stores, so the NC update chains overlap
+template <class G, class R, bool CELL, int NC>
 __device__ __forceinline__ void coarse_sweeps(const CoarseLevel<R>& A, int nsweeps) {
     const MGLev& L = A.L;
     const int plane = L.w * L.h;
@@ -508,68 +513,74 @@ __device__ __forceinline__ void coarse_sweeps(const CoarseLevel<R>& A, int nswee
             const int id = j * L.w + i;
             const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
             const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-            // every load of both components before either store: a colour sweep reads only the
-            // other colour, so the two update chains are independent and overlap
+            // a colour sweep reads only the other colour: the components' chains are independent
             const R inv = A.dinv[id];
-            const R* p0 = A.cor;
-            const R* p1 = A.cor + plane;
-            const R a0 = p0[im], b0 = p0[ip], c0 = p0[jm], d0 = p0[jp], r0 = A.res[id];
-            const R a1 = p1[im], b1 = p1[ip], c1 = p1[jm], d1 = p1[jp], r1 = A.res[plane + id];
-            const R v0 = mg_gs_inv<R, CELL>(L, i, j, a0, b0, c0, d0, r0, inv, A.facx, A.facy);
-            const R v1 = mg_gs_inv<R, CELL>(L, i, j, a1, b1, c1, d1, r1, inv, A.facx, A.facy);
-            A.cor[id] = v0;
-            A.cor[plane + id] = v1;
+            R a[NC], b[NC], c[NC], d[NC], r[NC], v[NC];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                const R* p = A.cor + q * plane;
+                a[q] = p[im]; b[q] = p[ip]; c[q] = p[jm]; d[q] = p[jp]; r[q] = A.res[q * plane + id];
+            }
+#pragma unroll
+            for (int q = 0; q < NC; ++q) v[q] = mg_gs_inv<R, CELL>(L, i, j, a[q], b[q], c[q], d[q], r[q], inv, A.facx, A.facy);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) A.cor[q * plane + id] = v[q];
         });
         G::sync();
     }
 }
 
 // 4 sweeps, the residual, and its restriction into the next level's right-hand side
-template <class G, class R, bool CELL>
+template <class G, class R, bool CELL, int NC>
 __device__ __forceinline__ void coarse_down(const CoarseLevel<R>& A, const CoarseLevel<R>& C) {
-    coarse_sweeps<G, R, CELL>(A, 4);
+    coarse_sweeps<G, R, CELL, NC>(A, 4);
     const MGLev& L = A.L;
     const int plane = L.w * L.h;
     G::valid(L, [&](int i, int j) {
         const int id = j * L.w + i;
         const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
         const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
-        const R a = A.acf[id];
-        const R* p0 = A.cor;
-        const R* p1 = A.cor + plane;
-        const R e0 = p0[id], a0 = p0[im], b0 = p0[ip], c0 = p0[jm], d0 = p0[jp], r0 = A.res[id];
-        const R e1 = p1[id], a1 = p1[im], b1 = p1[ip], c1 = p1[jm], d1 = p1[jp], r1 = A.res[plane + id];
-        const R q0 = r0 + a * e0 - mg_lap<R, CELL>(L, i, j, e0, a0, b0, c0, d0, A.facx, A.facy);
-        const R q1 = r1 + a * e1 - mg_lap<R, CELL>(L, i, j, e1, a1, b1, c1, d1, A.facx, A.facy);
-        A.rsc[id] = q0;
-        A.rsc[plane + id] = q1;
+        const R ac = A.acf[id];
+        R e[NC], a[NC], b[NC], c[NC], d[NC], r[NC], q[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const R* p = A.cor + k * plane;
+            e[k] = p[id]; a[k] = p[im]; b[k] = p[ip]; c[k] = p[jm]; d[k] = p[jp]; r[k] = A.res[k * plane + id];
+        }
+#pragma unroll
+        for (int k = 0; k < NC; ++k) q[k] = r[k] + ac * e[k] - mg_lap<R, CELL>(L, i, j, e[k], a[k], b[k], c[k], d[k], A.facx, A.facy);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) A.rsc[k * plane + id] = q[k];
     });
     G::sync();
-    MV<R> fine{{A.rsc, A.rsc + plane}, L.w, 0};
+    MV<R> fine{{A.rsc, A.rsc + (NC > 1 ? plane : 0)}, L.w, 0};
     const int cplane = C.L.w * C.L.h;
     G::valid(C.L, [&](int i, int j) {
-        const R q0 = mg_restrict1<R, CELL>(fine, i, j, 0), q1 = mg_restrict1<R, CELL>(fine, i, j, 1);
-        C.res[j * C.L.w + i] = q0;
-        C.res[cplane + j * C.L.w + i] = q1;
+        R q[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) q[k] = mg_restrict1<R, CELL>(fine, i, j, k);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) C.res[k * cplane + j * C.L.w + i] = q[k];
     });
     G::sync();
 }
 
 // interpolation of the coarser correction, then 4 sweeps
-template <class G, class R, bool CELL>
+template <class G, class R, bool CELL, int NC>
 __device__ __forceinline__ void coarse_up(const CoarseLevel<R>& A, const CoarseLevel<R>& C) {
     const MGLev& L = A.L;
     const int plane = L.w * L.h;
-    MV<R> crse{{C.cor, C.cor + C.L.w * C.L.h}, C.L.w, 0};
+    MV<R> crse{{C.cor, C.cor + (NC > 1 ? C.L.w * C.L.h : 0)}, C.L.w, 0};
     G::valid(L, [&](int i, int j) {
         const int id = j * L.w + i;
-        const R u0 = A.cor[id] + mg_interp1<R, CELL>(crse, i, j, 0);
-        const R u1 = A.cor[plane + id] + mg_interp1<R, CELL>(crse, i, j, 1);
-        A.cor[id] = u0;
-        A.cor[plane + id] = u1;
+        R u[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) u[k] = A.cor[k * plane + id] + mg_interp1<R, CELL>(crse, i, j, k);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) A.cor[k * plane + id] = u[k];
     });
     G::sync();
-    coarse_sweeps<G, R, CELL>(A, 4);
+    coarse_sweeps<G, R, CELL, NC>(A, 4);
 }
 
 __device__ __forceinline__ unsigned long long tc_clock_ns();
@@ -577,7 +588,9 @@ __device__ __forceinline__ unsigned long long tc_clock_ns();
 // bt (tracing only): thread 0 records the global timer at the start, after the set-up, after each
 // level of the down sweep, after the coarsest level, after each level of the up sweep and at the
 // end: bt[0] = count, bt[1..]
-template <class R, bool CELL, bool GA = false>
+// NC = 2: both components (res_g, cor_g: two planes of the first level); NC = 1: one component
+// (res_g, cor_g point at its plane), the other one solved by another block
+template <class R, bool CELL, bool GA = false, int NC = 2>
 __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
                                                 R facy0, unsigned char* smem_raw, bool init,
                                                 unsigned long long* bt = nullptr) {
@@ -589,17 +602,19 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     __syncthreads();  // the block may have used the shared memory just before
     // GA: the arena in global memory (M.garena), else in shared memory, known at compile time
     R* arena = GA ? static_cast<R*>(M.garena) : reinterpret_cast<R*>(smem_raw);
-    // level l: cor (2n), res (2n), rescor (2n), acf (n), 1/diagonal (n)
-    auto cor = [&](int l) { return arena + M.off[l]; };
-    auto res = [&](int l) { return arena + M.off[l] + 2 * (size_t)M.L[l].w * M.L[l].h; };
-    auto rsc = [&](int l) { return arena + M.off[l] + 4 * (size_t)M.L[l].w * M.L[l].h; };
-    auto acf = [&](int l) { return arena + M.off[l] + 6 * (size_t)M.L[l].w * M.L[l].h; };
-    auto dinv = [&](int l) { return arena + M.off[l] + 7 * (size_t)M.L[l].w * M.L[l].h; };
+    // level l (n points, 3 NC + 2 planes from (3 NC + 2) M.poff[l]): cor (NC n), res (NC n),
+    // rescor (NC n), acf (n), 1/diagonal (n)
+    auto nn = [&](int l) { return (size_t)M.L[l].w * M.L[l].h; };
+    auto cor = [&](int l) { return arena + (3 * NC + 2) * M.poff[l]; };
+    auto res = [&](int l) { return cor(l) + NC * nn(l); };
+    auto rsc = [&](int l) { return cor(l) + 2 * NC * nn(l); };
+    auto acf = [&](int l) { return cor(l) + 3 * NC * nn(l); };
+    auto dinv = [&](int l) { return cor(l) + (3 * NC + 1) * nn(l); };
     const int n0 = M.L[0].w * M.L[0].h;
     if (init) {
         for (int l = 0; l < M.nl; ++l) {
             const int n = M.L[l].w * M.L[l].h;
-            for (int k = threadIdx.x; k < 8 * n; k += blockDim.x) cor(l)[k] = R(0);
+            for (int k = threadIdx.x; k < (3 * NC + 2) * n; k += blockDim.x) cor(l)[k] = R(0);
         }
         __syncthreads();
         for (int k = threadIdx.x; k < n0; k += blockDim.x) acf(0)[k] = acf_g[k];
@@ -623,13 +638,10 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     } else {
         for (int l = 0; l < M.nl; ++l) {
             const int n = M.L[l].w * M.L[l].h;
-            for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) cor(l)[k] = R(0);
+            for (int k = threadIdx.x; k < NC * n; k += blockDim.x) cor(l)[k] = R(0);
         }
     }
-    for (int k = threadIdx.x; k < n0; k += blockDim.x) {
-        res(0)[k] = res_g[k];
-        res(0)[n0 + k] = res_g[n0 + k];
-    }
+    for (int k = threadIdx.x; k < NC * n0; k += blockDim.x) res(0)[k] = res_g[k];
     __syncthreads();
     bstamp();
     // down to the first warp level (block-wide), the smallest levels by warp 0 alone (down,
@@ -643,27 +655,27 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         return CoarseLevel<R>{M.L[l], cor(l), res(l), rsc(l), acf(l), dinv(l), fac(l, facx0), fac(l, facy0)};
     };
     for (int l = 0; l < lw && l < M.nl - 1; ++l) {
-        coarse_down<BlockGroup, R, CELL>(arena_level(l), arena_level(l + 1));
+        coarse_down<BlockGroup, R, CELL, NC>(arena_level(l), arena_level(l + 1));
         bstamp();
     }
     if (lw >= M.nl - 1 && lw == M.nl) {
-        if (M.ns_bottom == 16) coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), 16);
-        else coarse_sweeps<BlockGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
+        if (M.ns_bottom == 16) coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), 16);
+        else coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
         bstamp();
     } else {
         if (threadIdx.x < 32) {
-            for (int l = lw; l < M.nl - 1; ++l) coarse_down<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
-            coarse_sweeps<WarpGroup, R, CELL>(arena_level(M.nl - 1), M.ns_bottom);
-            for (int l = M.nl - 2; l >= lw; --l) coarse_up<WarpGroup, R, CELL>(arena_level(l), arena_level(l + 1));
+            for (int l = lw; l < M.nl - 1; ++l) coarse_down<WarpGroup, R, CELL, NC>(arena_level(l), arena_level(l + 1));
+            coarse_sweeps<WarpGroup, R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
+            for (int l = M.nl - 2; l >= lw; --l) coarse_up<WarpGroup, R, CELL, NC>(arena_level(l), arena_level(l + 1));
         }
         __syncthreads();
         bstamp();
     }
     for (int l = (lw < M.nl ? lw : M.nl - 1) - 1; l >= 0; --l) {
-        coarse_up<BlockGroup, R, CELL>(arena_level(l), arena_level(l + 1));
+        coarse_up<BlockGroup, R, CELL, NC>(arena_level(l), arena_level(l + 1));
         bstamp();
     }
-    for (int k = threadIdx.x; k < 2 * n0; k += blockDim.x) cor_g[k] = cor(0)[k];
+    for (int k = threadIdx.x; k < NC * n0; k += blockDim.x) cor_g[k] = cor(0)[k];
     bstamp();
     if (bt && threadIdx.x == 0) bt[0] = nbt;
 }
@@ -1035,7 +1047,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
     int* err = &ctl->mgp_bar_err;
     const int nb = gridDim.x;
     // trace: [0] count, [1..127] block 0 after each grid barrier; [128] count, [129..255] the
-    // moment the phase's work of block 1 (tiles) or block 0 (coarse levels) is done
+    // moment the phase's work of block 2, the first tile block, is done
     int nstamp = 0, nwork = 0;
     auto stamp = [&]() {
         if (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && nstamp < 126) P.trace[1 + nstamp++] = tc_clock_ns();
@@ -1053,10 +1065,10 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
         a.ctl = ctl;
         return a;
     };
-    // block 0 runs the coarse levels and keeps them resident in its shared memory; the tiles
-    // go to the other blocks
-    const int tb = (nb > 1) ? (int)blockIdx.x - 1 : 0, ntb = (nb > 1) ? nb - 1 : 1;
-    const bool tile_block = (nb == 1) || blockIdx.x > 0;
+    // blocks 0 and 1 run the coarse levels, one component each, and keep them resident in their
+    // shared memory; the tiles go to the other blocks (the launch has at least 3 blocks)
+    const int tb = (int)blockIdx.x - 2, ntb = nb - 2;
+    const bool tile_block = blockIdx.x >= 2;
     // levels >= 1 also take 32^2 tiles in the 32^2 form where there are enough of them
     // (bit l of P.l32_mask)
     auto big = [&](int l) { return T0 == 32 && ((P.l32_mask >> l) & 1u) != 0; };
@@ -1131,7 +1143,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 for (int t = tb; tile_block && t < nt; t += ntb)
                     mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (it == 0) restrict_acf(l + 1);
-            wstamp(1);
+            wstamp(2);
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
@@ -1162,12 +1174,16 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 }
                 if (ph + 1 < nph && !grid_barrier(bar, err)) return;
             }
-        } else if (blockIdx.x == 0) {
-            // levels sb .. nl-1 in block 0
-            mg_bottom_block<R, CELL, false>(P.coarse, P.res[P.sb], P.acf[P.sb], P.cor[P.sb], P.facx[P.sb], P.facy[P.sb], smem_raw,
-                                     it == 0 || nb == 1, P.trace ? P.trace + 256 : nullptr);
+        } else if (blockIdx.x < 2) {
+            // levels sb .. nl-1: component c in block c (the components share the operator and
+            // are coupled only through the norms, which are taken on level 0)
+            const int c = (int)blockIdx.x;
+            const size_t nsb = (size_t)P.lev[P.sb].w * P.lev[P.sb].h;
+            mg_bottom_block<R, CELL, false, 1>(P.coarse, P.res[P.sb] + c * nsb, P.acf[P.sb], P.cor[P.sb] + c * nsb,
+                                               P.facx[P.sb], P.facy[P.sb], smem_raw, it == 0,
+                                               (P.trace && c == 0) ? P.trace + 256 : nullptr);
         }
-        wstamp(1);
+        wstamp(2);
         if (!grid_barrier(bar, err)) return;
         stamp();
         // up: levels sb-1 .. 1, interpolation of the coarser correction + 4 sweeps
@@ -1189,7 +1205,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             if (!done)
                 for (int t = tb; tile_block && t < nt; t += ntb)
                     mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
-            wstamp(1);
+            wstamp(2);
             if (!grid_barrier(bar, err)) return;
             stamp();
         }
@@ -1223,7 +1239,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                     for (int t = tb; tile_block && t < nt; t += ntb)
                         mg_smooth_tile<R, CELL, T0, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                 }
-                wstamp(1);
+                wstamp(2);
             }
             if (!grid_barrier(bar, err)) return;
             stamp();
@@ -1249,7 +1265,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 }
                 block_max2(bmax, brhs);
                 if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
-                wstamp(1);
+                wstamp(2);
             }
         } else
         // level 0: up-sweep and the next down-sweep (8 colour sweeps), residual, restriction,
@@ -1276,7 +1292,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             }
             block_max2(bmax, brhs);
             if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
-            wstamp(1);
+            wstamp(2);
         }
         if (!grid_barrier(bar, err)) return;
         stamp();
@@ -1302,7 +1318,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
         ctl->mg_go = 0;
         if (P.trace) P.trace[0] = nstamp;
     }
-    if (P.trace && blockIdx.x == 1 && threadIdx.x == 0) P.trace[128] = nwork;
+    if (P.trace && blockIdx.x == 2 && threadIdx.x == 0) P.trace[128] = nwork;
     // solution: the last level-0 output (cor[0] after an even number of cycles, else up[0]; the
     // FP64 solution slot it & 1 in single precision)
     const MV<R> fin = ((it & 1) && !split) ? mg_own<R>(P.up, P.lev, 0) : mg_own<R>(P.cor, P.lev, 0);
@@ -1333,7 +1349,8 @@ public:
     unsigned int* counter = nullptr;
     int sb = 1;  // first level of the single-block bottom solve
     int nl = 0;
-    size_t bottom_smem = 0;
+    size_t bottom_smem = 0;   // single-block bottom solve, both components (k_mg_bottom)
+    size_t bottom_smem1 = 0;  // one component (each bottom block of the persistent solve)
     MGCoarse coarse{};
 
     void init(int nx, int ny, double dx_, double dy_) {
@@ -1364,6 +1381,8 @@ public:
         for (int l = 1; l < nl; ++l) if (smem_from(l) <= 160 * 1024 && (long long)lev[l].w * lev[l].h <= 4096) { sb = l; break; }
         if (nl - sb > 16) sb = nl - 16;
         bottom_smem = smem_from(sb);
+        // the persistent solve's two bottom blocks carry one component each: 5 planes per level
+        bottom_smem1 = bottom_smem / 8 * 5;
         coarse.garena = nullptr;
         if (bottom_smem > kBottomSmemMax) {
             // the coarsest level alone is too large for shared memory: the bottom block works on
@@ -1371,6 +1390,7 @@ public:
             HPQ_CUDA(cudaMalloc(&coarse.garena, bottom_smem));
             HPQ_CUDA(cudaMemset(coarse.garena, 0, bottom_smem));
             bottom_smem = 0;
+            bottom_smem1 = 0;
         }
         coarse.nl = nl - sb;
         // the bottom solve of HpMultiGrid's CPU build (HpMultiGrid.cpp:1584-1592): 16 sweeps, or
@@ -1387,8 +1407,8 @@ public:
         size_t off = 0;
         for (int l = sb; l < nl; ++l) {
             coarse.L[l - sb] = lev[l];
-            coarse.off[l - sb] = off;
-            off += 8 * (size_t)lev[l].w * lev[l].h;
+            coarse.poff[l - sb] = off;
+            off += (size_t)lev[l].w * lev[l].h;
         }
         acf.assign(nl, nullptr); res.assign(nl, nullptr); cor.assign(nl, nullptr); up.assign(nl, nullptr);
         for (int l = 0; l < nl; ++l) {
@@ -1440,7 +1460,7 @@ public:
             snprintf(buf, sizeof(buf), " %.2f", (double)(h[1 + k] - h[k]) / 1000.0);
             line += buf;
         }
-        // block 1 finished the work of phase w + 2 (the first smoothing, phase 1, has no stamp)
+        // block 2 (the first tile block) finished the work of phase w + 2 (the first smoothing, phase 1, has no stamp)
         // at h[129 + w]; relative to the start of that phase (the barrier before it)
         const int nw = (int)std::min<unsigned long long>(h[128], 126);
         for (int w = 0; w < nw && w + 2 < n; ++w) {
@@ -1465,7 +1485,7 @@ public:
         const char* e = getenv("HPQ_MG");
         if (e && std::string(e) == "kernels") return;
         if (nl > kMGMaxLevels) return;
-        coop_smem = std::max({SmoothSmem<16, 8>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
+        coop_smem = std::max({SmoothSmem<16, 8>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem1});
         if (const char* t = getenv("HPQ_MG_TRACE")) {
             if (t[0] == '1') {
                 HPQ_CUDA(cudaMalloc(&trace, 320 * sizeof(unsigned long long)));
@@ -1497,12 +1517,12 @@ public:
         HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, coop_smem));
         const MGLev& L = lev[0];
         const int nt0 = ((L.vhi_i - L.vlo + 16) / 16) * ((L.vhi_j - L.vlo + 16) / 16);
-        coop_blocks = std::min(per * sms, nt0 + 1);  // + block 0 for the coarse levels
-        coop_ok = coop && per > 0 && coop_blocks > 0;
+        coop_blocks = std::min(per * sms, nt0 + 2);  // + blocks 0 and 1 for the coarse levels
+        coop_ok = coop && per > 0 && coop_blocks >= 3;
         // split level-0 phase once every tile block sweeps at least 4 tiles (HPQ_MG_SPLIT=0/1
         // in the environment forces either form)
         const char* es = getenv("HPQ_MG_SPLIT");
-        split0 = es ? (es[0] == '1') : (nt0 >= 4 * std::max(coop_blocks - 1, 1));
+        split0 = es ? (es[0] == '1') : (nt0 >= 4 * std::max(coop_blocks - 2, 1));
         // single precision: HPQ_MG_REFINE=0/1 forces plain FP32 V-cycles or FP64 refinement
         const char* er = getenv("HPQ_MG_REFINE");
         refine_force = er ? (er[0] == '1' ? 1 : 0) : -1;
@@ -1511,9 +1531,9 @@ public:
         const int nt32 = ((L.vhi_i - L.vlo + 32) / 32) * ((L.vhi_j - L.vlo + 32) / 32);
         const char* e32 = getenv("HPQ_MG_T0");
         // (the 32^2 form is taken where it keeps the blocks per SM of the 16^2 form)
-        use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : nt32 >= 2 * std::max(coop_blocks - 1, 1));
+        use32 = coop_ok && (e32 ? std::atoi(e32) == 32 : nt32 >= 2 * std::max(coop_blocks - 2, 1));
         if (use32) {
-            coop_smem32 = std::max({SmoothSmem<32, 4>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem});
+            coop_smem32 = std::max({SmoothSmem<32, 4>::template bytes<R>(), SmoothSmem<16, 4>::template bytes<R>(), bottom_smem1});
             // single precision may run level 0 as one 8-sweep pass of 32^2 tiles
             if (std::is_same<R, float>::value) coop_smem32 = std::max(coop_smem32, SmoothSmem<32, 8>::template bytes<R>());
             const char* es32 = getenv("HPQ_MG_SPLIT");
@@ -1522,8 +1542,8 @@ public:
             HPQ_CUDA(cudaFuncSetAttribute(k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coop_smem32));
             int per32 = 0;
             HPQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k32, 256, coop_smem32));
-            coop_blocks32 = std::min(per32 * sms, nt32 + 1);
-            use32 = per32 > 0 && (e32 || per32 >= per);
+            coop_blocks32 = std::min(per32 * sms, nt32 + 2);
+            use32 = per32 > 0 && coop_blocks32 >= 3 && (e32 || per32 >= per);
             // levels >= 1 in 32^2 tiles once they occupy at least half of the tile blocks
             // (HPQ_MG_L1=16/32 forces either form on level 1)
             l32_mask = 0;
@@ -1531,7 +1551,7 @@ public:
             for (int l = 1; l < std::min(sb, 32); ++l) {
                 const MGLev& Ll = lev[l];
                 const int ntl = ((Ll.vhi_i - Ll.vlo + 32) / 32) * ((Ll.vhi_j - Ll.vlo + 32) / 32);
-                const bool on = (l == 1 && el1) ? std::atoi(el1) == 32 : 2 * ntl >= coop_blocks32 - 1;
+                const bool on = (l == 1 && el1) ? std::atoi(el1) == 32 : 2 * ntl >= coop_blocks32 - 2;
                 if (on) l32_mask |= 1u << l;
             }
         }

@@ -413,9 +413,7 @@ public:
         if (SB.base) cudaFree(SB.base);
         SB.base = nullptr;
         if (quad) cudaFree(quad);
-        if (sxy) cudaFree(sxy);
         quad = nullptr;
-        sxy = nullptr;
         if (bin_key) cudaFree(bin_key);
         if (bin_hist) cudaFree(bin_hist);
         if (bin_total) cudaFree(bin_total);
@@ -515,10 +513,6 @@ public:
         SB = S;
         HPQ_CUDA(cudaMalloc(&SB.base, S.cstride * (C_PSI + 1) * sizeof(R)));
         if (cfg.explicit_solver) HPQ_CUDA(cudaMalloc(&quad, S.cstride * sizeof(Quad<R>)));
-        if (cfg.explicit_solver && std::is_same<R, float>::value) {
-            HPQ_CUDA(cudaMalloc(&sxy, 2 * S.cstride * sizeof(R)));
-            HPQ_CUDA(cudaMemset(sxy, 0, 2 * S.cstride * sizeof(R)));
-        }
         HPQ_CUDA(cudaMemset(SB.base, 0, S.cstride * (C_PSI + 1) * sizeof(R)));
         dst.init(nx, ny, g.dx[0], g.dx[1], 3);
         if (!cfg.explicit_solver) pc_dst.init(nx, ny, g.dx[0], g.dx[1], 2);
@@ -1330,12 +1324,8 @@ public:
     // ExplicitDeposition (ExplicitDeposition.cpp:20-265): Sx, Sy += the plasma contribution;
     // the four fields it gathers are first packed cell by cell (Quad)
     Quad<R>* quad = nullptr;
-    // single precision: interleaved (Sx, Sy) accumulator of the explicit deposit (one float2
-    // atomic per cell instead of two scalar ones), folded into Sx, Sy after the deposits
-    R* sxy = nullptr;
     void explicit_deposit() {
         bool packed = false;
-        R* sx2 = det.w[0] ? nullptr : sxy;
         for (size_t s = 0; s < pl.size(); ++s) {
             if (pl[s].n == 0) continue;
             Scope sc(this, "explicit_deposit");
@@ -1347,15 +1337,11 @@ public:
             const int nb = blocks_for(pl[s].n, 256);
             const bool d = det.w[0] != nullptr;
             const Quad<R>* q = quad;
-            if (cfg.depos_derivative_type == 0) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 0, true, ORD> : k_explicit_deposit<R, 0, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det, sx2); });
-            else if (cfg.depos_derivative_type == 1) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 1, true, ORD> : k_explicit_deposit<R, 1, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det, sx2); });
-            else with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 2, true, ORD> : k_explicit_deposit<R, 2, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det, sx2); });
+            if (cfg.depos_derivative_type == 0) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 0, true, ORD> : k_explicit_deposit<R, 0, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
+            else if (cfg.depos_derivative_type == 1) with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 1, true, ORD> : k_explicit_deposit<R, 1, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
+            else with_order([&](auto o_) { constexpr int ORD = decltype(o_)::value; hpq_launch(d ? k_explicit_deposit<R, 2, true, ORD> : k_explicit_deposit<R, 2, false, ORD>, dim3(nb), dim3(256), 0, st, pl[s], S, g, q, det); });
             HPQ_LAUNCH_CHECK();
             det_flush({C_SX, C_SY});
-        }
-        if (packed && sx2) {
-            hpq_launch(k_add_sxy<R>, dim3(blocks_for((long long)S.cstride, 256, 148 * 8)), dim3(256), 0, st, S, sx2);
-            HPQ_LAUNCH_CHECK();
         }
     }
 

@@ -21,8 +21,8 @@ def rel_l2(a, b):
     return d / n if n > 0 else d
 
 
-def run_pair(text, comps, steps, share_beam=True):
-    g = hp.Hipace(text, graphs=False)
+def run_pair(text, comps, steps, share_beam=True, deterministic=False):
+    g = hp.Hipace(text, graphs=False, deterministic=deterministic)
     g.init_data()
     o = Oracle(text)
     if share_beam:
@@ -474,11 +474,13 @@ def test_bluestein_dst_on_odd_grids_matches_oracle(monkeypatch):
 def test_large_coarsest_multigrid_level_matches_oracle():
     """150 x 100 cells coarsen only once (to 75 x 50): the coarsest multigrid level's arrays do
     not fit in shared memory, so the bottom solve works on an arena in global memory (76 sweeps
-    of the 75 x 50 level, HpMultiGrid's CPU rule). Fields and beam vs the oracle."""
+    of the 75 x 50 level, HpMultiGrid's CPU rule). Fields and beam vs the oracle, with
+    deterministic deposition: Bz, whose norm is small on this near-symmetric case, carries the
+    run-to-run spread of the floating-point atomics at 3e-11 to 8e-11 (2.3e-11 deterministic)."""
     text = (EXPLICIT_MOVING.replace("amr.n_cell = 33 33 40", "amr.n_cell = 150 100 8")
             .replace("beam.density = 5.", "beam.density = 0.5")
             .replace("hipace.MG_tolerance_rel = 1e-12", "hipace.MG_tolerance_rel = 1e-6"))
-    g, o = run_pair(text, EXPLICIT_COMPS, 2)
+    g, o = run_pair(text, EXPLICIT_COMPS, 2, deterministic=True)
     for k in EXPLICIT_COMPS:
         e = rel_l2(g.get_diag(k), o.get_diag(k))
         assert e <= 1e-10, (k, e)
