@@ -41,10 +41,11 @@ PUSH_BYTES = {8: 5 * 8 + 1 + 10 * 8, 4: 5 * 4 + 1 + 10 * 4}
 # the first smoothing
 MG_REALS_PER_POINT_VCYCLE = 4.0 / 3.0 * 9.0
 MG_REALS_PER_POINT_FIRST = 9.0
-# DRAM bytes (read 2 925 824 + write 0) of one k_mg_solve launch of the current kernel from ncu
-# (blowout_255, FP64, one launch after 300, `--set full`): the level-0
-# arrays stay in L2, so DRAM traffic is far below the algorithmic bytes
-MG_NCU_DRAM_BYTES_FP64_255 = 2925824
+# DRAM bytes (read 2 936 064 + write 0) of one k_mg_solve launch of the current kernel (two
+# coarse-level blocks) from ncu (blowout_255, FP64, one launch after 300, `--set full`,
+# profiles/k_mg_solve_blowout_255_fp64.md): the level-0 arrays stay in L2, so DRAM traffic is far
+# below the algorithmic bytes
+MG_NCU_DRAM_BYTES_FP64_255 = 2936064
 
 
 def parse():

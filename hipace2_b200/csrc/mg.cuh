@@ -5,9 +5,10 @@
 //     :162-183, 265-294), node-centred otherwise (Dirichlet on the first guard node) (:1043-1100)
 //   * smoother: 4 red-black Gauss-Seidel colour sweeps, optionally followed by the residual,
 //     computed tile-by-tile in shared memory with a 5-cell halo (:412-592)
-//   * V-cycle: smooth+residual, restrict down to the levels that fit one block; a single block
-//     does those levels including 16 bottom sweeps (:854-1040); interpolate and smooth back up
-//     (:1429-1512)
+//   * V-cycle: smooth+residual, restrict down to the levels that fit one block's shared memory;
+//     those levels, including max(16, longest side) bottom sweeps, run in one block per
+//     component in the persistent solve (one block for both in the multi-kernel form)
+//     (:854-1040, 1584-1592); interpolate and smooth back up (:1429-1512)
 //   * convergence: max-norm residual <= max(tol_abs, tol_rel * max(|rhs|, |res0|)) (:1340-1398)
 // The iteration count is decided on the device (Ctl::mg_go), so the whole solve can sit inside
 // a CUDA graph with a conditional while node.
@@ -422,10 +423,11 @@ __global__ void __launch_bounds__(256) k_mg_smooth(SmoothArgs<R> A) {
 }
 
 // ------------------------------------------------------------------------------------------
-// The coarse levels [sb, nl) in one block with shared memory (bottomsolve_gpu,
-// HpMultiGrid.cpp:854-1040): down with 4 sweeps + residual + restriction per level, 16 sweeps
-// on the coarsest level, up with interpolation + 4 sweeps. The coefficient of the levels below
-// sb is restricted here as well (average_down_acoef, :1640-1700).
+// The coarse levels [sb, nl) in one block with shared memory, for one or both components
+// (bottomsolve_gpu, HpMultiGrid.cpp:854-1040): down with 4 sweeps + residual + restriction per
+// level, max(16, longest side) sweeps on the coarsest level, up with interpolation + 4 sweeps.
+// The coefficient of the levels below sb is restricted here as well (average_down_acoef,
+// :1640-1700).
 // ------------------------------------------------------------------------------------------
 struct MGCoarse {
     int nl;
