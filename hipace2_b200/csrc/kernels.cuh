@@ -87,8 +87,8 @@ struct Ctl {
     int pc_iter, pc_go, pc_mixnow, pc_pad;
     unsigned int pc_cnt[2];  // arrivals of the blocks of the norm and mix kernels (last block decides)
     // persistent multigrid solve (one cooperative launch): |rhs| max, residual norms by
-    // iteration parity and the grid barrier {arrivals, generation}, cleared before every solve;
-    // the barrier's timeout flag, cleared when a step begins
+    // iteration parity and the grid barrier's arrival counter (mgp_bar[0]; [1] unused), cleared
+    // before every solve; the barrier's timeout flag, cleared when a step begins
     double mgp_rhsnorm, mgp_norm[2];
     unsigned int mgp_bar[2];
     int mgp_bar_err, mgp_pad;

@@ -751,36 +751,30 @@ __device__ __forceinline__ unsigned long long tc_clock_ns() {
     return t;
 }
 
-// Grid-wide barrier for a cooperative launch (all blocks co-resident). Arrival is one
-// acquire-release atomic per block; the last block to arrive resets the counter and bumps the
-// generation word with a release, the others poll it with acquire loads. Bounded: a block that
-// polls longer than kBarrierSpins, or sees the error flag, sets the flag and returns false;
-// every block then leaves the kernel at its next barrier.
+// Grid-wide barrier for a cooperative launch (all blocks co-resident). Arrival is one release
+// reduction per block on a counter that only grows during a solve (cleared before every
+// launch): a block's n-th barrier is passed once the counter reaches n x (blocks in the grid),
+// which the waiting blocks read from the counter itself with acquire loads, so the last block to
+// arrive has nothing more to publish. Bounded: a block that polls longer than kBarrierSpins, or
+// sees the error flag, sets the flag and returns false; every block then leaves the kernel at
+// its next barrier. `seq` counts the barriers this block has passed (thread 0's copy is used).
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, int* err) {
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, int* err, unsigned int& seq) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile int* verr = err;
-        const unsigned int g = ld_acquire(bar + 1);
-        unsigned int arrived;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
-        if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
-            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
-        } else {
-            // poll without sleeping first (a barrier is released within a few microseconds),
-            // then with short sleeps
-            long long it = 0;
-            while (ld_acquire(bar + 1) == g) {
-                if (*verr) break;
-                if (++it > kBarrierSpins) { atomicExch(err, 1); break; }
-                if (it > kBarrierFastSpins) __nanosleep(32);
-            }
+        const unsigned int target = ++seq * (gridDim.x * gridDim.y * gridDim.z);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+        long long it = 0;
+        while (ld_acquire(bar) < target) {
+            if (*verr) break;
+            if (++it > kBarrierSpins) { atomicExch(err, 1); break; }
+            if (it > kBarrierFastSpins) __nanosleep(32);
         }
         s_ok = (*verr == 0);
     }
@@ -1045,8 +1039,9 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
     const bool refine = kRefinable && P.refine != 0;  // FP64 refinement of level 0 (tight tolerances)
     const bool split = (T0 != 16 && !kFloat) || P.split0 != 0;
     Ctl* ctl = P.ctl;
-    unsigned int* bar = ctl->mgp_bar;
+    unsigned int* bar = ctl->mgp_bar;  // arrivals (mgp_bar[1] unused)
     int* err = &ctl->mgp_bar_err;
+    unsigned int bseq = 0;  // grid barriers passed
     const int nb = gridDim.x;
     // trace: [0] count, [1..127] block 0 after each grid barrier; [128] count, [129..255] the
     // moment the phase's work of block 2, the first tile block, is done
@@ -1114,7 +1109,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             atomic_max_nonneg(&ctl->mgp_rhsnorm, brhs);
         }
     }
-    if (!grid_barrier(bar, err)) return;
+    if (!grid_barrier(bar, err, bseq)) return;
     stamp();
     if (threadIdx.x == 0) {
         const double r0 = atomic_read(&ctl->mgp_norm[0]), m0 = atomic_read(&ctl->mgp_rhsnorm);
@@ -1146,7 +1141,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                     mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (it == 0) restrict_acf(l + 1);
             wstamp(2);
-            if (!grid_barrier(bar, err)) return;
+            if (!grid_barrier(bar, err, bseq)) return;
             stamp();
         }
         if constexpr (TB) {
@@ -1174,7 +1169,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                         else mg_smooth_tile<R, CELL, 16, MG_INIT_VIEW, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
                     }
                 }
-                if (ph + 1 < nph && !grid_barrier(bar, err)) return;
+                if (ph + 1 < nph && !grid_barrier(bar, err, bseq)) return;
             }
         } else if (blockIdx.x < 2) {
             // levels sb .. nl-1: component c in block c (the components share the operator and
@@ -1186,7 +1181,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                                                (P.trace && c == 0) ? P.trace + 256 : nullptr);
         }
         wstamp(2);
-        if (!grid_barrier(bar, err)) return;
+        if (!grid_barrier(bar, err, bseq)) return;
         stamp();
         // up: levels sb-1 .. 1, interpolation of the coarser correction + 4 sweeps
         for (int l = P.sb - 1; l >= 1; --l) {
@@ -1208,7 +1203,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 for (int t = tb; tile_block && t < nt; t += ntb)
                     mg_smooth_tile<R, CELL, 16, MG_INIT_INTERP, false, false, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             wstamp(2);
-            if (!grid_barrier(bar, err)) return;
+            if (!grid_barrier(bar, err, bseq)) return;
             stamp();
         }
         // level 0, split form (double precision on large grids): interpolation + 4 up-sweeps
@@ -1243,7 +1238,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 }
                 wstamp(2);
             }
-            if (!grid_barrier(bar, err)) return;
+            if (!grid_barrier(bar, err, bseq)) return;
             stamp();
             {
                 int ntx;
@@ -1296,7 +1291,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             if (threadIdx.x == 0) atomic_max_nonneg(&ctl->mgp_norm[(it + 1) & 1], bmax);
             wstamp(2);
         }
-        if (!grid_barrier(bar, err)) return;
+        if (!grid_barrier(bar, err, bseq)) return;
         stamp();
         ++it;
         if (threadIdx.x == 0) {
