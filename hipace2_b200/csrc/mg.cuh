@@ -532,6 +532,55 @@ __device__ __forceinline__ void coarse_sweeps(const CoarseLevel<R>& A, int nswee
     }
 }
 
+// The colour sweeps of a level of at most 32 valid points in warp 0 with the values in
+// registers: lane k holds valid point k (row-major in the valid box) and reads its neighbours of
+// the other colour with shuffles, or from the arena where a neighbour lies outside the valid box
+// (those values do not change during the sweeps). The same point updates in the same order of
+// colours as coarse_sweeps, so the values are the same; the result goes back to the arena. Call
+// with all 32 lanes of warp 0.
+template <class R, bool CELL, int NC>
+__device__ __forceinline__ void coarse_sweeps_lanes(const CoarseLevel<R>& A, int nsweeps) {
+    const MGLev& L = A.L;
+    const int plane = L.w * L.h;
+    const int lane = threadIdx.x & 31;
+    const int vw = L.vhi_i - L.vlo + 1, np = vw * (L.vhi_j - L.vlo + 1);
+    const bool mine = lane < np;
+    const int k = mine ? lane : 0;
+    const int i = L.vlo + k % vw, j = L.vlo + k / vw;
+    const int id = j * L.w + i;
+    const int im = i > 0 ? id - 1 : id, ip = i < L.w - 1 ? id + 1 : id;
+    const int jm = j > 0 ? id - L.w : id, jp = j < L.h - 1 ? id + L.w : id;
+    // neighbour inside the valid box: the lane holding it, else -1 (value from the arena)
+    const int lm = (i - 1 >= L.vlo && im != id) ? k - 1 : -1, lp = (i + 1 <= L.vhi_i && ip != id) ? k + 1 : -1;
+    const int ljm = (j - 1 >= L.vlo && jm != id) ? k - vw : -1, ljp = (j + 1 <= L.vhi_j && jp != id) ? k + vw : -1;
+    const R inv = A.dinv[id];
+    R v[NC], r[NC], em[NC], ep[NC], ejm[NC], ejp[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const R* p = A.cor + q * plane;
+        v[q] = p[id];
+        r[q] = A.res[q * plane + id];
+        em[q] = p[im]; ep[q] = p[ip]; ejm[q] = p[jm]; ejp[q] = p[jp];
+    }
+    for (int s = 0; s < nsweeps; ++s) {
+        const bool upd = mine && ((i + j + s) & 1) == 0;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            const R a = __shfl_sync(0xffffffffu, v[q], lm < 0 ? lane : lm);
+            const R b = __shfl_sync(0xffffffffu, v[q], lp < 0 ? lane : lp);
+            const R c = __shfl_sync(0xffffffffu, v[q], ljm < 0 ? lane : ljm);
+            const R d = __shfl_sync(0xffffffffu, v[q], ljp < 0 ? lane : ljp);
+            const R nv = mg_gs_inv<R, CELL>(L, i, j, lm < 0 ? em[q] : a, lp < 0 ? ep[q] : b, ljm < 0 ? ejm[q] : c,
+                                            ljp < 0 ? ejp[q] : d, r[q], inv, A.facx, A.facy);
+            if (upd) v[q] = nv;
+        }
+    }
+    if (mine) {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) A.cor[q * plane + id] = v[q];
+    }
+}
+
 // 4 sweeps, the residual, and its restriction into the next level's right-hand side
 template <class G, class R, bool CELL, int NC>
 __device__ __forceinline__ void coarse_down(const CoarseLevel<R>& A, const CoarseLevel<R>& C) {
@@ -661,8 +710,19 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         bstamp();
     }
     if (lw >= M.nl - 1 && lw == M.nl) {
-        if (M.ns_bottom == 16) coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), 16);
-        else coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
+        const MGLev& Lc = M.L[M.nl - 1];
+        if (sizeof(R) == 8 && NC == 1 && (Lc.vhi_i - Lc.vlo + 1) * (Lc.vhi_j - Lc.vlo + 1) <= 32) {
+            // a coarsest level of at most 32 points: its sweeps in registers of warp 0 (double
+            // precision in the persistent solve; the single-precision kernels keep the block form,
+            // which fits their register budget, and so does the multi-kernel form, against which
+            // the persistent solve is checked bit for bit)
+            if (threadIdx.x < 32) coarse_sweeps_lanes<R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
+            __syncthreads();
+        } else if (M.ns_bottom == 16) {
+            coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), 16);
+        } else {
+            coarse_sweeps<BlockGroup, R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
+        }
         bstamp();
     } else {
         if (threadIdx.x < 32) {
