@@ -641,7 +641,9 @@ __device__ __forceinline__ unsigned long long tc_clock_ns();
 // end: bt[0] = count, bt[1..]
 // NC = 2: both components (res_g, cor_g: two planes of the first level); NC = 1: one component
 // (res_g, cor_g point at its plane), the other one solved by another block
-template <class R, bool CELL, bool GA = false, int NC = 2>
+// LANES: a coarsest level of at most 32 points is swept in registers of warp 0
+// (coarse_sweeps_lanes) instead of by the block
+template <class R, bool CELL, bool GA = false, int NC = 2, bool LANES = false>
 __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_g, const R* acf_g, R* cor_g, R facx0,
                                                 R facy0, unsigned char* smem_raw, bool init,
                                                 unsigned long long* bt = nullptr) {
@@ -711,11 +713,8 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
     }
     if (lw >= M.nl - 1 && lw == M.nl) {
         const MGLev& Lc = M.L[M.nl - 1];
-        if (sizeof(R) == 8 && NC == 1 && (Lc.vhi_i - Lc.vlo + 1) * (Lc.vhi_j - Lc.vlo + 1) <= 32) {
-            // a coarsest level of at most 32 points: its sweeps in registers of warp 0 (double
-            // precision in the persistent solve; the single-precision kernels keep the block form,
-            // which fits their register budget, and so does the multi-kernel form, against which
-            // the persistent solve is checked bit for bit)
+        if (LANES && (Lc.vhi_i - Lc.vlo + 1) * (Lc.vhi_j - Lc.vlo + 1) <= 32) {
+            // a coarsest level of at most 32 points: its sweeps in registers of warp 0
             if (threadIdx.x < 32) coarse_sweeps_lanes<R, CELL, NC>(arena_level(M.nl - 1), M.ns_bottom);
             __syncthreads();
         } else if (M.ns_bottom == 16) {
@@ -1236,7 +1235,10 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             // are coupled only through the norms, which are taken on level 0)
             const int c = (int)blockIdx.x;
             const size_t nsb = (size_t)P.lev[P.sb].w * P.lev[P.sb].h;
-            mg_bottom_block<R, CELL, false, 1>(P.coarse, P.res[P.sb] + c * nsb, P.acf[P.sb], P.cor[P.sb] + c * nsb,
+            // (the lane form in every persistent kernel but the single-precision 32^2 one, which
+            // has no registers to spare; the multi-kernel form keeps the block form, and the
+            // persistent solve is checked against it)
+            mg_bottom_block<R, CELL, false, 1, (sizeof(R) == 8 || T0 == 16)>(P.coarse, P.res[P.sb] + c * nsb, P.acf[P.sb], P.cor[P.sb] + c * nsb,
                                                P.facx[P.sb], P.facy[P.sb], smem_raw, it == 0,
                                                (P.trace && c == 0) ? P.trace + 256 : nullptr);
         }
