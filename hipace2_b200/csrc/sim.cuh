@@ -417,6 +417,9 @@ public:
         if (bin_key) cudaFree(bin_key);
         if (bin_hist) cudaFree(bin_hist);
         if (bin_total) cudaFree(bin_total);
+        if (valid_h) cudaFreeHost(valid_h);
+        valid_h = nullptr;
+        valid_cap = valid_n = 0;
         bin_key = bin_hist = nullptr;
         bin_total = nullptr;
         bin_key_cap = bin_hist_cap = 0;
@@ -1037,11 +1040,22 @@ public:
     // particles of the current store in slice-descending order; invalid particles (absorbed at a
     // boundary, removed by SALAME) are reported with weight 0, which hpq_set_beam reads back as
     // invalid
-    std::vector<uint8_t> valid_h;
+    // validity flags of the last read-back (pinned, so that their copy is a plain DMA)
+    uint8_t* valid_h = nullptr;
+    long long valid_cap = 0, valid_n = 0;
     void get_beam(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
                   long long* id) override {
         get_beam_raw(b, x, y, z, w, ux, uy, uz, id);
-        for (long long k = 0; k < (long long)valid_h.size(); ++k)
+        // eight flags at a time: runs of valid particles (flag 1) are skipped with one compare
+        long long k = 0;
+        for (; k + 8 <= valid_n; k += 8) {
+            uint64_t q;
+            std::memcpy(&q, valid_h + k, 8);
+            if (q == 0x0101010101010101ull) continue;
+            for (int t = 0; t < 8; ++t)
+                if (!valid_h[k + t]) w[k + t] = 0.0;
+        }
+        for (; k < valid_n; ++k)
             if (!valid_h[k]) w[k] = 0.0;
     }
     void get_beam_raw(int b, double* x, double* y, double* z, double* w, double* ux, double* uy, double* uz,
@@ -1061,14 +1075,21 @@ public:
             if (cnt[sl] && start[sl] != start[nz - 1] + total) contiguous = false;
             total += cnt[sl];
         }
-        valid_h.resize(total);
+        if (total > valid_cap) {
+            if (valid_h) HPQ_CUDA(cudaFreeHost(valid_h));
+            valid_h = nullptr;
+            valid_cap = 0;
+            HPQ_CUDA(cudaMallocHost(&valid_h, (size_t)total));
+            valid_cap = total;
+        }
+        valid_n = total;
         if (contiguous) {
             if (total > 0) {
                 const size_t o = start[nz - 1];
                 for (int a = 0; a < 7; ++a)
                     HPQ_CUDA(cudaMemcpyAsync(outs[a], ins[a] + o, total * sizeof(double), cudaMemcpyDeviceToHost, st));
                 if (id) HPQ_CUDA(cudaMemcpyAsync(id, s.id + o, total * sizeof(long long), cudaMemcpyDeviceToHost, st));
-                HPQ_CUDA(cudaMemcpyAsync(valid_h.data(), s.valid + o, total, cudaMemcpyDeviceToHost, st));
+                HPQ_CUDA(cudaMemcpyAsync(valid_h, s.valid + o, total, cudaMemcpyDeviceToHost, st));
                 HPQ_CUDA(cudaStreamSynchronize(st));
             }
             return;
@@ -1079,7 +1100,7 @@ public:
             if (!n) continue;
             for (int a = 0; a < 7; ++a) HPQ_CUDA(cudaMemcpy(outs[a] + k, ins[a] + o, n * sizeof(double), cudaMemcpyDeviceToHost));
             if (id) HPQ_CUDA(cudaMemcpy(id + k, s.id + o, n * sizeof(long long), cudaMemcpyDeviceToHost));
-            HPQ_CUDA(cudaMemcpy(valid_h.data() + k, s.valid + o, n, cudaMemcpyDeviceToHost));
+            HPQ_CUDA(cudaMemcpy(valid_h + k, s.valid + o, n, cudaMemcpyDeviceToHost));
             k += n;
         }
     }
