@@ -641,6 +641,55 @@ __device__ __forceinline__ unsigned long long tc_clock_ns();
 // end: bt[0] = count, bt[1..]
 // NC = 2: both components (res_g, cor_g: two planes of the first level); NC = 1: one component
 // (res_g, cor_g point at its plane), the other one solved by another block
+// Coefficient hierarchy of the coarse levels in a bottom block's arena (NC components per
+// level): from the coefficient of the first coarse level, already in acf(0) (the rest of the
+// arena zero), the restrictions to the coarser levels (average_down_acoef, :1640-1700) and the
+// inverse diagonals of every level.
+template <class R, bool CELL, int NC>
+__device__ __forceinline__ void mg_coarse_coef(const MGCoarse& M, R* arena, R facx0, R facy0) {
+    auto nn = [&](int l) { return (size_t)M.L[l].w * M.L[l].h; };
+    auto acf = [&](int l) { return arena + (3 * NC + 2) * M.poff[l] + 3 * NC * nn(l); };
+    auto dinv = [&](int l) { return arena + (3 * NC + 2) * M.poff[l] + (3 * NC + 1) * nn(l); };
+    for (int l = 1; l < M.nl; ++l) {
+        const MGLev& C = M.L[l];
+        MV<R> fine{{acf(l - 1), acf(l - 1)}, M.L[l - 1].w, 0};
+        for_valid(C, [&](int i, int j) { acf(l)[j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, 0); });
+        __syncthreads();
+    }
+    R fx = facx0, fy = facy0;
+    for (int l = 0; l < M.nl; ++l) {
+        const MGLev& L = M.L[l];
+        for_valid(L, [&](int i, int j) {
+            dinv(l)[j * L.w + i] = mg_diag_inv<R, CELL>(L, i, j, acf(l)[j * L.w + i], fx, fy);
+        });
+        fx *= R(0.25);
+        fy *= R(0.25);
+    }
+}
+
+// The same hierarchy built ahead of the first bottom solve of a persistent solve, by a bottom
+// block during the phase before it: the first coarse level's coefficient is restricted here from
+// the finer level's `fine` (the same restriction, on the same values, as the grid-wide one that
+// writes it to global memory in that phase).
+template <class R, bool CELL, int NC>
+__device__ __forceinline__ void mg_bottom_prebuild(const MGCoarse& M, const MV<R>& fine, R facx0, R facy0,
+                                                   unsigned char* smem_raw) {
+    __syncthreads();
+    R* arena = reinterpret_cast<R*>(smem_raw);
+    for (int l = 0; l < M.nl; ++l) {
+        const int n = M.L[l].w * M.L[l].h;
+        R* a = arena + (3 * NC + 2) * M.poff[l];
+        for (int k = threadIdx.x; k < (3 * NC + 2) * n; k += blockDim.x) a[k] = R(0);
+    }
+    __syncthreads();
+    const MGLev& C = M.L[0];
+    R* acf0 = arena + 3 * NC * (size_t)C.w * C.h;
+    for_valid(C, [&](int i, int j) { acf0[j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, 0); });
+    __syncthreads();
+    mg_coarse_coef<R, CELL, NC>(M, arena, facx0, facy0);
+    __syncthreads();
+}
+
 // LANES: a coarsest level of at most 32 points is swept in registers of warp 0
 // (coarse_sweeps_lanes) instead of by the block
 template <class R, bool CELL, bool GA = false, int NC = 2, bool LANES = false>
@@ -673,21 +722,7 @@ __device__ __forceinline__ void mg_bottom_block(const MGCoarse& M, const R* res_
         for (int k = threadIdx.x; k < n0; k += blockDim.x) acf(0)[k] = acf_g[k];
         __syncthreads();
         // coefficient hierarchy below sb
-        for (int l = 1; l < M.nl; ++l) {
-            const MGLev& C = M.L[l];
-            MV<R> fine{{acf(l - 1), acf(l - 1)}, M.L[l - 1].w, 0};
-            for_valid(C, [&](int i, int j) { acf(l)[j * C.w + i] = mg_restrict1<R, CELL>(fine, i, j, 0); });
-            __syncthreads();
-        }
-        R fx = facx0, fy = facy0;
-        for (int l = 0; l < M.nl; ++l) {
-            const MGLev& L = M.L[l];
-            for_valid(L, [&](int i, int j) {
-                dinv(l)[j * L.w + i] = mg_diag_inv<R, CELL>(L, i, j, acf(l)[j * L.w + i], fx, fy);
-            });
-            fx *= R(0.25);
-            fy *= R(0.25);
-        }
+        mg_coarse_coef<R, CELL, NC>(M, arena, facx0, facy0);
     } else {
         for (int l = 0; l < M.nl; ++l) {
             const int n = M.L[l].w * M.L[l].h;
@@ -1145,6 +1180,18 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             crse(i, j, 0) = mg_restrict1<R, CELL>(fine, i, j, 0);
         }
     };
+    // the bottom blocks build their coefficient hierarchy in the phase before the first bottom
+    // solve (they have no tiles there): from the coefficient of level sb - 1, written grid-wide in
+    // the phase before that (level 0's is an input)
+    auto prebuild = [&]() {
+        if constexpr (!TB) {
+            if (blockIdx.x < 2) {
+                const int l = P.sb - 1;
+                const MV<R> fine = (l == 0) ? P.a0 : mg_own<R>(P.acf, P.lev, l, 1);
+                mg_bottom_prebuild<R, CELL, 1>(P.coarse, fine, P.facx[P.sb], P.facy[P.sb], smem_raw);
+            }
+        }
+    };
     double bmax = 0, brhs = 0;
     // ---- first smoothing of level 0 (residual, restriction, norms) and the level-1 coefficient
     {
@@ -1162,6 +1209,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 mg_smooth_tile<R, CELL, T0, MG_INIT_VIEW, true, true, MG_NORM_FIRST, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
         }
         restrict_acf(1);
+        if (P.sb == 1) prebuild();
         block_max2(bmax, brhs);
         if (threadIdx.x == 0) {
             atomic_max_nonneg(&ctl->mgp_norm[0], bmax);
@@ -1199,6 +1247,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
                 for (int t = tb; tile_block && t < nt; t += ntb)
                     mg_smooth_tile<R, CELL, 16, MG_INIT_ZERO, true, true, MG_NORM_NONE, 4>(a, t % ntx, t / ntx, false, smem_raw, bmax, brhs);
             if (it == 0) restrict_acf(l + 1);
+            if (it == 0 && l == P.sb - 1) prebuild();
             wstamp(2);
             if (!grid_barrier(bar, err, bseq)) return;
             stamp();
@@ -1239,7 +1288,7 @@ __global__ void __launch_bounds__(256, 2) k_mg_solve(MGSolveArgs<R> P) {
             // has no registers to spare; the multi-kernel form keeps the block form, and the
             // persistent solve is checked against it)
             mg_bottom_block<R, CELL, false, 1, (sizeof(R) == 8 || T0 == 16)>(P.coarse, P.res[P.sb] + c * nsb, P.acf[P.sb], P.cor[P.sb] + c * nsb,
-                                               P.facx[P.sb], P.facy[P.sb], smem_raw, it == 0,
+                                               P.facx[P.sb], P.facy[P.sb], smem_raw, false,
                                                (P.trace && c == 0) ? P.trace + 256 : nullptr);
         }
         wstamp(2);
